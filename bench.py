@@ -1,0 +1,303 @@
+"""Benchmark: molecule-pair energies per second of erdst's refs-mode frame.
+
+One step = one engconst frame of the refs workload "refs-ring12-water4096":
+4,096 rigid 3-site waters in a 49.6 A box, a 12-site benzene-like test
+particle inserted 2,000 times (uniform position + orientation), PME 64^3
+order 4, ecorr on.  Units = insertions x solvent molecules = 8.19e6 per step.
+
+  value  device time of K steps (CUDA events on the engine's stream, inputs
+         resident in HBM), L2 flushed (256 MiB write) before every step
+  e2e    the same K steps through the host C-ABI (ermod_engconst with host
+         coordinates, H2D inside) plus a D2H read of edens each step, host
+         wall time of the synchronous calls
+  --impl reference   the reference's algorithm on the host cores (the CPU
+         restatement under oracle/: brute-force pairs, one PME solve per
+         insertion, binary-search binning, per-insertion ecorr update)
+
+Multi-GPU (torchrun): frames are independent, each rank runs its own
+frames with no collective in the step (weak scaling); the max device time
+over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIG = 2
+METRIC = "mol-pair energies/s"
+UNIT = "mol-pairs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--maxins", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=500, help="insertions per CPU reference step")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = [r.split(", ") for r in self.out.strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int, maxdst: int) -> float:
+    """Algorithmic DRAM bytes of ONE launch of each of the engine's kernels."""
+    K = w.params["ms1max"]
+    n = w.params["splodr"]
+    KK, KH = K ** 3, K * K * (K // 2 + 1)
+    if stage == "gather_bin":   # potential grid once + real-space energies + splines + count increments
+        return chunk * KK * 4 + slvmax * chunk * 8 + natoms * (12 * n + 16) + slvmax * chunk * 4
+    if stage == "influence":    # spectrum read + write, influence function read
+        return chunk * KH * 8 * 2 + KH * 4
+    if stage == "spread":       # zero + scatter of the charge grids
+        return chunk * KK * 4
+    if stage == "real":         # solvent coordinates + real-space energy matrix write
+        return natoms * 16 + slvmax * chunk * 8
+    if stage == "ecorr":        # counts read twice + ecorr read-modify-write
+        return 2 * maxdst * ermax * 4 + 16 * ermax * ermax
+    return 0.0
+
+
+def traffic_from_profiles(kernel: str):
+    """dram bytes per launch of `kernel` from profiles/ncu_traffic.txt (written from an ncu capture)."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) >= 2 and not line.startswith("#") and f[0] == kernel:
+            return float(f[1])
+    return None
+
+
+def cpu_baseline(w, sample: int, threads: int):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the reference's algorithm restated on the CPU (the checker)
+    prm = dict(w.params, maxins=sample)
+    orc = oracle.Oracle(prm, w.topo, w.hist, precision=4, nthreads=threads)
+    pos, cell = w.frame(0)
+    orc.engconst(1, pos, cell)     # warm
+    t0 = time.perf_counter()
+    orc.engconst(2, pos, cell)
+    dt = time.perf_counter() - t0
+    units = sample * (w.topo.nummol - 1)
+    return units / dt, dt, units
+
+
+def run_reference(args, w):
+    ws, rank, _ = dist_init()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    prm = dict(w.params, maxins=args.ref_sample)
+    orc = oracle.Oracle(prm, w.topo, w.hist, precision=4, nthreads=threads)
+    frames = [w.frame(i) for i in range(args.warmup + args.steps)]
+    for i in range(args.warmup):
+        orc.engconst(i + 1, *frames[i])
+    t = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        orc.engconst(args.warmup + i + 1, *frames[args.warmup + i])
+        t.append(time.perf_counter() - t0)
+    units = args.ref_sample * (w.topo.nummol - 1)
+    total = sum(t)
+    val = units * args.steps / total
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": w.name, "waters": int(w.topo.nummol - 1), "pme_grid": w.params["ms1max"],
+                       "insertions_per_step": args.ref_sample,
+                       "insertions_per_frame_full": w.params["maxins"]},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.ref_sample} insertions x {w.topo.nummol - 1} waters per step, "
+                                       f"{args.steps} steps, FP32 restatement of the reference algorithm"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    from ermod_openacc_b200 import systems as S
+    w = S.make_workload(CONFIG, maxins=args.maxins)
+    if args.impl == "reference":
+        run_reference(args, w)
+        return
+    import torch
+    ws, rank, local = dist_init()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    import __graft_entry__ as ge
+    if rank == 0:
+        ge.build_engine()
+    if ws > 1:
+        dist.barrier()
+    from ermod_openacc_b200 import Engine
+    eng = Engine(w.params, w.topo, w.hist, device=local)
+    nfr = args.warmup + args.steps
+    frames = [w.frame(rank * nfr + i) for i in range(nfr)]
+    cell = frames[0][1]
+    dev_pos = torch.from_numpy(np.stack([f[0] for f in frames])).to(f"cuda:{local}")
+    host_pos = torch.from_numpy(np.stack([f[0] for f in frames])).pin_memory()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+    units = eng.maxdst * eng.slvmax
+
+    for i in range(args.warmup):
+        eng.engconst_dev(i + 1, dev_pos[i].data_ptr(), cell)
+    torch.cuda.synchronize()
+    launches0 = eng.launch_count()
+    stage = {k: 0.0 for k in Engine.STAGES}
+    dev_ms = 0.0
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            eng.engconst_dev(args.warmup + i + 1, dev_pos[args.warmup + i].data_ptr(), cell)
+            t = eng.timings()
+            dev_ms += t["total"]
+            for k, v in t.items():
+                stage[k] += v
+    torch.cuda.synchronize()
+    launches = eng.launch_count() - launches0
+    if ws > 1:
+        tt = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_ms = float(tt.item())
+        dist.barrier()
+    # e2e: host coordinates in pinned memory -> C-ABI (H2D inside) -> D2H of edens
+    eng2 = eng
+    e2e_s = 0.0
+    edens = None
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng2.engconst(nfr + i + 1, host_pos[args.warmup + i].numpy(), cell)
+        edens = eng2.accum()["edens"]
+        e2e_s += time.perf_counter() - t0
+    if ws > 1:
+        tt = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    assert edens is not None and edens.sum() > 0
+    value = ws * units * args.steps / (dev_ms * 1e-3)
+    e2e = ws * units * args.steps / e2e_s
+    # roofline of the dominant engine kernel (cuFFT's own kernels are library code)
+    ours = ["real", "spread", "influence", "gather_bin", "ecorr"]
+    dom = max(ours, key=lambda k: stage[k])
+    per_frame_launches = {"real": stage["chunks"], "spread": stage["chunks"], "influence": stage["chunks"],
+                          "gather_bin": stage["chunks"], "ecorr": 1.0}
+    n_launch = per_frame_launches[dom]  # summed over steps in `stage`
+    per_launch_ms = stage[dom] / n_launch
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    chunk = 32
+    bytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst)
+    achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
+    kname = {"gather_bin": "k_gather_bin", "real": "k_real", "spread": "k_spread", "influence": "k_influence",
+             "ecorr": "k_ecorr"}[dom]
+    traffic = traffic_from_profiles(kname)
+    stage_share = {k: round(stage[k] / max(stage["total"], 1e-9), 4) for k in Engine.STAGES
+                   if k not in ("total", "chunks")}
+    if rank != 0:
+        if ws > 1:
+            dist.destroy_process_group()
+        return
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name, "waters": int(eng.slvmax), "insertions_per_frame": int(eng.maxdst),
+                       "solute_sites": int(eng.nsite_slt), "pme_grid": w.params["ms1max"],
+                       "pme_order": w.params["splodr"], "ermax": int(eng.ermax),
+                       "l2": "flushed before every step (256 MiB write)",
+                       "parallelism": f"frames sharded over {ws} rank(s), no collective in the step"},
+            "stage_share": stage_share,
+            "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": bytes_launch, "launch_ms": per_launch_ms},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(4 * 3 * eng.natoms + 4 * eng.maxdst),
+                    "d2h_bytes_per_step": int(8 * eng.ermax + 8 * 4 + 4 * 2 * (eng.numslv + 1) + 16)},
+            "gpu_launches": int(launches)}
+    clk_s = clk.summary()
+    if clk_s:
+        line["clocks"] = clk_s
+    if ws == 1 and not args.no_cpu_baseline:
+        v, dt, u = cpu_baseline(w, 2000, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"one frame of 2000 insertions x {u // 2000} waters ({dt:.1f} s), "
+                                          "FP32 restatement of the reference algorithm on all host threads"}
+    print(json.dumps(line))
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,193 @@
+// common.cuh -- device-side building blocks shared by the engine's kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cfloat>
+#include <cstdint>
+
+namespace erm {
+
+constexpr double kPi = 3.1415926535897932;   // erdst/engmain.F90:249
+
+// Normalised periodic cell, the state realcal_prepare / normalize_periodic
+// leave in module realcal (erdst/realcal.F90:22-27, 859-896), plus the
+// inverted raw cell used by the PME splines (engproc.F90:1049-1070).
+struct CellGeom {
+  float cn[3][3];     // cell_normal(i,j): row i, column j
+  float inv[3];       // invcell_normal
+  float len[3];       // cell_len_normal
+  float half[3];      // 0.5 * cell_len_normal
+  float rot[3][3];    // Q of the QR step (applied as Q^T x) when `rotated`
+  float invcl[3][3];  // inverse of the raw cell
+  float cell[3][3];   // raw cell
+  float volume;
+  int rotated, cuboid, periodic;
+};
+
+// Constants of the pair energy of realcal (erdst/realcal.F90:62-96, 131-197).
+struct PairParams {
+  float lw, up, lw2, up2, lw3, up3, lw6, up6;
+  float repA, repB, repC, attA, attB, attC;
+  float reelcut;      // elecut when periodic, FLT_MAX otherwise
+  float screen;
+  int ljswitch;
+  int bare;           // cltype == bare Coulomb (realcal_bare)
+};
+
+// Minimum image of a difference of normalised coordinates (realcal.F90:115-128).
+__device__ __forceinline__ void min_image(const CellGeom& g, float& x, float& y, float& z) {
+  if (!g.periodic) return;
+  if (g.cuboid) {
+    x = g.half[0] - fabsf(g.half[0] - fabsf(x));
+    y = g.half[1] - fabsf(g.half[1] - fabsf(y));
+    z = g.half[2] - fabsf(g.half[2] - fabsf(z));
+  } else {
+    float f = roundf(z * g.inv[2]);
+    x -= g.cn[0][2] * f; y -= g.cn[1][2] * f; z -= g.cn[2][2] * f;
+    f = roundf(y * g.inv[1]);
+    x -= g.cn[0][1] * f; y -= g.cn[1][1] * f; z -= g.cn[2][1] * f;
+    f = roundf(x * g.inv[0]);
+    x -= g.cn[0][0] * f; y -= g.cn[1][0] * f; z -= g.cn[2][0] * f;
+  }
+}
+
+// Lennard-Jones with the four switching forms plus real-space Ewald (or bare)
+// Coulomb for one site pair at squared distance dis2 (realcal.F90:129-197).
+// FP32, as the reference's default build.  erfcf replaces 1-erf (more
+// accurate for large arguments; the difference is below FP32 resolution of
+// the pair energy).
+__device__ __forceinline__ float pair_energy(const PairParams& P, float dis2, float ljeps, float ljsgm2,
+                                             float qq) {
+  const float rst = sqrtf(dis2);
+  float eplj = 0.0f;
+  if (!(rst > P.up)) {
+    const float invr2 = ljsgm2 / dis2;
+    const float invr6 = invr2 * invr2 * invr2;
+    if (P.ljswitch <= 1) {
+      eplj = 4.0f * ljeps * invr6 * (invr6 - 1.0f);
+      if (rst > P.lw) {
+        float swth;
+        if (P.ljswitch == 0) {
+          const float d = P.up2 - P.lw2;
+          const float e = dis2 - P.up2;
+          swth = (2.0f * dis2 + P.up2 - 3.0f * P.lw2) * (e * e) / (d * d * d);
+        } else {
+          const float s = (rst - P.lw) / (P.up - P.lw);
+          const float s3 = s * s * s;
+          swth = 1.0f - 10.0f * s3 + 15.0f * (s3 * s) - 6.0f * (s3 * s * s);
+        }
+        eplj = swth * eplj;
+      }
+    } else if (P.ljswitch == 2) {
+      const float ljsgm6 = ljsgm2 * ljsgm2 * ljsgm2;
+      float vdwa, vdwb;
+      if (rst <= P.lw) {
+        vdwa = invr6 * invr6 - ljsgm6 * ljsgm6 / (P.lw6 * P.up6);
+        vdwb = invr6 - ljsgm6 / (P.lw3 * P.up3);
+      } else {
+        const float invr3 = sqrtf(invr6), ljsgm3 = sqrtf(ljsgm6);
+        const float a = invr6 - ljsgm6 / P.up6, b = invr3 - ljsgm3 / P.up3;
+        vdwa = P.up6 / (P.up6 - P.lw6) * (a * a);
+        vdwb = P.up3 / (P.up3 - P.lw3) * (b * b);
+      }
+      eplj = 4.0f * ljeps * (vdwa - vdwb);
+    } else {
+      const float ljsgm6 = ljsgm2 * ljsgm2 * ljsgm2;
+      float vdwa, vdwb;
+      if (rst <= P.lw) {
+        vdwa = invr6 * invr6 - ljsgm6 * ljsgm6 * P.repC;
+        vdwb = invr6 - ljsgm6 * P.attC;
+      } else {
+        const float s = rst - P.lw, s3 = s * s * s, s4 = s3 * s;
+        vdwa = invr6 * invr6 - ljsgm6 * ljsgm6 * (P.repA * s3 + P.repB * s4 + P.repC);
+        vdwb = invr6 - ljsgm6 * (P.attA * s3 + P.attB * s4 + P.attC);
+      }
+      eplj = 4.0f * ljeps * (vdwa - vdwb);
+    }
+  }
+  float epcl = 0.0f;
+  if (rst < P.reelcut) epcl = P.bare ? qq / rst : qq * erfcf(P.screen * rst) / rst;
+  return eplj + epcl;
+}
+
+// Philox4x32-10 (Salmon et al., SC'11); the insertion stream is keyed by
+// (iseed, "ERMD") with counter (insertion, stnum, attempt, purpose).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) { k.x += 0x9E3779B9u; k.y += 0xBB67AE85u; }
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+  }
+  return c;
+}
+__device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+constexpr uint32_t kStreamTag = 0x45524D44u;
+
+// Cardinal B-spline M_n(x) (erdst/spline.F90:25-58); coeff[i] = (-1)^i n / (i!(n-i)!).
+__device__ __forceinline__ float spline_value(const float* coeff, int order, float x) {
+  float f = 0.0f;
+  if (x > 0.0f && x < (float)order) {
+    const int k = (int)x;
+    for (int i = 0; i <= k; ++i) {
+      const float d = x - (float)i;
+      float pw = 1.0f;
+      for (int e = 0; e < order - 1; ++e) pw *= d;
+      f += coeff[i] * pw;
+    }
+  }
+  return f;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+// float atomics through the ordered integer images of IEEE floats
+__device__ __forceinline__ void atomic_min_f(float* a, float v) {
+  if (v >= 0.0f) atomicMin((int*)a, __float_as_int(v));
+  else atomicMax((unsigned int*)a, __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_f(float* a, float v) {
+  if (v >= 0.0f) atomicMax((int*)a, __float_as_int(v));
+  else atomicMin((unsigned int*)a, __float_as_uint(v));
+}
+
+// Device error word bits (set by kernels, read by the host after a frame).
+enum : int {
+  kErrEngMin = 1,     // eng_min
+  kErrEngSft = 2,     // eng_sft
+  kErrEngCns = 4,     // eng_cns
+  kWarnMbin = 8,      // mbin warning
+  kErrOverflow = 16,  // internal capacity exceeded
+  kErrGrid = 32,      // a PME grid index outside the grid
+};
+
+struct DevStatus {
+  int flags;
+  int first_bad_mol;
+  int first_bad_ins;
+  float first_bad_value;
+};
+
+__device__ __forceinline__ void report(DevStatus* st, int bit, int mol, int ins, float v) {
+  const int old = atomicOr(&st->flags, bit);
+  if ((old & bit) == 0) {
+    st->first_bad_mol = mol;
+    st->first_bad_ins = ins;
+    st->first_bad_value = v;
+  }
+}
+
+}  // namespace erm

@@ -1,0 +1,864 @@
+// engine.cu -- C-ABI of the engine: context setup and the per-frame pipeline.
+//
+// One ermod_engconst call runs, on one CUDA stream:
+//   H2D coordinates -> solvent normalisation + splines -> cell list ->
+//   insertion placement -> per chunk of `chunk` targets:
+//     [PME] zero + spread -> cuFFT R2C -> influence multiply / self energy ->
+//           cuFFT C2R into a target-fastest potential grid
+//     real space (cell list) -> gather + residual + binning (integer atomics)
+//   per batch of targets: weights -> edens -> ecorr
+// and reads one status word back.  See kernels.cu for the kernel map to the
+// reference routines.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.cuh"
+
+using namespace erm;
+
+#define CK(x)                                                   \
+  do {                                                          \
+    cudaError_t e_ = (x);                                       \
+    if (e_ != cudaSuccess) {                                    \
+      ctx->err = std::string("cuda: ") + cudaGetErrorString(e_); \
+      return ERMOD_ERR_CUDA;                                    \
+    }                                                           \
+  } while (0)
+
+#define CF(x)                                              \
+  do {                                                     \
+    cufftResult r_ = (x);                                  \
+    if (r_ != CUFFT_SUCCESS) {                             \
+      ctx->err = "cufft error " + std::to_string((int)r_); \
+      return ERMOD_ERR_CUDA;                               \
+    }                                                      \
+  } while (0)
+
+// Engine extensions declared in ecorr_tc.cu
+namespace erm {
+int ecorr_tc_available();
+int launch_ecorr_tc(const DeviceState& d, int base, int n, int ermax, int ermax_pad, int count_base,
+                    int weight_bits, void* work, size_t work_bytes, cudaStream_t s);
+size_t ecorr_tc_workspace(int n, int ermax);
+}  // namespace erm
+
+struct ermod_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[9] = {};
+  ermod_params p{};
+  // host topology
+  int nummol = 0, numatm = 0, natoms = 0, slvmax = 0, numslt = 0, s = 0, maxdst = 0;
+  int numslv = 0, ermax = 0, esmax = 0, ermax_pad = 0;
+  int ljtype_max = 0;
+  std::vector<int> numsite, sluvid, uvspec, tagpt, sltlist, molbeg_all, tgt_k;
+  std::vector<float> charge, mass;
+  double qslt_refs = 0.0;
+  std::vector<double> uvcrd, escrd;
+  std::vector<int> uvmax, uvsoft;
+  DeviceState d;
+  int chunk = 32, batch = 0, ncell_cap = 0;
+  cufftHandle r2c = 0, c2r = 0;
+  bool plans = false;
+  void* tc_work = nullptr;
+  size_t tc_work_bytes = 0;
+  // reference state carried between frames
+  float invcell_prev[3] = {0.f, 0.f, 0.f};
+  float prevcl[9] = {0};
+  bool pme_init = false, usreal_init = false, warn_bin_firsttime = true;
+  float spl_coeff[kMaxOrder + 1] = {0};
+  float* h_pin = nullptr;
+  size_t h_pin_bytes = 0;
+  std::string err;
+  // stage timing: events recorded on the stream between stages, read once per frame
+  std::vector<cudaEvent_t> pev;
+  std::vector<int> ptag;
+  int pused = 0;
+  float timings[12] = {0};
+  long long launches = 0;
+  int use_tc = 1;
+};
+
+enum Stage { kStPrep = 1, kStIns = 2, kStReal = 3, kStSpread = 4, kStR2C = 5, kStInfl = 6, kStC2R = 7,
+             kStGather = 8, kStWeights = 9, kStEcorr = 10 };
+
+namespace {
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n) {
+  if (n == 0) n = 1;
+  return cudaMalloc((void**)p, n * sizeof(T));
+}
+
+template <class T>
+cudaError_t h2d(T* dst, const T* src, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  return cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+void free_all(ermod_ctx* c) {
+  DeviceState& d = c->d;
+  void* ptrs[] = {d.molbeg, d.molspec, d.molq, d.atom_lj, d.atom_q, d.ljene, d.ljlensq, d.slt_lj, d.slt_q,
+                  d.slt_mass, d.bfcoord, d.uvcrd, d.spec_off, d.uvsoft, d.escrd, d.posraw, d.slvn, d.spl, d.grd,
+                  d.anchor, d.cellof, d.cellcount, d.cellstart, d.molsorted, d.rmol, d.ins_conf, d.insw_in,
+                  d.tgt_raw, d.tgt_n, d.tgt_c, d.tgt_mol, d.selfreal, d.selfrec, d.u0, d.w, d.etot, d.flceng,
+                  d.grid, d.spec, d.phi, d.engfac, d.splfc, d.E, d.uvengy, d.counts, d.edens, d.ecorr, d.eself,
+                  d.slnuv, d.minuv, d.maxuv, d.scal, d.status, c->tc_work};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (c->plans) {
+    cufftDestroy(c->r2c);
+    cufftDestroy(c->c2r);
+  }
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : c->pev)
+    if (e) cudaEventDestroy(e);
+  if (c->h_pin) cudaFreeHost(c->h_pin);
+  if (c->st) cudaStreamDestroy(c->st);
+}
+
+// spline.F90:25-44
+void spline_coeff(int order, float* coeff) {
+  for (int i = 0; i <= order; ++i) {
+    float f = 1.0f;
+    for (int k = 1; k <= i; ++k) f *= (float)k;
+    for (int k = 1; k <= order - i; ++k) f *= (float)k;
+    f = (float)order / f;
+    if (i % 2 == 1) f = -f;
+    coeff[i] = f;
+  }
+}
+
+double spline_value_d(int order, double x) {
+  double c[kMaxOrder + 1];
+  for (int i = 0; i <= order; ++i) {
+    double f = 1.0;
+    for (int k = 1; k <= i; ++k) f *= k;
+    for (int k = 1; k <= order - i; ++k) f *= k;
+    f = order / f;
+    if (i % 2 == 1) f = -f;
+    c[i] = f;
+  }
+  double r = 0.0;
+  if (x > 0.0 && x < order) {
+    const int k = (int)x;
+    for (int i = 0; i <= k; ++i) r += c[i] * std::pow(x - i, order - 1);
+  }
+  return r;
+}
+
+// init_spline_axis (recpcal.F90:97-119) in FP64
+void spline_axis(int K, int order, double* out) {
+  for (int rci = 0; rci < K; ++rci) {
+    double re = 0.0, im = 0.0;
+    for (int spi = 0; spi <= order - 2; ++spi) {
+      const double chr = spline_value_d(order, spi + 1.0);
+      const double a = 2.0 * kPi * (double)(spi * rci) / (double)K;
+      re += chr * std::cos(a);
+      im += chr * std::sin(a);
+    }
+    out[rci] = re * re + im * im;
+  }
+}
+
+int set_error(ermod_ctx* c, int code, const char* name) {
+  c->err = name;
+  return code;
+}
+
+// record a stage boundary: the time since the previous mark belongs to `tag`
+void mark(ermod_ctx* c, int tag) {
+  if (c->pused == (int)c->pev.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->pev.push_back(e);
+    c->ptag.push_back(0);
+  }
+  cudaEventRecord(c->pev[c->pused], c->st);
+  c->ptag[c->pused] = tag;
+  ++c->pused;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ermod_abi_version(void) { return ERMOD_ABI_VERSION; }
+
+// enginit mesh (engproc.F90:171-226, 264-281) for one &hist set shared by all species
+int32_t ermod_enginit_mesh(const ermod_hist* h, int32_t numslv, double* uvcrd, int32_t* uvmax, int32_t* uvsoft,
+                           double* escrd, int32_t* ermax, int32_t* esmax) {
+  if (!h || numslv <= 0) return ERMOD_ERR_ARG;
+  const int rglmax = 5;
+  double ecdmin = h->ecdmin, ecfmns = h->ecfmns, ecdcen = h->ecdcen, eccore = h->eccore, ecdmax = h->ecdmax;
+  const double eclbin = h->eclbin, ecfbin = h->ecfbin, ec0bin = h->ec0bin, finfac = h->finfac;
+  const int pecore = h->pecore;
+  if (pecore == 1) return ERMOD_ERR_ENG_ECD;
+  const double ectmvl = finfac * ecfbin;
+  ecdmin -= ectmvl;
+  ecfmns -= ectmvl;
+  const double ecmns0 = ecdcen - ectmvl, ecpls0 = 2.0 * ecdcen - ecmns0, ecfpls = 2.0 * ecdcen - ecfmns;
+  eccore = eccore + ecfpls - ecdcen;
+  const double v[7] = {ecdmin, ecfmns, ecmns0, ecpls0, ecfpls, eccore, ecdmax};
+  int up[7];
+  up[0] = 1;
+  for (int r = 1; r <= rglmax; ++r) {
+    const double f = (r == 1 || r == 5) ? eclbin : (r == 2 || r == 4) ? ecfbin : ec0bin;
+    const double inc = v[r] - v[r - 1];
+    if (inc < f) return ERMOD_ERR_ENG_ECD;
+    up[r] = up[r - 1] + (int)std::lround(inc / f);
+  }
+  const int pesoft = up[rglmax] - up[0], pemax = pesoft + pecore;
+  up[rglmax + 1] = pemax;
+  std::vector<double> e(std::max(pemax, up[rglmax]) + 2, 0.0);
+  for (int r = 0; r <= rglmax + 1; ++r) e[up[r]] = v[r];
+  const int last = pecore == 0 ? rglmax : rglmax + 1;
+  for (int r = 1; r <= last; ++r) {
+    const int lo = up[r - 1], hi = up[r];
+    const double inc = r <= rglmax ? e[hi] - e[lo] : std::log(e[hi] / e[lo]);
+    const double f = inc / (double)(hi - lo);
+    for (int i = lo; i < hi; ++i) e[i] = r <= rglmax ? e[lo] + f * (i - lo) : e[lo] * std::exp(f * (i - lo));
+  }
+  if (ermax) *ermax = numslv * pemax;
+  if (esmax) *esmax = pesoft;
+  for (int q = 0; q < numslv; ++q) {
+    if (uvmax) uvmax[q] = pemax;
+    if (uvsoft) uvsoft[q] = pesoft;
+    if (uvcrd) for (int i = 0; i < pemax; ++i) uvcrd[(size_t)q * pemax + i] = e[i + 1];
+  }
+  if (escrd) for (int i = 0; i < pesoft; ++i) escrd[i] = e[i + 1];
+  return ERMOD_OK;
+}
+
+int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, const ermod_topology* t,
+                     const ermod_mesh* m) {
+  if (!out || !prm || !t || !m) return ERMOD_ERR_ARG;
+  *out = nullptr;
+  ermod_ctx* ctx = new ermod_ctx();
+  ctx->device = device;
+  ctx->p = *prm;
+  const ermod_params& p = ctx->p;
+  auto bad = [&](int code, const char* name) {
+    ctx->err = name;
+    *out = ctx;
+    return code;
+  };
+  if (p.cltype != ERMOD_EL_PME && p.cltype != ERMOD_EL_COULOMB) return bad(ERMOD_ERR_UNSUPPORTED, "set_prs");
+  if (p.cltype == ERMOD_EL_PME && (p.splodr < 2 || p.splodr > kMaxOrder)) return bad(ERMOD_ERR_ARG, "set_ewa");
+  if (p.boxshp == ERMOD_SYS_NONPERIODIC && (p.estype == ERMOD_ES_NPT || p.cltype != ERMOD_EL_COULOMB))
+    return bad(ERMOD_ERR_ARG, "set_prs");
+  if (p.slttype < 1 || p.slttype > 3) return bad(ERMOD_ERR_ARG, "set_slt");
+  if (p.slttype != ERMOD_SLT_SOLN &&
+      !((p.insposition == ERMOD_INSPOS_RANDOM || p.insposition == ERMOD_INSPOS_NOCHANGE) &&
+        (p.insorient == ERMOD_INSROT_RANDOM || p.insorient == ERMOD_INSROT_NOCHANGE)))
+    return bad(ERMOD_ERR_UNSUPPORTED, "ins_geo");
+  // topology (setparam / enginit / engconst bookkeeping)
+  ctx->nummol = t->nummol;
+  ctx->numsite.assign(t->numsite, t->numsite + t->nummol);
+  ctx->sluvid.assign(t->sluvid, t->sluvid + t->nummol);
+  ctx->uvspec.assign(t->uvspec, t->uvspec + t->nummol);
+  ctx->molbeg_all.resize(ctx->nummol + 1, 0);
+  for (int i = 0; i < ctx->nummol; ++i) ctx->molbeg_all[i + 1] = ctx->molbeg_all[i] + ctx->numsite[i];
+  ctx->numatm = ctx->molbeg_all[ctx->nummol];
+  ctx->charge.assign(t->charge, t->charge + ctx->numatm);
+  ctx->mass.assign(t->sitemass, t->sitemass + ctx->numatm);
+  for (int i = 0; i < ctx->nummol; ++i) {
+    if (ctx->sluvid[i] < 0 || ctx->sluvid[i] > 3) return bad(ERMOD_ERR_ARG, "eng_bug");
+    if (ctx->sluvid[i] == ERMOD_PT_SOLVENT || ctx->sluvid[i] == ERMOD_PT_SOLUTE) ctx->tagpt.push_back(i);
+    if (ctx->sluvid[i] > 0) ctx->sltlist.push_back(i);
+  }
+  ctx->slvmax = (int)ctx->tagpt.size();
+  ctx->numslt = (int)ctx->sltlist.size();
+  if (ctx->numslt <= 0 || ctx->slvmax <= 0) return bad(ERMOD_ERR_ARG, "eng_num");
+  const bool refs = p.slttype != ERMOD_SLT_SOLN;
+  if (refs) {
+    if (ctx->numslt != 1 || ctx->sltlist[0] != ctx->nummol - 1) return bad(ERMOD_ERR_ARG, "eng_ins");
+    for (int i = 0; i < ctx->nummol; ++i) if (ctx->sluvid[i] == ERMOD_PT_SOLUTE) return bad(ERMOD_ERR_ARG, "eng_par");
+    ctx->maxdst = p.maxins;
+    if (ctx->maxdst < 1) return bad(ERMOD_ERR_ARG, "set_ins");
+  } else {
+    for (int i = 0; i < ctx->nummol; ++i) if (ctx->sluvid[i] >= 2) return bad(ERMOD_ERR_ARG, "eng_par");
+    ctx->maxdst = ctx->numslt;
+  }
+  ctx->s = ctx->numsite[ctx->sltlist[0]];
+  for (int i : ctx->sltlist) if (ctx->numsite[i] != ctx->s) return bad(ERMOD_ERR_ARG, "set_slt");
+  if (ctx->s > kMaxSoluteSites) return bad(ERMOD_ERR_OVERFLOW, "ins_siz");
+  ctx->ljtype_max = t->ljtype_max;
+  ctx->numslv = m->numslv;
+  ctx->ermax = m->ermax;
+  ctx->esmax = m->esmax;
+  ctx->uvcrd.assign(m->uvcrd, m->uvcrd + m->ermax);
+  ctx->uvmax.assign(m->uvmax, m->uvmax + m->numslv);
+  ctx->uvsoft.assign(m->uvsoft, m->uvsoft + m->numslv);
+  if (p.selfcal && (!m->escrd || m->esmax <= 0)) return bad(ERMOD_ERR_ARG, "eng_ecd");
+  if (m->escrd && m->esmax > 0) ctx->escrd.assign(m->escrd, m->escrd + m->esmax);
+  for (int i : ctx->tagpt)
+    if (ctx->uvspec[i] < 0 || ctx->uvspec[i] > ctx->numslv) return bad(ERMOD_ERR_ARG, "eng_bug");
+  ctx->ermax_pad = (ctx->ermax + 127) / 128 * 128;
+  {
+    int sum = 0;
+    for (int q = 0; q < ctx->numslv; ++q) sum += ctx->uvmax[q];
+    if (sum != ctx->ermax) return bad(ERMOD_ERR_ARG, "eng_bug");
+  }
+  // tagpt-order physical atoms
+  std::vector<int> molbeg(ctx->slvmax + 1, 0), molspec(ctx->slvmax), atom_lj, tagk(ctx->nummol, -1);
+  std::vector<float> molq(ctx->slvmax), atom_q;
+  for (int k = 0; k < ctx->slvmax; ++k) {
+    const int i = ctx->tagpt[k];
+    tagk[i] = k;
+    molbeg[k + 1] = molbeg[k] + ctx->numsite[i];
+    molspec[k] = ctx->uvspec[i];
+    float q = 0.0f;
+    for (int a = ctx->molbeg_all[i]; a < ctx->molbeg_all[i + 1]; ++a) {
+      q += ctx->charge[a];
+      atom_q.push_back(ctx->charge[a]);
+      atom_lj.push_back(t->ljtype[a] - 1);
+    }
+    molq[k] = q;
+  }
+  ctx->natoms = molbeg[ctx->slvmax];
+  const int slt = ctx->sltlist[0];
+  std::vector<int> slt_lj(ctx->s);
+  std::vector<float> slt_q(ctx->s), slt_m(ctx->s);
+  float qs = 0.0f;
+  for (int a = 0; a < ctx->s; ++a) {
+    slt_lj[a] = t->ljtype[ctx->molbeg_all[slt] + a] - 1;
+    slt_q[a] = ctx->charge[ctx->molbeg_all[slt] + a];
+    slt_m[a] = ctx->mass[ctx->molbeg_all[slt] + a];
+    qs += slt_q[a];
+  }
+  ctx->qslt_refs = qs;
+  if (!refs) for (int c = 0; c < ctx->maxdst; ++c) ctx->tgt_k.push_back(tagk[ctx->sltlist[c]]);
+  for (int a : atom_lj) if (a < 0 || a >= ctx->ljtype_max) return bad(ERMOD_ERR_ARG, "set_ljt");
+  for (int a : slt_lj) if (a < 0 || a >= ctx->ljtype_max) return bad(ERMOD_ERR_ARG, "set_ljt");
+  // engine shape
+  ctx->chunk = 32;
+  const int K1 = p.ms1max, K2 = p.ms2max, K3 = p.ms3max, Kh1 = K1 / 2 + 1;
+  const bool pme = p.cltype == ERMOD_EL_PME;
+  ctx->batch = p.ecorr_batch > 0 ? p.ecorr_batch : 4096;
+  ctx->batch = std::max(ctx->chunk, (ctx->batch + ctx->chunk - 1) / ctx->chunk * ctx->chunk);
+  ctx->batch = std::min(ctx->batch, (ctx->maxdst + ctx->chunk - 1) / ctx->chunk * ctx->chunk);
+  ctx->ncell_cap = 64 * 64 * 64;
+  spline_coeff(pme ? p.splodr : 4, ctx->spl_coeff);
+  *out = ctx;
+
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+  for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
+  DeviceState& d = ctx->d;
+  const size_t NA = ctx->natoms, SM = ctx->slvmax, MD = ctx->maxdst, S = ctx->s;
+  const int order = pme ? p.splodr : 1;
+  CK(dalloc(&d.molbeg, SM + 1)); CK(dalloc(&d.molspec, SM)); CK(dalloc(&d.molq, SM));
+  CK(dalloc(&d.atom_lj, NA)); CK(dalloc(&d.atom_q, NA));
+  CK(dalloc(&d.ljene, (size_t)ctx->ljtype_max * ctx->ljtype_max));
+  CK(dalloc(&d.ljlensq, (size_t)ctx->ljtype_max * ctx->ljtype_max));
+  CK(dalloc(&d.slt_lj, S)); CK(dalloc(&d.slt_q, S)); CK(dalloc(&d.slt_mass, S)); CK(dalloc(&d.bfcoord, 3 * S));
+  CK(dalloc(&d.uvcrd, ctx->ermax)); CK(dalloc(&d.spec_off, ctx->numslv + 1)); CK(dalloc(&d.uvsoft, ctx->numslv));
+  CK(dalloc(&d.escrd, std::max(1, ctx->esmax)));
+  CK(dalloc(&d.posraw, 3 * NA)); CK(dalloc(&d.slvn, NA)); CK(dalloc(&d.spl, NA * 3 * order)); CK(dalloc(&d.grd, NA));
+  CK(dalloc(&d.anchor, SM)); CK(dalloc(&d.cellof, SM)); CK(dalloc(&d.cellcount, ctx->ncell_cap));
+  CK(dalloc(&d.cellstart, ctx->ncell_cap + 1)); CK(dalloc(&d.molsorted, SM)); CK(dalloc(&d.rmol, 1));
+  CK(dalloc(&d.ins_conf, 3 * S * MD)); CK(dalloc(&d.insw_in, MD));
+  CK(dalloc(&d.tgt_raw, MD * S)); CK(dalloc(&d.tgt_n, MD * S)); CK(dalloc(&d.tgt_c, MD)); CK(dalloc(&d.tgt_mol, MD));
+  CK(dalloc(&d.selfreal, MD)); CK(dalloc(&d.selfrec, MD)); CK(dalloc(&d.u0, MD)); CK(dalloc(&d.w, MD));
+  CK(dalloc(&d.etot, MD)); CK(dalloc(&d.flceng, MD * ctx->numslv));
+  const size_t KK = (size_t)K1 * K2 * K3, KH = (size_t)K3 * K2 * Kh1;
+  if (pme) {
+    CK(dalloc(&d.grid, (size_t)ctx->chunk * KK)); CK(dalloc(&d.spec, (size_t)ctx->chunk * KH));
+    CK(dalloc(&d.phi, (size_t)ctx->chunk * KK)); CK(dalloc(&d.engfac, KH)); CK(dalloc(&d.splfc, K1 + K2 + K3));
+  }
+  CK(dalloc(&d.E, SM * ctx->chunk));
+  if (p.keep_uvengy) CK(dalloc(&d.uvengy, MD * SM));
+  CK(dalloc(&d.counts, (size_t)ctx->batch * ctx->ermax_pad));
+  CK(dalloc(&d.edens, ctx->ermax));
+  if (p.corrcal) CK(dalloc(&d.ecorr, (size_t)ctx->ermax * ctx->ermax));
+  CK(dalloc(&d.eself, std::max(1, ctx->esmax))); CK(dalloc(&d.slnuv, ctx->numslv));
+  CK(dalloc(&d.minuv, ctx->numslv + 1)); CK(dalloc(&d.maxuv, ctx->numslv + 1));
+  CK(dalloc(&d.scal, 8)); CK(dalloc(&d.status, 1));
+  // static uploads
+  cudaStream_t st = ctx->st;
+  CK(h2d(d.molbeg, molbeg.data(), SM + 1, st)); CK(h2d(d.molspec, molspec.data(), SM, st));
+  CK(h2d(d.molq, molq.data(), SM, st)); CK(h2d(d.atom_lj, atom_lj.data(), NA, st));
+  CK(h2d(d.atom_q, atom_q.data(), NA, st));
+  CK(h2d(d.ljene, t->ljene_mat, (size_t)ctx->ljtype_max * ctx->ljtype_max, st));
+  CK(h2d(d.ljlensq, t->ljlensq_mat, (size_t)ctx->ljtype_max * ctx->ljtype_max, st));
+  CK(h2d(d.slt_lj, slt_lj.data(), S, st)); CK(h2d(d.slt_q, slt_q.data(), S, st));
+  CK(h2d(d.slt_mass, slt_m.data(), S, st));
+  std::vector<float> bf(3 * S, 0.0f);
+  if (t->bfcoord) std::memcpy(bf.data(), t->bfcoord, sizeof(float) * 3 * S);
+  CK(h2d(d.bfcoord, bf.data(), 3 * S, st));
+  CK(h2d(d.uvcrd, ctx->uvcrd.data(), ctx->ermax, st));
+  std::vector<int> off(ctx->numslv + 1, 0);
+  for (int q = 0; q < ctx->numslv; ++q) off[q + 1] = off[q] + ctx->uvmax[q];
+  CK(h2d(d.spec_off, off.data(), ctx->numslv + 1, st));
+  CK(h2d(d.uvsoft, ctx->uvsoft.data(), ctx->numslv, st));
+  if (!ctx->escrd.empty()) CK(h2d(d.escrd, ctx->escrd.data(), ctx->esmax, st));
+  std::vector<int> tm(MD, -1);
+  if (!refs) for (size_t c = 0; c < MD; ++c) tm[c] = ctx->tgt_k[c];
+  CK(h2d(d.tgt_mol, tm.data(), MD, st));
+  if (pme) {
+    std::vector<double> sf(K1 + K2 + K3);
+    spline_axis(K1, p.splodr, sf.data());
+    spline_axis(K2, p.splodr, sf.data() + K1);
+    spline_axis(K3, p.splodr, sf.data() + K1 + K2);
+    CK(h2d(d.splfc, sf.data(), K1 + K2 + K3, st));
+    int n[3] = {K3, K2, K1};
+    int inR[3] = {K3, K2, K1}, onC[3] = {K3, K2, Kh1};
+    CF(cufftPlanMany(&ctx->r2c, 3, n, inR, 1, (int)KK, onC, 1, (int)KH, CUFFT_R2C, ctx->chunk));
+    int inC[3] = {K3, K2, Kh1}, onR[3] = {K3, K2, K1};
+    CF(cufftPlanMany(&ctx->c2r, 3, n, inC, 1, (int)KH, onR, ctx->chunk, 1, CUFFT_C2R, ctx->chunk));
+    ctx->plans = true;
+    CF(cufftSetStream(ctx->r2c, st));
+    CF(cufftSetStream(ctx->c2r, st));
+  }
+  ctx->use_tc = (p.corrcal && ecorr_tc_available() && p.ecorr_path == 0) ? 1 : 0;
+  if (ctx->use_tc) {
+    ctx->tc_work_bytes = ecorr_tc_workspace(ctx->batch, ctx->ermax);
+    CK(cudaMalloc(&ctx->tc_work, ctx->tc_work_bytes));
+  }
+  const int rc = ermod_engclear(ctx);
+  if (rc != ERMOD_OK) return rc;
+  // minuv / maxuv / voffset start values (enginit, engproc.F90:299-303)
+  std::vector<float> mn(ctx->numslv + 1, FLT_MAX), mx(ctx->numslv + 1, -FLT_MAX);
+  CK(h2d(d.minuv, mn.data(), mn.size(), st));
+  CK(h2d(d.maxuv, mx.data(), mx.size(), st));
+  double sc[8] = {0, 0, 0, -(double)FLT_MAX, 0, 0, 0, 0};
+  CK(h2d(d.scal, sc, 8, st));
+  CK(cudaStreamSynchronize(st));
+  return ERMOD_OK;
+}
+
+int32_t ermod_engclear(ermod_ctx* ctx) {
+  if (!ctx) return ERMOD_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  DeviceState& d = ctx->d;
+  cudaStream_t st = ctx->st;
+  CK(cudaMemsetAsync(d.edens, 0, sizeof(double) * ctx->ermax, st));
+  if (d.ecorr) CK(cudaMemsetAsync(d.ecorr, 0, sizeof(double) * ctx->ermax * ctx->ermax, st));
+  CK(cudaMemsetAsync(d.eself, 0, sizeof(double) * std::max(1, ctx->esmax), st));
+  CK(cudaMemsetAsync(d.slnuv, 0, sizeof(double) * ctx->numslv, st));
+  // avslf, engnorm, engsmpl (scal[0..2]); voffset and the self-energy reuse persist
+  CK(cudaMemsetAsync(d.scal, 0, sizeof(double) * 3, st));
+  CK(cudaStreamSynchronize(st));
+  return ERMOD_OK;
+}
+
+static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float wsys, bool use_conf) {
+  const ermod_params& p = ctx->p;
+  DeviceState& d = ctx->d;
+  cudaStream_t st = ctx->st;
+  const bool refs = p.slttype != ERMOD_SLT_SOLN;
+  const bool pme = p.cltype == ERMOD_EL_PME;
+  const int K1 = p.ms1max, K2 = p.ms2max, K3 = p.ms3max;
+  // ---- cell (engproc.F90:1049-1070, realcal.F90:776-896) on the host ----
+  double c[3][3];
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) c[i][j] = cellin[j * 3 + i];
+  float cf[3][3];
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) cf[i][j] = cellin[j * 3 + i];
+  // FP32 as the reference's get_inverted_cell
+  const float vol = cf[0][0] * cf[1][1] * cf[2][2] + cf[0][1] * cf[1][2] * cf[2][0] + cf[0][2] * cf[1][0] * cf[2][1] -
+                    cf[0][2] * cf[1][1] * cf[2][0] - cf[0][1] * cf[1][0] * cf[2][2] - cf[0][0] * cf[1][2] * cf[2][1];
+  const double vold = c[0][0] * c[1][1] * c[2][2] + c[0][1] * c[1][2] * c[2][0] + c[0][2] * c[1][0] * c[2][1] -
+                      c[0][2] * c[1][1] * c[2][0] - c[0][1] * c[1][0] * c[2][2] - c[0][0] * c[1][2] * c[2][1];
+  double inv[3][3];
+  inv[0][0] = c[1][1] * c[2][2] - c[1][2] * c[2][1];
+  inv[0][1] = c[0][2] * c[2][1] - c[0][1] * c[2][2];
+  inv[0][2] = c[0][1] * c[1][2] - c[0][2] * c[1][1];
+  inv[1][0] = c[1][2] * c[2][0] - c[1][0] * c[2][2];
+  inv[1][1] = c[0][0] * c[2][2] - c[0][2] * c[2][0];
+  inv[1][2] = c[0][2] * c[1][0] - c[0][0] * c[1][2];
+  inv[2][0] = c[1][0] * c[2][1] - c[1][1] * c[2][0];
+  inv[2][1] = c[0][1] * c[2][0] - c[0][0] * c[2][1];
+  inv[2][2] = c[0][0] * c[1][1] - c[0][1] * c[1][0];
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) inv[i][j] /= vold;
+  FrameArgs a{};
+  CellGeom& g = a.g;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      g.cell[i][j] = cf[i][j];
+      g.invcl[i][j] = (float)inv[i][j];
+      g.rot[i][j] = i == j ? 1.f : 0.f;
+    }
+  g.volume = vol;
+  g.periodic = p.boxshp == ERMOD_SYS_PERIODIC;
+  if (g.periodic) {
+    float cn[3][3];
+    if (cf[1][0] == 0.f && cf[2][0] == 0.f && cf[2][1] == 0.f) {
+      for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) cn[i][j] = cf[i][j];
+      g.rotated = 0;
+    } else {  // modified Gram-Schmidt (realcal.F90:794-816)
+      float q[3][3] = {}, r[3][3] = {}, tmp[3][3];
+      for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) tmp[i][j] = cf[i][j];
+      for (int i = 0; i < 3; ++i) {
+        const float len = std::sqrt(tmp[0][0] * tmp[0][0] + tmp[1][0] * tmp[1][0] + tmp[2][0] * tmp[2][0]);
+        for (int k = 0; k < 3; ++k) q[k][i] = tmp[k][i] / len;
+        r[i][i] = len;
+        for (int j = i + 1; j < 3; ++j) {
+          r[i][j] = q[0][i] * tmp[0][j] + q[1][i] * tmp[1][j] + q[2][i] * tmp[2][j];
+          for (int k = 0; k < 3; ++k) tmp[k][j] -= r[i][j] * q[k][i];
+        }
+      }
+      for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) { cn[i][j] = r[i][j]; g.rot[i][j] = q[i][j]; }
+      g.rotated = 1;
+    }
+    for (int i = 0; i < 3; ++i)  // normalize_cell_vector (realcal.F90:826-830)
+      if (cn[0][0] < 0.f) for (int k = 0; k < 3; ++k) cn[k][i] = -cn[k][i];
+    const float thr = 1e-4f;
+    if (std::fabs(cn[0][1]) > 0.5f * cn[0][0] + thr) {
+      const float f = std::round(cn[0][1] * ctx->invcell_prev[0]);
+      for (int k = 0; k < 3; ++k) cn[k][1] -= cn[k][0] * f;
+    }
+    if (std::fabs(cn[0][2]) > 0.5f * cn[0][0] + thr) {
+      const float f = std::round(cn[0][2] * ctx->invcell_prev[0]);
+      for (int k = 0; k < 3; ++k) cn[k][2] -= cn[k][0] * f;
+    }
+    if (std::fabs(cn[1][2]) > 0.5f * cn[1][1] + thr) {
+      const float f = std::round(cn[1][2] * ctx->invcell_prev[1]);
+      for (int k = 0; k < 3; ++k) cn[k][2] -= cn[k][1] * f;
+    }
+    const float cut = std::min(p.elecut, p.upljcut);
+    for (int i = 0; i < 3; ++i)
+      if (cut > cn[i][i] * 0.5f) return set_error(ctx, ERMOD_ERR_CELL, "cel_siz");
+    for (int i = 0; i < 3; ++i) {
+      g.len[i] = std::fabs(cn[i][i]);
+      g.inv[i] = 1.0f / g.len[i];
+      g.half[i] = 0.5f * g.len[i];
+      ctx->invcell_prev[i] = g.inv[i];
+    }
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) g.cn[i][j] = cn[i][j];
+    g.cuboid = !(std::fabs(cf[0][1]) > 1e-8f || std::fabs(cf[0][2]) > 1e-8f || std::fabs(cf[1][2]) > 1e-8f);
+  } else {
+    g.cuboid = 1;
+  }
+  if (refs && p.insposition == ERMOD_INSPOS_RANDOM && !g.periodic) return set_error(ctx, ERMOD_ERR_INS_GEO, "ins_geo");
+  // ---- pair / PME constants ----
+  PairParams& P = a.pp;
+  P.lw = p.lwljcut; P.up = p.upljcut; P.lw2 = p.lwljcut * p.lwljcut; P.up2 = p.upljcut * p.upljcut;
+  P.lw3 = P.lw2 * p.lwljcut; P.up3 = P.up2 * p.upljcut; P.lw6 = P.lw3 * P.lw3; P.up6 = P.up3 * P.up3;
+  auto gmx = [&](int pw, float& A, float& B, float& C) {  // realcal.F90:899-915
+    const float lw = p.lwljcut, up = p.upljcut, df = up - lw;
+    float uppw2 = 1.f, uppw = 1.f;
+    for (int i = 0; i < pw + 2; ++i) uppw2 *= up;
+    for (int i = 0; i < pw; ++i) uppw *= up;
+    A = -(float)pw * ((float)(pw + 4) * up - (float)(pw + 1) * lw) / (uppw2 * (df * df)) / 3.0f;
+    B = (float)pw * ((float)(pw + 3) * up - (float)(pw + 1) * lw) / (uppw2 * (df * df * df)) / 4.0f;
+    C = 1.0f / uppw - A * (df * df * df) - B * (df * df * df * df);
+  };
+  gmx(12, P.repA, P.repB, P.repC);
+  gmx(6, P.attA, P.attB, P.attC);
+  P.reelcut = g.periodic ? p.elecut : FLT_MAX;
+  P.screen = p.screen;
+  P.ljswitch = p.ljswitch;
+  P.bare = p.cltype == ERMOD_EL_COULOMB;
+  a.slvmax = ctx->slvmax; a.natoms = ctx->natoms; a.nsite = ctx->s; a.maxdst = ctx->maxdst;
+  a.K1 = K1; a.K2 = K2; a.K3 = K3; a.order = pme ? p.splodr : 1; a.Kh1 = K1 / 2 + 1;
+  for (int i = 0; i <= kMaxOrder; ++i) a.spl_coeff[i] = ctx->spl_coeff[i];
+  a.ljtype_max = ctx->ljtype_max;
+  a.pme = pme;
+  a.pivol = pme ? kPi / ((double)p.screen * (double)p.screen) / vold : 0.0;
+  a.rcut = g.periodic ? std::max(p.elecut, p.upljcut) : (P.bare ? FLT_MAX : p.upljcut);
+  if (P.bare && !g.periodic) a.rcut = FLT_MAX;
+  // cell list only for cuboid periodic boxes
+  a.use_cells = 0;
+  int ncell = 1;
+  if (g.periodic && g.cuboid && !g.rotated) {
+    const float hmin = 4.0f;
+    bool ok = true;
+    for (int dd = 0; dd < 3; ++dd) {
+      a.nc[dd] = std::max(1, std::min(64, (int)std::floor(g.len[dd] / hmin)));
+      a.ch[dd] = g.len[dd] / (float)a.nc[dd];
+      if (a.nc[dd] < 3) ok = false;
+    }
+    ncell = a.nc[0] * a.nc[1] * a.nc[2];
+    a.use_cells = ok && ncell <= ctx->ncell_cap;
+  }
+  ctx->pused = 0;
+  mark(ctx, 0);
+  // ---- PME influence function when the cell changes (engconst :423-433) ----
+  if (pme) {
+    bool changed = !ctx->pme_init;
+    for (int i = 0; i < 9; ++i) if (ctx->prevcl[i] != cellin[i]) changed = true;
+    if (changed) launch_engfac(a, d, inv, vold, (double)p.screen, st);
+    for (int i = 0; i < 9; ++i) ctx->prevcl[i] = cellin[i];
+    ctx->pme_init = true;
+  }
+  CK(cudaMemsetAsync(d.status, 0, sizeof(DevStatus), st));
+  launch_prepare_solvent(a, d, st);
+  launch_cells(a, d, ncell, st);
+  long long nl = 1 + (a.slvmax > 0 ? (a.use_cells ? 3 : 2) : 0) + (pme && ctx->pme_init ? 0 : 0);
+  mark(ctx, kStPrep);
+  // ---- targets ----
+  if (refs) launch_insert(a, d, stnum, p.iseed, p.insposition, p.insorient, use_conf ? 1 : 0, st);
+  else launch_targets_soln(a, d, nullptr, st);
+  CK(cudaMemsetAsync(d.selfrec, 0, sizeof(double) * ctx->maxdst, st));
+  CK(cudaMemsetAsync(d.etot, 0, sizeof(double) * ctx->maxdst, st));
+  CK(cudaMemsetAsync(d.flceng, 0, sizeof(double) * ctx->maxdst * ctx->numslv, st));
+  if (d.uvengy) CK(cudaMemsetAsync(d.uvengy, 0, sizeof(double) * ctx->maxdst * ctx->slvmax, st));
+  const bool rigid = p.slttype == ERMOD_SLT_REFS_RIGID;
+  if (!P.bare) {
+    if (rigid) {
+      if (!ctx->usreal_init) { launch_selfreal(a, d, 0, 1, (double)p.screen, st); ctx->usreal_init = true; }
+    } else {
+      launch_selfreal(a, d, 0, ctx->maxdst, (double)p.screen, st);
+    }
+  } else {
+    CK(cudaMemsetAsync(d.selfreal, 0, sizeof(double) * ctx->maxdst, st));
+  }
+  nl += 1 + (P.bare ? 0 : (rigid ? 0 : 1));
+  mark(ctx, kStIns);
+  // ---- weights args ----
+  WeightArgs wa{};
+  wa.slttype = p.slttype; wa.wgtslf = p.wgtslf; wa.estype = p.estype; wa.selfcal = p.selfcal;
+  wa.numslv = ctx->numslv; wa.esmax = ctx->esmax; wa.rigid = rigid && !P.bare;
+  wa.temp = p.temp;
+  wa.stat_weight_system = wsys;
+  double qslt = refs ? ctx->qslt_refs : 0.0;
+  if (!refs) {  // soln solutes share one site layout; charge of the first solute
+    float q = 0.f;
+    const int i = ctx->sltlist[0];
+    for (int at = ctx->molbeg_all[i]; at < ctx->molbeg_all[i + 1]; ++at) q += ctx->charge[at];
+    qslt = q;
+  }
+  wa.resid_self = P.bare ? 0.0 : -(kPi * qslt * qslt / (double)p.screen / (double)p.screen / vold) / 2.0;
+  wa.npt_factor = 1.0;
+  if (p.estype == ERMOD_ES_NPT) {  // volcorrect (engproc.F90:1022-1038)
+    double qt = 0.0;
+    for (int k = 0; k < ctx->slvmax; ++k) {
+      const int i = ctx->tagpt[k];
+      float q = 0.f;
+      for (int at = ctx->molbeg_all[i]; at < ctx->molbeg_all[i + 1]; ++at) q += ctx->charge[at];
+      qt += q;
+    }
+    double f = vold;
+    if (pme) f *= std::exp(kPi * qt * qt / ((double)p.screen * p.screen) / vold / 2.0 / p.temp);
+    wa.npt_factor = f;
+  }
+  BinArgs ba{};
+  ba.ermax_pad = ctx->ermax_pad; ba.numslv = ctx->numslv; ba.slttype = p.slttype;
+  ba.keep_uvengy = d.uvengy != nullptr;
+  // ---- chunks / batches ----
+  const int chunk = ctx->chunk;
+  for (int bb = 0; bb < ctx->maxdst; bb += ctx->batch) {
+    const int nbatch = std::min(ctx->batch, ctx->maxdst - bb);
+    CK(cudaMemsetAsync(d.counts, 0, sizeof(uint32_t) * (size_t)ctx->batch * ctx->ermax_pad, st));
+    ba.count_base = bb;
+    for (int cb = bb; cb < bb + nbatch; cb += chunk) {
+      const int nb = std::min(chunk, bb + nbatch - cb);
+      if (pme) {
+        launch_spread(a, d, cb, nb, chunk, st);
+        mark(ctx, kStSpread);
+        CF(cufftExecR2C(ctx->r2c, d.grid, (cufftComplex*)d.spec));
+        mark(ctx, kStR2C);
+        launch_influence(a, d, cb, nb, chunk, st);
+        mark(ctx, kStInfl);
+        CF(cufftExecC2R(ctx->c2r, (cufftComplex*)d.spec, d.phi));
+        mark(ctx, kStC2R);
+        nl += 2;
+      }
+      launch_real(a, d, cb, nb, chunk, st);
+      mark(ctx, kStReal);
+      launch_gather_bin(a, d, ba, cb, nb, chunk, st);
+      mark(ctx, kStGather);
+      nl += 2;
+    }
+    launch_weights(d, wa, bb, nbatch, st);
+    launch_edens(d, bb, nbatch, ctx->ermax, ctx->ermax_pad, bb, st);
+    nl += 3;
+    mark(ctx, kStWeights);
+    if (p.corrcal) {
+      if (ctx->use_tc) {
+        const int rc = launch_ecorr_tc(d, bb, nbatch, ctx->ermax, ctx->ermax_pad, bb, p.weight_bits, ctx->tc_work,
+                                       ctx->tc_work_bytes, st);
+        if (rc != 0) return set_error(ctx, ERMOD_ERR_CUDA, "ecorr_tc");
+      } else {
+        launch_ecorr_simt(d, bb, nbatch, ctx->ermax, ctx->ermax_pad, bb, st);
+      }
+      nl += 1;
+    }
+    mark(ctx, kStEcorr);
+  }
+  DevStatus hs;
+  CK(cudaMemcpyAsync(&hs, d.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  CK(cudaGetLastError());
+  for (float& t : ctx->timings) t = 0.f;
+  for (int k = 1; k < ctx->pused; ++k) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->pev[k - 1], ctx->pev[k]);
+    ctx->timings[ctx->ptag[k]] += ms;
+    ctx->timings[0] += ms;
+  }
+  ctx->timings[11] = (float)((ctx->maxdst + chunk - 1) / chunk);
+  ctx->launches += nl;
+  if (hs.flags & kErrEngCns) return set_error(ctx, ERMOD_ERR_ENG_CNS, "eng_cns");
+  if (hs.flags & kErrEngMin) return set_error(ctx, ERMOD_ERR_ENG_MIN, "eng_min");
+  if (hs.flags & kErrEngSft) return set_error(ctx, ERMOD_ERR_ENG_SFT, "eng_sft");
+  if (hs.flags & kErrOverflow) return set_error(ctx, ERMOD_ERR_OVERFLOW, "ermod_ovf");
+  if ((hs.flags & kWarnMbin) && ctx->warn_bin_firsttime) {
+    ctx->warn_bin_firsttime = false;
+    return set_error(ctx, ERMOD_WARN_MBIN, "mbin");
+  }
+  return ERMOD_OK;
+}
+
+int32_t ermod_engconst(ermod_ctx* ctx, int32_t stnum, const float* sitepos, const float* cell,
+                       float stat_weight_system, const float* ins_conf, const float* ins_weight, float* flceng) {
+  if (!ctx || !sitepos || !cell) return ERMOD_ERR_ARG;
+  ctx->err.clear();
+  CK(cudaSetDevice(ctx->device));
+  const ermod_params& p = ctx->p;
+  const bool refs = p.slttype != ERMOD_SLT_SOLN;
+  const size_t npos = 3 * (size_t)ctx->natoms;
+  const size_t nconf = (refs && ins_conf) ? 3 * (size_t)ctx->s * ctx->maxdst : 0;
+  const size_t need = sizeof(float) * (npos + nconf + ctx->maxdst);
+  if (ctx->h_pin_bytes < need) {
+    if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
+    ctx->h_pin = nullptr;
+    CK(cudaMallocHost((void**)&ctx->h_pin, need));
+    ctx->h_pin_bytes = need;
+  }
+  std::memcpy(ctx->h_pin, sitepos, sizeof(float) * npos);
+  CK(cudaMemcpyAsync(ctx->d.posraw, ctx->h_pin, sizeof(float) * npos, cudaMemcpyHostToDevice, ctx->st));
+  if (nconf) {
+    std::memcpy(ctx->h_pin + npos, ins_conf, sizeof(float) * nconf);
+    CK(cudaMemcpyAsync(ctx->d.ins_conf, ctx->h_pin + npos, sizeof(float) * nconf, cudaMemcpyHostToDevice, ctx->st));
+  }
+  float* hw = ctx->h_pin + npos + nconf;
+  for (int i = 0; i < ctx->maxdst; ++i) hw[i] = (refs && ins_weight) ? ins_weight[i] : 1.0f;
+  CK(cudaMemcpyAsync(ctx->d.insw_in, hw, sizeof(float) * ctx->maxdst, cudaMemcpyHostToDevice, ctx->st));
+  const int rc = engconst_impl(ctx, stnum, cell, stat_weight_system, nconf > 0);
+  if (rc < 0) return rc;
+  if (flceng && !refs) {
+    std::vector<double> f((size_t)ctx->maxdst * ctx->numslv);
+    CK(cudaMemcpy(f.data(), ctx->d.flceng, sizeof(double) * f.size(), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < f.size(); ++i) flceng[i] = (float)f[i];
+  }
+  return rc;
+}
+
+int32_t ermod_engconst_dev(ermod_ctx* ctx, int32_t stnum, const float* sitepos_dev, const float* cell,
+                           float stat_weight_system, const float* ins_conf_dev, const float* ins_weight_dev) {
+  if (!ctx || !sitepos_dev || !cell) return ERMOD_ERR_ARG;
+  ctx->err.clear();
+  CK(cudaSetDevice(ctx->device));
+  const bool refs = ctx->p.slttype != ERMOD_SLT_SOLN;
+  CK(cudaMemcpyAsync(ctx->d.posraw, sitepos_dev, sizeof(float) * 3 * ctx->natoms, cudaMemcpyDeviceToDevice, ctx->st));
+  if (refs && ins_conf_dev)
+    CK(cudaMemcpyAsync(ctx->d.ins_conf, ins_conf_dev, sizeof(float) * 3 * ctx->s * ctx->maxdst,
+                       cudaMemcpyDeviceToDevice, ctx->st));
+  if (refs && ins_weight_dev) {
+    CK(cudaMemcpyAsync(ctx->d.insw_in, ins_weight_dev, sizeof(float) * ctx->maxdst, cudaMemcpyDeviceToDevice, ctx->st));
+  } else {
+    std::vector<float> one(ctx->maxdst, 1.0f);
+    CK(cudaMemcpyAsync(ctx->d.insw_in, one.data(), sizeof(float) * ctx->maxdst, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  return engconst_impl(ctx, stnum, cell, stat_weight_system, refs && ins_conf_dev);
+}
+
+int32_t ermod_fetch_accum(ermod_ctx* ctx, ermod_accum* o) {
+  if (!ctx || !o) return ERMOD_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->st));
+  const DeviceState& d = ctx->d;
+  if (o->edens) CK(cudaMemcpy(o->edens, d.edens, sizeof(double) * ctx->ermax, cudaMemcpyDeviceToHost));
+  if (o->ecorr && d.ecorr)
+    CK(cudaMemcpy(o->ecorr, d.ecorr, sizeof(double) * ctx->ermax * ctx->ermax, cudaMemcpyDeviceToHost));
+  if (o->eself && ctx->p.selfcal) CK(cudaMemcpy(o->eself, d.eself, sizeof(double) * ctx->esmax, cudaMemcpyDeviceToHost));
+  if (o->slnuv) {
+    std::vector<double> s(ctx->numslv);
+    CK(cudaMemcpy(s.data(), d.slnuv, sizeof(double) * ctx->numslv, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < ctx->numslv; ++i) o->slnuv[i] = (float)s[i];
+  }
+  if (o->minuv) CK(cudaMemcpy(o->minuv, d.minuv, sizeof(float) * (ctx->numslv + 1), cudaMemcpyDeviceToHost));
+  if (o->maxuv) CK(cudaMemcpy(o->maxuv, d.maxuv, sizeof(float) * (ctx->numslv + 1), cudaMemcpyDeviceToHost));
+  double sc[8];
+  CK(cudaMemcpy(sc, d.scal, sizeof(sc), cudaMemcpyDeviceToHost));
+  o->avslf = sc[0];
+  o->engnorm = sc[1];
+  o->engsmpl = sc[2];
+  o->voffset = sc[3];
+  o->voffset_initialized = sc[4] != 0.0;
+  return ERMOD_OK;
+}
+
+int32_t ermod_engstore(ermod_ctx* ctx, ermod_accum* o, double* avediv) {
+  if (!ctx || !o) return ERMOD_ERR_ARG;
+  const int rc = ermod_fetch_accum(ctx, o);
+  if (rc != ERMOD_OK) return rc;
+  const double nrm = o->engnorm;  // engproc.F90:609-628
+  if (o->edens) for (int i = 0; i < ctx->ermax; ++i) o->edens[i] /= nrm;
+  if (o->ecorr && ctx->d.ecorr) for (size_t i = 0; i < (size_t)ctx->ermax * ctx->ermax; ++i) o->ecorr[i] /= nrm;
+  if (o->eself && ctx->p.selfcal) for (int i = 0; i < ctx->esmax; ++i) o->eself[i] /= nrm;
+  const double avslf = o->avslf / nrm;
+  if (avediv) {
+    avediv[0] = o->engnorm / o->engsmpl;
+    avediv[1] = ctx->p.slttype == ERMOD_SLT_SOLN ? o->voffset - ctx->p.temp * std::log(avslf)
+                                                 : o->voffset + ctx->p.temp * std::log(avslf);
+  }
+  o->avslf = avslf;
+  return ERMOD_OK;
+}
+
+int32_t ermod_get_uvengy(ermod_ctx* ctx, double* uvengy, double* uvengy0) {
+  if (!ctx) return ERMOD_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (uvengy) {
+    if (!ctx->d.uvengy) return set_error(ctx, ERMOD_ERR_ARG, "uv_nokeep");
+    CK(cudaMemcpy(uvengy, ctx->d.uvengy, sizeof(double) * ctx->maxdst * ctx->slvmax, cudaMemcpyDeviceToHost));
+  }
+  if (uvengy0) CK(cudaMemcpy(uvengy0, ctx->d.u0, sizeof(double) * ctx->maxdst, cudaMemcpyDeviceToHost));
+  return ERMOD_OK;
+}
+
+int32_t ermod_get_insertions(ermod_ctx* ctx, float* ins, double* w) {
+  if (!ctx) return ERMOD_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (ins) {
+    std::vector<float4> t((size_t)ctx->maxdst * ctx->s);
+    CK(cudaMemcpy(t.data(), ctx->d.tgt_raw, sizeof(float4) * t.size(), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < t.size(); ++i) { ins[3 * i] = t[i].x; ins[3 * i + 1] = t[i].y; ins[3 * i + 2] = t[i].z; }
+  }
+  if (w) {
+    std::vector<float> f(ctx->maxdst);
+    CK(cudaMemcpy(f.data(), ctx->d.insw_in, sizeof(float) * ctx->maxdst, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < ctx->maxdst; ++i) w[i] = f[i];
+  }
+  return ERMOD_OK;
+}
+
+int32_t ermod_get_sizes(ermod_ctx* ctx, int32_t* slvmax, int32_t* maxdst, int32_t* ns, int32_t* natoms) {
+  if (!ctx) return ERMOD_ERR_ARG;
+  if (slvmax) *slvmax = ctx->slvmax;
+  if (maxdst) *maxdst = ctx->maxdst;
+  if (ns) *ns = ctx->s;
+  if (natoms) *natoms = ctx->natoms;
+  return ERMOD_OK;
+}
+
+const char* ermod_last_error(const ermod_ctx* ctx) { return ctx ? ctx->err.c_str() : "null"; }
+
+int32_t ermod_get_timings(const ermod_ctx* ctx, float* ms, int32_t n) {
+  if (!ctx || !ms) return ERMOD_ERR_ARG;
+  for (int i = 0; i < n && i < 12; ++i) ms[i] = ctx->timings[i];
+  return ERMOD_OK;
+}
+
+int64_t ermod_get_launch_count(const ermod_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+void ermod_destroy(ermod_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  free_all(ctx);
+  delete ctx;
+}
+
+}  // extern "C"

@@ -1,0 +1,131 @@
+// engine.cuh -- device buffers of one engine context and the kernel launchers.
+#pragma once
+#include <cufft.h>
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ermod_b200.h"
+#include "common.cuh"
+
+namespace erm {
+
+constexpr int kMaxOrder = 8;       // PME spline order limit (splodr)
+constexpr int kMaxSoluteSites = 1024;
+constexpr int kMaxLjTypes = 64;
+
+// Everything the frame kernels read, passed by value.
+struct FrameArgs {
+  CellGeom g;
+  PairParams pp;
+  int slvmax, natoms, nsite, maxdst;
+  int K1, K2, K3, order, Kh1;      // Kh1 = K1/2+1
+  float spl_coeff[kMaxOrder + 1];
+  int ljtype_max;
+  int pme;
+  double pivol;                    // pi / screen^2 / volume (residual terms, engproc.F90:974,994)
+  // cell list (cuboid periodic boxes)
+  int use_cells, nc[3];
+  float ch[3];                     // cell edge lengths
+  float rcut;                      // max(elecut, upljcut): beyond it every pair term is zero
+};
+
+// Device-resident state of one context.
+struct DeviceState {
+  // topology (physical molecules in tagpt order)
+  int* molbeg = nullptr;     // [slvmax+1]
+  int* molspec = nullptr;    // [slvmax] uvspec
+  float* molq = nullptr;     // [slvmax] mol_charge
+  int* atom_lj = nullptr;    // [natoms] ljtype-1
+  float* atom_q = nullptr;   // [natoms]
+  float* ljene = nullptr;    // [ljtype_max^2]
+  float* ljlensq = nullptr;  // [ljtype_max^2]
+  // solute site tables
+  int* slt_lj = nullptr;     // [s]
+  float* slt_q = nullptr;    // [s]
+  float* slt_mass = nullptr; // [s]
+  float* bfcoord = nullptr;  // [3s]
+  // mesh
+  double* uvcrd = nullptr;   // [ermax]
+  int* spec_off = nullptr;   // [numslv+1]
+  int* uvsoft = nullptr;     // [numslv]
+  double* escrd = nullptr;   // [esmax]
+  // per frame: solvent
+  float* posraw = nullptr;   // [3*natoms]
+  float4* slvn = nullptr;    // [natoms] normalised x,y,z + charge
+  float* spl = nullptr;      // [natoms*3*order]
+  int4* grd = nullptr;       // [natoms]
+  float4* anchor = nullptr;  // [slvmax] first-site position, w = molecule extent
+  int* cellof = nullptr;     // [slvmax]
+  int* cellcount = nullptr;  // [ncell_cap]
+  int* cellstart = nullptr;  // [ncell_cap+1]
+  int* molsorted = nullptr;  // [slvmax]
+  float* rmol = nullptr;     // [1] max molecule extent
+  // per frame: targets (insertions or soln solutes)
+  float* ins_conf = nullptr; // [3*s*maxdst] staging of caller conformations
+  float* insw_in = nullptr;  // [maxdst]
+  float4* tgt_raw = nullptr; // [maxdst*s]
+  float4* tgt_n = nullptr;   // [maxdst*s] normalised + charge
+  float4* tgt_c = nullptr;   // [maxdst] wrapped COM + radius
+  int* tgt_mol = nullptr;    // [maxdst] soln: excluded molecule (k index), refs: -1
+  double* selfreal = nullptr;// [maxdst]
+  double* selfrec = nullptr; // [maxdst]
+  double* u0 = nullptr;      // [maxdst] uvengy0
+  double* w = nullptr;       // [maxdst] engnmfc
+  double* etot = nullptr;    // [maxdst] sum of solute-solvent energies
+  double* flceng = nullptr;  // [maxdst*numslv]
+  // PME chunk buffers
+  float* grid = nullptr;     // [chunk*K^3]
+  float2* spec = nullptr;    // [chunk*K3*K2*Kh1]
+  float* phi = nullptr;      // [K^3*chunk], insertion fastest
+  float* engfac = nullptr;   // [K3*K2*Kh1]
+  double* splfc = nullptr;   // [K1+K2+K3]
+  double* E = nullptr;       // [slvmax*chunk] real-space energies of the chunk
+  double* uvengy = nullptr;  // [maxdst*slvmax] kept when requested
+  uint32_t* counts = nullptr;// [batch*ermax_pad]
+  // accumulators
+  double* edens = nullptr;   // [ermax]
+  double* ecorr = nullptr;   // [ermax*ermax]
+  double* eself = nullptr;   // [esmax]
+  double* slnuv = nullptr;   // [numslv]
+  float* minuv = nullptr;    // [numslv+1]
+  float* maxuv = nullptr;    // [numslv+1]
+  double* scal = nullptr;    // [8]: avslf, engnorm, engsmpl, voffset, voffset_init, usreal, usreal_init
+  DevStatus* status = nullptr;
+};
+
+// ---- launchers (kernels.cu) -------------------------------------------
+void launch_prepare_solvent(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
+void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStream_t s);
+void launch_insert(const FrameArgs& a, const DeviceState& d, int stnum, int iseed, int insposition,
+                   int insorient, int use_conf, cudaStream_t s);
+void launch_targets_soln(const FrameArgs& a, const DeviceState& d, const int* tgt_k_host_dev, cudaStream_t s);
+void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int count, double screen,
+                     cudaStream_t s);
+void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
+void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[3][3], double volume,
+                   double screen, cudaStream_t s);
+void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
+void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
+
+struct BinArgs {
+  int ermax_pad, numslv, slttype, keep_uvengy, count_base, nslv_spec;
+  double qslt_unused;
+};
+void launch_gather_bin(const FrameArgs& a, const DeviceState& d, const BinArgs& b, int base, int nb, int chunk,
+                       cudaStream_t s);
+
+struct WeightArgs {
+  int slttype, wgtslf, estype, selfcal, numslv, esmax, rigid;
+  double temp, npt_factor;  // exp(pi Q^2/(2 a^2 V)/temp) * V for NPT, else 1
+  float stat_weight_system;
+  double resid_self;        // residual_self_ene of the solute
+};
+void launch_weights(const DeviceState& d, const WeightArgs& w, int base, int n, cudaStream_t s);
+void launch_edens(const DeviceState& d, int base, int n, int ermax, int ermax_pad, int count_base,
+                  cudaStream_t s);
+void launch_ecorr_simt(const DeviceState& d, int base, int n, int ermax, int ermax_pad, int count_base,
+                       cudaStream_t s);
+
+}  // namespace erm

@@ -1,0 +1,796 @@
+// kernels.cu -- frame kernels of the energy-distribution engine (sm_100a).
+//
+// Stage map (reference routine each kernel replaces):
+//   k_prepare_solvent  normalize_periodic (realcal.F90:859-896) + solvent splines
+//                      (recpcal_prepare_solvent / calc_spline_molecule, recpcal.F90:340-357, 504-538)
+//   k_anchor / k_cell_*  cell list of solvent molecules (no reference counterpart:
+//                      the reference evaluates every site pair, realcal.F90:257-361)
+//   k_insert           instslt('proc') for uniform insertion (insertion.F90:38-375)
+//   k_selfreal         realcal_self(_refs) in FP64 (realcal.F90:669-771)
+//   k_real             realcal_refs / realcal_soln / realcal_bare (realcal.F90:51-666)
+//   k_engfac           recpcal_spline_greenfunc (recpcal.F90:121-163)
+//   k_spread           charge spreading of recpcal_prepare_solute(_refs) (recpcal.F90:380-399, 453-473)
+//   k_influence        self energy + influence multiply (recpcal.F90:482-497)
+//   k_gather_bin       recpcal_energy_refs/soln (recpcal.F90:592-710) + residual_ene(_refs)
+//                      (engproc.F90:979-1020) + getiduv / update_histogram counting
+//                      (engproc.F90:917-937, 1111-1171), fused
+//   k_weights          update_histogram weights and scalar accumulators (engproc.F90:883-915, 939-941)
+//   k_edens            edens += engnmfc * insdst (engproc.F90:943-947)
+//   k_ecorr_simt       ecorr += engnmfc * insdst insdst^T (engproc.F90:948-962), FP64 reference kernel
+#include <cfloat>
+#include <cstdio>
+
+#include "engine.cuh"
+
+namespace erm {
+
+// ---------------------------------------------------------------------------
+// solvent preparation
+// ---------------------------------------------------------------------------
+__global__ void k_prepare_solvent(FrameArgs a, const float* __restrict__ posraw, const float* __restrict__ atom_q,
+                                  float4* __restrict__ slvn, float* __restrict__ spl, int4* __restrict__ grd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.natoms) return;
+  const float x = posraw[3 * i], y = posraw[3 * i + 1], z = posraw[3 * i + 2];
+  const CellGeom& g = a.g;
+  if (a.pme) {
+    float inm[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float f = g.invcl[k][0] * x + g.invcl[k][1] * y + g.invcl[k][2] * z;
+      inm[k] = f - floorf(f);
+    }
+    const int K[3] = {a.K1, a.K2, a.K3};
+    int gi[3];
+    for (int m = 0; m < 3; ++m) {
+      const float f = inm[m] * (float)K[m];
+      const int rci = (int)f;
+      for (int spi = 0; spi < a.order; ++spi)
+        spl[((size_t)i * 3 + m) * a.order + spi] = spline_value(a.spl_coeff, a.order, f - (float)(rci - spi));
+      gi[m] = rci;
+    }
+    grd[i] = make_int4(gi[0], gi[1], gi[2], 0);
+  }
+  float nx = x, ny = y, nz = z;
+  if (g.periodic) {
+    if (g.rotated) {
+      nx = g.rot[0][0] * x + g.rot[1][0] * y + g.rot[2][0] * z;
+      ny = g.rot[0][1] * x + g.rot[1][1] * y + g.rot[2][1] * z;
+      nz = g.rot[0][2] * x + g.rot[1][2] * y + g.rot[2][2] * z;
+    }
+    float f = floorf(g.inv[2] * nz);
+    nx -= g.cn[0][2] * f; ny -= g.cn[1][2] * f; nz -= g.cn[2][2] * f;
+    f = floorf(g.inv[1] * ny);
+    nx -= g.cn[0][1] * f; ny -= g.cn[1][1] * f; nz -= g.cn[2][1] * f;
+    f = floorf(g.inv[0] * nx);
+    nx -= g.cn[0][0] * f; ny -= g.cn[1][0] * f; nz -= g.cn[2][0] * f;
+  }
+  slvn[i] = make_float4(nx, ny, nz, atom_q[i]);
+}
+
+void launch_prepare_solvent(const FrameArgs& a, const DeviceState& d, cudaStream_t s) {
+  if (a.natoms <= 0) return;
+  k_prepare_solvent<<<(a.natoms + 255) / 256, 256, 0, s>>>(a, d.posraw, d.atom_q, d.slvn, d.spl, d.grd);
+}
+
+// ---------------------------------------------------------------------------
+// cell list of solvent molecules, keyed by the normalised first site
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int cell_coord(float x, float h, int n) {
+  int c = (int)floorf(x / h);
+  return c < 0 ? 0 : (c >= n ? n - 1 : c);
+}
+
+__global__ void k_anchor(FrameArgs a, const int* __restrict__ molbeg, const float4* __restrict__ slvn,
+                         float4* __restrict__ anchor, int* __restrict__ cellof, int* __restrict__ cellcount,
+                         float* rmol) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.slvmax) return;
+  const int b0 = molbeg[k], b1 = molbeg[k + 1];
+  const float4 p0 = slvn[b0];
+  float ext = 0.0f;
+  for (int at = b0 + 1; at < b1; ++at) {
+    const float4 q = slvn[at];
+    float dx = q.x - p0.x, dy = q.y - p0.y, dz = q.z - p0.z;
+    min_image(a.g, dx, dy, dz);
+    ext = fmaxf(ext, sqrtf(dx * dx + dy * dy + dz * dz));
+  }
+  anchor[k] = make_float4(p0.x, p0.y, p0.z, ext);
+  atomicMax((int*)rmol, __float_as_int(ext));
+  if (a.use_cells) {
+    const int cx = cell_coord(p0.x, a.ch[0], a.nc[0]);
+    const int cy = cell_coord(p0.y, a.ch[1], a.nc[1]);
+    const int cz = cell_coord(p0.z, a.ch[2], a.nc[2]);
+    const int cid = (cz * a.nc[1] + cy) * a.nc[0] + cx;
+    cellof[k] = cid;
+    atomicAdd(&cellcount[cid], 1);
+  }
+}
+
+// exclusive scan of the cell counts in one block; leaves cellcount = start (fill cursor)
+__global__ void k_cell_scan(int ncell, int* __restrict__ cellcount, int* __restrict__ cellstart) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int per = (ncell + nt - 1) / nt;
+  const int lo = t * per, hi = min(ncell, lo + per);
+  int s = 0;
+  for (int i = lo; i < hi; ++i) s += cellcount[i];
+  part[t] = s;
+  __syncthreads();
+  for (int off = 1; off < nt; off <<= 1) {
+    const int v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - s;
+  for (int i = lo; i < hi; ++i) {
+    const int c = cellcount[i];
+    cellstart[i] = run;
+    cellcount[i] = run;
+    run += c;
+  }
+  if (t == nt - 1) cellstart[ncell] = part[nt - 1];
+}
+
+__global__ void k_cell_fill(int slvmax, const int* __restrict__ cellof, int* __restrict__ cursor,
+                            int* __restrict__ molsorted) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= slvmax) return;
+  const int pos = atomicAdd(&cursor[cellof[k]], 1);
+  molsorted[pos] = k;
+}
+
+__global__ void k_iota(int n, int* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = k;
+}
+
+void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStream_t s) {
+  if (a.slvmax <= 0) return;
+  cudaMemsetAsync(d.rmol, 0, sizeof(float), s);
+  if (a.use_cells) cudaMemsetAsync(d.cellcount, 0, sizeof(int) * ncell, s);
+  k_anchor<<<(a.slvmax + 255) / 256, 256, 0, s>>>(a, d.molbeg, d.slvn, d.anchor, d.cellof, d.cellcount, d.rmol);
+  if (a.use_cells) {
+    k_cell_scan<<<1, 1024, 0, s>>>(ncell, d.cellcount, d.cellstart);
+    k_cell_fill<<<(a.slvmax + 255) / 256, 256, 0, s>>>(a.slvmax, d.cellof, d.cellcount, d.molsorted);
+  } else {
+    k_iota<<<(a.slvmax + 255) / 256, 256, 0, s>>>(a.slvmax, d.molsorted);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// targets: insertions (refs) or solute molecules taken from the frame (soln)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void wrap_point(const CellGeom& g, float& x, float& y, float& z) {
+  if (!g.periodic) return;
+  float nx = x, ny = y, nz = z;
+  if (g.rotated) {
+    nx = g.rot[0][0] * x + g.rot[1][0] * y + g.rot[2][0] * z;
+    ny = g.rot[0][1] * x + g.rot[1][1] * y + g.rot[2][1] * z;
+    nz = g.rot[0][2] * x + g.rot[1][2] * y + g.rot[2][2] * z;
+  }
+  float f = floorf(g.inv[2] * nz);
+  nx -= g.cn[0][2] * f; ny -= g.cn[1][2] * f; nz -= g.cn[2][2] * f;
+  f = floorf(g.inv[1] * ny);
+  nx -= g.cn[0][1] * f; ny -= g.cn[1][1] * f; nz -= g.cn[2][1] * f;
+  f = floorf(g.inv[0] * nx);
+  nx -= g.cn[0][0] * f; ny -= g.cn[1][0] * f; nz -= g.cn[2][0] * f;
+  x = nx; y = ny; z = nz;
+}
+
+// normalised copies + search sphere (centre = first site, radius = max min-image distance)
+__device__ void finish_target(const FrameArgs& a, int cnt, float4* __restrict__ raw, float4* __restrict__ nrm,
+                              float4* __restrict__ ctr, const float* __restrict__ qsite) {
+  const int s = a.nsite;
+  for (int i = 0; i < s; ++i) {
+    float4 r = raw[i];
+    float x = r.x, y = r.y, z = r.z;
+    wrap_point(a.g, x, y, z);
+    nrm[i] = make_float4(x, y, z, qsite ? qsite[i] : r.w);
+  }
+  const float4 c = nrm[0];
+  float rad = 0.0f;
+  for (int i = 1; i < s; ++i) {
+    float dx = nrm[i].x - c.x, dy = nrm[i].y - c.y, dz = nrm[i].z - c.z;
+    min_image(a.g, dx, dy, dz);
+    rad = fmaxf(rad, sqrtf(dx * dx + dy * dy + dz * dz));
+  }
+  ctr[cnt] = make_float4(c.x, c.y, c.z, rad);
+}
+
+__global__ void k_insert(FrameArgs a, int stnum, int iseed, int insposition, int insorient, int use_conf,
+                         const float* __restrict__ conf_all, const float* __restrict__ bfcoord,
+                         const float* __restrict__ mass, const float* __restrict__ qsite,
+                         float4* __restrict__ tgt_raw, float4* __restrict__ tgt_n, float4* __restrict__ tgt_c) {
+  const int cnt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cnt >= a.maxdst) return;
+  const int s = a.nsite;
+  float4* out = tgt_raw + (size_t)cnt * s;
+  const float* conf = use_conf ? conf_all + (size_t)3 * s * cnt : bfcoord;
+  float msum = 0.0f;
+  for (int i = 0; i < s; ++i) {
+    out[i] = make_float4(conf[3 * i], conf[3 * i + 1], conf[3 * i + 2], qsite[i]);
+    msum += mass[i];
+  }
+  auto com = [&](float c[3]) {  // center_of_mass (bestfit.F90:252-266)
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    for (int i = 0; i < s; ++i) { sx += out[i].x * mass[i]; sy += out[i].y * mass[i]; sz += out[i].z * mass[i]; }
+    c[0] = sx / msum; c[1] = sy / msum; c[2] = sz / msum;
+  };
+  const uint2 key = make_uint2((uint32_t)iseed, kStreamTag);
+  if (insposition == ERMOD_INSPOS_RANDOM) {
+    float c[3];
+    com(c);  // set_solute_origin: COM to the origin (insertion.F90:116-119)
+    for (int i = 0; i < s; ++i) { out[i].x -= c[0]; out[i].y -= c[1]; out[i].z -= c[2]; }
+    const uint4 r4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, 0u, 0u), key);
+    const float r[3] = {u01(r4.x), u01(r4.y), u01(r4.z)};
+    float cm[3];  // com = cell . r (insertion.F90:157-161)
+    for (int k = 0; k < 3; ++k) cm[k] = a.g.cell[k][0] * r[0] + a.g.cell[k][1] * r[1] + a.g.cell[k][2] * r[2];
+    com(c);
+    for (int i = 0; i < s; ++i) {
+      out[i].x = (out[i].x - c[0]) + cm[0];
+      out[i].y = (out[i].y - c[1]) + cm[1];
+      out[i].z = (out[i].z - c[2]) + cm[2];
+    }
+  }
+  if (insorient == ERMOD_INSROT_RANDOM) {  // apply_orientation (insertion.F90:348-369)
+    float c[3];
+    com(c);
+    for (int i = 0; i < s; ++i) { out[i].x -= c[0]; out[i].y -= c[1]; out[i].z -= c[2]; }
+    float q0 = 1.f, q1 = 0.f, q2 = 0.f, q3 = 0.f;
+    for (uint32_t att = 1; att <= 64; ++att) {
+      const uint4 r4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, att, 1u), key);
+      const float t0 = u01(r4.x) * 2.f - 1.f, t1 = u01(r4.y) * 2.f - 1.f;
+      const float t2 = u01(r4.z) * 2.f - 1.f, t3 = u01(r4.w) * 2.f - 1.f;
+      const float n2 = t0 * t0 + t1 * t1 + t2 * t2 + t3 * t3;
+      if (n2 < 1.f) {
+        const float nn = sqrtf(n2);
+        q0 = t0 / nn; q1 = t1 / nn; q2 = t2 / nn; q3 = t3 / nn;
+        break;
+      }
+    }
+    for (int i = 0; i < s; ++i) {  // q (0,v) q* (bestfit.F90:62-74)
+      const float v0 = out[i].x, v1 = out[i].y, v2 = out[i].z;
+      const float t0 = -(q1 * v0 + q2 * v1 + q3 * v2);
+      const float t1 = q2 * v2 - q3 * v1 + q0 * v0;
+      const float t2 = q3 * v0 - q1 * v2 + q0 * v1;
+      const float t3 = q1 * v1 - q2 * v0 + q0 * v2;
+      const float c1 = -q1, c2 = -q2, c3 = -q3;
+      out[i].x = (t2 * c3 - t3 * c2 + t0 * c1 + q0 * t1) + c[0];
+      out[i].y = (t3 * c1 - t1 * c3 + t0 * c2 + q0 * t2) + c[1];
+      out[i].z = (t1 * c2 - t2 * c1 + t0 * c3 + q0 * t3) + c[2];
+    }
+  }
+  finish_target(a, cnt, out, tgt_n + (size_t)cnt * s, tgt_c, qsite);
+}
+
+void launch_insert(const FrameArgs& a, const DeviceState& d, int stnum, int iseed, int insposition, int insorient,
+                   int use_conf, cudaStream_t s) {
+  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum, iseed, insposition, insorient, use_conf, d.ins_conf,
+                                                    d.bfcoord, d.slt_mass, d.slt_q, d.tgt_raw, d.tgt_n, d.tgt_c);
+}
+
+__global__ void k_targets_soln(FrameArgs a, const int* __restrict__ tgt_mol, const int* __restrict__ molbeg,
+                               const float* __restrict__ posraw, const float* __restrict__ atom_q,
+                               float4* __restrict__ tgt_raw, float4* __restrict__ tgt_n, float4* __restrict__ tgt_c) {
+  const int cnt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cnt >= a.maxdst) return;
+  const int k = tgt_mol[cnt], b0 = molbeg[k], s = a.nsite;
+  float4* out = tgt_raw + (size_t)cnt * s;
+  for (int i = 0; i < s; ++i)
+    out[i] = make_float4(posraw[3 * (b0 + i)], posraw[3 * (b0 + i) + 1], posraw[3 * (b0 + i) + 2], atom_q[b0 + i]);
+  finish_target(a, cnt, out, tgt_n + (size_t)cnt * s, tgt_c, nullptr);
+}
+
+void launch_targets_soln(const FrameArgs& a, const DeviceState& d, const int*, cudaStream_t s) {
+  k_targets_soln<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, d.tgt_mol, d.molbeg, d.posraw, d.atom_q, d.tgt_raw,
+                                                          d.tgt_n, d.tgt_c);
+}
+
+// realcal_self(_refs) (realcal.F90:669-771), FP64 on normalised coordinates
+__global__ void k_selfreal(FrameArgs a, int first, double screen, const float4* __restrict__ tgt_n,
+                           double* __restrict__ selfreal) {
+  const int cnt = first + blockIdx.x;
+  const int s = a.nsite;
+  const float4* x = tgt_n + (size_t)cnt * s;
+  double acc = 0.0;
+  const double sqpi = sqrt(kPi);
+  for (int i = threadIdx.x; i < s; i += blockDim.x) acc -= (double)x[i].w * (double)x[i].w * screen / sqpi;
+  for (int i = 0; i < s; ++i)
+    for (int j = i + 1 + threadIdx.x; j < s; j += blockDim.x) {
+      float dx = x[i].x - x[j].x, dy = x[i].y - x[j].y, dz = x[i].z - x[j].z;
+      if (a.g.cuboid) {
+        dx = a.g.half[0] - fabsf(a.g.half[0] - fabsf(dx));
+        dy = a.g.half[1] - fabsf(a.g.half[1] - fabsf(dy));
+        dz = a.g.half[2] - fabsf(a.g.half[2] - fabsf(dz));
+      } else {
+        CellGeom g = a.g;
+        g.periodic = 1;
+        min_image(g, dx, dy, dz);
+      }
+      const double r = sqrt((double)dx * dx + (double)dy * dy + (double)dz * dz);
+      acc -= (double)x[i].w * (double)x[j].w * erf(screen * r) / r;
+    }
+  __shared__ double red[32];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) selfreal[cnt] = v;
+  }
+}
+
+void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int count, double screen, cudaStream_t s) {
+  if (count <= 0) return;
+  k_selfreal<<<count, 128, 0, s>>>(a, first, screen, d.tgt_n, d.selfreal);
+}
+
+// ---------------------------------------------------------------------------
+// real space: one CTA per target, a warp per candidate molecule, lanes over
+// the site pairs, FP64 warp-shuffle reduction of the molecule sum
+// ---------------------------------------------------------------------------
+constexpr int kRealThreads = 256;
+
+__global__ void __launch_bounds__(kRealThreads) k_real(FrameArgs a, int base, int chunk,
+    const float4* __restrict__ tgt_n, const float4* __restrict__ tgt_c, const int* __restrict__ tgt_mol,
+    const int* __restrict__ slt_lj_tab, const int* __restrict__ molbeg, const float4* __restrict__ slvn,
+    const int* __restrict__ atom_lj, const float* __restrict__ ljene, const float* __restrict__ ljlensq,
+    const float4* __restrict__ anchor, const int* __restrict__ cellstart, const int* __restrict__ molsorted,
+    const float* __restrict__ rmol_p, double* __restrict__ E) {
+  __shared__ float4 ss[kMaxSoluteSites];
+  __shared__ int slj[kMaxSoluteSites];
+  const int b = blockIdx.x, cnt = base + b, s = a.nsite;
+  const float4* tn = tgt_n + (size_t)cnt * s;
+  for (int i = threadIdx.x; i < s; i += blockDim.x) {
+    ss[i] = tn[i];
+    slj[i] = slt_lj_tab ? slt_lj_tab[i] : 0;
+  }
+  const int excl = tgt_mol ? tgt_mol[cnt] : -1;
+  // soln: solute site LJ types come from the solute molecule's atoms
+  if (excl >= 0)
+    for (int i = threadIdx.x; i < s; i += blockDim.x) slj[i] = atom_lj[molbeg[excl] + i];
+  __syncthreads();
+  const float4 c = tgt_c[cnt];
+  const float rmol = *rmol_p;
+  const float margin = 1.0e-2f;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int ljmax = a.ljtype_max;
+
+  auto do_mol = [&](int k) {
+    if (k == excl) return;
+    const float4 an = anchor[k];
+    float dx = an.x - c.x, dy = an.y - c.y, dz = an.z - c.z;
+    min_image(a.g, dx, dy, dz);
+    const float lim = a.rcut + c.w + an.w + margin;
+    if (dx * dx + dy * dy + dz * dz > lim * lim) return;  // every site pair beyond the cutoff
+    const int b0 = molbeg[k], nj = molbeg[k + 1] - b0;
+    const int P = s * nj;
+    double acc = 0.0;
+    for (int t = lane; t < P; t += 32) {
+      const int is = t / nj, js = t - is * nj;
+      const float4 xi = ss[is];
+      const float4 xj = slvn[b0 + js];
+      float ex = xi.x - xj.x, ey = xi.y - xj.y, ez = xi.z - xj.z;
+      min_image(a.g, ex, ey, ez);
+      const float dis2 = ex * ex + ey * ey + ez * ez;
+      const int li = slj[is], lj = atom_lj[b0 + js];
+      const float eps = __ldg(&ljene[lj * ljmax + li]);
+      const float sg2 = __ldg(&ljlensq[lj * ljmax + li]);
+      acc += (double)pair_energy(a.pp, dis2, eps, sg2, xi.w * xj.w);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) E[(size_t)k * chunk + b] = acc;
+  };
+
+  (void)rmol;
+  if (a.use_cells) {
+    const float R = a.rcut + c.w + rmol + margin;
+    int lo[3], n[3];
+    const float cc[3] = {c.x, c.y, c.z};
+    for (int d3 = 0; d3 < 3; ++d3) {
+      lo[d3] = (int)floorf((cc[d3] - R) / a.ch[d3]);
+      const int hi = (int)floorf((cc[d3] + R) / a.ch[d3]);
+      n[d3] = hi - lo[d3] + 1;
+      if (n[d3] >= a.nc[d3]) { lo[d3] = 0; n[d3] = a.nc[d3]; }
+    }
+    const int total = n[0] * n[1] * n[2];
+    for (int t = warp; t < total; t += nw) {
+      const int ix = t % n[0], iy = (t / n[0]) % n[1], iz = t / (n[0] * n[1]);
+      int cx = (lo[0] + ix) % a.nc[0]; if (cx < 0) cx += a.nc[0];
+      int cy = (lo[1] + iy) % a.nc[1]; if (cy < 0) cy += a.nc[1];
+      int cz = (lo[2] + iz) % a.nc[2]; if (cz < 0) cz += a.nc[2];
+      const int cid = (cz * a.nc[1] + cy) * a.nc[0] + cx;
+      const int m0 = cellstart[cid], m1 = cellstart[cid + 1];
+      for (int m = m0; m < m1; ++m) do_mol(molsorted[m]);
+    }
+  } else {
+    for (int k = warp; k < a.slvmax; k += nw) do_mol(k);
+  }
+}
+
+void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
+  cudaMemsetAsync(d.E, 0, sizeof(double) * (size_t)a.slvmax * chunk, s);
+  if (nb <= 0) return;
+  k_real<<<nb, kRealThreads, 0, s>>>(a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, d.slt_lj, d.molbeg, d.slvn,
+                                      d.atom_lj, d.ljene, d.ljlensq, d.anchor, d.cellstart, d.molsorted, d.rmol, d.E);
+}
+
+// ---------------------------------------------------------------------------
+// PME
+// ---------------------------------------------------------------------------
+struct Mat3d { double m[3][3]; };
+
+__global__ void k_engfac(int K1, int K2, int K3, int Kh1, int order, Mat3d invcl, double volume, double screen,
+                         const double* __restrict__ splfc, float* __restrict__ engfac) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = K3 * K2 * Kh1;
+  if (i >= n) return;
+  const int r1 = i % Kh1, r2 = (i / Kh1) % K2, r3 = i / (Kh1 * K2);
+  double factor = 0.0;
+  if (!(r1 == 0 && r2 == 0 && r3 == 0)) {
+    const int rc[3] = {r1, r2, r3}, K[3] = {K1, K2, K3};
+    double inm[3];
+    bool zero = false;
+    for (int m = 0; m < 3; ++m) {
+      if ((order % 2 == 1) && (2 * abs(rc[m]) == K[m])) zero = true;
+      inm[m] = rc[m] <= K[m] / 2 ? (double)rc[m] : (double)(rc[m] - K[m]);
+    }
+    if (!zero) {
+      double xs[3];
+      for (int m = 0; m < 3; ++m) xs[m] = invcl.m[0][m] * inm[0] + invcl.m[1][m] * inm[1] + invcl.m[2][m] * inm[2];
+      const double rtp2 = xs[0] * xs[0] + xs[1] * xs[1] + xs[2] * xs[2];
+      const double chr = kPi * kPi * rtp2 / (screen * screen);
+      factor = exp(-chr) / rtp2 / kPi / volume;
+      factor /= splfc[r1] * splfc[K1 + r2] * splfc[K1 + K2 + r3];
+    }
+  }
+  engfac[i] = (float)factor;
+}
+
+void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[3][3], double volume, double screen,
+                   cudaStream_t s) {
+  Mat3d m;
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) m.m[i][j] = invcl[i][j];
+  const int n = a.K3 * a.K2 * a.Kh1;
+  k_engfac<<<(n + 255) / 256, 256, 0, s>>>(a.K1, a.K2, a.K3, a.Kh1, a.order, m, volume, screen, d.splfc, d.engfac);
+}
+
+// a warp per (target, site): lanes over the order^3 stencil points, global atomics
+__global__ void k_spread(FrameArgs a, int base, int nb, const float4* __restrict__ tgt_raw, float* __restrict__ grid) {
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int s = a.nsite;
+  if (wid >= nb * s) return;
+  const int b = wid / s, site = wid - b * s;
+  const float4 r = tgt_raw[(size_t)(base + b) * s + site];
+  const CellGeom& g = a.g;
+  float w[3][kMaxOrder];
+  int gi[3];
+  const int K[3] = {a.K1, a.K2, a.K3};
+  for (int m = 0; m < 3; ++m) {
+    float f = g.invcl[m][0] * r.x + g.invcl[m][1] * r.y + g.invcl[m][2] * r.z;
+    f = f - floorf(f);
+    f = f * (float)K[m];
+    const int rci = (int)f;
+    for (int spi = 0; spi < a.order; ++spi) w[m][spi] = spline_value(a.spl_coeff, a.order, f - (float)(rci - spi));
+    gi[m] = rci;
+  }
+  const int n = a.order, n3 = n * n * n;
+  float* gb = grid + (size_t)b * a.K1 * a.K2 * a.K3;
+  for (int t = lane; t < n3; t += 32) {
+    const int c1 = t % n, c2 = (t / n) % n, c3 = t / (n * n);
+    int r1 = (gi[0] - c1) % a.K1; if (r1 < 0) r1 += a.K1;
+    int r2 = (gi[1] - c2) % a.K2; if (r2 < 0) r2 += a.K2;
+    int r3 = (gi[2] - c3) % a.K3; if (r3 < 0) r3 += a.K3;
+    const float v = r.w * w[0][c1] * w[1][c2] * w[2][c3];
+    atomicAdd(&gb[((size_t)r3 * a.K2 + r2) * a.K1 + r1], v);
+  }
+}
+
+void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
+  cudaMemsetAsync(d.grid, 0, sizeof(float) * (size_t)chunk * a.K1 * a.K2 * a.K3, s);
+  const int warps = nb * a.nsite;
+  if (warps <= 0) return;
+  k_spread<<<(warps * 32 + 255) / 256, 256, 0, s>>>(a, base, nb, d.tgt_raw, d.grid);
+}
+
+// influence multiply + FP64 self energy of each target (recpcal.F90:482-497)
+__global__ void k_influence(FrameArgs a, int base, int nb, float2* __restrict__ spec, const float* __restrict__ engfac,
+                            double* __restrict__ selfrec) {
+  const int b = blockIdx.y;
+  const int n = a.K3 * a.K2 * a.Kh1;
+  float2* sp = spec + (size_t)b * n;
+  double acc = 0.0;
+  const int even = (a.K1 % 2) == 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float2 v = sp[i];
+    const float e = engfac[i];
+    const int r1 = i % a.Kh1;
+    const double wgt = (r1 == 0 || (even && r1 == a.Kh1 - 1)) ? 0.5 : 1.0;
+    acc += wgt * (double)e * ((double)v.x * v.x + (double)v.y * v.y);
+    sp[i] = make_float2(v.x * e, v.y * e);
+  }
+  __shared__ double red[32];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0 && b < nb) atomicAdd(&selfrec[base + b], v);
+  }
+}
+
+void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
+  const int n = a.K3 * a.K2 * a.Kh1;
+  int bx = (n + 256 * 8 - 1) / (256 * 8);
+  if (bx > 256) bx = 256;
+  k_influence<<<dim3(bx, chunk), 256, 0, s>>>(a, base, nb, d.spec, d.engfac, d.selfrec);
+}
+
+// ---------------------------------------------------------------------------
+// gather + residual + binning.  A warp per solvent molecule, lane = target
+// of the chunk (chunk == 32): the potential grid is stored target-fastest,
+// so each stencil point is one coalesced 128-byte row.
+// ---------------------------------------------------------------------------
+constexpr int kGatherThreads = 256;
+constexpr int kMaxSpecSmem = 128;
+
+__global__ void __launch_bounds__(kGatherThreads) k_gather_bin(FrameArgs a, BinArgs ba, int base, int nb, int chunk,
+    const int* __restrict__ molsorted, const int* __restrict__ molbeg, const int* __restrict__ molspec,
+    const float* __restrict__ molq, const float* __restrict__ atom_q, const float* __restrict__ spl,
+    const int4* __restrict__ grd, const float* __restrict__ phi, const double* __restrict__ E,
+    const int* __restrict__ tgt_mol, const float4* __restrict__ tgt_n,
+    const double* __restrict__ uvcrd, const int* __restrict__ spec_off, const int* __restrict__ uvsoft,
+    double* __restrict__ uvengy, uint32_t* __restrict__ counts, double* __restrict__ etot, double* __restrict__ flceng,
+    float* __restrict__ minuv, float* __restrict__ maxuv, DevStatus* st) {
+  __shared__ float smin[kMaxSpecSmem], smax[kMaxSpecSmem];
+  for (int i = threadIdx.x; i < kMaxSpecSmem; i += blockDim.x) { smin[i] = FLT_MAX; smax[i] = -FLT_MAX; }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwt = (gridDim.x * blockDim.x) >> 5;
+  const int b = lane;
+  const bool active = b < nb;
+  const int cnt = base + b;
+  const int excl = (active && tgt_mol) ? tgt_mol[cnt] : -1;
+  // solute net charge of this target (sum of its site charges)
+  double qslt = 0.0;
+  if (active) {
+    const float4* tn = tgt_n + (size_t)cnt * a.nsite;
+    for (int i = 0; i < a.nsite; ++i) qslt += (double)tn[i].w;
+    qslt = (double)(float)qslt;
+  }
+  double my_etot = 0.0;
+  const int n = a.order;
+  for (int m = gw; m < a.slvmax; m += nwt) {
+    const int k = molsorted[m];
+    double e = E[(size_t)k * chunk + b];
+    const int b0 = molbeg[k], b1 = molbeg[k + 1];
+    if (a.pme) {
+      for (int at = b0; at < b1; ++at) {
+        const float q = atom_q[at];
+        const float* w = spl + (size_t)at * 3 * n;
+        const int4 gd = grd[at];
+        for (int c3 = 0; c3 < n; ++c3) {
+          int r3 = (gd.z - c3) % a.K3; if (r3 < 0) r3 += a.K3;
+          const float fac1 = q * w[2 * n + c3];
+          for (int c2 = 0; c2 < n; ++c2) {
+            int r2 = (gd.y - c2) % a.K2; if (r2 < 0) r2 += a.K2;
+            const float fac2 = fac1 * w[n + c2];
+            const size_t row = ((size_t)r3 * a.K2 + r2) * a.K1;
+            float part = 0.0f;
+            for (int c1 = 0; c1 < n; ++c1) {
+              int r1 = (gd.x - c1) % a.K1; if (r1 < 0) r1 += a.K1;
+              part += (fac2 * w[c1]) * phi[(row + r1) * chunk + b];
+            }
+            e += (double)part;
+          }
+        }
+      }
+      e -= a.pivol * qslt * (double)molq[k];
+    }
+    if (!active || k == excl) continue;
+    if (ba.keep_uvengy) uvengy[(size_t)cnt * a.slvmax + k] = e;
+    const int pti = molspec[k];
+    if (pti <= 0) { report(st, kErrEngCns, k, cnt, (float)e); continue; }
+    const int lo = spec_off[pti - 1], num = spec_off[pti] - lo;
+    const double* c = uvcrd + lo;
+    int idp;
+    if (e < c[0]) idp = 0;
+    else if (e > c[num - 1]) idp = num;
+    else {
+      int l = 0, h = num;  // first index with c[i] >= e
+      while (l < h) { const int mid = (l + h) >> 1; if (c[mid] < e) l = mid + 1; else h = mid; }
+      idp = l;
+    }
+    if (idp <= 0) { report(st, kErrEngMin, k, cnt, (float)e); continue; }
+    if (ba.slttype == ERMOD_SLT_SOLN && idp > uvsoft[pti - 1]) { report(st, kErrEngSft, k, cnt, (float)e); continue; }
+    if (idp == num && e < 1.0e3) report(st, kWarnMbin, k, cnt, (float)e);
+    atomicAdd(&counts[(size_t)(cnt - ba.count_base) * ba.ermax_pad + lo + idp - 1], 1u);
+    my_etot += e;
+    if (ba.slttype == ERMOD_SLT_SOLN) atomicAdd(&flceng[(size_t)cnt * ba.numslv + pti - 1], e);
+    const float ef = (float)e;
+    if (pti < kMaxSpecSmem) {
+      atomic_min_f(&smin[pti], ef);
+      atomic_max_f(&smax[pti], ef);
+    } else {
+      atomic_min_f(&minuv[pti], ef);
+      atomic_max_f(&maxuv[pti], ef);
+    }
+  }
+  if (active && my_etot != 0.0) atomicAdd(&etot[cnt], my_etot);
+  __syncthreads();
+  for (int i = threadIdx.x; i < kMaxSpecSmem && i <= ba.numslv; i += blockDim.x) {
+    if (i == 0) continue;
+    if (smin[i] != FLT_MAX) atomic_min_f(&minuv[i], smin[i]);
+    if (smax[i] != -FLT_MAX) atomic_max_f(&maxuv[i], smax[i]);
+  }
+}
+
+void launch_gather_bin(const FrameArgs& a, const DeviceState& d, const BinArgs& ba, int base, int nb, int chunk,
+                       cudaStream_t s) {
+  int blocks = (a.slvmax * 32 + kGatherThreads - 1) / kGatherThreads;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  if (blocks < 1) blocks = 1;
+  k_gather_bin<<<blocks, kGatherThreads, 0, s>>>(a, ba, base, nb, chunk, d.molsorted, d.molbeg, d.molspec, d.molq,
+                                                 d.atom_q, d.spl, d.grd, d.phi, d.E, d.tgt_mol, d.tgt_n, d.uvcrd,
+                                                 d.spec_off, d.uvsoft, d.uvengy, d.counts, d.etot, d.flceng, d.minuv,
+                                                 d.maxuv, d.status);
+}
+
+// ---------------------------------------------------------------------------
+// weights and accumulators
+// ---------------------------------------------------------------------------
+__global__ void k_offset_init(WeightArgs wa, int base, const double* __restrict__ selfrec,
+                              const double* __restrict__ selfreal, double* __restrict__ scal) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (wa.rigid && scal[6] == 0.0) { scal[5] = selfreal[base]; scal[6] = 1.0; }
+  if (wa.wgtslf && scal[4] == 0.0) {
+    const double sr = wa.rigid ? scal[5] : selfreal[base];
+    scal[3] = selfrec[base] + sr + wa.resid_self;
+    scal[4] = 1.0;
+  }
+}
+
+__global__ void k_weights(WeightArgs wa, int base, int n, const double* __restrict__ selfrec,
+                          const double* __restrict__ selfreal, const float* __restrict__ insw,
+                          const double* __restrict__ escrd, const double* __restrict__ flceng,
+                          double* __restrict__ u0, double* __restrict__ w, double* __restrict__ scal,
+                          double* __restrict__ eself, double* __restrict__ slnuv, float* __restrict__ minuv,
+                          float* __restrict__ maxuv, DevStatus* st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double wn = 0.0, tw = 0.0, cntv = 0.0;
+  float mn = FLT_MAX, mx = -FLT_MAX;
+  if (i < n) {
+    const int cnt = base + i;
+    const double sr = wa.rigid ? scal[5] : selfreal[cnt];
+    const double uu = selfrec[cnt] + sr + wa.resid_self;
+    u0[cnt] = uu;
+    double e = 1.0;
+    if (wa.wgtslf) {
+      const double f = uu - scal[3];
+      e = wa.slttype == ERMOD_SLT_SOLN ? exp(f / wa.temp) : exp(-f / wa.temp);
+    }
+    tw = (double)wa.stat_weight_system * (double)insw[cnt] * wa.npt_factor;
+    e *= tw;
+    w[cnt] = e;
+    wn = e;
+    cntv = 1.0;
+    if (wa.selfcal) {
+      int l = 0, h = wa.esmax;
+      if (uu < escrd[0]) l = 0;
+      else if (uu > escrd[wa.esmax - 1]) l = wa.esmax;
+      else { while (l < h) { const int mid = (l + h) >> 1; if (escrd[mid] < uu) l = mid + 1; else h = mid; } }
+      if (l <= 0) report(st, kErrEngMin, -1, cnt, (float)uu);
+      else {
+        if (l == wa.esmax && uu < 1.0e3) report(st, kWarnMbin, -1, cnt, (float)uu);
+        atomicAdd(&eself[l - 1], e);
+      }
+    }
+    if (wa.slttype == ERMOD_SLT_SOLN)
+      for (int q = 0; q < wa.numslv; ++q) atomicAdd(&slnuv[q], flceng[(size_t)cnt * wa.numslv + q] * e);
+    mn = mx = (float)uu;
+  }
+  __shared__ double r0[32], r1[32], r2[32];
+  __shared__ float rm[32], rx[32];
+  wn = warp_sum(wn); tw = warp_sum(tw); cntv = warp_sum(cntv);
+  mn = warp_min(mn); mx = warp_max(mx);
+  if ((threadIdx.x & 31) == 0) {
+    r0[threadIdx.x >> 5] = wn; r1[threadIdx.x >> 5] = tw; r2[threadIdx.x >> 5] = cntv;
+    rm[threadIdx.x >> 5] = mn; rx[threadIdx.x >> 5] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const bool ok = threadIdx.x < (blockDim.x >> 5);
+    wn = warp_sum(ok ? r0[threadIdx.x] : 0.0);
+    tw = warp_sum(ok ? r1[threadIdx.x] : 0.0);
+    cntv = warp_sum(ok ? r2[threadIdx.x] : 0.0);
+    mn = warp_min(ok ? rm[threadIdx.x] : FLT_MAX);
+    mx = warp_max(ok ? rx[threadIdx.x] : -FLT_MAX);
+    if (threadIdx.x == 0 && cntv > 0.0) {
+      atomicAdd(&scal[1], wn);
+      atomicAdd(&scal[2], cntv);
+      atomicAdd(&scal[0], tw);
+      atomic_min_f(&minuv[0], mn);
+      atomic_max_f(&maxuv[0], mx);
+    }
+  }
+}
+
+void launch_weights(const DeviceState& d, const WeightArgs& wa, int base, int n, cudaStream_t s) {
+  if (n <= 0) return;
+  k_offset_init<<<1, 32, 0, s>>>(wa, base, d.selfrec, d.selfreal, d.scal);
+  k_weights<<<(n + 255) / 256, 256, 0, s>>>(wa, base, n, d.selfrec, d.selfreal, d.insw_in, d.escrd, d.flceng,
+                                             d.u0, d.w, d.scal, d.eself, d.slnuv, d.minuv, d.maxuv, d.status);
+}
+
+__global__ void k_edens(int base, int n, int ermax, int ermax_pad, int count_base, const double* __restrict__ w,
+                        const uint32_t* __restrict__ counts, double* __restrict__ edens) {
+  const int bin = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bin >= ermax) return;
+  double acc = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const uint32_t c = counts[(size_t)(base + i - count_base) * ermax_pad + bin];
+    if (c) acc += w[base + i] * (double)c;
+  }
+  edens[bin] += acc;
+}
+
+void launch_edens(const DeviceState& d, int base, int n, int ermax, int ermax_pad, int count_base, cudaStream_t s) {
+  if (n <= 0) return;
+  k_edens<<<(ermax + 127) / 128, 128, 0, s>>>(base, n, ermax, ermax_pad, count_base, d.w, d.counts, d.edens);
+}
+
+// FP64 CUDA-core ecorr update, 64x64 tile per 256 threads (4x4 per thread)
+__global__ void __launch_bounds__(256) k_ecorr_simt(int base, int n, int ermax, int ermax_pad, int count_base,
+    const double* __restrict__ w, const uint32_t* __restrict__ counts, double* __restrict__ ecorr) {
+  __shared__ double As[16][64];
+  __shared__ double Bs[16][64];
+  const int i0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < n; k0 += 16) {
+    for (int t = threadIdx.x; t < 16 * 64; t += 256) {
+      const int kk = t / 64, col = t % 64;
+      const int cnt = base + k0 + kk;
+      double va = 0.0, vb = 0.0;
+      if (k0 + kk < n) {
+        const uint32_t* row = counts + (size_t)(cnt - count_base) * ermax_pad;
+        if (i0 + col < ermax) va = w[cnt] * (double)row[i0 + col];
+        if (j0 + col < ermax) vb = (double)row[j0 + col];
+      }
+      As[kk][col] = va;
+      Bs[kk][col] = vb;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { av[u] = As[kk][ty * 4 + u]; bv[u] = Bs[kk][tx * 4 + u]; }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] += av[u] * bv[v];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+      if (i < ermax && j < ermax) ecorr[(size_t)i * ermax + j] += acc[u][v];
+    }
+}
+
+void launch_ecorr_simt(const DeviceState& d, int base, int n, int ermax, int ermax_pad, int count_base, cudaStream_t s) {
+  if (n <= 0) return;
+  dim3 grid((ermax + 63) / 64, (ermax + 63) / 64);
+  k_ecorr_simt<<<grid, 256, 0, s>>>(base, n, ermax, ermax_pad, count_base, d.w, d.counts, d.ecorr);
+}
+
+}  // namespace erm

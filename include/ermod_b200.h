@@ -1,0 +1,271 @@
+/*
+ * ermod_b200.h -- C-ABI of the B200 (sm_100a) energy-distribution engine.
+ *
+ * This library replaces the per-frame hot path of ERmod's `erdst`:
+ *   realcal   (erdst/realcal.F90)   solute-solvent LJ + real-space Ewald pair energies
+ *   insertion (erdst/insertion.F90) test-particle placement for refs mode
+ *   recpcal   (erdst/recpcal.F90)   smooth-PME reciprocal-space energies (cuFFT for the FFT)
+ *   engproc   (erdst/engproc.F90)   binning onto the energy mesh, edens / ecorr accumulation
+ *
+ * The reference drives that path through the module-procedure trio
+ *   engclear        erdst/engproc.F90:321-340
+ *   engconst(stnum) erdst/engproc.F90:353-517
+ *   engstore(stnum) erdst/engproc.F90:520-725
+ * called from trjmain (erdst/enganal.F90:86-95) with all state in module
+ * `engmain` (erdst/engmain.F90:314-348).  The entry points below keep that
+ * call structure: a Fortran host binds them through ISO_C_BINDING (the
+ * interface module is given in INTEGRATION.md), a C/C++ host calls them
+ * directly.  All state lives in an opaque context instead of module globals.
+ *
+ * Conventions
+ *   - Plain C types only.  Arrays are caller-owned HOST memory unless a
+ *     name ends in `_dev`.  Multi-dimensional arrays use the reference's
+ *     Fortran (column-major) layout: sitepos(3, n) is x,y,z per atom.
+ *   - Indices stored in arrays (ljtype, uvspec, ...) are 1-based as in the
+ *     reference.
+ *   - Every call is synchronous: on return the device work is complete and
+ *     host outputs are written.
+ *   - Return value: 0 success, > 0 warning (the reference's `warning`,
+ *     erdst/mpiproc.F90:238-252), < 0 error (the reference's
+ *     `halt_with_error`, erdst/mpiproc.F90:181-236).  The reference's
+ *     7-character code ("eng_min", "eng_sft", ...) is available from
+ *     ermod_last_error().  The library never aborts the process.
+ *   - One context per host thread; a context is not re-entrant.
+ */
+#ifndef ERMOD_B200_H
+#define ERMOD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ERMOD_ABI_VERSION 1
+
+/* ---- status codes --------------------------------------------------- */
+#define ERMOD_OK               0
+#define ERMOD_WARN_MBIN        1   /* warning('mbin'): energy in the last bin (engproc.F90:1161-1166) */
+#define ERMOD_ERR_ARG        (-1)  /* invalid argument / unsupported parameter combination */
+#define ERMOD_ERR_CUDA       (-2)  /* CUDA / cuFFT failure */
+#define ERMOD_ERR_ENG_MIN   (-10)  /* halt_with_error('eng_min') engproc.F90:1143-1146 */
+#define ERMOD_ERR_ENG_SFT   (-11)  /* halt_with_error('eng_sft') engproc.F90:1151-1156 */
+#define ERMOD_ERR_ENG_CNS   (-12)  /* halt_with_error('eng_cns') engproc.F90:924 */
+#define ERMOD_ERR_RCP_CNS   (-13)  /* halt_with_error('rcp_cns') recpcal.F90:350 */
+#define ERMOD_ERR_INS_GEO   (-14)  /* halt_with_error('ins_geo') insertion.F90:154-156 */
+#define ERMOD_ERR_ENG_ECD   (-15)  /* halt_with_error('eng_ecd') engproc.F90:193 (mesh) */
+#define ERMOD_ERR_CELL      (-16)  /* cell too small for the cutoff (realcal.F90:849-856) */
+#define ERMOD_ERR_OVERFLOW  (-17)  /* an internal fixed-size limit was exceeded */
+#define ERMOD_ERR_UNSUPPORTED (-20)
+
+/* ---- constants mirrored from erdst/engmain.F90:352-375 --------------- */
+#define ERMOD_SLT_SOLN        1
+#define ERMOD_SLT_REFS_RIGID  2
+#define ERMOD_SLT_REFS_FLEX   3
+#define ERMOD_PT_SOLVENT      0
+#define ERMOD_PT_SOLUTE       1
+#define ERMOD_PT_TEST_RIGID   2
+#define ERMOD_PT_TEST_FLEX    3
+#define ERMOD_SYS_NONPERIODIC 0
+#define ERMOD_SYS_PERIODIC    1
+#define ERMOD_ES_NVT          1
+#define ERMOD_ES_NPT          2
+#define ERMOD_EL_COULOMB      0
+#define ERMOD_EL_EWALD        1
+#define ERMOD_EL_PME          2
+#define ERMOD_EL_PPPM         3
+#define ERMOD_LJSWT_POT_CHM   0
+#define ERMOD_LJSWT_POT_GMX   1
+#define ERMOD_LJSWT_FRC_CHM   2
+#define ERMOD_LJSWT_FRC_GMX   3
+#define ERMOD_INSPOS_RANDOM   0
+#define ERMOD_INSPOS_NOCHANGE 1
+#define ERMOD_INSROT_RANDOM   0
+#define ERMOD_INSROT_NOCHANGE 1
+
+/* Insertion proposal (refs mode). */
+#define ERMOD_PROPOSAL_UNIFORM 0   /* the reference's uniform insertion (insertion.F90:152-162) */
+#define ERMOD_PROPOSAL_LEARNED 1   /* MLP voxel proposal mixed with uniform, p/q weighted */
+
+/*
+ * Run parameters: &ene_param after iniparam (erdst/setconf.F90:133-438)
+ * has applied its defaults.  `temp` is kcal/mol (setconf.F90:304).
+ */
+typedef struct ermod_params {
+  int32_t slttype, boxshp, estype, cltype, ljswitch;
+  int32_t splodr, ms1max, ms2max, ms3max;
+  int32_t maxins;                 /* insertions per frame (refs); ignored in soln */
+  int32_t corrcal, selfcal, wgtslf;
+  int32_t insposition, insorient;
+  int32_t iseed;                  /* seed of the insertion random stream */
+  double  temp;                   /* kcal/mol */
+  float   elecut, lwljcut, upljcut, screen;
+  /* engine options (no reference counterpart; 0 = automatic) */
+  int32_t ins_chunk;              /* insertions per PME chunk (16 or 32; 0 = tuned) */
+  int32_t ecorr_batch;            /* insertions per ecorr GEMM batch (0 = auto) */
+  int32_t weight_bits;            /* fixed-point bits of ecorr weights (0 = 24) */
+  int32_t proposal;               /* ERMOD_PROPOSAL_* */
+  int32_t keep_uvengy;            /* 1: keep per-molecule energies for ermod_get_uvengy */
+  int32_t ecorr_path;             /* 0: INT8 tensor-core GEMM, 1: FP64 CUDA-core kernel */
+  int32_t reserved[6];
+} ermod_params;
+
+/*
+ * System topology after setparam (erdst/setconf.F90:516-844).
+ * Molecules are ordered as in the reference: for refs mode the test
+ * particle is the LAST molecule (engproc.F90:99-101).  Atom arrays cover
+ * numatm = sum(numsite) atoms, i.e. one copy of the test particle.
+ */
+typedef struct ermod_topology {
+  int32_t nummol;
+  const int32_t* numsite;     /* [nummol] */
+  const int32_t* sluvid;      /* [nummol] ERMOD_PT_* */
+  const int32_t* uvspec;      /* [nummol] solvent species 1..numslv, 0 = solute (engproc.F90:112-118) */
+  const float*   charge;      /* [numatm] already x18.22261721 (setconf.F90:834) */
+  const int32_t* ljtype;      /* [numatm] 1-based into the LJ tables */
+  const float*   sitemass;    /* [numatm] */
+  int32_t        ljtype_max;
+  const float*   ljene_mat;   /* [ljtype_max*ljtype_max] column-major (setconf.F90:813-826) */
+  const float*   ljlensq_mat; /* [ljtype_max*ljtype_max] */
+  const float*   bfcoord;     /* [3*s] body-fixed test-particle coordinates (refs rigid), else NULL */
+} ermod_topology;
+
+/* Energy mesh built by enginit (erdst/engproc.F90:36-319). */
+typedef struct ermod_mesh {
+  int32_t numslv, ermax, esmax;
+  const double*  uvcrd;      /* [ermax] concatenated over species */
+  const int32_t* uvmax;      /* [numslv] */
+  const int32_t* uvsoft;     /* [numslv] */
+  const double*  escrd;      /* [esmax] self-energy mesh (may be NULL if selfcal == 0) */
+} ermod_mesh;
+
+/* &hist namelist (engproc.F90:68-70). */
+typedef struct ermod_hist {
+  double ecdmin, ecfmns, ecdcen, eccore, ecdmax;
+  double eclbin, ecfbin, ec0bin, finfac;
+  int32_t pecore;
+} ermod_hist;
+
+/* Per-division accumulators (engmain.F90:327-347), fetched by engstore. */
+typedef struct ermod_accum {
+  double* edens;      /* [ermax] */
+  double* ecorr;      /* [ermax*ermax] column-major, or NULL */
+  double* eself;      /* [esmax] or NULL */
+  float*  slnuv;      /* [numslv] soln only, or NULL */
+  float*  minuv;      /* [numslv+1], index 0 = self energy */
+  float*  maxuv;      /* [numslv+1] */
+  double  avslf, engnorm, engsmpl, voffset;
+  int32_t voffset_initialized;
+} ermod_accum;
+
+typedef struct ermod_ctx ermod_ctx;
+
+/* ABI version (ERMOD_ABI_VERSION). */
+int32_t ermod_abi_version(void);
+
+/*
+ * enginit's energy-coordinate mesh (engproc.F90:171-226, 264-281) for
+ * `numslv` species sharing one &hist set, without EcdInfo/EcdMesh files.
+ * Outputs may be NULL to query sizes: *ermax, *esmax, *pemax, *pesoft.
+ * uvcrd needs numslv*pemax entries, escrd pesoft entries.
+ */
+int32_t ermod_enginit_mesh(const ermod_hist* hist, int32_t numslv,
+                           double* uvcrd, int32_t* uvmax, int32_t* uvsoft,
+                           double* escrd, int32_t* ermax, int32_t* esmax);
+
+/*
+ * Create a context on CUDA device `device`.  Copies everything it needs;
+ * the caller's arrays may be freed afterwards.  Replaces the one-time
+ * setup done by enginit (engproc.F90:36-319), recpcal_init
+ * (recpcal.F90:40-95) and instslt('init') (insertion.F90:48-62).
+ */
+int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* params,
+                     const ermod_topology* topo, const ermod_mesh* mesh);
+
+/* engclear (engproc.F90:321-340): zero the per-division accumulators. */
+int32_t ermod_engclear(ermod_ctx* ctx);
+
+/*
+ * engconst (engproc.F90:353-517) for one frame.
+ *   sitepos             [3*numatm_phys]: coordinates of the physical atoms
+ *                       (solvent + soln solute) as read by getconf_parallel
+ *                       (setconf.F90:849-986); the test particle is NOT included.
+ *   cell                [9] column-major cell vectors (engmain.F90:323).
+ *   stat_weight_system  frame weight (setconf.F90:974).
+ *   ins_conf            refs only: NULL = rigid bfcoord for every insertion;
+ *                       else [3*s*maxins] per-insertion solute coordinates
+ *                       (what getsolute reads from SltConf, insertion.F90:393-543),
+ *                       to which insposition / insorient are then applied.
+ *   ins_weight          refs only: NULL = 1.0, else [maxins] per-insertion
+ *                       structure weight (insertion.F90:541-542).
+ *   flceng              soln only: [numslv*numslt] per-solute energy sums
+ *                       (engproc.F90:918,932), or NULL.
+ */
+int32_t ermod_engconst(ermod_ctx* ctx, int32_t stnum, const float* sitepos,
+                       const float* cell, float stat_weight_system,
+                       const float* ins_conf, const float* ins_weight,
+                       float* flceng);
+
+/* Same as ermod_engconst with the inputs already in device memory. */
+int32_t ermod_engconst_dev(ermod_ctx* ctx, int32_t stnum, const float* sitepos_dev,
+                           const float* cell, float stat_weight_system,
+                           const float* ins_conf_dev, const float* ins_weight_dev);
+
+/*
+ * Raw accumulators of the current division (engstore's inputs,
+ * engproc.F90:578-604, before normalisation).  NULL members are skipped.
+ */
+int32_t ermod_fetch_accum(ermod_ctx* ctx, ermod_accum* out);
+
+/*
+ * engstore normalisation (engproc.F90:609-628): edens, ecorr and eself
+ * divided by engnorm, avslf / engnorm, and the two avediv entries
+ * avediv(division,1) = engnorm/engsmpl,
+ * avediv(division,2) = voffset -/+ temp*log(avslf)  (soln / refs).
+ * Writes the normalised arrays into `out` (same members as ermod_fetch_accum)
+ * and avediv[2].  Does not clear the accumulators (call ermod_engclear).
+ */
+int32_t ermod_engstore(ermod_ctx* ctx, ermod_accum* out, double* avediv);
+
+/*
+ * Per-molecule energies of the last engconst call, the reference's
+ * uvengy(slvmax, maxdst) and uvengy0(maxdst) (engproc.F90:369-370,
+ * 442-457) in FP64.  uvengy is column-major: molecule index fastest,
+ * molecules in tagpt order (physical molecules in input order).
+ * Either pointer may be NULL.
+ */
+int32_t ermod_get_uvengy(ermod_ctx* ctx, double* uvengy, double* uvengy0);
+
+/*
+ * Solute coordinates of every insertion of the last engconst call
+ * ([3*s*maxins], the reference's sitepos(:, numatm+1 ...) copies written
+ * by instslt, insertion.F90:100-375) and the per-insertion importance
+ * weights ([maxins], 1.0 for uniform insertion).  Either may be NULL.
+ */
+int32_t ermod_get_insertions(ermod_ctx* ctx, float* ins_sitepos, double* ins_weight);
+
+/* Sizes: slvmax, maxdst, number of solute sites s, numatm_phys. */
+int32_t ermod_get_sizes(ermod_ctx* ctx, int32_t* slvmax, int32_t* maxdst,
+                        int32_t* nsite_solute, int32_t* numatm_phys);
+
+/* The reference's 7-char error code of the last failing call ("" if none). */
+const char* ermod_last_error(const ermod_ctx* ctx);
+
+/* Device time (ms) of the stages of the last engconst, measured with CUDA
+ * events on the engine's stream (no reference counterpart; profiling):
+ * [0] total, [1] prepare + cell list, [2] insertion, [3] real space,
+ * [4] PME spread, [5] FFT R2C, [6] influence multiply, [7] FFT C2R,
+ * [8] gather + bin, [9] weights + edens, [10] ecorr, [11] number of
+ * target chunks.  n <= 12. */
+int32_t ermod_get_timings(const ermod_ctx* ctx, float* ms, int32_t n);
+
+/* Kernel launches of this library since the context was created, cuFFT's
+ * own kernels excluded (no reference counterpart; profiling). */
+int64_t ermod_get_launch_count(const ermod_ctx* ctx);
+
+void ermod_destroy(ermod_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ERMOD_B200_H */

@@ -1,0 +1,229 @@
+"""GPU parity: the CUDA engine through its C-ABI against the CPU oracle.
+
+Tolerances (stated here, used everywhere below):
+  per-molecule energies   |dE| <= 1e-5 |E| + 2e-5 kcal/mol  (soft region, |E| < 1e3)
+                          |dE| <= 1e-4 |E|                  (core region, overlapping atoms)
+  bin counts              identical except energies within that tolerance of a mesh edge
+  insertion placement     1e-5 A (FP32 placement vs the FP64 restatement)
+  accumulators            1e-9 relative (FP64 sums in a different order)
+"""
+import numpy as np
+import pytest
+
+from ermod_openacc_b200 import Engine, ErmodError
+from ermod_openacc_b200 import _capi as A
+from ermod_openacc_b200 import systems as S
+from _helpers import (COULOMB, MADELUNG_NACL, WIGNER_SC, bins_of, energy_tol, near_edge, nacl_system,
+                      phys_uvspec)
+
+pytestmark = pytest.mark.gpu
+
+
+def check_energies(u, uo):
+    soft = np.abs(uo) < 1.0e3
+    err = np.abs(u - uo)
+    assert np.all(err[soft] <= energy_tol(uo[soft])), f"soft max err {err[soft].max():.3e}"
+    if (~soft).any():
+        assert np.all(err[~soft] <= 1e-4 * np.abs(uo[~soft])), "core region"
+    return err
+
+
+def file_driven(params):
+    """Same run as a flexible solute whose conformations are given per insertion, unchanged."""
+    return dict(params, slttype=A.SLT_REFS_FLEX, insposition=A.INSPOS_NOCHANGE, insorient=A.INSROT_NOCHANGE)
+
+
+def flex_topo(topo):
+    kinds = [A.PT_TEST_FLEX if k == A.PT_TEST_RIGID else k for k in topo.kinds]
+    return S.Topology(topo.species, topo.counts, kinds)
+
+
+@pytest.fixture(scope="module")
+def lib(engine_lib):
+    return engine_lib
+
+
+def test_soln_ljsite(lib, oracle_mod):
+    w = S.make_workload(1, small=True)
+    prm = dict(w.params, keep_uvengy=1)
+    eng = Engine(prm, w.topo, w.hist)
+    orc = oracle_mod.Oracle(prm, w.topo, w.hist)
+    for fr in range(2):
+        pos, cell = w.frame(fr)
+        assert eng.engconst(fr + 1, pos, cell) >= 0
+        assert orc.engconst(fr + 1, pos, cell) >= 0
+        u, u0 = eng.uvengy()
+        uo, u0o = orc.uvengy()
+        check_energies(u, uo)
+        assert u[0, 0] == 0.0   # the solute itself is skipped (engproc.F90:922)
+        np.testing.assert_allclose(eng.flceng, orc.flceng.reshape(eng.flceng.shape), rtol=1e-5, atol=1e-3)
+    a, b = eng.accum(), orc.accum()
+    assert a["engnorm"] == pytest.approx(b["engnorm"], rel=1e-12)
+    assert a["engsmpl"] == b["engsmpl"] == 2
+    np.testing.assert_allclose(a["slnuv"], b["slnuv"], rtol=1e-5, atol=1e-3)
+
+
+def test_refs_ring_placement(lib, oracle_mod):
+    w = S.make_workload(2, small=True, maxins=64)
+    eng = Engine(w.params, w.topo, w.hist)
+    orc = oracle_mod.Oracle(w.params, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    assert eng.engconst(3, pos, cell) >= 0
+    assert orc.engconst(3, pos, cell) >= 0
+    ins, wts = eng.insertions()
+    np.testing.assert_allclose(ins, orc.insertions(), atol=1e-5)
+    assert np.all(wts == 1.0)
+
+
+@pytest.mark.parametrize("config", [2, 3])
+def test_refs_energies_and_bins(lib, oracle_mod, config):
+    w = S.make_workload(config, small=True, maxins=96)
+    prm = dict(w.params, keep_uvengy=1)
+    eng = Engine(prm, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, u0 = eng.uvengy()
+    ins, _ = eng.insertions()
+    # FP64 oracle on the GPU's own placements (file-driven, unchanged)
+    orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist)
+    assert orc.engconst(1, pos, cell, ins_conf=ins) >= 0
+    uo, u0o = orc.uvengy()
+    check_energies(u, uo)
+    np.testing.assert_allclose(u0, u0o, rtol=1e-6, atol=2e-5)
+    # bins: identical except near an edge
+    spec = phys_uvspec(w.topo)
+    bg = bins_of(u, eng.uvcrd, eng.uvmax, spec)
+    bo = bins_of(uo, eng.uvcrd, eng.uvmax, spec)
+    exempt = near_edge(uo, eng.uvcrd, energy_tol(uo))
+    assert np.all((bg == bo) | exempt)
+    assert eng.accum()["engnorm"] == pytest.approx(orc.accum()["engnorm"], rel=1e-6)
+
+
+def test_histogram_is_exact_count(lib):
+    """With unit weights (wgtslf=0, NVT) edens is the exact integer histogram of the energies."""
+    w = S.make_workload(2, small=True, maxins=96)
+    prm = dict(w.params, keep_uvengy=1, wgtslf=0, estype=A.ES_NVT)
+    eng = Engine(prm, w.topo, w.hist)
+    pos, cell = w.frame(2)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, _ = eng.uvengy()
+    bg = bins_of(u, eng.uvcrd, eng.uvmax, phys_uvspec(w.topo))
+    cnt = np.zeros((u.shape[0], eng.ermax))
+    for i in range(u.shape[0]):
+        np.add.at(cnt[i], bg[i], 1.0)
+    a = eng.accum()
+    assert a["engnorm"] == u.shape[0]
+    np.testing.assert_array_equal(a["edens"], cnt.sum(axis=0))
+    np.testing.assert_array_equal(a["ecorr"], cnt.T @ cnt)
+
+
+def test_refs_accumulators_match_oracle(lib, oracle_mod):
+    """edens / ecorr / scalars over two frames agree with the oracle run on the same placements."""
+    w = S.make_workload(2, small=True, maxins=64)
+    prm = dict(w.params, keep_uvengy=1)
+    eng = Engine(prm, w.topo, w.hist)
+    orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist)
+    flips = 0
+    for fr in range(2):
+        pos, cell = w.frame(fr)
+        assert eng.engconst(fr + 1, pos, cell) >= 0
+        ins, _ = eng.insertions()
+        assert orc.engconst(fr + 1, pos, cell, ins_conf=ins) >= 0
+        u, _ = eng.uvengy()
+        uo, _ = orc.uvengy()
+        spec = phys_uvspec(w.topo)
+        flips += int((bins_of(u, eng.uvcrd, eng.uvmax, spec) != bins_of(uo, eng.uvcrd, eng.uvmax, spec)).sum())
+    a, b = eng.accum(), orc.accum()
+    for k in ("engnorm", "avslf", "engsmpl", "voffset"):
+        assert a[k] == pytest.approx(b[k], rel=1e-6), k
+    n = w.topo.nummol - 1
+    if flips == 0:
+        np.testing.assert_allclose(a["edens"], b["edens"], rtol=1e-6, atol=1e-9 * b["engnorm"])
+        np.testing.assert_allclose(a["ecorr"], b["ecorr"], rtol=1e-6, atol=1e-9 * b["engnorm"] * n)
+    # sum_j ecorr(j, i) = N_mol * edens(i)
+    np.testing.assert_allclose(a["ecorr"].sum(axis=0), n * a["edens"], rtol=1e-6, atol=1e-6 * a["engnorm"])
+    np.testing.assert_allclose(a["minuv"], b["minuv"], rtol=1e-4)
+    np.testing.assert_allclose(a["maxuv"], b["maxuv"], rtol=1e-3)
+
+
+def test_engstore_normalisation(lib):
+    w = S.make_workload(2, small=True, maxins=32)
+    eng = Engine(w.params, w.topo, w.hist)
+    for fr in range(3):
+        pos, cell = w.frame(fr)
+        eng.engconst(fr + 1, pos, cell)
+    raw = eng.accum()
+    norm, avediv = eng.engstore()
+    np.testing.assert_allclose(norm["edens"], raw["edens"] / raw["engnorm"], rtol=1e-15)
+    assert norm["edens"].sum() == pytest.approx(w.topo.nummol - 1, rel=1e-12)
+    assert avediv[0] == pytest.approx(raw["engnorm"] / raw["engsmpl"], rel=1e-15)
+    assert avediv[1] == pytest.approx(raw["voffset"] + w.params["temp"] * np.log(raw["avslf"] / raw["engnorm"]),
+                                      rel=1e-12)
+    eng.engclear()
+    z = eng.accum()
+    assert z["engnorm"] == 0 and not z["edens"].any() and not z["ecorr"].any()
+
+
+@pytest.mark.parametrize("K,order", [(32, 6), (32, 4)])
+def test_madelung_gpu(lib, K, order):
+    prm, topo, hist, pos, cell, ins, L = nacl_system(K=K, order=order)
+    eng = Engine(dict(prm, keep_uvengy=1), topo, hist)
+    assert eng.engconst(1, pos, cell, ins_conf=ins) >= 0
+    u, u0 = eng.uvengy()
+    e_int = COULOMB * (-MADELUNG_NACL / 2.8 - WIGNER_SC / L)
+    e_self = 0.5 * COULOMB * WIGNER_SC / L
+    assert u.sum() == pytest.approx(e_int, rel=2e-6)
+    assert u0[0] == pytest.approx(e_self, rel=2e-6)
+
+
+@pytest.mark.parametrize("ljswitch", [0, 1, 2, 3])
+def test_lj_switch_forms(lib, oracle_mod, ljswitch):
+    w = S.make_workload(2, small=True, maxins=32)
+    prm = dict(w.params, keep_uvengy=1, ljswitch=ljswitch)
+    eng = Engine(prm, w.topo, w.hist)
+    pos, cell = w.frame(1)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, _ = eng.uvengy()
+    ins, _ = eng.insertions()
+    orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist)
+    assert orc.engconst(1, pos, cell, ins_conf=ins) >= 0
+    check_energies(u, orc.uvengy()[0])
+
+
+def test_bare_coulomb_periodic(lib, oracle_mod):
+    w = S.make_workload(2, small=True, maxins=32)
+    prm = dict(w.params, keep_uvengy=1, cltype=A.EL_COULOMB, wgtslf=0, ecorr_path=1)
+    eng = Engine(prm, w.topo, dict(ecdmin=-80.0))
+    pos, cell = w.frame(0)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, u0 = eng.uvengy()
+    ins, _ = eng.insertions()
+    orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), dict(ecdmin=-80.0))
+    assert orc.engconst(1, pos, cell, ins_conf=ins) >= 0
+    uo, u0o = orc.uvengy()
+    check_energies(u, uo)
+    assert np.all(u0 == 0.0)
+
+
+def test_eng_min_is_reported(lib):
+    w = S.make_workload(2, small=True, maxins=32)
+    eng = Engine(w.params, w.topo, dict(ecdmin=-0.1, ecfmns=-0.05))
+    pos, cell = w.frame(0)
+    with pytest.raises(ErmodError) as ei:
+        eng.engconst(1, pos, cell)
+    assert ei.value.name == "eng_min"
+
+
+def test_ecorr_paths_agree(lib):
+    """The FP64 CUDA-core ecorr kernel and the default path give the same matrix."""
+    w = S.make_workload(2, small=True, maxins=128)
+    pos, cell = w.frame(0)
+    res = []
+    for path in (0, 1):
+        eng = Engine(dict(w.params, ecorr_path=path), w.topo, w.hist)
+        eng.engconst(1, pos, cell)
+        res.append(eng.accum())
+        eng.close()
+    a, b = res
+    np.testing.assert_allclose(a["edens"], b["edens"], rtol=1e-12)
+    np.testing.assert_allclose(a["ecorr"], b["ecorr"], rtol=2e-7, atol=1e-12 * b["engnorm"])
