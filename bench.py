@@ -103,14 +103,18 @@ def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int
     K = w.params["ms1max"]
     n = w.params["splodr"]
     KK, KH = K ** 3, K * K * (K // 2 + 1)
-    if stage == "gather_bin":   # potential grid once + real-space energies + splines + count increments
-        return chunk * KK * 4 + slvmax * chunk * 8 + natoms * (12 * n + 16) + slvmax * chunk * 4
+    if stage == "gather":       # potential grid once + real-space energies in + totals out + splines
+        return chunk * KK * 4 + slvmax * chunk * 8 * 2 + natoms * (12 * n + 16)
+    if stage == "bin":          # every target's energy row in, its count row out (one launch per batch)
+        return min(maxdst, 4096) * (slvmax * 8 + ermax * 4)
     if stage == "influence":    # spectrum read + write, influence function read
         return chunk * KH * 8 * 2 + KH * 4
+    if stage == "transpose":    # potential grids read once, written once
+        return 2 * chunk * KK * 4
     if stage == "spread":       # zero + scatter of the charge grids
         return chunk * KK * 4
-    if stage == "real":         # solvent coordinates + real-space energy matrix write
-        return natoms * 16 + slvmax * chunk * 8
+    if stage == "real":         # solvent coordinates + real-space energy matrix of the batch
+        return natoms * 16 + slvmax * maxdst * 8
     if stage == "ecorr":        # counts read twice + ecorr read-modify-write
         return 2 * maxdst * ermax * 4 + 16 * ermax * ermax
     return 0.0
@@ -249,11 +253,12 @@ def main():
     value = ws * units * args.steps / (dev_ms * 1e-3)
     e2e = ws * units * args.steps / e2e_s
     # roofline of the dominant engine kernel (cuFFT's own kernels are library code)
-    ours = ["real", "spread", "influence", "gather_bin", "ecorr"]
+    ours = ["real", "spread", "influence", "transpose", "gather", "bin", "ecorr"]
     dom = max(ours, key=lambda k: stage[k])
-    per_frame_launches = {"real": stage["chunks"], "spread": stage["chunks"], "influence": stage["chunks"],
-                          "gather_bin": stage["chunks"], "ecorr": 1.0}
-    n_launch = per_frame_launches[dom]  # summed over steps in `stage`
+    nbatch = -(-eng.maxdst // 4096)
+    per_frame_launches = {"real": nbatch, "spread": stage["chunks"], "influence": stage["chunks"],
+                          "transpose": stage["chunks"], "gather": stage["chunks"], "bin": nbatch, "ecorr": nbatch}
+    n_launch = per_frame_launches[dom] * (args.steps if dom in ("real", "bin", "ecorr") else 1)
     per_launch_ms = stage[dom] / n_launch
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak, peak_src = 6650.0, "fallback"
@@ -262,8 +267,8 @@ def main():
     chunk = 32
     bytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst)
     achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
-    kname = {"gather_bin": "k_gather_bin", "real": "k_real", "spread": "k_spread", "influence": "k_influence",
-             "ecorr": "k_ecorr"}[dom]
+    kname = {"gather": "k_gather", "bin": "k_bin", "real": "k_real", "spread": "k_spread_box", "transpose": "k_transpose_phi",
+             "influence": "k_influence", "ecorr": "k_ecorr"}[dom]
     traffic = traffic_from_profiles(kname)
     stage_share = {k: round(stage[k] / max(stage["total"], 1e-9), 4) for k in Engine.STAGES
                    if k not in ("total", "chunks")}

@@ -139,6 +139,12 @@ __device__ __forceinline__ float spline_value(const float* coeff, int order, flo
   return f;
 }
 
+// grid index r in [-(order-1), K] wrapped into [0, K) (the reference's modulo, recpcal.F90:388-390)
+__device__ __forceinline__ int wrapk(int r, int K) {
+  r += (r < 0) ? K : 0;
+  return r - ((r >= K) ? K : 0);
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -80,13 +80,14 @@ struct ermod_ctx {
   std::vector<cudaEvent_t> pev;
   std::vector<int> ptag;
   int pused = 0;
-  float timings[12] = {0};
+  float timings[14] = {0};
   long long launches = 0;
   int use_tc = 1;
 };
 
 enum Stage { kStPrep = 1, kStIns = 2, kStReal = 3, kStSpread = 4, kStR2C = 5, kStInfl = 6, kStC2R = 7,
-             kStGather = 8, kStWeights = 9, kStEcorr = 10 };
+             kStGather = 8, kStBin = 9, kStWeights = 10, kStEcorr = 11, kStChunks = 12, kStTranspose = 13,
+             kNumTimings = 14 };
 
 namespace {
 
@@ -108,7 +109,8 @@ void free_all(ermod_ctx* c) {
                   d.slt_mass, d.bfcoord, d.uvcrd, d.spec_off, d.uvsoft, d.escrd, d.posraw, d.slvn, d.spl, d.grd,
                   d.anchor, d.cellof, d.cellcount, d.cellstart, d.molsorted, d.rmol, d.ins_conf, d.insw_in,
                   d.tgt_raw, d.tgt_n, d.tgt_c, d.tgt_mol, d.selfreal, d.selfrec, d.u0, d.w, d.etot, d.flceng,
-                  d.grid, d.spec, d.phi, d.engfac, d.splfc, d.E, d.uvengy, d.counts, d.edens, d.ecorr, d.eself,
+                  d.grid, d.spec, d.phi, d.engfac, d.splfc, d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
+                  d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.ecorr, d.eself,
                   d.slnuv, d.minuv, d.maxuv, d.scal, d.status, c->tc_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -252,6 +254,10 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   };
   if (p.cltype != ERMOD_EL_PME && p.cltype != ERMOD_EL_COULOMB) return bad(ERMOD_ERR_UNSUPPORTED, "set_prs");
   if (p.cltype == ERMOD_EL_PME && (p.splodr < 2 || p.splodr > kMaxOrder)) return bad(ERMOD_ERR_ARG, "set_ewa");
+  if (p.cltype == ERMOD_EL_PME &&
+      (p.ms1max < p.splodr || p.ms2max < p.splodr || p.ms3max < p.splodr || p.ms1max > kMaxGrid ||
+       p.ms2max > kMaxGrid || p.ms3max > kMaxGrid))
+    return bad(ERMOD_ERR_ARG, "set_ewa");
   if (p.boxshp == ERMOD_SYS_NONPERIODIC && (p.estype == ERMOD_ES_NPT || p.cltype != ERMOD_EL_COULOMB))
     return bad(ERMOD_ERR_ARG, "set_prs");
   if (p.slttype < 1 || p.slttype > 3) return bad(ERMOD_ERR_ARG, "set_slt");
@@ -374,7 +380,19 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     CK(dalloc(&d.grid, (size_t)ctx->chunk * KK)); CK(dalloc(&d.spec, (size_t)ctx->chunk * KH));
     CK(dalloc(&d.phi, (size_t)ctx->chunk * KK)); CK(dalloc(&d.engfac, KH)); CK(dalloc(&d.splfc, K1 + K2 + K3));
   }
-  CK(dalloc(&d.E, SM * ctx->chunk));
+  CK(dalloc(&d.E, SM * ctx->batch));
+  CK(dalloc(&d.Etot, SM * ctx->batch));
+  CK(dalloc(&d.tgtq, MD));
+  CK(dalloc(&d.twt, MD));
+  CK(dalloc(&d.sbin, MD));
+  if (pme) {
+    CK(dalloc(&d.gacc, (size_t)ctx->chunk * KK));
+    CK(dalloc(&d.boxinfo, 2 * (size_t)ctx->chunk));
+    CK(dalloc(&d.partial, (size_t)ctx->chunk * kInflBlocks));
+    CK(dalloc(&d.done, (size_t)ctx->chunk));
+    CK(cudaMemsetAsync(d.done, 0, sizeof(unsigned int) * ctx->chunk, ctx->st));
+    if (setup_spread_smem() != 0) return bad(ERMOD_ERR_CUDA, "spr_smem");
+  }
   if (p.keep_uvengy) CK(dalloc(&d.uvengy, MD * SM));
   CK(dalloc(&d.counts, (size_t)ctx->batch * ctx->ermax_pad));
   CK(dalloc(&d.edens, ctx->ermax));
@@ -403,6 +421,23 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   std::vector<int> tm(MD, -1);
   if (!refs) for (size_t c = 0; c < MD; ++c) tm[c] = ctx->tgt_k[c];
   CK(h2d(d.tgt_mol, tm.data(), MD, st));
+  {  // net solute charge of every target (mol_charge(tagslt), engproc.F90:994, 1014)
+    std::vector<double> q(MD, (double)qs);
+    if (!refs)
+      for (size_t c = 0; c < MD; ++c) {
+        float s = 0.f;
+        const int i = ctx->sltlist[c];
+        for (int at = ctx->molbeg_all[i]; at < ctx->molbeg_all[i + 1]; ++at) s += ctx->charge[at];
+        q[c] = s;
+      }
+    CK(h2d(d.tgtq, q.data(), MD, st));
+  }
+  {
+    BinArgs ba{};
+    ba.ermax = ctx->ermax;
+    ba.ermax_pad = ctx->ermax_pad;
+    if (setup_bin_smem(ba) != 0) return bad(ERMOD_ERR_OVERFLOW, "ermax_lim");
+  }
   if (pme) {
     std::vector<double> sf(K1 + K2 + K3);
     spline_axis(K1, p.splodr, sf.data());
@@ -413,7 +448,7 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     int inR[3] = {K3, K2, K1}, onC[3] = {K3, K2, Kh1};
     CF(cufftPlanMany(&ctx->r2c, 3, n, inR, 1, (int)KK, onC, 1, (int)KH, CUFFT_R2C, ctx->chunk));
     int inC[3] = {K3, K2, Kh1}, onR[3] = {K3, K2, K1};
-    CF(cufftPlanMany(&ctx->c2r, 3, n, inC, 1, (int)KH, onR, ctx->chunk, 1, CUFFT_C2R, ctx->chunk));
+    CF(cufftPlanMany(&ctx->c2r, 3, n, inC, 1, (int)KH, onR, 1, (int)KK, CUFFT_C2R, ctx->chunk));
     ctx->plans = true;
     CF(cufftSetStream(ctx->r2c, st));
     CF(cufftSetStream(ctx->c2r, st));
@@ -641,14 +676,14 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
     wa.npt_factor = f;
   }
   BinArgs ba{};
-  ba.ermax_pad = ctx->ermax_pad; ba.numslv = ctx->numslv; ba.slttype = p.slttype;
-  ba.keep_uvengy = d.uvengy != nullptr;
-  // ---- chunks / batches ----
+  ba.ermax = ctx->ermax; ba.ermax_pad = ctx->ermax_pad; ba.numslv = ctx->numslv; ba.slttype = p.slttype;
+  // ---- batches of targets, each in chunks of `chunk` PME solves ----
   const int chunk = ctx->chunk;
   for (int bb = 0; bb < ctx->maxdst; bb += ctx->batch) {
     const int nbatch = std::min(ctx->batch, ctx->maxdst - bb);
-    CK(cudaMemsetAsync(d.counts, 0, sizeof(uint32_t) * (size_t)ctx->batch * ctx->ermax_pad, st));
-    ba.count_base = bb;
+    launch_real(a, d, bb, nbatch, ctx->batch, st);
+    mark(ctx, kStReal);
+    nl += 1;
     for (int cb = bb; cb < bb + nbatch; cb += chunk) {
       const int nb = std::min(chunk, bb + nbatch - cb);
       if (pme) {
@@ -658,16 +693,22 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
         mark(ctx, kStR2C);
         launch_influence(a, d, cb, nb, chunk, st);
         mark(ctx, kStInfl);
-        CF(cufftExecC2R(ctx->c2r, (cufftComplex*)d.spec, d.phi));
+        CF(cufftExecC2R(ctx->c2r, (cufftComplex*)d.spec, d.grid));  // natural layout, reuses the charge grid
         mark(ctx, kStC2R);
-        nl += 2;
+        launch_transpose_phi(a, d, st);
+        mark(ctx, kStTranspose);
+        nl += 4;
       }
-      launch_real(a, d, cb, nb, chunk, st);
-      mark(ctx, kStReal);
-      launch_gather_bin(a, d, ba, cb, nb, chunk, st);
+      launch_gather(a, d, cb, bb, nb, chunk, ctx->batch, st);
       mark(ctx, kStGather);
-      nl += 2;
+      nl += 1;
     }
+    launch_bin(d, ba, bb, nbatch, ctx->slvmax, st);
+    mark(ctx, kStBin);
+    nl += 1;
+    if (d.uvengy)
+      CK(cudaMemcpyAsync(d.uvengy + (size_t)bb * ctx->slvmax, d.Etot, sizeof(double) * (size_t)nbatch * ctx->slvmax,
+                         cudaMemcpyDeviceToDevice, st));
     launch_weights(d, wa, bb, nbatch, st);
     launch_edens(d, bb, nbatch, ctx->ermax, ctx->ermax_pad, bb, st);
     nl += 3;
@@ -695,12 +736,13 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
     ctx->timings[ctx->ptag[k]] += ms;
     ctx->timings[0] += ms;
   }
-  ctx->timings[11] = (float)((ctx->maxdst + chunk - 1) / chunk);
+  ctx->timings[kStChunks] = (float)((ctx->maxdst + chunk - 1) / chunk);
   ctx->launches += nl;
   if (hs.flags & kErrEngCns) return set_error(ctx, ERMOD_ERR_ENG_CNS, "eng_cns");
   if (hs.flags & kErrEngMin) return set_error(ctx, ERMOD_ERR_ENG_MIN, "eng_min");
   if (hs.flags & kErrEngSft) return set_error(ctx, ERMOD_ERR_ENG_SFT, "eng_sft");
   if (hs.flags & kErrOverflow) return set_error(ctx, ERMOD_ERR_OVERFLOW, "ermod_ovf");
+  if (hs.flags & kErrGrid) return set_error(ctx, ERMOD_ERR_OVERFLOW, "spr_box");
   if ((hs.flags & kWarnMbin) && ctx->warn_bin_firsttime) {
     ctx->warn_bin_firsttime = false;
     return set_error(ctx, ERMOD_WARN_MBIN, "mbin");
@@ -847,7 +889,7 @@ const char* ermod_last_error(const ermod_ctx* ctx) { return ctx ? ctx->err.c_str
 
 int32_t ermod_get_timings(const ermod_ctx* ctx, float* ms, int32_t n) {
   if (!ctx || !ms) return ERMOD_ERR_ARG;
-  for (int i = 0; i < n && i < 12; ++i) ms[i] = ctx->timings[i];
+  for (int i = 0; i < n && i < kNumTimings; ++i) ms[i] = ctx->timings[i];
   return ERMOD_OK;
 }
 

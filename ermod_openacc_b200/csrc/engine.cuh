@@ -14,6 +14,8 @@ namespace erm {
 constexpr int kMaxOrder = 8;       // PME spline order limit (splodr)
 constexpr int kMaxSoluteSites = 1024;
 constexpr int kMaxLjTypes = 64;
+constexpr int kInflBlocks = 64;    // CTAs per target in the influence multiply
+constexpr int kMaxGrid = 256;      // largest PME grid dimension (x rows are one CTA dimension)
 
 // Everything the frame kernels read, passed by value.
 struct FrameArgs {
@@ -81,7 +83,15 @@ struct DeviceState {
   float* phi = nullptr;      // [K^3*chunk], insertion fastest
   float* engfac = nullptr;   // [K3*K2*Kh1]
   double* splfc = nullptr;   // [K1+K2+K3]
-  double* E = nullptr;       // [slvmax*chunk] real-space energies of the chunk
+  double* E = nullptr;       // [slvmax*batch] real-space energies of the batch, molecule-major
+  double* Etot = nullptr;    // [batch*slvmax] total pair energies of the batch, target-major (uvengy layout)
+  double* tgtq = nullptr;    // [maxdst] net charge of each target's solute
+  double* twt = nullptr;     // [maxdst] total_weight of each target
+  int* sbin = nullptr;       // [maxdst] self-energy bin of each target (-1: none)
+  long long* gacc = nullptr; // [chunk*K^3] fixed-point spreading box for large solutes
+  int4* boxinfo = nullptr;   // [2*chunk] spreading box origin / extent per target
+  double* partial = nullptr; // [chunk*kInflBlocks] self-energy partial sums
+  unsigned int* done = nullptr; // [chunk] block counters of the self-energy reduction
   double* uvengy = nullptr;  // [maxdst*slvmax] kept when requested
   uint32_t* counts = nullptr;// [batch*ermax_pad]
   // accumulators
@@ -107,14 +117,17 @@ void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int
 void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[3][3], double volume,
                    double screen, cudaStream_t s);
 void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
+int setup_spread_smem();
+void launch_transpose_phi(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
 
 struct BinArgs {
-  int ermax_pad, numslv, slttype, keep_uvengy, count_base, nslv_spec;
-  double qslt_unused;
+  int ermax, ermax_pad, numslv, slttype;
 };
-void launch_gather_bin(const FrameArgs& a, const DeviceState& d, const BinArgs& b, int base, int nb, int chunk,
-                       cudaStream_t s);
+void launch_gather(const FrameArgs& a, const DeviceState& d, int base, int bb, int nb, int chunk, int batch,
+                   cudaStream_t s);
+void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int slvmax, cudaStream_t s);
+int setup_bin_smem(const BinArgs& ba);
 
 struct WeightArgs {
   int slttype, wgtslf, estype, selfcal, numslv, esmax, rigid;

@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(kRealThreads) k_real(FrameArgs a, int base, in
 
 void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
   cudaMemsetAsync(d.E, 0, sizeof(double) * (size_t)a.slvmax * chunk, s);
-  if (nb <= 0) return;
+  if (nb <= 0) return;  // `chunk` is the row stride of E: the batch size
   k_real<<<nb, kRealThreads, 0, s>>>(a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, d.slt_lj, d.molbeg, d.slvn,
                                       d.atom_lj, d.ljene, d.ljlensq, d.anchor, d.cellstart, d.molsorted, d.rmol, d.E);
 }
@@ -458,46 +458,167 @@ void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[
   k_engfac<<<(n + 255) / 256, 256, 0, s>>>(a.K1, a.K2, a.K3, a.Kh1, a.order, m, volume, screen, d.splfc, d.engfac);
 }
 
-// a warp per (target, site): lanes over the order^3 stencil points, global atomics
-__global__ void k_spread(FrameArgs a, int base, int nb, const float4* __restrict__ tgt_raw, float* __restrict__ grid) {
-  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  const int s = a.nsite;
-  if (wid >= nb * s) return;
-  const int b = wid / s, site = wid - b * s;
-  const float4 r = tgt_raw[(size_t)(base + b) * s + site];
-  const CellGeom& g = a.g;
-  float w[3][kMaxOrder];
-  int gi[3];
+// ---------------------------------------------------------------------------
+// Charge spreading, deterministic.  A CTA per target accumulates the
+// order^3 stencil of every solute site into a box around the solute as
+// 2^-40 fixed-point integers (shared memory, or a global scratch box when
+// the solute is large), so the sum does not depend on the order of the
+// additions; the box is written into the grid and k_zero_outside clears the
+// rest of the grid.  The reference spreads with FP32 atomics in global
+// memory (recpcal.F90:453-473), whose sum order varies from run to run.
+// ---------------------------------------------------------------------------
+constexpr int kSpreadThreads = 256;
+constexpr double kFixScale = 1099511627776.0;   // 2^40
+constexpr int kSpreadSmemBytes = 96 * 1024;
+
+// calc_spline_molecule_refs for one site (recpcal.F90:553-574)
+__device__ __forceinline__ void site_spline(const FrameArgs& a, float4 r, float w[3][kMaxOrder], int gi[3]) {
   const int K[3] = {a.K1, a.K2, a.K3};
   for (int m = 0; m < 3; ++m) {
-    float f = g.invcl[m][0] * r.x + g.invcl[m][1] * r.y + g.invcl[m][2] * r.z;
+    float f = a.g.invcl[m][0] * r.x + a.g.invcl[m][1] * r.y + a.g.invcl[m][2] * r.z;
     f = f - floorf(f);
     f = f * (float)K[m];
     const int rci = (int)f;
     for (int spi = 0; spi < a.order; ++spi) w[m][spi] = spline_value(a.spl_coeff, a.order, f - (float)(rci - spi));
     gi[m] = rci;
   }
-  const int n = a.order, n3 = n * n * n;
-  float* gb = grid + (size_t)b * a.K1 * a.K2 * a.K3;
-  for (int t = lane; t < n3; t += 32) {
-    const int c1 = t % n, c2 = (t / n) % n, c3 = t / (n * n);
-    int r1 = (gi[0] - c1) % a.K1; if (r1 < 0) r1 += a.K1;
-    int r2 = (gi[1] - c2) % a.K2; if (r2 < 0) r2 += a.K2;
-    int r3 = (gi[2] - c3) % a.K3; if (r3 < 0) r3 += a.K3;
-    const float v = r.w * w[0][c1] * w[1][c2] * w[2][c3];
-    atomicAdd(&gb[((size_t)r3 * a.K2 + r2) * a.K1 + r1], v);
+}
+
+__device__ __forceinline__ int wrap_half(int d, int K) {  // into (-K/2, K/2]
+  d = wrapk(wrapk(d, K), K);
+  return d > K / 2 ? d - K : d;
+}
+
+// Box coordinate of a site along axis m: the wrapped grid index gi lifted onto
+// the branch of the unwrapped coordinate floor(K * invcl.x) of the raw (whole,
+// unwrapped) solute coordinates, so a solute of any extent up to the grid gets
+// a consistent box; lifted indices equal gi modulo K.
+__device__ __forceinline__ int lifted_index(const FrameArgs& a, float4 r, int m, int gi) {
+  const int K = m == 0 ? a.K1 : (m == 1 ? a.K2 : a.K3);
+  const float f = a.g.invcl[m][0] * r.x + a.g.invcl[m][1] * r.y + a.g.invcl[m][2] * r.z;
+  const int gu = (int)floorf(f * (float)K);
+  const int d = wrap_half(gi - gu, K);  // ~0 up to rounding at a grid line
+  return gu + d;
+}
+
+__global__ void __launch_bounds__(kSpreadThreads) k_spread_box(FrameArgs a, int base, int nb, int cap,
+    const float4* __restrict__ tgt_raw, float* __restrict__ grid, long long* __restrict__ gacc,
+    int4* __restrict__ boxinfo, DevStatus* st) {
+  extern __shared__ long long sacc[];
+  __shared__ int g0[3], lo[3], hi[3];
+  const int b = blockIdx.x;
+  const int K[3] = {a.K1, a.K2, a.K3};
+  const size_t KK = (size_t)a.K1 * a.K2 * a.K3;
+  if (b >= nb) {  // empty slot of a partial chunk: k_zero_outside clears the whole grid
+    if (threadIdx.x == 0) { boxinfo[2 * b] = make_int4(0, 0, 0, 0); boxinfo[2 * b + 1] = make_int4(0, 0, 0, 0); }
+    return;
+  }
+  const int s = a.nsite, n = a.order;
+  const float4* sites = tgt_raw + (size_t)(base + b) * s;
+  if (threadIdx.x == 0) {
+    float w[3][kMaxOrder];
+    int gi[3];
+    site_spline(a, sites[0], w, gi);
+    for (int m = 0; m < 3; ++m) {
+      g0[m] = lifted_index(a, sites[0], m, gi[m]);
+      lo[m] = 1 << 30;
+      hi[m] = -(1 << 30);
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < s; t += blockDim.x) {
+    float w[3][kMaxOrder];
+    int gi[3];
+    site_spline(a, sites[t], w, gi);
+    for (int m = 0; m < 3; ++m) {
+      const int d = lifted_index(a, sites[t], m, gi[m]) - g0[m];
+      atomicMin(&lo[m], d - (n - 1));
+      atomicMax(&hi[m], d);
+    }
+  }
+  __syncthreads();
+  const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+  if (n0 > a.K1 || n1 > a.K2 || n2 > a.K3) {  // solute wider than the periodic grid
+    if (threadIdx.x == 0) {
+      report(st, kErrGrid, -1, base + b, (float)max(n0, max(n1, n2)));
+      boxinfo[2 * b] = make_int4(0, 0, 0, 0);
+      boxinfo[2 * b + 1] = make_int4(0, 0, 0, 0);
+    }
+    return;
+  }
+  const int vol = n0 * n1 * n2;
+  long long* acc = vol <= cap ? sacc : gacc + (size_t)b * KK;
+  for (int i = threadIdx.x; i < vol; i += blockDim.x) acc[i] = 0;
+  __syncthreads();
+  // a warp per site, lanes over the stencil points
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int n3 = n * n * n;
+  for (int t = warp; t < s; t += nw) {
+    const float4 r = sites[t];
+    float w[3][kMaxOrder];
+    int gi[3];
+    site_spline(a, r, w, gi);
+    int d[3];
+    for (int m = 0; m < 3; ++m) d[m] = lifted_index(a, r, m, gi[m]) - g0[m] - lo[m];
+    for (int p = lane; p < n3; p += 32) {
+      const int c1 = p % n, c2 = (p / n) % n, c3 = p / (n * n);
+      const float v = r.w * w[0][c1] * w[1][c2] * w[2][c3];   // recpcal.F90:464-465
+      const int idx = ((d[2] - c3) * n1 + (d[1] - c2)) * n0 + (d[0] - c1);
+      atomicAdd((unsigned long long*)&acc[idx], (unsigned long long)llrint((double)v * kFixScale));
+    }
+  }
+  __syncthreads();
+  float* gb = grid + (size_t)b * KK;
+  auto posmod = [](int x, int K) { const int r = x % K; return r < 0 ? r + K : r; };
+  const int o0 = posmod(g0[0] + lo[0], a.K1), o1 = posmod(g0[1] + lo[1], a.K2), o2 = posmod(g0[2] + lo[2], a.K3);
+  for (int i = threadIdx.x; i < vol; i += blockDim.x) {
+    const int x = i % n0, y = (i / n0) % n1, z = i / (n0 * n1);
+    const int r1 = wrapk(o0 + x, a.K1), r2 = wrapk(o1 + y, a.K2), r3 = wrapk(o2 + z, a.K3);
+    gb[((size_t)r3 * a.K2 + r2) * a.K1 + r1] = (float)((double)acc[i] * (1.0 / kFixScale));
+  }
+  if (threadIdx.x == 0) {
+    boxinfo[2 * b] = make_int4(o0, o1, o2, 1);
+    boxinfo[2 * b + 1] = make_int4(n0, n1, n2, 0);
   }
 }
 
-void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
-  cudaMemsetAsync(d.grid, 0, sizeof(float) * (size_t)chunk * a.K1 * a.K2 * a.K3, s);
-  const int warps = nb * a.nsite;
-  if (warps <= 0) return;
-  k_spread<<<(warps * 32 + 255) / 256, 256, 0, s>>>(a, base, nb, d.tgt_raw, d.grid);
+// zero every grid point outside its target's box (run after k_spread_box).
+// block = (K1 threads along x) x (kRowsPerBlock rows), grid = (K2*K3/kRowsPerBlock, chunk)
+constexpr int kRowsPerBlock = 4;
+
+__global__ void k_zero_outside(FrameArgs a, const int4* __restrict__ boxinfo, float* __restrict__ grid) {
+  const int b = blockIdx.y;
+  const int r1 = threadIdx.x;
+  const int row = blockIdx.x * kRowsPerBlock + threadIdx.y;
+  if (row >= a.K2 * a.K3 || r1 >= a.K1) return;
+  const int r2 = row % a.K2, r3 = row / a.K2;
+  const int4 o = boxinfo[2 * b], ne = boxinfo[2 * b + 1];
+  bool inside = false;
+  if (o.w) {
+    const int x = wrapk(r1 - o.x, a.K1), y = wrapk(r2 - o.y, a.K2), z = wrapk(r3 - o.z, a.K3);
+    inside = x < ne.x && y < ne.y && z < ne.z;
+  }
+  if (!inside) grid[((size_t)b * a.K3 * a.K2 + row) * a.K1 + r1] = 0.0f;
 }
 
-// influence multiply + FP64 self energy of each target (recpcal.F90:482-497)
+void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
+  k_spread_box<<<chunk, kSpreadThreads, kSpreadSmemBytes, s>>>(a, base, nb, kSpreadSmemBytes / 8, d.tgt_raw, d.grid,
+                                                               d.gacc, d.boxinfo, d.status);
+  dim3 blk(a.K1, kRowsPerBlock);
+  dim3 grd((a.K2 * a.K3 + kRowsPerBlock - 1) / kRowsPerBlock, chunk);
+  k_zero_outside<<<grd, blk, 0, s>>>(a, d.boxinfo, d.grid);
+}
+
+int setup_spread_smem() {
+  return cudaFuncSetAttribute(k_spread_box, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpreadSmemBytes) ==
+                 cudaSuccess ? 0 : -1;
+}
+
+// influence multiply + FP64 self energy of each target (recpcal.F90:482-497).
+// The self energy is reduced deterministically: per-block partials, summed in
+// block order by the last block of each target.
 __global__ void k_influence(FrameArgs a, int base, int nb, float2* __restrict__ spec, const float* __restrict__ engfac,
+                            double* __restrict__ partial, unsigned int* __restrict__ done,
                             double* __restrict__ selfrec) {
   const int b = blockIdx.y;
   const int n = a.K3 * a.K2 * a.Kh1;
@@ -513,91 +634,168 @@ __global__ void k_influence(FrameArgs a, int base, int nb, float2* __restrict__ 
     sp[i] = make_float2(v.x * e, v.y * e);
   }
   __shared__ double red[32];
+  __shared__ bool last;
   acc = warp_sum(acc);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
   if (threadIdx.x < 32) {
     double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
     v = warp_sum(v);
-    if (threadIdx.x == 0 && b < nb) atomicAdd(&selfrec[base + b], v);
+    if (threadIdx.x == 0) {
+      partial[(size_t)b * gridDim.x + blockIdx.x] = v;
+      __threadfence();
+      last = atomicAdd(&done[b], 1u) == gridDim.x - 1;
+    }
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double sum = 0.0;
+    const volatile double* pp = partial + (size_t)b * gridDim.x;
+    for (int i = 0; i < (int)gridDim.x; ++i) sum += pp[i];
+    if (b < nb) selfrec[base + b] = sum;
+    done[b] = 0u;
   }
 }
 
+// potential grids [chunk][K^3] (cuFFT's natural C2R output) -> [K^3][chunk]
+// (target fastest, the layout the gather reads one 128-byte row per point)
+__global__ void k_transpose_phi(int KK, const float* __restrict__ in, float* __restrict__ out) {
+  __shared__ float tile[32][33];
+  const int p0 = blockIdx.x * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // (32, 8)
+#pragma unroll
+  for (int j = 0; j < 32; j += 8) {
+    const int b = ty + j, p = p0 + tx;
+    tile[b][tx] = p < KK ? in[(size_t)b * KK + p] : 0.0f;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 32; j += 8) {
+    const int p = p0 + ty + j;
+    if (p < KK) out[(size_t)p * 32 + tx] = tile[tx][ty + j];
+  }
+}
+
+void launch_transpose_phi(const FrameArgs& a, const DeviceState& d, cudaStream_t s) {
+  const int KK = a.K1 * a.K2 * a.K3;
+  k_transpose_phi<<<(KK + 31) / 32, dim3(32, 8), 0, s>>>(KK, d.grid, d.phi);
+}
+
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
-  const int n = a.K3 * a.K2 * a.Kh1;
-  int bx = (n + 256 * 8 - 1) / (256 * 8);
-  if (bx > 256) bx = 256;
-  k_influence<<<dim3(bx, chunk), 256, 0, s>>>(a, base, nb, d.spec, d.engfac, d.selfrec);
+  k_influence<<<dim3(kInflBlocks, chunk), 256, 0, s>>>(a, base, nb, d.spec, d.engfac, d.partial, d.done, d.selfrec);
 }
 
 // ---------------------------------------------------------------------------
-// gather + residual + binning.  A warp per solvent molecule, lane = target
-// of the chunk (chunk == 32): the potential grid is stored target-fastest,
-// so each stencil point is one coalesced 128-byte row.
+// PME gather + residual.  A warp per solvent molecule, lane = target of the
+// chunk (chunk == 32): the potential grid is stored target-fastest, so each
+// stencil point is one coalesced 128-byte row.  Writes the total energy of
+// every (target, molecule) pair into Etot[target][molecule] (the uvengy layout).
 // ---------------------------------------------------------------------------
 constexpr int kGatherThreads = 256;
-constexpr int kMaxSpecSmem = 128;
 
-__global__ void __launch_bounds__(kGatherThreads) k_gather_bin(FrameArgs a, BinArgs ba, int base, int nb, int chunk,
-    const int* __restrict__ molsorted, const int* __restrict__ molbeg, const int* __restrict__ molspec,
-    const float* __restrict__ molq, const float* __restrict__ atom_q, const float* __restrict__ spl,
-    const int4* __restrict__ grd, const float* __restrict__ phi, const double* __restrict__ E,
-    const int* __restrict__ tgt_mol, const float4* __restrict__ tgt_n,
-    const double* __restrict__ uvcrd, const int* __restrict__ spec_off, const int* __restrict__ uvsoft,
-    double* __restrict__ uvengy, uint32_t* __restrict__ counts, double* __restrict__ etot, double* __restrict__ flceng,
-    float* __restrict__ minuv, float* __restrict__ maxuv, DevStatus* st) {
-  __shared__ float smin[kMaxSpecSmem], smax[kMaxSpecSmem];
-  for (int i = threadIdx.x; i < kMaxSpecSmem; i += blockDim.x) { smin[i] = FLT_MAX; smax[i] = -FLT_MAX; }
-  __syncthreads();
+template <int NO>
+__global__ void __launch_bounds__(kGatherThreads) k_gather(FrameArgs a, int base, int bb, int nb, int chunk, int batch,
+    const int* __restrict__ molsorted, const int* __restrict__ molbeg, const float* __restrict__ molq,
+    const float* __restrict__ atom_q, const float* __restrict__ spl, const int4* __restrict__ grd,
+    const float* __restrict__ phi, const double* __restrict__ Ereal, const double* __restrict__ tgtq,
+    const int* __restrict__ tgt_mol, double* __restrict__ Etot) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwt = (gridDim.x * blockDim.x) >> 5;
   const int b = lane;
   const bool active = b < nb;
-  const int cnt = base + b;
+  const int cnt = base + b, bi = cnt - bb;
+  const double qslt = active ? tgtq[cnt] : 0.0;
   const int excl = (active && tgt_mol) ? tgt_mol[cnt] : -1;
-  // solute net charge of this target (sum of its site charges)
-  double qslt = 0.0;
-  if (active) {
-    const float4* tn = tgt_n + (size_t)cnt * a.nsite;
-    for (int i = 0; i < a.nsite; ++i) qslt += (double)tn[i].w;
-    qslt = (double)(float)qslt;
-  }
-  double my_etot = 0.0;
-  const int n = a.order;
+  const int n = NO > 0 ? NO : a.order;
+  const int K1 = a.K1, K2 = a.K2, K3 = a.K3;
   for (int m = gw; m < a.slvmax; m += nwt) {
     const int k = molsorted[m];
-    double e = E[(size_t)k * chunk + b];
+    double e = active ? Ereal[(size_t)k * batch + bi] : 0.0;
     const int b0 = molbeg[k], b1 = molbeg[k + 1];
     if (a.pme) {
       for (int at = b0; at < b1; ++at) {
         const float q = atom_q[at];
         const float* w = spl + (size_t)at * 3 * n;
         const int4 gd = grd[at];
-        for (int c3 = 0; c3 < n; ++c3) {
-          int r3 = (gd.z - c3) % a.K3; if (r3 < 0) r3 += a.K3;
+        float w1[NO > 0 ? NO : kMaxOrder];
+        int r1[NO > 0 ? NO : kMaxOrder];
+#pragma unroll
+        for (int c1 = 0; c1 < (NO > 0 ? NO : kMaxOrder); ++c1)
+          if (c1 < n) { w1[c1] = w[c1]; r1[c1] = wrapk(gd.x - c1, K1); }
+#pragma unroll
+        for (int c3 = 0; c3 < (NO > 0 ? NO : kMaxOrder); ++c3) {
+          if (c3 >= n) break;
+          const int r3 = wrapk(gd.z - c3, K3);
           const float fac1 = q * w[2 * n + c3];
-          for (int c2 = 0; c2 < n; ++c2) {
-            int r2 = (gd.y - c2) % a.K2; if (r2 < 0) r2 += a.K2;
+#pragma unroll
+          for (int c2 = 0; c2 < (NO > 0 ? NO : kMaxOrder); ++c2) {
+            if (c2 >= n) break;
+            const int r2 = wrapk(gd.y - c2, K2);
             const float fac2 = fac1 * w[n + c2];
-            const size_t row = ((size_t)r3 * a.K2 + r2) * a.K1;
+            const float* rowp = phi + ((size_t)(r3 * K2 + r2) * K1) * chunk + b;
             float part = 0.0f;
-            for (int c1 = 0; c1 < n; ++c1) {
-              int r1 = (gd.x - c1) % a.K1; if (r1 < 0) r1 += a.K1;
-              part += (fac2 * w[c1]) * phi[(row + r1) * chunk + b];
-            }
+#pragma unroll
+            for (int c1 = 0; c1 < (NO > 0 ? NO : kMaxOrder); ++c1)
+              if (c1 < n) part += (fac2 * w1[c1]) * rowp[(size_t)r1[c1] * chunk];
             e += (double)part;
           }
         }
       }
       e -= a.pivol * qslt * (double)molq[k];
     }
-    if (!active || k == excl) continue;
-    if (ba.keep_uvengy) uvengy[(size_t)cnt * a.slvmax + k] = e;
+    if (active) Etot[(size_t)bi * a.slvmax + k] = (k == excl) ? 0.0 : e;
+  }
+}
+
+void launch_gather(const FrameArgs& a, const DeviceState& d, int base, int bb, int nb, int chunk, int batch,
+                   cudaStream_t s) {
+  int blocks = (a.slvmax * 32 + kGatherThreads - 1) / kGatherThreads;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  if (blocks < 1) blocks = 1;
+#define ERM_GATHER(NO) k_gather<NO><<<blocks, kGatherThreads, 0, s>>>(a, base, bb, nb, chunk, batch, d.molsorted, \
+      d.molbeg, d.molq, d.atom_q, d.spl, d.grd, d.phi, d.E, d.tgtq, d.tgt_mol, d.Etot)
+  if (a.pme && a.order == 4) ERM_GATHER(4);
+  else if (a.pme && a.order == 6) ERM_GATHER(6);
+  else ERM_GATHER(0);
+#undef ERM_GATHER
+}
+
+// ---------------------------------------------------------------------------
+// binning: a CTA per target, the molecule energies of its row binned into a
+// shared-memory histogram (getiduv, engproc.F90:1111-1171; insdst,
+// :917-937), written out as that target's count row.
+// ---------------------------------------------------------------------------
+constexpr int kBinThreads = 256;
+constexpr int kMaxSpecSmem = 128;
+
+__global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slvmax, const double* __restrict__ Etot,
+    const int* __restrict__ molspec, const int* __restrict__ spec_off, const double* __restrict__ uvcrd,
+    const int* __restrict__ uvsoft, const int* __restrict__ tgt_mol, uint32_t* __restrict__ counts,
+    double* __restrict__ etot, double* __restrict__ flceng, float* __restrict__ minuv, float* __restrict__ maxuv,
+    DevStatus* st) {
+  extern __shared__ unsigned char smem_raw[];
+  double* mesh = (double*)smem_raw;                                  // [ermax]
+  uint32_t* hist = (uint32_t*)(mesh + ba.ermax);                     // [ermax_pad]
+  __shared__ float smin[kMaxSpecSmem], smax[kMaxSpecSmem];
+  __shared__ double sfl[kMaxSpecSmem];
+  __shared__ double red[32];
+  const int bi = blockIdx.x, cnt = bb + bi;
+  for (int i = threadIdx.x; i < ba.ermax; i += blockDim.x) mesh[i] = uvcrd[i];
+  for (int i = threadIdx.x; i < ba.ermax_pad; i += blockDim.x) hist[i] = 0u;
+  for (int i = threadIdx.x; i < kMaxSpecSmem; i += blockDim.x) { smin[i] = FLT_MAX; smax[i] = -FLT_MAX; sfl[i] = 0.0; }
+  __syncthreads();
+  const int excl = tgt_mol ? tgt_mol[cnt] : -1;
+  const double* row = Etot + (size_t)bi * slvmax;
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < slvmax; k += blockDim.x) {
+    if (k == excl) continue;
+    const double e = row[k];
     const int pti = molspec[k];
     if (pti <= 0) { report(st, kErrEngCns, k, cnt, (float)e); continue; }
     const int lo = spec_off[pti - 1], num = spec_off[pti] - lo;
-    const double* c = uvcrd + lo;
+    const double* c = mesh + lo;
     int idp;
     if (e < c[0]) idp = 0;
     else if (e > c[num - 1]) idp = num;
@@ -609,36 +807,49 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather_bin(FrameArgs a, BinA
     if (idp <= 0) { report(st, kErrEngMin, k, cnt, (float)e); continue; }
     if (ba.slttype == ERMOD_SLT_SOLN && idp > uvsoft[pti - 1]) { report(st, kErrEngSft, k, cnt, (float)e); continue; }
     if (idp == num && e < 1.0e3) report(st, kWarnMbin, k, cnt, (float)e);
-    atomicAdd(&counts[(size_t)(cnt - ba.count_base) * ba.ermax_pad + lo + idp - 1], 1u);
-    my_etot += e;
-    if (ba.slttype == ERMOD_SLT_SOLN) atomicAdd(&flceng[(size_t)cnt * ba.numslv + pti - 1], e);
+    atomicAdd(&hist[lo + idp - 1], 1u);
+    acc += e;
     const float ef = (float)e;
     if (pti < kMaxSpecSmem) {
       atomic_min_f(&smin[pti], ef);
       atomic_max_f(&smax[pti], ef);
+      if (ba.slttype == ERMOD_SLT_SOLN) atomicAdd(&sfl[pti], e);
     } else {
       atomic_min_f(&minuv[pti], ef);
       atomic_max_f(&maxuv[pti], ef);
+      if (ba.slttype == ERMOD_SLT_SOLN) atomicAdd(&flceng[(size_t)cnt * ba.numslv + pti - 1], e);
     }
   }
-  if (active && my_etot != 0.0) atomicAdd(&etot[cnt], my_etot);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
-  for (int i = threadIdx.x; i < kMaxSpecSmem && i <= ba.numslv; i += blockDim.x) {
-    if (i == 0) continue;
+  uint32_t* crow = counts + (size_t)bi * ba.ermax_pad;
+  for (int i = threadIdx.x; i < ba.ermax_pad; i += blockDim.x) crow[i] = hist[i];
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) etot[cnt] = v;
+  }
+  for (int i = threadIdx.x + 1; i < kMaxSpecSmem && i <= ba.numslv; i += blockDim.x) {
     if (smin[i] != FLT_MAX) atomic_min_f(&minuv[i], smin[i]);
     if (smax[i] != -FLT_MAX) atomic_max_f(&maxuv[i], smax[i]);
+    if (ba.slttype == ERMOD_SLT_SOLN) flceng[(size_t)cnt * ba.numslv + i - 1] = sfl[i];
   }
 }
 
-void launch_gather_bin(const FrameArgs& a, const DeviceState& d, const BinArgs& ba, int base, int nb, int chunk,
-                       cudaStream_t s) {
-  int blocks = (a.slvmax * 32 + kGatherThreads - 1) / kGatherThreads;
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  if (blocks < 1) blocks = 1;
-  k_gather_bin<<<blocks, kGatherThreads, 0, s>>>(a, ba, base, nb, chunk, d.molsorted, d.molbeg, d.molspec, d.molq,
-                                                 d.atom_q, d.spl, d.grd, d.phi, d.E, d.tgt_mol, d.tgt_n, d.uvcrd,
-                                                 d.spec_off, d.uvsoft, d.uvengy, d.counts, d.etot, d.flceng, d.minuv,
-                                                 d.maxuv, d.status);
+size_t bin_smem_bytes(const BinArgs& ba) { return sizeof(double) * ba.ermax + sizeof(uint32_t) * ba.ermax_pad; }
+
+void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int slvmax, cudaStream_t s) {
+  if (nbatch <= 0) return;
+  k_bin<<<nbatch, kBinThreads, bin_smem_bytes(ba), s>>>(ba, bb, slvmax, d.Etot, d.molspec, d.spec_off, d.uvcrd,
+                                                        d.uvsoft, d.tgt_mol, d.counts, d.etot, d.flceng, d.minuv,
+                                                        d.maxuv, d.status);
+}
+
+int setup_bin_smem(const BinArgs& ba) {
+  const size_t b = bin_smem_bytes(ba);
+  if (b > 200 * 1024) return -1;
+  return cudaFuncSetAttribute(k_bin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b) == cudaSuccess ? 0 : -1;
 }
 
 // ---------------------------------------------------------------------------
@@ -655,17 +866,16 @@ __global__ void k_offset_init(WeightArgs wa, int base, const double* __restrict_
   }
 }
 
+// per-target weight engnmfc (engproc.F90:883-903, volcorrect :1022-1038)
 __global__ void k_weights(WeightArgs wa, int base, int n, const double* __restrict__ selfrec,
                           const double* __restrict__ selfreal, const float* __restrict__ insw,
-                          const double* __restrict__ escrd, const double* __restrict__ flceng,
-                          double* __restrict__ u0, double* __restrict__ w, double* __restrict__ scal,
-                          double* __restrict__ eself, double* __restrict__ slnuv, float* __restrict__ minuv,
-                          float* __restrict__ maxuv, DevStatus* st) {
+                          const double* __restrict__ escrd, double* __restrict__ u0, double* __restrict__ w,
+                          double* __restrict__ twt, int* __restrict__ sbin, const double* __restrict__ scal,
+                          DevStatus* st) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double wn = 0.0, tw = 0.0, cntv = 0.0;
-  float mn = FLT_MAX, mx = -FLT_MAX;
   if (i < n) {
     const int cnt = base + i;
+    double tw;
     const double sr = wa.rigid ? scal[5] : selfreal[cnt];
     const double uu = selfrec[cnt] + sr + wa.resid_self;
     u0[cnt] = uu;
@@ -677,54 +887,82 @@ __global__ void k_weights(WeightArgs wa, int base, int n, const double* __restri
     tw = (double)wa.stat_weight_system * (double)insw[cnt] * wa.npt_factor;
     e *= tw;
     w[cnt] = e;
-    wn = e;
-    cntv = 1.0;
-    if (wa.selfcal) {
-      int l = 0, h = wa.esmax;
-      if (uu < escrd[0]) l = 0;
-      else if (uu > escrd[wa.esmax - 1]) l = wa.esmax;
-      else { while (l < h) { const int mid = (l + h) >> 1; if (escrd[mid] < uu) l = mid + 1; else h = mid; } }
-      if (l <= 0) report(st, kErrEngMin, -1, cnt, (float)uu);
+    twt[cnt] = tw;
+    int l = -1;
+    if (wa.selfcal) {  // getiduv(0, uvengy0) (engproc.F90:910-913)
+      int lo = 0, h = wa.esmax;
+      if (uu < escrd[0]) lo = 0;
+      else if (uu > escrd[wa.esmax - 1]) lo = wa.esmax;
+      else { while (lo < h) { const int mid = (lo + h) >> 1; if (escrd[mid] < uu) lo = mid + 1; else h = mid; } }
+      if (lo <= 0) report(st, kErrEngMin, -1, cnt, (float)uu);
       else {
-        if (l == wa.esmax && uu < 1.0e3) report(st, kWarnMbin, -1, cnt, (float)uu);
-        atomicAdd(&eself[l - 1], e);
+        if (lo == wa.esmax && uu < 1.0e3) report(st, kWarnMbin, -1, cnt, (float)uu);
+        l = lo - 1;
       }
     }
-    if (wa.slttype == ERMOD_SLT_SOLN)
-      for (int q = 0; q < wa.numslv; ++q) atomicAdd(&slnuv[q], flceng[(size_t)cnt * wa.numslv + q] * e);
-    mn = mx = (float)uu;
+    sbin[cnt] = l;
   }
-  __shared__ double r0[32], r1[32], r2[32];
+}
+
+// Scalar accumulators of one batch, summed in a fixed order by one CTA
+// (engproc.F90:905-915, 939-941): engnorm, engsmpl, avslf, the self-energy
+// histogram, slnuv (soln) and the self-energy min / max.
+constexpr int kSumThreads = 1024;
+
+__global__ void __launch_bounds__(kSumThreads) k_wsum(WeightArgs wa, int base, int n, const double* __restrict__ w,
+    const double* __restrict__ twt, const double* __restrict__ u0, const int* __restrict__ sbin,
+    const double* __restrict__ flceng, double* __restrict__ scal, double* __restrict__ eself,
+    double* __restrict__ slnuv, float* __restrict__ minuv, float* __restrict__ maxuv) {
+  __shared__ double r0[32], r1[32];
   __shared__ float rm[32], rx[32];
-  wn = warp_sum(wn); tw = warp_sum(tw); cntv = warp_sum(cntv);
-  mn = warp_min(mn); mx = warp_max(mx);
-  if ((threadIdx.x & 31) == 0) {
-    r0[threadIdx.x >> 5] = wn; r1[threadIdx.x >> 5] = tw; r2[threadIdx.x >> 5] = cntv;
-    rm[threadIdx.x >> 5] = mn; rx[threadIdx.x >> 5] = mx;
+  double a0 = 0.0, a1 = 0.0;
+  float mn = FLT_MAX, mx = -FLT_MAX;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    a0 += w[base + i];
+    a1 += twt[base + i];
+    const float u = (float)u0[base + i];
+    mn = fminf(mn, u);
+    mx = fmaxf(mx, u);
   }
+  a0 = warp_sum(a0); a1 = warp_sum(a1); mn = warp_min(mn); mx = warp_max(mx);
+  if ((threadIdx.x & 31) == 0) { r0[threadIdx.x >> 5] = a0; r1[threadIdx.x >> 5] = a1; rm[threadIdx.x >> 5] = mn; rx[threadIdx.x >> 5] = mx; }
   __syncthreads();
   if (threadIdx.x < 32) {
     const bool ok = threadIdx.x < (blockDim.x >> 5);
-    wn = warp_sum(ok ? r0[threadIdx.x] : 0.0);
-    tw = warp_sum(ok ? r1[threadIdx.x] : 0.0);
-    cntv = warp_sum(ok ? r2[threadIdx.x] : 0.0);
+    a0 = warp_sum(ok ? r0[threadIdx.x] : 0.0);
+    a1 = warp_sum(ok ? r1[threadIdx.x] : 0.0);
     mn = warp_min(ok ? rm[threadIdx.x] : FLT_MAX);
     mx = warp_max(ok ? rx[threadIdx.x] : -FLT_MAX);
-    if (threadIdx.x == 0 && cntv > 0.0) {
-      atomicAdd(&scal[1], wn);
-      atomicAdd(&scal[2], cntv);
-      atomicAdd(&scal[0], tw);
-      atomic_min_f(&minuv[0], mn);
-      atomic_max_f(&maxuv[0], mx);
+    if (threadIdx.x == 0) {
+      scal[1] += a0;
+      scal[2] += (double)n;
+      scal[0] += a1;
+      minuv[0] = fminf(minuv[0], mn);
+      maxuv[0] = fmaxf(maxuv[0], mx);
+      if (wa.slttype == ERMOD_SLT_SOLN)
+        for (int q = 0; q < wa.numslv; ++q) {
+          double sq = 0.0;
+          for (int i = 0; i < n; ++i) sq += flceng[(size_t)(base + i) * wa.numslv + q] * w[base + i];
+          slnuv[q] += sq;
+        }
     }
   }
+  if (wa.selfcal)
+    for (int bin = threadIdx.x; bin < wa.esmax; bin += blockDim.x) {
+      double sb = 0.0;
+      for (int i = 0; i < n; ++i)
+        if (sbin[base + i] == bin) sb += w[base + i];
+      eself[bin] += sb;
+    }
 }
 
 void launch_weights(const DeviceState& d, const WeightArgs& wa, int base, int n, cudaStream_t s) {
   if (n <= 0) return;
   k_offset_init<<<1, 32, 0, s>>>(wa, base, d.selfrec, d.selfreal, d.scal);
-  k_weights<<<(n + 255) / 256, 256, 0, s>>>(wa, base, n, d.selfrec, d.selfreal, d.insw_in, d.escrd, d.flceng,
-                                             d.u0, d.w, d.scal, d.eself, d.slnuv, d.minuv, d.maxuv, d.status);
+  k_weights<<<(n + 255) / 256, 256, 0, s>>>(wa, base, n, d.selfrec, d.selfreal, d.insw_in, d.escrd, d.u0, d.w,
+                                             d.twt, d.sbin, d.scal, d.status);
+  k_wsum<<<1, kSumThreads, 0, s>>>(wa, base, n, d.w, d.twt, d.u0, d.sbin, d.flceng, d.scal, d.eself, d.slnuv,
+                                   d.minuv, d.maxuv);
 }
 
 __global__ void k_edens(int base, int n, int ermax, int ermax_pad, int count_base, const double* __restrict__ w,

@@ -154,13 +154,13 @@ class Engine:
         self._check(self.lib.ermod_get_insertions(self.ctx, A.ptr(o, C.c_float), A.ptr(w, C.c_double)))
         return o, w
 
-    STAGES = ["total", "prepare", "insert", "real", "spread", "r2c", "influence", "c2r", "gather_bin",
-              "weights_edens", "ecorr", "chunks"]
+    STAGES = ["total", "prepare", "insert", "real", "spread", "r2c", "influence", "c2r", "gather", "bin",
+              "weights_edens", "ecorr", "chunks", "transpose"]
 
     def timings(self):
         """Device milliseconds per stage of the last engconst (CUDA events on the engine stream)."""
-        t = np.zeros(12, dtype=np.float32)
-        self.lib.ermod_get_timings(self.ctx, A.ptr(t, C.c_float), 12)
+        t = np.zeros(len(self.STAGES), dtype=np.float32)
+        self.lib.ermod_get_timings(self.ctx, A.ptr(t, C.c_float), len(self.STAGES))
         return dict(zip(self.STAGES, t.tolist()))
 
     def launch_count(self) -> int:

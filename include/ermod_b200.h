@@ -255,8 +255,9 @@ const char* ermod_last_error(const ermod_ctx* ctx);
  * events on the engine's stream (no reference counterpart; profiling):
  * [0] total, [1] prepare + cell list, [2] insertion, [3] real space,
  * [4] PME spread, [5] FFT R2C, [6] influence multiply, [7] FFT C2R,
- * [8] gather + bin, [9] weights + edens, [10] ecorr, [11] number of
- * target chunks.  n <= 12. */
+ * [8] PME gather, [9] binning, [10] weights + edens, [11] ecorr,
+ * [12] number of PME target chunks, [13] potential-grid transpose.
+ * n <= 14. */
 int32_t ermod_get_timings(const ermod_ctx* ctx, float* ms, int32_t n);
 
 /* Kernel launches of this library since the context was created, cuFFT's

