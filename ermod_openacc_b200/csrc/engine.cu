@@ -109,7 +109,7 @@ void free_all(ermod_ctx* c) {
                   d.slt_mass, d.bfcoord, d.uvcrd, d.spec_off, d.uvsoft, d.escrd, d.posraw, d.slvn, d.spl, d.grd,
                   d.anchor, d.cellof, d.cellcount, d.cellstart, d.molsorted, d.rmol, d.ins_conf, d.insw_in,
                   d.tgt_raw, d.tgt_n, d.tgt_c, d.tgt_mol, d.selfreal, d.selfrec, d.u0, d.w, d.etot, d.flceng,
-                  d.grid, d.spec, d.phi, d.engfac, d.splfc, d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
+                  d.grid, d.spec, d.phin, d.phi, d.engfac, d.splfc, d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
                   d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.ecorr, d.eself,
                   d.slnuv, d.minuv, d.maxuv, d.scal, d.status, c->tc_work};
   for (void* p : ptrs)
@@ -378,6 +378,8 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   const size_t KK = (size_t)K1 * K2 * K3, KH = (size_t)K3 * K2 * Kh1;
   if (pme) {
     CK(dalloc(&d.grid, (size_t)ctx->chunk * KK)); CK(dalloc(&d.spec, (size_t)ctx->chunk * KH));
+    CK(cudaMemsetAsync(d.grid, 0, sizeof(float) * ctx->chunk * KK, ctx->st));  // kept zero outside the boxes
+    CK(dalloc(&d.phin, (size_t)ctx->chunk * KK));
     CK(dalloc(&d.phi, (size_t)ctx->chunk * KK)); CK(dalloc(&d.engfac, KH)); CK(dalloc(&d.splfc, K1 + K2 + K3));
   }
   CK(dalloc(&d.E, SM * ctx->batch));
@@ -691,13 +693,14 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
         mark(ctx, kStSpread);
         CF(cufftExecR2C(ctx->r2c, d.grid, (cufftComplex*)d.spec));
         mark(ctx, kStR2C);
+        launch_clear_box(a, d, chunk, st);
         launch_influence(a, d, cb, nb, chunk, st);
         mark(ctx, kStInfl);
-        CF(cufftExecC2R(ctx->c2r, (cufftComplex*)d.spec, d.grid));  // natural layout, reuses the charge grid
+        CF(cufftExecC2R(ctx->c2r, (cufftComplex*)d.spec, d.phin));
         mark(ctx, kStC2R);
         launch_transpose_phi(a, d, st);
         mark(ctx, kStTranspose);
-        nl += 4;
+        nl += 5;
       }
       launch_gather(a, d, cb, bb, nb, chunk, ctx->batch, st);
       mark(ctx, kStGather);

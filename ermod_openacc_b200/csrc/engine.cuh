@@ -80,6 +80,7 @@ struct DeviceState {
   // PME chunk buffers
   float* grid = nullptr;     // [chunk*K^3]
   float2* spec = nullptr;    // [chunk*K3*K2*Kh1]
+  float* phin = nullptr;     // [chunk*K^3] potential grids as the C2R writes them
   float* phi = nullptr;      // [K^3*chunk], insertion fastest
   float* engfac = nullptr;   // [K3*K2*Kh1]
   double* splfc = nullptr;   // [K1+K2+K3]
@@ -119,6 +120,7 @@ void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[
 void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
 int setup_spread_smem();
 void launch_transpose_phi(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
+void launch_clear_box(const FrameArgs& a, const DeviceState& d, int chunk, cudaStream_t s);
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
 
 struct BinArgs {

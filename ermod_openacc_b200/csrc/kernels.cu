@@ -507,9 +507,8 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_box(FrameArgs a, int 
   extern __shared__ long long sacc[];
   __shared__ int g0[3], lo[3], hi[3];
   const int b = blockIdx.x;
-  const int K[3] = {a.K1, a.K2, a.K3};
   const size_t KK = (size_t)a.K1 * a.K2 * a.K3;
-  if (b >= nb) {  // empty slot of a partial chunk: k_zero_outside clears the whole grid
+  if (b >= nb) {  // empty slot of a partial chunk: its grid stays all zero
     if (threadIdx.x == 0) { boxinfo[2 * b] = make_int4(0, 0, 0, 0); boxinfo[2 * b + 1] = make_int4(0, 0, 0, 0); }
     return;
   }
@@ -537,17 +536,13 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_box(FrameArgs a, int 
     }
   }
   __syncthreads();
-  const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
-  if (n0 > a.K1 || n1 > a.K2 || n2 > a.K3) {  // solute wider than the periodic grid
-    if (threadIdx.x == 0) {
-      report(st, kErrGrid, -1, base + b, (float)max(n0, max(n1, n2)));
-      boxinfo[2 * b] = make_int4(0, 0, 0, 0);
-      boxinfo[2 * b + 1] = make_int4(0, 0, 0, 0);
-    }
-    return;
-  }
+  int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+  // a solute whose stencils span more than the grid wraps onto itself: spread
+  // over the whole grid with wrapped indices (the reference's modulo)
+  const bool full = n0 > a.K1 || n1 > a.K2 || n2 > a.K3;
+  if (full) { n0 = a.K1; n1 = a.K2; n2 = a.K3; }
   const int vol = n0 * n1 * n2;
-  long long* acc = vol <= cap ? sacc : gacc + (size_t)b * KK;
+  long long* acc = (!full && vol <= cap) ? sacc : gacc + (size_t)b * KK;
   for (int i = threadIdx.x; i < vol; i += blockDim.x) acc[i] = 0;
   __syncthreads();
   // a warp per site, lanes over the stencil points
@@ -559,18 +554,20 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_box(FrameArgs a, int 
     int gi[3];
     site_spline(a, r, w, gi);
     int d[3];
-    for (int m = 0; m < 3; ++m) d[m] = lifted_index(a, r, m, gi[m]) - g0[m] - lo[m];
+    for (int m = 0; m < 3; ++m) d[m] = full ? gi[m] : lifted_index(a, r, m, gi[m]) - g0[m] - lo[m];
     for (int p = lane; p < n3; p += 32) {
       const int c1 = p % n, c2 = (p / n) % n, c3 = p / (n * n);
       const float v = r.w * w[0][c1] * w[1][c2] * w[2][c3];   // recpcal.F90:464-465
-      const int idx = ((d[2] - c3) * n1 + (d[1] - c2)) * n0 + (d[0] - c1);
+      const int idx = full ? (wrapk(d[2] - c3, a.K3) * n1 + wrapk(d[1] - c2, a.K2)) * n0 + wrapk(d[0] - c1, a.K1)
+                           : ((d[2] - c3) * n1 + (d[1] - c2)) * n0 + (d[0] - c1);
       atomicAdd((unsigned long long*)&acc[idx], (unsigned long long)llrint((double)v * kFixScale));
     }
   }
   __syncthreads();
   float* gb = grid + (size_t)b * KK;
   auto posmod = [](int x, int K) { const int r = x % K; return r < 0 ? r + K : r; };
-  const int o0 = posmod(g0[0] + lo[0], a.K1), o1 = posmod(g0[1] + lo[1], a.K2), o2 = posmod(g0[2] + lo[2], a.K3);
+  const int o0 = full ? 0 : posmod(g0[0] + lo[0], a.K1), o1 = full ? 0 : posmod(g0[1] + lo[1], a.K2),
+            o2 = full ? 0 : posmod(g0[2] + lo[2], a.K3);
   for (int i = threadIdx.x; i < vol; i += blockDim.x) {
     const int x = i % n0, y = (i / n0) % n1, z = i / (n0 * n1);
     const int r1 = wrapk(o0 + x, a.K1), r2 = wrapk(o1 + y, a.K2), r3 = wrapk(o2 + z, a.K3);
@@ -582,31 +579,29 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_box(FrameArgs a, int 
   }
 }
 
-// zero every grid point outside its target's box (run after k_spread_box).
-// block = (K1 threads along x) x (kRowsPerBlock rows), grid = (K2*K3/kRowsPerBlock, chunk)
-constexpr int kRowsPerBlock = 4;
-
-__global__ void k_zero_outside(FrameArgs a, const int4* __restrict__ boxinfo, float* __restrict__ grid) {
-  const int b = blockIdx.y;
-  const int r1 = threadIdx.x;
-  const int row = blockIdx.x * kRowsPerBlock + threadIdx.y;
-  if (row >= a.K2 * a.K3 || r1 >= a.K1) return;
-  const int r2 = row % a.K2, r3 = row / a.K2;
+// After the forward FFT has read the charge grids, put zeros back where the
+// boxes were written, so the grids are all zero again for the next chunk
+// (the grids are zeroed once at context creation).
+__global__ void k_clear_box(FrameArgs a, const int4* __restrict__ boxinfo, float* __restrict__ grid) {
+  const int b = blockIdx.x;
   const int4 o = boxinfo[2 * b], ne = boxinfo[2 * b + 1];
-  bool inside = false;
-  if (o.w) {
-    const int x = wrapk(r1 - o.x, a.K1), y = wrapk(r2 - o.y, a.K2), z = wrapk(r3 - o.z, a.K3);
-    inside = x < ne.x && y < ne.y && z < ne.z;
+  if (!o.w) return;
+  float* gb = grid + (size_t)b * a.K1 * a.K2 * a.K3;
+  const int vol = ne.x * ne.y * ne.z;
+  for (int i = threadIdx.x; i < vol; i += blockDim.x) {
+    const int x = i % ne.x, y = (i / ne.x) % ne.y, z = i / (ne.x * ne.y);
+    const int r1 = wrapk(o.x + x, a.K1), r2 = wrapk(o.y + y, a.K2), r3 = wrapk(o.z + z, a.K3);
+    gb[((size_t)r3 * a.K2 + r2) * a.K1 + r1] = 0.0f;
   }
-  if (!inside) grid[((size_t)b * a.K3 * a.K2 + row) * a.K1 + r1] = 0.0f;
 }
 
 void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
   k_spread_box<<<chunk, kSpreadThreads, kSpreadSmemBytes, s>>>(a, base, nb, kSpreadSmemBytes / 8, d.tgt_raw, d.grid,
                                                                d.gacc, d.boxinfo, d.status);
-  dim3 blk(a.K1, kRowsPerBlock);
-  dim3 grd((a.K2 * a.K3 + kRowsPerBlock - 1) / kRowsPerBlock, chunk);
-  k_zero_outside<<<grd, blk, 0, s>>>(a, d.boxinfo, d.grid);
+}
+
+void launch_clear_box(const FrameArgs& a, const DeviceState& d, int chunk, cudaStream_t s) {
+  k_clear_box<<<chunk, 256, 0, s>>>(a, d.boxinfo, d.grid);
 }
 
 int setup_spread_smem() {
@@ -679,7 +674,7 @@ __global__ void k_transpose_phi(int KK, const float* __restrict__ in, float* __r
 
 void launch_transpose_phi(const FrameArgs& a, const DeviceState& d, cudaStream_t s) {
   const int KK = a.K1 * a.K2 * a.K3;
-  k_transpose_phi<<<(KK + 31) / 32, dim3(32, 8), 0, s>>>(KK, d.grid, d.phi);
+  k_transpose_phi<<<(KK + 31) / 32, dim3(32, 8), 0, s>>>(KK, d.phin, d.phi);
 }
 
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
