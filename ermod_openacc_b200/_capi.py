@@ -124,7 +124,11 @@ SIGNATURES = {
     "ermod_get_timings": (C.c_int32, [C.c_void_p, _f32p, C.c_int32]),
     "ermod_get_launch_count": (C.c_int64, [C.c_void_p]),
     "ermod_destroy": (None, [C.c_void_p]),
+    "ermod_histogram_noalloc": (C.c_int32, [C.c_int32, C.c_int32, _f64p, C.c_int32, C.c_int32, _i32p, _f64p,
+                                            _i32p, _i32p, C.c_int32, _f64p, _f64p]),
 }
+
+NOALLOC_SCRATCH_BYTES = 32 << 20
 
 _LIB = None
 

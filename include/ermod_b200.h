@@ -266,6 +266,35 @@ int64_t ermod_get_launch_count(const ermod_ctx* ctx);
 
 void ermod_destroy(ermod_ctx* ctx);
 
+/*
+ * Energy histogram without device allocation.  No counterpart in the
+ * reference: it serves hosts that may not allocate GPU memory themselves,
+ * e.g. a Fortran erdst whose device memory belongs to its OpenACC runtime,
+ * or an MPI rank held to a fixed GPU memory budget by its scheduler.
+ *
+ * Bins the per-molecule energies uvengy (host, [ntarget*nmol], molecule
+ * fastest, as returned by ermod_get_uvengy) with getiduv's rule and returns
+ * edens(i) = sum over targets of weight(target) * count(target, i) (host,
+ * [ermax] with ermax = sum(uvmax)).  uvspec [nmol] gives each molecule's
+ * solvent species (0 = skipped with eng_cns as in the engine), uvcrd /
+ * uvmax / uvsoft the mesh (uvsoft may be NULL; it is used only when
+ * slttype == ERMOD_SLT_SOLN).  Status codes as ermod_engconst.
+ *
+ * All device memory it uses is one array of ERMOD_NOALLOC_SCRATCH_BYTES
+ * compiled into the library, which every GPU that loads the library holds
+ * until the process exits; requests that do not fit return
+ * ERMOD_ERR_OVERFLOW.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress) and caches it; make that first
+ * call before any stream capture.  Calls run on the legacy default stream
+ * and share the one array: calls that overlap on the GPU (other host
+ * threads, other streams) race and must be serialised by the caller.
+ */
+#define ERMOD_NOALLOC_SCRATCH_BYTES (32u << 20)
+int32_t ermod_histogram_noalloc(int32_t device, int32_t slttype, const double* uvengy, int32_t ntarget,
+                                int32_t nmol, const int32_t* uvspec, const double* uvcrd,
+                                const int32_t* uvmax, const int32_t* uvsoft, int32_t numslv,
+                                const double* weight, double* edens);
+
 #ifdef __cplusplus
 }
 #endif
