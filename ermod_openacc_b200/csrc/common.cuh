@@ -178,6 +178,7 @@ enum : int {
   kWarnMbin = 8,      // mbin warning
   kErrOverflow = 16,  // internal capacity exceeded
   kErrGrid = 32,      // a PME grid index outside the grid
+  kErrTimeout = 64,   // a bounded wait on an mbarrier expired
 };
 
 struct DevStatus {

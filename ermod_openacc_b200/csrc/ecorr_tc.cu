@@ -1,7 +1,382 @@
-// ecorr_tc.cu -- placeholder until the tcgen05 INT8 path lands.
+// ecorr_tc.cu -- ecorr accumulation as exact INT8 tensor-core GEMMs (tcgen05, sm_100a).
+//
+// The reference adds, per insertion, engnmfc * k_i * k_j to ecorr(j, i) over
+// every pair of non-empty bins of that insertion's count vector
+// (erdst/engproc.F90:948-962).  Over a batch of insertions that is
+//     ecorr += C^T diag(w) C,        C[cnt][bin] = counts, w = engnmfc.
+// Counts are small integers, so C^T X C with integer X is exact on the INT8
+// tensor cores (u8 x u8 -> s32).  The FP64 weights are made integer by
+//     w_cnt = w_min + m_cnt * q,   m_cnt in [0, 2^P - 1],  q = (w_max - w_min) / (2^P - 1)
+// with P chosen per batch so that |w - (w_min + m q)| <= 2^-25 w_min, and
+//     C^T diag(w) C = w_min C^T C + q sum_d 2^d C^T diag(bit_d(m)) C :
+// one plain GEMM plus P GEMMs whose A operand has the insertions without
+// bit d masked out.  Counts above 255 are split into two base-256 limbs
+// (c = 256 h + l), adding the h-l, l-h and h-h products.  Every GEMM is
+// exact in INT32 (at most 4096 * 255^2 per entry); the FP64 combination
+// runs in a fixed order, so the result is deterministic.
+//
+// Kernel structure: a CTA per 128 x 64 tile of ecorr.  Per K tile of 128
+// insertions the CTA stages B (64 bin rows x 128 bytes) and up to eight
+// masked copies of A (128 bin rows x 128 bytes) in shared memory in the
+// 128-byte-swizzled K-major layout, one thread issues the tcgen05.mma
+// instructions (M=128, N=64, K=32 each) into up to eight TMEM accumulators
+// (8 x 64 columns), and a tcgen05.commit signals an mbarrier.  The epilogue
+// reads the accumulators with tcgen05.ld and adds scale * value into ecorr.
+// Every wait on the mbarrier has an iteration limit; on expiry the kernel
+// records an error, frees its TMEM and returns.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
 #include "engine.cuh"
+
 namespace erm {
-int ecorr_tc_available() { return 0; }
-size_t ecorr_tc_workspace(int, int) { return 0; }
-int launch_ecorr_tc(const DeviceState&, int, int, int, int, int, int, void*, size_t, cudaStream_t) { return -1; }
+
+namespace {
+
+constexpr int kTileM = 128;          // bins of the A side (TMEM lanes)
+constexpr int kTileN = 64;           // bins of the B side (TMEM columns per accumulator)
+constexpr int kTileK = 128;          // insertions per K tile (one 128-byte swizzle row)
+constexpr int kMaxGroup = 8;         // accumulators per pass: 8 x 64 = 512 TMEM columns
+constexpr int kThreads = 256;
+constexpr int kMaxDigits = 30;
+constexpr long long kSpinLimit = 1LL << 26;
+
+struct QuantParams {
+  int P;              // weight digits
+  int has_high;       // some count > 255 in the batch
+  int kpad;           // insertions rounded up to kTileK
+  int pad;
+  double wmin, q;     // w = wmin + m * q
+};
+
+// ---- PTX helpers --------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// K-major, 128-byte swizzle, 8-row groups 1024 bytes apart (CUTLASS UMMA::SmemDescriptor layout)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
+  d |= (uint64_t)1 << 16;                          // leading byte offset (16 B units), unused for SW128 K-major
+  d |= (uint64_t)(1024 >> 4) << 32;                // stride byte offset: 8-row groups
+  d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                          // SWIZZLE_128B
+  return d;
+}
+
+// instruction descriptor: kind::i8, D = s32, A = B = u8, both K-major, M = 128, N = 64
+__host__ __device__ constexpr uint32_t idesc_i8() {
+  return (2u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(kTileN >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  const uint32_t idesc = idesc_i8();
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// byte offset of (row, 16-byte chunk) in a 128-byte-swizzled K-major tile
+__device__ __forceinline__ uint32_t swz(int row, int chunk) {
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4));
+}
+
+// 4 mask bits -> 4 bytes of 0x00 / 0xFF
+__device__ __forceinline__ uint32_t expand4(uint32_t b) {
+  return ((b & 1u) ? 0x000000FFu : 0u) | ((b & 2u) ? 0x0000FF00u : 0u) | ((b & 4u) ? 0x00FF0000u : 0u) |
+         ((b & 8u) ? 0xFF000000u : 0u);
+}
+
+// ---- preparation --------------------------------------------------------
+// counts[cnt][bin] (u32, batch rows) -> CT_l / CT_h [bin][kpad] (u8, insertions contiguous)
+__global__ void k_counts_to_ct(int n, int kpad, int ermax_pad, const uint32_t* __restrict__ counts,
+                               uint8_t* __restrict__ ctl, uint8_t* __restrict__ cth, int* __restrict__ high) {
+  __shared__ uint32_t tile[32][33];
+  const int b0 = blockIdx.x * 32, c0 = blockIdx.y * 32;  // bins, insertions
+  const int tx = threadIdx.x, ty = threadIdx.y;          // (32, 8)
+  for (int j = 0; j < 32; j += 8) {
+    const int cnt = c0 + ty + j, bin = b0 + tx;
+    tile[ty + j][tx] = (cnt < n && bin < ermax_pad) ? counts[(size_t)cnt * ermax_pad + bin] : 0u;
+  }
+  __syncthreads();
+  int hi = 0;
+  for (int j = 0; j < 32; j += 8) {
+    const int bin = b0 + ty + j, cnt = c0 + tx;
+    if (bin < ermax_pad && cnt < kpad) {
+      const uint32_t v = tile[tx][ty + j];
+      ctl[(size_t)bin * kpad + cnt] = (uint8_t)(v & 255u);
+      cth[(size_t)bin * kpad + cnt] = (uint8_t)((v >> 8) & 255u);
+      hi |= v > 255u;
+    }
+  }
+  if (__syncthreads_or(hi) && tx == 0 && ty == 0) atomicOr(high, 1);
+}
+
+// weights -> (wmin, q, P, m_cnt), one CTA, fixed-order reductions
+__global__ void k_quantize(int base, int n, int kpad, int bits, const double* __restrict__ w,
+                           uint32_t* __restrict__ m, QuantParams* qp, const int* __restrict__ high) {
+  __shared__ double smin[32], smax[32];
+  double lo = 1e300, hi = -1e300;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    lo = fmin(lo, w[base + i]);
+    hi = fmax(hi, w[base + i]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) { smin[threadIdx.x >> 5] = lo; smax[threadIdx.x >> 5] = hi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) { lo = fmin(lo, smin[i]); hi = fmax(hi, smax[i]); }
+    lo = fmin(lo, smin[0]);
+    hi = fmax(hi, smax[0]);
+    const double span = hi - lo;
+    int P = 0;
+    if (span > 0.0) {
+      if (lo > 0.0) P = (int)ceil((double)bits + 1.0 + log2(span / lo));
+      else P = kMaxDigits;
+      P = P < 1 ? 1 : (P > kMaxDigits ? kMaxDigits : P);
+    }
+    qp->P = P;
+    qp->has_high = *high;
+    qp->kpad = kpad;
+    qp->wmin = lo;
+    qp->q = P > 0 ? span / (double)((1u << P) - 1u) : 0.0;
+    smin[0] = lo;
+    smax[0] = qp->q;
+  }
+  __syncthreads();
+  const double wmin = smin[0], q = smax[0];
+  for (int i = threadIdx.x; i < kpad; i += blockDim.x)
+    m[i] = (i < n && q > 0.0) ? (uint32_t)llrint((w[base + i] - wmin) / q) : 0u;
+}
+
+// ---- the GEMM ------------------------------------------------------------
+struct TcSmem {
+  uint8_t a[kMaxGroup][kTileM * kTileK];   // masked A copies (16 KB each, 1024-B aligned)
+  uint8_t b[kTileN * kTileK];              // B tile (8 KB)
+  uint16_t bits[kMaxDigits + 1][kTileK / 16];  // per digit, per 16-insertion chunk: mask bits
+  uint64_t bar;
+  uint32_t tmem_base;
+};
+
+__global__ void __launch_bounds__(kThreads, 1) k_ecorr_tc(int ermax, int kpad, const uint8_t* __restrict__ ctl,
+    const uint8_t* __restrict__ cth, const uint32_t* __restrict__ m, const QuantParams* __restrict__ qp,
+    double* __restrict__ ecorr, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte alignment of the swizzled tiles
+  TcSmem& S = *reinterpret_cast<TcSmem*>((void*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int i0 = blockIdx.y * kTileM, j0 = blockIdx.x * kTileN;
+  const QuantParams Q = *qp;
+  const int P = Q.P;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    mbar_init(&S.bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+  uint32_t phase = 0;
+  bool ok = true;
+
+  // terms: (limb pair, digit) with digit -1 = the plain w_min product
+  const int npairs = Q.has_high ? 4 : 1;
+  const int nterms_pair = 1 + P;
+  for (int pair = 0; pair < npairs && ok; ++pair) {
+    const uint8_t* A = (pair == 0 || pair == 1) ? ctl : cth;   // 0: l-l, 1: l-h, 2: h-l, 3: h-h
+    const uint8_t* B = (pair == 0 || pair == 2) ? ctl : cth;
+    const double limb = pair == 0 ? 1.0 : (pair == 3 ? 65536.0 : 256.0);
+    for (int t0 = 0; t0 < nterms_pair && ok; t0 += kMaxGroup) {
+      const int G = min(kMaxGroup, nterms_pair - t0);
+      for (int k0 = 0; k0 < kpad && ok; k0 += kTileK) {
+        // digit masks of this K tile: bit c of chunk (16 insertions) for digit d
+        for (int x = tid; x < (kMaxDigits + 1) * (kTileK / 16); x += blockDim.x) {
+          const int d = x / (kTileK / 16), c = x % (kTileK / 16);
+          uint32_t v = 0;
+          if (d <= P)
+            for (int e = 0; e < 16; ++e) {
+              const uint32_t mm = m[k0 + c * 16 + e];
+              const uint32_t bit = d == 0 ? 1u : ((mm >> (d - 1)) & 1u);   // d = 0: all insertions
+              v |= bit << e;
+            }
+          S.bits[d][c] = (uint16_t)v;
+        }
+        // B tile: 64 rows x 8 chunks
+        for (int x = tid; x < kTileN * (kTileK / 16); x += blockDim.x) {
+          const int r = x >> 3, c = x & 7;
+          uint4 v = make_uint4(0, 0, 0, 0);
+          if (j0 + r < ermax) v = *reinterpret_cast<const uint4*>(B + (size_t)(j0 + r) * kpad + k0 + c * 16);
+          *reinterpret_cast<uint4*>(S.b + swz(r, c)) = v;
+        }
+        __syncthreads();
+        // A tile: 128 rows x 8 chunks, one masked copy per term of the group
+        for (int x = tid; x < kTileM * (kTileK / 16); x += blockDim.x) {
+          const int r = x >> 3, c = x & 7;
+          uint4 v = make_uint4(0, 0, 0, 0);
+          if (i0 + r < ermax) v = *reinterpret_cast<const uint4*>(A + (size_t)(i0 + r) * kpad + k0 + c * 16);
+          for (int g = 0; g < G; ++g) {
+            const uint32_t bits = S.bits[t0 + g][c];
+            uint4 mv;
+            mv.x = v.x & expand4(bits & 15u);
+            mv.y = v.y & expand4((bits >> 4) & 15u);
+            mv.z = v.z & expand4((bits >> 8) & 15u);
+            mv.w = v.w & expand4((bits >> 12) & 15u);
+            *reinterpret_cast<uint4*>(S.a[g] + swz(r, c)) = mv;
+          }
+        }
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+          tc_fence_after();
+          const uint64_t db0 = smem_desc(smem_u32(S.b));
+          for (int g = 0; g < G; ++g) {
+            const uint64_t da0 = smem_desc(smem_u32(S.a[g]));
+#pragma unroll
+            for (int ks = 0; ks < kTileK / 32; ++ks)   // K = 32 bytes per MMA: advance 32 B = 2 x 16 B
+              mma_i8(tmem + (uint32_t)(g * kTileN), da0 + (uint64_t)(ks * 2), db0 + (uint64_t)(ks * 2),
+                     (k0 > 0 || ks > 0) ? 1u : 0u);
+          }
+          mma_commit(&S.bar);
+        }
+        __syncwarp();
+        bool done = mbar_wait(&S.bar, phase);
+        phase ^= 1u;
+        ok = __syncthreads_and(done) != 0;   // uniform across the CTA
+      }
+      if (!ok) break;
+      // epilogue: warps 0-3 own TMEM lanes 32w..32w+31 = rows i0 + 32w + lane
+      tc_fence_after();
+      if (warp < 4) {
+        const int row = i0 + warp * 32 + lane;
+        for (int cc = 0; cc < kTileN; cc += 32) {
+          double acc[32];
+#pragma unroll
+          for (int e = 0; e < 32; ++e) acc[e] = 0.0;
+          for (int g = 0; g < G; ++g) {
+            const int term = t0 + g;
+            const double scale = limb * (term == 0 ? Q.wmin : ldexp(Q.q, term - 1));
+            uint32_t v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(g * kTileN + cc), v);
+#pragma unroll
+            for (int e = 0; e < 32; ++e) acc[e] += scale * (double)(int32_t)v[e];
+          }
+          if (row < ermax) {
+            double* out = ecorr + (size_t)row * ermax + j0 + cc;
+#pragma unroll
+            for (int e = 0; e < 32; ++e)
+              if (j0 + cc + e < ermax) out[e] += acc[e];
+          }
+        }
+      }
+      tc_fence_before();
+      __syncthreads();
+    }
+  }
+  if (!ok) {
+    // record the failure and give the MMAs still in flight a bounded time to finish
+    // before the TMEM they write is released
+    if (tid == 0) atomicOr(err, kErrTimeout);
+    mbar_wait(&S.bar, phase ^ 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+}
+
+constexpr size_t kSmemBytes = sizeof(TcSmem) + 1024;
+
+}  // namespace
+
+int ecorr_tc_available() { return 1; }
+
+size_t ecorr_tc_workspace(int n, int ermax) {
+  const size_t kpad = (size_t)(n + kTileK - 1) / kTileK * kTileK;
+  const size_t ermax_pad = (size_t)(ermax + 127) / 128 * 128;
+  return 2 * ermax_pad * kpad + 4 * kpad + 256 + 64;
+}
+
+// ecorr += C^T diag(w) C for targets [base, base+n) of the batch starting at count_base
+int launch_ecorr_tc(const DeviceState& d, int base, int n, int ermax, int ermax_pad, int count_base, int weight_bits,
+                    void* work, size_t work_bytes, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_ecorr_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) != cudaSuccess)
+      return -1;
+    attr = true;
+  }
+  const int kpad = (n + kTileK - 1) / kTileK * kTileK;
+  const size_t need = 2 * (size_t)ermax_pad * kpad + 4 * (size_t)kpad + 256 + 64;
+  if (need > work_bytes) return -2;
+  uint8_t* ctl = (uint8_t*)work;
+  uint8_t* cth = ctl + (size_t)ermax_pad * kpad;
+  uint32_t* m = (uint32_t*)(cth + (size_t)ermax_pad * kpad);
+  QuantParams* qp = (QuantParams*)((uint8_t*)(m + kpad) + 0);
+  int* high = (int*)((uint8_t*)qp + 64);
+  int* errw = &d.status->flags;   // kErrTimeout if an mbarrier wait expires
+  cudaMemsetAsync(high, 0, sizeof(int), s);
+  dim3 tb(32, 8), tg((ermax_pad + 31) / 32, (kpad + 31) / 32);
+  k_counts_to_ct<<<tg, tb, 0, s>>>(n, kpad, ermax_pad, d.counts + (size_t)(base - count_base) * ermax_pad, ctl, cth,
+                                   high);
+  k_quantize<<<1, 1024, 0, s>>>(base, n, kpad, weight_bits > 0 ? weight_bits : 24, d.w, m, qp, high);
+  dim3 gg((ermax_pad + kTileN - 1) / kTileN, (ermax_pad + kTileM - 1) / kTileM);
+  k_ecorr_tc<<<gg, kThreads, kSmemBytes, s>>>(ermax, kpad, ctl, cth, m, qp, d.ecorr, errw);
+  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
 }  // namespace erm

@@ -746,6 +746,7 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
   if (hs.flags & kErrEngSft) return set_error(ctx, ERMOD_ERR_ENG_SFT, "eng_sft");
   if (hs.flags & kErrOverflow) return set_error(ctx, ERMOD_ERR_OVERFLOW, "ermod_ovf");
   if (hs.flags & kErrGrid) return set_error(ctx, ERMOD_ERR_OVERFLOW, "spr_box");
+  if (hs.flags & kErrTimeout) return set_error(ctx, ERMOD_ERR_CUDA, "tc_wait");
   if ((hs.flags & kWarnMbin) && ctx->warn_bin_firsttime) {
     ctx->warn_bin_firsttime = false;
     return set_error(ctx, ERMOD_WARN_MBIN, "mbin");

@@ -242,6 +242,46 @@ def test_eng_min_is_reported(lib):
     assert ei.value.name == "eng_min"
 
 
+def test_ecorr_tensor_core_matches_fp64(lib):
+    """INT8 tcgen05 path (weights as w_min + P-bit digits) against the FP64 CUDA-core kernel:
+    same energies and counts (deterministic engine), ecorr within the 2^-26 weight quantisation."""
+    w = S.make_workload(2, small=True, maxins=200)
+    res = []
+    for path in (0, 1):
+        eng = Engine(dict(w.params, ecorr_path=path), w.topo, w.hist)
+        for fr in range(2):
+            pos, cell = w.frame(fr)
+            assert eng.engconst(fr + 1, pos, cell) >= 0
+        res.append(eng.accum())
+        eng.close()
+    tc, ref = res
+    np.testing.assert_array_equal(tc["edens"], ref["edens"])
+    np.testing.assert_allclose(tc["ecorr"], ref["ecorr"], rtol=1e-7, atol=1e-12 * ref["engnorm"])
+    n = w.topo.nummol - 1
+    np.testing.assert_allclose(tc["ecorr"].sum(axis=0), n * tc["edens"], rtol=1e-7, atol=1e-9 * tc["engnorm"])
+
+
+def test_ecorr_tensor_core_counts_above_255(lib):
+    """A neutral LJ test particle leaves every molecule beyond the cutoff at exactly zero energy,
+    so one bin holds hundreds of molecules per insertion: the two-limb (c = 256 h + l) path."""
+    nside, box = 10, 31.04
+    topo = S.Topology([S.water(), S.lj_site()], [nside ** 3, 1], [A.PT_SOLVENT, A.PT_TEST_RIGID])
+    prm = S.default_params(ms1max=32, maxins=64, wgtslf=0, estype=A.ES_NVT, keep_uvengy=1)
+    w = S.Workload("lj-refs", prm, topo, {}, box, nside, 2, 11)
+    eng = Engine(prm, topo, {})
+    pos, cell = w.frame(0)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, _ = eng.uvengy()
+    bg = bins_of(u, eng.uvcrd, eng.uvmax, phys_uvspec(topo))
+    cnt = np.zeros((u.shape[0], eng.ermax))
+    for i in range(u.shape[0]):
+        np.add.at(cnt[i], bg[i], 1.0)
+    assert cnt.max() > 255
+    a = eng.accum()
+    np.testing.assert_array_equal(a["edens"], cnt.sum(axis=0))
+    np.testing.assert_array_equal(a["ecorr"], cnt.T @ cnt)
+
+
 def test_runs_are_bit_reproducible(lib):
     """Two contexts fed the same frames produce bit-identical energies and accumulators:
     spreading sums in fixed point and every FP64 reduction runs in a fixed order."""
