@@ -40,7 +40,7 @@ constexpr int kTileK = 128;          // insertions per K tile (one 128-byte swiz
 constexpr int kMaxGroup = 8;         // accumulators per pass: 8 x 64 = 512 TMEM columns
 constexpr int kThreads = 256;
 constexpr int kMaxDigits = 30;
-constexpr long long kSpinLimit = 1LL << 26;
+constexpr long long kSpinLimit = 1LL << 22;   // try_wait polls: a few seconds at most
 
 struct QuantParams {
   int P;              // weight digits
