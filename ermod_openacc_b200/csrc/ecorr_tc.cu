@@ -16,14 +16,17 @@
 // runs in a fixed order, so the result is deterministic.
 //
 // Kernel structure: a CTA per 128 x 64 tile of ecorr.  Per K tile of 128
-// insertions the CTA stages B (64 bin rows x 128 bytes) and up to eight
-// masked copies of A (128 bin rows x 128 bytes) in shared memory in the
-// 128-byte-swizzled K-major layout, one thread issues the tcgen05.mma
-// instructions (M=128, N=64, K=32 each) into up to eight TMEM accumulators
-// (8 x 64 columns), and a tcgen05.commit signals an mbarrier.  The epilogue
-// reads the accumulators with tcgen05.ld and adds scale * value into ecorr.
-// Every wait on the mbarrier has an iteration limit; on expiry the kernel
-// records an error, frees its TMEM and returns.
+// insertions the CTA stages A (128 bin rows x 128 bytes) and up to eight
+// masked copies of B (64 bin rows x 128 bytes, one per term of the group)
+// in shared memory in the 128-byte-swizzled K-major layout, in one of two
+// stages so that the next K tile is staged while the tensor cores work on
+// the current one.  One thread issues the tcgen05.mma instructions (M=128,
+// N=64, K=32 each) into up to eight TMEM accumulators (8 x 64 columns) and a
+// tcgen05.commit signals the stage's mbarrier.  The epilogue reads the
+// accumulators with tcgen05.ld and adds scale * value into ecorr.  Every wait
+// on an mbarrier has an iteration limit; on expiry the kernel records an
+// error, waits (again bounded) for its MMAs in flight, frees its TMEM and
+// returns.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -162,7 +165,8 @@ __global__ void k_counts_to_ct(int n, int kpad, int ermax_pad, const uint32_t* _
 
 // weights -> (wmin, q, P, m_cnt), one CTA, fixed-order reductions
 __global__ void k_quantize(int base, int n, int kpad, int bits, const double* __restrict__ w,
-                           uint32_t* __restrict__ m, QuantParams* qp, const int* __restrict__ high) {
+                           uint32_t* __restrict__ m, uint16_t* __restrict__ gbits, QuantParams* qp,
+                           const int* __restrict__ high) {
   __shared__ double smin[32], smax[32];
   double lo = 1e300, hi = -1e300;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -198,107 +202,150 @@ __global__ void k_quantize(int base, int n, int kpad, int bits, const double* __
   const double wmin = smin[0], q = smax[0];
   for (int i = threadIdx.x; i < kpad; i += blockDim.x)
     m[i] = (i < n && q > 0.0) ? (uint32_t)llrint((w[base + i] - wmin) / q) : 0u;
+  __syncthreads();
+  // mask bits per (K tile, term, 16-insertion chunk): term 0 = every insertion,
+  // term d >= 1 = insertions whose digit d-1 is set
+  const int P = qp->P;
+  const int nk = kpad / kTileK;
+  for (int x = threadIdx.x; x < nk * (kMaxDigits + 1) * 8; x += blockDim.x) {
+    const int kt = x / ((kMaxDigits + 1) * 8), rem = x % ((kMaxDigits + 1) * 8);
+    const int d = rem / 8, c = rem % 8;
+    uint32_t v = 0;
+    if (d <= P)
+      for (int e = 0; e < 16; ++e) {
+        const uint32_t mm = m[kt * kTileK + c * 16 + e];
+        v |= (d == 0 ? 1u : ((mm >> (d - 1)) & 1u)) << e;
+      }
+    gbits[x] = (uint16_t)v;
+  }
 }
 
 // ---- the GEMM ------------------------------------------------------------
+// Two shared-memory stages, each holding the unmasked A tile and one masked
+// copy of the B tile per term of the group: while the tensor cores run the
+// MMAs of one K tile, the threads load the next K tile from global memory
+// into registers and then fill the other stage.
+constexpr int kStages = 2;
+constexpr int kBitRows = kMaxDigits + 1;   // term 0 (all insertions) + digits 1..P
+
+struct TcStage {
+  uint8_t b[kMaxGroup][kTileN * kTileK];   // masked B copies, 8 KB each (1024-B aligned)
+  uint8_t a[kTileM * kTileK];              // A tile, 16 KB
+};
+
 struct TcSmem {
-  uint8_t a[kMaxGroup][kTileM * kTileK];   // masked A copies (16 KB each, 1024-B aligned)
-  uint8_t b[kTileN * kTileK];              // B tile (8 KB)
-  uint16_t bits[kMaxDigits + 1][kTileK / 16];  // per digit, per 16-insertion chunk: mask bits
-  uint64_t bar;
+  TcStage st[kStages];
+  uint64_t bar[kStages];
   uint32_t tmem_base;
 };
 
 __global__ void __launch_bounds__(kThreads, 1) k_ecorr_tc(int ermax, int kpad, const uint8_t* __restrict__ ctl,
-    const uint8_t* __restrict__ cth, const uint32_t* __restrict__ m, const QuantParams* __restrict__ qp,
+    const uint8_t* __restrict__ cth, const uint16_t* __restrict__ gbits, const QuantParams* __restrict__ qp,
     double* __restrict__ ecorr, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // 1024-byte alignment of the swizzled tiles
   TcSmem& S = *reinterpret_cast<TcSmem*>((void*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int i0 = blockIdx.y * kTileM, j0 = blockIdx.x * kTileN;
   const QuantParams Q = *qp;
   const int P = Q.P;
+  const int nk = kpad / kTileK;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
                  "r"(512));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    mbar_init(&S.bar, 1);
+    for (int s = 0; s < kStages; ++s) mbar_init(&S.bar[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = S.tmem_base;
-  uint32_t phase = 0;
+  uint32_t phase[kStages] = {0u, 0u};
+  bool used[kStages] = {false, false};
   bool ok = true;
+  // this thread's share of a K tile: 4 A chunks (rows tid/8 + 32 q), 2 B chunks
+  // (rows tid/8, tid/8 + 32), all in 16-byte chunk column c = tid % 8
+  const int c = tid & 7, r0 = tid >> 3;
+  uint4 ra[4], rb[2];
+  uint32_t rbits[kMaxGroup];
 
-  // terms: (limb pair, digit) with digit -1 = the plain w_min product
   const int npairs = Q.has_high ? 4 : 1;
-  const int nterms_pair = 1 + P;
+  const int nterms = 1 + P;
   for (int pair = 0; pair < npairs && ok; ++pair) {
     const uint8_t* A = (pair == 0 || pair == 1) ? ctl : cth;   // 0: l-l, 1: l-h, 2: h-l, 3: h-h
     const uint8_t* B = (pair == 0 || pair == 2) ? ctl : cth;
     const double limb = pair == 0 ? 1.0 : (pair == 3 ? 65536.0 : 256.0);
-    for (int t0 = 0; t0 < nterms_pair && ok; t0 += kMaxGroup) {
-      const int G = min(kMaxGroup, nterms_pair - t0);
-      for (int k0 = 0; k0 < kpad && ok; k0 += kTileK) {
-        // digit masks of this K tile: bit c of chunk (16 insertions) for digit d
-        for (int x = tid; x < (kMaxDigits + 1) * (kTileK / 16); x += blockDim.x) {
-          const int d = x / (kTileK / 16), c = x % (kTileK / 16);
-          uint32_t v = 0;
-          if (d <= P)
-            for (int e = 0; e < 16; ++e) {
-              const uint32_t mm = m[k0 + c * 16 + e];
-              const uint32_t bit = d == 0 ? 1u : ((mm >> (d - 1)) & 1u);   // d = 0: all insertions
-              v |= bit << e;
-            }
-          S.bits[d][c] = (uint16_t)v;
+    for (int t0 = 0; t0 < nterms && ok; t0 += kMaxGroup) {
+      const int G = min(kMaxGroup, nterms - t0);
+      auto load_tile = [&](int kt) {
+        const int k0 = kt * kTileK;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int r = r0 + 32 * q;
+          ra[q] = (i0 + r < ermax) ? *reinterpret_cast<const uint4*>(A + (size_t)(i0 + r) * kpad + k0 + c * 16)
+                                   : make_uint4(0, 0, 0, 0);
         }
-        // B tile: 64 rows x 8 chunks
-        for (int x = tid; x < kTileN * (kTileK / 16); x += blockDim.x) {
-          const int r = x >> 3, c = x & 7;
-          uint4 v = make_uint4(0, 0, 0, 0);
-          if (j0 + r < ermax) v = *reinterpret_cast<const uint4*>(B + (size_t)(j0 + r) * kpad + k0 + c * 16);
-          *reinterpret_cast<uint4*>(S.b + swz(r, c)) = v;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int r = r0 + 32 * q;
+          rb[q] = (j0 + r < ermax) ? *reinterpret_cast<const uint4*>(B + (size_t)(j0 + r) * kpad + k0 + c * 16)
+                                   : make_uint4(0, 0, 0, 0);
         }
-        __syncthreads();
-        // A tile: 128 rows x 8 chunks, one masked copy per term of the group
-        for (int x = tid; x < kTileM * (kTileK / 16); x += blockDim.x) {
-          const int r = x >> 3, c = x & 7;
-          uint4 v = make_uint4(0, 0, 0, 0);
-          if (i0 + r < ermax) v = *reinterpret_cast<const uint4*>(A + (size_t)(i0 + r) * kpad + k0 + c * 16);
-          for (int g = 0; g < G; ++g) {
-            const uint32_t bits = S.bits[t0 + g][c];
-            uint4 mv;
-            mv.x = v.x & expand4(bits & 15u);
-            mv.y = v.y & expand4((bits >> 4) & 15u);
-            mv.z = v.z & expand4((bits >> 8) & 15u);
-            mv.w = v.w & expand4((bits >> 12) & 15u);
-            *reinterpret_cast<uint4*>(S.a[g] + swz(r, c)) = mv;
+#pragma unroll
+        for (int g = 0; g < kMaxGroup; ++g)
+          rbits[g] = g < G ? (uint32_t)gbits[((size_t)kt * kBitRows + t0 + g) * 8 + c] : 0u;
+      };
+      load_tile(0);
+      for (int kt = 0; kt < nk; ++kt) {
+        const int s = kt & 1;
+        if (used[s]) {  // the MMAs that last read this stage must be done
+          const bool done = mbar_wait(&S.bar[s], phase[s]);
+          phase[s] ^= 1u;
+          used[s] = false;
+          ok = __syncthreads_and(done) != 0;
+          if (!ok) break;
+        }
+        TcStage& T = S.st[s];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) *reinterpret_cast<uint4*>(T.a + swz(r0 + 32 * q, c)) = ra[q];
+        for (int g = 0; g < G; ++g) {
+          const uint32_t bits = rbits[g];
+          const uint32_t m0 = expand4(bits & 15u), m1 = expand4((bits >> 4) & 15u);
+          const uint32_t m2 = expand4((bits >> 8) & 15u), m3 = expand4((bits >> 12) & 15u);
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            uint4 v = rb[q];
+            v.x &= m0; v.y &= m1; v.z &= m2; v.w &= m3;
+            *reinterpret_cast<uint4*>(T.b[g] + swz(r0 + 32 * q, c)) = v;
           }
         }
         fence_proxy_async();
         __syncthreads();
         if (tid == 0) {
           tc_fence_after();
-          const uint64_t db0 = smem_desc(smem_u32(S.b));
+          const uint64_t da0 = smem_desc(smem_u32(T.a));
           for (int g = 0; g < G; ++g) {
-            const uint64_t da0 = smem_desc(smem_u32(S.a[g]));
+            const uint64_t db0 = smem_desc(smem_u32(T.b[g]));
 #pragma unroll
             for (int ks = 0; ks < kTileK / 32; ++ks)   // K = 32 bytes per MMA: advance 32 B = 2 x 16 B
               mma_i8(tmem + (uint32_t)(g * kTileN), da0 + (uint64_t)(ks * 2), db0 + (uint64_t)(ks * 2),
-                     (k0 > 0 || ks > 0) ? 1u : 0u);
+                     (kt > 0 || ks > 0) ? 1u : 0u);
           }
-          mma_commit(&S.bar);
+          mma_commit(&S.bar[s]);
         }
-        __syncwarp();
-        bool done = mbar_wait(&S.bar, phase);
-        phase ^= 1u;
-        ok = __syncthreads_and(done) != 0;   // uniform across the CTA
+        used[s] = true;
+        if (kt + 1 < nk) load_tile(kt + 1);   // global loads overlap the MMAs just issued
       }
+      // drain both stages
+      for (int s = 0; s < kStages && ok; ++s)
+        if (used[s]) {
+          const bool done = mbar_wait(&S.bar[s], phase[s]);
+          phase[s] ^= 1u;
+          used[s] = false;
+          ok = __syncthreads_and(done) != 0;
+        }
       if (!ok) break;
       // epilogue: warps 0-3 own TMEM lanes 32w..32w+31 = rows i0 + 32w + lane
       tc_fence_after();
@@ -332,7 +379,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_ecorr_tc(int ermax, int kpad, c
     // record the failure and give the MMAs still in flight a bounded time to finish
     // before the TMEM they write is released
     if (tid == 0) atomicOr(err, kErrTimeout);
-    mbar_wait(&S.bar, phase ^ 1u);
+    for (int s = 0; s < kStages; ++s)
+      if (used[s]) mbar_wait(&S.bar[s], phase[s]);
   }
   tc_fence_before();
   __syncthreads();
@@ -348,7 +396,7 @@ int ecorr_tc_available() { return 1; }
 size_t ecorr_tc_workspace(int n, int ermax) {
   const size_t kpad = (size_t)(n + kTileK - 1) / kTileK * kTileK;
   const size_t ermax_pad = (size_t)(ermax + 127) / 128 * 128;
-  return 2 * ermax_pad * kpad + 4 * kpad + 256 + 64;
+  return 2 * ermax_pad * kpad + 4 * kpad + (kpad / kTileK) * (kMaxDigits + 1) * 8 * 2 + 256 + 64;
 }
 
 // ecorr += C^T diag(w) C for targets [base, base+n) of the batch starting at count_base
@@ -361,21 +409,23 @@ int launch_ecorr_tc(const DeviceState& d, int base, int n, int ermax, int ermax_
     attr = true;
   }
   const int kpad = (n + kTileK - 1) / kTileK * kTileK;
-  const size_t need = 2 * (size_t)ermax_pad * kpad + 4 * (size_t)kpad + 256 + 64;
+  const size_t nbits = (size_t)(kpad / kTileK) * (kMaxDigits + 1) * 8;
+  const size_t need = 2 * (size_t)ermax_pad * kpad + 4 * (size_t)kpad + 2 * nbits + 256 + 64;
   if (need > work_bytes) return -2;
   uint8_t* ctl = (uint8_t*)work;
   uint8_t* cth = ctl + (size_t)ermax_pad * kpad;
   uint32_t* m = (uint32_t*)(cth + (size_t)ermax_pad * kpad);
-  QuantParams* qp = (QuantParams*)((uint8_t*)(m + kpad) + 0);
+  uint16_t* gbits = (uint16_t*)(m + kpad);
+  QuantParams* qp = (QuantParams*)((uint8_t*)(gbits + nbits) + ((16 - (nbits * 2) % 16) % 16));
   int* high = (int*)((uint8_t*)qp + 64);
   int* errw = &d.status->flags;   // kErrTimeout if an mbarrier wait expires
   cudaMemsetAsync(high, 0, sizeof(int), s);
   dim3 tb(32, 8), tg((ermax_pad + 31) / 32, (kpad + 31) / 32);
   k_counts_to_ct<<<tg, tb, 0, s>>>(n, kpad, ermax_pad, d.counts + (size_t)(base - count_base) * ermax_pad, ctl, cth,
                                    high);
-  k_quantize<<<1, 1024, 0, s>>>(base, n, kpad, weight_bits > 0 ? weight_bits : 24, d.w, m, qp, high);
+  k_quantize<<<1, 1024, 0, s>>>(base, n, kpad, weight_bits > 0 ? weight_bits : 24, d.w, m, gbits, qp, high);
   dim3 gg((ermax_pad + kTileN - 1) / kTileN, (ermax_pad + kTileM - 1) / kTileM);
-  k_ecorr_tc<<<gg, kThreads, kSmemBytes, s>>>(ermax, kpad, ctl, cth, m, qp, d.ecorr, errw);
+  k_ecorr_tc<<<gg, kThreads, kSmemBytes, s>>>(ermax, kpad, ctl, cth, gbits, qp, d.ecorr, errw);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 

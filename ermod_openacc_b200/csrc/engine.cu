@@ -110,7 +110,7 @@ void free_all(ermod_ctx* c) {
                   d.anchor, d.cellof, d.cellcount, d.cellstart, d.molsorted, d.rmol, d.ins_conf, d.insw_in,
                   d.tgt_raw, d.tgt_n, d.tgt_c, d.tgt_mol, d.selfreal, d.selfrec, d.u0, d.w, d.etot, d.flceng,
                   d.grid, d.spec, d.phin, d.phi, d.engfac, d.splfc, d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
-                  d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.ecorr, d.eself,
+                  d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.edens_part, d.ecorr, d.eself,
                   d.slnuv, d.minuv, d.maxuv, d.scal, d.status, c->tc_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -398,6 +398,7 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   if (p.keep_uvengy) CK(dalloc(&d.uvengy, MD * SM));
   CK(dalloc(&d.counts, (size_t)ctx->batch * ctx->ermax_pad));
   CK(dalloc(&d.edens, ctx->ermax));
+  CK(dalloc(&d.edens_part, (size_t)kEdensSlices * ctx->ermax));
   if (p.corrcal) CK(dalloc(&d.ecorr, (size_t)ctx->ermax * ctx->ermax));
   CK(dalloc(&d.eself, std::max(1, ctx->esmax))); CK(dalloc(&d.slnuv, ctx->numslv));
   CK(dalloc(&d.minuv, ctx->numslv + 1)); CK(dalloc(&d.maxuv, ctx->numslv + 1));

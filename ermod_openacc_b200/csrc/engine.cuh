@@ -15,6 +15,7 @@ constexpr int kMaxOrder = 8;       // PME spline order limit (splodr)
 constexpr int kMaxSoluteSites = 1024;
 constexpr int kMaxLjTypes = 64;
 constexpr int kInflBlocks = 64;    // CTAs per target in the influence multiply
+constexpr int kEdensSlices = 32;   // target slices of the edens reduction
 constexpr int kMaxGrid = 256;      // largest PME grid dimension (x rows are one CTA dimension)
 
 // Everything the frame kernels read, passed by value.
@@ -97,6 +98,7 @@ struct DeviceState {
   uint32_t* counts = nullptr;// [batch*ermax_pad]
   // accumulators
   double* edens = nullptr;   // [ermax]
+  double* edens_part = nullptr; // [kEdensSlices*ermax] partial sums (NULL: one-pass edens kernel)
   double* ecorr = nullptr;   // [ermax*ermax]
   double* eself = nullptr;   // [esmax]
   double* slnuv = nullptr;   // [numslv]

@@ -972,9 +972,39 @@ __global__ void k_edens(int base, int n, int ermax, int ermax_pad, int count_bas
   edens[bin] += acc;
 }
 
+// edens over kEdensSlices slices of the targets: per-slice partial sums, then
+// one fixed-order sum over the slices (deterministic, like the one-pass kernel)
+__global__ void k_edens_part(int base, int n, int ermax, int ermax_pad, int count_base, const double* __restrict__ w,
+                             const uint32_t* __restrict__ counts, double* __restrict__ part) {
+  const int bin = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bin >= ermax) return;
+  const int sl = blockIdx.y, ns = gridDim.y;
+  const int lo = (int)((long long)n * sl / ns), hi = (int)((long long)n * (sl + 1) / ns);
+  double acc = 0.0;
+  for (int i = lo; i < hi; ++i) {
+    const uint32_t c = counts[(size_t)(base + i - count_base) * ermax_pad + bin];
+    if (c) acc += w[base + i] * (double)c;
+  }
+  part[(size_t)sl * ermax + bin] = acc;
+}
+
+__global__ void k_edens_sum(int ermax, int ns, const double* __restrict__ part, double* __restrict__ edens) {
+  const int bin = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bin >= ermax) return;
+  double acc = 0.0;
+  for (int sl = 0; sl < ns; ++sl) acc += part[(size_t)sl * ermax + bin];
+  edens[bin] += acc;
+}
+
 void launch_edens(const DeviceState& d, int base, int n, int ermax, int ermax_pad, int count_base, cudaStream_t s) {
   if (n <= 0) return;
-  k_edens<<<(ermax + 127) / 128, 128, 0, s>>>(base, n, ermax, ermax_pad, count_base, d.w, d.counts, d.edens);
+  if (!d.edens_part) {
+    k_edens<<<(ermax + 127) / 128, 128, 0, s>>>(base, n, ermax, ermax_pad, count_base, d.w, d.counts, d.edens);
+    return;
+  }
+  k_edens_part<<<dim3((ermax + 127) / 128, kEdensSlices), 128, 0, s>>>(base, n, ermax, ermax_pad, count_base, d.w,
+                                                                        d.counts, d.edens_part);
+  k_edens_sum<<<(ermax + 127) / 128, 128, 0, s>>>(ermax, kEdensSlices, d.edens_part, d.edens);
 }
 
 // FP64 CUDA-core ecorr update, 64x64 tile per 256 threads (4x4 per thread)
