@@ -109,6 +109,8 @@ def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int
         return min(maxdst, 4096) * (slvmax * 8 + ermax * 4)
     if stage == "influence":    # spectrum read + write, influence function read
         return chunk * KH * 8 * 2 + KH * 4
+    if stage == "spectrum":     # influence-weighted spectra written once, influence function read
+        return chunk * KH * 8 + KH * 4
     if stage == "transpose":    # potential grids read once, written once
         return 2 * chunk * KK * 4
     if stage == "spread":       # zero + scatter of the charge grids
@@ -253,11 +255,12 @@ def main():
     value = ws * units * args.steps / (dev_ms * 1e-3)
     e2e = ws * units * args.steps / e2e_s
     # roofline of the dominant engine kernel (cuFFT's own kernels are library code)
-    ours = ["real", "spread", "influence", "transpose", "gather", "bin", "ecorr"]
+    ours = ["real", "spread", "influence", "spectrum", "transpose", "gather", "bin", "ecorr"]
     dom = max(ours, key=lambda k: stage[k])
     nbatch = -(-eng.maxdst // 4096)
     per_frame_launches = {"real": nbatch, "spread": stage["chunks"], "influence": stage["chunks"],
-                          "transpose": stage["chunks"], "gather": stage["chunks"], "bin": nbatch, "ecorr": nbatch}
+                          "transpose": stage["chunks"], "gather": stage["chunks"], "bin": nbatch, "ecorr": nbatch,
+                          "spectrum": stage["chunks"]}
     n_launch = per_frame_launches[dom] * (args.steps if dom in ("real", "bin", "ecorr") else 1)
     per_launch_ms = stage[dom] / n_launch
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -268,6 +271,7 @@ def main():
     bytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst)
     achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
     kname = {"gather": "k_gather", "bin": "k_bin", "real": "k_real", "spread": "k_spread_box", "transpose": "k_transpose_phi",
+             "spectrum": "k_spectrum_direct",
              "influence": "k_influence", "ecorr": "k_ecorr"}[dom]
     traffic = traffic_from_profiles(kname)
     stage_share = {k: round(stage[k] / max(stage["total"], 1e-9), 4) for k in Engine.STAGES

@@ -53,8 +53,8 @@ class ErmodParams(C.Structure):
         ("elecut", C.c_float), ("lwljcut", C.c_float), ("upljcut", C.c_float), ("screen", C.c_float),
         ("ins_chunk", C.c_int32), ("ecorr_batch", C.c_int32), ("weight_bits", C.c_int32),
         ("proposal", C.c_int32),
-        ("keep_uvengy", C.c_int32), ("ecorr_path", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("keep_uvengy", C.c_int32), ("ecorr_path", C.c_int32), ("spectrum_path", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

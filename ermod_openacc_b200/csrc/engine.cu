@@ -80,14 +80,19 @@ struct ermod_ctx {
   std::vector<cudaEvent_t> pev;
   std::vector<int> ptag;
   int pused = 0;
-  float timings[14] = {0};
+  float timings[15] = {0};
   long long launches = 0;
   int use_tc = 1;
+  int direct = -1;   // spectrum path: -1 undecided, 0 spread + R2C, 1 direct site sums
 };
+
+// Solutes up to this many sites use the direct spectrum when spectrum_path == 0:
+// its cost grows with the site count while spreading + R2C does not.
+constexpr int kDirectAutoSites = 64;
 
 enum Stage { kStPrep = 1, kStIns = 2, kStReal = 3, kStSpread = 4, kStR2C = 5, kStInfl = 6, kStC2R = 7,
              kStGather = 8, kStBin = 9, kStWeights = 10, kStEcorr = 11, kStChunks = 12, kStTranspose = 13,
-             kNumTimings = 14 };
+             kStSpectrum = 14, kNumTimings = 15 };
 
 namespace {
 
@@ -690,18 +695,31 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
     for (int cb = bb; cb < bb + nbatch; cb += chunk) {
       const int nb = std::min(chunk, bb + nbatch - cb);
       if (pme) {
-        launch_spread(a, d, cb, nb, chunk, st);
-        mark(ctx, kStSpread);
-        CF(cufftExecR2C(ctx->r2c, d.grid, (cufftComplex*)d.spec));
-        mark(ctx, kStR2C);
-        launch_clear_box(a, d, chunk, st);
-        launch_influence(a, d, cb, nb, chunk, st);
-        mark(ctx, kStInfl);
+        if (ctx->direct < 0) {  // first frame: decide the spectrum path
+          const bool ok = direct_supported(a) && setup_direct(a) == 0;
+          const int sp = p.spectrum_path;
+          ctx->direct = (sp == 2 && ok) || (sp == 0 && ok && ctx->s <= kDirectAutoSites) ? 1 : 0;
+          if (sp == 2 && !ok) return set_error(ctx, ERMOD_ERR_UNSUPPORTED, "spc_path");
+        }
+        if (ctx->direct) {
+          launch_spectrum_direct(a, d, cb, nb, chunk, st);
+          mark(ctx, kStSpectrum);
+          nl += 1;
+        } else {
+          launch_spread(a, d, cb, nb, chunk, st);
+          mark(ctx, kStSpread);
+          CF(cufftExecR2C(ctx->r2c, d.grid, (cufftComplex*)d.spec));
+          mark(ctx, kStR2C);
+          launch_clear_box(a, d, chunk, st);
+          launch_influence(a, d, cb, nb, chunk, st);
+          mark(ctx, kStInfl);
+          nl += 3;
+        }
         CF(cufftExecC2R(ctx->c2r, (cufftComplex*)d.spec, d.phin));
         mark(ctx, kStC2R);
         launch_transpose_phi(a, d, st);
         mark(ctx, kStTranspose);
-        nl += 5;
+        nl += 1;
       }
       launch_gather(a, d, cb, bb, nb, chunk, ctx->batch, st);
       mark(ctx, kStGather);

@@ -123,6 +123,9 @@ void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, i
 int setup_spread_smem();
 void launch_transpose_phi(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
 void launch_clear_box(const FrameArgs& a, const DeviceState& d, int chunk, cudaStream_t s);
+bool direct_supported(const FrameArgs& a);
+int setup_direct(const FrameArgs& a);
+void launch_spectrum_direct(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
 
 struct BinArgs {

@@ -256,7 +256,7 @@ def default_params(**kw) -> dict:
              corrcal=1, selfcal=0, wgtslf=1, insposition=A.INSPOS_RANDOM, insorient=A.INSROT_RANDOM,
              iseed=123456789, temp=300.0 * KB_KCAL, elecut=12.0, lwljcut=10.0, upljcut=12.0, screen=0.35,
              ins_chunk=0, ecorr_batch=0, weight_bits=0, proposal=A.PROPOSAL_UNIFORM,
-             keep_uvengy=0, ecorr_path=0)
+             keep_uvengy=0, ecorr_path=0, spectrum_path=0)
     p.update(kw)
     p["ms2max"] = p["ms3max"] = p["ms1max"] if "ms2max" not in kw else p["ms2max"]
     return p

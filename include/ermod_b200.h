@@ -107,7 +107,8 @@ typedef struct ermod_params {
   int32_t proposal;               /* ERMOD_PROPOSAL_* */
   int32_t keep_uvengy;            /* 1: keep per-molecule energies for ermod_get_uvengy */
   int32_t ecorr_path;             /* 0: INT8 tensor-core GEMM, 1: FP64 CUDA-core kernel */
-  int32_t reserved[6];
+  int32_t spectrum_path;          /* 0: by solute size, 1: spread + cuFFT R2C, 2: direct site sums */
+  int32_t reserved[5];
 } ermod_params;
 
 /*
@@ -256,8 +257,8 @@ const char* ermod_last_error(const ermod_ctx* ctx);
  * [0] total, [1] prepare + cell list, [2] insertion, [3] real space,
  * [4] PME spread, [5] FFT R2C, [6] influence multiply, [7] FFT C2R,
  * [8] PME gather, [9] binning, [10] weights + edens, [11] ecorr,
- * [12] number of PME target chunks, [13] potential-grid transpose.
- * n <= 14. */
+ * [12] number of PME target chunks, [13] potential-grid transpose,
+ * [14] direct solute spectrum.  n <= 15. */
 int32_t ermod_get_timings(const ermod_ctx* ctx, float* ms, int32_t n);
 
 /* Kernel launches of this library since the context was created, cuFFT's

@@ -81,10 +81,11 @@ def test_refs_ring_placement(lib, oracle_mod):
     assert np.all(wts == 1.0)
 
 
-@pytest.mark.parametrize("config", [2, 3])
-def test_refs_energies_and_bins(lib, oracle_mod, config):
+@pytest.mark.parametrize("config,path", [(2, 1), (2, 2), (3, 1), (3, 2)])
+def test_refs_energies_and_bins(lib, oracle_mod, config, path):
+    """spectrum path 1: fixed-point spreading + cuFFT R2C; 2: direct sums over the sites."""
     w = S.make_workload(config, small=True, maxins=96)
-    prm = dict(w.params, keep_uvengy=1)
+    prm = dict(w.params, keep_uvengy=1, spectrum_path=path)
     eng = Engine(prm, w.topo, w.hist)
     pos, cell = w.frame(0)
     assert eng.engconst(1, pos, cell) >= 0
@@ -194,10 +195,10 @@ def test_engstore_normalisation(lib):
     assert z["engnorm"] == 0 and not z["edens"].any() and not z["ecorr"].any()
 
 
-@pytest.mark.parametrize("K,order", [(32, 6), (32, 4)])
-def test_madelung_gpu(lib, K, order):
+@pytest.mark.parametrize("K,order,path", [(32, 6, 1), (32, 4, 1), (32, 6, 2), (64, 8, 2)])
+def test_madelung_gpu(lib, K, order, path):
     prm, topo, hist, pos, cell, ins, L = nacl_system(K=K, order=order)
-    eng = Engine(dict(prm, keep_uvengy=1), topo, hist)
+    eng = Engine(dict(prm, keep_uvengy=1, spectrum_path=path), topo, hist)
     assert eng.engconst(1, pos, cell, ins_conf=ins) >= 0
     u, u0 = eng.uvengy()
     e_int = COULOMB * (-MADELUNG_NACL / 2.8 - WIGNER_SC / L)
