@@ -98,7 +98,7 @@ def dist_init():
     return ws, rank, local
 
 
-def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int, maxdst: int) -> float:
+def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int, maxdst: int, nsite: int) -> float:
     """Algorithmic DRAM bytes of ONE launch of each of the engine's kernels."""
     K = w.params["ms1max"]
     n = w.params["splodr"]
@@ -109,8 +109,10 @@ def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int
         return min(maxdst, 4096) * (slvmax * 8 + ermax * 4)
     if stage == "influence":    # spectrum read + write, influence function read
         return chunk * KH * 8 * 2 + KH * 4
-    if stage == "spectrum":     # influence-weighted spectra written once, influence function read
-        return chunk * KH * 8 + KH * 4
+    if stage == "pme_plane":    # solute sites in, transformed planes out once, influence function in
+        return chunk * KH * 8 + KH * 4 + chunk * nsite * 16
+    if stage == "pme_rows":     # transformed planes in, potential grids out (insertion-fastest)
+        return chunk * KH * 8 + chunk * KK * 4
     if stage == "transpose":    # potential grids read once, written once
         return 2 * chunk * KK * 4
     if stage == "spread":       # zero + scatter of the charge grids
@@ -255,24 +257,22 @@ def main():
     value = ws * units * args.steps / (dev_ms * 1e-3)
     e2e = ws * units * args.steps / e2e_s
     # roofline of the dominant engine kernel (cuFFT's own kernels are library code)
-    ours = ["real", "spread", "influence", "spectrum", "transpose", "gather", "bin", "ecorr"]
+    ours = ["real", "spread", "influence", "pme_plane", "pme_rows", "transpose", "gather", "bin", "ecorr"]
     dom = max(ours, key=lambda k: stage[k])
     nbatch = -(-eng.maxdst // 4096)
-    per_frame_launches = {"real": nbatch, "spread": stage["chunks"], "influence": stage["chunks"],
-                          "transpose": stage["chunks"], "gather": stage["chunks"], "bin": nbatch, "ecorr": nbatch,
-                          "spectrum": stage["chunks"]}
-    n_launch = per_frame_launches[dom] * (args.steps if dom in ("real", "bin", "ecorr") else 1)
+    per_batch = ("real", "bin", "ecorr")
+    # stage["chunks"] sums the per-frame chunk counts over the timed steps
+    n_launch = nbatch * args.steps if dom in per_batch else stage["chunks"]
     per_launch_ms = stage[dom] / n_launch
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
         peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     chunk = 32
-    bytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst)
+    bytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
     achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
-    kname = {"gather": "k_gather", "bin": "k_bin", "real": "k_real", "spread": "k_spread_box", "transpose": "k_transpose_phi",
-             "spectrum": "k_spectrum_direct",
-             "influence": "k_influence", "ecorr": "k_ecorr"}[dom]
+    kname = {"gather": "k_gather", "bin": "k_bin", "real": "k_real", "spread": "k_spread_box",
+             "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane", "pme_rows": "k_pme_rows", "influence": "k_influence", "ecorr": "k_ecorr_tc"}[dom]
     traffic = traffic_from_profiles(kname)
     stage_share = {k: round(stage[k] / max(stage["total"], 1e-9), 4) for k in Engine.STAGES
                    if k not in ("total", "chunks")}
@@ -286,6 +286,8 @@ def main():
             "config": {"workload": w.name, "waters": int(eng.slvmax), "insertions_per_frame": int(eng.maxdst),
                        "solute_sites": int(eng.nsite_slt), "pme_grid": w.params["ms1max"],
                        "pme_order": w.params["splodr"], "ermax": int(eng.ermax),
+                       "pme_solve": {0: "none", 1: "spread + cuFFT", 2: "fused, direct site sums",
+                                     3: "fused, plane spreading + FFT"}[eng.paths()["spectrum_path"]],
                        "l2": "flushed before every step (256 MiB write)",
                        "parallelism": f"frames sharded over {ws} rank(s), no collective in the step"},
             "stage_share": stage_share,

@@ -123,6 +123,7 @@ SIGNATURES = {
     "ermod_last_error": (C.c_char_p, [C.c_void_p]),
     "ermod_get_timings": (C.c_int32, [C.c_void_p, _f32p, C.c_int32]),
     "ermod_get_launch_count": (C.c_int64, [C.c_void_p]),
+    "ermod_get_paths": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ermod_destroy": (None, [C.c_void_p]),
     "ermod_histogram_noalloc": (C.c_int32, [C.c_int32, C.c_int32, _f64p, C.c_int32, C.c_int32, _i32p, _f64p,
                                             _i32p, _i32p, C.c_int32, _f64p, _f64p]),

@@ -124,19 +124,23 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
 __device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
 constexpr uint32_t kStreamTag = 0x45524D44u;
 
-// Cardinal B-spline M_n(x) (erdst/spline.F90:25-58); coeff[i] = (-1)^i n / (i!(n-i)!).
-__device__ __forceinline__ float spline_value(const float* coeff, int order, float x) {
-  float f = 0.0f;
-  if (x > 0.0f && x < (float)order) {
-    const int k = (int)x;
-    for (int i = 0; i <= k; ++i) {
-      const float d = x - (float)i;
-      float pw = 1.0f;
-      for (int e = 0; e < order - 1; ++e) pw *= d;
-      f += coeff[i] * pw;
-    }
+// Cardinal B-spline weights w[c] = M_n(u + c), c = 0..n-1, of a site at
+// fractional grid offset u in [0, 1): the stencil of calc_spline_molecule
+// (recpcal.F90:506-574).  The reference evaluates M_n by the truncated-power
+// sum of spline.F90:45-58, sum_i (-1)^i n/(i!(n-i)!) (x-i)^(n-1), whose terms
+// reach ~3e2 at order 8 while M_n is O(1), so FP32 loses ~1e-5 absolute
+// there.  The same function is formed here by the Cox-de Boor recursion
+// M_k(x) = (x M_{k-1}(x) + (k-x) M_{k-1}(x-1)) / (k-1) (Essmann et al.,
+// J. Chem. Phys. 103, 8577 (1995), eq. 4.1), whose terms are all positive.
+__device__ __forceinline__ void spline_weights(float u, int order, float* w) {
+  w[0] = 1.0f;                                  // M_1(u)
+  for (int k = 2; k <= order; ++k) {
+    const float rk = 1.0f / (float)(k - 1);
+    w[k - 1] = (1.0f - u) * w[k - 2] * rk;      // x = u + k - 1: x M(x) term vanishes (M_{k-1}(x) = 0)
+    for (int c = k - 2; c >= 1; --c)
+      w[c] = ((u + (float)c) * w[c] + ((float)k - u - (float)c) * w[c - 1]) * rk;
+    w[0] = u * w[0] * rk;
   }
-  return f;
 }
 
 // grid index r in [-(order-1), K] wrapped into [0, K) (the reference's modulo, recpcal.F90:388-390)

@@ -72,7 +72,6 @@ struct ermod_ctx {
   float invcell_prev[3] = {0.f, 0.f, 0.f};
   float prevcl[9] = {0};
   bool pme_init = false, usreal_init = false, warn_bin_firsttime = true;
-  float spl_coeff[kMaxOrder + 1] = {0};
   float* h_pin = nullptr;
   size_t h_pin_bytes = 0;
   std::string err;
@@ -80,19 +79,20 @@ struct ermod_ctx {
   std::vector<cudaEvent_t> pev;
   std::vector<int> ptag;
   int pused = 0;
-  float timings[15] = {0};
+  float timings[16] = {0};
   long long launches = 0;
   int use_tc = 1;
-  int direct = -1;   // spectrum path: -1 undecided, 0 spread + R2C, 1 direct site sums
+  int spath = 1;     // PME solve: 1 spread + cuFFT, 2 fused with direct site sums, 3 fused with plane spreading
 };
 
-// Solutes up to this many sites use the direct spectrum when spectrum_path == 0:
-// its cost grows with the site count while spreading + R2C does not.
-constexpr int kDirectAutoSites = 64;
+// With spectrum_path == 0 the fused solve builds the solute spectrum by direct
+// site sums up to this many sites and by plane spreading + forward FFT above:
+// the sums cost s * K2 * K3 per plane, the FFT a fixed ~K2 * K3 * log(K2 K3).
+constexpr int kDirectAutoSites = 16;
 
 enum Stage { kStPrep = 1, kStIns = 2, kStReal = 3, kStSpread = 4, kStR2C = 5, kStInfl = 6, kStC2R = 7,
              kStGather = 8, kStBin = 9, kStWeights = 10, kStEcorr = 11, kStChunks = 12, kStTranspose = 13,
-             kStSpectrum = 14, kNumTimings = 15 };
+             kStPlane = 14, kStRows = 15, kNumTimings = 16 };
 
 namespace {
 
@@ -114,7 +114,8 @@ void free_all(ermod_ctx* c) {
                   d.slt_mass, d.bfcoord, d.uvcrd, d.spec_off, d.uvsoft, d.escrd, d.posraw, d.slvn, d.spl, d.grd,
                   d.anchor, d.cellof, d.cellcount, d.cellstart, d.molsorted, d.rmol, d.ins_conf, d.insw_in,
                   d.tgt_raw, d.tgt_n, d.tgt_c, d.tgt_mol, d.selfreal, d.selfrec, d.u0, d.w, d.etot, d.flceng,
-                  d.grid, d.spec, d.phin, d.phi, d.engfac, d.splfc, d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
+                  d.grid, d.spec, d.phin, d.phi, d.engfac, d.engfacT, d.fft_tw, d.fft_twd, d.splfc,
+                  d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
                   d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.edens_part, d.ecorr, d.eself,
                   d.slnuv, d.minuv, d.maxuv, d.scal, d.status, c->tc_work};
   for (void* p : ptrs)
@@ -132,17 +133,6 @@ void free_all(ermod_ctx* c) {
 }
 
 // spline.F90:25-44
-void spline_coeff(int order, float* coeff) {
-  for (int i = 0; i <= order; ++i) {
-    float f = 1.0f;
-    for (int k = 1; k <= i; ++k) f *= (float)k;
-    for (int k = 1; k <= order - i; ++k) f *= (float)k;
-    f = (float)order / f;
-    if (i % 2 == 1) f = -f;
-    coeff[i] = f;
-  }
-}
-
 double spline_value_d(int order, double x) {
   double c[kMaxOrder + 1];
   for (int i = 0; i <= order; ++i) {
@@ -357,7 +347,6 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   ctx->batch = std::max(ctx->chunk, (ctx->batch + ctx->chunk - 1) / ctx->chunk * ctx->chunk);
   ctx->batch = std::min(ctx->batch, (ctx->maxdst + ctx->chunk - 1) / ctx->chunk * ctx->chunk);
   ctx->ncell_cap = 64 * 64 * 64;
-  spline_coeff(pme ? p.splodr : 4, ctx->spl_coeff);
   *out = ctx;
 
   CK(cudaSetDevice(device));
@@ -381,11 +370,33 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   CK(dalloc(&d.selfreal, MD)); CK(dalloc(&d.selfrec, MD)); CK(dalloc(&d.u0, MD)); CK(dalloc(&d.w, MD));
   CK(dalloc(&d.etot, MD)); CK(dalloc(&d.flceng, MD * ctx->numslv));
   const size_t KK = (size_t)K1 * K2 * K3, KH = (size_t)K3 * K2 * Kh1;
+  // PME solve path (spectrum_path): the fused solve where the mesh allows it
+  FrameArgs fa{};
+  fa.pme = pme; fa.K1 = K1; fa.K2 = K2; fa.K3 = K3; fa.Kh1 = Kh1; fa.nsite = ctx->s; fa.order = order;
+  const bool fused_ok = pme && fused_supported(fa);
+  if (p.spectrum_path < 0 || p.spectrum_path > 3) return bad(ERMOD_ERR_ARG, "spc_path");
+  if (pme && p.spectrum_path >= 2 && !fused_ok) return bad(ERMOD_ERR_UNSUPPORTED, "spc_path");
+  if (p.spectrum_path == 0) ctx->spath = fused_ok ? (ctx->s <= kDirectAutoSites ? 2 : 3) : 1;
+  else ctx->spath = p.spectrum_path;
   if (pme) {
-    CK(dalloc(&d.grid, (size_t)ctx->chunk * KK)); CK(dalloc(&d.spec, (size_t)ctx->chunk * KH));
-    CK(cudaMemsetAsync(d.grid, 0, sizeof(float) * ctx->chunk * KK, ctx->st));  // kept zero outside the boxes
-    CK(dalloc(&d.phin, (size_t)ctx->chunk * KK));
+    CK(dalloc(&d.spec, (size_t)ctx->chunk * KH));
     CK(dalloc(&d.phi, (size_t)ctx->chunk * KK)); CK(dalloc(&d.engfac, KH)); CK(dalloc(&d.splfc, K1 + K2 + K3));
+    if (ctx->spath == 1) {
+      CK(dalloc(&d.grid, (size_t)ctx->chunk * KK));
+      CK(cudaMemsetAsync(d.grid, 0, sizeof(float) * ctx->chunk * KK, ctx->st));  // kept zero outside the boxes
+      CK(dalloc(&d.phin, (size_t)ctx->chunk * KK));
+    } else {
+      CK(dalloc(&d.engfacT, KH));
+      std::vector<float2> tw;
+      std::vector<double2> twd;
+      fused_twiddles(K1, K2, K3, tw, twd);
+      CK(dalloc(&d.fft_tw, tw.size()));
+      CK(dalloc(&d.fft_twd, twd.size()));
+      CK(cudaMemcpyAsync(d.fft_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice, ctx->st));
+      CK(cudaMemcpyAsync(d.fft_twd, twd.data(), sizeof(double2) * twd.size(), cudaMemcpyHostToDevice, ctx->st));
+      CK(cudaStreamSynchronize(ctx->st));
+      if (setup_fused(fa) != 0) return bad(ERMOD_ERR_CUDA, "pme_smem");
+    }
   }
   CK(dalloc(&d.E, SM * ctx->batch));
   CK(dalloc(&d.Etot, SM * ctx->batch));
@@ -393,9 +404,9 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   CK(dalloc(&d.twt, MD));
   CK(dalloc(&d.sbin, MD));
   if (pme) {
-    CK(dalloc(&d.gacc, (size_t)ctx->chunk * KK));
+    if (ctx->spath == 1) CK(dalloc(&d.gacc, (size_t)ctx->chunk * KK));
     CK(dalloc(&d.boxinfo, 2 * (size_t)ctx->chunk));
-    CK(dalloc(&d.partial, (size_t)ctx->chunk * kInflBlocks));
+    CK(dalloc(&d.partial, (size_t)ctx->chunk * std::max(kInflBlocks, Kh1)));
     CK(dalloc(&d.done, (size_t)ctx->chunk));
     CK(cudaMemsetAsync(d.done, 0, sizeof(unsigned int) * ctx->chunk, ctx->st));
     if (setup_spread_smem() != 0) return bad(ERMOD_ERR_CUDA, "spr_smem");
@@ -452,6 +463,8 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     spline_axis(K2, p.splodr, sf.data() + K1);
     spline_axis(K3, p.splodr, sf.data() + K1 + K2);
     CK(h2d(d.splfc, sf.data(), K1 + K2 + K3, st));
+  }
+  if (pme && ctx->spath == 1) {
     int n[3] = {K3, K2, K1};
     int inR[3] = {K3, K2, K1}, onC[3] = {K3, K2, Kh1};
     CF(cufftPlanMany(&ctx->r2c, 3, n, inR, 1, (int)KK, onC, 1, (int)KH, CUFFT_R2C, ctx->chunk));
@@ -602,7 +615,6 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
   P.bare = p.cltype == ERMOD_EL_COULOMB;
   a.slvmax = ctx->slvmax; a.natoms = ctx->natoms; a.nsite = ctx->s; a.maxdst = ctx->maxdst;
   a.K1 = K1; a.K2 = K2; a.K3 = K3; a.order = pme ? p.splodr : 1; a.Kh1 = K1 / 2 + 1;
-  for (int i = 0; i <= kMaxOrder; ++i) a.spl_coeff[i] = ctx->spl_coeff[i];
   a.ljtype_max = ctx->ljtype_max;
   a.pme = pme;
   a.pivol = pme ? kPi / ((double)p.screen * (double)p.screen) / vold : 0.0;
@@ -694,27 +706,21 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
     nl += 1;
     for (int cb = bb; cb < bb + nbatch; cb += chunk) {
       const int nb = std::min(chunk, bb + nbatch - cb);
-      if (pme) {
-        if (ctx->direct < 0) {  // first frame: decide the spectrum path
-          const bool ok = direct_supported(a) && setup_direct(a) == 0;
-          const int sp = p.spectrum_path;
-          ctx->direct = (sp == 2 && ok) || (sp == 0 && ok && ctx->s <= kDirectAutoSites) ? 1 : 0;
-          if (sp == 2 && !ok) return set_error(ctx, ERMOD_ERR_UNSUPPORTED, "spc_path");
-        }
-        if (ctx->direct) {
-          launch_spectrum_direct(a, d, cb, nb, chunk, st);
-          mark(ctx, kStSpectrum);
-          nl += 1;
-        } else {
-          launch_spread(a, d, cb, nb, chunk, st);
-          mark(ctx, kStSpread);
-          CF(cufftExecR2C(ctx->r2c, d.grid, (cufftComplex*)d.spec));
-          mark(ctx, kStR2C);
-          launch_clear_box(a, d, chunk, st);
-          launch_influence(a, d, cb, nb, chunk, st);
-          mark(ctx, kStInfl);
-          nl += 3;
-        }
+      if (pme && ctx->spath != 1) {
+        launch_pme_plane(a, d, cb, nb, ctx->spath == 2, st);
+        mark(ctx, kStPlane);
+        launch_pme_rows(a, d, nb, st);
+        mark(ctx, kStRows);
+        nl += 2;
+      } else if (pme) {
+        launch_spread(a, d, cb, nb, chunk, st);
+        mark(ctx, kStSpread);
+        CF(cufftExecR2C(ctx->r2c, d.grid, (cufftComplex*)d.spec));
+        mark(ctx, kStR2C);
+        launch_clear_box(a, d, chunk, st);
+        launch_influence(a, d, cb, nb, chunk, st);
+        mark(ctx, kStInfl);
+        nl += 3;
         CF(cufftExecC2R(ctx->c2r, (cufftComplex*)d.spec, d.phin));
         mark(ctx, kStC2R);
         launch_transpose_phi(a, d, st);
@@ -917,6 +923,13 @@ int32_t ermod_get_timings(const ermod_ctx* ctx, float* ms, int32_t n) {
 }
 
 int64_t ermod_get_launch_count(const ermod_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int32_t ermod_get_paths(const ermod_ctx* ctx, int32_t* spectrum_path, int32_t* ecorr_path) {
+  if (!ctx) return ERMOD_ERR_ARG;
+  if (spectrum_path) *spectrum_path = ctx->p.cltype == ERMOD_EL_PME ? ctx->spath : 0;
+  if (ecorr_path) *ecorr_path = ctx->p.corrcal ? (ctx->use_tc ? 0 : 1) : -1;
+  return ERMOD_OK;
+}
 
 void ermod_destroy(ermod_ctx* ctx) {
   if (!ctx) return;

@@ -24,7 +24,6 @@ struct FrameArgs {
   PairParams pp;
   int slvmax, natoms, nsite, maxdst;
   int K1, K2, K3, order, Kh1;      // Kh1 = K1/2+1
-  float spl_coeff[kMaxOrder + 1];
   int ljtype_max;
   int pme;
   double pivol;                    // pi / screen^2 / volume (residual terms, engproc.F90:974,994)
@@ -84,6 +83,9 @@ struct DeviceState {
   float* phin = nullptr;     // [chunk*K^3] potential grids as the C2R writes them
   float* phi = nullptr;      // [K^3*chunk], insertion fastest
   float* engfac = nullptr;   // [K3*K2*Kh1]
+  float* engfacT = nullptr;  // [Kh1*K3*K2] influence function, k1-major (fused PME solve)
+  float2* fft_tw = nullptr;  // [K1+K2+K3+K1/2] FP32 twiddle tables of the fused PME solve
+  double2* fft_twd = nullptr;// [K1+K2+K3] FP64 twiddle tables (stencil transforms)
   double* splfc = nullptr;   // [K1+K2+K3]
   double* E = nullptr;       // [slvmax*batch] real-space energies of the batch, molecule-major
   double* Etot = nullptr;    // [batch*slvmax] total pair energies of the batch, target-major (uvengy layout)
@@ -123,9 +125,12 @@ void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, i
 int setup_spread_smem();
 void launch_transpose_phi(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
 void launch_clear_box(const FrameArgs& a, const DeviceState& d, int chunk, cudaStream_t s);
-bool direct_supported(const FrameArgs& a);
-int setup_direct(const FrameArgs& a);
-void launch_spectrum_direct(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
+// fused PME solve (pme_fused.cu)
+bool fused_supported(const FrameArgs& a);
+int setup_fused(const FrameArgs& a);
+void fused_twiddles(int K1, int K2, int K3, std::vector<float2>& tw, std::vector<double2>& twd);
+void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int nb, bool direct, cudaStream_t s);
+void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int nb, cudaStream_t s);
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
 
 struct BinArgs {

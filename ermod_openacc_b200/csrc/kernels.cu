@@ -45,8 +45,9 @@ __global__ void k_prepare_solvent(FrameArgs a, const float* __restrict__ posraw,
     for (int m = 0; m < 3; ++m) {
       const float f = inm[m] * (float)K[m];
       const int rci = (int)f;
-      for (int spi = 0; spi < a.order; ++spi)
-        spl[((size_t)i * 3 + m) * a.order + spi] = spline_value(a.spl_coeff, a.order, f - (float)(rci - spi));
+      float w[kMaxOrder];
+      spline_weights(f - (float)rci, a.order, w);
+      for (int spi = 0; spi < a.order; ++spi) spl[((size_t)i * 3 + m) * a.order + spi] = w[spi];
       gi[m] = rci;
     }
     grd[i] = make_int4(gi[0], gi[1], gi[2], 0);
@@ -424,7 +425,8 @@ void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int
 struct Mat3d { double m[3][3]; };
 
 __global__ void k_engfac(int K1, int K2, int K3, int Kh1, int order, Mat3d invcl, double volume, double screen,
-                         const double* __restrict__ splfc, float* __restrict__ engfac) {
+                         const double* __restrict__ splfc, float* __restrict__ engfac,
+                         float* __restrict__ engfacT) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = K3 * K2 * Kh1;
   if (i >= n) return;
@@ -448,6 +450,7 @@ __global__ void k_engfac(int K1, int K2, int K3, int Kh1, int order, Mat3d invcl
     }
   }
   engfac[i] = (float)factor;
+  if (engfacT) engfacT[((size_t)r1 * K3 + r3) * K2 + r2] = (float)factor;   // [k1][k3][k2] for k_pme_plane
 }
 
 void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[3][3], double volume, double screen,
@@ -455,7 +458,8 @@ void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[
   Mat3d m;
   for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) m.m[i][j] = invcl[i][j];
   const int n = a.K3 * a.K2 * a.Kh1;
-  k_engfac<<<(n + 255) / 256, 256, 0, s>>>(a.K1, a.K2, a.K3, a.Kh1, a.order, m, volume, screen, d.splfc, d.engfac);
+  k_engfac<<<(n + 255) / 256, 256, 0, s>>>(a.K1, a.K2, a.K3, a.Kh1, a.order, m, volume, screen, d.splfc, d.engfac,
+                                         d.engfacT);
 }
 
 // ---------------------------------------------------------------------------
@@ -479,7 +483,7 @@ __device__ __forceinline__ void site_spline(const FrameArgs& a, float4 r, float 
     f = f - floorf(f);
     f = f * (float)K[m];
     const int rci = (int)f;
-    for (int spi = 0; spi < a.order; ++spi) w[m][spi] = spline_value(a.spl_coeff, a.order, f - (float)(rci - spi));
+    spline_weights(f - (float)rci, a.order, w[m]);
     gi[m] = rci;
   }
 }
@@ -679,170 +683,6 @@ void launch_transpose_phi(const FrameArgs& a, const DeviceState& d, cudaStream_t
 
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
   k_influence<<<dim3(kInflBlocks, chunk), 256, 0, s>>>(a, base, nb, d.spec, d.engfac, d.partial, d.done, d.selfrec);
-}
-
-// ---------------------------------------------------------------------------
-// Direct spectrum of the spread solute charges.  The forward FFT of the
-// B-spline-spread grid (recpcal.F90:453-475) is, mode by mode,
-//   Qhat(k) = sum_a q_a B1_a(k1) B2_a(k2) B3_a(k3),
-//   B_{a,m}(k) = sum_c w_{a,m,c} exp(-2 pi i k (g_{a,m} - c) / K_m),
-// the product of the 1-D transforms of each site's spline stencil: exactly
-// the transform of the spread grid, without building the grid.  For small
-// solutes the sum costs less than spreading a full grid and transforming
-// it.  The kernel applies the influence function and forms the FP64 self
-// energy as k_influence does (recpcal.F90:482-497), and leaves the
-// influence-weighted spectrum for cuFFT's C2R.  CTA = (target, slab of k3
-// planes) with one (k2, k3) row of modes per thread; the site tables sit in
-// shared memory and the rows are staged there for coalesced stores.
-// ---------------------------------------------------------------------------
-constexpr int kDirThreads = 256;
-constexpr int kDirMaxKh1 = 65;          // K1 <= 128
-
-size_t direct_smem_bytes(const FrameArgs& a) {
-  const int slab = kDirThreads / a.K2;
-  return sizeof(float2) * (size_t)(a.K1 + a.K2 + a.K3)                       // twiddles
-         + sizeof(float) * (size_t)a.nsite * 3 * (kMaxOrder + 1)                // weights + grid index
-         + sizeof(float2) * (size_t)a.nsite * (a.Kh1 + a.K2 + slab)             // site transforms
-         + sizeof(float2) * (size_t)kDirThreads * a.Kh1                         // staged output rows
-         + 16;                                                                   // alignment pad
-}
-
-bool direct_supported(const FrameArgs& a) {
-  return a.pme && a.Kh1 <= kDirMaxKh1 && a.K2 <= kDirThreads && (kDirThreads % a.K2) == 0 &&
-         (a.K3 % (kDirThreads / a.K2)) == 0 && direct_smem_bytes(a) <= 200 * 1024;
-}
-
-__global__ void __launch_bounds__(kDirThreads) k_spectrum_direct(FrameArgs a, int base, int nb,
-    const float4* __restrict__ tgt_raw, const float* __restrict__ engfac, float2* __restrict__ spec,
-    double* __restrict__ partial, unsigned int* __restrict__ done, double* __restrict__ selfrec) {
-  extern __shared__ __align__(16) unsigned char dsm[];
-  const int b = blockIdx.y;
-  if (b >= nb) return;   // unused slot of a partial chunk: its spectrum is never read
-  const int slab = kDirThreads / a.K2, k30 = blockIdx.x * slab;
-  const int K1 = a.K1, K2 = a.K2, K3 = a.K3, Kh1 = a.Kh1, s = a.nsite, n = a.order;
-  float2* tw1 = (float2*)dsm;
-  float2* tw2 = tw1 + K1;
-  float2* tw3 = tw2 + K2;
-  float* sw = (float*)(tw3 + K3);                  // [s][3][n] weights, [s][3] grid index as float
-  float* sg = sw + (size_t)s * 3 * kMaxOrder;
-  float2* B1 = (float2*)(sg + (size_t)s * 3 + ((s * 3) & 1));
-  float2* B2 = B1 + (size_t)s * Kh1;
-  float2* B3 = B2 + (size_t)s * K2;
-  float2* outs = B3 + (size_t)s * slab;
-  const int tid = threadIdx.x;
-  // twiddles exp(-2 pi i p / K)
-  for (int p = tid; p < K1 + K2 + K3; p += blockDim.x) {
-    const int m = p < K1 ? 0 : (p < K1 + K2 ? 1 : 2);
-    const int q = p - (m == 0 ? 0 : (m == 1 ? K1 : K1 + K2));
-    const int K = m == 0 ? K1 : (m == 1 ? K2 : K3);
-    double sn, cs;
-    sincospi(2.0 * (double)q / (double)K, &sn, &cs);
-    tw1[p] = make_float2((float)cs, (float)-sn);
-  }
-  const float4* sites = tgt_raw + (size_t)(base + b) * s;
-  for (int t = tid; t < s; t += blockDim.x) {
-    float w[3][kMaxOrder];
-    int gi[3];
-    site_spline(a, sites[t], w, gi);
-    for (int m = 0; m < 3; ++m) {
-      for (int c = 0; c < n; ++c) sw[((size_t)t * 3 + m) * kMaxOrder + c] = w[m][c];
-      sg[(size_t)t * 3 + m] = (float)gi[m];
-    }
-  }
-  __syncthreads();
-  // 1-D transforms of every site's stencil (B1 carries the charge)
-  const int per = Kh1 + K2 + slab;
-  for (int x = tid; x < s * per; x += blockDim.x) {
-    const int t = x / per, r = x - t * per;
-    int m, k, K;
-    float2* dst;
-    const float2* tw;
-    if (r < Kh1) { m = 0; k = r; K = K1; dst = B1 + (size_t)t * Kh1 + k; tw = tw1; }
-    else if (r < Kh1 + K2) { m = 1; k = r - Kh1; K = K2; dst = B2 + (size_t)t * K2 + k; tw = tw2; }
-    else { m = 2; k = k30 + r - Kh1 - K2; K = K3; dst = B3 + (size_t)t * slab + (r - Kh1 - K2); tw = tw3; }
-    const int g = (int)sg[(size_t)t * 3 + m];
-    float re = 0.f, im = 0.f;
-    for (int c = 0; c < n; ++c) {
-      int gc = g - c;
-      gc = gc < 0 ? gc + K : (gc >= K ? gc - K : gc);
-      const int p = (k * gc) % K;
-      const float wc = sw[((size_t)t * 3 + m) * kMaxOrder + c];
-      re += wc * tw[p].x;
-      im += wc * tw[p].y;
-    }
-    if (m == 0) { const float q = sites[t].w; re *= q; im *= q; }
-    *dst = make_float2(re, im);
-  }
-  __syncthreads();
-  // one (k2, k3) row of Kh1 modes per thread
-  const int k2 = tid % K2, k3l = tid / K2, k3 = k30 + k3l;
-  float2 acc[kDirMaxKh1];
-#pragma unroll
-  for (int k1 = 0; k1 < kDirMaxKh1; ++k1) acc[k1] = make_float2(0.f, 0.f);
-  for (int t = 0; t < s; ++t) {
-    const float2 u = B2[(size_t)t * K2 + k2], v = B3[(size_t)t * slab + k3l];
-    const float2 c23 = make_float2(u.x * v.x - u.y * v.y, u.x * v.y + u.y * v.x);
-    const float2* b1 = B1 + (size_t)t * Kh1;
-#pragma unroll
-    for (int k1 = 0; k1 < kDirMaxKh1; ++k1)
-      if (k1 < Kh1) {
-        const float2 w1 = b1[k1];
-        acc[k1].x += w1.x * c23.x - w1.y * c23.y;
-        acc[k1].y += w1.x * c23.y + w1.y * c23.x;
-      }
-  }
-  // influence function, self energy, staged row
-  const int even = (K1 % 2) == 0;
-  const size_t row0 = ((size_t)k3 * K2 + k2) * Kh1;
-  double self = 0.0;
-#pragma unroll
-  for (int k1 = 0; k1 < kDirMaxKh1; ++k1)
-    if (k1 < Kh1) {
-      const float e = engfac[row0 + k1];
-      const double wgt = (k1 == 0 || (even && k1 == Kh1 - 1)) ? 0.5 : 1.0;
-      self += wgt * (double)e * ((double)acc[k1].x * acc[k1].x + (double)acc[k1].y * acc[k1].y);
-      outs[(size_t)tid * Kh1 + k1] = make_float2(acc[k1].x * e, acc[k1].y * e);
-    }
-  __syncthreads();
-  // rows tid = k3l*K2 + k2 are consecutive in spec: one contiguous block of kDirThreads*Kh1 modes
-  float2* dst = spec + (size_t)b * K3 * K2 * Kh1 + (size_t)k30 * K2 * Kh1;
-  for (int x = tid; x < kDirThreads * Kh1; x += blockDim.x) dst[x] = outs[x];
-  // deterministic self-energy reduction over the slabs of this target
-  __shared__ double red[32];
-  __shared__ bool last;
-  self = warp_sum(self);
-  if ((tid & 31) == 0) red[tid >> 5] = self;
-  __syncthreads();
-  if (tid < 32) {
-    double v = tid < (blockDim.x >> 5) ? red[tid] : 0.0;
-    v = warp_sum(v);
-    if (tid == 0) {
-      partial[(size_t)b * gridDim.x + blockIdx.x] = v;
-      __threadfence();
-      last = atomicAdd(&done[b], 1u) == gridDim.x - 1;
-    }
-  }
-  __syncthreads();
-  if (last && tid == 0) {
-    __threadfence();
-    double sum = 0.0;
-    const volatile double* pp = partial + (size_t)b * gridDim.x;
-    for (int i = 0; i < (int)gridDim.x; ++i) sum += pp[i];
-    selfrec[base + b] = sum;
-    done[b] = 0u;
-  }
-}
-
-int setup_direct(const FrameArgs& a) {
-  if (!direct_supported(a)) return -1;
-  return cudaFuncSetAttribute(k_spectrum_direct, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)direct_smem_bytes(a)) == cudaSuccess ? 0 : -1;
-}
-
-void launch_spectrum_direct(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
-  const int slab = kDirThreads / a.K2;
-  k_spectrum_direct<<<dim3(a.K3 / slab, chunk), kDirThreads, direct_smem_bytes(a), s>>>(
-      a, base, nb, d.tgt_raw, d.engfac, d.spec, d.partial, d.done, d.selfrec);
 }
 
 // ---------------------------------------------------------------------------

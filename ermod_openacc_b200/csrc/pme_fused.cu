@@ -1,0 +1,504 @@
+// pme_fused.cu -- the PME solve of a chunk of 32 targets without cuFFT and
+// without a spread grid in HBM, for power-of-two meshes of 16..128 points a
+// side.
+//
+// recpcal's per-insertion work (recpcal.F90:380-497 spreading, forward FFT,
+// influence multiply, self energy; :592-710 the inverse FFT the gather reads)
+// is, for a grid of K3 x K2 x K1 points and the half spectrum k1 < K1/2+1:
+//
+//   k_pme_plane     CTA = (target, k1 plane).  Forms the B-spline stencils of
+//                   the solute sites (recpcal.F90:553-574) and their 1-D
+//                   transforms B_m(k) = sum_c w_mc exp(-2 pi i k (g_m - c) / K_m)
+//                   in FP64, builds the plane of the solute spectrum
+//                   Qhat(k1, k2, k3) -- either directly,
+//                   sum_a q_a B1_a(k1) B2_a(k2) B3_a(k3), or by spreading
+//                   q_a B1_a(k1) w2 w3 on the (n2, n3) plane and a forward 2-D
+//                   FFT -- multiplies by the influence function, adds the
+//                   plane's share of the FP64 self energy, and runs the
+//                   inverse 2-D FFT over (k2, k3) in shared memory.  The plane
+//                   Y[b][k1][n3][n2] is written once (it stays in L2 for the
+//                   next kernel).
+//   k_pme_rows      CTA = (n3, group of n2 rows), all 32 targets: the
+//                   complex-to-real transform along k1 (a half-length
+//                   complex FFT of the Hermitian-packed row), written
+//                   straight into the insertion-fastest potential layout
+//                   phi[(n3*K2 + n2)*K1 + n1][32] that the gather reads.
+//
+// The FFTs are radix-8/4/2 Stockham stages (Govindaraju et al., "High
+// performance discrete Fourier transforms on graphics processors", SC08):
+// every thread holds its butterflies in registers across one barrier, so a
+// stage runs in place in shared memory.  Twiddle tables are FP64 values
+// rounded to FP32.  All sums run in a fixed order, so results are bitwise
+// reproducible.  The result equals spreading + R2C + influence + C2R of the
+// cuFFT path up to FP32 rounding.
+#include <cmath>
+
+#include "engine.cuh"
+
+namespace erm {
+
+namespace {
+
+constexpr float kRsqrt2 = 0.70710678118654752f;
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// a * (+i) for the inverse direction, a * (-i) for the forward one
+template <bool INV>
+__device__ __forceinline__ float2 rot90(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft2(float2& a, float2& b) {
+  const float2 t = a;
+  a = cadd(t, b);
+  b = csub(t, b);
+}
+
+// X[q] = sum_r v[r] w^(rq), w = exp(-+2 pi i / 4)
+template <bool INV>
+__device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2& v3) {
+  const float2 a0 = cadd(v0, v2), a1 = csub(v0, v2);
+  const float2 b0 = cadd(v1, v3), b1 = rot90<INV>(csub(v1, v3));
+  v0 = cadd(a0, b0);
+  v2 = csub(a0, b0);
+  v1 = cadd(a1, b1);
+  v3 = csub(a1, b1);
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2 (&v)[R]) {
+  if constexpr (R == 2) {
+    dft2<INV>(v[0], v[1]);
+  } else if constexpr (R == 4) {
+    dft4<INV>(v[0], v[1], v[2], v[3]);
+  } else {
+    // radix 8 as two radix-4 transforms of the even and odd inputs
+    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
+    // o_q *= w8^q, w8 = exp(-+2 pi i / 8)
+    const float s = INV ? 1.f : -1.f;
+    o1 = make_float2((o1.x - s * o1.y) * kRsqrt2, (o1.y + s * o1.x) * kRsqrt2);
+    o2 = rot90<INV>(o2);
+    o3 = make_float2((-o3.x - s * o3.y) * kRsqrt2, (-o3.y + s * o3.x) * kRsqrt2);
+    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+  }
+}
+
+// Placement of the transforms of one batched FFT in shared memory.
+// Transform bt starts at (bt >> lbg) * bpitch + (bt & (2^lbg - 1)) * bstride;
+// its elements are es apart.  Transforms: 2^lnb, length 2^ln.
+struct FftMap {
+  int ln, lnb, lbg, bpitch, bstride, es;
+};
+
+// One radix-R Stockham stage of every transform of the batch, in place.
+// tw[m] = exp(-2 pi i m / N) (FP32 of an FP64 value).
+template <int R, int BPT, bool INV>
+__device__ __forceinline__ void fft_stage(float2* buf, const FftMap& f, int lns, const float2* __restrict__ tw,
+                                          int tid, int nthr) {
+  float2 v[BPT][R];
+  int dst[BPT];
+  const int N = 1 << f.ln, NR = N / R, Ns = 1 << lns;
+  const int tstep = N / (Ns * R);
+  const int nbm = (1 << f.lnb) - 1, bgm = (1 << f.lbg) - 1;
+#pragma unroll
+  for (int i = 0; i < BPT; ++i) {
+    const int idx = tid + i * nthr;
+    const int bt = idx & nbm, j = idx >> f.lnb;
+    const int off = (bt >> f.lbg) * f.bpitch + (bt & bgm) * f.bstride;
+    const int k = j & (Ns - 1);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      float2 x = buf[off + (j + r * NR) * f.es];
+      if (r > 0) {
+        float2 w = tw[k * r * tstep];
+        if (INV) w.y = -w.y;
+        x = cmul(x, w);
+      }
+      v[i][r] = x;
+    }
+    dft<R, INV>(v[i]);
+    dst[i] = off + ((j - k) * R + k) * f.es;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < BPT; ++i)
+#pragma unroll
+    for (int r = 0; r < R; ++r) buf[dst[i] + r * Ns * f.es] = v[i][r];
+  __syncthreads();
+}
+
+// Every transform of the batch, E elements per thread (E * nthr = 2^(ln+lnb)).
+template <int E, bool INV>
+__device__ void fft_batch(float2* buf, const FftMap& f, const float2* __restrict__ tw, int tid, int nthr) {
+  int lns = 0;
+  while (lns < f.ln) {
+    const int rem = f.ln - lns;
+    if (rem >= 3) {
+      fft_stage<8, E / 8, INV>(buf, f, lns, tw, tid, nthr);
+      lns += 3;
+    } else if (rem == 2) {
+      fft_stage<4, E / 4, INV>(buf, f, lns, tw, tid, nthr);
+      lns += 2;
+    } else {
+      fft_stage<2, E / 2, INV>(buf, f, lns, tw, tid, nthr);
+      lns += 1;
+    }
+  }
+}
+
+__device__ __forceinline__ int ilog2(int x) { return 31 - __clz(x); }
+
+constexpr int kSiteTile = 32;                  // solute sites staged in shared memory at a time
+constexpr int kRowThreads = 512;
+constexpr int kRowElems = 16;                  // complex values per thread in k_pme_rows
+constexpr int kLoadBatch = 8;                  // global loads a thread keeps in flight while staging
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// k_pme_plane<E, DIRECT>: grid (Kh1, targets), K2*K3/E threads, E plane
+// points per thread.  Per tile of solute sites: the stencils (thread per site
+// and axis), then the stencil transforms the plane needs, summed in FP64 from
+// an FP64 twiddle table -- B1_a(k1) only for plane spreading, B1_a(k1),
+// B2_a(all k2), B3_a(all k3) for the direct sums.
+// ---------------------------------------------------------------------------
+template <int E, bool DIRECT>
+__global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_plane(FrameArgs a, int base,
+    const float4* __restrict__ tgt_raw, const float* __restrict__ engfacT, const float2* __restrict__ fft_tw,
+    const double2* __restrict__ fft_twd, float2* __restrict__ Y, double* __restrict__ partial,
+    unsigned int* __restrict__ done, double* __restrict__ selfrec) {
+  extern __shared__ __align__(16) unsigned char psm[];
+  const int k1 = blockIdx.x, b = blockIdx.y;
+  const int K1 = a.K1, K2 = a.K2, K3 = a.K3, Kh1 = a.Kh1, s = a.nsite, n = a.order;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int pitch = K2 + 1;
+  const int ntw = DIRECT ? K1 + K2 + K3 : K1;
+  double2* twd = (double2*)psm;                        // [ntw]  exp(-2 pi i m / K), FP64
+  float2* tw2 = (float2*)(twd + ntw);                  // [K2]
+  float2* tw3 = tw2 + K2;                              // [K3]
+  float2* plane = tw3 + K3;                            // [K3][pitch]
+  float2* c1 = plane + (size_t)K3 * pitch;             // [kSiteTile] q_a B1_a(k1)
+  float2* b2 = c1 + kSiteTile;                         // DIRECT: [kSiteTile][K2]
+  float2* b3 = b2 + (DIRECT ? kSiteTile * K2 : 0);     // DIRECT: [kSiteTile][K3]
+  float* sw = (float*)(b3 + (DIRECT ? kSiteTile * K3 : 0));   // [kSiteTile][3][kMaxOrder] stencil weights
+  int* sg = (int*)(sw + kSiteTile * 3 * kMaxOrder);    // [kSiteTile][3] stencil origins
+  float* sq = (float*)(sg + kSiteTile * 3);            // [kSiteTile] charges
+  for (int p = tid; p < ntw; p += nthr) twd[p] = fft_twd[p];
+  for (int p = tid; p < K2 + K3; p += nthr) tw2[p] = fft_tw[K1 + p];
+  const float4* sites = tgt_raw + (size_t)(base + b) * s;
+  // ownership: thread tid holds plane points (k3 = k3b + e * k3s, k2)
+  const int k2 = tid & (K2 - 1), k3b = tid / K2, k3s = nthr / K2;
+  float2 acc[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
+  for (int a0 = 0; a0 < s; a0 += kSiteTile) {
+    const int nt = min(kSiteTile, s - a0);
+    __syncthreads();
+    // stencils (calc_spline_molecule, recpcal.F90:553-574)
+    for (int x = tid; x < nt * 3; x += nthr) {
+      const int t = x / 3, m = x - 3 * t;
+      const float4 r = sites[a0 + t];
+      const int K = m == 0 ? K1 : (m == 1 ? K2 : K3);
+      float f = a.g.invcl[m][0] * r.x + a.g.invcl[m][1] * r.y + a.g.invcl[m][2] * r.z;
+      f = f - floorf(f);
+      f = f * (float)K;
+      const int rci = (int)f;
+      float w[kMaxOrder];
+      spline_weights(f - (float)rci, n, w);
+      for (int c = 0; c < n; ++c) sw[x * kMaxOrder + c] = w[c];
+      sg[x] = rci & (K - 1);
+      if (m == 0) sq[t] = r.w;
+    }
+    __syncthreads();
+    // stencil transforms B_m(k) = sum_c w_c exp(-2 pi i k (g - c) / K_m), FP64
+    const int per = DIRECT ? 1 + K2 + K3 : 1;
+    for (int x = tid; x < nt * per; x += nthr) {
+      const int t = x / per, r = x - t * per;
+      int m, k, K, t0;
+      if (r == 0) { m = 0; k = k1; K = K1; t0 = 0; }
+      else if (r <= K2) { m = 1; k = r - 1; K = K2; t0 = K1; }
+      else { m = 2; k = r - 1 - K2; K = K3; t0 = K1 + K2; }
+      const int g = sg[t * 3 + m];
+      const float* wc = sw + (t * 3 + m) * kMaxOrder;
+      double re = 0.0, im = 0.0;
+      for (int c = 0; c < n; ++c) {
+        const double2 e = twd[t0 + ((k * ((g - c) & (K - 1))) & (K - 1))];
+        re += (double)wc[c] * e.x;
+        im += (double)wc[c] * e.y;
+      }
+      if (m == 0) {
+        const double q = (double)sq[t];
+        c1[t] = make_float2((float)(re * q), (float)(im * q));
+      } else if (m == 1) {
+        b2[t * K2 + k] = make_float2((float)re, (float)im);
+      } else {
+        b3[t * K3 + k] = make_float2((float)re, (float)im);
+      }
+    }
+    __syncthreads();
+    if (DIRECT) {
+      for (int t = 0; t < nt; ++t) {
+        const float2 c = cmul(c1[t], b2[t * K2 + k2]);
+        const float2* bt = b3 + t * K3 + k3b;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const float2 u = bt[e * k3s];
+          acc[e].x += c.x * u.x - c.y * u.y;
+          acc[e].y += c.x * u.y + c.y * u.x;
+        }
+      }
+    } else {
+      // q_a B1_a(k1) w2 w3 on the (n2, n3) plane, accumulated in site order by the point's owner
+      for (int t = 0; t < nt; ++t) {
+        const int c2 = (sg[t * 3 + 1] - k2) & (K2 - 1);
+        if (c2 >= n) continue;
+        const float2 c = c1[t];
+        const float w2 = sw[(t * 3 + 1) * kMaxOrder + c2];
+        const float2 f = make_float2(c.x * w2, c.y * w2);
+        const int g3 = sg[t * 3 + 2];
+        const float* w3 = sw + (t * 3 + 2) * kMaxOrder;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int c3 = (g3 - (k3b + e * k3s)) & (K3 - 1);
+          if (c3 < n) {
+            acc[e].x += f.x * w3[c3];
+            acc[e].y += f.y * w3[c3];
+          }
+        }
+      }
+    }
+  }
+  // (DIRECT) acc holds Qhat(k1, k2, k3); otherwise the k1-transformed plane, still in (n2, n3)
+  const FftMap rows{ilog2(K2), ilog2(K3), 30, 0, pitch, 1};
+  const FftMap cols{ilog2(K3), ilog2(K2), 30, 0, 1, pitch};
+  if (!DIRECT) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) plane[(k3b + e * k3s) * pitch + k2] = acc[e];
+    __syncthreads();
+    fft_batch<E, false>(plane, rows, tw2, tid, nthr);
+    fft_batch<E, false>(plane, cols, tw3, tid, nthr);
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[e] = plane[(k3b + e * k3s) * pitch + k2];
+  }
+  // influence function and the plane's share of the self energy (recpcal.F90:482-497)
+  double self = 0.0;
+  const float* gk = engfacT + (size_t)k1 * K3 * K2;
+  float g[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) g[e] = gk[(k3b + e * k3s) * K2 + k2];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    self += (double)g[e] * ((double)acc[e].x * acc[e].x + (double)acc[e].y * acc[e].y);
+    plane[(k3b + e * k3s) * pitch + k2] = make_float2(acc[e].x * g[e], acc[e].y * g[e]);
+  }
+  if (k1 == 0 || 2 * k1 == K1) self *= 0.5;
+  __syncthreads();
+  fft_batch<E, true>(plane, rows, tw2, tid, nthr);
+  fft_batch<E, true>(plane, cols, tw3, tid, nthr);
+  float2* y = Y + ((size_t)b * Kh1 + k1) * K3 * K2;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int p = tid + e * nthr;
+    y[p] = plane[(p / K2) * pitch + (p & (K2 - 1))];
+  }
+  // deterministic self-energy reduction over the planes of this target
+  __shared__ double red[32];
+  __shared__ bool last;
+  self = warp_sum(self);
+  if ((tid & 31) == 0) red[tid >> 5] = self;
+  __syncthreads();
+  if (tid < 32) {
+    double v = tid < (nthr >> 5) ? red[tid] : 0.0;
+    v = warp_sum(v);
+    if (tid == 0) {
+      partial[(size_t)b * Kh1 + k1] = v;
+      __threadfence();
+      last = atomicAdd(&done[b], 1u) == (unsigned)Kh1 - 1;
+    }
+  }
+  __syncthreads();
+  if (last && tid == 0) {
+    __threadfence();
+    double sum = 0.0;
+    const volatile double* pp = partial + (size_t)b * Kh1;
+    for (int i = 0; i < Kh1; ++i) sum += pp[i];
+    selfrec[base + b] = sum;
+    done[b] = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_pme_rows: grid (K3, K2 / G2), kRowThreads threads, G2 = 256 / M rows of
+// n2 for all 32 targets; M = K1 / 2.  Shared rows k1 = 0..M hold
+// Y[b][k1][n3][n2] at column (n2 - n2g) * 33 + b.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb, const float2* __restrict__ Y,
+    const float2* __restrict__ fft_tw, float* __restrict__ phi) {
+  extern __shared__ __align__(16) unsigned char rsm[];
+  const int K1 = a.K1, K2 = a.K2, K3 = a.K3, Kh1 = a.Kh1, M = K1 / 2;
+  const int G2 = 256 / M, T = 32 * G2, TP = G2 * 33;
+  const int n3 = blockIdx.x, n2g = blockIdx.y * G2;
+  const int tid = threadIdx.x;
+  float2* twk = (float2*)rsm;          // [K1] exp(-2 pi i m / K1)
+  float2* twm = twk + K1;              // [M]  exp(-2 pi i m / M)
+  float2* S = twm + M;                 // [Kh1][TP]
+  for (int p = tid; p < K1; p += kRowThreads) twk[p] = fft_tw[p];
+  for (int p = tid; p < M; p += kRowThreads) twm[p] = fft_tw[K1 + K2 + K3 + p];
+  // stage Y with kLoadBatch independent loads in flight per thread
+  const int total = T * Kh1;
+  for (int x0 = 0; x0 < total; x0 += kLoadBatch * kRowThreads) {
+    float2 v[kLoadBatch];
+    int dst[kLoadBatch];
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; ++u) {
+      const int x = x0 + u * kRowThreads + tid;
+      dst[u] = -1;
+      v[u] = make_float2(0.f, 0.f);
+      if (x < total) {
+        const int j = x & (G2 - 1), r = x / G2;
+        const int k1 = r % Kh1, b = r / Kh1;
+        dst[u] = k1 * TP + j * 33 + b;
+        if (b < nb) v[u] = Y[(((size_t)b * Kh1 + k1) * K3 + n3) * K2 + n2g + j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; ++u)
+      if (dst[u] >= 0) S[dst[u]] = v[u];
+  }
+  __syncthreads();
+  // Hermitian packing into a length-M complex sequence Z (rows 0..M-1):
+  //   Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) exp(+2 pi i k / K1)
+  // so that x[2n] = Re z[n], x[2n+1] = Im z[n] for z = inverse DFT_M(Z).
+  for (int x = tid; x < T * (M / 2 + 1); x += kRowThreads) {
+    const int t = x & (T - 1), k = x / T;
+    const int c = (t >> 5) * 33 + (t & 31);
+    float2 xk = S[k * TP + c], xm = S[(M - k) * TP + c];
+    if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
+    {
+      const float2 cm = make_float2(xm.x, -xm.y);
+      const float2 w = make_float2(twk[k].x, -twk[k].y);
+      const float2 d = cmul(csub(xk, cm), w);
+      S[k * TP + c] = make_float2(xk.x + cm.x - d.y, xk.y + cm.y + d.x);
+    }
+    if (k != 0 && 2 * k != M) {
+      const float2 ck = make_float2(xk.x, -xk.y);
+      const float2 w = make_float2(twk[M - k].x, -twk[M - k].y);
+      const float2 d = cmul(csub(xm, ck), w);
+      S[(M - k) * TP + c] = make_float2(xm.x + ck.x - d.y, xm.y + ck.y + d.x);
+    }
+  }
+  __syncthreads();
+  const FftMap f{ilog2(M), ilog2(T), 5, 33, 1, TP};
+  fft_batch<kRowElems, true>(S, f, twm, tid, kRowThreads);
+  // phi[p][b], p = (n3 K2 + n2) K1 + n1, two n1 per complex value
+  float* out = phi + ((size_t)n3 * K2 + n2g) * K1 * 32;
+  for (int x = tid; x < T * M; x += kRowThreads) {
+    const int b = x & 31, r = x >> 5;
+    const int n = r & (M - 1), j = r / M;
+    const float2 z = S[n * TP + j * 33 + b];
+    float* o = out + ((size_t)j * K1 + 2 * n) * 32 + b;
+    o[0] = z.x;
+    o[32] = z.y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+bool pow2_in(int k, int lo, int hi) { return k >= lo && k <= hi && (k & (k - 1)) == 0; }
+
+int plane_elems(const FrameArgs& a) { return a.K2 * a.K3 <= 4096 ? 16 : 32; }
+
+size_t plane_smem(const FrameArgs& a, bool direct) {
+  const size_t ntw = direct ? a.K1 + a.K2 + a.K3 : a.K1;
+  return sizeof(double2) * ntw + sizeof(float2) * (size_t)(a.K2 + a.K3) + sizeof(float2) * (size_t)a.K3 * (a.K2 + 1) +
+         sizeof(float2) * kSiteTile * (1 + (direct ? a.K2 + a.K3 : 0)) +
+         sizeof(float) * kSiteTile * (3 * kMaxOrder + 3 + 1);
+}
+
+size_t rows_smem(const FrameArgs& a) {
+  const int M = a.K1 / 2, G2 = 256 / M;
+  return sizeof(float2) * (size_t)(a.K1 + M) + sizeof(float2) * (size_t)a.Kh1 * G2 * 33;
+}
+
+template <int E, bool D>
+cudaError_t plane_attr(const FrameArgs& a) {
+  return cudaFuncSetAttribute(k_pme_plane<E, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem(a, D));
+}
+}  // namespace
+
+bool fused_supported(const FrameArgs& a) {
+  if (!a.pme) return false;
+  if (!pow2_in(a.K1, 16, 128) || !pow2_in(a.K2, 16, 128) || !pow2_in(a.K3, 16, 128)) return false;
+  const int M = a.K1 / 2, G2 = 256 / M;
+  if (G2 > a.K2) return false;                       // one CTA of k_pme_rows spans G2 rows of n2
+  if (a.K2 * a.K3 < 512) return false;               // at least 32 threads per plane
+  const int E = plane_elems(a);
+  if (a.K3 < E) return false;                        // ownership map needs K2 | threads
+  return plane_smem(a, true) <= 220 * 1024 && rows_smem(a) <= 220 * 1024;
+}
+
+int setup_fused(const FrameArgs& a) {
+  if (!fused_supported(a)) return -1;
+  cudaError_t e = cudaSuccess;
+  if (plane_elems(a) == 16) {
+    if (e == cudaSuccess) e = plane_attr<16, true>(a);
+    if (e == cudaSuccess) e = plane_attr<16, false>(a);
+  } else {
+    if (e == cudaSuccess) e = plane_attr<32, true>(a);
+    if (e == cudaSuccess) e = plane_attr<32, false>(a);
+  }
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_pme_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem(a));
+  return e == cudaSuccess ? 0 : -1;
+}
+
+void fused_twiddles(int K1, int K2, int K3, std::vector<float2>& tw, std::vector<double2>& twd) {
+  // tw:  [K1 | K2 | K3 | K1/2] tables of exp(-2 pi i m / N), FP64 rounded to FP32
+  // twd: [K1 | K2 | K3] the same in FP64
+  tw.clear();
+  twd.clear();
+  const int Ns[4] = {K1, K2, K3, K1 / 2};
+  for (int t = 0; t < 4; ++t)
+    for (int m = 0; m < Ns[t]; ++m) {
+      const double ang = 2.0 * kPi * (double)m / (double)Ns[t];
+      const double c = std::cos(ang), sn = -std::sin(ang);
+      tw.push_back(make_float2((float)c, (float)sn));
+      if (t < 3) twd.push_back(make_double2(c, sn));
+    }
+}
+
+void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int nb, bool direct, cudaStream_t s) {
+  const int E = plane_elems(a);
+  const int nthr = a.K2 * a.K3 / E;
+  const dim3 grid(a.Kh1, nb);
+  const size_t sm = plane_smem(a, direct);
+#define ERM_PLANE(EE, DD)                                                                                 \
+  k_pme_plane<EE, DD><<<grid, nthr, sm, s>>>(a, base, d.tgt_raw, d.engfacT, d.fft_tw, d.fft_twd, d.spec, \
+                                             d.partial, d.done, d.selfrec)
+  if (E == 16) {
+    if (direct) ERM_PLANE(16, true); else ERM_PLANE(16, false);
+  } else {
+    if (direct) ERM_PLANE(32, true); else ERM_PLANE(32, false);
+  }
+#undef ERM_PLANE
+}
+
+void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int nb, cudaStream_t s) {
+  const int G2 = 256 / (a.K1 / 2);
+  k_pme_rows<<<dim3(a.K3, a.K2 / G2), kRowThreads, rows_smem(a), s>>>(a, nb, d.spec, d.fft_tw, d.phi);
+}
+
+}  // namespace erm

@@ -155,7 +155,7 @@ class Engine:
         return o, w
 
     STAGES = ["total", "prepare", "insert", "real", "spread", "r2c", "influence", "c2r", "gather", "bin",
-              "weights_edens", "ecorr", "chunks", "transpose", "spectrum"]
+              "weights_edens", "ecorr", "chunks", "transpose", "pme_plane", "pme_rows"]
 
     def timings(self):
         """Device milliseconds per stage of the last engconst (CUDA events on the engine stream)."""
@@ -165,3 +165,9 @@ class Engine:
 
     def launch_count(self) -> int:
         return int(self.lib.ermod_get_launch_count(self.ctx))
+
+    def paths(self) -> dict:
+        """Resolved kernel choices: spectrum_path 1 cuFFT / 2 fused direct / 3 fused spread, ecorr_path."""
+        sp, ep = C.c_int32(), C.c_int32()
+        self._check(self.lib.ermod_get_paths(self.ctx, C.byref(sp), C.byref(ep)))
+        return dict(spectrum_path=sp.value, ecorr_path=ep.value)

@@ -258,7 +258,9 @@ def default_params(**kw) -> dict:
              ins_chunk=0, ecorr_batch=0, weight_bits=0, proposal=A.PROPOSAL_UNIFORM,
              keep_uvengy=0, ecorr_path=0, spectrum_path=0)
     p.update(kw)
-    p["ms2max"] = p["ms3max"] = p["ms1max"] if "ms2max" not in kw else p["ms2max"]
+    for k in ("ms2max", "ms3max"):
+        if k not in kw:
+            p[k] = p["ms1max"]
     return p
 
 

@@ -107,7 +107,10 @@ typedef struct ermod_params {
   int32_t proposal;               /* ERMOD_PROPOSAL_* */
   int32_t keep_uvengy;            /* 1: keep per-molecule energies for ermod_get_uvengy */
   int32_t ecorr_path;             /* 0: INT8 tensor-core GEMM, 1: FP64 CUDA-core kernel */
-  int32_t spectrum_path;          /* 0: by solute size, 1: spread + cuFFT R2C, 2: direct site sums */
+  int32_t spectrum_path;          /* PME solve. 0: automatic, 1: spread grid + cuFFT R2C/C2R,
+                                     2: fused solve, spectrum by direct site sums,
+                                     3: fused solve, spectrum by plane spreading + FFT
+                                     (2 and 3 need power-of-two meshes of 16..128) */
   int32_t reserved[5];
 } ermod_params;
 
@@ -258,8 +261,15 @@ const char* ermod_last_error(const ermod_ctx* ctx);
  * [4] PME spread, [5] FFT R2C, [6] influence multiply, [7] FFT C2R,
  * [8] PME gather, [9] binning, [10] weights + edens, [11] ecorr,
  * [12] number of PME target chunks, [13] potential-grid transpose,
- * [14] direct solute spectrum.  n <= 15. */
+ * [14] fused solve: stencil transforms, spectrum planes and 2-D FFTs,
+ * [15] fused solve: k1 transforms into the potential grids.  n <= 16. */
 int32_t ermod_get_timings(const ermod_ctx* ctx, float* ms, int32_t n);
+
+/* The PME solve the context runs (1..3 as ermod_params.spectrum_path, 0 when
+ * there is no reciprocal-space term) and the ecorr kernel (0 tensor-core
+ * GEMM, 1 FP64 kernel, -1 no ecorr); resolves the automatic choices (no
+ * reference counterpart). */
+int32_t ermod_get_paths(const ermod_ctx* ctx, int32_t* spectrum_path, int32_t* ecorr_path);
 
 /* Kernel launches of this library since the context was created, cuFFT's
  * own kernels excluded (no reference counterpart; profiling). */

@@ -81,9 +81,10 @@ def test_refs_ring_placement(lib, oracle_mod):
     assert np.all(wts == 1.0)
 
 
-@pytest.mark.parametrize("config,path", [(2, 1), (2, 2), (3, 1), (3, 2)])
+@pytest.mark.parametrize("config,path", [(2, 1), (2, 2), (2, 3), (3, 1), (3, 2), (3, 3)])
 def test_refs_energies_and_bins(lib, oracle_mod, config, path):
-    """spectrum path 1: fixed-point spreading + cuFFT R2C; 2: direct sums over the sites."""
+    """PME solve 1: fixed-point spreading + cuFFT; fused solve with the solute spectrum
+    from 2: direct sums over the sites, 3: plane spreading + forward FFT."""
     w = S.make_workload(config, small=True, maxins=96)
     prm = dict(w.params, keep_uvengy=1, spectrum_path=path)
     eng = Engine(prm, w.topo, w.hist)
@@ -195,7 +196,8 @@ def test_engstore_normalisation(lib):
     assert z["engnorm"] == 0 and not z["edens"].any() and not z["ecorr"].any()
 
 
-@pytest.mark.parametrize("K,order,path", [(32, 6, 1), (32, 4, 1), (32, 6, 2), (64, 8, 2)])
+@pytest.mark.parametrize("K,order,path", [(32, 6, 1), (32, 4, 1), (64, 8, 1), (32, 6, 2), (32, 6, 3), (64, 8, 2),
+                                           (64, 8, 3), (128, 4, 2), (32, 4, 3)])
 def test_madelung_gpu(lib, K, order, path):
     prm, topo, hist, pos, cell, ins, L = nacl_system(K=K, order=order)
     eng = Engine(dict(prm, keep_uvengy=1, spectrum_path=path), topo, hist)
@@ -286,13 +288,15 @@ def test_ecorr_tensor_core_counts_above_255(lib):
     np.testing.assert_array_equal(a["ecorr"], cnt.T @ cnt)
 
 
-def test_runs_are_bit_reproducible(lib):
+@pytest.mark.parametrize("path", [1, 2, 3])
+def test_runs_are_bit_reproducible(lib, path):
     """Two contexts fed the same frames produce bit-identical energies and accumulators:
-    spreading sums in fixed point and every FP64 reduction runs in a fixed order."""
+    spreading sums in fixed point or in a fixed site order, and every FP64 reduction
+    runs in a fixed order."""
     w = S.make_workload(2, small=True, maxins=128)
     res = []
     for _ in range(2):
-        eng = Engine(dict(w.params, keep_uvengy=1), w.topo, w.hist)
+        eng = Engine(dict(w.params, keep_uvengy=1, spectrum_path=path), w.topo, w.hist)
         for fr in range(2):
             pos, cell = w.frame(fr)
             eng.engconst(fr + 1, pos, cell)
@@ -306,3 +310,23 @@ def test_runs_are_bit_reproducible(lib):
         np.testing.assert_array_equal(a[k], b[k])
     for k in ("engnorm", "avslf", "engsmpl", "voffset"):
         assert a[k] == b[k]
+
+
+@pytest.mark.parametrize("mesh", [(32, 64, 16), (128, 32, 64), (16, 32, 32)])
+def test_fused_solve_matches_cufft_on_mixed_meshes(lib, mesh):
+    """The fused PME solve (both spectrum builds) against spreading + cuFFT on meshes
+    with a different size along every axis."""
+    w = S.make_workload(2, small=True, maxins=64)
+    prm = dict(w.params, keep_uvengy=1, ms1max=mesh[0], ms2max=mesh[1], ms3max=mesh[2])
+    pos, cell = w.frame(0)
+    out = {}
+    for path in (1, 2, 3):
+        eng = Engine(dict(prm, spectrum_path=path), w.topo, w.hist)
+        assert eng.engconst(1, pos, cell) >= 0
+        out[path] = eng.uvengy()
+        eng.close()
+    u1, u01 = out[1]
+    for path in (2, 3):
+        u, u0 = out[path]
+        check_energies(u, u1)
+        np.testing.assert_allclose(u0, u01, rtol=1e-6, atol=2e-5)
