@@ -694,7 +694,7 @@ void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb
 constexpr int kGatherThreads = 256;
 
 template <int NO>
-__global__ void __launch_bounds__(kGatherThreads) k_gather(FrameArgs a, int base, int bb, int nb, int chunk, int batch,
+__global__ void __launch_bounds__(kGatherThreads, 4) k_gather(FrameArgs a, int base, int bb, int nb, int chunk, int batch,
     const int* __restrict__ molsorted, const int* __restrict__ molbeg, const float* __restrict__ molq,
     const float* __restrict__ atom_q, const float* __restrict__ spl, const int4* __restrict__ grd,
     const float* __restrict__ phi, const double* __restrict__ Ereal, const double* __restrict__ tgtq,

@@ -24,7 +24,7 @@
 //                   straight into the insertion-fastest potential layout
 //                   phi[(n3*K2 + n2)*K1 + n1][32] that the gather reads.
 //
-// The FFTs are radix-8/4/2 Stockham stages (Govindaraju et al., "High
+// The FFTs are radix-8/4 Stockham stages (Govindaraju et al., "High
 // performance discrete Fourier transforms on graphics processors", SC08):
 // every thread holds its butterflies in registers across one barrier, so a
 // stage runs in place in shared memory.  Twiddle tables are FP64 values
@@ -52,13 +52,6 @@ __device__ __forceinline__ float2 rot90(float2 a) {
   return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
-template <bool INV>
-__device__ __forceinline__ void dft2(float2& a, float2& b) {
-  const float2 t = a;
-  a = cadd(t, b);
-  b = csub(t, b);
-}
-
 // X[q] = sum_r v[r] w^(rq), w = exp(-+2 pi i / 4)
 template <bool INV>
 __device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2& v3) {
@@ -72,9 +65,8 @@ __device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2&
 
 template <int R, bool INV>
 __device__ __forceinline__ void dft(float2 (&v)[R]) {
-  if constexpr (R == 2) {
-    dft2<INV>(v[0], v[1]);
-  } else if constexpr (R == 4) {
+  static_assert(R == 4 || R == 8, "radix 4 or 8");
+  if constexpr (R == 4) {
     dft4<INV>(v[0], v[1], v[2], v[3]);
   } else {
     // radix 8 as two radix-4 transforms of the even and odd inputs
@@ -108,8 +100,9 @@ __device__ __forceinline__ void fft_stage(float2* buf, const FftMap& f, int lns,
                                           int tid, int nthr) {
   float2 v[BPT][R];
   int dst[BPT];
-  const int N = 1 << f.ln, NR = N / R, Ns = 1 << lns;
-  const int tstep = N / (Ns * R);
+  constexpr int LR = R == 8 ? 3 : 2;
+  const int NR = 1 << (f.ln - LR), Ns = 1 << lns;
+  const int lts = f.ln - lns - LR;                 // twiddle index step 2^lts = N / (Ns R)
   const int nbm = (1 << f.lnb) - 1, bgm = (1 << f.lbg) - 1;
 #pragma unroll
   for (int i = 0; i < BPT; ++i) {
@@ -120,8 +113,8 @@ __device__ __forceinline__ void fft_stage(float2* buf, const FftMap& f, int lns,
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       float2 x = buf[off + (j + r * NR) * f.es];
-      if (r > 0) {
-        float2 w = tw[k * r * tstep];
+      if (r > 0 && lns > 0) {                      // the first stage has k = 0: unit twiddles
+        float2 w = tw[(k * r) << lts];
         if (INV) w.y = -w.y;
         x = cmul(x, w);
       }
@@ -138,21 +131,20 @@ __device__ __forceinline__ void fft_stage(float2* buf, const FftMap& f, int lns,
   __syncthreads();
 }
 
-// Every transform of the batch, E elements per thread (E * nthr = 2^(ln+lnb)).
+// Every transform of the batch, E elements per thread (E * nthr = 2^(ln+lnb)),
+// length 2^ln >= 4: radix-8 stages, radix-4 for the remaining factors
+// (2^4 = 4 * 4 rather than 8 * 2, so no radix-2 stage is ever needed).
 template <int E, bool INV>
 __device__ void fft_batch(float2* buf, const FftMap& f, const float2* __restrict__ tw, int tid, int nthr) {
   int lns = 0;
   while (lns < f.ln) {
     const int rem = f.ln - lns;
-    if (rem >= 3) {
+    if (rem >= 3 && rem != 4) {
       fft_stage<8, E / 8, INV>(buf, f, lns, tw, tid, nthr);
       lns += 3;
-    } else if (rem == 2) {
+    } else {
       fft_stage<4, E / 4, INV>(buf, f, lns, tw, tid, nthr);
       lns += 2;
-    } else {
-      fft_stage<2, E / 2, INV>(buf, f, lns, tw, tid, nthr);
-      lns += 1;
     }
   }
 }
@@ -198,7 +190,8 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
   for (int p = tid; p < K2 + K3; p += nthr) tw2[p] = fft_tw[K1 + p];
   const float4* sites = tgt_raw + (size_t)(base + b) * s;
   // ownership: thread tid holds plane points (k3 = k3b + e * k3s, k2)
-  const int k2 = tid & (K2 - 1), k3b = tid / K2, k3s = nthr / K2;
+  const int lk2 = ilog2(K2);
+  const int k2 = tid & (K2 - 1), k3b = tid >> lk2, k3s = nthr >> lk2;
   float2 acc[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
@@ -221,19 +214,27 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
       if (m == 0) sq[t] = r.w;
     }
     __syncthreads();
-    // stencil transforms B_m(k) = sum_c w_c exp(-2 pi i k (g - c) / K_m), FP64
-    const int per = DIRECT ? 1 + K2 + K3 : 1;
-    for (int x = tid; x < nt * per; x += nthr) {
-      const int t = x / per, r = x - t * per;
-      int m, k, K, t0;
-      if (r == 0) { m = 0; k = k1; K = K1; t0 = 0; }
-      else if (r <= K2) { m = 1; k = r - 1; K = K2; t0 = K1; }
-      else { m = 2; k = r - 1 - K2; K = K3; t0 = K1 + K2; }
+    // stencil transforms B_m(k) = sum_c w_c exp(-2 pi i k (g - c) / K_m), FP64:
+    // exp(-2 pi i k g / K) times powers of exp(+2 pi i k / K)
+    const int nent = DIRECT ? nt * (1 + K2 + K3) : nt;
+    for (int x = tid; x < nent; x += nthr) {
+      int t, m, k, lk, t0;
+      if (x < nt) { t = x; m = 0; k = k1; lk = ilog2(K1); t0 = 0; }
+      else if (x < nt + (nt << ilog2(K2))) {
+        const int y = x - nt;
+        lk = ilog2(K2); t = y >> lk; k = y & (K2 - 1); m = 1; t0 = K1;
+      } else {
+        const int y = x - nt - (nt << ilog2(K2));
+        lk = ilog2(K3); t = y >> lk; k = y & (K3 - 1); m = 2; t0 = K1 + K2;
+      }
+      const int K = 1 << lk;
       const int g = sg[t * 3 + m];
       const float* wc = sw + (t * 3 + m) * kMaxOrder;
-      double re = 0.0, im = 0.0;
-      for (int c = 0; c < n; ++c) {
-        const double2 e = twd[t0 + ((k * ((g - c) & (K - 1))) & (K - 1))];
+      double2 e = twd[t0 + ((k * g) & (K - 1))];
+      const double2 st = twd[t0 + ((K - k) & (K - 1))];   // exp(+2 pi i k / K)
+      double re = (double)wc[0] * e.x, im = (double)wc[0] * e.y;
+      for (int c = 1; c < n; ++c) {
+        e = make_double2(e.x * st.x - e.y * st.y, e.x * st.y + e.y * st.x);
         re += (double)wc[c] * e.x;
         im += (double)wc[c] * e.y;
       }
@@ -292,6 +293,7 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
     for (int e = 0; e < E; ++e) acc[e] = plane[(k3b + e * k3s) * pitch + k2];
   }
   // influence function and the plane's share of the self energy (recpcal.F90:482-497)
+  // (each mode's energy G |Qhat|^2 is formed in FP32, ~1e-7 relative, and summed in FP64)
   double self = 0.0;
   const float* gk = engfacT + (size_t)k1 * K3 * K2;
   float g[E];
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
   for (int e = 0; e < E; ++e) g[e] = gk[(k3b + e * k3s) * K2 + k2];
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    self += (double)g[e] * ((double)acc[e].x * acc[e].x + (double)acc[e].y * acc[e].y);
+    self += (double)(g[e] * (acc[e].x * acc[e].x + acc[e].y * acc[e].y));
     plane[(k3b + e * k3s) * pitch + k2] = make_float2(acc[e].x * g[e], acc[e].y * g[e]);
   }
   if (k1 == 0 || 2 * k1 == K1) self *= 0.5;
@@ -310,7 +312,7 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
 #pragma unroll
   for (int e = 0; e < E; ++e) {
     const int p = tid + e * nthr;
-    y[p] = plane[(p / K2) * pitch + (p & (K2 - 1))];
+    y[p] = plane[(p >> lk2) * pitch + (p & (K2 - 1))];
   }
   // deterministic self-energy reduction over the planes of this target
   __shared__ double red[32];
@@ -348,6 +350,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
   extern __shared__ __align__(16) unsigned char rsm[];
   const int K1 = a.K1, K2 = a.K2, K3 = a.K3, Kh1 = a.Kh1, M = K1 / 2;
   const int G2 = 256 / M, T = 32 * G2, TP = G2 * 33;
+  const int lg2 = ilog2(G2), lt = lg2 + 5, lm = ilog2(M);
   const int n3 = blockIdx.x, n2g = blockIdx.y * G2;
   const int tid = threadIdx.x;
   float2* twk = (float2*)rsm;          // [K1] exp(-2 pi i m / K1)
@@ -366,8 +369,8 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
       dst[u] = -1;
       v[u] = make_float2(0.f, 0.f);
       if (x < total) {
-        const int j = x & (G2 - 1), r = x / G2;
-        const int k1 = r % Kh1, b = r / Kh1;
+        const int j = x & (G2 - 1), r = x >> lg2;   // r = k1 * 32 + b
+        const int b = r & 31, k1 = r >> 5;
         dst[u] = k1 * TP + j * 33 + b;
         if (b < nb) v[u] = Y[(((size_t)b * Kh1 + k1) * K3 + n3) * K2 + n2g + j];
       }
@@ -381,7 +384,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
   //   Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) exp(+2 pi i k / K1)
   // so that x[2n] = Re z[n], x[2n+1] = Im z[n] for z = inverse DFT_M(Z).
   for (int x = tid; x < T * (M / 2 + 1); x += kRowThreads) {
-    const int t = x & (T - 1), k = x / T;
+    const int t = x & (T - 1), k = x >> lt;
     const int c = (t >> 5) * 33 + (t & 31);
     float2 xk = S[k * TP + c], xm = S[(M - k) * TP + c];
     if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
@@ -399,13 +402,13 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
     }
   }
   __syncthreads();
-  const FftMap f{ilog2(M), ilog2(T), 5, 33, 1, TP};
+  const FftMap f{lm, lt, 5, 33, 1, TP};
   fft_batch<kRowElems, true>(S, f, twm, tid, kRowThreads);
   // phi[p][b], p = (n3 K2 + n2) K1 + n1, two n1 per complex value
   float* out = phi + ((size_t)n3 * K2 + n2g) * K1 * 32;
   for (int x = tid; x < T * M; x += kRowThreads) {
     const int b = x & 31, r = x >> 5;
-    const int n = r & (M - 1), j = r / M;
+    const int n = r & (M - 1), j = r >> lm;
     const float2 z = S[n * TP + j * 33 + b];
     float* o = out + ((size_t)j * K1 + 2 * n) * 32 + b;
     o[0] = z.x;
