@@ -86,112 +86,123 @@ __device__ __forceinline__ void dft(float2 (&v)[R]) {
   }
 }
 
-// Placement of the transforms of one batched FFT in shared memory.
-// Transform bt starts at (bt >> lbg) * bpitch + (bt & (2^lbg - 1)) * bstride;
-// its elements are es apart.  Transforms: 2^lnb, length 2^ln.
-struct FftMap {
-  int ln, lnb, lbg, bpitch, bstride, es;
+// Placement of a batch of 2^LNB transforms of length 2^LN in shared memory:
+// transform bt starts at (bt >> LBG) * BPITCH + (bt & (2^LBG - 1)) * BSTRIDE
+// and its elements are ES apart.  Everything is a compile-time constant, so
+// shared-memory addresses are immediates off one register per butterfly.
+template <int LN_, int LNB_, int LBG_, int BPITCH_, int BSTRIDE_, int ES_>
+struct FftShape {
+  static constexpr int LN = LN_, LNB = LNB_, LBG = LBG_, BPITCH = BPITCH_, BSTRIDE = BSTRIDE_, ES = ES_;
 };
 
-// One radix-R Stockham stage of every transform of the batch, in place.
-// tw[m] = exp(-2 pi i m / N) (FP32 of an FP64 value).
-template <int R, int BPT, bool INV>
-__device__ __forceinline__ void fft_stage(float2* buf, const FftMap& f, int lns, const float2* __restrict__ tw,
-                                          int tid, int nthr) {
+// One radix-R Stockham stage (input stride N/R, output groups of Ns = 2^LNS)
+// of every transform of the batch, in place: each thread loads its
+// butterflies, the block synchronises, then stores.  tw[m] = exp(-2 pi i m / N).
+template <class S, int R, int LNS, int NTHR, bool INV>
+__device__ __forceinline__ void fft_stage(float2* buf, const float2* __restrict__ tw, int tid) {
+  constexpr int LR = R == 8 ? 3 : 2;
+  constexpr int NR = 1 << (S::LN - LR), NS = 1 << LNS, LTS = S::LN - LNS - LR;
+  constexpr int NBUT = (1 << (S::LN + S::LNB)) / R;
+  constexpr int BPT = NBUT / NTHR;
+  static_assert(BPT * NTHR == NBUT, "butterflies must divide evenly over the threads");
   float2 v[BPT][R];
   int dst[BPT];
-  constexpr int LR = R == 8 ? 3 : 2;
-  const int NR = 1 << (f.ln - LR), Ns = 1 << lns;
-  const int lts = f.ln - lns - LR;                 // twiddle index step 2^lts = N / (Ns R)
-  const int nbm = (1 << f.lnb) - 1, bgm = (1 << f.lbg) - 1;
 #pragma unroll
   for (int i = 0; i < BPT; ++i) {
-    const int idx = tid + i * nthr;
-    const int bt = idx & nbm, j = idx >> f.lnb;
-    const int off = (bt >> f.lbg) * f.bpitch + (bt & bgm) * f.bstride;
-    const int k = j & (Ns - 1);
+    const int idx = tid + i * NTHR;
+    const int bt = idx & ((1 << S::LNB) - 1), j = idx >> S::LNB;
+    const int off = (bt >> S::LBG) * S::BPITCH + (bt & ((1 << S::LBG) - 1)) * S::BSTRIDE;
+    const int k = j & (NS - 1);
+    const float2* src = buf + off + j * S::ES;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      float2 x = buf[off + (j + r * NR) * f.es];
-      if (r > 0 && lns > 0) {                      // the first stage has k = 0: unit twiddles
-        float2 w = tw[(k * r) << lts];
-        if (INV) w.y = -w.y;
-        x = cmul(x, w);
+      float2 x = src[r * NR * S::ES];
+      if (LNS > 0 && r > 0) {                      // the first stage has k = 0: unit twiddles
+        const float2 w = tw[(k * r) << LTS];
+        x = INV ? make_float2(x.x * w.x + x.y * w.y, x.y * w.x - x.x * w.y) : cmul(x, w);
       }
       v[i][r] = x;
     }
     dft<R, INV>(v[i]);
-    dst[i] = off + ((j - k) * R + k) * f.es;
+    dst[i] = off + ((j - k) * R + k) * S::ES;
   }
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < BPT; ++i)
 #pragma unroll
-    for (int r = 0; r < R; ++r) buf[dst[i] + r * Ns * f.es] = v[i][r];
+    for (int r = 0; r < R; ++r) buf[dst[i] + r * NS * S::ES] = v[i][r];
   __syncthreads();
 }
 
-// Every transform of the batch, E elements per thread (E * nthr = 2^(ln+lnb)),
-// length 2^ln >= 4: radix-8 stages, radix-4 for the remaining factors
-// (2^4 = 4 * 4 rather than 8 * 2, so no radix-2 stage is ever needed).
-template <int E, bool INV>
-__device__ void fft_batch(float2* buf, const FftMap& f, const float2* __restrict__ tw, int tid, int nthr) {
-  int lns = 0;
-  while (lns < f.ln) {
-    const int rem = f.ln - lns;
-    if (rem >= 3 && rem != 4) {
-      fft_stage<8, E / 8, INV>(buf, f, lns, tw, tid, nthr);
-      lns += 3;
-    } else {
-      fft_stage<4, E / 4, INV>(buf, f, lns, tw, tid, nthr);
-      lns += 2;
-    }
+// All stages of every transform of the batch: radix 8, radix 4 for the
+// remaining factors (2^4 = 4 * 4 rather than 8 * 2; lengths are >= 8).
+template <class S, int LNS, int NTHR, bool INV>
+__device__ __forceinline__ void fft_stages(float2* buf, const float2* __restrict__ tw, int tid) {
+  if constexpr (LNS < S::LN) {
+    constexpr int REM = S::LN - LNS;
+    constexpr int R = (REM >= 3 && REM != 4) ? 8 : 4;
+    fft_stage<S, R, LNS, NTHR, INV>(buf, tw, tid);
+    fft_stages<S, LNS + (R == 8 ? 3 : 2), NTHR, INV>(buf, tw, tid);
   }
+}
+
+template <class S, int NTHR, bool INV>
+__device__ __forceinline__ void fft_batch(float2* buf, const float2* __restrict__ tw, int tid) {
+  static_assert(S::LN >= 3, "transform length >= 8");
+  fft_stages<S, 0, NTHR, INV>(buf, tw, tid);
 }
 
 __device__ __forceinline__ int ilog2(int x) { return 31 - __clz(x); }
 
 constexpr int kSiteTile = 32;                  // solute sites staged in shared memory at a time
 constexpr int kRowThreads = 512;
-constexpr int kRowElems = 16;                  // complex values per thread in k_pme_rows
 constexpr int kLoadBatch = 8;                  // global loads a thread keeps in flight while staging
+
+template <int LK2, int LK3>
+struct PlaneCfg {
+  static constexpr int K2 = 1 << LK2, K3 = 1 << LK3, PITCH = K2 + 1;
+  static constexpr int E = LK2 + LK3 <= 12 ? 16 : 32;     // plane points per thread
+  static constexpr int NTHR = (K2 * K3) / E;
+  static constexpr int MINB = E == 16 ? 3 : 1;
+  static_assert(K3 % E == 0, "a thread owns E consecutive k3 of one k2 column");
+};
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// k_pme_plane<E, DIRECT>: grid (Kh1, targets), K2*K3/E threads, E plane
-// points per thread.  Per tile of solute sites: the stencils (thread per site
-// and axis), then the stencil transforms the plane needs, summed in FP64 from
-// an FP64 twiddle table -- B1_a(k1) only for plane spreading, B1_a(k1),
-// B2_a(all k2), B3_a(all k3) for the direct sums.
+// k_pme_plane<LK2, LK3, DIRECT>: grid (Kh1, targets), K2*K3/E threads.  Thread
+// tid owns the points (k2 = tid mod K2, k3 = (tid / K2) * E + e), e < E.  Per
+// tile of solute sites: the stencils (thread per site and axis), then the
+// stencil transforms the plane needs, summed in FP64 from an FP64 twiddle
+// table -- B1_a(k1) only for plane spreading, B1_a(k1), B2_a(all k2),
+// B3_a(all k3) for the direct sums.
 // ---------------------------------------------------------------------------
-template <int E, bool DIRECT>
-__global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_plane(FrameArgs a, int base,
-    const float4* __restrict__ tgt_raw, const float* __restrict__ engfacT, const float2* __restrict__ fft_tw,
+template <int LK2, int LK3, bool DIRECT>
+__global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::MINB) k_pme_plane(FrameArgs a,
+    int base, const float4* __restrict__ tgt_raw, const float* __restrict__ engfacT, const float2* __restrict__ fft_tw,
     const double2* __restrict__ fft_twd, float2* __restrict__ Y, double* __restrict__ partial,
     unsigned int* __restrict__ done, double* __restrict__ selfrec) {
+  using C = PlaneCfg<LK2, LK3>;
+  constexpr int K2 = C::K2, K3 = C::K3, PITCH = C::PITCH, E = C::E, NTHR = C::NTHR;
   extern __shared__ __align__(16) unsigned char psm[];
   const int k1 = blockIdx.x, b = blockIdx.y;
-  const int K1 = a.K1, K2 = a.K2, K3 = a.K3, Kh1 = a.Kh1, s = a.nsite, n = a.order;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const int pitch = K2 + 1;
+  const int K1 = a.K1, Kh1 = a.Kh1, s = a.nsite, n = a.order;
+  const int tid = threadIdx.x;
   const int ntw = DIRECT ? K1 + K2 + K3 : K1;
   double2* twd = (double2*)psm;                        // [ntw]  exp(-2 pi i m / K), FP64
   float2* tw2 = (float2*)(twd + ntw);                  // [K2]
   float2* tw3 = tw2 + K2;                              // [K3]
-  float2* plane = tw3 + K3;                            // [K3][pitch]
-  float2* c1 = plane + (size_t)K3 * pitch;             // [kSiteTile] q_a B1_a(k1)
+  float2* plane = tw3 + K3;                            // [K3][PITCH]
+  float2* c1 = plane + K3 * PITCH;                     // [kSiteTile] q_a B1_a(k1)
   float2* b2 = c1 + kSiteTile;                         // DIRECT: [kSiteTile][K2]
   float2* b3 = b2 + (DIRECT ? kSiteTile * K2 : 0);     // DIRECT: [kSiteTile][K3]
   float* sw = (float*)(b3 + (DIRECT ? kSiteTile * K3 : 0));   // [kSiteTile][3][kMaxOrder] stencil weights
   int* sg = (int*)(sw + kSiteTile * 3 * kMaxOrder);    // [kSiteTile][3] stencil origins
   float* sq = (float*)(sg + kSiteTile * 3);            // [kSiteTile] charges
-  for (int p = tid; p < ntw; p += nthr) twd[p] = fft_twd[p];
-  for (int p = tid; p < K2 + K3; p += nthr) tw2[p] = fft_tw[K1 + p];
+  for (int p = tid; p < ntw; p += NTHR) twd[p] = fft_twd[p];
+  for (int p = tid; p < K2 + K3; p += NTHR) tw2[p] = fft_tw[K1 + p];
   const float4* sites = tgt_raw + (size_t)(base + b) * s;
-  // ownership: thread tid holds plane points (k3 = k3b + e * k3s, k2)
-  const int lk2 = ilog2(K2);
-  const int k2 = tid & (K2 - 1), k3b = tid >> lk2, k3s = nthr >> lk2;
+  const int k2 = tid & (K2 - 1), k30 = (tid >> LK2) * E;
   float2 acc[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
@@ -199,7 +210,7 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
     const int nt = min(kSiteTile, s - a0);
     __syncthreads();
     // stencils (calc_spline_molecule, recpcal.F90:553-574)
-    for (int x = tid; x < nt * 3; x += nthr) {
+    for (int x = tid; x < nt * 3; x += NTHR) {
       const int t = x / 3, m = x - 3 * t;
       const float4 r = sites[a0 + t];
       const int K = m == 0 ? K1 : (m == 1 ? K2 : K3);
@@ -217,17 +228,11 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
     // stencil transforms B_m(k) = sum_c w_c exp(-2 pi i k (g - c) / K_m), FP64:
     // exp(-2 pi i k g / K) times powers of exp(+2 pi i k / K)
     const int nent = DIRECT ? nt * (1 + K2 + K3) : nt;
-    for (int x = tid; x < nent; x += nthr) {
-      int t, m, k, lk, t0;
-      if (x < nt) { t = x; m = 0; k = k1; lk = ilog2(K1); t0 = 0; }
-      else if (x < nt + (nt << ilog2(K2))) {
-        const int y = x - nt;
-        lk = ilog2(K2); t = y >> lk; k = y & (K2 - 1); m = 1; t0 = K1;
-      } else {
-        const int y = x - nt - (nt << ilog2(K2));
-        lk = ilog2(K3); t = y >> lk; k = y & (K3 - 1); m = 2; t0 = K1 + K2;
-      }
-      const int K = 1 << lk;
+    for (int x = tid; x < nent; x += NTHR) {
+      int t, m, k, K, t0;
+      if (x < nt) { t = x; m = 0; k = k1; K = K1; t0 = 0; }
+      else if (x < nt * (1 + K2)) { const int y = x - nt; t = y >> LK2; k = y & (K2 - 1); m = 1; K = K2; t0 = K1; }
+      else { const int y = x - nt * (1 + K2); t = y >> LK3; k = y & (K3 - 1); m = 2; K = K3; t0 = K1 + K2; }
       const int g = sg[t * 3 + m];
       const float* wc = sw + (t * 3 + m) * kMaxOrder;
       double2 e = twd[t0 + ((k * g) & (K - 1))];
@@ -251,12 +256,14 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
     if (DIRECT) {
       for (int t = 0; t < nt; ++t) {
         const float2 c = cmul(c1[t], b2[t * K2 + k2]);
-        const float2* bt = b3 + t * K3 + k3b;
+        const float4* bt = (const float4*)(b3 + t * K3 + k30);   // two k3 per 16-byte load
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-          const float2 u = bt[e * k3s];
+        for (int e = 0; e < E; e += 2) {
+          const float4 u = bt[e / 2];
           acc[e].x += c.x * u.x - c.y * u.y;
           acc[e].y += c.x * u.y + c.y * u.x;
+          acc[e + 1].x += c.x * u.z - c.y * u.w;
+          acc[e + 1].y += c.x * u.w + c.y * u.z;
         }
       }
     } else {
@@ -271,7 +278,7 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
         const float* w3 = sw + (t * 3 + 2) * kMaxOrder;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-          const int c3 = (g3 - (k3b + e * k3s)) & (K3 - 1);
+          const int c3 = (g3 - (k30 + e)) & (K3 - 1);
           if (c3 < n) {
             acc[e].x += f.x * w3[c3];
             acc[e].y += f.y * w3[c3];
@@ -281,38 +288,39 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
     }
   }
   // (DIRECT) acc holds Qhat(k1, k2, k3); otherwise the k1-transformed plane, still in (n2, n3)
-  const FftMap rows{ilog2(K2), ilog2(K3), 30, 0, pitch, 1};
-  const FftMap cols{ilog2(K3), ilog2(K2), 30, 0, 1, pitch};
+  using Rows = FftShape<LK2, LK3, 30, 0, PITCH, 1>;
+  using Cols = FftShape<LK3, LK2, 30, 0, 1, PITCH>;
+  float2* own = plane + k30 * PITCH + k2;
   if (!DIRECT) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) plane[(k3b + e * k3s) * pitch + k2] = acc[e];
+    for (int e = 0; e < E; ++e) own[e * PITCH] = acc[e];
     __syncthreads();
-    fft_batch<E, false>(plane, rows, tw2, tid, nthr);
-    fft_batch<E, false>(plane, cols, tw3, tid, nthr);
+    fft_batch<Rows, NTHR, false>(plane, tw2, tid);
+    fft_batch<Cols, NTHR, false>(plane, tw3, tid);
 #pragma unroll
-    for (int e = 0; e < E; ++e) acc[e] = plane[(k3b + e * k3s) * pitch + k2];
+    for (int e = 0; e < E; ++e) acc[e] = own[e * PITCH];
   }
-  // influence function and the plane's share of the self energy (recpcal.F90:482-497)
-  // (each mode's energy G |Qhat|^2 is formed in FP32, ~1e-7 relative, and summed in FP64)
+  // influence function and the plane's share of the self energy (recpcal.F90:482-497);
+  // each mode's G |Qhat|^2 is formed in FP32 (~1e-7 relative) and summed in FP64
   double self = 0.0;
-  const float* gk = engfacT + (size_t)k1 * K3 * K2;
+  const float* gk = engfacT + ((size_t)k1 * K3 + k30) * K2 + k2;
   float g[E];
 #pragma unroll
-  for (int e = 0; e < E; ++e) g[e] = gk[(k3b + e * k3s) * K2 + k2];
+  for (int e = 0; e < E; ++e) g[e] = gk[e * K2];
 #pragma unroll
   for (int e = 0; e < E; ++e) {
     self += (double)(g[e] * (acc[e].x * acc[e].x + acc[e].y * acc[e].y));
-    plane[(k3b + e * k3s) * pitch + k2] = make_float2(acc[e].x * g[e], acc[e].y * g[e]);
+    own[e * PITCH] = make_float2(acc[e].x * g[e], acc[e].y * g[e]);
   }
   if (k1 == 0 || 2 * k1 == K1) self *= 0.5;
   __syncthreads();
-  fft_batch<E, true>(plane, rows, tw2, tid, nthr);
-  fft_batch<E, true>(plane, cols, tw3, tid, nthr);
+  fft_batch<Rows, NTHR, true>(plane, tw2, tid);
+  fft_batch<Cols, NTHR, true>(plane, tw3, tid);
   float2* y = Y + ((size_t)b * Kh1 + k1) * K3 * K2;
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    const int p = tid + e * nthr;
-    y[p] = plane[(p >> lk2) * pitch + (p & (K2 - 1))];
+    const int p = tid + e * NTHR;
+    y[p] = plane[(p >> LK2) * PITCH + (p & (K2 - 1))];
   }
   // deterministic self-energy reduction over the planes of this target
   __shared__ double red[32];
@@ -321,7 +329,7 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
   if ((tid & 31) == 0) red[tid >> 5] = self;
   __syncthreads();
   if (tid < 32) {
-    double v = tid < (nthr >> 5) ? red[tid] : 0.0;
+    double v = tid < (NTHR >> 5) ? red[tid] : 0.0;
     v = warp_sum(v);
     if (tid == 0) {
       partial[(size_t)b * Kh1 + k1] = v;
@@ -341,16 +349,17 @@ __global__ void __launch_bounds__(E == 16 ? 256 : 512, E == 16 ? 3 : 1) k_pme_pl
 }
 
 // ---------------------------------------------------------------------------
-// k_pme_rows: grid (K3, K2 / G2), kRowThreads threads, G2 = 256 / M rows of
-// n2 for all 32 targets; M = K1 / 2.  Shared rows k1 = 0..M hold
+// k_pme_rows<LM>: grid (K3, K2 / G2), kRowThreads threads, G2 = 256 / M rows
+// of n2 for all 32 targets; M = K1 / 2 = 2^LM.  Shared rows k1 = 0..M hold
 // Y[b][k1][n3][n2] at column (n2 - n2g) * 33 + b.
 // ---------------------------------------------------------------------------
+template <int LM>
 __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb, const float2* __restrict__ Y,
     const float2* __restrict__ fft_tw, float* __restrict__ phi) {
+  constexpr int M = 1 << LM, K1 = 2 * M, Kh1 = M + 1;
+  constexpr int G2 = 256 / M, LG2 = 8 - LM, T = 32 * G2, LT = LG2 + 5, TP = G2 * 33;
   extern __shared__ __align__(16) unsigned char rsm[];
-  const int K1 = a.K1, K2 = a.K2, K3 = a.K3, Kh1 = a.Kh1, M = K1 / 2;
-  const int G2 = 256 / M, T = 32 * G2, TP = G2 * 33;
-  const int lg2 = ilog2(G2), lt = lg2 + 5, lm = ilog2(M);
+  const int K2 = a.K2, K3 = a.K3;
   const int n3 = blockIdx.x, n2g = blockIdx.y * G2;
   const int tid = threadIdx.x;
   float2* twk = (float2*)rsm;          // [K1] exp(-2 pi i m / K1)
@@ -359,7 +368,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
   for (int p = tid; p < K1; p += kRowThreads) twk[p] = fft_tw[p];
   for (int p = tid; p < M; p += kRowThreads) twm[p] = fft_tw[K1 + K2 + K3 + p];
   // stage Y with kLoadBatch independent loads in flight per thread
-  const int total = T * Kh1;
+  constexpr int total = T * Kh1;
   for (int x0 = 0; x0 < total; x0 += kLoadBatch * kRowThreads) {
     float2 v[kLoadBatch];
     int dst[kLoadBatch];
@@ -369,7 +378,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
       dst[u] = -1;
       v[u] = make_float2(0.f, 0.f);
       if (x < total) {
-        const int j = x & (G2 - 1), r = x >> lg2;   // r = k1 * 32 + b
+        const int j = x & (G2 - 1), r = x >> LG2;   // r = k1 * 32 + b
         const int b = r & 31, k1 = r >> 5;
         dst[u] = k1 * TP + j * 33 + b;
         if (b < nb) v[u] = Y[(((size_t)b * Kh1 + k1) * K3 + n3) * K2 + n2g + j];
@@ -384,7 +393,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
   //   Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) exp(+2 pi i k / K1)
   // so that x[2n] = Re z[n], x[2n+1] = Im z[n] for z = inverse DFT_M(Z).
   for (int x = tid; x < T * (M / 2 + 1); x += kRowThreads) {
-    const int t = x & (T - 1), k = x >> lt;
+    const int t = x & (T - 1), k = x >> LT;
     const int c = (t >> 5) * 33 + (t & 31);
     float2 xk = S[k * TP + c], xm = S[(M - k) * TP + c];
     if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
@@ -402,13 +411,12 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
     }
   }
   __syncthreads();
-  const FftMap f{lm, lt, 5, 33, 1, TP};
-  fft_batch<kRowElems, true>(S, f, twm, tid, kRowThreads);
+  fft_batch<FftShape<LM, LT, 5, 33, 1, TP>, kRowThreads, true>(S, twm, tid);
   // phi[p][b], p = (n3 K2 + n2) K1 + n1, two n1 per complex value
   float* out = phi + ((size_t)n3 * K2 + n2g) * K1 * 32;
   for (int x = tid; x < T * M; x += kRowThreads) {
     const int b = x & 31, r = x >> 5;
-    const int n = r & (M - 1), j = r >> lm;
+    const int n = r & (M - 1), j = r >> LM;
     const float2 z = S[n * TP + j * 33 + b];
     float* o = out + ((size_t)j * K1 + 2 * n) * 32 + b;
     o[0] = z.x;
@@ -421,6 +429,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
 // ---------------------------------------------------------------------------
 namespace {
 bool pow2_in(int k, int lo, int hi) { return k >= lo && k <= hi && (k & (k - 1)) == 0; }
+int lg(int k) { int l = 0; while ((1 << l) < k) ++l; return l; }
 
 int plane_elems(const FrameArgs& a) { return a.K2 * a.K3 <= 4096 ? 16 : 32; }
 
@@ -436,9 +445,30 @@ size_t rows_smem(const FrameArgs& a) {
   return sizeof(float2) * (size_t)(a.K1 + M) + sizeof(float2) * (size_t)a.Kh1 * G2 * 33;
 }
 
-template <int E, bool D>
+// Compile-time plane sizes: every (K2, K3) in {16..128}^2 with K2 K3 >= 512.
+#define ERM_PLANE_SIZES(X) \
+  X(4, 5) X(4, 6) X(4, 7) X(5, 4) X(5, 5) X(5, 6) X(5, 7) X(6, 4) X(6, 5) X(6, 6) X(6, 7) X(7, 4) X(7, 5) X(7, 6) X(7, 7)
+
+template <int L2, int L3>
 cudaError_t plane_attr(const FrameArgs& a) {
-  return cudaFuncSetAttribute(k_pme_plane<E, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane_smem(a, D));
+  cudaError_t e = cudaFuncSetAttribute(k_pme_plane<L2, L3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)plane_smem(a, true));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_pme_plane<L2, L3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)plane_smem(a, false));
+  return e;
+}
+
+template <int L2, int L3>
+void plane_launch(const FrameArgs& a, const DeviceState& d, int base, int nb, bool direct, cudaStream_t s) {
+  using C = PlaneCfg<L2, L3>;
+  const dim3 grid(a.Kh1, nb);
+  if (direct)
+    k_pme_plane<L2, L3, true><<<grid, C::NTHR, plane_smem(a, true), s>>>(
+        a, base, d.tgt_raw, d.engfacT, d.fft_tw, d.fft_twd, d.spec, d.partial, d.done, d.selfrec);
+  else
+    k_pme_plane<L2, L3, false><<<grid, C::NTHR, plane_smem(a, false), s>>>(
+        a, base, d.tgt_raw, d.engfacT, d.fft_tw, d.fft_twd, d.spec, d.partial, d.done, d.selfrec);
 }
 }  // namespace
 
@@ -448,23 +478,24 @@ bool fused_supported(const FrameArgs& a) {
   const int M = a.K1 / 2, G2 = 256 / M;
   if (G2 > a.K2) return false;                       // one CTA of k_pme_rows spans G2 rows of n2
   if (a.K2 * a.K3 < 512) return false;               // at least 32 threads per plane
-  const int E = plane_elems(a);
-  if (a.K3 < E) return false;                        // ownership map needs K2 | threads
+  if (a.K3 % plane_elems(a) != 0) return false;      // a thread owns E consecutive k3
   return plane_smem(a, true) <= 220 * 1024 && rows_smem(a) <= 220 * 1024;
 }
 
 int setup_fused(const FrameArgs& a) {
   if (!fused_supported(a)) return -1;
-  cudaError_t e = cudaSuccess;
-  if (plane_elems(a) == 16) {
-    if (e == cudaSuccess) e = plane_attr<16, true>(a);
-    if (e == cudaSuccess) e = plane_attr<16, false>(a);
-  } else {
-    if (e == cudaSuccess) e = plane_attr<32, true>(a);
-    if (e == cudaSuccess) e = plane_attr<32, false>(a);
-  }
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_pme_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem(a));
+  const int l2 = lg(a.K2), l3 = lg(a.K3);
+  cudaError_t e = cudaErrorInvalidValue;
+#define ERM_ATTR(L2, L3) if (l2 == L2 && l3 == L3) e = plane_attr<L2, L3>(a);
+  ERM_PLANE_SIZES(ERM_ATTR)
+#undef ERM_ATTR
+  if (e != cudaSuccess) return -1;
+  const int lm = lg(a.K1 / 2);
+  const int sm = (int)rows_smem(a);
+  if (lm == 3) e = cudaFuncSetAttribute(k_pme_rows<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (lm == 4) e = cudaFuncSetAttribute(k_pme_rows<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (lm == 5) e = cudaFuncSetAttribute(k_pme_rows<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (lm == 6) e = cudaFuncSetAttribute(k_pme_rows<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   return e == cudaSuccess ? 0 : -1;
 }
 
@@ -484,24 +515,22 @@ void fused_twiddles(int K1, int K2, int K3, std::vector<float2>& tw, std::vector
 }
 
 void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int nb, bool direct, cudaStream_t s) {
-  const int E = plane_elems(a);
-  const int nthr = a.K2 * a.K3 / E;
-  const dim3 grid(a.Kh1, nb);
-  const size_t sm = plane_smem(a, direct);
-#define ERM_PLANE(EE, DD)                                                                                 \
-  k_pme_plane<EE, DD><<<grid, nthr, sm, s>>>(a, base, d.tgt_raw, d.engfacT, d.fft_tw, d.fft_twd, d.spec, \
-                                             d.partial, d.done, d.selfrec)
-  if (E == 16) {
-    if (direct) ERM_PLANE(16, true); else ERM_PLANE(16, false);
-  } else {
-    if (direct) ERM_PLANE(32, true); else ERM_PLANE(32, false);
-  }
-#undef ERM_PLANE
+  const int l2 = lg(a.K2), l3 = lg(a.K3);
+#define ERM_LAUNCH(L2, L3) if (l2 == L2 && l3 == L3) plane_launch<L2, L3>(a, d, base, nb, direct, s);
+  ERM_PLANE_SIZES(ERM_LAUNCH)
+#undef ERM_LAUNCH
 }
 
 void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int nb, cudaStream_t s) {
-  const int G2 = 256 / (a.K1 / 2);
-  k_pme_rows<<<dim3(a.K3, a.K2 / G2), kRowThreads, rows_smem(a), s>>>(a, nb, d.spec, d.fft_tw, d.phi);
+  const int M = a.K1 / 2, G2 = 256 / M;
+  const dim3 grid(a.K3, a.K2 / G2);
+  const size_t sm = rows_smem(a);
+  switch (lg(M)) {
+    case 3: k_pme_rows<3><<<grid, kRowThreads, sm, s>>>(a, nb, d.spec, d.fft_tw, d.phi); break;
+    case 4: k_pme_rows<4><<<grid, kRowThreads, sm, s>>>(a, nb, d.spec, d.fft_tw, d.phi); break;
+    case 5: k_pme_rows<5><<<grid, kRowThreads, sm, s>>>(a, nb, d.spec, d.fft_tw, d.phi); break;
+    default: k_pme_rows<6><<<grid, kRowThreads, sm, s>>>(a, nb, d.spec, d.fft_tw, d.phi); break;
+  }
 }
 
 }  // namespace erm
