@@ -109,8 +109,10 @@ def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int
         return min(maxdst, 4096) * (slvmax * 8 + ermax * 4)
     if stage == "influence":    # spectrum read + write, influence function read
         return chunk * KH * 8 * 2 + KH * 4
-    if stage == "pme_plane":    # solute sites in, transformed planes out once, influence function in
-        return chunk * KH * 8 + KH * 4 + chunk * nsite * 16
+    if stage == "pme_plane":    # site tables in, transformed planes out once, influence function in
+        return chunk * KH * 8 + KH * 4 + chunk * nsite * (K // 2 + 1 + 2 * K) * 8
+    if stage == "site_tables":  # solute sites in, per-site stencil transforms out (one launch per batch)
+        return min(maxdst, 4096) * nsite * (16 + (K // 2 + 1 + 2 * K) * 8)
     if stage == "pme_rows":     # transformed planes in, potential grids out (insertion-fastest)
         return chunk * KH * 8 + chunk * KK * 4
     if stage == "transpose":    # potential grids read once, written once
@@ -257,10 +259,11 @@ def main():
     value = ws * units * args.steps / (dev_ms * 1e-3)
     e2e = ws * units * args.steps / e2e_s
     # roofline of the dominant engine kernel (cuFFT's own kernels are library code)
-    ours = ["real", "spread", "influence", "pme_plane", "pme_rows", "transpose", "gather", "bin", "ecorr"]
+    ours = ["real", "spread", "influence", "pme_plane", "pme_rows", "site_tables", "transpose", "gather", "bin",
+            "ecorr"]
     dom = max(ours, key=lambda k: stage[k])
     nbatch = -(-eng.maxdst // 4096)
-    per_batch = ("real", "bin", "ecorr")
+    per_batch = ("real", "bin", "ecorr", "site_tables")
     # stage["chunks"] sums the per-frame chunk counts over the timed steps
     n_launch = nbatch * args.steps if dom in per_batch else stage["chunks"]
     per_launch_ms = stage[dom] / n_launch
@@ -272,7 +275,8 @@ def main():
     bytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
     achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
     kname = {"gather": "k_gather", "bin": "k_bin", "real": "k_real", "spread": "k_spread_box",
-             "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane", "pme_rows": "k_pme_rows", "influence": "k_influence", "ecorr": "k_ecorr_tc"}[dom]
+             "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane", "pme_rows": "k_pme_rows",
+             "site_tables": "k_site_tables", "influence": "k_influence", "ecorr": "k_ecorr_tc"}[dom]
     traffic = traffic_from_profiles(kname)
     stage_share = {k: round(stage[k] / max(stage["total"], 1e-9), 4) for k in Engine.STAGES
                    if k not in ("total", "chunks")}

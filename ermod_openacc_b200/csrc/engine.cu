@@ -79,7 +79,7 @@ struct ermod_ctx {
   std::vector<cudaEvent_t> pev;
   std::vector<int> ptag;
   int pused = 0;
-  float timings[16] = {0};
+  float timings[17] = {0};
   long long launches = 0;
   int use_tc = 1;
   int spath = 1;     // PME solve: 1 spread + cuFFT, 2 fused with direct site sums, 3 fused with plane spreading
@@ -92,7 +92,7 @@ constexpr int kDirectAutoSites = 16;
 
 enum Stage { kStPrep = 1, kStIns = 2, kStReal = 3, kStSpread = 4, kStR2C = 5, kStInfl = 6, kStC2R = 7,
              kStGather = 8, kStBin = 9, kStWeights = 10, kStEcorr = 11, kStChunks = 12, kStTranspose = 13,
-             kStPlane = 14, kStRows = 15, kNumTimings = 16 };
+             kStPlane = 14, kStRows = 15, kStSiteTab = 16, kNumTimings = 17 };
 
 namespace {
 
@@ -114,7 +114,8 @@ void free_all(ermod_ctx* c) {
                   d.slt_mass, d.bfcoord, d.uvcrd, d.spec_off, d.uvsoft, d.escrd, d.posraw, d.slvn, d.spl, d.grd,
                   d.anchor, d.cellof, d.cellcount, d.cellstart, d.molsorted, d.rmol, d.ins_conf, d.insw_in,
                   d.tgt_raw, d.tgt_n, d.tgt_c, d.tgt_mol, d.selfreal, d.selfrec, d.u0, d.w, d.etot, d.flceng,
-                  d.grid, d.spec, d.phin, d.phi, d.engfac, d.engfacT, d.fft_tw, d.fft_twd, d.splfc,
+                  d.grid, d.spec, d.phin, d.phi, d.engfac, d.engfacT, d.fft_tw, d.fft_twd, d.sitetab, d.sitestn,
+                  d.splfc,
                   d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
                   d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.edens_part, d.ecorr, d.eself,
                   d.slnuv, d.minuv, d.maxuv, d.scal, d.status, c->tc_work};
@@ -392,6 +393,8 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
       fused_twiddles(K1, K2, K3, tw, twd);
       CK(dalloc(&d.fft_tw, tw.size()));
       CK(dalloc(&d.fft_twd, twd.size()));
+      CK(dalloc(&d.sitetab, fused_sitetab_elems(fa, ctx->batch, ctx->spath == 2)));
+      if (ctx->spath == 3) CK(dalloc(&d.sitestn, fused_sitestn_elems(fa, ctx->batch)));
       CK(cudaMemcpyAsync(d.fft_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice, ctx->st));
       CK(cudaMemcpyAsync(d.fft_twd, twd.data(), sizeof(double2) * twd.size(), cudaMemcpyHostToDevice, ctx->st));
       CK(cudaStreamSynchronize(ctx->st));
@@ -704,10 +707,15 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
     launch_real(a, d, bb, nbatch, ctx->batch, st);
     mark(ctx, kStReal);
     nl += 1;
+    if (pme && ctx->spath != 1) {
+      launch_site_tables(a, d, bb, nbatch, ctx->spath == 2, st);
+      mark(ctx, kStSiteTab);
+      nl += 1;
+    }
     for (int cb = bb; cb < bb + nbatch; cb += chunk) {
       const int nb = std::min(chunk, bb + nbatch - cb);
       if (pme && ctx->spath != 1) {
-        launch_pme_plane(a, d, cb, nb, ctx->spath == 2, st);
+        launch_pme_plane(a, d, cb, cb - bb, nb, ctx->spath == 2, st);
         mark(ctx, kStPlane);
         launch_pme_rows(a, d, nb, st);
         mark(ctx, kStRows);

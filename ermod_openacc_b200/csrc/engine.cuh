@@ -86,6 +86,8 @@ struct DeviceState {
   float* engfacT = nullptr;  // [Kh1*K3*K2] influence function, k1-major (fused PME solve)
   float2* fft_tw = nullptr;  // [K1+K2+K3+K1/2] FP32 twiddle tables of the fused PME solve
   double2* fft_twd = nullptr;// [K1+K2+K3] FP64 twiddle tables (stencil transforms)
+  float2* sitetab = nullptr; // [batch*s*(Kh1 [+K2+K3])] per (target, site) stencil transforms of a batch
+  float* sitestn = nullptr;  // [batch*s*(2+2*kMaxOrder)] per (target, site) stencils (plane spreading)
   double* splfc = nullptr;   // [K1+K2+K3]
   double* E = nullptr;       // [slvmax*batch] real-space energies of the batch, molecule-major
   double* Etot = nullptr;    // [batch*slvmax] total pair energies of the batch, target-major (uvengy layout)
@@ -129,7 +131,11 @@ void launch_clear_box(const FrameArgs& a, const DeviceState& d, int chunk, cudaS
 bool fused_supported(const FrameArgs& a);
 int setup_fused(const FrameArgs& a);
 void fused_twiddles(int K1, int K2, int K3, std::vector<float2>& tw, std::vector<double2>& twd);
-void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int nb, bool direct, cudaStream_t s);
+size_t fused_sitetab_elems(const FrameArgs& a, int batch, bool direct);
+size_t fused_sitestn_elems(const FrameArgs& a, int batch);
+void launch_site_tables(const FrameArgs& a, const DeviceState& d, int bb, int nbatch, bool direct, cudaStream_t s);
+void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int tbase, int nb, bool direct,
+                      cudaStream_t s);
 void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int nb, cudaStream_t s);
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
 

@@ -694,11 +694,11 @@ void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb
 constexpr int kGatherThreads = 256;
 
 template <int NO>
-__global__ void __launch_bounds__(kGatherThreads, 4) k_gather(FrameArgs a, int base, int bb, int nb, int chunk, int batch,
-    const int* __restrict__ molsorted, const int* __restrict__ molbeg, const float* __restrict__ molq,
-    const float* __restrict__ atom_q, const float* __restrict__ spl, const int4* __restrict__ grd,
-    const float* __restrict__ phi, const double* __restrict__ Ereal, const double* __restrict__ tgtq,
-    const int* __restrict__ tgt_mol, double* __restrict__ Etot) {
+__global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(FrameArgs a, int base, int bb, int nb,
+    int chunk, int batch, const int* __restrict__ molsorted, const int* __restrict__ molbeg,
+    const float* __restrict__ molq, const float* __restrict__ atom_q, const float* __restrict__ spl,
+    const int4* __restrict__ grd, const float* __restrict__ phi, const double* __restrict__ Ereal,
+    const double* __restrict__ tgtq, const int* __restrict__ tgt_mol, double* __restrict__ Etot) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwt = (gridDim.x * blockDim.x) >> 5;
@@ -718,27 +718,58 @@ __global__ void __launch_bounds__(kGatherThreads, 4) k_gather(FrameArgs a, int b
         const float q = atom_q[at];
         const float* w = spl + (size_t)at * 3 * n;
         const int4 gd = grd[at];
-        float w1[NO > 0 ? NO : kMaxOrder];
-        int r1[NO > 0 ? NO : kMaxOrder];
+        if constexpr (NO > 0) {
+          // the stencil rows of CS planes c3 in flight at once (one 128-byte row per load):
+          // the whole 4^3 stencil for order 4, one 6^2 plane for order 6
+          constexpr int CS = NO <= 4 ? NO : 1;
+          int r1[NO];
 #pragma unroll
-        for (int c1 = 0; c1 < (NO > 0 ? NO : kMaxOrder); ++c1)
-          if (c1 < n) { w1[c1] = w[c1]; r1[c1] = wrapk(gd.x - c1, K1); }
+          for (int c1 = 0; c1 < NO; ++c1) r1[c1] = wrapk(gd.x - c1, K1) * chunk + b;
 #pragma unroll
-        for (int c3 = 0; c3 < (NO > 0 ? NO : kMaxOrder); ++c3) {
-          if (c3 >= n) break;
-          const int r3 = wrapk(gd.z - c3, K3);
-          const float fac1 = q * w[2 * n + c3];
+          for (int c30 = 0; c30 < NO; c30 += CS) {
+            float v[CS * NO * NO];
 #pragma unroll
-          for (int c2 = 0; c2 < (NO > 0 ? NO : kMaxOrder); ++c2) {
-            if (c2 >= n) break;
-            const int r2 = wrapk(gd.y - c2, K2);
-            const float fac2 = fac1 * w[n + c2];
-            const float* rowp = phi + ((size_t)(r3 * K2 + r2) * K1) * chunk + b;
-            float part = 0.0f;
+            for (int cs = 0; cs < CS; ++cs) {
+              const int r3 = wrapk(gd.z - (c30 + cs), K3);
 #pragma unroll
-            for (int c1 = 0; c1 < (NO > 0 ? NO : kMaxOrder); ++c1)
-              if (c1 < n) part += (fac2 * w1[c1]) * rowp[(size_t)r1[c1] * chunk];
-            e += (double)part;
+              for (int c2 = 0; c2 < NO; ++c2) {
+                const float* rowp = phi + (size_t)(r3 * K2 + wrapk(gd.y - c2, K2)) * K1 * chunk;
+#pragma unroll
+                for (int c1 = 0; c1 < NO; ++c1) v[(cs * NO + c2) * NO + c1] = rowp[r1[c1]];
+              }
+            }
+#pragma unroll
+            for (int cs = 0; cs < CS; ++cs) {
+              const float fac1 = q * w[2 * NO + c30 + cs];
+#pragma unroll
+              for (int c2 = 0; c2 < NO; ++c2) {
+                const float fac2 = fac1 * w[NO + c2];
+                float part = 0.0f;
+#pragma unroll
+                for (int c1 = 0; c1 < NO; ++c1) part += (fac2 * w[c1]) * v[(cs * NO + c2) * NO + c1];
+                e += (double)part;
+              }
+            }
+          }
+        } else {
+          float w1[kMaxOrder];
+          int r1[kMaxOrder];
+#pragma unroll
+          for (int c1 = 0; c1 < kMaxOrder; ++c1)
+            if (c1 < n) { w1[c1] = w[c1]; r1[c1] = wrapk(gd.x - c1, K1); }
+          for (int c3 = 0; c3 < n; ++c3) {
+            const int r3 = wrapk(gd.z - c3, K3);
+            const float fac1 = q * w[2 * n + c3];
+            for (int c2 = 0; c2 < n; ++c2) {
+              const int r2 = wrapk(gd.y - c2, K2);
+              const float fac2 = fac1 * w[n + c2];
+              const float* rowp = phi + ((size_t)(r3 * K2 + r2) * K1) * chunk + b;
+              float part = 0.0f;
+#pragma unroll
+              for (int c1 = 0; c1 < kMaxOrder; ++c1)
+                if (c1 < n) part += (fac2 * w1[c1]) * rowp[(size_t)r1[c1] * chunk];
+              e += (double)part;
+            }
           }
         }
       }

@@ -154,7 +154,9 @@ __device__ __forceinline__ void fft_batch(float2* buf, const float2* __restrict_
 
 __device__ __forceinline__ int ilog2(int x) { return 31 - __clz(x); }
 
-constexpr int kSiteTile = 32;                  // solute sites staged in shared memory at a time
+constexpr int kSiteTile = 32;                  // solute sites staged in shared memory at a time (at most)
+constexpr int kTabPairs = 8;                   // (target, site) pairs per CTA of k_site_tables
+constexpr int kStn = 2 + 2 * kMaxOrder;        // stencil record: g2, g3, w2[kMaxOrder], w3[kMaxOrder]
 constexpr int kRowThreads = 512;
 constexpr int kLoadBatch = 8;                  // global loads a thread keeps in flight while staging
 
@@ -163,94 +165,136 @@ struct PlaneCfg {
   static constexpr int K2 = 1 << LK2, K3 = 1 << LK3, PITCH = K2 + 1;
   static constexpr int E = LK2 + LK3 <= 12 ? 16 : 32;     // plane points per thread
   static constexpr int NTHR = (K2 * K3) / E;
-  static constexpr int MINB = E == 16 ? 3 : 1;
+  static constexpr int MINB = E == 16 ? 4 : 1;
   static_assert(K3 % E == 0, "a thread owns E consecutive k3 of one k2 column");
 };
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// k_site_tables: per (target, site) of a batch, the B-spline stencil
+// (calc_spline_molecule, recpcal.F90:553-574) and its 1-D transforms
+//   B_m(k) = sum_c w_mc exp(-2 pi i k (g_m - c) / K_m),
+// summed in FP64 as exp(-2 pi i k g / K) times powers of exp(+2 pi i k / K).
+// tab[pair][nk]: q B1(k1) for k1 < Kh1, then (direct sums) B2(k2), B3(k3).
+// stn[pair][kStn]: g2, g3 (as floats), w2[kMaxOrder], w3[kMaxOrder].
+// A CTA takes kTabPairs pairs: stencils first, then every entry of its pairs.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_site_tables(FrameArgs a, int base, int npairs, int nk,
+    const float4* __restrict__ tgt_raw, const double2* __restrict__ fft_twd, float2* __restrict__ tab,
+    float* __restrict__ stn) {
+  __shared__ float sw[kTabPairs][3][kMaxOrder];
+  __shared__ int sg[kTabPairs][3];
+  __shared__ float sq[kTabPairs];
+  const int K1 = a.K1, K2 = a.K2, K3 = a.K3, Kh1 = a.Kh1, n = a.order;
+  const int p0 = blockIdx.x * kTabPairs;
+  const int np = min(kTabPairs, npairs - p0);
+  const float4* sites = tgt_raw + (size_t)base * a.nsite;
+  for (int x = threadIdx.x; x < np * 3; x += blockDim.x) {
+    const int t = x / 3, m = x - 3 * t;
+    const float4 r = sites[p0 + t];
+    const int K = m == 0 ? K1 : (m == 1 ? K2 : K3);
+    float f = a.g.invcl[m][0] * r.x + a.g.invcl[m][1] * r.y + a.g.invcl[m][2] * r.z;
+    f = f - floorf(f);
+    f = f * (float)K;
+    const int rci = (int)f;
+    float w[kMaxOrder];
+    spline_weights(f - (float)rci, n, w);
+    for (int c = 0; c < kMaxOrder; ++c) sw[t][m][c] = c < n ? w[c] : 0.f;
+    sg[t][m] = rci & (K - 1);
+    if (m == 0) sq[t] = r.w;
+  }
+  __syncthreads();
+  if (stn) {
+    for (int x = threadIdx.x; x < np * kStn; x += blockDim.x) {
+      const int t = x / kStn, r = x - t * kStn;
+      float v;
+      if (r < 2) v = (float)sg[t][1 + r];
+      else if (r < 2 + kMaxOrder) v = sw[t][1][r - 2];
+      else v = sw[t][2][r - 2 - kMaxOrder];
+      stn[(size_t)(p0 + t) * kStn + r] = v;
+    }
+  }
+  for (int x = threadIdx.x; x < np * nk; x += blockDim.x) {
+    const int t = x / nk, r = x - t * nk;
+    int m, k, K, t0;
+    if (r < Kh1) { m = 0; k = r; K = K1; t0 = 0; }
+    else if (r < Kh1 + K2) { m = 1; k = r - Kh1; K = K2; t0 = K1; }
+    else { m = 2; k = r - Kh1 - K2; K = K3; t0 = K1 + K2; }
+    const int g = sg[t][m];
+    double2 e = fft_twd[t0 + ((k * g) & (K - 1))];
+    const double2 st = fft_twd[t0 + ((K - k) & (K - 1))];   // exp(+2 pi i k / K)
+    double re = (double)sw[t][m][0] * e.x, im = (double)sw[t][m][0] * e.y;
+    for (int c = 1; c < n; ++c) {
+      e = make_double2(e.x * st.x - e.y * st.y, e.x * st.y + e.y * st.x);
+      re += (double)sw[t][m][c] * e.x;
+      im += (double)sw[t][m][c] * e.y;
+    }
+    if (m == 0) {
+      const double q = (double)sq[t];
+      re *= q;
+      im *= q;
+    }
+    tab[(size_t)(p0 + t) * nk + r] = make_float2((float)re, (float)im);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // k_pme_plane<LK2, LK3, DIRECT>: grid (Kh1, targets), K2*K3/E threads.  Thread
-// tid owns the points (k2 = tid mod K2, k3 = (tid / K2) * E + e), e < E.  Per
-// tile of solute sites: the stencils (thread per site and axis), then the
-// stencil transforms the plane needs, summed in FP64 from an FP64 twiddle
-// table -- B1_a(k1) only for plane spreading, B1_a(k1), B2_a(all k2),
-// B3_a(all k3) for the direct sums.
+// tid owns the points (k2 = tid mod K2, k3 = (tid / K2) * E + e), e < E.
+// Solute sites are staged ts at a time from the batch's site tables.
 // ---------------------------------------------------------------------------
 template <int LK2, int LK3, bool DIRECT>
 __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::MINB) k_pme_plane(FrameArgs a,
-    int base, const float4* __restrict__ tgt_raw, const float* __restrict__ engfacT, const float2* __restrict__ fft_tw,
-    const double2* __restrict__ fft_twd, float2* __restrict__ Y, double* __restrict__ partial,
-    unsigned int* __restrict__ done, double* __restrict__ selfrec) {
+    int base, int tbase, int ts, const float2* __restrict__ tab, const float* __restrict__ stn,
+    const float* __restrict__ engfacT, const float2* __restrict__ fft_tw, float2* __restrict__ Y,
+    double* __restrict__ partial, unsigned int* __restrict__ done, double* __restrict__ selfrec) {
   using C = PlaneCfg<LK2, LK3>;
   constexpr int K2 = C::K2, K3 = C::K3, PITCH = C::PITCH, E = C::E, NTHR = C::NTHR;
   extern __shared__ __align__(16) unsigned char psm[];
   const int k1 = blockIdx.x, b = blockIdx.y;
   const int K1 = a.K1, Kh1 = a.Kh1, s = a.nsite, n = a.order;
+  const int nk = Kh1 + (DIRECT ? K2 + K3 : 0);
   const int tid = threadIdx.x;
-  const int ntw = DIRECT ? K1 + K2 + K3 : K1;
-  double2* twd = (double2*)psm;                        // [ntw]  exp(-2 pi i m / K), FP64
-  float2* tw2 = (float2*)(twd + ntw);                  // [K2]
+  float2* tw2 = (float2*)psm;                          // [K2]
   float2* tw3 = tw2 + K2;                              // [K3]
   float2* plane = tw3 + K3;                            // [K3][PITCH]
-  float2* c1 = plane + K3 * PITCH;                     // [kSiteTile] q_a B1_a(k1)
-  float2* b2 = c1 + kSiteTile;                         // DIRECT: [kSiteTile][K2]
-  float2* b3 = b2 + (DIRECT ? kSiteTile * K2 : 0);     // DIRECT: [kSiteTile][K3]
-  float* sw = (float*)(b3 + (DIRECT ? kSiteTile * K3 : 0));   // [kSiteTile][3][kMaxOrder] stencil weights
-  int* sg = (int*)(sw + kSiteTile * 3 * kMaxOrder);    // [kSiteTile][3] stencil origins
-  float* sq = (float*)(sg + kSiteTile * 3);            // [kSiteTile] charges
-  for (int p = tid; p < ntw; p += NTHR) twd[p] = fft_twd[p];
+  float2* c1 = plane + K3 * PITCH;                     // [ts] q_a B1_a(k1), padded to even length
+  float2* b2 = c1 + ((ts + 1) & ~1);                   // DIRECT: [ts][K2] (16-byte aligned: K's are even)
+  float2* b3 = b2 + (DIRECT ? ts * K2 : 0);            // DIRECT: [ts][K3]
+  float* sst = (float*)b3;                             // spreading: [ts][kStn] stencils
   for (int p = tid; p < K2 + K3; p += NTHR) tw2[p] = fft_tw[K1 + p];
-  const float4* sites = tgt_raw + (size_t)(base + b) * s;
+  const size_t pair0 = (size_t)(tbase + b) * s;       // first (target, site) pair of this target in the tables
   const int k2 = tid & (K2 - 1), k30 = (tid >> LK2) * E;
   float2 acc[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
-  for (int a0 = 0; a0 < s; a0 += kSiteTile) {
-    const int nt = min(kSiteTile, s - a0);
+  for (int a0 = 0; a0 < s; a0 += ts) {
+    const int nt = min(ts, s - a0);
     __syncthreads();
-    // stencils (calc_spline_molecule, recpcal.F90:553-574)
-    for (int x = tid; x < nt * 3; x += NTHR) {
-      const int t = x / 3, m = x - 3 * t;
-      const float4 r = sites[a0 + t];
-      const int K = m == 0 ? K1 : (m == 1 ? K2 : K3);
-      float f = a.g.invcl[m][0] * r.x + a.g.invcl[m][1] * r.y + a.g.invcl[m][2] * r.z;
-      f = f - floorf(f);
-      f = f * (float)K;
-      const int rci = (int)f;
-      float w[kMaxOrder];
-      spline_weights(f - (float)rci, n, w);
-      for (int c = 0; c < n; ++c) sw[x * kMaxOrder + c] = w[c];
-      sg[x] = rci & (K - 1);
-      if (m == 0) sq[t] = r.w;
-    }
-    __syncthreads();
-    // stencil transforms B_m(k) = sum_c w_c exp(-2 pi i k (g - c) / K_m), FP64:
-    // exp(-2 pi i k g / K) times powers of exp(+2 pi i k / K)
-    const int nent = DIRECT ? nt * (1 + K2 + K3) : nt;
-    for (int x = tid; x < nent; x += NTHR) {
-      int t, m, k, K, t0;
-      if (x < nt) { t = x; m = 0; k = k1; K = K1; t0 = 0; }
-      else if (x < nt * (1 + K2)) { const int y = x - nt; t = y >> LK2; k = y & (K2 - 1); m = 1; K = K2; t0 = K1; }
-      else { const int y = x - nt * (1 + K2); t = y >> LK3; k = y & (K3 - 1); m = 2; K = K3; t0 = K1 + K2; }
-      const int g = sg[t * 3 + m];
-      const float* wc = sw + (t * 3 + m) * kMaxOrder;
-      double2 e = twd[t0 + ((k * g) & (K - 1))];
-      const double2 st = twd[t0 + ((K - k) & (K - 1))];   // exp(+2 pi i k / K)
-      double re = (double)wc[0] * e.x, im = (double)wc[0] * e.y;
-      for (int c = 1; c < n; ++c) {
-        e = make_double2(e.x * st.x - e.y * st.y, e.x * st.y + e.y * st.x);
-        re += (double)wc[c] * e.x;
-        im += (double)wc[c] * e.y;
+    for (int x = tid; x < nt; x += NTHR) c1[x] = tab[(pair0 + a0 + x) * nk + k1];
+    if (DIRECT) {
+      // B2 then B3 of each site: K2 + K3 consecutive table entries, kLoadBatch loads in flight
+      const int per = K2 + K3, tot = nt * per;
+      for (int x0 = 0; x0 < tot; x0 += kLoadBatch * NTHR) {
+        float2 v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+          const int x = x0 + u * NTHR + tid;
+          if (x < tot) v[u] = tab[(pair0 + a0 + x / per) * nk + Kh1 + x % per];
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+          const int x = x0 + u * NTHR + tid;
+          if (x < tot) {
+            const int t = x / per, r = x - t * per;
+            if (r < K2) b2[t * K2 + r] = v[u];
+            else b3[t * K3 + r - K2] = v[u];
+          }
+        }
       }
-      if (m == 0) {
-        const double q = (double)sq[t];
-        c1[t] = make_float2((float)(re * q), (float)(im * q));
-      } else if (m == 1) {
-        b2[t * K2 + k] = make_float2((float)re, (float)im);
-      } else {
-        b3[t * K3 + k] = make_float2((float)re, (float)im);
-      }
+    } else {
+      for (int x = tid; x < nt * kStn; x += NTHR) sst[x] = stn[(pair0 + a0) * kStn + x];
     }
     __syncthreads();
     if (DIRECT) {
@@ -269,13 +313,14 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
     } else {
       // q_a B1_a(k1) w2 w3 on the (n2, n3) plane, accumulated in site order by the point's owner
       for (int t = 0; t < nt; ++t) {
-        const int c2 = (sg[t * 3 + 1] - k2) & (K2 - 1);
+        const float* st = sst + t * kStn;
+        const int c2 = ((int)st[0] - k2) & (K2 - 1);
         if (c2 >= n) continue;
         const float2 c = c1[t];
-        const float w2 = sw[(t * 3 + 1) * kMaxOrder + c2];
+        const float w2 = st[2 + c2];
         const float2 f = make_float2(c.x * w2, c.y * w2);
-        const int g3 = sg[t * 3 + 2];
-        const float* w3 = sw + (t * 3 + 2) * kMaxOrder;
+        const int g3 = (int)st[1];
+        const float* w3 = st + 2 + kMaxOrder;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
           const int c3 = (g3 - (k30 + e)) & (K3 - 1);
@@ -433,11 +478,13 @@ int lg(int k) { int l = 0; while ((1 << l) < k) ++l; return l; }
 
 int plane_elems(const FrameArgs& a) { return a.K2 * a.K3 <= 4096 ? 16 : 32; }
 
+int site_tile(const FrameArgs& a) { return std::min(a.nsite, kSiteTile); }
+int site_table_entries(const FrameArgs& a, bool direct) { return a.Kh1 + (direct ? a.K2 + a.K3 : 0); }
+
 size_t plane_smem(const FrameArgs& a, bool direct) {
-  const size_t ntw = direct ? a.K1 + a.K2 + a.K3 : a.K1;
-  return sizeof(double2) * ntw + sizeof(float2) * (size_t)(a.K2 + a.K3) + sizeof(float2) * (size_t)a.K3 * (a.K2 + 1) +
-         sizeof(float2) * kSiteTile * (1 + (direct ? a.K2 + a.K3 : 0)) +
-         sizeof(float) * kSiteTile * (3 * kMaxOrder + 3 + 1);
+  const size_t ts = site_tile(a), tsa = (ts + 1) & ~(size_t)1;
+  const size_t tile = sizeof(float2) * tsa + (direct ? sizeof(float2) * ts * (a.K2 + a.K3) : sizeof(float) * ts * kStn);
+  return sizeof(float2) * (size_t)(a.K2 + a.K3) + sizeof(float2) * (size_t)a.K3 * (a.K2 + 1) + tile;
 }
 
 size_t rows_smem(const FrameArgs& a) {
@@ -460,15 +507,16 @@ cudaError_t plane_attr(const FrameArgs& a) {
 }
 
 template <int L2, int L3>
-void plane_launch(const FrameArgs& a, const DeviceState& d, int base, int nb, bool direct, cudaStream_t s) {
+void plane_launch(const FrameArgs& a, const DeviceState& d, int base, int tbase, int nb, bool direct, cudaStream_t s) {
   using C = PlaneCfg<L2, L3>;
   const dim3 grid(a.Kh1, nb);
+  const int ts = site_tile(a);
   if (direct)
     k_pme_plane<L2, L3, true><<<grid, C::NTHR, plane_smem(a, true), s>>>(
-        a, base, d.tgt_raw, d.engfacT, d.fft_tw, d.fft_twd, d.spec, d.partial, d.done, d.selfrec);
+        a, base, tbase, ts, d.sitetab, d.sitestn, d.engfacT, d.fft_tw, d.spec, d.partial, d.done, d.selfrec);
   else
     k_pme_plane<L2, L3, false><<<grid, C::NTHR, plane_smem(a, false), s>>>(
-        a, base, d.tgt_raw, d.engfacT, d.fft_tw, d.fft_twd, d.spec, d.partial, d.done, d.selfrec);
+        a, base, tbase, ts, d.sitetab, d.sitestn, d.engfacT, d.fft_tw, d.spec, d.partial, d.done, d.selfrec);
 }
 }  // namespace
 
@@ -499,6 +547,11 @@ int setup_fused(const FrameArgs& a) {
   return e == cudaSuccess ? 0 : -1;
 }
 
+size_t fused_sitetab_elems(const FrameArgs& a, int batch, bool direct) {
+  return (size_t)batch * a.nsite * site_table_entries(a, direct);
+}
+size_t fused_sitestn_elems(const FrameArgs& a, int batch) { return (size_t)batch * a.nsite * kStn; }
+
 void fused_twiddles(int K1, int K2, int K3, std::vector<float2>& tw, std::vector<double2>& twd) {
   // tw:  [K1 | K2 | K3 | K1/2] tables of exp(-2 pi i m / N), FP64 rounded to FP32
   // twd: [K1 | K2 | K3] the same in FP64
@@ -514,9 +567,17 @@ void fused_twiddles(int K1, int K2, int K3, std::vector<float2>& tw, std::vector
     }
 }
 
-void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int nb, bool direct, cudaStream_t s) {
+void launch_site_tables(const FrameArgs& a, const DeviceState& d, int bb, int nbatch, bool direct, cudaStream_t s) {
+  const int npairs = nbatch * a.nsite;
+  k_site_tables<<<(npairs + kTabPairs - 1) / kTabPairs, 256, 0, s>>>(a, bb, npairs, site_table_entries(a, direct),
+                                                                     d.tgt_raw, d.fft_twd, d.sitetab,
+                                                                     direct ? nullptr : d.sitestn);
+}
+
+void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int tbase, int nb, bool direct,
+                      cudaStream_t s) {
   const int l2 = lg(a.K2), l3 = lg(a.K3);
-#define ERM_LAUNCH(L2, L3) if (l2 == L2 && l3 == L3) plane_launch<L2, L3>(a, d, base, nb, direct, s);
+#define ERM_LAUNCH(L2, L3) if (l2 == L2 && l3 == L3) plane_launch<L2, L3>(a, d, base, tbase, nb, direct, s);
   ERM_PLANE_SIZES(ERM_LAUNCH)
 #undef ERM_LAUNCH
 }

@@ -155,7 +155,7 @@ class Engine:
         return o, w
 
     STAGES = ["total", "prepare", "insert", "real", "spread", "r2c", "influence", "c2r", "gather", "bin",
-              "weights_edens", "ecorr", "chunks", "transpose", "pme_plane", "pme_rows"]
+              "weights_edens", "ecorr", "chunks", "transpose", "pme_plane", "pme_rows", "site_tables"]
 
     def timings(self):
         """Device milliseconds per stage of the last engconst (CUDA events on the engine stream)."""

@@ -262,7 +262,8 @@ const char* ermod_last_error(const ermod_ctx* ctx);
  * [8] PME gather, [9] binning, [10] weights + edens, [11] ecorr,
  * [12] number of PME target chunks, [13] potential-grid transpose,
  * [14] fused solve: stencil transforms, spectrum planes and 2-D FFTs,
- * [15] fused solve: k1 transforms into the potential grids.  n <= 16. */
+ * [15] fused solve: k1 transforms into the potential grids, [16] fused
+ * solve: per-site stencil transforms of a batch.  n <= 17. */
 int32_t ermod_get_timings(const ermod_ctx* ctx, float* ms, int32_t n);
 
 /* The PME solve the context runs (1..3 as ermod_params.spectrum_path, 0 when
