@@ -99,7 +99,8 @@ def dist_init():
 
 
 def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int, maxdst: int, nsite: int) -> float:
-    """Algorithmic DRAM bytes of ONE launch of each of the engine's kernels."""
+    """Algorithmic DRAM bytes of ONE launch of each of the engine's kernels: what the launch must read and
+    write at least once (inputs in, outputs out), independent of how the kernel stages them."""
     K = w.params["ms1max"]
     n = w.params["splodr"]
     KK, KH = K ** 3, K * K * (K // 2 + 1)

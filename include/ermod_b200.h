@@ -13,9 +13,9 @@
  *   engstore(stnum) erdst/engproc.F90:520-725
  * called from trjmain (erdst/enganal.F90:86-95) with all state in module
  * `engmain` (erdst/engmain.F90:314-348).  The entry points below keep that
- * call structure: a Fortran host binds them through ISO_C_BINDING (the
- * interface module is given in INTEGRATION.md), a C/C++ host calls them
- * directly.  All state lives in an opaque context instead of module globals.
+ * call structure: a Fortran host binds them through ISO_C_BINDING
+ * (bind(C) interfaces over these plain-C signatures), a C/C++ host calls
+ * them directly.  All state lives in an opaque context instead of module globals.
  *
  * Conventions
  *   - Plain C types only.  Arrays are caller-owned HOST memory unless a
