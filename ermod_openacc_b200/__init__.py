@@ -5,5 +5,5 @@ recpcal, engproc binning and ecorr) with CUDA kernels behind the C-ABI in
 include/ermod_b200.h.  `Engine` mirrors engclear / engconst / engstore.
 """
 from ._capi import load_library  # noqa: F401
-from .engine import Engine, ErmodError, enginit_mesh  # noqa: F401
+from .engine import Batch, Engine, ErmodError, enginit_mesh  # noqa: F401
 from . import systems  # noqa: F401

@@ -54,7 +54,8 @@ class ErmodParams(C.Structure):
         ("ins_chunk", C.c_int32), ("ecorr_batch", C.c_int32), ("weight_bits", C.c_int32),
         ("proposal", C.c_int32),
         ("keep_uvengy", C.c_int32), ("ecorr_path", C.c_int32), ("spectrum_path", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("graph_mode", C.c_int32), ("stage_timing", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -124,6 +125,13 @@ SIGNATURES = {
     "ermod_get_timings": (C.c_int32, [C.c_void_p, _f32p, C.c_int32]),
     "ermod_get_launch_count": (C.c_int64, [C.c_void_p]),
     "ermod_get_paths": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "ermod_batch_create": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
+    "ermod_batch_engconst": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                         C.c_float]),
+    "ermod_batch_engconst_dev": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_float), C.c_float]),
+    "ermod_batch_last_ms": (C.c_float, [C.c_void_p]),
+    "ermod_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "ermod_batch_destroy": (None, [C.c_void_p]),
     "ermod_destroy": (None, [C.c_void_p]),
     "ermod_histogram_noalloc": (C.c_int32, [C.c_int32, C.c_int32, _f64p, C.c_int32, C.c_int32, _i32p, _f64p,
                                             _i32p, _i32p, C.c_int32, _f64p, _f64p]),

@@ -83,6 +83,13 @@ struct ermod_ctx {
   long long launches = 0;
   int use_tc = 1;
   int spath = 1;     // PME solve: 1 spread + cuFFT, 2 fused with direct site sums, 3 fused with plane spreading
+  int real_threads = 0;           // block size of k_real chosen by the autotuner (0: not tuned yet)
+  // the frame as a CUDA graph, re-captured when the frame plan changes
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<unsigned char> gkey;
+  long long graph_launches = 0;
+  int* h_frame = nullptr;         // pinned: [0] stnum of the frame being staged
+  DevStatus* h_status = nullptr;  // pinned: status word written by the frame
 };
 
 // With spectrum_path == 0 the fused solve builds the solute spectrum by direct
@@ -118,7 +125,7 @@ void free_all(ermod_ctx* c) {
                   d.splfc,
                   d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
                   d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.edens_part, d.ecorr, d.eself,
-                  d.slnuv, d.minuv, d.maxuv, d.scal, d.status, c->tc_work};
+                  d.slnuv, d.minuv, d.maxuv, d.scal, d.status, d.frame_i, c->tc_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->plans) {
@@ -130,6 +137,9 @@ void free_all(ermod_ctx* c) {
   for (auto& e : c->pev)
     if (e) cudaEventDestroy(e);
   if (c->h_pin) cudaFreeHost(c->h_pin);
+  if (c->h_frame) cudaFreeHost(c->h_frame);
+  if (c->h_status) cudaFreeHost(c->h_status);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->st) cudaStreamDestroy(c->st);
 }
 
@@ -421,7 +431,10 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   if (p.corrcal) CK(dalloc(&d.ecorr, (size_t)ctx->ermax * ctx->ermax));
   CK(dalloc(&d.eself, std::max(1, ctx->esmax))); CK(dalloc(&d.slnuv, ctx->numslv));
   CK(dalloc(&d.minuv, ctx->numslv + 1)); CK(dalloc(&d.maxuv, ctx->numslv + 1));
-  CK(dalloc(&d.scal, 8)); CK(dalloc(&d.status, 1));
+  CK(dalloc(&d.scal, 8)); CK(dalloc(&d.status, 1)); CK(dalloc(&d.frame_i, 4));
+  CK(cudaMallocHost((void**)&ctx->h_frame, 4 * sizeof(int)));
+  CK(cudaMallocHost((void**)&ctx->h_status, sizeof(DevStatus)));
+  if (p.graph_mode < 0 || p.graph_mode > 1 || p.stage_timing < 0 || p.stage_timing > 1) return bad(ERMOD_ERR_ARG, "opt_arg");
   // static uploads
   cudaStream_t st = ctx->st;
   CK(h2d(d.molbeg, molbeg.data(), SM + 1, st)); CK(h2d(d.molspec, molspec.data(), SM, st));
@@ -509,14 +522,40 @@ int32_t ermod_engclear(ermod_ctx* ctx) {
   return ERMOD_OK;
 }
 
-static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float wsys, bool use_conf) {
+}  // extern "C"
+
+// ---- the per-frame pipeline ------------------------------------------------
+// frame_plan   host: cell normalisation and every per-frame constant (FramePlan);
+// frame_enqueue device work of one frame on one stream, no host synchronisation;
+//              the frame's inputs (coordinates, stnum) are staged in fixed device
+//              buffers beforehand, so the enqueued work can be captured once as a
+//              CUDA graph and replayed while the plan stays the same;
+// frame_finish host: status word and stage timings after the stream is done.
+
+// Everything the enqueued work depends on besides the staged inputs.  Compared
+// bytewise to decide whether a captured graph is still valid, so it is
+// zero-filled before use.
+struct FramePlan {
+  FrameArgs a;
+  WeightArgs wa;
+  BinArgs ba;
+  int ncell, use_conf, selfreal, real_threads;
+};
+
+struct FramePlanHost {
+  FramePlan k;
+  bool engfac;          // influence function to rebuild before the frame
+  double inv[3][3], vold;
+};
+
+static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_conf, FramePlanHost& ph) {
   const ermod_params& p = ctx->p;
-  DeviceState& d = ctx->d;
-  cudaStream_t st = ctx->st;
+  std::memset(&ph, 0, sizeof(ph));
+  FramePlan& fp = ph.k;
   const bool refs = p.slttype != ERMOD_SLT_SOLN;
   const bool pme = p.cltype == ERMOD_EL_PME;
   const int K1 = p.ms1max, K2 = p.ms2max, K3 = p.ms3max;
-  // ---- cell (engproc.F90:1049-1070, realcal.F90:776-896) on the host ----
+  // ---- cell (engproc.F90:1049-1070, realcal.F90:776-896) ----
   double c[3][3];
   for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) c[i][j] = cellin[j * 3 + i];
   float cf[3][3];
@@ -526,7 +565,7 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
                     cf[0][2] * cf[1][1] * cf[2][0] - cf[0][1] * cf[1][0] * cf[2][2] - cf[0][0] * cf[1][2] * cf[2][1];
   const double vold = c[0][0] * c[1][1] * c[2][2] + c[0][1] * c[1][2] * c[2][0] + c[0][2] * c[1][0] * c[2][1] -
                       c[0][2] * c[1][1] * c[2][0] - c[0][1] * c[1][0] * c[2][2] - c[0][0] * c[1][2] * c[2][1];
-  double inv[3][3];
+  double (&inv)[3][3] = ph.inv;
   inv[0][0] = c[1][1] * c[2][2] - c[1][2] * c[2][1];
   inv[0][1] = c[0][2] * c[2][1] - c[0][1] * c[2][2];
   inv[0][2] = c[0][1] * c[1][2] - c[0][2] * c[1][1];
@@ -537,7 +576,8 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
   inv[2][1] = c[0][1] * c[2][0] - c[0][0] * c[2][1];
   inv[2][2] = c[0][0] * c[1][1] - c[0][1] * c[1][0];
   for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) inv[i][j] /= vold;
-  FrameArgs a{};
+  ph.vold = vold;
+  FrameArgs& a = fp.a;
   CellGeom& g = a.g;
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) {
@@ -625,7 +665,7 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
   if (P.bare && !g.periodic) a.rcut = FLT_MAX;
   // cell list only for cuboid periodic boxes
   a.use_cells = 0;
-  int ncell = 1;
+  fp.ncell = 1;
   if (g.periodic && g.cuboid && !g.rotated) {
     const float hmin = 4.0f;
     bool ok = true;
@@ -634,45 +674,22 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
       a.ch[dd] = g.len[dd] / (float)a.nc[dd];
       if (a.nc[dd] < 3) ok = false;
     }
-    ncell = a.nc[0] * a.nc[1] * a.nc[2];
-    a.use_cells = ok && ncell <= ctx->ncell_cap;
+    fp.ncell = a.nc[0] * a.nc[1] * a.nc[2];
+    a.use_cells = ok && fp.ncell <= ctx->ncell_cap;
   }
-  ctx->pused = 0;
-  mark(ctx, 0);
-  // ---- PME influence function when the cell changes (engconst :423-433) ----
+  // ---- influence function when the cell changes (engconst :423-433) ----
   if (pme) {
     bool changed = !ctx->pme_init;
     for (int i = 0; i < 9; ++i) if (ctx->prevcl[i] != cellin[i]) changed = true;
-    if (changed) launch_engfac(a, d, inv, vold, (double)p.screen, st);
-    for (int i = 0; i < 9; ++i) ctx->prevcl[i] = cellin[i];
-    ctx->pme_init = true;
+    ph.engfac = changed;
   }
-  CK(cudaMemsetAsync(d.status, 0, sizeof(DevStatus), st));
-  launch_prepare_solvent(a, d, st);
-  launch_cells(a, d, ncell, st);
-  long long nl = 1 + (a.slvmax > 0 ? (a.use_cells ? 3 : 2) : 0) + (pme && ctx->pme_init ? 0 : 0);
-  mark(ctx, kStPrep);
-  // ---- targets ----
-  if (refs) launch_insert(a, d, stnum, p.iseed, p.insposition, p.insorient, use_conf ? 1 : 0, st);
-  else launch_targets_soln(a, d, nullptr, st);
-  CK(cudaMemsetAsync(d.selfrec, 0, sizeof(double) * ctx->maxdst, st));
-  CK(cudaMemsetAsync(d.etot, 0, sizeof(double) * ctx->maxdst, st));
-  CK(cudaMemsetAsync(d.flceng, 0, sizeof(double) * ctx->maxdst * ctx->numslv, st));
-  if (d.uvengy) CK(cudaMemsetAsync(d.uvengy, 0, sizeof(double) * ctx->maxdst * ctx->slvmax, st));
+  // ---- real-space self term: per insertion, or once for a rigid solute ----
   const bool rigid = p.slttype == ERMOD_SLT_REFS_RIGID;
-  if (!P.bare) {
-    if (rigid) {
-      if (!ctx->usreal_init) { launch_selfreal(a, d, 0, 1, (double)p.screen, st); ctx->usreal_init = true; }
-    } else {
-      launch_selfreal(a, d, 0, ctx->maxdst, (double)p.screen, st);
-    }
-  } else {
-    CK(cudaMemsetAsync(d.selfreal, 0, sizeof(double) * ctx->maxdst, st));
-  }
-  nl += 1 + (P.bare ? 0 : (rigid ? 0 : 1));
-  mark(ctx, kStIns);
-  // ---- weights args ----
-  WeightArgs wa{};
+  fp.selfreal = P.bare ? 0 : (rigid ? (ctx->usreal_init ? 3 : 1) : 2);
+  fp.use_conf = use_conf ? 1 : 0;
+  fp.real_threads = ctx->real_threads;
+  // ---- weights ----
+  WeightArgs& wa = fp.wa;
   wa.slttype = p.slttype; wa.wgtslf = p.wgtslf; wa.estype = p.estype; wa.selfcal = p.selfcal;
   wa.numslv = ctx->numslv; wa.esmax = ctx->esmax; wa.rigid = rigid && !P.bare;
   wa.temp = p.temp;
@@ -698,57 +715,125 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
     if (pme) f *= std::exp(kPi * qt * qt / ((double)p.screen * p.screen) / vold / 2.0 / p.temp);
     wa.npt_factor = f;
   }
-  BinArgs ba{};
+  BinArgs& ba = fp.ba;
   ba.ermax = ctx->ermax; ba.ermax_pad = ctx->ermax_pad; ba.numslv = ctx->numslv; ba.slttype = p.slttype;
+  return ERMOD_OK;
+}
+
+// Host-side state the plan consumed, committed once the frame is enqueued.
+static void frame_commit(ermod_ctx* ctx, const float* cellin, const FramePlanHost& ph) {
+  if (ph.k.a.pme) {
+    for (int i = 0; i < 9; ++i) ctx->prevcl[i] = cellin[i];
+    ctx->pme_init = true;
+  }
+  if (ph.k.selfreal == 1) ctx->usreal_init = true;
+}
+
+// Block size of k_real: the autotuner's candidates all give bit-identical
+// energies (a warp per molecule whatever the block size), so the choice only
+// moves time.  Tuned on the first frame with the frame's own data.
+static const int kRealCandidates[] = {128, 256, 512};
+
+static int tune_real(ermod_ctx* ctx, const FrameArgs& a, int nbatch, cudaStream_t st) {
+  float best = 1e30f;
+  int pick = 256;
+  cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1];
+  for (int rep = 0; rep < 2; ++rep)
+    for (int nt : kRealCandidates) {
+      CK(cudaEventRecord(e0, st));
+      launch_real(a, ctx->d, 0, nbatch, ctx->batch, nt, st);
+      CK(cudaEventRecord(e1, st));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep == 1 && ms < best) { best = ms; pick = nt; }
+    }
+  ctx->real_threads = pick;
+  return ERMOD_OK;
+}
+
+// Enqueue the device work of one frame on `st`.  `timed` records stage events
+// (direct launches only).  Adds the number of kernel launches to `nl`.
+static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, bool timed, long long& nl) {
+  const ermod_params& p = ctx->p;
+  DeviceState& d = ctx->d;
+  const FrameArgs& a = fp.a;
+  const bool refs = p.slttype != ERMOD_SLT_SOLN;
+  const bool pme = a.pme;
+  auto M = [&](int tag) { if (timed) mark(ctx, tag); };
+  CK(cudaMemsetAsync(d.status, 0, sizeof(DevStatus), st));
+  launch_prepare_solvent(a, d, st);
+  launch_cells(a, d, fp.ncell, st);
+  nl += 1 + (a.slvmax > 0 ? (a.use_cells ? 3 : 2) : 0);
+  M(kStPrep);
+  // ---- targets ----
+  if (refs) launch_insert(a, d, d.frame_i, p.iseed, p.insposition, p.insorient, fp.use_conf, st);
+  else launch_targets_soln(a, d, nullptr, st);
+  CK(cudaMemsetAsync(d.selfrec, 0, sizeof(double) * ctx->maxdst, st));
+  CK(cudaMemsetAsync(d.etot, 0, sizeof(double) * ctx->maxdst, st));
+  CK(cudaMemsetAsync(d.flceng, 0, sizeof(double) * ctx->maxdst * ctx->numslv, st));
+  if (d.uvengy) CK(cudaMemsetAsync(d.uvengy, 0, sizeof(double) * ctx->maxdst * ctx->slvmax, st));
+  switch (fp.selfreal) {
+    case 0: CK(cudaMemsetAsync(d.selfreal, 0, sizeof(double) * ctx->maxdst, st)); break;
+    case 1: launch_selfreal(a, d, 0, 1, (double)p.screen, st); nl += 1; break;
+    case 2: launch_selfreal(a, d, 0, ctx->maxdst, (double)p.screen, st); nl += 1; break;
+    default: break;   // rigid solute: the first insertion's term is kept (engproc.F90:839-851)
+  }
+  nl += 1;
+  M(kStIns);
   // ---- batches of targets, each in chunks of `chunk` PME solves ----
   const int chunk = ctx->chunk;
   for (int bb = 0; bb < ctx->maxdst; bb += ctx->batch) {
     const int nbatch = std::min(ctx->batch, ctx->maxdst - bb);
-    launch_real(a, d, bb, nbatch, ctx->batch, st);
-    mark(ctx, kStReal);
+    if (ctx->real_threads == 0) {
+      const int rc = tune_real(ctx, a, nbatch, st);
+      if (rc != ERMOD_OK) return rc;
+    }
+    launch_real(a, d, bb, nbatch, ctx->batch, ctx->real_threads, st);
+    M(kStReal);
     nl += 1;
     if (pme && ctx->spath != 1) {
       launch_site_tables(a, d, bb, nbatch, ctx->spath == 2, st);
-      mark(ctx, kStSiteTab);
+      M(kStSiteTab);
       nl += 1;
     }
     for (int cb = bb; cb < bb + nbatch; cb += chunk) {
       const int nb = std::min(chunk, bb + nbatch - cb);
       if (pme && ctx->spath != 1) {
         launch_pme_plane(a, d, cb, cb - bb, nb, ctx->spath == 2, st);
-        mark(ctx, kStPlane);
+        M(kStPlane);
         launch_pme_rows(a, d, nb, st);
-        mark(ctx, kStRows);
+        M(kStRows);
         nl += 2;
       } else if (pme) {
         launch_spread(a, d, cb, nb, chunk, st);
-        mark(ctx, kStSpread);
+        M(kStSpread);
         CF(cufftExecR2C(ctx->r2c, d.grid, (cufftComplex*)d.spec));
-        mark(ctx, kStR2C);
+        M(kStR2C);
         launch_clear_box(a, d, chunk, st);
         launch_influence(a, d, cb, nb, chunk, st);
-        mark(ctx, kStInfl);
+        M(kStInfl);
         nl += 3;
         CF(cufftExecC2R(ctx->c2r, (cufftComplex*)d.spec, d.phin));
-        mark(ctx, kStC2R);
+        M(kStC2R);
         launch_transpose_phi(a, d, st);
-        mark(ctx, kStTranspose);
+        M(kStTranspose);
         nl += 1;
       }
       launch_gather(a, d, cb, bb, nb, chunk, ctx->batch, st);
-      mark(ctx, kStGather);
+      M(kStGather);
       nl += 1;
     }
-    launch_bin(d, ba, bb, nbatch, ctx->slvmax, st);
-    mark(ctx, kStBin);
+    launch_bin(d, fp.ba, bb, nbatch, ctx->slvmax, st);
+    M(kStBin);
     nl += 1;
     if (d.uvengy)
       CK(cudaMemcpyAsync(d.uvengy + (size_t)bb * ctx->slvmax, d.Etot, sizeof(double) * (size_t)nbatch * ctx->slvmax,
                          cudaMemcpyDeviceToDevice, st));
-    launch_weights(d, wa, bb, nbatch, st);
+    launch_weights(d, fp.wa, bb, nbatch, st);
     launch_edens(d, bb, nbatch, ctx->ermax, ctx->ermax_pad, bb, st);
     nl += 3;
-    mark(ctx, kStWeights);
+    M(kStWeights);
     if (p.corrcal) {
       if (ctx->use_tc) {
         const int rc = launch_ecorr_tc(d, bb, nbatch, ctx->ermax, ctx->ermax_pad, bb, p.weight_bits, ctx->tc_work,
@@ -759,21 +844,27 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
       }
       nl += 1;
     }
-    mark(ctx, kStEcorr);
+    M(kStEcorr);
   }
-  DevStatus hs;
-  CK(cudaMemcpyAsync(&hs, d.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ctx->h_status, d.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+  return ERMOD_OK;
+}
+
+// After the frame's stream work is complete: stage timings and the status word.
+static int frame_finish(ermod_ctx* ctx, bool timed, float total_ms) {
   for (float& t : ctx->timings) t = 0.f;
-  for (int k = 1; k < ctx->pused; ++k) {
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, ctx->pev[k - 1], ctx->pev[k]);
-    ctx->timings[ctx->ptag[k]] += ms;
-    ctx->timings[0] += ms;
+  if (timed) {
+    for (int k = 1; k < ctx->pused; ++k) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ctx->pev[k - 1], ctx->pev[k]);
+      ctx->timings[ctx->ptag[k]] += ms;
+      ctx->timings[0] += ms;
+    }
+  } else {
+    ctx->timings[0] = total_ms;
   }
-  ctx->timings[kStChunks] = (float)((ctx->maxdst + chunk - 1) / chunk);
-  ctx->launches += nl;
+  ctx->timings[kStChunks] = (float)((ctx->maxdst + ctx->chunk - 1) / ctx->chunk);
+  const DevStatus hs = *ctx->h_status;
   if (hs.flags & kErrEngCns) return set_error(ctx, ERMOD_ERR_ENG_CNS, "eng_cns");
   if (hs.flags & kErrEngMin) return set_error(ctx, ERMOD_ERR_ENG_MIN, "eng_min");
   if (hs.flags & kErrEngSft) return set_error(ctx, ERMOD_ERR_ENG_SFT, "eng_sft");
@@ -787,13 +878,81 @@ static int engconst_impl(ermod_ctx* ctx, int stnum, const float* cellin, float w
   return ERMOD_OK;
 }
 
-int32_t ermod_engconst(ermod_ctx* ctx, int32_t stnum, const float* sitepos, const float* cell,
-                       float stat_weight_system, const float* ins_conf, const float* ins_weight, float* flceng) {
-  if (!ctx || !sitepos || !cell) return ERMOD_ERR_ARG;
-  ctx->err.clear();
-  CK(cudaSetDevice(ctx->device));
-  const ermod_params& p = ctx->p;
-  const bool refs = p.slttype != ERMOD_SLT_SOLN;
+// Capture `body` on `st` as a graph and make `*exec` run it: update the
+// existing executable when the topology allows, else instantiate anew.
+template <class Body>
+static cudaError_t capture_graph(cudaStream_t st, cudaGraphExec_t* exec, Body body, int* body_rc) {
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) return e;
+  *body_rc = body();
+  e = cudaStreamEndCapture(st, &graph);
+  if (*body_rc != ERMOD_OK || e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return e != cudaSuccess ? e : cudaErrorUnknown;
+  }
+  if (*exec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(*exec, graph, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(*exec);
+      *exec = nullptr;
+    }
+  }
+  if (!*exec) e = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  return e;
+}
+
+// One frame of one context, its inputs already staged on ctx->st.
+static int engconst_run(ermod_ctx* ctx, int stnum, const float* cellin, float wsys, bool use_conf) {
+  FramePlanHost ph;
+  int rc = frame_plan(ctx, cellin, wsys, use_conf, ph);
+  if (rc != ERMOD_OK) return rc;
+  cudaStream_t st = ctx->st;
+  ctx->h_frame[0] = stnum;
+  CK(cudaMemcpyAsync(ctx->d.frame_i, ctx->h_frame, sizeof(int), cudaMemcpyHostToDevice, st));
+  if (ph.engfac) launch_engfac(ph.k.a, ctx->d, ph.inv, ph.vold, (double)ctx->p.screen, st);
+  const bool timed = ctx->p.stage_timing != 0;
+  const bool graph = !timed && ctx->p.graph_mode == 0 && ctx->real_threads != 0;
+  float total = 0.f;
+  if (!graph) {
+    ctx->pused = 0;
+    if (timed) mark(ctx, 0);
+    else CK(cudaEventRecord(ctx->ev[2], st));
+    long long nl = 0;
+    rc = frame_enqueue(ctx, ph.k, st, timed, nl);
+    if (rc != ERMOD_OK) return rc;
+    if (!timed) CK(cudaEventRecord(ctx->ev[3], st));
+    ctx->launches += nl;
+  } else {
+    if (!ctx->gexec || ctx->gkey.size() != sizeof(FramePlan) ||
+        std::memcmp(ctx->gkey.data(), &ph.k, sizeof(FramePlan)) != 0) {
+      long long nl = 0;
+      int brc = ERMOD_OK;
+      const cudaError_t e =
+          capture_graph(st, &ctx->gexec, [&]() { return frame_enqueue(ctx, ph.k, st, false, nl); }, &brc);
+      if (brc != ERMOD_OK) return brc;
+      CK(e);
+      ctx->gkey.assign((const unsigned char*)&ph.k, (const unsigned char*)&ph.k + sizeof(FramePlan));
+      ctx->graph_launches = nl;
+    }
+    CK(cudaEventRecord(ctx->ev[2], st));
+    CK(cudaGraphLaunch(ctx->gexec, st));
+    CK(cudaEventRecord(ctx->ev[3], st));
+    ctx->launches += ctx->graph_launches;
+  }
+  frame_commit(ctx, cellin, ph);
+  CK(cudaStreamSynchronize(st));
+  CK(cudaGetLastError());
+  if (!timed) CK(cudaEventElapsedTime(&total, ctx->ev[2], ctx->ev[3]));
+  return frame_finish(ctx, timed, total);
+}
+
+// Stage the host inputs of a frame into the context's device buffers.
+static int stage_host_inputs(ermod_ctx* ctx, const float* sitepos, const float* ins_conf, const float* ins_weight,
+                             size_t* nconf_out) {
+  const bool refs = ctx->p.slttype != ERMOD_SLT_SOLN;
   const size_t npos = 3 * (size_t)ctx->natoms;
   const size_t nconf = (refs && ins_conf) ? 3 * (size_t)ctx->s * ctx->maxdst : 0;
   const size_t need = sizeof(float) * (npos + nconf + ctx->maxdst);
@@ -803,6 +962,7 @@ int32_t ermod_engconst(ermod_ctx* ctx, int32_t stnum, const float* sitepos, cons
     CK(cudaMallocHost((void**)&ctx->h_pin, need));
     ctx->h_pin_bytes = need;
   }
+  CK(cudaStreamSynchronize(ctx->st));   // the staging buffer may still feed the previous frame's copies
   std::memcpy(ctx->h_pin, sitepos, sizeof(float) * npos);
   CK(cudaMemcpyAsync(ctx->d.posraw, ctx->h_pin, sizeof(float) * npos, cudaMemcpyHostToDevice, ctx->st));
   if (nconf) {
@@ -812,7 +972,22 @@ int32_t ermod_engconst(ermod_ctx* ctx, int32_t stnum, const float* sitepos, cons
   float* hw = ctx->h_pin + npos + nconf;
   for (int i = 0; i < ctx->maxdst; ++i) hw[i] = (refs && ins_weight) ? ins_weight[i] : 1.0f;
   CK(cudaMemcpyAsync(ctx->d.insw_in, hw, sizeof(float) * ctx->maxdst, cudaMemcpyHostToDevice, ctx->st));
-  const int rc = engconst_impl(ctx, stnum, cell, stat_weight_system, nconf > 0);
+  *nconf_out = nconf;
+  return ERMOD_OK;
+}
+
+extern "C" {
+
+int32_t ermod_engconst(ermod_ctx* ctx, int32_t stnum, const float* sitepos, const float* cell,
+                       float stat_weight_system, const float* ins_conf, const float* ins_weight, float* flceng) {
+  if (!ctx || !sitepos || !cell) return ERMOD_ERR_ARG;
+  ctx->err.clear();
+  CK(cudaSetDevice(ctx->device));
+  const bool refs = ctx->p.slttype != ERMOD_SLT_SOLN;
+  size_t nconf = 0;
+  int rc = stage_host_inputs(ctx, sitepos, ins_conf, ins_weight, &nconf);
+  if (rc != ERMOD_OK) return rc;
+  rc = engconst_run(ctx, stnum, cell, stat_weight_system, nconf > 0);
   if (rc < 0) return rc;
   if (flceng && !refs) {
     std::vector<double> f((size_t)ctx->maxdst * ctx->numslv);
@@ -832,14 +1007,204 @@ int32_t ermod_engconst_dev(ermod_ctx* ctx, int32_t stnum, const float* sitepos_d
   if (refs && ins_conf_dev)
     CK(cudaMemcpyAsync(ctx->d.ins_conf, ins_conf_dev, sizeof(float) * 3 * ctx->s * ctx->maxdst,
                        cudaMemcpyDeviceToDevice, ctx->st));
-  if (refs && ins_weight_dev) {
+  if (refs && ins_weight_dev)
     CK(cudaMemcpyAsync(ctx->d.insw_in, ins_weight_dev, sizeof(float) * ctx->maxdst, cudaMemcpyDeviceToDevice, ctx->st));
-  } else {
-    std::vector<float> one(ctx->maxdst, 1.0f);
-    CK(cudaMemcpyAsync(ctx->d.insw_in, one.data(), sizeof(float) * ctx->maxdst, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+  else
+    launch_fill(ctx->d.insw_in, 1.0f, ctx->maxdst, ctx->st);
+  return engconst_run(ctx, stnum, cell, stat_weight_system, refs && ins_conf_dev);
+}
+
+// ---- batches of contexts: one graph launch per frame ---------------------
+//
+// Solutes of different sizes share one solvent frame: every member context
+// runs its own unchanged pipeline on its own stream, and the frame of all
+// members is captured as ONE CUDA graph with a branch per member, launched
+// once per frame.  Each member's results are bit-identical to calling
+// ermod_engconst on it alone: the same kernels with the same arguments, no
+// state shared between members, every reduction in a fixed order.
+
+}  // extern "C"
+
+struct ermod_batch {
+  int device = 0;
+  std::vector<ermod_ctx*> m;
+  cudaStream_t st = nullptr;
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<unsigned char> gkey;
+  std::vector<long long> member_launches;   // kernel launches of each member in the captured graph
+  float* h_pos = nullptr;
+  float* d_pos = nullptr;
+  size_t npos = 0;
+  float last_ms = 0.f;
+  int failed = -1;
+  std::string err;
+};
+
+extern "C" {
+
+int32_t ermod_batch_create(ermod_batch** out, int32_t n, ermod_ctx* const* members) {
+  if (!out || n <= 0 || !members) return ERMOD_ERR_ARG;
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!members[i]) return ERMOD_ERR_ARG;
+    if (members[i]->device != members[0]->device || members[i]->natoms != members[0]->natoms)
+      return ERMOD_ERR_ARG;   // members share the device and the solvent frame
+    for (int j = 0; j < i; ++j)
+      if (members[j] == members[i]) return ERMOD_ERR_ARG;
   }
-  return engconst_impl(ctx, stnum, cell, stat_weight_system, refs && ins_conf_dev);
+  ermod_batch* b = new ermod_batch();
+  b->device = members[0]->device;
+  b->m.assign(members, members + n);
+  b->npos = 3 * (size_t)members[0]->natoms;
+  auto fail = [&]() {
+    ermod_batch_destroy(b);
+    return ERMOD_ERR_CUDA;
+  };
+  if (cudaSetDevice(b->device) != cudaSuccess) return fail();
+  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess) return fail();
+  if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) return fail();
+  if (cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess) return fail();
+  b->join.resize(n, nullptr);
+  b->member_launches.assign(n, 0);
+  for (auto& e : b->join)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail();
+  if (cudaMallocHost((void**)&b->h_pos, sizeof(float) * std::max<size_t>(b->npos, 1)) != cudaSuccess) return fail();
+  if (cudaMalloc((void**)&b->d_pos, sizeof(float) * std::max<size_t>(b->npos, 1)) != cudaSuccess) return fail();
+  *out = b;
+  return ERMOD_OK;
+}
+
+static int batch_run(ermod_batch* b, int stnum, const float* cell, float wsys) {
+  const int n = (int)b->m.size();
+  b->failed = -1;
+  b->err.clear();
+  auto fail_member = [&](int i, int rc) {
+    b->failed = i;
+    b->err = "member " + std::to_string(i) + ": " + b->m[i]->err;
+    return rc;
+  };
+  std::vector<FramePlanHost> ph(n);
+  bool tuned = true;
+  for (int i = 0; i < n; ++i) {
+    ermod_ctx* ctx = b->m[i];
+    ctx->err.clear();
+    const int rc = frame_plan(ctx, cell, wsys, false, ph[i]);
+    if (rc != ERMOD_OK) return fail_member(i, rc);
+    if (ctx->real_threads == 0) tuned = false;
+  }
+  // stage every member's inputs on the batch stream, ahead of the graph
+  for (int i = 0; i < n; ++i) {
+    ermod_ctx* ctx = b->m[i];
+    if (cudaMemcpyAsync(ctx->d.posraw, b->d_pos, sizeof(float) * b->npos, cudaMemcpyDeviceToDevice, b->st) !=
+        cudaSuccess)
+      return ERMOD_ERR_CUDA;
+    ctx->h_frame[0] = stnum;
+    if (cudaMemcpyAsync(ctx->d.frame_i, ctx->h_frame, sizeof(int), cudaMemcpyHostToDevice, b->st) != cudaSuccess)
+      return ERMOD_ERR_CUDA;
+    launch_fill(ctx->d.insw_in, 1.0f, ctx->maxdst, b->st);
+    if (ph[i].engfac) launch_engfac(ph[i].k.a, ctx->d, ph[i].inv, ph[i].vold, (double)ctx->p.screen, b->st);
+  }
+  if (cudaEventRecord(b->t0, b->st) != cudaSuccess) return ERMOD_ERR_CUDA;
+  if (!tuned) {
+    // first frame: direct launches on the member streams (the autotuner runs here)
+    if (cudaEventRecord(b->fork, b->st) != cudaSuccess) return ERMOD_ERR_CUDA;
+    for (int i = 0; i < n; ++i) {
+      ermod_ctx* ctx = b->m[i];
+      if (cudaStreamWaitEvent(ctx->st, b->fork, 0) != cudaSuccess) return ERMOD_ERR_CUDA;
+      long long nl = 0;
+      ctx->pused = 0;
+      const int rc = frame_enqueue(ctx, ph[i].k, ctx->st, false, nl);
+      if (rc != ERMOD_OK) return fail_member(i, rc);
+      ctx->launches += nl;
+      if (cudaEventRecord(b->join[i], ctx->st) != cudaSuccess) return ERMOD_ERR_CUDA;
+      if (cudaStreamWaitEvent(b->st, b->join[i], 0) != cudaSuccess) return ERMOD_ERR_CUDA;
+    }
+  } else {
+    std::vector<unsigned char> key;
+    for (int i = 0; i < n; ++i)
+      key.insert(key.end(), (const unsigned char*)&ph[i].k, (const unsigned char*)&ph[i].k + sizeof(FramePlan));
+    if (!b->gexec || key != b->gkey) {
+      long long nl = 0;
+      (void)nl;
+      int brc = ERMOD_OK, bad = -1;
+      const cudaError_t e = capture_graph(b->st, &b->gexec, [&]() {
+        if (cudaEventRecord(b->fork, b->st) != cudaSuccess) return (int)ERMOD_ERR_CUDA;
+        for (int i = 0; i < n; ++i) {
+          ermod_ctx* ctx = b->m[i];
+          if (cudaStreamWaitEvent(ctx->st, b->fork, 0) != cudaSuccess) return (int)ERMOD_ERR_CUDA;
+          long long nli = 0;
+          const int rc = frame_enqueue(ctx, ph[i].k, ctx->st, false, nli);
+          if (rc != ERMOD_OK) { bad = i; return rc; }
+          b->member_launches[i] = nli;
+          nl += nli;
+          if (cudaEventRecord(b->join[i], ctx->st) != cudaSuccess) return (int)ERMOD_ERR_CUDA;
+          if (cudaStreamWaitEvent(b->st, b->join[i], 0) != cudaSuccess) return (int)ERMOD_ERR_CUDA;
+        }
+        return (int)ERMOD_OK;
+      }, &brc);
+      if (brc != ERMOD_OK) return bad >= 0 ? fail_member(bad, brc) : brc;
+      if (e != cudaSuccess) {
+        b->err = std::string("cuda: ") + cudaGetErrorString(e);
+        return ERMOD_ERR_CUDA;
+      }
+      b->gkey = key;
+    }
+    if (cudaGraphLaunch(b->gexec, b->st) != cudaSuccess) return ERMOD_ERR_CUDA;
+    for (int i = 0; i < n; ++i) b->m[i]->launches += b->member_launches[i];
+  }
+  if (cudaEventRecord(b->t1, b->st) != cudaSuccess) return ERMOD_ERR_CUDA;
+  for (int i = 0; i < n; ++i) frame_commit(b->m[i], cell, ph[i]);
+  if (cudaStreamSynchronize(b->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ERMOD_ERR_CUDA;
+  cudaEventElapsedTime(&b->last_ms, b->t0, b->t1);
+  int worst = ERMOD_OK;
+  for (int i = 0; i < n; ++i) {
+    const int rc = frame_finish(b->m[i], false, b->last_ms);
+    if (rc < 0) return fail_member(i, rc);
+    if (rc > 0 && worst == ERMOD_OK) { worst = rc; b->failed = i; b->err = "member " + std::to_string(i) + ": " + b->m[i]->err; }
+  }
+  return worst;
+}
+
+int32_t ermod_batch_engconst(ermod_batch* b, int32_t stnum, const float* sitepos, const float* cell,
+                             float stat_weight_system) {
+  if (!b || !sitepos || !cell) return ERMOD_ERR_ARG;
+  if (cudaSetDevice(b->device) != cudaSuccess) return ERMOD_ERR_CUDA;
+  if (cudaStreamSynchronize(b->st) != cudaSuccess) return ERMOD_ERR_CUDA;
+  std::memcpy(b->h_pos, sitepos, sizeof(float) * b->npos);
+  if (cudaMemcpyAsync(b->d_pos, b->h_pos, sizeof(float) * b->npos, cudaMemcpyHostToDevice, b->st) != cudaSuccess)
+    return ERMOD_ERR_CUDA;
+  return batch_run(b, stnum, cell, stat_weight_system);
+}
+
+int32_t ermod_batch_engconst_dev(ermod_batch* b, int32_t stnum, const float* sitepos_dev, const float* cell,
+                                 float stat_weight_system) {
+  if (!b || !sitepos_dev || !cell) return ERMOD_ERR_ARG;
+  if (cudaSetDevice(b->device) != cudaSuccess) return ERMOD_ERR_CUDA;
+  if (cudaMemcpyAsync(b->d_pos, sitepos_dev, sizeof(float) * b->npos, cudaMemcpyDeviceToDevice, b->st) !=
+      cudaSuccess)
+    return ERMOD_ERR_CUDA;
+  return batch_run(b, stnum, cell, stat_weight_system);
+}
+
+float ermod_batch_last_ms(const ermod_batch* b) { return b ? b->last_ms : -1.f; }
+
+const char* ermod_batch_last_error(const ermod_batch* b) { return b ? b->err.c_str() : "null"; }
+
+void ermod_batch_destroy(ermod_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->st) cudaStreamSynchronize(b->st);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  for (auto e : b->join) if (e) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->t0) cudaEventDestroy(b->t0);
+  if (b->t1) cudaEventDestroy(b->t1);
+  if (b->h_pos) cudaFreeHost(b->h_pos);
+  if (b->d_pos) cudaFree(b->d_pos);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
 }
 
 int32_t ermod_fetch_accum(ermod_ctx* ctx, ermod_accum* o) {

@@ -110,17 +110,19 @@ struct DeviceState {
   float* maxuv = nullptr;    // [numslv+1]
   double* scal = nullptr;    // [8]: avslf, engnorm, engsmpl, voffset, voffset_init, usreal, usreal_init
   DevStatus* status = nullptr;
+  int* frame_i = nullptr;    // [4] per-frame scalars staged before the frame: [0] stnum
 };
 
 // ---- launchers (kernels.cu) -------------------------------------------
 void launch_prepare_solvent(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
 void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStream_t s);
-void launch_insert(const FrameArgs& a, const DeviceState& d, int stnum, int iseed, int insposition,
+void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, int insposition,
                    int insorient, int use_conf, cudaStream_t s);
 void launch_targets_soln(const FrameArgs& a, const DeviceState& d, const int* tgt_k_host_dev, cudaStream_t s);
 void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int count, double screen,
                      cudaStream_t s);
-void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
+void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, int threads, cudaStream_t s);
+void launch_fill(float* p, float v, int n, cudaStream_t s);
 void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[3][3], double volume,
                    double screen, cudaStream_t s);
 void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);

@@ -69,6 +69,15 @@ __global__ void k_prepare_solvent(FrameArgs a, const float* __restrict__ posraw,
   slvn[i] = make_float4(nx, ny, nz, atom_q[i]);
 }
 
+__global__ void k_fill(float* __restrict__ p, float v, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+void launch_fill(float* p, float v, int n, cudaStream_t s) {
+  if (n > 0) k_fill<<<(n + 255) / 256, 256, 0, s>>>(p, v, n);
+}
+
 void launch_prepare_solvent(const FrameArgs& a, const DeviceState& d, cudaStream_t s) {
   if (a.natoms <= 0) return;
   k_prepare_solvent<<<(a.natoms + 255) / 256, 256, 0, s>>>(a, d.posraw, d.atom_q, d.slvn, d.spl, d.grd);
@@ -200,13 +209,15 @@ __device__ void finish_target(const FrameArgs& a, int cnt, float4* __restrict__ 
   ctr[cnt] = make_float4(c.x, c.y, c.z, rad);
 }
 
-__global__ void k_insert(FrameArgs a, int stnum, int iseed, int insposition, int insorient, int use_conf,
+__global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int iseed, int insposition, int insorient,
+                         int use_conf,
                          const float* __restrict__ conf_all, const float* __restrict__ bfcoord,
                          const float* __restrict__ mass, const float* __restrict__ qsite,
                          float4* __restrict__ tgt_raw, float4* __restrict__ tgt_n, float4* __restrict__ tgt_c) {
   const int cnt = blockIdx.x * blockDim.x + threadIdx.x;
   if (cnt >= a.maxdst) return;
   const int s = a.nsite;
+  const int stnum = *stnum_dev;   // staged per frame, so a captured frame graph replays with the new value
   float4* out = tgt_raw + (size_t)cnt * s;
   const float* conf = use_conf ? conf_all + (size_t)3 * s * cnt : bfcoord;
   float msum = 0.0f;
@@ -266,9 +277,9 @@ __global__ void k_insert(FrameArgs a, int stnum, int iseed, int insposition, int
   finish_target(a, cnt, out, tgt_n + (size_t)cnt * s, tgt_c, qsite);
 }
 
-void launch_insert(const FrameArgs& a, const DeviceState& d, int stnum, int iseed, int insposition, int insorient,
-                   int use_conf, cudaStream_t s) {
-  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum, iseed, insposition, insorient, use_conf, d.ins_conf,
+void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, int insposition,
+                   int insorient, int use_conf, cudaStream_t s) {
+  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum_dev, iseed, insposition, insorient, use_conf, d.ins_conf,
                                                     d.bfcoord, d.slt_mass, d.slt_q, d.tgt_raw, d.tgt_n, d.tgt_c);
 }
 
@@ -333,9 +344,9 @@ void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int co
 // real space: one CTA per target, a warp per candidate molecule, lanes over
 // the site pairs, FP64 warp-shuffle reduction of the molecule sum
 // ---------------------------------------------------------------------------
-constexpr int kRealThreads = 256;
+constexpr int kRealMaxThreads = 512;
 
-__global__ void __launch_bounds__(kRealThreads) k_real(FrameArgs a, int base, int chunk,
+__global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base, int chunk,
     const float4* __restrict__ tgt_n, const float4* __restrict__ tgt_c, const int* __restrict__ tgt_mol,
     const int* __restrict__ slt_lj_tab, const int* __restrict__ molbeg, const float4* __restrict__ slvn,
     const int* __restrict__ atom_lj, const float* __restrict__ ljene, const float* __restrict__ ljlensq,
@@ -412,10 +423,14 @@ __global__ void __launch_bounds__(kRealThreads) k_real(FrameArgs a, int base, in
   }
 }
 
-void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
+// `threads` (a multiple of 32, <= kRealMaxThreads) only changes how many warps
+// share a target's molecules: each molecule's energy is one warp's fixed-order
+// sum whatever the block size.
+void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, int threads, cudaStream_t s) {
   cudaMemsetAsync(d.E, 0, sizeof(double) * (size_t)a.slvmax * chunk, s);
   if (nb <= 0) return;  // `chunk` is the row stride of E: the batch size
-  k_real<<<nb, kRealThreads, 0, s>>>(a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, d.slt_lj, d.molbeg, d.slvn,
+  if (threads <= 0 || threads > kRealMaxThreads || threads % 32) threads = 256;
+  k_real<<<nb, threads, 0, s>>>(a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, d.slt_lj, d.molbeg, d.slvn,
                                       d.atom_lj, d.ljene, d.ljlensq, d.anchor, d.cellstart, d.molsorted, d.rmol, d.E);
 }
 

@@ -152,8 +152,6 @@ __device__ __forceinline__ void fft_batch(float2* buf, const float2* __restrict_
   fft_stages<S, 0, NTHR, INV>(buf, tw, tid);
 }
 
-__device__ __forceinline__ int ilog2(int x) { return 31 - __clz(x); }
-
 constexpr int kSiteTile = 32;                  // solute sites staged in shared memory at a time (at most)
 constexpr int kTabPairs = 8;                   // (target, site) pairs per CTA of k_site_tables
 constexpr int kStn = 2 + 2 * kMaxOrder;        // stencil record: g2, g3, w2[kMaxOrder], w3[kMaxOrder]

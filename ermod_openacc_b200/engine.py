@@ -166,8 +166,54 @@ class Engine:
     def launch_count(self) -> int:
         return int(self.lib.ermod_get_launch_count(self.ctx))
 
+    def last_ms(self) -> float:
+        """Device time of the last frame (the stage timings' total)."""
+        return self.timings()["total"]
+
     def paths(self) -> dict:
         """Resolved kernel choices: spectrum_path 1 cuFFT / 2 fused direct / 3 fused spread, ecorr_path."""
         sp, ep = C.c_int32(), C.c_int32()
         self._check(self.lib.ermod_get_paths(self.ctx, C.byref(sp), C.byref(ep)))
         return dict(spectrum_path=sp.value, ecorr_path=ep.value)
+
+
+class Batch:
+    """Solutes sharing one solvent frame, run as one CUDA-graph launch per frame
+    (ermod_batch_*).  Each member Engine keeps its own accumulators, bit-identical
+    to running it alone."""
+
+    def __init__(self, members: list[Engine]):
+        self.lib = A.load_library()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.ctx.value for m in self.members])
+        self.h = C.c_void_p()
+        rc = self.lib.ermod_batch_create(C.byref(self.h), len(self.members), arr)
+        if rc != 0:
+            raise ErmodError(rc, "batch")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ermod_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def engconst(self, stnum: int, sitepos, cell, stat_weight_system: float = 1.0) -> int:
+        sp, cl = A.as_f32(sitepos), A.as_f32(cell)
+        rc = self.lib.ermod_batch_engconst(self.h, stnum, A.ptr(sp, C.c_float), A.ptr(cl, C.c_float),
+                                           stat_weight_system)
+        if rc < 0:
+            raise ErmodError(rc, self.lib.ermod_batch_last_error(self.h).decode())
+        return rc
+
+    def engconst_dev(self, stnum: int, sitepos_ptr: int, cell, stat_weight_system: float = 1.0) -> int:
+        cl = A.as_f32(cell)
+        rc = self.lib.ermod_batch_engconst_dev(self.h, stnum, C.c_void_p(sitepos_ptr), A.ptr(cl, C.c_float),
+                                               stat_weight_system)
+        if rc < 0:
+            raise ErmodError(rc, self.lib.ermod_batch_last_error(self.h).decode())
+        return rc
+
+    def last_ms(self) -> float:
+        return float(self.lib.ermod_batch_last_ms(self.h))

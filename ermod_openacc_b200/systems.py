@@ -256,7 +256,7 @@ def default_params(**kw) -> dict:
              corrcal=1, selfcal=0, wgtslf=1, insposition=A.INSPOS_RANDOM, insorient=A.INSROT_RANDOM,
              iseed=123456789, temp=300.0 * KB_KCAL, elecut=12.0, lwljcut=10.0, upljcut=12.0, screen=0.35,
              ins_chunk=0, ecorr_batch=0, weight_bits=0, proposal=A.PROPOSAL_UNIFORM,
-             keep_uvengy=0, ecorr_path=0, spectrum_path=0)
+             keep_uvengy=0, ecorr_path=0, spectrum_path=0, graph_mode=0, stage_timing=0)
     p.update(kw)
     for k in ("ms2max", "ms3max"):
         if k not in kw:
@@ -345,3 +345,23 @@ def make_workload(config: int, small: bool = False, maxins: int | None = None, s
         prm = default_params(ms1max=K, maxins=mi)
         return Workload("precision-chain60-water32768", prm, topo, dict(ecdmin=-80.0), box, nside, 10, seed)
     raise ValueError(config)
+
+
+def make_batch_workloads(nsolutes: int = 64, small: bool = False, maxins=None, seed: int = 7,
+                         site_range=(10, 300)) -> list[Workload]:
+    """Configuration 4: `nsolutes` rigid solutes of seeded sizes U[site_range] built with the ring
+    recipe, each with its own insertion stream, all sharing the configuration-2 water box and frames.
+    `maxins` may be an int or one count per solute."""
+    rng = np.random.default_rng(seed + 404)
+    sizes = rng.integers(site_range[0], site_range[1] + 1, size=nsolutes)
+    base = make_workload(4, small=small, seed=seed)
+    counts = [maxins] * nsolutes if maxins is None or np.isscalar(maxins) else list(maxins)
+    out = []
+    for j, n in enumerate(sizes):
+        slt = ring_recipe_solute(int(n), seed * 7919 + j)
+        topo = Topology([water(), slt], [base.nside ** 3, 1], [A.PT_SOLVENT, A.PT_TEST_RIGID])
+        prm = dict(base.params, iseed=int(base.params["iseed"]) + j)
+        if counts[j] is not None:
+            prm["maxins"] = int(counts[j])
+        out.append(Workload(f"batch{j}-s{int(n)}", prm, topo, {}, base.box, base.nside, base.nframes, seed))
+    return out

@@ -111,7 +111,11 @@ typedef struct ermod_params {
                                      2: fused solve, spectrum by direct site sums,
                                      3: fused solve, spectrum by plane spreading + FFT
                                      (2 and 3 need power-of-two meshes of 16..128) */
-  int32_t reserved[5];
+  int32_t graph_mode;             /* 0: a frame runs as one CUDA graph launch (captured again
+                                     only when the frame's constants change), 1: direct launches */
+  int32_t stage_timing;           /* 1: CUDA events between stages for ermod_get_timings
+                                     (implies direct launches); 0: total frame time only */
+  int32_t reserved[3];
 } ermod_params;
 
 /*
@@ -277,6 +281,30 @@ int32_t ermod_get_paths(const ermod_ctx* ctx, int32_t* spectrum_path, int32_t* e
 int64_t ermod_get_launch_count(const ermod_ctx* ctx);
 
 void ermod_destroy(ermod_ctx* ctx);
+
+/*
+ * Batches of solutes sharing one solvent frame (no reference counterpart).
+ * `members` are contexts created by ermod_create on one device for the same
+ * solvent (same numatm_phys), each with its own solute, insertion count and
+ * options.  ermod_batch_engconst runs the frame of every member as ONE
+ * CUDA-graph launch with a branch per member; each member's results are
+ * bit-identical to calling ermod_engconst on that member alone with the
+ * same inputs, and are read with the member functions (ermod_fetch_accum,
+ * ermod_engstore, ermod_get_uvengy, ...).  Refs-mode members use their rigid
+ * solute (no per-insertion conformations).  The batch does not own the
+ * members; destroy it before them.
+ */
+typedef struct ermod_batch ermod_batch;
+int32_t ermod_batch_create(ermod_batch** out, int32_t n, ermod_ctx* const* members);
+int32_t ermod_batch_engconst(ermod_batch* b, int32_t stnum, const float* sitepos, const float* cell,
+                             float stat_weight_system);
+int32_t ermod_batch_engconst_dev(ermod_batch* b, int32_t stnum, const float* sitepos_dev, const float* cell,
+                                 float stat_weight_system);
+/* Device time (ms) of the last batch frame, CUDA events around the graph launch. */
+float ermod_batch_last_ms(const ermod_batch* b);
+/* "member <i>: <code>" for the first member that failed in the last call, "" if none. */
+const char* ermod_batch_last_error(const ermod_batch* b);
+void ermod_batch_destroy(ermod_batch* b);
 
 /*
  * Energy histogram without device allocation.  No counterpart in the
