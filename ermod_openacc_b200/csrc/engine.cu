@@ -1241,6 +1241,9 @@ int32_t ermod_engstore(ermod_ctx* ctx, ermod_accum* o, double* avediv) {
   if (o->edens) for (int i = 0; i < ctx->ermax; ++i) o->edens[i] /= nrm;
   if (o->ecorr && ctx->d.ecorr) for (size_t i = 0; i < (size_t)ctx->ermax * ctx->ermax; ++i) o->ecorr[i] /= nrm;
   if (o->eself && ctx->p.selfcal) for (int i = 0; i < ctx->esmax; ++i) o->eself[i] /= nrm;
+  // soln: aveuv(division, :) = slnuv / engnorm (engproc.F90:622), returned in slnuv
+  if (o->slnuv && ctx->p.slttype == ERMOD_SLT_SOLN)
+    for (int i = 0; i < ctx->numslv; ++i) o->slnuv[i] = (float)((double)o->slnuv[i] / nrm);
   const double avslf = o->avslf / nrm;
   if (avediv) {
     avediv[0] = o->engnorm / o->engsmpl;

@@ -1,0 +1,179 @@
+"""Solvation free energy from the energy distributions (slvfe's chmpot).
+
+The downstream step of erdst: slvfe (slvfe/slvfe.F90) turns the solution
+distribution rho (engsln), the reference-solvent distribution rho0 (engref)
+and correlation chi0 (corref) into the solvation free energy with the
+energy-representation functional.  This module evaluates that functional for
+one data set with slvfe's defaults (slvfe/sfemain.F90:22-64):
+
+  functional 'py-hnc', invmtrx 'reg', zerosft 'eczr', wgtfnform 'harm',
+  extsln 'lin', extthres 1, minthres 0, normalize 'yes', slncor 'not',
+  ljlrc 'not', uvread 'yes' (aveuv given), no bin merging (group 1, inft 0).
+
+Steps (slvfe.F90 line ranges):
+  distnorm   1467-1542  rho, rho0 scaled to N per species; chi0 made
+                        consistent with rho0 by the fixed-point row scaling
+  getslncv   875-1001   omega_sln = -kT log(rho/rho0) - eps, linear
+                        extrapolation into bins sampled on one side only
+  getinscv   1003-1232  omega_ref from (chi0 - rho0 rho0^T + reg) x =
+                        -kT (rho - rho0), Cholesky solve
+  chmpot     744-803    the PY/HNC-interpolated functional per species
+
+The arithmetic is FP64 on the host (the reference uses FP32).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+__all__ = ["kT_of", "delta_mu"]
+
+
+def kT_of(temp_K: float) -> float:
+    """kT in kcal/mol as slvfe computes it (slvfe.F90:272)."""
+    return temp_K * 8.314510e-3 / 4.184
+
+
+def _pyhnc_soln(f):
+    with np.errstate(over="ignore", invalid="ignore", divide="ignore"):
+        py = f + f / (np.exp(-f) - 1.0) + 1.0
+    return np.where(f < 0.0, py, f / 2.0)
+
+
+def _pyhnc_refs(f):
+    with np.errstate(invalid="ignore", divide="ignore"):
+        py = np.log1p(-f) * (1.0 / f - 1.0) + 1.0
+    return np.where(f < 0.0, py, f / 2.0)
+
+
+def _normalise(edist, edens, ecorr, spec, nummol, tol=1.0e-8, itrmax=100):
+    """distnorm: per-species scaling of rho and rho0, and the row scaling of chi0
+    (a Gauss-Seidel sweep over the bins, as slvfe.F90:1503-1525 updates in place)."""
+    rho = edist.copy()
+    rho0 = edens.copy()
+    nsp = len(nummol)
+    masks = [spec == p for p in range(1, nsp + 1)]
+    for p, m in enumerate(masks):
+        s = rho[m].sum()
+        rho[m] *= nummol[p] / s if s > 0.0 else 0.0
+        s0 = rho0[m].sum()
+        rho0[m] *= nummol[p] / s0 if s0 > 0.0 else 0.0
+    chi = ecorr.copy()
+    corr = np.ones(len(rho0))
+    for it in range(itrmax + 1):
+        for i in range(len(rho0)):
+            acc = 0.0
+            for p, m in enumerate(masks):
+                a = float(np.dot(corr[m], chi[m, i]))
+                if a > 0.0:
+                    acc += nummol[p] / a
+            corr[i] = acc / nsp * rho0[i]
+        chi *= np.outer(corr, corr)
+        err = np.max(np.abs(corr - 1.0)[rho0 > 0.0])
+        if err <= tol:
+            return rho, rho0, chi
+        if it + 1 >= itrmax:
+            break
+    raise RuntimeError(f"chi0 normalisation did not converge (max correction {err:.3e})")
+
+
+def _zero_bin(crd, dens, mask, tiny=1.0e-8):
+    idx = np.nonzero(mask)[0]
+    k = None
+    for a, b in zip(idx[:-1], idx[1:]):
+        if b != a + 1 or not (crd[a] <= 0.0 <= crd[b]):
+            continue
+        lo, hi = abs(crd[a]), crd[b]
+        if hi > lo + tiny:
+            k = a
+        elif hi < lo - tiny:
+            k = b
+        else:
+            k = a if dens[a] >= dens[b] else b
+    if k is None:
+        raise ValueError("the energy mesh has no bin pair around zero")
+    return k
+
+
+def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0):
+    """(per-species solvation free energies, total) in kcal/mol.
+
+    edist: rho (solution, engstore-normalised); edens, ecorr: rho0 and chi0
+    (reference solvent); uvcrd: bin coordinates; uvspec: 1-based species of
+    each bin; aveuv: average solute-solvent energy per species in solution;
+    slfeng: solute self energy (slfslt = 'yes')."""
+    rd = np.asarray(edist, dtype=np.float64)
+    rr = np.asarray(edens, dtype=np.float64)
+    cr = np.asarray(ecorr, dtype=np.float64)
+    crd = np.asarray(uvcrd, dtype=np.float64)
+    spec = np.asarray(uvspec)
+    nsp = int(spec.max())
+    n = len(rd)
+    kT = kT_of(temp_K)
+    nummol = [float(np.rint(rd[spec == p].sum())) for p in range(1, nsp + 1)]
+    rho, rho0, chi = _normalise(rd, rr, cr, spec, nummol)
+    # omega in solution: direct where both distributions are sampled
+    ratio_s = np.minimum(rho / rd[rd > 0.0].min(), 10.0)
+    ratio_r = np.minimum(rho0 / rr[rr > 0.0].min(), 10.0)
+    both = (np.rint(ratio_s) >= 1) & (np.rint(ratio_r) >= 1)
+    omega = np.zeros(n)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        omega[both] = -kT * np.log(rho[both] / rho0[both]) - crd[both]
+    hsum = rho + rho0
+    harm = np.where(hsum > 0.0, rho * rho0 / np.where(hsum > 0.0, hsum, 1.0), 0.0)
+    for i in np.nonzero(~both)[0]:
+        if rho[i] <= 0.0:
+            omega[i] = 0.0
+            continue
+        same = (spec == spec[i]) & both
+        lower = np.nonzero(same[:i])[0]
+        upper = np.nonzero(same[i + 1:])[0] + i + 1
+        m = lower[-1] if len(lower) else 0
+        k = upper[0] if len(upper) else n - 1
+        if both[m] and both[k]:
+            j = m if abs(m - i) < abs(k - i) else k
+        elif both[m] or both[k]:
+            j = m if both[m] else k
+        else:
+            raise ValueError(f"cannot extrapolate omega at energy {crd[i]}")
+        sel = np.nonzero(same)[0]
+        shift = crd[sel] - crd[j]
+        shift = np.where(sel < i, -shift - 2.0 * (crd[j] - crd[i]), shift)
+        w = np.exp(-shift / kT) * harm[sel]
+        keep = w > 0.0
+        sel, w = sel[keep], w[keep] / w[keep].sum()
+        x, y = crd[sel], omega[sel]
+        m1, m2 = np.dot(w, x), np.dot(w, x * x)
+        c0 = (m2 * np.dot(w, y) - m1 * np.dot(w, x * y)) / (m2 - m1 * m1)
+        c1 = (np.dot(w, x * y) - m1 * np.dot(w, y)) / (m2 - m1 * m1)
+        omega[i] = c0 + c1 * crd[i]
+    # omega in the reference solvent: regularised correlation solve
+    pos = rho0 > 0.0
+    A = np.where(np.outer(pos, pos), chi - np.outer(rho0, rho0), 0.0)
+    A[~pos, ~pos] = 1.0
+    A[np.diag_indices(n)] = np.where(pos, np.diag(A), 1.0)
+    ddiff = -kT * (rho - rho0)
+    rhs = np.where(pos, ddiff, 0.0)
+    Areg = A.copy()
+    for p in range(1, nsp + 1):
+        sp = pos & (spec == p)
+        reg = np.trace(A[np.ix_(sp, sp)]) / sp.sum() ** 2
+        Areg[np.ix_(sp, sp)] += reg
+    try:
+        L = np.linalg.cholesky(Areg)
+        x = np.linalg.solve(L.T, np.linalg.solve(L, rhs))
+    except np.linalg.LinAlgError:
+        val, vec = np.linalg.eigh(A)
+        coef = (vec[pos, nsp:].T @ ddiff[pos]) / val[nsp:]
+        x = vec[:, nsp:] @ coef
+    zero_x = np.array([x[_zero_bin(crd, rho0, spec == p)] for p in range(1, nsp + 1)])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        omega0 = np.where(pos, ddiff / np.where(pos, rho0, 1.0) - x, 0.0)
+    omega0 += zero_x[spec - 1]
+    # the functional
+    live = (rho > 0.0) | (rho0 > 0.0)
+    lcent = -(omega + crd)
+    w = np.where(rho >= rho0, 1.0, 1.0 - ((rho - rho0) / np.where(hsum > 0.0, hsum, 1.0)) ** 2)
+    fac = w * _pyhnc_soln(omega / kT) + (1.0 - w) * _pyhnc_refs(omega0 / kT)
+    terms = -kT * (rho - rho0) + lcent * rho + kT * fac * (rho - rho0)
+    chmpt = np.array([terms[live & (spec == p)].sum() for p in range(1, nsp + 1)]) + np.asarray(aveuv)
+    return chmpt, float(chmpt.sum() + slfeng)

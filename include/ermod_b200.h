@@ -230,7 +230,8 @@ int32_t ermod_fetch_accum(ermod_ctx* ctx, ermod_accum* out);
  * divided by engnorm, avslf / engnorm, and the two avediv entries
  * avediv(division,1) = engnorm/engsmpl,
  * avediv(division,2) = voffset -/+ temp*log(avslf)  (soln / refs).
- * Writes the normalised arrays into `out` (same members as ermod_fetch_accum)
+ * Writes the normalised arrays into `out` (same members as ermod_fetch_accum;
+ * in soln mode `slnuv` receives aveuv = slnuv / engnorm, engproc.F90:622)
  * and avediv[2].  Does not clear the accumulators (call ermod_engclear).
  */
 int32_t ermod_engstore(ermod_ctx* ctx, ermod_accum* out, double* avediv);

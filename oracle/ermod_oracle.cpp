@@ -984,7 +984,7 @@ template <class T> struct Oracle {
     if (o->edens) for (int i = 0; i < ermax; ++i) o->edens[i] = edens[i] / nrm;
     if (o->ecorr && p.corrcal) for (size_t i = 0; i < ecorr.size(); ++i) o->ecorr[i] = ecorr[i] / nrm;
     if (o->eself && p.selfcal) for (int i = 0; i < esmax; ++i) o->eself[i] = eself[i] / nrm;
-    if (o->slnuv) for (int i = 0; i < numslv; ++i) o->slnuv[i] = (float)slnuv[i];
+    if (o->slnuv) for (int i = 0; i < numslv; ++i) o->slnuv[i] = (float)(slnuv[i] / nrm);   // aveuv (engproc.F90:622)
     if (o->minuv) for (int i = 0; i <= numslv; ++i) o->minuv[i] = (float)minuv[i];
     if (o->maxuv) for (int i = 0; i <= numslv; ++i) o->maxuv[i] = (float)maxuv[i];
     o->avslf = avslf / nrm;

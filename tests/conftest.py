@@ -25,3 +25,9 @@ def engine_lib():
     ge.build_engine()
     from ermod_openacc_b200 import _capi
     return _capi.load_library()
+
+
+@pytest.fixture(scope="session")
+def slvfe_oracle():
+    import slvfe_oracle
+    return slvfe_oracle

@@ -1,0 +1,75 @@
+"""slvfe's free-energy functional: product module against the restatement.
+
+ermod_openacc_b200.slvfe (vectorised, the library's downstream step) and
+oracle/slvfe_oracle.py (slvfe.F90 restated loop by loop) must agree on
+energy distributions produced by the FP64 oracle engine, and both must
+satisfy the identities the functional has by construction.
+"""
+import numpy as np
+import pytest
+
+from ermod_openacc_b200 import slvfe as SF
+from ermod_openacc_b200 import systems as S
+from ermod_openacc_b200 import _capi as A
+
+
+def synthetic(nbins=120, seed=3):
+    rng = np.random.default_rng(seed)
+    crd = np.concatenate([np.linspace(-8.0, -0.05, nbins // 2), np.linspace(0.05, 40.0, nbins // 2)])
+    rho0 = rng.uniform(0.5, 2.0, nbins)
+    rho0 *= 100.0 / rho0.sum()
+    chi0 = np.outer(rho0, rho0) + np.diag(rho0)
+    return crd, rho0, chi0
+
+
+def test_identical_distributions_give_aveuv(slvfe_oracle):
+    crd, rho0, chi0 = synthetic()
+    spec = np.ones(len(crd), dtype=int)
+    for f in (SF.delta_mu, slvfe_oracle.delta_mu):
+        per, tot = f(rho0, rho0, chi0, crd, spec, 300.0, [-3.25], slfeng=0.5)
+        assert per[0] == pytest.approx(-3.25, abs=1e-10)
+        assert tot == pytest.approx(-2.75, abs=1e-10)
+
+
+def test_kT_matches_slvfe():
+    assert SF.kT_of(300.0) == pytest.approx(300.0 * 8.314510e-3 / 4.184, rel=1e-15)
+
+
+def test_product_matches_restatement_on_synthetic_shift(slvfe_oracle):
+    crd, rho0, chi0 = synthetic(seed=5)
+    spec = np.ones(len(crd), dtype=int)
+    rho = rho0 * np.exp(-0.3 * np.tanh(crd / 3.0))
+    rho[-5:] = 0.0                      # core bins empty in solution
+    rho *= 100.0 / rho.sum()
+    a = SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0])
+    b = slvfe_oracle.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0])
+    np.testing.assert_allclose(a[0], b[0], rtol=1e-10, atol=1e-10)
+
+
+def _distributions(oracle_mod):
+    """rho from a soln run of an LJ site in water, rho0/chi0 from refs insertions of the same site."""
+    w = S.make_workload(1, small=True)
+    orc = oracle_mod.Oracle(w.params, w.topo, w.hist, precision=8)
+    for fr in range(3):
+        pos, cell = w.frame(fr)
+        assert orc.engconst(fr + 1, pos, cell) >= 0
+    sln = orc.accum(normalise=True)
+    topo = S.Topology([S.water(), S.lj_site()], [w.nside ** 3, 1], [A.PT_SOLVENT, A.PT_TEST_RIGID])
+    prm = S.default_params(ms1max=32, maxins=3000)
+    ref = oracle_mod.Oracle(prm, topo, w.hist, precision=8)
+    wr = S.Workload("refs-ljsite", prm, topo, {}, w.box, w.nside, 4, w.seed + 11)
+    for fr in range(4):
+        pos, cell = wr.frame(fr)
+        assert ref.engconst(fr + 1, pos, cell) >= 0
+    rfa = ref.accum(normalise=True)
+    return orc, sln, rfa
+
+
+def test_product_matches_restatement_on_engine_distributions(oracle_mod, slvfe_oracle):
+    orc, sln, rfa = _distributions(oracle_mod)
+    spec = np.ones(orc.ermax, dtype=int)
+    aveuv = [float(sln["slnuv"][0])]    # engstore-normalised: aveuv (engproc.F90:622)
+    a = SF.delta_mu(sln["edens"], rfa["edens"], rfa["ecorr"], orc.uvcrd, spec, 300.0, aveuv)
+    b = slvfe_oracle.delta_mu(sln["edens"], rfa["edens"], rfa["ecorr"], orc.uvcrd, spec, 300.0, aveuv)
+    assert np.isfinite(a[1]) and abs(a[1]) < 1e3
+    assert a[1] == pytest.approx(b[1], rel=1e-6, abs=1e-6)
