@@ -132,6 +132,18 @@ SIGNATURES = {
     "ermod_batch_last_ms": (C.c_float, [C.c_void_p]),
     "ermod_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "ermod_batch_destroy": (None, [C.c_void_p]),
+    "ermod_proposal_config": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.POINTER(C.c_float)]),
+    "ermod_get_insertion_samples": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_double),
+                                                C.POINTER(C.c_int32)]),
+    "ermod_mlp_create": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.POINTER(C.c_float)]),
+    "ermod_mlp_nparams": (C.c_int32, []),
+    "ermod_mlp_forward": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_float)]),
+    "ermod_mlp_gradients": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32,
+                                        C.POINTER(C.c_float), C.POINTER(C.c_double)]),
+    "ermod_mlp_train_step": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32,
+                                         C.c_float, C.POINTER(C.c_double)]),
+    "ermod_mlp_get_params": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float)]),
+    "ermod_mlp_destroy": (None, [C.c_void_p]),
     "ermod_destroy": (None, [C.c_void_p]),
     "ermod_histogram_noalloc": (C.c_int32, [C.c_int32, C.c_int32, _f64p, C.c_int32, C.c_int32, _i32p, _f64p,
                                             _i32p, _i32p, C.c_int32, _f64p, _f64p]),

@@ -90,6 +90,10 @@ struct ermod_ctx {
   long long graph_launches = 0;
   int* h_frame = nullptr;         // pinned: [0] stnum of the frame being staged
   DevStatus* h_status = nullptr;  // pinned: status word written by the frame
+  // insertion proposal: voxels per side (0: off), uniform mixture weight, network loaded
+  int prop_gv = 0, prop_gf = 0;
+  float prop_eps = 0.1f;
+  bool prop_params = false;
 };
 
 // With spectrum_path == 0 the fused solve builds the solute spectrum by direct
@@ -125,7 +129,8 @@ void free_all(ermod_ctx* c) {
                   d.splfc,
                   d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
                   d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.edens_part, d.ecorr, d.eself,
-                  d.slnuv, d.minuv, d.maxuv, d.scal, d.status, d.frame_i, c->tc_work};
+                  d.slnuv, d.minuv, d.maxuv, d.scal, d.status, d.frame_i, d.dens, d.feat, d.mlp_f, d.mlp_b,
+                  d.vact, d.vlogit, d.vcdf, d.vq, d.ins_voxel, d.ins_feat, c->tc_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->plans) {
@@ -540,6 +545,8 @@ struct FramePlan {
   WeightArgs wa;
   BinArgs ba;
   int ncell, use_conf, selfreal, real_threads;
+  int prop_gv, prop_gf, prop_learned;   // proposal voxels and feature cells per side (0: none), network on
+  float prop_eps;
 };
 
 struct FramePlanHost {
@@ -688,6 +695,14 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
   fp.selfreal = P.bare ? 0 : (rigid ? (ctx->usreal_init ? 3 : 1) : 2);
   fp.use_conf = use_conf ? 1 : 0;
   fp.real_threads = ctx->real_threads;
+  // ---- insertion proposal (refs mode, random positions only) ----
+  const bool learned = refs && p.proposal == ERMOD_PROPOSAL_LEARNED;
+  if (learned && (ctx->prop_gv <= 0 || !ctx->prop_params)) return set_error(ctx, ERMOD_ERR_ARG, "prp_set");
+  if (learned && p.insposition != ERMOD_INSPOS_RANDOM) return set_error(ctx, ERMOD_ERR_ARG, "prp_pos");
+  fp.prop_gv = (refs && p.insposition == ERMOD_INSPOS_RANDOM) ? ctx->prop_gv : 0;
+  fp.prop_gf = ctx->prop_gf;
+  fp.prop_learned = learned ? 1 : 0;
+  fp.prop_eps = ctx->prop_eps;
   // ---- weights ----
   WeightArgs& wa = fp.wa;
   wa.slttype = p.slttype; wa.wgtslf = p.wgtslf; wa.estype = p.estype; wa.selfcal = p.selfcal;
@@ -767,7 +782,14 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
   nl += 1 + (a.slvmax > 0 ? (a.use_cells ? 3 : 2) : 0);
   M(kStPrep);
   // ---- targets ----
-  if (refs) launch_insert(a, d, d.frame_i, p.iseed, p.insposition, p.insorient, fp.use_conf, st);
+  if (refs && fp.prop_gv > 0) {
+    const int n = launch_proposal(a, d, fp.prop_gv, fp.prop_gf, fp.prop_eps, fp.prop_learned != 0, st);
+    if (n < 0) return set_error(ctx, ERMOD_ERR_CUDA, "prp_run");
+    nl += n;
+  }
+  if (refs)
+    launch_insert(a, d, d.frame_i, p.iseed, p.insposition, p.insorient, fp.use_conf, fp.prop_gv, fp.prop_learned,
+                  st);
   else launch_targets_soln(a, d, nullptr, st);
   CK(cudaMemsetAsync(d.selfrec, 0, sizeof(double) * ctx->maxdst, st));
   CK(cudaMemsetAsync(d.etot, 0, sizeof(double) * ctx->maxdst, st));
@@ -1299,6 +1321,66 @@ int32_t ermod_get_timings(const ermod_ctx* ctx, float* ms, int32_t n) {
 }
 
 int64_t ermod_get_launch_count(const ermod_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int32_t ermod_proposal_config(ermod_ctx* ctx, int32_t voxels_per_side, int32_t feature_cells, float mix_uniform,
+                              const float* params) {
+  if (!ctx) return ERMOD_ERR_ARG;
+  if (feature_cells == 0) feature_cells = 2 * voxels_per_side;
+  if (voxels_per_side < 2 || voxels_per_side > 64 || feature_cells < 4 || feature_cells > 128 ||
+      !(mix_uniform > 0.f) || !(mix_uniform <= 1.f))
+    return set_error(ctx, ERMOD_ERR_ARG, "prp_arg");
+  if (ctx->p.slttype == ERMOD_SLT_SOLN) return set_error(ctx, ERMOD_ERR_ARG, "prp_sln");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->st));
+  DeviceState& d = ctx->d;
+  const int gv = voxels_per_side, V = gv * gv * gv, gf = feature_cells;
+  if (gv != ctx->prop_gv || gf != ctx->prop_gf) {
+    void* old[] = {d.dens, d.feat, d.vact, d.vlogit, d.vcdf, d.vq};
+    for (void* q : old) if (q) cudaFree(q);
+    d.dens = nullptr; d.feat = nullptr; d.vact = nullptr; d.vlogit = nullptr; d.vcdf = nullptr; d.vq = nullptr;
+    CK(dalloc(&d.dens, (size_t)gf * gf * gf));
+    CK(dalloc(&d.feat, (size_t)V * kMlpIn));
+    CK(dalloc(&d.vact, (size_t)3 * V * kMlpHidden));
+    CK(dalloc(&d.vlogit, V));
+    CK(dalloc(&d.vcdf, V));
+    CK(dalloc(&d.vq, V));
+    if (!d.ins_voxel) CK(dalloc(&d.ins_voxel, ctx->maxdst));
+    CK(cudaMemsetAsync(d.ins_voxel, 0, sizeof(int) * ctx->maxdst, ctx->st));   // valid voxels before any frame
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; ctx->gkey.clear(); }
+  }
+  ctx->prop_gv = gv;
+  ctx->prop_gf = gf;
+  ctx->prop_eps = mix_uniform;
+  if (params) {
+    const int np = mlp_layout().n;
+    if (!d.mlp_f) CK(dalloc(&d.mlp_f, np));
+    if (!d.mlp_b) CK(dalloc(&d.mlp_b, np));
+    CK(cudaMemcpyAsync(d.mlp_f, params, sizeof(float) * np, cudaMemcpyHostToDevice, ctx->st));
+    launch_to_bf16(np, d.mlp_f, d.mlp_b, ctx->st);
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaGetLastError());
+    ctx->prop_params = true;
+  }
+  return ERMOD_OK;
+}
+
+int32_t ermod_get_insertion_samples(ermod_ctx* ctx, float* features, double* etot, int32_t* voxel) {
+  if (!ctx) return ERMOD_ERR_ARG;
+  if (ctx->prop_gv <= 0 || !ctx->d.ins_voxel) return set_error(ctx, ERMOD_ERR_ARG, "prp_set");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->st));
+  DeviceState& d = ctx->d;
+  if (features) {
+    if (!d.ins_feat) CK(dalloc(&d.ins_feat, (size_t)ctx->maxdst * kMlpIn));
+    launch_gather_ins_features(d, ctx->maxdst, d.ins_feat, ctx->st);
+    CK(cudaMemcpyAsync(features, d.ins_feat, sizeof(float) * ctx->maxdst * kMlpIn, cudaMemcpyDeviceToHost, ctx->st));
+  }
+  if (etot) CK(cudaMemcpyAsync(etot, d.etot, sizeof(double) * ctx->maxdst, cudaMemcpyDeviceToHost, ctx->st));
+  if (voxel) CK(cudaMemcpyAsync(voxel, d.ins_voxel, sizeof(int) * ctx->maxdst, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaGetLastError());
+  return ERMOD_OK;
+}
 
 int32_t ermod_get_paths(const ermod_ctx* ctx, int32_t* spectrum_path, int32_t* ecorr_path) {
   if (!ctx) return ERMOD_ERR_ARG;

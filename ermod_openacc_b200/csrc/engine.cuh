@@ -1,5 +1,6 @@
 // engine.cuh -- device buffers of one engine context and the kernel launchers.
 #pragma once
+#include <cuda_bf16.h>
 #include <cufft.h>
 #include <cuda_runtime.h>
 
@@ -17,6 +18,13 @@ constexpr int kMaxLjTypes = 64;
 constexpr int kInflBlocks = 64;    // CTAs per target in the influence multiply
 constexpr int kEdensSlices = 32;   // target slices of the edens reduction
 constexpr int kMaxGrid = 256;      // largest PME grid dimension (x rows are one CTA dimension)
+constexpr int kMlpIn = 64;         // proposal network: 4x4x4 local density inputs
+constexpr int kMlpHidden = 128;    // width of its three hidden layers
+
+// Offsets of the proposal network's parameters in its FP32 vector.
+struct MlpLayout {
+  int w1, b1, w2, b2, w3, b3, w4, b4, n;
+};
 
 // Everything the frame kernels read, passed by value.
 struct FrameArgs {
@@ -111,13 +119,33 @@ struct DeviceState {
   double* scal = nullptr;    // [8]: avslf, engnorm, engsmpl, voffset, voffset_init, usreal, usreal_init
   DevStatus* status = nullptr;
   int* frame_i = nullptr;    // [4] per-frame scalars staged before the frame: [0] stnum
+  // insertion proposal (refs mode)
+  int* dens = nullptr;       // [F^3] solvent first-site counts on the feature grid
+  float* feat = nullptr;     // [G^3][64] per-voxel network inputs
+  float* mlp_f = nullptr;    // [nparams] network parameters, FP32 (biases are used from here)
+  __nv_bfloat16* mlp_b = nullptr;  // [nparams] the same rounded to BF16 (weight matrices)
+  float* vact = nullptr;     // [3][G^3][128] hidden activations of the voxels
+  float* vlogit = nullptr;   // [G^3]
+  double* vcdf = nullptr;    // [G^3] CDF of the proposal over the voxels
+  float* vq = nullptr;       // [G^3] proposal probability of each voxel
+  int* ins_voxel = nullptr;  // [maxdst] voxel of each insertion
+  float* ins_feat = nullptr; // [maxdst][64] features of each insertion's voxel (training data, on request)
 };
 
 // ---- launchers (kernels.cu) -------------------------------------------
 void launch_prepare_solvent(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
 void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStream_t s);
 void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, int insposition,
-                   int insorient, int use_conf, cudaStream_t s);
+                   int insorient, int use_conf, int gv, int learned, cudaStream_t s);
+// proposal (proposal.cu) and its network (mlp.cu)
+MlpLayout mlp_layout();
+void mlp_forward(const __nv_bfloat16* pw, const float* pf, const float* x, int n, float* act, float* logits,
+                 cudaStream_t s);
+int mlp_forward_launches();
+void launch_to_bf16(int n, const float* src, __nv_bfloat16* dst, cudaStream_t s);
+int launch_proposal(const FrameArgs& a, const DeviceState& d, int gv, int gf, float eps, bool learned,
+                    cudaStream_t s);
+void launch_gather_ins_features(const DeviceState& d, int n, float* out, cudaStream_t s);
 void launch_targets_soln(const FrameArgs& a, const DeviceState& d, const int* tgt_k_host_dev, cudaStream_t s);
 void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int count, double screen,
                      cudaStream_t s);

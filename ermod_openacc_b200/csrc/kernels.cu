@@ -209,8 +209,12 @@ __device__ void finish_target(const FrameArgs& a, int cnt, float4* __restrict__ 
   ctr[cnt] = make_float4(c.x, c.y, c.z, rad);
 }
 
+// gv > 0: record each insertion's voxel of the G^3 proposal grid; learned: draw
+// the voxel from the proposal CDF and scale the insertion's weight by
+// p/q = (1/G^3) / q_v (the position inside the voxel stays uniform).
 __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int iseed, int insposition, int insorient,
-                         int use_conf,
+                         int use_conf, int gv, int learned, const double* __restrict__ cdf,
+                         const float* __restrict__ qv, int* __restrict__ ins_voxel, float* __restrict__ insw,
                          const float* __restrict__ conf_all, const float* __restrict__ bfcoord,
                          const float* __restrict__ mass, const float* __restrict__ qsite,
                          float4* __restrict__ tgt_raw, float4* __restrict__ tgt_n, float4* __restrict__ tgt_c) {
@@ -236,7 +240,28 @@ __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int ise
     com(c);  // set_solute_origin: COM to the origin (insertion.F90:116-119)
     for (int i = 0; i < s; ++i) { out[i].x -= c[0]; out[i].y -= c[1]; out[i].z -= c[2]; }
     const uint4 r4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, 0u, 0u), key);
-    const float r[3] = {u01(r4.x), u01(r4.y), u01(r4.z)};
+    float r[3] = {u01(r4.x), u01(r4.y), u01(r4.z)};
+    if (gv > 0) {
+      const int V = gv * gv * gv;
+      int v;
+      if (learned) {
+        const double target = (double)u01(r4.w) * cdf[V - 1];
+        int lo = 0, hi = V - 1;   // first v with cdf[v] > target
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (cdf[mid] > target) hi = mid; else lo = mid + 1;
+        }
+        v = lo;
+        const int vv[3] = {v % gv, (v / gv) % gv, v / (gv * gv)};
+        for (int m = 0; m < 3; ++m) r[m] = ((float)vv[m] + r[m]) / (float)gv;
+        insw[cnt] *= (float)(1.0 / ((double)V * (double)qv[v]));
+      } else {
+        int vv[3];
+        for (int m = 0; m < 3; ++m) vv[m] = min(gv - 1, (int)(r[m] * (float)gv));
+        v = (vv[2] * gv + vv[1]) * gv + vv[0];
+      }
+      ins_voxel[cnt] = v;
+    }
     float cm[3];  // com = cell . r (insertion.F90:157-161)
     for (int k = 0; k < 3; ++k) cm[k] = a.g.cell[k][0] * r[0] + a.g.cell[k][1] * r[1] + a.g.cell[k][2] * r[2];
     com(c);
@@ -278,8 +303,9 @@ __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int ise
 }
 
 void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, int insposition,
-                   int insorient, int use_conf, cudaStream_t s) {
-  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum_dev, iseed, insposition, insorient, use_conf, d.ins_conf,
+                   int insorient, int use_conf, int gv, int learned, cudaStream_t s) {
+  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum_dev, iseed, insposition, insorient, use_conf, gv, learned,
+                                                    d.vcdf, d.vq, d.ins_voxel, d.insw_in, d.ins_conf,
                                                     d.bfcoord, d.slt_mass, d.slt_q, d.tgt_raw, d.tgt_n, d.tgt_c);
 }
 

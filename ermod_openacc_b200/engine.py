@@ -170,6 +170,23 @@ class Engine:
         """Device time of the last frame (the stage timings' total)."""
         return self.timings()["total"]
 
+    def proposal_config(self, voxels_per_side: int, mix_uniform: float = 0.1, params=None, feature_cells: int = 0):
+        """Voxel grid (and feature-cell grid, 0: twice as fine) of the insertion proposal; with `params`
+        (FP32 network parameters) and params['proposal'] == PROPOSAL_LEARNED, insertions are drawn from
+        the network's proposal."""
+        pp = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self.lib.ermod_proposal_config(self.ctx, voxels_per_side, feature_cells, mix_uniform,
+                                                   A.ptr(pp, C.c_float)))
+
+    def insertion_samples(self):
+        """(features [maxdst, 64], total solute-solvent energy [maxdst], voxel [maxdst]) of the last frame."""
+        f = np.zeros(self.maxdst * 64, dtype=np.float32)
+        e = np.zeros(self.maxdst)
+        v = np.zeros(self.maxdst, dtype=np.int32)
+        self._check(self.lib.ermod_get_insertion_samples(self.ctx, A.ptr(f, C.c_float), A.ptr(e, C.c_double),
+                                                         A.ptr(v, C.c_int32)))
+        return f.reshape(self.maxdst, 64), e, v
+
     def paths(self) -> dict:
         """Resolved kernel choices: spectrum_path 1 cuFFT / 2 fused direct / 3 fused spread, ecorr_path."""
         sp, ep = C.c_int32(), C.c_int32()

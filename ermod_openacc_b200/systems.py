@@ -121,9 +121,50 @@ def _rot_from_quat(q):
                      [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
 
 
-def water_box_frame(nside: int, box: float, seed: int, jitter=0.3, avoid=None, avoid_r=3.0):
-    """Coordinates (3, 3*nside^3) of a water lattice with random orientations.
+def random_packing(n: int, box: float, rng, dmin: float = 2.5, max_tries: int = 5000):
+    """n points in a periodic cube by random sequential addition with a minimum
+    separation `dmin`: a disordered packing with the density fluctuations and
+    cavities of a liquid (the lattice has none)."""
+    nc = max(1, int(box // dmin))
+    h = box / nc
+    cells = {}
+    pts = np.empty((n, 3))
+    k = 0
+    while k < n:
+        for _ in range(max_tries):
+            p = rng.uniform(0.0, box, 3)
+            c = tuple((p // h).astype(int) % nc)
+            ok = True
+            for dz in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dx in (-1, 0, 1):
+                        for j in cells.get(((c[0] + dx) % nc, (c[1] + dy) % nc, (c[2] + dz) % nc), ()):
+                            d = pts[j] - p
+                            d -= box * np.round(d / box)
+                            if d @ d < dmin * dmin:
+                                ok = False
+                                break
+                        if not ok:
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                pts[k] = p
+                cells.setdefault(c, []).append(k)
+                k += 1
+                break
+        else:
+            raise RuntimeError("random packing: too dense for the minimum separation")
+    return pts
 
+
+def water_box_frame(nside: int, box: float, seed: int, jitter=0.3, avoid=None, avoid_r=3.0, packing="lattice"):
+    """Coordinates (3, 3*nside^3) of nside^3 waters with random orientations.
+
+    packing "lattice": centres of mass on the n^3 lattice plus Gaussian
+    `jitter`; "random": a random sequential packing at the same density.
     `avoid`: optional point; water oxygens closer than `avoid_r` are pushed
     radially out to `avoid_r` (keeps a soln solute out of the hard core).
     """
@@ -132,9 +173,12 @@ def water_box_frame(nside: int, box: float, seed: int, jitter=0.3, avoid=None, a
     com_body = (wat.coords * wat.mass).sum(axis=1) / wat.mass.sum()
     body = wat.coords - com_body[:, None]
     n = nside ** 3
-    g = (np.arange(nside) + 0.5) * (box / nside)
-    cz, cy, cx = np.meshgrid(g, g, g, indexing="ij")
-    com = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], axis=1) + rng.normal(0.0, jitter, size=(n, 3))
+    if packing == "random":
+        com = random_packing(n, box, rng)
+    else:
+        g = (np.arange(nside) + 0.5) * (box / nside)
+        cz, cy, cx = np.meshgrid(g, g, g, indexing="ij")
+        com = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], axis=1) + rng.normal(0.0, jitter, size=(n, 3))
     q = rng.normal(size=(n, 4))
     q /= np.linalg.norm(q, axis=1, keepdims=True)
     out = np.empty((n, 3, 3))
@@ -290,11 +334,12 @@ class Workload:
     nframes: int
     seed: int
     solute_center: np.ndarray | None = None     # soln: fixed solute position
+    packing: str = "lattice"                     # water centres: "lattice" + jitter or "random"
 
     def frame(self, i: int):
         """sitepos (3*numatm_phys float32, Fortran order) and cell (9 float32) of frame i."""
         avoid = self.solute_center
-        wat = water_box_frame(self.nside, self.box, self.seed * 1000003 + i, avoid=avoid)
+        wat = water_box_frame(self.nside, self.box, self.seed * 1000003 + i, avoid=avoid, packing=self.packing)
         parts = []
         for sp, cnt, kind in zip(self.topo.species, self.topo.counts, self.topo.kinds):
             if kind == A.PT_SOLVENT and sp.name == "water":

@@ -168,6 +168,11 @@ typedef struct ermod_accum {
 
 typedef struct ermod_ctx ermod_ctx;
 
+/* Learned insertion proposal: network size (no reference counterpart). */
+#define ERMOD_MLP_IN       64     /* 4x4x4 local solvent-density inputs */
+#define ERMOD_MLP_HIDDEN   128    /* width of the three hidden layers */
+#define ERMOD_MLP_NPARAMS  41473  /* W1[128][64] b1[128] W2[128][128] b2[128] W3[128][128] b3[128] w4[128] b4 */
+
 /* ABI version (ERMOD_ABI_VERSION). */
 int32_t ermod_abi_version(void);
 
@@ -295,6 +300,42 @@ void ermod_destroy(ermod_ctx* ctx);
  * solute (no per-insertion conformations).  The batch does not own the
  * members; destroy it before them.
  */
+/*
+ * Learned insertion proposal (refs mode, insposition random; no reference
+ * counterpart).  The cell is cut into G^3 voxels (G = voxels_per_side) and,
+ * for the network's inputs, into F^3 feature cells (F = feature_cells,
+ * 0: 2G): a voxel's inputs are the 4x4x4 feature cells nearest its centre;
+ * with ermod_params.proposal == ERMOD_PROPOSAL_LEARNED an insertion's
+ * voxel is drawn from q_v = mix_uniform / G^3 + (1 - mix_uniform) *
+ * softmax(s)_v, s_v the network's logit from the voxel's 4x4x4 local
+ * density of solvent first sites, the point inside the voxel uniformly, and
+ * the insertion's weight is multiplied by p/q = 1 / (G^3 q_v).  `params`
+ * (ERMOD_MLP_NPARAMS FP32, layout above; weight matrices are used rounded
+ * to BF16) may be NULL to only record voxels and features with uniform
+ * insertion (training data).  mix_uniform in (0, 1].
+ */
+int32_t ermod_proposal_config(ermod_ctx* ctx, int32_t voxels_per_side, int32_t feature_cells, float mix_uniform,
+                              const float* params);
+/* Per insertion of the last frame: its voxel's 64 network inputs
+ * ([maxdst*64]), its total solute-solvent energy ([maxdst]) and its voxel
+ * index ([maxdst]); any pointer may be NULL. */
+int32_t ermod_get_insertion_samples(ermod_ctx* ctx, float* features, double* etot, int32_t* voxel);
+
+/*
+ * The proposal network's trainer: hand-written forward, backward and Adam
+ * kernels on one device (no reference counterpart).  Loss: mean binary
+ * cross-entropy of the logit against labels y in [0, 1].  Batches are host
+ * arrays x[n*64], y[n], n <= max_batch.
+ */
+typedef struct ermod_mlp ermod_mlp;
+int32_t ermod_mlp_create(ermod_mlp** out, int32_t device, int32_t max_batch, const float* init_params);
+int32_t ermod_mlp_nparams(void);
+int32_t ermod_mlp_forward(ermod_mlp* m, const float* x, int32_t n, float* logits);
+int32_t ermod_mlp_gradients(ermod_mlp* m, const float* x, const float* y, int32_t n, float* grad, double* loss);
+int32_t ermod_mlp_train_step(ermod_mlp* m, const float* x, const float* y, int32_t n, float lr, double* loss);
+int32_t ermod_mlp_get_params(ermod_mlp* m, float* params);
+void ermod_mlp_destroy(ermod_mlp* m);
+
 typedef struct ermod_batch ermod_batch;
 int32_t ermod_batch_create(ermod_batch** out, int32_t n, ermod_ctx* const* members);
 int32_t ermod_batch_engconst(ermod_batch* b, int32_t stnum, const float* sitepos, const float* cell,
