@@ -150,6 +150,7 @@ void launch_targets_soln(const FrameArgs& a, const DeviceState& d, const int* tg
 void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int count, double screen,
                      cudaStream_t s);
 void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, int threads, cudaStream_t s);
+int setup_real_smem(const FrameArgs& a);
 void launch_fill(float* p, float v, int n, cudaStream_t s);
 void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[3][3], double volume,
                    double screen, cudaStream_t s);

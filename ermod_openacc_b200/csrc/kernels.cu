@@ -372,19 +372,32 @@ void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int co
 // ---------------------------------------------------------------------------
 constexpr int kRealMaxThreads = 512;
 
+// WIDE (large solutes): lanes over the solute sites, the molecule's atoms in
+// turn; otherwise lanes over the (site, atom) pairs.  Either way a molecule's
+// energy is one warp's fixed-order FP64 sum.  The solute sites and the LJ
+// tables sit in shared memory (dynamic: s float4 + s int + 2 ljmax^2 float).
+template <bool WIDE>
 __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base, int chunk,
     const float4* __restrict__ tgt_n, const float4* __restrict__ tgt_c, const int* __restrict__ tgt_mol,
     const int* __restrict__ slt_lj_tab, const int* __restrict__ molbeg, const float4* __restrict__ slvn,
     const int* __restrict__ atom_lj, const float* __restrict__ ljene, const float* __restrict__ ljlensq,
     const float4* __restrict__ anchor, const int* __restrict__ cellstart, const int* __restrict__ molsorted,
     const float* __restrict__ rmol_p, double* __restrict__ E) {
-  __shared__ float4 ss[kMaxSoluteSites];
-  __shared__ int slj[kMaxSoluteSites];
+  extern __shared__ __align__(16) unsigned char rsm_real[];
   const int b = blockIdx.x, cnt = base + b, s = a.nsite;
+  const int ljmax = a.ljtype_max;
+  float4* ss = (float4*)rsm_real;
+  int* slj = (int*)(ss + s);
+  float* lje = (float*)(slj + s);
+  float* ljs = lje + ljmax * ljmax;
   const float4* tn = tgt_n + (size_t)cnt * s;
   for (int i = threadIdx.x; i < s; i += blockDim.x) {
     ss[i] = tn[i];
     slj[i] = slt_lj_tab ? slt_lj_tab[i] : 0;
+  }
+  for (int i = threadIdx.x; i < ljmax * ljmax; i += blockDim.x) {
+    lje[i] = ljene[i];
+    ljs[i] = ljlensq[i];
   }
   const int excl = tgt_mol ? tgt_mol[cnt] : -1;
   // soln: solute site LJ types come from the solute molecule's atoms
@@ -395,7 +408,8 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
   const float rmol = *rmol_p;
   const float margin = 1.0e-2f;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int ljmax = a.ljtype_max;
+  // pairs beyond rcut (>= elecut and > upljcut) are zero; the slack keeps r == rcut with pair_energy
+  const float rskip2 = a.rcut * a.rcut * 1.0001f;
 
   auto do_mol = [&](int k) {
     if (k == excl) return;
@@ -405,19 +419,34 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
     const float lim = a.rcut + c.w + an.w + margin;
     if (dx * dx + dy * dy + dz * dz > lim * lim) return;  // every site pair beyond the cutoff
     const int b0 = molbeg[k], nj = molbeg[k + 1] - b0;
-    const int P = s * nj;
     double acc = 0.0;
-    for (int t = lane; t < P; t += 32) {
-      const int is = t / nj, js = t - is * nj;
-      const float4 xi = ss[is];
-      const float4 xj = slvn[b0 + js];
-      float ex = xi.x - xj.x, ey = xi.y - xj.y, ez = xi.z - xj.z;
-      min_image(a.g, ex, ey, ez);
-      const float dis2 = ex * ex + ey * ey + ez * ez;
-      const int li = slj[is], lj = atom_lj[b0 + js];
-      const float eps = __ldg(&ljene[lj * ljmax + li]);
-      const float sg2 = __ldg(&ljlensq[lj * ljmax + li]);
-      acc += (double)pair_energy(a.pp, dis2, eps, sg2, xi.w * xj.w);
+    if (WIDE) {
+      for (int js = 0; js < nj; ++js) {
+        const float4 xj = slvn[b0 + js];
+        const int lj = atom_lj[b0 + js];
+        for (int is = lane; is < s; is += 32) {
+          const float4 xi = ss[is];
+          float ex = xi.x - xj.x, ey = xi.y - xj.y, ez = xi.z - xj.z;
+          min_image(a.g, ex, ey, ez);
+          const float dis2 = ex * ex + ey * ey + ez * ez;
+          if (dis2 > rskip2) continue;
+          const int li = slj[is];
+          acc += (double)pair_energy(a.pp, dis2, lje[lj * ljmax + li], ljs[lj * ljmax + li], xi.w * xj.w);
+        }
+      }
+    } else {
+      const int P = s * nj;
+      for (int t = lane; t < P; t += 32) {
+        const int is = t / nj, js = t - is * nj;
+        const float4 xi = ss[is];
+        const float4 xj = slvn[b0 + js];
+        float ex = xi.x - xj.x, ey = xi.y - xj.y, ez = xi.z - xj.z;
+        min_image(a.g, ex, ey, ez);
+        const float dis2 = ex * ex + ey * ey + ez * ez;
+        if (dis2 > rskip2) continue;
+        const int li = slj[is], lj = atom_lj[b0 + js];
+        acc += (double)pair_energy(a.pp, dis2, lje[lj * ljmax + li], ljs[lj * ljmax + li], xi.w * xj.w);
+      }
     }
     acc = warp_sum(acc);
     if (lane == 0) E[(size_t)k * chunk + b] = acc;
@@ -449,6 +478,20 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
   }
 }
 
+// Solutes above this many sites run the WIDE real-space variant.
+constexpr int kRealWideSites = 24;
+
+size_t real_smem(const FrameArgs& a) {
+  return (sizeof(float4) + sizeof(int)) * (size_t)a.nsite + 2 * sizeof(float) * (size_t)a.ljtype_max * a.ljtype_max;
+}
+
+int setup_real_smem(const FrameArgs& a) {
+  const int b = (int)real_smem(a);
+  if (cudaFuncSetAttribute(k_real<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess) return -1;
+  if (cudaFuncSetAttribute(k_real<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess) return -1;
+  return 0;
+}
+
 // `threads` (a multiple of 32, <= kRealMaxThreads) only changes how many warps
 // share a target's molecules: each molecule's energy is one warp's fixed-order
 // sum whatever the block size.
@@ -456,8 +499,15 @@ void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int
   cudaMemsetAsync(d.E, 0, sizeof(double) * (size_t)a.slvmax * chunk, s);
   if (nb <= 0) return;  // `chunk` is the row stride of E: the batch size
   if (threads <= 0 || threads > kRealMaxThreads || threads % 32) threads = 256;
-  k_real<<<nb, threads, 0, s>>>(a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, d.slt_lj, d.molbeg, d.slvn,
-                                      d.atom_lj, d.ljene, d.ljlensq, d.anchor, d.cellstart, d.molsorted, d.rmol, d.E);
+  const size_t sm = real_smem(a);
+  if (a.nsite > kRealWideSites)
+    k_real<true><<<nb, threads, sm, s>>>(a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, d.slt_lj, d.molbeg, d.slvn,
+                                          d.atom_lj, d.ljene, d.ljlensq, d.anchor, d.cellstart, d.molsorted, d.rmol,
+                                          d.E);
+  else
+    k_real<false><<<nb, threads, sm, s>>>(a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, d.slt_lj, d.molbeg, d.slvn,
+                                           d.atom_lj, d.ljene, d.ljlensq, d.anchor, d.cellstart, d.molsorted, d.rmol,
+                                           d.E);
 }
 
 // ---------------------------------------------------------------------------

@@ -164,6 +164,9 @@ struct PlaneCfg {
   static constexpr int E = LK2 + LK3 <= 12 ? 16 : 32;     // plane points per thread
   static constexpr int NTHR = (K2 * K3) / E;
   static constexpr int MINB = E == 16 ? 4 : 1;
+  // plane spreading accumulates in 2^-40 fixed point in shared memory when the
+  // int64 plane fits beside the FP32 plane (up to 8192 points)
+  static constexpr bool FIXED = K2 * K3 <= 8192;
   static_assert(K3 % E == 0, "a thread owns E consecutive k3 of one k2 column");
 };
 
@@ -261,70 +264,103 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
   float2* b2 = c1 + ((ts + 1) & ~1);                   // DIRECT: [ts][K2] (16-byte aligned: K's are even)
   float2* b3 = b2 + (DIRECT ? ts * K2 : 0);            // DIRECT: [ts][K3]
   float* sst = (float*)b3;                             // spreading: [ts][kStn] stencils
+  long long* facc = (long long*)(((uintptr_t)(sst + ts * kStn) + 15) & ~(uintptr_t)15);   // spreading: [K3*K2]
   for (int p = tid; p < K2 + K3; p += NTHR) tw2[p] = fft_tw[K1 + p];
   const size_t pair0 = (size_t)(tbase + b) * s;       // first (target, site) pair of this target in the tables
   const int k2 = tid & (K2 - 1), k30 = (tid >> LK2) * E;
   float2 acc[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
-  for (int a0 = 0; a0 < s; a0 += ts) {
-    const int nt = min(ts, s - a0);
-    __syncthreads();
-    for (int x = tid; x < nt; x += NTHR) c1[x] = tab[(pair0 + a0 + x) * nk + k1];
-    if (DIRECT) {
-      // B2 then B3 of each site: K2 + K3 consecutive table entries, kLoadBatch loads in flight
-      const int per = K2 + K3, tot = nt * per;
-      for (int x0 = 0; x0 < tot; x0 += kLoadBatch * NTHR) {
-        float2 v[kLoadBatch];
-#pragma unroll
-        for (int u = 0; u < kLoadBatch; ++u) {
-          const int x = x0 + u * NTHR + tid;
-          if (x < tot) v[u] = tab[(pair0 + a0 + x / per) * nk + Kh1 + x % per];
+  if (!DIRECT && C::FIXED) {
+    // q_a B1_a(k1) w2 w3 scattered on the (n2, n3) plane: a thread per (site, stencil point),
+    // integer atomics in 2^-40 fixed point (exact, order-independent), real then imaginary part
+    constexpr double kFix = 1099511627776.0, kUnfix = 1.0 / 1099511627776.0;
+    for (int part = 0; part < 2; ++part) {
+      __syncthreads();
+      for (int p = tid; p < K2 * K3; p += NTHR) facc[p] = 0;
+      for (int a0 = 0; a0 < s; a0 += ts) {
+        const int nt = min(ts, s - a0);
+        __syncthreads();
+        for (int x = tid; x < nt; x += NTHR) c1[x] = tab[(pair0 + a0 + x) * nk + k1];
+        for (int x = tid; x < nt * kStn; x += NTHR) sst[x] = stn[(pair0 + a0) * kStn + x];
+        __syncthreads();
+        const int nn = n * n;
+        for (int x = tid; x < nt * nn; x += NTHR) {
+          const int t = x / nn, c = x - t * nn, c3 = c / n, c2 = c - c3 * n;
+          const float* st = sst + t * kStn;
+          const float v = (part ? c1[t].y : c1[t].x) * st[2 + c2] * st[2 + kMaxOrder + c3];
+          const int n2 = ((int)st[0] - c2) & (K2 - 1), n3 = ((int)st[1] - c3) & (K3 - 1);
+          atomicAdd((unsigned long long*)&facc[n3 * K2 + n2], (unsigned long long)__double2ll_rn((double)v * kFix));
         }
+      }
+      __syncthreads();
 #pragma unroll
-        for (int u = 0; u < kLoadBatch; ++u) {
-          const int x = x0 + u * NTHR + tid;
-          if (x < tot) {
-            const int t = x / per, r = x - t * per;
-            if (r < K2) b2[t * K2 + r] = v[u];
-            else b3[t * K3 + r - K2] = v[u];
+      for (int e = 0; e < E; ++e) {
+        const float v = (float)((double)facc[(k30 + e) * K2 + k2] * kUnfix);
+        if (part) acc[e].y = v; else acc[e].x = v;
+      }
+    }
+  } else {
+    for (int a0 = 0; a0 < s; a0 += ts) {
+      const int nt = min(ts, s - a0);
+      __syncthreads();
+      for (int x = tid; x < nt; x += NTHR) c1[x] = tab[(pair0 + a0 + x) * nk + k1];
+      if (DIRECT) {
+        // B2 then B3 of each site: K2 + K3 consecutive table entries, kLoadBatch loads in flight
+        const int per = K2 + K3, tot = nt * per;
+        for (int x0 = 0; x0 < tot; x0 += kLoadBatch * NTHR) {
+          float2 v[kLoadBatch];
+#pragma unroll
+          for (int u = 0; u < kLoadBatch; ++u) {
+            const int x = x0 + u * NTHR + tid;
+            if (x < tot) v[u] = tab[(pair0 + a0 + x / per) * nk + Kh1 + x % per];
+          }
+#pragma unroll
+          for (int u = 0; u < kLoadBatch; ++u) {
+            const int x = x0 + u * NTHR + tid;
+            if (x < tot) {
+              const int t = x / per, r = x - t * per;
+              if (r < K2) b2[t * K2 + r] = v[u];
+              else b3[t * K3 + r - K2] = v[u];
+            }
           }
         }
+      } else {
+        for (int x = tid; x < nt * kStn; x += NTHR) sst[x] = stn[(pair0 + a0) * kStn + x];
       }
-    } else {
-      for (int x = tid; x < nt * kStn; x += NTHR) sst[x] = stn[(pair0 + a0) * kStn + x];
-    }
-    __syncthreads();
-    if (DIRECT) {
-      for (int t = 0; t < nt; ++t) {
-        const float2 c = cmul(c1[t], b2[t * K2 + k2]);
-        const float4* bt = (const float4*)(b3 + t * K3 + k30);   // two k3 per 16-byte load
+      __syncthreads();
+      if (DIRECT) {
+        for (int t = 0; t < nt; ++t) {
+          const float2 c = cmul(c1[t], b2[t * K2 + k2]);
+          const float4* bt = (const float4*)(b3 + t * K3 + k30);   // two k3 per 16-byte load
 #pragma unroll
-        for (int e = 0; e < E; e += 2) {
-          const float4 u = bt[e / 2];
-          acc[e].x += c.x * u.x - c.y * u.y;
-          acc[e].y += c.x * u.y + c.y * u.x;
-          acc[e + 1].x += c.x * u.z - c.y * u.w;
-          acc[e + 1].y += c.x * u.w + c.y * u.z;
+          for (int e = 0; e < E; e += 2) {
+            const float4 u = bt[e / 2];
+            acc[e].x += c.x * u.x - c.y * u.y;
+            acc[e].y += c.x * u.y + c.y * u.x;
+            acc[e + 1].x += c.x * u.z - c.y * u.w;
+            acc[e + 1].y += c.x * u.w + c.y * u.z;
+          }
         }
-      }
-    } else {
-      // q_a B1_a(k1) w2 w3 on the (n2, n3) plane, accumulated in site order by the point's owner
-      for (int t = 0; t < nt; ++t) {
-        const float* st = sst + t * kStn;
-        const int c2 = ((int)st[0] - k2) & (K2 - 1);
-        if (c2 >= n) continue;
-        const float2 c = c1[t];
-        const float w2 = st[2 + c2];
-        const float2 f = make_float2(c.x * w2, c.y * w2);
-        const int g3 = (int)st[1];
-        const float* w3 = st + 2 + kMaxOrder;
+      } else {
+        // large planes: q_a B1_a(k1) w2 w3 accumulated in site order by the point's owner
+        for (int t = 0; t < nt; ++t) {
+          const float* st = sst + t * kStn;
+          const int c2 = ((int)st[0] - k2) & (K2 - 1);
+          if (c2 >= n) continue;
+          const int g3 = (int)st[1];
+          if (((g3 - k30) & (K3 - 1)) >= E + n - 1) continue;   // the site's rows miss this thread's rows
+          const float2 c = c1[t];
+          const float w2 = st[2 + c2];
+          const float2 f = make_float2(c.x * w2, c.y * w2);
+          const float* w3 = st + 2 + kMaxOrder;
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-          const int c3 = (g3 - (k30 + e)) & (K3 - 1);
-          if (c3 < n) {
-            acc[e].x += f.x * w3[c3];
-            acc[e].y += f.y * w3[c3];
+          for (int e = 0; e < E; ++e) {
+            const int c3 = (g3 - (k30 + e)) & (K3 - 1);
+            if (c3 < n) {
+              acc[e].x += f.x * w3[c3];
+              acc[e].y += f.y * w3[c3];
+            }
           }
         }
       }
@@ -481,7 +517,9 @@ int site_table_entries(const FrameArgs& a, bool direct) { return a.Kh1 + (direct
 
 size_t plane_smem(const FrameArgs& a, bool direct) {
   const size_t ts = site_tile(a), tsa = (ts + 1) & ~(size_t)1;
-  const size_t tile = sizeof(float2) * tsa + (direct ? sizeof(float2) * ts * (a.K2 + a.K3) : sizeof(float) * ts * kStn);
+  const size_t pts = (size_t)a.K2 * a.K3;
+  const size_t tile = sizeof(float2) * tsa + (direct ? sizeof(float2) * ts * (a.K2 + a.K3)
+                                                     : sizeof(float) * ts * kStn + 16 + (pts <= 8192 ? 8 * pts : 0));
   return sizeof(float2) * (size_t)(a.K2 + a.K3) + sizeof(float2) * (size_t)a.K3 * (a.K2 + 1) + tile;
 }
 
@@ -525,7 +563,7 @@ bool fused_supported(const FrameArgs& a) {
   if (G2 > a.K2) return false;                       // one CTA of k_pme_rows spans G2 rows of n2
   if (a.K2 * a.K3 < 512) return false;               // at least 32 threads per plane
   if (a.K3 % plane_elems(a) != 0) return false;      // a thread owns E consecutive k3
-  return plane_smem(a, true) <= 220 * 1024 && rows_smem(a) <= 220 * 1024;
+  return plane_smem(a, true) <= 220 * 1024 && plane_smem(a, false) <= 220 * 1024 && rows_smem(a) <= 220 * 1024;
 }
 
 int setup_fused(const FrameArgs& a) {
