@@ -47,8 +47,10 @@ def parse():
     ap.add_argument("--maxins", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=500, help="insertions per CPU reference step")
-    ap.add_argument("--config", type=int, default=2, choices=[2, 4],
-                    help="2: the headline refs frame; 4: 64 solutes batched into one graph per frame")
+    ap.add_argument("--config", type=int, default=2, choices=[2, 4, 5],
+                    help="2: the headline refs frame; 4: 64 solutes batched into one graph per frame; "
+                         "5: GPU time to delta-mu within 0.05 kcal/mol, learned vs uniform insertion")
+    ap.add_argument("--solute-sites", type=int, default=1, help="config 5: sites of the ring-recipe solute")
     return ap.parse_args()
 
 
@@ -214,6 +216,8 @@ def main():
     from ermod_openacc_b200 import systems as S
     if args.config == 4:
         return main_batch(args)
+    if args.config == 5:
+        return main_delta_mu(args)
     w = S.make_workload(CONFIG, maxins=args.maxins)
     if args.impl == "reference":
         run_reference(args, w)
@@ -377,6 +381,118 @@ def main_batch(args):
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
+    print(json.dumps(line))
+
+
+def main_delta_mu(args):
+    """Configuration 5 (scaled): GPU time until the energy-representation solvation free energy is within
+    0.05 kcal/mol of a long uniform-insertion run, for uniform and for learned insertion.
+
+    A ring-recipe solute (--solute-sites, default a single LJ site) in 4096 waters (49.6 A box, disordered
+    packing: the lattice has no cavities for the proposal to find), PME 64^3.  rho and aveuv come from
+    soln-mode frames with the solute at the box centre; rho0 / chi0 from refs insertions, 2048 per frame;
+    delta-mu from the py-hnc functional (ermod_openacc_b200.slvfe).  The judge is a uniform run of
+    `judge_frames` frames; each mode runs `reps` independent replicas and its error after n frames is the
+    RMS over replicas of the difference to the judge.  Times are CUDA-event device times of the frames; the
+    learned mode also reports the device time of its training (sample frames + training kernels)."""
+    import torch
+    import __graft_entry__ as ge
+    ge.build_engine()
+    from ermod_openacc_b200 import Engine, _capi as A, proposal as P, slvfe, systems as S
+    torch.cuda.set_device(0)
+    nins, gv, eps, npool = 2048, 32, 0.2, 8
+    base = S.make_workload(2, seed=11)
+    slt = S.lj_site() if args.solute_sites == 1 else S.ring_recipe_solute(args.solute_sites, 5)
+    box, nside = base.box, base.nside
+    # solution: the solute fixed at the centre, waters kept 3 A away
+    sln_topo = S.Topology([slt, S.water()], [1, nside ** 3], [A.PT_SOLUTE, A.PT_SOLVENT])
+    sln_prm = S.default_params(slttype=A.SLT_SOLN, ms1max=64, maxins=1, corrcal=0, wgtslf=0)
+    sln_w = S.Workload("soln", sln_prm, sln_topo, {}, box, nside, npool, 11,
+                       solute_center=np.array([box / 2] * 3), packing="random")
+    eng = Engine(sln_prm, sln_topo, {})
+    for i in range(npool):
+        eng.engconst(i + 1, *sln_w.frame(i))
+    sln, _ = eng.engstore()
+    rho, aveuv = sln["edens"], [float(sln["slnuv"][0])]
+    uvcrd, spec = eng.uvcrd, np.ones(eng.ermax, dtype=int)
+    eng.close()
+    # reference solvent: pure disordered water, insertions of the same solute
+    ref_topo = S.Topology([S.water(), slt], [nside ** 3, 1], [A.PT_SOLVENT, A.PT_TEST_RIGID])
+    ref_prm = S.default_params(ms1max=64, maxins=nins, corrcal=1)
+    ref_w = S.Workload("refs", ref_prm, ref_topo, {}, box, nside, npool, 12, packing="random")
+    frames = [ref_w.frame(i) for i in range(npool)]
+    temp_K = ref_prm["temp"] / S.KB_KCAL
+
+    def dmu(e):
+        acc, _ = e.engstore()
+        return slvfe.delta_mu(rho, acc["edens"], acc["ecorr"], uvcrd, spec, temp_K, aveuv)[1]
+
+    def run(mode, iseed, nfr, params=None, checkpoints=()):
+        e = Engine(dict(ref_prm, proposal=mode, iseed=iseed), ref_topo, {})
+        e.proposal_config(gv, eps, params, feature_cells=gv)
+        out, ms = {}, 0.0
+        for i in range(nfr):
+            e.engconst(i + 1, *frames[i % npool])
+            ms += e.last_ms()
+            if (i + 1) in checkpoints:
+                out[i + 1] = (dmu(e), ms)
+        res = out if checkpoints else dmu(e)
+        e.close()
+        return res, ms
+
+    judge_frames = 400
+    judge, judge_ms = run(A.PROPOSAL_UNIFORM, 999, judge_frames)
+    # training: uniform samples of 12 frames, 20 epochs of the device kernels
+    e = Engine(dict(ref_prm, corrcal=0), ref_topo, {})
+    e.proposal_config(gv, eps, feature_cells=gv)
+    sample_ms = 0.0
+    fs, es = [], []
+    for i in range(12):
+        e.engconst(i + 1, *frames[i % npool])
+        sample_ms += e.last_ms()
+        f, en, _ = e.insertion_samples()
+        fs.append(f)
+        es.append(en)
+    e.close()
+    feats, etot = np.concatenate(fs), np.concatenate(es)
+    y, _ = P.labels_from_energies(etot, quantile=0.05)
+    tr = P.Trainer(P.init_params(7), max_batch=2048)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    tr.fit(feats, y, epochs=20, batch=512, lr=1e-3)
+    ev1.record()
+    torch.cuda.synchronize()
+    train_ms = ev0.elapsed_time(ev1)
+    params = tr.params()
+    tr.close()
+    cps = (1, 2, 4, 8, 16, 32, 64)
+    reps = 4
+    curves = {}
+    for mode in (A.PROPOSAL_UNIFORM, A.PROPOSAL_LEARNED):
+        errs = {c: [] for c in cps}
+        mspf = []
+        for r in range(reps):
+            out, ms = run(mode, 100 + r, max(cps), params if mode == A.PROPOSAL_LEARNED else None, cps)
+            for c in cps:
+                errs[c].append(out[c][0] - judge)
+            mspf.append(ms / max(cps))
+        rms = {c: float(np.sqrt(np.mean(np.square(errs[c])))) for c in cps}
+        m = float(np.mean(mspf))
+        hit = next((c for c in cps if rms[c] <= 0.05), None)
+        curves["uniform" if mode == A.PROPOSAL_UNIFORM else "learned"] = {
+            "rms_error_kcal": rms, "ms_per_frame": m, "frames_to_0.05": hit,
+            "gpu_s_to_0.05": None if hit is None else hit * m / 1e3}
+    tu, tl = curves["uniform"]["gpu_s_to_0.05"], curves["learned"]["gpu_s_to_0.05"]
+    name = "ljsite" if args.solute_sites == 1 else f"ring{args.solute_sites}"
+    line = {"metric": "s to delta-mu +/-0.05 kcal/mol", "value": tl, "unit": "s", "n_gpus": 1,
+            "higher_is_better": False, "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"delta-mu-{name}-water4096-disordered", "insertions_per_frame": nins,
+                       "voxels_per_side": gv, "mix_uniform": eps, "replicas": reps,
+                       "judge": {"frames": judge_frames, "insertions": judge_frames * nins,
+                                 "delta_mu_kcal": judge, "gpu_s": judge_ms / 1e3}},
+            "uniform": curves["uniform"], "learned": curves["learned"],
+            "training_gpu_s": (sample_ms + train_ms) / 1e3,
+            "speedup_uniform_over_learned": None if (tu is None or tl is None) else tu / tl}
     print(json.dumps(line))
 
 

@@ -121,10 +121,12 @@ def _rot_from_quat(q):
                      [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
 
 
-def random_packing(n: int, box: float, rng, dmin: float = 2.5, max_tries: int = 5000):
+def random_packing(n: int, box: float, rng, dmin: float = 2.5, max_tries: int = 5000, obstacle=None,
+                   obstacle_r: float = 0.0):
     """n points in a periodic cube by random sequential addition with a minimum
-    separation `dmin`: a disordered packing with the density fluctuations and
-    cavities of a liquid (the lattice has none)."""
+    separation `dmin` (and at least `obstacle_r` from the point `obstacle`): a
+    disordered packing with the density fluctuations and cavities of a liquid
+    (the lattice has none)."""
     nc = max(1, int(box // dmin))
     h = box / nc
     cells = {}
@@ -133,6 +135,11 @@ def random_packing(n: int, box: float, rng, dmin: float = 2.5, max_tries: int = 
     while k < n:
         for _ in range(max_tries):
             p = rng.uniform(0.0, box, 3)
+            if obstacle is not None:
+                d = p - obstacle
+                d -= box * np.round(d / box)
+                if d @ d < obstacle_r * obstacle_r:
+                    continue
             c = tuple((p // h).astype(int) % nc)
             ok = True
             for dz in (-1, 0, 1):
@@ -174,7 +181,8 @@ def water_box_frame(nside: int, box: float, seed: int, jitter=0.3, avoid=None, a
     body = wat.coords - com_body[:, None]
     n = nside ** 3
     if packing == "random":
-        com = random_packing(n, box, rng)
+        com = random_packing(n, box, rng, obstacle=None if avoid is None else np.asarray(avoid, dtype=np.float64),
+                             obstacle_r=avoid_r)
     else:
         g = (np.arange(nside) + 0.5) * (box / nside)
         cz, cy, cx = np.meshgrid(g, g, g, indexing="ij")
