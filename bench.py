@@ -280,6 +280,11 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
     assert edens is not None and edens.sum() > 0
+    if ws > 1:
+        # the division's exchange (engstore's reduction, after the timed region): sums over ranks
+        from ermod_openacc_b200 import parallel
+        red, _ = parallel.engstore_all(eng, device=f"cuda:{local}")
+        assert abs(red["edens"].sum() - eng.slvmax) < 1e-6 * eng.slvmax
     value = ws * units * args.steps / (dev_ms * 1e-3)
     e2e = ws * units * args.steps / e2e_s
     paths = eng.paths()
