@@ -10,12 +10,16 @@
 // with P chosen per batch so that |w - (w_min + m q)| <= 2^-25 w_min, and
 //     C^T diag(w) C = w_min C^T C + q sum_d 2^d C^T diag(bit_d(m)) C :
 // one plain GEMM plus P GEMMs whose A operand has the insertions without
-// bit d masked out.  Counts above 255 are split into two base-256 limbs
-// (c = 256 h + l), adding the h-l, l-h and h-h products.  Every GEMM is
-// exact in INT32 (at most 4096 * 255^2 per entry); the FP64 combination
-// runs in a fixed order, so the result is deterministic.
+// bit d masked out.  Counts above 255 occur in few bins (far solvent piles
+// up near zero energy): the GEMM multiplies the low bytes l = c mod 256 and
+// k_ecorr_high adds sum_i w_i (c_b c_h - l_b l_h) for those bins in FP64 with
+// the exact weights; past kMaxHigh such bins the GEMM instead adds the
+// base-256 limb products (c = 256 h + l: h-l, l-h, h-h).  Every GEMM is exact
+// in INT32 (at most 4096 * 255^2 per entry); the FP64 combination runs in a
+// fixed order, so the result is deterministic.
 //
-// Kernel structure: a CTA per 128 x 64 tile of ecorr.  Per K tile of 128
+// Kernel structure: a CTA per 128 x 64 tile of the upper triangle of ecorr
+// (the epilogue also writes the mirror).  Per K tile of 128
 // insertions the CTA stages A (128 bin rows x 128 bytes) and up to eight
 // masked copies of B (64 bin rows x 128 bytes, one per term of the group)
 // in shared memory in the 128-byte-swizzled K-major layout, in one of two
@@ -43,6 +47,7 @@ constexpr int kTileK = 128;          // insertions per K tile (one 128-byte swiz
 constexpr int kMaxGroup = 8;         // accumulators per pass: 8 x 64 = 512 TMEM columns
 constexpr int kThreads = 256;
 constexpr int kMaxDigits = 30;
+constexpr int kMaxHigh = 64;         // bins with counts above 255 handled by the FP64 correction
 constexpr long long kSpinLimit = 1LL << 22;   // try_wait polls: a few seconds at most
 
 struct QuantParams {
@@ -141,7 +146,8 @@ __device__ __forceinline__ uint32_t expand4(uint32_t b) {
 // ---- preparation --------------------------------------------------------
 // counts[cnt][bin] (u32, batch rows) -> CT_l / CT_h [bin][kpad] (u8, insertions contiguous)
 __global__ void k_counts_to_ct(int n, int kpad, int ermax_pad, const uint32_t* __restrict__ counts,
-                               uint8_t* __restrict__ ctl, uint8_t* __restrict__ cth, int* __restrict__ high) {
+                               uint8_t* __restrict__ ctl, uint8_t* __restrict__ cth, int* __restrict__ high,
+                               int* __restrict__ hbin) {
   __shared__ uint32_t tile[32][33];
   const int b0 = blockIdx.x * 32, c0 = blockIdx.y * 32;  // bins, insertions
   const int tx = threadIdx.x, ty = threadIdx.y;          // (32, 8)
@@ -157,10 +163,57 @@ __global__ void k_counts_to_ct(int n, int kpad, int ermax_pad, const uint32_t* _
       const uint32_t v = tile[tx][ty + j];
       ctl[(size_t)bin * kpad + cnt] = (uint8_t)(v & 255u);
       cth[(size_t)bin * kpad + cnt] = (uint8_t)((v >> 8) & 255u);
-      hi |= v > 255u;
+      if (v > 255u) {
+        hi = 1;
+        atomicOr(&hbin[bin], 1);
+      }
     }
   }
   if (__syncthreads_or(hi) && tx == 0 && ty == 0) atomicOr(high, 1);
+}
+
+// Bins with a count above 255 in the batch, in bin order (one thread: a few
+// thousand flags).  Up to kMaxHigh of them go to the FP64 correction below and
+// the GEMM then multiplies the low bytes only; beyond that the GEMM adds the
+// base-256 limb products instead (*high stays 1).
+__global__ void k_high_list(int ermax, const int* __restrict__ hbin, int* __restrict__ hl, int* __restrict__ nh,
+                            int* __restrict__ high) {
+  if (threadIdx.x != 0) return;
+  int c = 0;
+  for (int b = 0; b < ermax; ++b)
+    if (hbin[b]) {
+      if (c < kMaxHigh) hl[c] = b;
+      ++c;
+    }
+  if (c <= kMaxHigh) {
+    *nh = c;
+    *high = 0;
+  } else {
+    *nh = 0;
+  }
+}
+
+// ecorr += sum_i w_i (C_ib C_ih - L_ib L_ih) for the high bins h (C: counts,
+// L = C mod 256, the part the low-byte GEMM added), over every bin b, and the
+// mirror element for b outside the high list.  A thread per (b, h), insertions
+// in order: FP64 with the exact weights, deterministic.
+__global__ void k_ecorr_high(int n, int ermax, int ermax_pad, const uint32_t* __restrict__ counts,
+                             const double* __restrict__ w, const int* __restrict__ hbin, const int* __restrict__ hl,
+                             const int* __restrict__ nh, double* __restrict__ ecorr) {
+  const int hi = blockIdx.y;
+  if (hi >= *nh) return;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= ermax) return;
+  const int h = hl[hi];
+  double acc = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const uint32_t cb = counts[(size_t)i * ermax_pad + b], ch = counts[(size_t)i * ermax_pad + h];
+    if (cb == 0u || ch == 0u) continue;
+    const double full = (double)cb * (double)ch, low = (double)(cb & 255u) * (double)(ch & 255u);
+    acc += w[i] * (full - low);
+  }
+  ecorr[(size_t)b * ermax + h] += acc;
+  if (!hbin[b]) ecorr[(size_t)h * ermax + b] += acc;
 }
 
 // weights -> (wmin, q, P, m_cnt), one CTA, fixed-order reductions
@@ -246,6 +299,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_ecorr_tc(int ermax, int kpad, c
   TcSmem& S = *reinterpret_cast<TcSmem*>((void*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int i0 = blockIdx.y * kTileM, j0 = blockIdx.x * kTileN;
+  // ecorr is symmetric: tiles whose columns all lie below the diagonal are the
+  // mirror of tiles computed elsewhere
+  if (j0 + kTileN <= i0) return;
   const QuantParams Q = *qp;
   const int P = Q.P;
   const int nk = kpad / kTileK;
@@ -364,10 +420,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_ecorr_tc(int ermax, int kpad, c
             for (int e = 0; e < 32; ++e) acc[e] += scale * (double)(int32_t)v[e];
           }
           if (row < ermax) {
-            double* out = ecorr + (size_t)row * ermax + j0 + cc;
+            // upper triangle and its mirror; the diagonal once
 #pragma unroll
-            for (int e = 0; e < 32; ++e)
-              if (j0 + cc + e < ermax) out[e] += acc[e];
+            for (int e = 0; e < 32; ++e) {
+              const int col = j0 + cc + e;
+              if (col >= ermax || col < row) continue;
+              ecorr[(size_t)row * ermax + col] += acc[e];
+              if (col > row) ecorr[(size_t)col * ermax + row] += acc[e];
+            }
           }
         }
       }
@@ -396,7 +456,8 @@ int ecorr_tc_available() { return 1; }
 size_t ecorr_tc_workspace(int n, int ermax) {
   const size_t kpad = (size_t)(n + kTileK - 1) / kTileK * kTileK;
   const size_t ermax_pad = (size_t)(ermax + 127) / 128 * 128;
-  return 2 * ermax_pad * kpad + 4 * kpad + (kpad / kTileK) * (kMaxDigits + 1) * 8 * 2 + 256 + 64;
+  return 2 * ermax_pad * kpad + 4 * kpad + (kpad / kTileK) * (kMaxDigits + 1) * 8 * 2 + 256 + 64 +
+         sizeof(int) * (ermax_pad + kMaxHigh + 4);
 }
 
 // ecorr += C^T diag(w) C for targets [base, base+n) of the batch starting at count_base
@@ -410,7 +471,8 @@ int launch_ecorr_tc(const DeviceState& d, int base, int n, int ermax, int ermax_
   }
   const int kpad = (n + kTileK - 1) / kTileK * kTileK;
   const size_t nbits = (size_t)(kpad / kTileK) * (kMaxDigits + 1) * 8;
-  const size_t need = 2 * (size_t)ermax_pad * kpad + 4 * (size_t)kpad + 2 * nbits + 256 + 64;
+  const size_t need = 2 * (size_t)ermax_pad * kpad + 4 * (size_t)kpad + 2 * nbits + 256 + 64 +
+                      sizeof(int) * (ermax_pad + kMaxHigh + 4);
   if (need > work_bytes) return -2;
   uint8_t* ctl = (uint8_t*)work;
   uint8_t* cth = ctl + (size_t)ermax_pad * kpad;
@@ -418,14 +480,20 @@ int launch_ecorr_tc(const DeviceState& d, int base, int n, int ermax, int ermax_
   uint16_t* gbits = (uint16_t*)(m + kpad);
   QuantParams* qp = (QuantParams*)((uint8_t*)(gbits + nbits) + ((16 - (nbits * 2) % 16) % 16));
   int* high = (int*)((uint8_t*)qp + 64);
+  int* nh = high + 1;
+  int* hl = high + 4;
+  int* hbin = hl + kMaxHigh;      // [ermax_pad]
   int* errw = &d.status->flags;   // kErrTimeout if an mbarrier wait expires
-  cudaMemsetAsync(high, 0, sizeof(int), s);
+  const uint32_t* cnt = d.counts + (size_t)(base - count_base) * ermax_pad;
+  cudaMemsetAsync(high, 0, sizeof(int) * (4 + kMaxHigh + ermax_pad), s);
   dim3 tb(32, 8), tg((ermax_pad + 31) / 32, (kpad + 31) / 32);
-  k_counts_to_ct<<<tg, tb, 0, s>>>(n, kpad, ermax_pad, d.counts + (size_t)(base - count_base) * ermax_pad, ctl, cth,
-                                   high);
+  k_counts_to_ct<<<tg, tb, 0, s>>>(n, kpad, ermax_pad, cnt, ctl, cth, high, hbin);
+  k_high_list<<<1, 32, 0, s>>>(ermax, hbin, hl, nh, high);
   k_quantize<<<1, 1024, 0, s>>>(base, n, kpad, weight_bits > 0 ? weight_bits : 24, d.w, m, gbits, qp, high);
   dim3 gg((ermax_pad + kTileN - 1) / kTileN, (ermax_pad + kTileM - 1) / kTileM);
   k_ecorr_tc<<<gg, kThreads, kSmemBytes, s>>>(ermax, kpad, ctl, cth, gbits, qp, d.ecorr, errw);
+  k_ecorr_high<<<dim3((ermax + 127) / 128, kMaxHigh), 128, 0, s>>>(n, ermax, ermax_pad, cnt, d.w + base, hbin, hl,
+                                                                     nh, d.ecorr);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 

@@ -863,10 +863,11 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
         const int rc = launch_ecorr_tc(d, bb, nbatch, ctx->ermax, ctx->ermax_pad, bb, p.weight_bits, ctx->tc_work,
                                        ctx->tc_work_bytes, st);
         if (rc != 0) return set_error(ctx, ERMOD_ERR_CUDA, "ecorr_tc");
+        nl += 5;   // counts transpose, high-count list, weight digits, GEMM, high-count correction
       } else {
         launch_ecorr_simt(d, bb, nbatch, ctx->ermax, ctx->ermax_pad, bb, st);
+        nl += 1;
       }
-      nl += 1;
     }
     M(kStEcorr);
   }
