@@ -667,6 +667,16 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
   P.bare = p.cltype == ERMOD_EL_COULOMB;
   a.slvmax = ctx->slvmax; a.natoms = ctx->natoms; a.nsite = ctx->s; a.maxdst = ctx->maxdst;
   a.K1 = K1; a.K2 = K2; a.K3 = K3; a.order = pme ? p.splodr : 1; a.Kh1 = K1 / 2 + 1;
+  // Fused solve: planes k1 whose every mode has exp(-pi^2 |k|^2 / screen^2) < kPlaneCut are not
+  // transformed (|k| >= k1 / |a1| in plane k1, a1 the first cell vector).  Their share of any
+  // molecule energy is below 1e-9 of the k = 0 Gaussian weight per mode, far under FP32 rounding.
+  a.k1max = K1 / 2;
+  if (pme) {
+    const double a1 = std::sqrt(c[0][0] * c[0][0] + c[1][0] * c[1][0] + c[2][0] * c[2][0]);
+    const double kPlaneCut = 1e-9;
+    const double mcut = std::sqrt(-std::log(kPlaneCut)) * (double)p.screen * a1 / kPi;
+    a.k1max = std::max(0, std::min(K1 / 2, (int)std::floor(mcut) + 1));
+  }
   a.ljtype_max = ctx->ljtype_max;
   a.pme = pme;
   a.pivol = pme ? kPi / ((double)p.screen * (double)p.screen) / vold : 0.0;

@@ -32,6 +32,7 @@ struct FrameArgs {
   PairParams pp;
   int slvmax, natoms, nsite, maxdst;
   int K1, K2, K3, order, Kh1;      // Kh1 = K1/2+1
+  int k1max;                       // last k1 plane the fused PME solve transforms (see frame_plan)
   int ljtype_max;
   int pme;
   double pivol;                    // pi / screen^2 / volume (residual terms, engproc.F90:974,994)

@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(256) k_site_tables(FrameArgs a, int base, int 
 }
 
 // ---------------------------------------------------------------------------
-// k_pme_plane<LK2, LK3, DIRECT>: grid (Kh1, targets), K2*K3/E threads.  Thread
+// k_pme_plane<LK2, LK3, DIRECT>: grid (k1max + 1, targets), K2*K3/E threads.  Thread
 // tid owns the points (k2 = tid mod K2, k3 = (tid / K2) * E + e), e < E.
 // Solute sites are staged ts at a time from the batch's site tables.
 // ---------------------------------------------------------------------------
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
     if (tid == 0) {
       partial[(size_t)b * Kh1 + k1] = v;
       __threadfence();
-      last = atomicAdd(&done[b], 1u) == (unsigned)Kh1 - 1;
+      last = atomicAdd(&done[b], 1u) == gridDim.x - 1;
     }
   }
   __syncthreads();
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
     __threadfence();
     double sum = 0.0;
     const volatile double* pp = partial + (size_t)b * Kh1;
-    for (int i = 0; i < Kh1; ++i) sum += pp[i];
+    for (int i = 0; i < (int)gridDim.x; ++i) sum += pp[i];
     selfrec[base + b] = sum;
     done[b] = 0u;
   }
@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
         const int j = x & (G2 - 1), r = x >> LG2;   // r = k1 * 32 + b
         const int b = r & 31, k1 = r >> 5;
         dst[u] = k1 * TP + j * 33 + b;
-        if (b < nb) v[u] = Y[(((size_t)b * Kh1 + k1) * K3 + n3) * K2 + n2g + j];
+        if (b < nb && k1 <= a.k1max) v[u] = Y[(((size_t)b * Kh1 + k1) * K3 + n3) * K2 + n2g + j];
       }
     }
 #pragma unroll
@@ -545,7 +545,7 @@ cudaError_t plane_attr(const FrameArgs& a) {
 template <int L2, int L3>
 void plane_launch(const FrameArgs& a, const DeviceState& d, int base, int tbase, int nb, bool direct, cudaStream_t s) {
   using C = PlaneCfg<L2, L3>;
-  const dim3 grid(a.Kh1, nb);
+  const dim3 grid(a.k1max + 1, nb);   // planes above k1max carry no influence-function weight
   const int ts = site_tile(a);
   if (direct)
     k_pme_plane<L2, L3, true><<<grid, C::NTHR, plane_smem(a, true), s>>>(
