@@ -172,48 +172,85 @@ __global__ void k_counts_to_ct(int n, int kpad, int ermax_pad, const uint32_t* _
   if (__syncthreads_or(hi) && tx == 0 && ty == 0) atomicOr(high, 1);
 }
 
-// Bins with a count above 255 in the batch, in bin order (one thread: a few
-// thousand flags).  Up to kMaxHigh of them go to the FP64 correction below and
-// the GEMM then multiplies the low bytes only; beyond that the GEMM adds the
-// base-256 limb products instead (*high stays 1).
-__global__ void k_high_list(int ermax, const int* __restrict__ hbin, int* __restrict__ hl, int* __restrict__ nh,
-                            int* __restrict__ high) {
-  if (threadIdx.x != 0) return;
-  int c = 0;
-  for (int b = 0; b < ermax; ++b)
-    if (hbin[b]) {
-      if (c < kMaxHigh) hl[c] = b;
-      ++c;
+// Bins with a count above 255 in the batch, in bin order (one block: ballot
+// and a fixed-order scan of the per-warp counts).  Up to kMaxHigh of them go
+// to the FP64 correction below and the GEMM then multiplies the low bytes only;
+// beyond that the GEMM adds the base-256 limb products instead (*high stays 1).
+constexpr int kListThreads = 1024;
+
+__global__ void __launch_bounds__(kListThreads) k_high_list(int ermax, const int* __restrict__ hbin,
+                                                            int* __restrict__ hl, int* __restrict__ nh,
+                                                            int* __restrict__ high) {
+  __shared__ int wcount[32];
+  __shared__ int base;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) base = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < ermax; b0 += kListThreads) {
+    const int b = b0 + tid;
+    const bool f = b < ermax && hbin[b] != 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wcount[warp] = __popc(bal);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < warp; ++w) off += wcount[w];
+    off += __popc(bal & ((1u << lane) - 1u));
+    if (f && off < kMaxHigh) hl[off] = b;
+    __syncthreads();
+    if (tid == 0) {
+      int t = 0;
+      for (int w = 0; w < kListThreads / 32; ++w) t += wcount[w];
+      base += t;
     }
-  if (c <= kMaxHigh) {
-    *nh = c;
-    *high = 0;
-  } else {
-    *nh = 0;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (base <= kMaxHigh) {
+      *nh = base;
+      *high = 0;
+    } else {
+      *nh = 0;
+    }
   }
 }
 
 // ecorr += sum_i w_i (C_ib C_ih - L_ib L_ih) for the high bins h (C: counts,
 // L = C mod 256, the part the low-byte GEMM added), over every bin b, and the
-// mirror element for b outside the high list.  A thread per (b, h), insertions
-// in order: FP64 with the exact weights, deterministic.
-__global__ void k_ecorr_high(int n, int ermax, int ermax_pad, const uint32_t* __restrict__ counts,
-                             const double* __restrict__ w, const int* __restrict__ hbin, const int* __restrict__ hl,
-                             const int* __restrict__ nh, double* __restrict__ ecorr) {
+// mirror element for b outside the high list.  A CTA per (32 bins, high bin):
+// lane = bin, each warp a contiguous slice of the insertions, the warps'
+// partial sums added in warp order -- FP64 with the exact weights,
+// deterministic.
+constexpr int kHighWarps = 16;
+
+__global__ void __launch_bounds__(kHighWarps * 32) k_ecorr_high(int n, int ermax, int ermax_pad,
+    const uint32_t* __restrict__ counts, const double* __restrict__ w, const int* __restrict__ hbin,
+    const int* __restrict__ hl, const int* __restrict__ nh, double* __restrict__ ecorr) {
+  __shared__ double red[kHighWarps][32];
   const int hi = blockIdx.y;
   if (hi >= *nh) return;
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= ermax) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int b = blockIdx.x * 32 + lane;
   const int h = hl[hi];
+  const int per = (n + kHighWarps - 1) / kHighWarps;
+  const int i0 = warp * per, i1 = min(n, i0 + per);
   double acc = 0.0;
-  for (int i = 0; i < n; ++i) {
-    const uint32_t cb = counts[(size_t)i * ermax_pad + b], ch = counts[(size_t)i * ermax_pad + h];
-    if (cb == 0u || ch == 0u) continue;
-    const double full = (double)cb * (double)ch, low = (double)(cb & 255u) * (double)(ch & 255u);
-    acc += w[i] * (full - low);
+  if (b < ermax)
+    for (int i = i0; i < i1; ++i) {
+      const uint32_t ch = counts[(size_t)i * ermax_pad + h];
+      if (ch == 0u) continue;
+      const uint32_t cb = counts[(size_t)i * ermax_pad + b];
+      if (cb == 0u) continue;
+      const double full = (double)cb * (double)ch, low = (double)(cb & 255u) * (double)(ch & 255u);
+      acc += w[i] * (full - low);
+    }
+  red[warp][lane] = acc;
+  __syncthreads();
+  if (warp == 0 && b < ermax) {
+    double t = 0.0;
+    for (int k = 0; k < kHighWarps; ++k) t += red[k][lane];
+    ecorr[(size_t)b * ermax + h] += t;
+    if (!hbin[b]) ecorr[(size_t)h * ermax + b] += t;
   }
-  ecorr[(size_t)b * ermax + h] += acc;
-  if (!hbin[b]) ecorr[(size_t)h * ermax + b] += acc;
 }
 
 // weights -> (wmin, q, P, m_cnt), one CTA, fixed-order reductions
@@ -488,12 +525,12 @@ int launch_ecorr_tc(const DeviceState& d, int base, int n, int ermax, int ermax_
   cudaMemsetAsync(high, 0, sizeof(int) * (4 + kMaxHigh + ermax_pad), s);
   dim3 tb(32, 8), tg((ermax_pad + 31) / 32, (kpad + 31) / 32);
   k_counts_to_ct<<<tg, tb, 0, s>>>(n, kpad, ermax_pad, cnt, ctl, cth, high, hbin);
-  k_high_list<<<1, 32, 0, s>>>(ermax, hbin, hl, nh, high);
+  k_high_list<<<1, kListThreads, 0, s>>>(ermax, hbin, hl, nh, high);
   k_quantize<<<1, 1024, 0, s>>>(base, n, kpad, weight_bits > 0 ? weight_bits : 24, d.w, m, gbits, qp, high);
   dim3 gg((ermax_pad + kTileN - 1) / kTileN, (ermax_pad + kTileM - 1) / kTileM);
   k_ecorr_tc<<<gg, kThreads, kSmemBytes, s>>>(ermax, kpad, ctl, cth, gbits, qp, d.ecorr, errw);
-  k_ecorr_high<<<dim3((ermax + 127) / 128, kMaxHigh), 128, 0, s>>>(n, ermax, ermax_pad, cnt, d.w + base, hbin, hl,
-                                                                     nh, d.ecorr);
+  k_ecorr_high<<<dim3((ermax + 31) / 32, kMaxHigh), kHighWarps * 32, 0, s>>>(n, ermax, ermax_pad, cnt, d.w + base,
+                                                                              hbin, hl, nh, d.ecorr);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 
