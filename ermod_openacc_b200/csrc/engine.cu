@@ -63,7 +63,7 @@ struct ermod_ctx {
   std::vector<double> uvcrd, escrd;
   std::vector<int> uvmax, uvsoft;
   DeviceState d;
-  int chunk = 32, batch = 0, ncell_cap = 0;
+  int chunk = kChunk, batch = 0, ncell_cap = 0;
   cufftHandle r2c = 0, c2r = 0;
   bool plans = false;
   void* tc_work = nullptr;
@@ -356,7 +356,7 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   for (int a : atom_lj) if (a < 0 || a >= ctx->ljtype_max) return bad(ERMOD_ERR_ARG, "set_ljt");
   for (int a : slt_lj) if (a < 0 || a >= ctx->ljtype_max) return bad(ERMOD_ERR_ARG, "set_ljt");
   // engine shape
-  ctx->chunk = 32;
+  ctx->chunk = kChunk;
   const int K1 = p.ms1max, K2 = p.ms2max, K3 = p.ms3max, Kh1 = K1 / 2 + 1;
   const bool pme = p.cltype == ERMOD_EL_PME;
   ctx->batch = p.ecorr_batch > 0 ? p.ecorr_batch : 4096;

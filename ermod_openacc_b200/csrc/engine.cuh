@@ -18,6 +18,7 @@ constexpr int kMaxLjTypes = 64;
 constexpr int kInflBlocks = 64;    // CTAs per target in the influence multiply
 constexpr int kEdensSlices = 32;   // target slices of the edens reduction
 constexpr int kMaxGrid = 256;      // largest PME grid dimension (x rows are one CTA dimension)
+constexpr int kChunk = 32;         // PME solves per chunk: one warp lane per target
 constexpr int kMlpIn = 64;         // proposal network: 4x4x4 local density inputs
 constexpr int kMlpHidden = 128;    // width of its three hidden layers
 

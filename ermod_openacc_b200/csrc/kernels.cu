@@ -813,6 +813,37 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
           // the stencil rows of CS planes c3 in flight at once (one 128-byte row per load):
           // the whole 4^3 stencil for order 4, one 6^2 plane for order 6
           constexpr int CS = NO <= 4 ? NO : 1;
+          if (gd.x >= NO - 1 && gd.y >= NO - 1 && gd.z >= NO - 1 && gd.x < K1 && gd.y < K2 && gd.z < K3) {
+            // no stencil index wraps (most sites): every point is a fixed offset from one
+            // pointer, the n1 neighbours compile-time ones (phi rows are kChunk floats)
+            const float* p0 = phi + ((size_t)(gd.z * K2 + gd.y) * K1 + gd.x) * kChunk + b;
+            const size_t s2 = (size_t)K1 * kChunk, s3 = (size_t)K2 * s2;
+#pragma unroll
+            for (int c30 = 0; c30 < NO; c30 += CS) {
+              float v[CS * NO * NO];
+#pragma unroll
+              for (int cs = 0; cs < CS; ++cs)
+#pragma unroll
+                for (int c2 = 0; c2 < NO; ++c2) {
+                  const float* rowp = p0 - (size_t)(c30 + cs) * s3 - (size_t)c2 * s2;
+#pragma unroll
+                  for (int c1 = 0; c1 < NO; ++c1) v[(cs * NO + c2) * NO + c1] = rowp[-c1 * kChunk];
+                }
+#pragma unroll
+              for (int cs = 0; cs < CS; ++cs) {
+                const float fac1 = q * w[2 * NO + c30 + cs];
+#pragma unroll
+                for (int c2 = 0; c2 < NO; ++c2) {
+                  const float fac2 = fac1 * w[NO + c2];
+                  float part = 0.0f;
+#pragma unroll
+                  for (int c1 = 0; c1 < NO; ++c1) part += (fac2 * w[c1]) * v[(cs * NO + c2) * NO + c1];
+                  e += (double)part;
+                }
+              }
+            }
+            continue;
+          }
           int r1[NO];
 #pragma unroll
           for (int c1 = 0; c1 < NO; ++c1) r1[c1] = wrapk(gd.x - c1, K1) * chunk + b;

@@ -18,11 +18,12 @@
 //                   inverse 2-D FFT over (k2, k3) in shared memory.  The plane
 //                   Y[b][k1][n3][n2] is written once (it stays in L2 for the
 //                   next kernel).
-//   k_pme_rows      CTA = (n3, group of n2 rows), all 32 targets: the
-//                   complex-to-real transform along k1 (a half-length
-//                   complex FFT of the Hermitian-packed row), written
-//                   straight into the insertion-fastest potential layout
-//                   phi[(n3*K2 + n2)*K1 + n1][32] that the gather reads.
+//   k_pme_lines     a thread per (n3, n2) line and target: the complex-to-real
+//                   transform along k1 (a half-length complex FFT of the
+//                   Hermitian-packed line) in registers, written straight
+//                   into the insertion-fastest potential layout
+//                   phi[(n3*K2 + n2)*K1 + n1][32] that the gather reads
+//                   (K1 <= 64; k_pme_rows does K1 = 128 in shared memory).
 //
 // The FFTs are radix-8/4 Stockham stages (Govindaraju et al., "High
 // performance discrete Fourier transforms on graphics processors", SC08):
@@ -34,57 +35,13 @@
 #include <cmath>
 
 #include "engine.cuh"
+#include "regfft.cuh"
 
 namespace erm {
 
+using namespace fft;
+
 namespace {
-
-constexpr float kRsqrt2 = 0.70710678118654752f;
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-// a * (+i) for the inverse direction, a * (-i) for the forward one
-template <bool INV>
-__device__ __forceinline__ float2 rot90(float2 a) {
-  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
-}
-
-// X[q] = sum_r v[r] w^(rq), w = exp(-+2 pi i / 4)
-template <bool INV>
-__device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2& v3) {
-  const float2 a0 = cadd(v0, v2), a1 = csub(v0, v2);
-  const float2 b0 = cadd(v1, v3), b1 = rot90<INV>(csub(v1, v3));
-  v0 = cadd(a0, b0);
-  v2 = csub(a0, b0);
-  v1 = cadd(a1, b1);
-  v3 = csub(a1, b1);
-}
-
-template <int R, bool INV>
-__device__ __forceinline__ void dft(float2 (&v)[R]) {
-  static_assert(R == 4 || R == 8, "radix 4 or 8");
-  if constexpr (R == 4) {
-    dft4<INV>(v[0], v[1], v[2], v[3]);
-  } else {
-    // radix 8 as two radix-4 transforms of the even and odd inputs
-    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-    float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
-    dft4<INV>(e0, e1, e2, e3);
-    dft4<INV>(o0, o1, o2, o3);
-    // o_q *= w8^q, w8 = exp(-+2 pi i / 8)
-    const float s = INV ? 1.f : -1.f;
-    o1 = make_float2((o1.x - s * o1.y) * kRsqrt2, (o1.y + s * o1.x) * kRsqrt2);
-    o2 = rot90<INV>(o2);
-    o3 = make_float2((-o3.x - s * o3.y) * kRsqrt2, (-o3.y + s * o3.x) * kRsqrt2);
-    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
-    v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
-    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
-    v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
-  }
-}
 
 // Placement of a batch of 2^LNB transforms of length 2^LN in shared memory:
 // transform bt starts at (bt >> LBG) * BPITCH + (bt & (2^LBG - 1)) * BSTRIDE
@@ -156,6 +113,7 @@ constexpr int kSiteTile = 32;                  // solute sites staged in shared 
 constexpr int kTabPairs = 8;                   // (target, site) pairs per CTA of k_site_tables
 constexpr int kStn = 2 + 2 * kMaxOrder;        // stencil record: g2, g3, w2[kMaxOrder], w3[kMaxOrder]
 constexpr int kRowThreads = 512;
+constexpr int kLineRows = 8;                   // n2 rows per CTA of k_pme_lines (a warp each)
 constexpr int kLoadBatch = 8;                  // global loads a thread keeps in flight while staging
 
 template <int LK2, int LK3>
@@ -504,6 +462,74 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
 }
 
 // ---------------------------------------------------------------------------
+// k_pme_lines<LM>: the same transform for K1 = 2M <= 64, a thread per line.
+// Grid (K3, K2 / kLineRows), 32 * kLineRows threads; warp j takes row
+// n2 = blockIdx.y * kLineRows + j, lane b the target.  The CTA first stages
+// the half spectra Y[b][k1][n3][n2], k1 <= k1max, of its kLineRows rows and
+// 32 targets in shared memory (16-byte loads along n2; S[k1][n2][b] with a
+// row pitch of 34, so the staging stores and the per-line reads are free of
+// bank conflicts).  Each thread then packs its line (hermitian_pack),
+// transforms it in registers (idft_reg) and writes phi[p][b] for the 2M
+// points of the line: every store of a warp is one 128-byte row of the
+// insertion-fastest layout.
+// ---------------------------------------------------------------------------
+constexpr int kLinePitch = 34;
+
+size_t lines_smem(int M) { return sizeof(float2) * (size_t)(M + 1) * kLineRows * kLinePitch; }
+
+template <int LM>
+__global__ void __launch_bounds__(32 * kLineRows, 2) k_pme_lines(FrameArgs a, int nb, const float2* __restrict__ Y,
+                                                                 Tw64 tw, float* __restrict__ phi) {
+  constexpr int M = 1 << LM, K1 = 2 * M, Kh1 = M + 1, NT = 32 * kLineRows;
+  constexpr int ROW = kLineRows * kLinePitch;             // float2 per k1 row of S
+  static_assert(kLineRows == 8, "a float4 carries two of the CTA's 8 rows; 4 float4 per (target, k1)");
+  extern __shared__ __align__(16) float2 S[];              // [M + 1][kLineRows][kLinePitch]
+  const int K2 = a.K2, K3 = a.K3;
+  const int tid = threadIdx.x;
+  const int n3 = blockIdx.x, n2g = blockIdx.y * kLineRows;
+  const size_t plane = (size_t)K3 * K2;
+  const int kmax = a.k1max;
+  {
+    // staging item (k1, bs, q): the float4 of rows 2q, 2q+1 of target bs at k1
+    const int q = tid & 3, bs = (tid >> 2) & 31;
+    const bool on = bs < nb;
+    const float4* src = (const float4*)(Y + (size_t)bs * Kh1 * plane + (size_t)n3 * K2 + n2g + 2 * q);
+    float2* dst = S + (2 * q) * kLinePitch + bs;
+    // every load is issued before the first store, from a clamped (always valid) k1, so that
+    // they are all in flight together; rows above k1max and targets past nb are not used
+    constexpr int PER = NT / 128;                           // k1 rows per pass of the CTA
+    constexpr int NPASS = (M + PER) / PER;                  // passes covering k1 = 0..M
+    float4 v[NPASS];
+#pragma unroll
+    for (int u = 0; u < NPASS; ++u) v[u] = __ldg(src + (size_t)min(u * PER + tid / 128, kmax) * (plane / 2));
+#pragma unroll
+    for (int u = 0; u < NPASS; ++u) {
+      const int k1 = u * PER + tid / 128;
+      if (k1 <= kmax) {
+        const float4 t = on ? v[u] : make_float4(0.f, 0.f, 0.f, 0.f);
+        dst[k1 * ROW] = make_float2(t.x, t.y);
+        dst[k1 * ROW + kLinePitch] = make_float2(t.z, t.w);
+      }
+    }
+  }
+  __syncthreads();
+  const int b = tid & 31, j = tid >> 5;
+  const float2* line = S + j * kLinePitch + b;
+  float2 Z[M];
+#pragma unroll
+  for (int k = 0; k < M; ++k) Z[k] = k <= kmax ? line[k * ROW] : make_float2(0.f, 0.f);
+  const float2 xM = M <= kmax ? line[M * ROW] : make_float2(0.f, 0.f);
+  hermitian_pack<LM>(Z, xM, tw);
+  idft_reg<LM>(Z, tw);
+  float* o = phi + (size_t)(n3 * K2 + n2g + j) * K1 * 32 + b;
+#pragma unroll
+  for (int n = 0; n < M; ++n) {
+    o[(2 * n) * 32] = Z[n].x;
+    o[(2 * n + 1) * 32] = Z[n].y;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 namespace {
@@ -576,9 +602,9 @@ int setup_fused(const FrameArgs& a) {
   if (e != cudaSuccess) return -1;
   const int lm = lg(a.K1 / 2);
   const int sm = (int)rows_smem(a);
-  if (lm == 3) e = cudaFuncSetAttribute(k_pme_rows<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (lm == 4) e = cudaFuncSetAttribute(k_pme_rows<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (lm == 5) e = cudaFuncSetAttribute(k_pme_rows<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (lm == 3) e = cudaFuncSetAttribute(k_pme_lines<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem(8));
+  if (lm == 4) e = cudaFuncSetAttribute(k_pme_lines<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem(16));
+  if (lm == 5) e = cudaFuncSetAttribute(k_pme_lines<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem(32));
   if (lm == 6) e = cudaFuncSetAttribute(k_pme_rows<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   return e == cudaSuccess ? 0 : -1;
 }
@@ -618,14 +644,30 @@ void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int tb
 #undef ERM_LAUNCH
 }
 
+namespace {
+Tw64 make_tw64() {
+  Tw64 t;
+  for (int m = 0; m < 64; ++m) {
+    const double ang = 2.0 * kPi * (double)m / 64.0;
+    t.w[m] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
+  }
+  return t;
+}
+}  // namespace
+
 void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int nb, cudaStream_t s) {
+  static const Tw64 tw = make_tw64();
+  const dim3 lgrid(a.K3, a.K2 / kLineRows);
+  switch (lg(a.K1 / 2)) {
+    case 3: k_pme_lines<3><<<lgrid, 32 * kLineRows, lines_smem(1 << 3), s>>>(a, nb, d.spec, tw, d.phi); return;
+    case 4: k_pme_lines<4><<<lgrid, 32 * kLineRows, lines_smem(1 << 4), s>>>(a, nb, d.spec, tw, d.phi); return;
+    case 5: k_pme_lines<5><<<lgrid, 32 * kLineRows, lines_smem(1 << 5), s>>>(a, nb, d.spec, tw, d.phi); return;
+    default: break;
+  }
   const int M = a.K1 / 2, G2 = 256 / M;
   const dim3 grid(a.K3, a.K2 / G2);
   const size_t sm = rows_smem(a);
   switch (lg(M)) {
-    case 3: k_pme_rows<3><<<grid, kRowThreads, sm, s>>>(a, nb, d.spec, d.fft_tw, d.phi); break;
-    case 4: k_pme_rows<4><<<grid, kRowThreads, sm, s>>>(a, nb, d.spec, d.fft_tw, d.phi); break;
-    case 5: k_pme_rows<5><<<grid, kRowThreads, sm, s>>>(a, nb, d.spec, d.fft_tw, d.phi); break;
     default: k_pme_rows<6><<<grid, kRowThreads, sm, s>>>(a, nb, d.spec, d.fft_tw, d.phi); break;
   }
 }
