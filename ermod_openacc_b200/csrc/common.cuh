@@ -149,6 +149,15 @@ __device__ __forceinline__ int wrapk(int r, int K) {
   return r - ((r >= K) ? K : 0);
 }
 
+// Programmatic dependent launch (PTX griddepcontrol): a kernel launched with
+// programmatic stream serialisation may start while its predecessor in the
+// stream is still running.  grid_dep_wait() blocks until the predecessor has
+// completed and its memory is visible (a no-op without such a predecessor);
+// grid_dep_launch() lets the successor start once every CTA of this grid has
+// called it or exited.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

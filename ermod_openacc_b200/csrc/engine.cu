@@ -831,12 +831,15 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
       M(kStSiteTab);
       nl += 1;
     }
+    // Fused solve, untimed: each chunk kernel may start while its predecessor finishes
+    // (programmatic dependent launch; the first plane of a batch follows the site tables).
+    const bool pdl = pme && ctx->spath != 1 && !timed;
     for (int cb = bb; cb < bb + nbatch; cb += chunk) {
       const int nb = std::min(chunk, bb + nbatch - cb);
       if (pme && ctx->spath != 1) {
-        launch_pme_plane(a, d, cb, cb - bb, nb, ctx->spath == 2, st);
+        launch_pme_plane(a, d, cb - bb, nb, ctx->spath == 2, pdl && cb > bb, st);
         M(kStPlane);
-        launch_pme_rows(a, d, nb, st);
+        launch_pme_rows(a, d, cb, nb, pdl, st);
         M(kStRows);
         nl += 2;
       } else if (pme) {
@@ -854,7 +857,7 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
         M(kStTranspose);
         nl += 1;
       }
-      launch_gather(a, d, cb, bb, nb, chunk, ctx->batch, st);
+      launch_gather(a, d, cb, bb, nb, chunk, ctx->batch, pdl, st);
       M(kStGather);
       nl += 1;
     }

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/ermod_b200.h"
@@ -44,6 +45,23 @@ struct FrameArgs {
 };
 
 // Device-resident state of one context.
+// Launch `k` on `s`, with programmatic stream serialisation when `pdl` (the
+// kernel orders itself against its predecessor with grid_dep_wait()).
+template <class... P, class... A>
+cudaError_t launch_k(bool pdl, dim3 grid, dim3 block, size_t smem, cudaStream_t s, void (*k)(P...), A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
 struct DeviceState {
   // topology (physical molecules in tagpt order)
   int* molbeg = nullptr;     // [slvmax+1]
@@ -167,16 +185,16 @@ void fused_twiddles(int K1, int K2, int K3, std::vector<float2>& tw, std::vector
 size_t fused_sitetab_elems(const FrameArgs& a, int batch, bool direct);
 size_t fused_sitestn_elems(const FrameArgs& a, int batch);
 void launch_site_tables(const FrameArgs& a, const DeviceState& d, int bb, int nbatch, bool direct, cudaStream_t s);
-void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int tbase, int nb, bool direct,
+void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int tbase, int nb, bool direct, bool pdl,
                       cudaStream_t s);
-void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int nb, cudaStream_t s);
+void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int base, int nb, bool pdl, cudaStream_t s);
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
 
 struct BinArgs {
   int ermax, ermax_pad, numslv, slttype;
 };
 void launch_gather(const FrameArgs& a, const DeviceState& d, int base, int bb, int nb, int chunk, int batch,
-                   cudaStream_t s);
+                   bool pdl, cudaStream_t s);
 void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int slvmax, cudaStream_t s);
 int setup_bin_smem(const BinArgs& ba);
 

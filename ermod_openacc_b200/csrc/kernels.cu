@@ -800,6 +800,8 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
   const int excl = (active && tgt_mol) ? tgt_mol[cnt] : -1;
   const int n = NO > 0 ? NO : a.order;
   const int K1 = a.K1, K2 = a.K2, K3 = a.K3;
+  grid_dep_wait();                                    // the potential grid of this chunk is complete
+  grid_dep_launch();                                  // the next chunk's planes may start filling the tail
   for (int m = gw; m < a.slvmax; m += nwt) {
     const int k = molsorted[m];
     double e = active ? Ereal[(size_t)k * batch + bi] : 0.0;
@@ -902,12 +904,14 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
 }
 
 void launch_gather(const FrameArgs& a, const DeviceState& d, int base, int bb, int nb, int chunk, int batch,
-                   cudaStream_t s) {
+                   bool pdl, cudaStream_t s) {
   int blocks = (a.slvmax * 32 + kGatherThreads - 1) / kGatherThreads;
   if (blocks > 148 * 8) blocks = 148 * 8;
   if (blocks < 1) blocks = 1;
-#define ERM_GATHER(NO) k_gather<NO><<<blocks, kGatherThreads, 0, s>>>(a, base, bb, nb, chunk, batch, d.molsorted, \
-      d.molbeg, d.molq, d.atom_q, d.spl, d.grd, d.phi, d.E, d.tgtq, d.tgt_mol, d.Etot)
+#define ERM_GATHER(NO) launch_k(pdl, blocks, kGatherThreads, 0, s, k_gather<NO>, a, base, bb, nb, chunk, batch, \
+      (const int*)d.molsorted, (const int*)d.molbeg, (const float*)d.molq, (const float*)d.atom_q,         \
+      (const float*)d.spl, (const int4*)d.grd, (const float*)d.phi, (const double*)d.E,                     \
+      (const double*)d.tgtq, (const int*)d.tgt_mol, d.Etot)
   if (a.pme && a.order == 4) ERM_GATHER(4);
   else if (a.pme && a.order == 6) ERM_GATHER(6);
   else ERM_GATHER(0);

@@ -113,7 +113,7 @@ constexpr int kSiteTile = 32;                  // solute sites staged in shared 
 constexpr int kTabPairs = 8;                   // (target, site) pairs per CTA of k_site_tables
 constexpr int kStn = 2 + 2 * kMaxOrder;        // stencil record: g2, g3, w2[kMaxOrder], w3[kMaxOrder]
 constexpr int kRowThreads = 512;
-constexpr int kLineRows = 8;                   // n2 rows per CTA of k_pme_lines (a warp each)
+constexpr int kLineRows = 4;                   // n2 rows per CTA of k_pme_lines (a warp each): 4 or 8
 constexpr int kLoadBatch = 8;                  // global loads a thread keeps in flight while staging
 
 template <int LK2, int LK3>
@@ -121,7 +121,7 @@ struct PlaneCfg {
   static constexpr int K2 = 1 << LK2, K3 = 1 << LK3, PITCH = K2 + 1;
   static constexpr int E = LK2 + LK3 <= 12 ? 16 : 32;     // plane points per thread
   static constexpr int NTHR = (K2 * K3) / E;
-  static constexpr int MINB = E == 16 ? 4 : 1;
+  static constexpr int MINB = E == 16 ? 3 : 1;
   // plane spreading accumulates in 2^-40 fixed point in shared memory when the
   // int64 plane fits beside the FP32 plane (up to 8192 points)
   static constexpr bool FIXED = K2 * K3 <= 8192;
@@ -205,9 +205,9 @@ __global__ void __launch_bounds__(256) k_site_tables(FrameArgs a, int base, int 
 // ---------------------------------------------------------------------------
 template <int LK2, int LK3, bool DIRECT>
 __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::MINB) k_pme_plane(FrameArgs a,
-    int base, int tbase, int ts, const float2* __restrict__ tab, const float* __restrict__ stn,
+    int tbase, int ts, const float2* __restrict__ tab, const float* __restrict__ stn,
     const float* __restrict__ engfacT, const float2* __restrict__ fft_tw, float2* __restrict__ Y,
-    double* __restrict__ partial, unsigned int* __restrict__ done, double* __restrict__ selfrec) {
+    double* __restrict__ partial) {
   using C = PlaneCfg<LK2, LK3>;
   constexpr int K2 = C::K2, K3 = C::K3, PITCH = C::PITCH, E = C::E, NTHR = C::NTHR;
   extern __shared__ __align__(16) unsigned char psm[];
@@ -353,36 +353,39 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
   __syncthreads();
   fft_batch<Rows, NTHR, true>(plane, tw2, tid);
   fft_batch<Cols, NTHR, true>(plane, tw3, tid);
+  grid_dep_launch();                                  // the k1 transform may start filling the tail
   float2* y = Y + ((size_t)b * Kh1 + k1) * K3 * K2;
 #pragma unroll
   for (int e = 0; e < E; ++e) {
     const int p = tid + e * NTHR;
     y[p] = plane[(p >> LK2) * PITCH + (p & (K2 - 1))];
   }
-  // deterministic self-energy reduction over the planes of this target
+  // the plane's share of the self energy, reduced in a fixed order; the k1 transform sums
+  // the planes of each target (self_energy_sum)
   __shared__ double red[32];
-  __shared__ bool last;
   self = warp_sum(self);
   if ((tid & 31) == 0) red[tid >> 5] = self;
   __syncthreads();
   if (tid < 32) {
     double v = tid < (NTHR >> 5) ? red[tid] : 0.0;
     v = warp_sum(v);
-    if (tid == 0) {
-      partial[(size_t)b * Kh1 + k1] = v;
-      __threadfence();
-      last = atomicAdd(&done[b], 1u) == gridDim.x - 1;
-    }
+    if (tid == 0) partial[(size_t)b * Kh1 + k1] = v;
   }
-  __syncthreads();
-  if (last && tid == 0) {
-    __threadfence();
-    double sum = 0.0;
-    const volatile double* pp = partial + (size_t)b * Kh1;
-    for (int i = 0; i < (int)gridDim.x; ++i) sum += pp[i];
-    selfrec[base + b] = sum;
-    done[b] = 0u;
-  }
+  // Launched behind the previous chunk's gather, which reads the potential grid that this
+  // chunk's k1 transform overwrites: this grid does not complete before that gather has.
+  grid_dep_wait();
+}
+
+// selfrec[base + b] = sum over the planes k1 <= k1max of target b's shares, in
+// plane order.  Run by the first CTA of the k1 transform: every plane of the
+// chunk is complete by then.
+__device__ __forceinline__ void self_energy_sum(const FrameArgs& a, int base, int nb, int Kh1,
+                                                const double* __restrict__ partial, double* __restrict__ selfrec) {
+  if (blockIdx.x != 0 || blockIdx.y != 0 || (int)threadIdx.x >= nb) return;
+  const int b = threadIdx.x;
+  double sum = 0.0;
+  for (int k1 = 0; k1 <= a.k1max; ++k1) sum += partial[(size_t)b * Kh1 + k1];
+  selfrec[base + b] = sum;
 }
 
 // ---------------------------------------------------------------------------
@@ -391,14 +394,17 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
 // Y[b][k1][n3][n2] at column (n2 - n2g) * 33 + b.
 // ---------------------------------------------------------------------------
 template <int LM>
-__global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb, const float2* __restrict__ Y,
-    const float2* __restrict__ fft_tw, float* __restrict__ phi) {
+__global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int base, int nb, const float2* __restrict__ Y,
+    const float2* __restrict__ fft_tw, const double* __restrict__ partial, double* __restrict__ selfrec,
+    float* __restrict__ phi) {
   constexpr int M = 1 << LM, K1 = 2 * M, Kh1 = M + 1;
   constexpr int G2 = 256 / M, LG2 = 8 - LM, T = 32 * G2, LT = LG2 + 5, TP = G2 * 33;
   extern __shared__ __align__(16) unsigned char rsm[];
   const int K2 = a.K2, K3 = a.K3;
   const int n3 = blockIdx.x, n2g = blockIdx.y * G2;
   const int tid = threadIdx.x;
+  grid_dep_wait();
+  self_energy_sum(a, base, nb, Kh1, partial, selfrec);
   float2* twk = (float2*)rsm;          // [K1] exp(-2 pi i m / K1)
   float2* twm = twk + K1;              // [M]  exp(-2 pi i m / M)
   float2* S = twm + M;                 // [Kh1][TP]
@@ -467,44 +473,50 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int nb
 // n2 = blockIdx.y * kLineRows + j, lane b the target.  The CTA first stages
 // the half spectra Y[b][k1][n3][n2], k1 <= k1max, of its kLineRows rows and
 // 32 targets in shared memory (16-byte loads along n2; S[k1][n2][b] with a
-// row pitch of 34, so the staging stores and the per-line reads are free of
-// bank conflicts).  Each thread then packs its line (hermitian_pack),
+// row pitch of kLinePitch, so the staging stores and the per-line reads are
+// free of bank conflicts).  Each thread then packs its line (hermitian_pack),
 // transforms it in registers (idft_reg) and writes phi[p][b] for the 2M
 // points of the line: every store of a warp is one 128-byte row of the
 // insertion-fastest layout.
 // ---------------------------------------------------------------------------
-constexpr int kLinePitch = 34;
+// pitch of the (n2, target) rows of S: 2 * 2q * pitch = 16 q (mod 32) words for the Q = kLineRows / 2
+// float4 of a staging load, so that a half-warp's 64-bit stores hit distinct banks
+constexpr int kLinePitch = kLineRows == 8 ? 34 : 36;
 
 size_t lines_smem(int M) { return sizeof(float2) * (size_t)(M + 1) * kLineRows * kLinePitch; }
 
 template <int LM>
-__global__ void __launch_bounds__(32 * kLineRows, 2) k_pme_lines(FrameArgs a, int nb, const float2* __restrict__ Y,
-                                                                 Tw64 tw, float* __restrict__ phi) {
+__global__ void __launch_bounds__(32 * kLineRows, 2) k_pme_lines(FrameArgs a, int base, int nb,
+    const float2* __restrict__ Y, Tw64 tw, const double* __restrict__ partial, double* __restrict__ selfrec,
+    float* __restrict__ phi) {
   constexpr int M = 1 << LM, K1 = 2 * M, Kh1 = M + 1, NT = 32 * kLineRows;
   constexpr int ROW = kLineRows * kLinePitch;             // float2 per k1 row of S
-  static_assert(kLineRows == 8, "a float4 carries two of the CTA's 8 rows; 4 float4 per (target, k1)");
+  constexpr int Q = kLineRows / 2;                        // float4 per (target, k1): two rows each
+  static_assert(kLineRows == 4 || kLineRows == 8, "4 or 8 rows per CTA");
   extern __shared__ __align__(16) float2 S[];              // [M + 1][kLineRows][kLinePitch]
   const int K2 = a.K2, K3 = a.K3;
   const int tid = threadIdx.x;
   const int n3 = blockIdx.x, n2g = blockIdx.y * kLineRows;
   const size_t plane = (size_t)K3 * K2;
   const int kmax = a.k1max;
+  grid_dep_wait();                                    // the planes of this chunk are complete
+  self_energy_sum(a, base, nb, Kh1, partial, selfrec);
   {
     // staging item (k1, bs, q): the float4 of rows 2q, 2q+1 of target bs at k1
-    const int q = tid & 3, bs = (tid >> 2) & 31;
+    const int q = tid & (Q - 1), bs = (tid / Q) & 31;
     const bool on = bs < nb;
     const float4* src = (const float4*)(Y + (size_t)bs * Kh1 * plane + (size_t)n3 * K2 + n2g + 2 * q);
     float2* dst = S + (2 * q) * kLinePitch + bs;
     // every load is issued before the first store, from a clamped (always valid) k1, so that
     // they are all in flight together; rows above k1max and targets past nb are not used
-    constexpr int PER = NT / 128;                           // k1 rows per pass of the CTA
+    constexpr int PER = NT / (32 * Q);                      // k1 rows per pass of the CTA
     constexpr int NPASS = (M + PER) / PER;                  // passes covering k1 = 0..M
     float4 v[NPASS];
 #pragma unroll
-    for (int u = 0; u < NPASS; ++u) v[u] = __ldg(src + (size_t)min(u * PER + tid / 128, kmax) * (plane / 2));
+    for (int u = 0; u < NPASS; ++u) v[u] = __ldg(src + (size_t)min(u * PER + tid / (32 * Q), kmax) * (plane / 2));
 #pragma unroll
     for (int u = 0; u < NPASS; ++u) {
-      const int k1 = u * PER + tid / 128;
+      const int k1 = u * PER + tid / (32 * Q);
       if (k1 <= kmax) {
         const float4 t = on ? v[u] : make_float4(0.f, 0.f, 0.f, 0.f);
         dst[k1 * ROW] = make_float2(t.x, t.y);
@@ -513,6 +525,7 @@ __global__ void __launch_bounds__(32 * kLineRows, 2) k_pme_lines(FrameArgs a, in
     }
   }
   __syncthreads();
+  grid_dep_launch();                                  // the gather may start filling the tail
   const int b = tid & 31, j = tid >> 5;
   const float2* line = S + j * kLinePitch + b;
   float2 Z[M];
@@ -569,16 +582,18 @@ cudaError_t plane_attr(const FrameArgs& a) {
 }
 
 template <int L2, int L3>
-void plane_launch(const FrameArgs& a, const DeviceState& d, int base, int tbase, int nb, bool direct, cudaStream_t s) {
+void plane_launch(const FrameArgs& a, const DeviceState& d, int tbase, int nb, bool direct, bool pdl, cudaStream_t s) {
   using C = PlaneCfg<L2, L3>;
   const dim3 grid(a.k1max + 1, nb);   // planes above k1max carry no influence-function weight
   const int ts = site_tile(a);
   if (direct)
-    k_pme_plane<L2, L3, true><<<grid, C::NTHR, plane_smem(a, true), s>>>(
-        a, base, tbase, ts, d.sitetab, d.sitestn, d.engfacT, d.fft_tw, d.spec, d.partial, d.done, d.selfrec);
+    launch_k(pdl, grid, C::NTHR, plane_smem(a, true), s, k_pme_plane<L2, L3, true>, a, tbase, ts,
+             (const float2*)d.sitetab, (const float*)d.sitestn, (const float*)d.engfacT, (const float2*)d.fft_tw,
+             d.spec, d.partial);
   else
-    k_pme_plane<L2, L3, false><<<grid, C::NTHR, plane_smem(a, false), s>>>(
-        a, base, tbase, ts, d.sitetab, d.sitestn, d.engfacT, d.fft_tw, d.spec, d.partial, d.done, d.selfrec);
+    launch_k(pdl, grid, C::NTHR, plane_smem(a, false), s, k_pme_plane<L2, L3, false>, a, tbase, ts,
+             (const float2*)d.sitetab, (const float*)d.sitestn, (const float*)d.engfacT, (const float2*)d.fft_tw,
+             d.spec, d.partial);
 }
 }  // namespace
 
@@ -636,10 +651,10 @@ void launch_site_tables(const FrameArgs& a, const DeviceState& d, int bb, int nb
                                                                      direct ? nullptr : d.sitestn);
 }
 
-void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int base, int tbase, int nb, bool direct,
+void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int tbase, int nb, bool direct, bool pdl,
                       cudaStream_t s) {
   const int l2 = lg(a.K2), l3 = lg(a.K3);
-#define ERM_LAUNCH(L2, L3) if (l2 == L2 && l3 == L3) plane_launch<L2, L3>(a, d, base, tbase, nb, direct, s);
+#define ERM_LAUNCH(L2, L3) if (l2 == L2 && l3 == L3) plane_launch<L2, L3>(a, d, tbase, nb, direct, pdl, s);
   ERM_PLANE_SIZES(ERM_LAUNCH)
 #undef ERM_LAUNCH
 }
@@ -655,20 +670,29 @@ Tw64 make_tw64() {
 }
 }  // namespace
 
-void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int nb, cudaStream_t s) {
+void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int base, int nb, bool pdl, cudaStream_t s) {
   static const Tw64 tw = make_tw64();
   const dim3 lgrid(a.K3, a.K2 / kLineRows);
   switch (lg(a.K1 / 2)) {
-    case 3: k_pme_lines<3><<<lgrid, 32 * kLineRows, lines_smem(1 << 3), s>>>(a, nb, d.spec, tw, d.phi); return;
-    case 4: k_pme_lines<4><<<lgrid, 32 * kLineRows, lines_smem(1 << 4), s>>>(a, nb, d.spec, tw, d.phi); return;
-    case 5: k_pme_lines<5><<<lgrid, 32 * kLineRows, lines_smem(1 << 5), s>>>(a, nb, d.spec, tw, d.phi); return;
+    case 3:
+      launch_k(pdl, lgrid, 32 * kLineRows, lines_smem(1 << 3), s, k_pme_lines<3>, a, base, nb, (const float2*)d.spec,
+               tw, (const double*)d.partial, d.selfrec, d.phi);
+      return;
+    case 4:
+      launch_k(pdl, lgrid, 32 * kLineRows, lines_smem(1 << 4), s, k_pme_lines<4>, a, base, nb, (const float2*)d.spec,
+               tw, (const double*)d.partial, d.selfrec, d.phi);
+      return;
+    case 5:
+      launch_k(pdl, lgrid, 32 * kLineRows, lines_smem(1 << 5), s, k_pme_lines<5>, a, base, nb, (const float2*)d.spec,
+               tw, (const double*)d.partial, d.selfrec, d.phi);
+      return;
     default: break;
   }
   const int M = a.K1 / 2, G2 = 256 / M;
   const dim3 grid(a.K3, a.K2 / G2);
   const size_t sm = rows_smem(a);
   switch (lg(M)) {
-    default: k_pme_rows<6><<<grid, kRowThreads, sm, s>>>(a, nb, d.spec, d.fft_tw, d.phi); break;
+    default: k_pme_rows<6><<<grid, kRowThreads, sm, s>>>(a, base, nb, d.spec, d.fft_tw, d.partial, d.selfrec, d.phi); break;
   }
 }
 
