@@ -367,15 +367,44 @@ void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int co
 }
 
 // ---------------------------------------------------------------------------
-// real space: one CTA per target, a warp per candidate molecule, lanes over
-// the site pairs, FP64 warp-shuffle reduction of the molecule sum
+// real space: one CTA per target, warps over the cells around it
 // ---------------------------------------------------------------------------
 constexpr int kRealMaxThreads = 512;
 
-// WIDE (large solutes): lanes over the solute sites, the molecule's atoms in
-// turn; otherwise lanes over the (site, atom) pairs.  Either way a molecule's
-// energy is one warp's fixed-order FP64 sum.  The solute sites and the LJ
-// tables sit in shared memory (dynamic: s float4 + s int + 2 ljmax^2 float).
+// Small solutes: the lanes of a warp test 32 candidate molecules at a time
+// against the cutoff sphere and queue those in range (ballot, per-warp queue
+// in shared memory); each full batch of 32 is then evaluated a molecule per
+// lane, all its (site, atom) pairs in turn.  WIDE (large solutes): a warp per
+// molecule, lanes over the solute sites, the molecule's atoms in turn, and a
+// warp-shuffle reduction.  Either way a molecule's energy is one fixed-order
+// FP64 sum.  The solute sites, the LJ tables and the queues sit in shared
+// memory (dynamic: s float4 + s int + 2 ljmax^2 float + 64 int per warp).
+// Molecule k's energy against the target's solute by one thread: pairs (is, js)
+// in order, summed in FP64.  Kept out of line, so that every call site runs
+// the same compiled body: with the body inlined at the full-batch and the
+// last-batch call sites, a few molecules came out differently (about 1e-7
+// relative) from run to run.
+__device__ __noinline__ void real_mol_serial(const FrameArgs& a, int k, int b, int chunk, int s, int ljmax,
+    const float4* ss, const int* slj, const float* lje, const float* ljs, const int* __restrict__ molbeg,
+    const float4* __restrict__ slvn, const int* __restrict__ atom_lj, float rskip2, double* __restrict__ E) {
+  const int b0 = molbeg[k], nj = molbeg[k + 1] - b0;
+  double acc = 0.0;
+  for (int is = 0; is < s; ++is) {
+    const float4 xi = ss[is];
+    const int li = slj[is];
+    for (int js = 0; js < nj; ++js) {
+      const float4 xj = slvn[b0 + js];
+      float ex = xi.x - xj.x, ey = xi.y - xj.y, ez = xi.z - xj.z;
+      min_image(a.g, ex, ey, ez);
+      const float dis2 = ex * ex + ey * ey + ez * ez;
+      if (dis2 > rskip2) continue;
+      const int lj = atom_lj[b0 + js];
+      acc += (double)pair_energy(a.pp, dis2, lje[lj * ljmax + li], ljs[lj * ljmax + li], xi.w * xj.w);
+    }
+  }
+  E[(size_t)k * chunk + b] = acc;
+}
+
 template <bool WIDE>
 __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base, int chunk,
     const float4* __restrict__ tgt_n, const float4* __restrict__ tgt_c, const int* __restrict__ tgt_mol,
@@ -411,40 +440,51 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
   // pairs beyond rcut (>= elecut and > upljcut) are zero; the slack keeps r == rcut with pair_energy
   const float rskip2 = a.rcut * a.rcut * 1.0001f;
 
-  auto do_mol = [&](int k) {
-    if (k == excl) return;
+  // candidate k (-1: none) can have a site pair within the cutoff
+  auto in_range = [&](int k) {
+    if (k < 0 || k == excl) return false;
     const float4 an = anchor[k];
     float dx = an.x - c.x, dy = an.y - c.y, dz = an.z - c.z;
     min_image(a.g, dx, dy, dz);
     const float lim = a.rcut + c.w + an.w + margin;
-    if (dx * dx + dy * dy + dz * dz > lim * lim) return;  // every site pair beyond the cutoff
+    return !(dx * dx + dy * dy + dz * dz > lim * lim);
+  };
+  auto mol_serial = [&](int k) {
+    real_mol_serial(a, k, b, chunk, s, ljmax, ss, slj, lje, ljs, molbeg, slvn, atom_lj, rskip2, E);
+  };
+  int* q = (int*)(ljs + ljmax * ljmax) + warp * 64;   // this warp's queue of molecules in range
+  int qn = 0;                                          // queued (warp-uniform)
+  // lanes offer candidates kl (-1: none); full batches of 32 are evaluated a molecule per lane
+  auto offer = [&](int kl) {
+    const bool in = in_range(kl);
+    const unsigned bal = __ballot_sync(0xffffffffu, in);
+    if (in) q[qn + __popc(bal & ((1u << lane) - 1u))] = kl;
+    qn += __popc(bal);
+    __syncwarp();
+    if (qn >= 32) {
+      mol_serial(q[lane]);
+      __syncwarp();
+      if (lane < qn - 32) q[lane] = q[32 + lane];
+      qn -= 32;
+      __syncwarp();
+    }
+  };
+
+  // WIDE: molecule k by the whole warp, lanes over the solute sites
+  auto do_mol = [&](int k) {
+    if (!in_range(k)) return;  // every site pair beyond the cutoff
     const int b0 = molbeg[k], nj = molbeg[k + 1] - b0;
     double acc = 0.0;
-    if (WIDE) {
-      for (int js = 0; js < nj; ++js) {
-        const float4 xj = slvn[b0 + js];
-        const int lj = atom_lj[b0 + js];
-        for (int is = lane; is < s; is += 32) {
-          const float4 xi = ss[is];
-          float ex = xi.x - xj.x, ey = xi.y - xj.y, ez = xi.z - xj.z;
-          min_image(a.g, ex, ey, ez);
-          const float dis2 = ex * ex + ey * ey + ez * ez;
-          if (dis2 > rskip2) continue;
-          const int li = slj[is];
-          acc += (double)pair_energy(a.pp, dis2, lje[lj * ljmax + li], ljs[lj * ljmax + li], xi.w * xj.w);
-        }
-      }
-    } else {
-      const int P = s * nj;
-      for (int t = lane; t < P; t += 32) {
-        const int is = t / nj, js = t - is * nj;
+    for (int js = 0; js < nj; ++js) {
+      const float4 xj = slvn[b0 + js];
+      const int lj = atom_lj[b0 + js];
+      for (int is = lane; is < s; is += 32) {
         const float4 xi = ss[is];
-        const float4 xj = slvn[b0 + js];
         float ex = xi.x - xj.x, ey = xi.y - xj.y, ez = xi.z - xj.z;
         min_image(a.g, ex, ey, ez);
         const float dis2 = ex * ex + ey * ey + ez * ez;
         if (dis2 > rskip2) continue;
-        const int li = slj[is], lj = atom_lj[b0 + js];
+        const int li = slj[is];
         acc += (double)pair_energy(a.pp, dis2, lje[lj * ljmax + li], ljs[lj * ljmax + li], xi.w * xj.w);
       }
     }
@@ -471,18 +511,26 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
       int cz = (lo[2] + iz) % a.nc[2]; if (cz < 0) cz += a.nc[2];
       const int cid = (cz * a.nc[1] + cy) * a.nc[0] + cx;
       const int m0 = cellstart[cid], m1 = cellstart[cid + 1];
-      for (int m = m0; m < m1; ++m) do_mol(molsorted[m]);
+      if (WIDE) {
+        for (int m = m0; m < m1; ++m) do_mol(molsorted[m]);
+      } else {
+        for (int m = m0; m < m1; m += 32) offer(m + lane < m1 ? molsorted[m + lane] : -1);
+      }
     }
-  } else {
+  } else if (WIDE) {
     for (int k = warp; k < a.slvmax; k += nw) do_mol(k);
+  } else {
+    for (int k0 = warp * 32; k0 < a.slvmax; k0 += nw * 32) offer(k0 + lane < a.slvmax ? k0 + lane : -1);
   }
+  if (!WIDE && lane < qn) mol_serial(q[lane]);   // the last, partial batch
 }
 
 // Solutes above this many sites run the WIDE real-space variant.
 constexpr int kRealWideSites = 24;
 
 size_t real_smem(const FrameArgs& a) {
-  return (sizeof(float4) + sizeof(int)) * (size_t)a.nsite + 2 * sizeof(float) * (size_t)a.ljtype_max * a.ljtype_max;
+  return (sizeof(float4) + sizeof(int)) * (size_t)a.nsite + 2 * sizeof(float) * (size_t)a.ljtype_max * a.ljtype_max +
+         sizeof(int) * 64 * (kRealMaxThreads / 32);
 }
 
 int setup_real_smem(const FrameArgs& a) {

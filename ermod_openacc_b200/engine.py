@@ -106,9 +106,9 @@ class Engine:
                                          C.c_void_p(ins_weight_ptr) if ins_weight_ptr else None)
         return self._check(rc)
 
-    def _accum_struct(self):
+    def _accum_struct(self, ecorr: bool = True):
         ed = np.zeros(self.ermax)
-        ec = np.zeros(self.ermax * self.ermax) if self.params["corrcal"] else None
+        ec = np.zeros(self.ermax * self.ermax) if self.params["corrcal"] and ecorr else None
         es = np.zeros(self.esmax) if self.params["selfcal"] else None
         sl = np.zeros(self.numslv, dtype=np.float32)
         mn = np.zeros(self.numslv + 1, dtype=np.float32)
@@ -123,9 +123,10 @@ class Engine:
                     minuv=mn, maxuv=mx, avslf=acc.avslf, engnorm=acc.engnorm, engsmpl=acc.engsmpl,
                     voffset=acc.voffset, voffset_initialized=acc.voffset_initialized)
 
-    def accum(self) -> dict:
-        """Raw accumulators of the current division (engstore's inputs)."""
-        acc, arrs = self._accum_struct()
+    def accum(self, ecorr: bool = True) -> dict:
+        """Raw accumulators of the current division (engstore's inputs); ecorr=False leaves
+        the ermax^2 correlation matrix on the device (its entry is None)."""
+        acc, arrs = self._accum_struct(ecorr)
         self._check(self.lib.ermod_fetch_accum(self.ctx, C.byref(acc)))
         return self._accum_dict(acc, arrs)
 
