@@ -373,38 +373,12 @@ constexpr int kRealMaxThreads = 512;
 
 // Small solutes: the lanes of a warp test 32 candidate molecules at a time
 // against the cutoff sphere and queue those in range (ballot, per-warp queue
-// in shared memory); each full batch of 32 is then evaluated a molecule per
+// in shared memory); each batch of up to 32 is then evaluated a molecule per
 // lane, all its (site, atom) pairs in turn.  WIDE (large solutes): a warp per
 // molecule, lanes over the solute sites, the molecule's atoms in turn, and a
 // warp-shuffle reduction.  Either way a molecule's energy is one fixed-order
 // FP64 sum.  The solute sites, the LJ tables and the queues sit in shared
 // memory (dynamic: s float4 + s int + 2 ljmax^2 float + 64 int per warp).
-// Molecule k's energy against the target's solute by one thread: pairs (is, js)
-// in order, summed in FP64.  Kept out of line, so that every call site runs
-// the same compiled body: with the body inlined at the full-batch and the
-// last-batch call sites, a few molecules came out differently (about 1e-7
-// relative) from run to run.
-__device__ __noinline__ void real_mol_serial(const FrameArgs& a, int k, int b, int chunk, int s, int ljmax,
-    const float4* ss, const int* slj, const float* lje, const float* ljs, const int* __restrict__ molbeg,
-    const float4* __restrict__ slvn, const int* __restrict__ atom_lj, float rskip2, double* __restrict__ E) {
-  const int b0 = molbeg[k], nj = molbeg[k + 1] - b0;
-  double acc = 0.0;
-  for (int is = 0; is < s; ++is) {
-    const float4 xi = ss[is];
-    const int li = slj[is];
-    for (int js = 0; js < nj; ++js) {
-      const float4 xj = slvn[b0 + js];
-      float ex = xi.x - xj.x, ey = xi.y - xj.y, ez = xi.z - xj.z;
-      min_image(a.g, ex, ey, ez);
-      const float dis2 = ex * ex + ey * ey + ez * ez;
-      if (dis2 > rskip2) continue;
-      const int lj = atom_lj[b0 + js];
-      acc += (double)pair_energy(a.pp, dis2, lje[lj * ljmax + li], ljs[lj * ljmax + li], xi.w * xj.w);
-    }
-  }
-  E[(size_t)k * chunk + b] = acc;
-}
-
 template <bool WIDE>
 __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base, int chunk,
     const float4* __restrict__ tgt_n, const float4* __restrict__ tgt_c, const int* __restrict__ tgt_mol,
@@ -449,27 +423,6 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
     const float lim = a.rcut + c.w + an.w + margin;
     return !(dx * dx + dy * dy + dz * dz > lim * lim);
   };
-  auto mol_serial = [&](int k) {
-    real_mol_serial(a, k, b, chunk, s, ljmax, ss, slj, lje, ljs, molbeg, slvn, atom_lj, rskip2, E);
-  };
-  int* q = (int*)(ljs + ljmax * ljmax) + warp * 64;   // this warp's queue of molecules in range
-  int qn = 0;                                          // queued (warp-uniform)
-  // lanes offer candidates kl (-1: none); full batches of 32 are evaluated a molecule per lane
-  auto offer = [&](int kl) {
-    const bool in = in_range(kl);
-    const unsigned bal = __ballot_sync(0xffffffffu, in);
-    if (in) q[qn + __popc(bal & ((1u << lane) - 1u))] = kl;
-    qn += __popc(bal);
-    __syncwarp();
-    if (qn >= 32) {
-      mol_serial(q[lane]);
-      __syncwarp();
-      if (lane < qn - 32) q[lane] = q[32 + lane];
-      qn -= 32;
-      __syncwarp();
-    }
-  };
-
   // WIDE: molecule k by the whole warp, lanes over the solute sites
   auto do_mol = [&](int k) {
     if (!in_range(k)) return;  // every site pair beyond the cutoff
@@ -492,10 +445,12 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
     if (lane == 0) E[(size_t)k * chunk + b] = acc;
   };
 
+  // the cells around the target (all cells when the range covers the box)
   (void)rmol;
+  int lo[3] = {0, 0, 0}, n[3] = {1, 1, 1};
+  int total;
   if (a.use_cells) {
     const float R = a.rcut + c.w + rmol + margin;
-    int lo[3], n[3];
     const float cc[3] = {c.x, c.y, c.z};
     for (int d3 = 0; d3 < 3; ++d3) {
       lo[d3] = (int)floorf((cc[d3] - R) / a.ch[d3]);
@@ -503,26 +458,91 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
       n[d3] = hi - lo[d3] + 1;
       if (n[d3] >= a.nc[d3]) { lo[d3] = 0; n[d3] = a.nc[d3]; }
     }
-    const int total = n[0] * n[1] * n[2];
+    total = n[0] * n[1] * n[2];
+  } else {
+    total = (a.slvmax + 7) / 8;   // without cells: runs of 8 molecules
+  }
+  auto cell_id = [&](int t) {
+    const int ix = t % n[0], iy = (t / n[0]) % n[1], iz = t / (n[0] * n[1]);
+    int cx = (lo[0] + ix) % a.nc[0]; if (cx < 0) cx += a.nc[0];
+    int cy = (lo[1] + iy) % a.nc[1]; if (cy < 0) cy += a.nc[1];
+    int cz = (lo[2] + iz) % a.nc[2]; if (cz < 0) cz += a.nc[2];
+    return (cz * a.nc[1] + cy) * a.nc[0] + cx;
+  };
+
+  if (WIDE) {
     for (int t = warp; t < total; t += nw) {
-      const int ix = t % n[0], iy = (t / n[0]) % n[1], iz = t / (n[0] * n[1]);
-      int cx = (lo[0] + ix) % a.nc[0]; if (cx < 0) cx += a.nc[0];
-      int cy = (lo[1] + iy) % a.nc[1]; if (cy < 0) cy += a.nc[1];
-      int cz = (lo[2] + iz) % a.nc[2]; if (cz < 0) cz += a.nc[2];
-      const int cid = (cz * a.nc[1] + cy) * a.nc[0] + cx;
-      const int m0 = cellstart[cid], m1 = cellstart[cid + 1];
-      if (WIDE) {
-        for (int m = m0; m < m1; ++m) do_mol(molsorted[m]);
+      if (a.use_cells) {
+        const int cid = cell_id(t);
+        for (int m = cellstart[cid]; m < cellstart[cid + 1]; ++m) do_mol(molsorted[m]);
       } else {
-        for (int m = m0; m < m1; m += 32) offer(m + lane < m1 ? molsorted[m + lane] : -1);
+        for (int k = 8 * t; k < min(8 * t + 8, a.slvmax); ++k) do_mol(k);
       }
     }
-  } else if (WIDE) {
-    for (int k = warp; k < a.slvmax; k += nw) do_mol(k);
-  } else {
-    for (int k0 = warp * 32; k0 < a.slvmax; k0 += nw * 32) offer(k0 + lane < a.slvmax ? k0 + lane : -1);
+    return;
   }
-  if (!WIDE && lane < qn) mol_serial(q[lane]);   // the last, partial batch
+
+  // Small solutes.  Each lane walks its own cells (t = warp * 32 + lane, then every
+  // nw * 32-th), so a ballot step tests up to 32 candidates; molecules in range go to
+  // the warp's queue, and every batch of up to 32 is evaluated a molecule per lane at the
+  // single call site below (one compiled body: a molecule's sum does not depend on which
+  // batch it lands in, and the order of molecules within a cell is not fixed).
+  int* q = (int*)(ljs + ljmax * ljmax) + warp * 64;   // this warp's queue of molecules in range
+  int qn = 0;                                          // queued (warp-uniform)
+  int tc = warp * 32 + lane, m = 0, m1 = 0;            // this lane's cell cursor and candidate range
+  auto next_cell = [&]() {
+    while (m >= m1 && tc < total) {
+      if (a.use_cells) {
+        const int cid = cell_id(tc);
+        m = cellstart[cid];
+        m1 = cellstart[cid + 1];
+      } else {
+        m = 8 * tc;
+        m1 = min(m + 8, a.slvmax);
+      }
+      tc += nw * 32;
+    }
+  };
+  next_cell();
+  for (;;) {
+    bool more = __any_sync(0xffffffffu, m < m1);
+    while (qn < 32 && more) {
+      int kl = -1;
+      if (m < m1) {
+        kl = a.use_cells ? molsorted[m] : m;
+        if (++m >= m1) next_cell();
+      }
+      const bool in = in_range(kl);
+      const unsigned bal = __ballot_sync(0xffffffffu, in);
+      if (in) q[qn + __popc(bal & ((1u << lane) - 1u))] = kl;
+      qn += __popc(bal);
+      more = __any_sync(0xffffffffu, m < m1);
+    }
+    __syncwarp();
+    if (qn == 0) break;
+    // lanes past the queue's end repeat entry 0 and store nothing
+    const int k = q[lane < qn ? lane : 0];
+    const int b0 = molbeg[k], nj = molbeg[k + 1] - b0;
+    double acc = 0.0;
+    for (int is = 0; is < s; ++is) {
+      const float4 xi = ss[is];
+      const int li = slj[is];
+      for (int js = 0; js < nj; ++js) {
+        const float4 xj = slvn[b0 + js];
+        float ex = xi.x - xj.x, ey = xi.y - xj.y, ez = xi.z - xj.z;
+        min_image(a.g, ex, ey, ez);
+        const float dis2 = ex * ex + ey * ey + ez * ez;
+        if (dis2 > rskip2) continue;
+        const int lj = atom_lj[b0 + js];
+        acc += (double)pair_energy(a.pp, dis2, lje[lj * ljmax + li], ljs[lj * ljmax + li], xi.w * xj.w);
+      }
+    }
+    if (lane < qn) E[(size_t)k * chunk + b] = acc;
+    __syncwarp();
+    if (lane < qn - 32) q[lane] = q[32 + lane];
+    qn = qn > 32 ? qn - 32 : 0;
+    __syncwarp();
+  }
 }
 
 // Solutes above this many sites run the WIDE real-space variant.
