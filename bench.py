@@ -317,7 +317,8 @@ def main():
     bytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
     achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
     kname = {"gather": "k_gather", "bin": "k_bin", "real": "k_real", "spread": "k_spread_box",
-             "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane", "pme_rows": "k_pme_rows",
+             "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane",
+             "pme_rows": "k_pme_lines" if w.params["ms1max"] <= 64 else "k_pme_rows",
              "site_tables": "k_site_tables", "influence": "k_influence", "ecorr": "k_ecorr_tc"}[dom]
     traffic = traffic_from_profiles(kname)
     stage_share = {k: round(stage[k] / max(stage["total"], 1e-9), 4) for k in Engine.STAGES
