@@ -107,7 +107,10 @@ def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int
     write at least once (inputs in, outputs out), independent of how the kernel stages them."""
     K = w.params["ms1max"]
     n = w.params["splodr"]
-    KK, KH = K ** 3, K * K * (K // 2 + 1)
+    # k1 planes the fused solve transforms: every mode above k1max has a Gaussian weight below 1e-9
+    a1 = float(np.linalg.norm(np.asarray(w.frame(0)[1], dtype=np.float64).reshape(3, 3)[0]))
+    k1max = min(K // 2, int(np.floor(np.sqrt(-np.log(1e-9)) * w.params["screen"] * a1 / np.pi)) + 1)
+    KK, KH = K ** 3, K * K * (k1max + 1)
     if stage == "gather":       # potential grid once + real-space energies in + totals out + splines
         return chunk * KK * 4 + slvmax * chunk * 8 * 2 + natoms * (12 * n + 16)
     if stage == "bin":          # every target's energy row in, its count row out (one launch per batch)
@@ -129,6 +132,18 @@ def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int
     if stage == "ecorr":        # counts read twice + ecorr read-modify-write
         return 2 * maxdst * ermax * 4 + 16 * ermax * ermax
     return 0.0
+
+
+def path_bytes_per_unit(w, natoms: int, slvmax: int, ermax: int, maxdst: int, nsite: int, batch: int = 4096) -> float:
+    """Algorithmic HBM bytes of the whole path per mol-pair, as the scope table defines them:
+    B = 16 N_atoms + 16 M s + 16 M K^3 + 16 M N_mol + 16 ermax^2 ceil(M / batch), divided by
+    the frame's M N_mol units (solvent read once, insertions, a spectrum and a potential grid
+    written and read per insertion, the FP64 energy matrix written and read, ecorr updated
+    once per batch)."""
+    K = w.params["ms1max"]
+    B = (16 * natoms + 16 * maxdst * nsite + 16 * maxdst * K ** 3 + 16 * maxdst * slvmax
+         + 16 * ermax * ermax * -(-maxdst // batch))
+    return B / (maxdst * slvmax)
 
 
 def traffic_from_profiles(kernel: str):
@@ -314,8 +329,14 @@ def main():
     if os.path.exists(peaks_path):
         peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     chunk = 32
-    bytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
+    # achieved: the scope table's per-unit bytes x the units one launch of the dominant kernel
+    # serves (a frame's units over its launches); the kernel's own input/output bytes beside it
+    b_unit = path_bytes_per_unit(w, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
+    units_launch = units * nst / n_launch
+    bytes_launch = b_unit * units_launch
     achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
+    kbytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
+    kachieved = kbytes_launch / (per_launch_ms * 1e-3) / 1e9
     kname = {"gather": "k_gather", "bin": "k_bin", "real": "k_real", "spread": "k_spread_box",
              "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane",
              "pme_rows": "k_pme_lines" if w.params["ms1max"] <= 64 else "k_pme_rows",
@@ -342,7 +363,10 @@ def main():
             "stage_share": stage_share,
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": bytes_launch, "launch_ms": per_launch_ms},
+                         "algorithmic_bytes_per_launch": bytes_launch, "bytes_per_unit": b_unit,
+                         "units_per_launch": units_launch, "launch_ms": per_launch_ms,
+                         "kernel_io_bytes_per_launch": kbytes_launch, "kernel_io_frac": kachieved / peak,
+                         "path_frac": value * b_unit / 1e9 / peak},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(4 * 3 * eng.natoms + 4 * eng.maxdst),
                     "d2h_bytes_per_step": d2h_bytes_per_step(eng)},
             "gpu_launches": int(launches)}
