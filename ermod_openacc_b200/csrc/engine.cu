@@ -398,7 +398,8 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   else ctx->spath = p.spectrum_path;
   if (pme) {
     CK(dalloc(&d.spec, (size_t)ctx->chunk * KH));
-    CK(dalloc(&d.phi, (size_t)ctx->chunk * KK)); CK(dalloc(&d.engfac, KH)); CK(dalloc(&d.splfc, K1 + K2 + K3));
+    CK(dalloc(&d.phi, (size_t)ctx->chunk * K3 * K2 * 2 * ((K1 + 1) / 2)));   // n1 pairs, see DeviceState::phi
+    CK(dalloc(&d.engfac, KH)); CK(dalloc(&d.splfc, K1 + K2 + K3));
     if (ctx->spath == 1) {
       CK(dalloc(&d.grid, (size_t)ctx->chunk * KK));
       CK(cudaMemsetAsync(d.grid, 0, sizeof(float) * ctx->chunk * KK, ctx->st));  // kept zero outside the boxes

@@ -62,6 +62,12 @@ cudaError_t launch_k(bool pdl, dim3 grid, dim3 block, size_t smem, cudaStream_t 
   return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
 }
 
+// Float offset of phi(n1) of grid line `line` (= n3 K2 + n2) and target b in the
+// pair layout: n1 pairs of kChunk targets, P1 = ceil(K1 / 2) pairs per line.
+__host__ __device__ __forceinline__ size_t phi_index(size_t line, int n1, int b, int P1) {
+  return ((line * P1 + (size_t)(n1 >> 1)) * kChunk + b) * 2 + (n1 & 1);
+}
+
 struct DeviceState {
   // topology (physical molecules in tagpt order)
   int* molbeg = nullptr;     // [slvmax+1]
@@ -109,7 +115,9 @@ struct DeviceState {
   float* grid = nullptr;     // [chunk*K^3]
   float2* spec = nullptr;    // [chunk*K3*K2*Kh1]
   float* phin = nullptr;     // [chunk*K^3] potential grids as the C2R writes them
-  float* phi = nullptr;      // [K^3*chunk], insertion fastest
+  float* phi = nullptr;      // potential grids, insertion fastest in n1 pairs: float2 (phi(2m), phi(2m+1)) of
+                             // line (n3 K2 + n2) and target b at float2 index (line P1 + m) chunk + b,
+                             // P1 = ceil(K1 / 2); see phi_index
   float* engfac = nullptr;   // [K3*K2*Kh1]
   float* engfacT = nullptr;  // [Kh1*K3*K2] influence function, k1-major (fused PME solve)
   float2* fft_tw = nullptr;  // [K1+K2+K3+K1/2] FP32 twiddle tables of the fused PME solve

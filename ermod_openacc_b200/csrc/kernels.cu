@@ -816,12 +816,13 @@ __global__ void k_influence(FrameArgs a, int base, int nb, float2* __restrict__ 
   }
 }
 
-// potential grids [chunk][K^3] (cuFFT's natural C2R output) -> [K^3][chunk]
-// (target fastest, the layout the gather reads one 128-byte row per point)
-__global__ void k_transpose_phi(int KK, const float* __restrict__ in, float* __restrict__ out) {
+// potential grids [chunk][K^3] (cuFFT's natural C2R output) -> the gather's
+// layout: target fastest, n1 in pairs (phi_index)
+__global__ void k_transpose_phi(int KK, int K1, const float* __restrict__ in, float* __restrict__ out) {
   __shared__ float tile[32][33];
   const int p0 = blockIdx.x * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // (32, 8)
+  const int P1 = (K1 + 1) / 2;
 #pragma unroll
   for (int j = 0; j < 32; j += 8) {
     const int b = ty + j, p = p0 + tx;
@@ -831,13 +832,13 @@ __global__ void k_transpose_phi(int KK, const float* __restrict__ in, float* __r
 #pragma unroll
   for (int j = 0; j < 32; j += 8) {
     const int p = p0 + ty + j;
-    if (p < KK) out[(size_t)p * 32 + tx] = tile[tx][ty + j];
+    if (p < KK) out[phi_index((size_t)(p / K1), p % K1, tx, P1)] = tile[tx][ty + j];
   }
 }
 
 void launch_transpose_phi(const FrameArgs& a, const DeviceState& d, cudaStream_t s) {
   const int KK = a.K1 * a.K2 * a.K3;
-  k_transpose_phi<<<(KK + 31) / 32, dim3(32, 8), 0, s>>>(KK, d.phin, d.phi);
+  k_transpose_phi<<<(KK + 31) / 32, dim3(32, 8), 0, s>>>(KK, a.K1, d.phin, d.phi);
 }
 
 void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s) {
@@ -851,6 +852,28 @@ void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb
 // every (target, molecule) pair into Etot[target][molecule] (the uvengy layout).
 // ---------------------------------------------------------------------------
 constexpr int kGatherThreads = 256;
+
+// The order-4 stencil rows of CS planes c3 (from c30) of one site, no wrap: v[(cs * 4 + c2) * 4 + c1]
+// = phi(gd.x - c1) of row (gd.z - c30 - cs, gd.y - c2).  p0 points at phi(gd.x) of the site's row;
+// in the pair layout phi(n - 1) is 1 float back when n is odd, 2 * kChunk - 1 back when n is even.
+template <int CS, bool ODD>
+__device__ __forceinline__ void gather_rows4(const float* __restrict__ p0, size_t s2, size_t s3, int c30,
+                                             float (&v)[CS * 16]) {
+#pragma unroll
+  for (int cs = 0; cs < CS; ++cs)
+#pragma unroll
+    for (int c2 = 0; c2 < 4; ++c2) {
+      const float* r = p0 - (size_t)(c30 + cs) * s3 - (size_t)c2 * s2;
+      float* o = v + (cs * 4 + c2) * 4;
+      if (ODD) {   // pairs (gd.x-1, gd.x) and (gd.x-3, gd.x-2)
+        const float2 a = *(const float2*)(r - 1), c = *(const float2*)(r - 1 - 2 * kChunk);
+        o[0] = a.y; o[1] = a.x; o[2] = c.y; o[3] = c.x;
+      } else {     // gd.x alone, pair (gd.x-2, gd.x-1), gd.x-3 alone
+        const float2 a = *(const float2*)(r - 2 * kChunk);
+        o[0] = r[0]; o[1] = a.y; o[2] = a.x; o[3] = r[-4 * kChunk + 1];
+      }
+    }
+}
 
 template <int NO>
 __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(FrameArgs a, int base, int bb, int nb,
@@ -867,7 +890,7 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
   const double qslt = active ? tgtq[cnt] : 0.0;
   const int excl = (active && tgt_mol) ? tgt_mol[cnt] : -1;
   const int n = NO > 0 ? NO : a.order;
-  const int K1 = a.K1, K2 = a.K2, K3 = a.K3;
+  const int K1 = a.K1, K2 = a.K2, K3 = a.K3, P1 = (K1 + 1) / 2;
   grid_dep_wait();                                    // the potential grid of this chunk is complete
   grid_dep_launch();                                  // the next chunk's planes may start filling the tail
   for (int m = gw; m < a.slvmax; m += nwt) {
@@ -883,22 +906,19 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
           // the stencil rows of CS planes c3 in flight at once (one 128-byte row per load):
           // the whole 4^3 stencil for order 4, one 6^2 plane for order 6
           constexpr int CS = NO <= 4 ? NO : 1;
-          if (gd.x >= NO - 1 && gd.y >= NO - 1 && gd.z >= NO - 1 && gd.x < K1 && gd.y < K2 && gd.z < K3) {
-            // no stencil index wraps (most sites): every point is a fixed offset from one
-            // pointer, the n1 neighbours compile-time ones (phi rows are kChunk floats)
-            const float* p0 = phi + ((size_t)(gd.z * K2 + gd.y) * K1 + gd.x) * kChunk + b;
-            const size_t s2 = (size_t)K1 * kChunk, s3 = (size_t)K2 * s2;
+          if constexpr (NO == 4) if (gd.x >= NO - 1 && gd.y >= NO - 1 && gd.z >= NO - 1 && gd.x < K1 &&
+                                     gd.y < K2 && gd.z < K3) {
+            // no stencil index wraps (most sites): every point is a fixed offset from phi(gd.x) of
+            // this target.  The four n1 values gd.x .. gd.x-3 are two whole pairs when gd.x is odd,
+            // else one pair and two single values: two or three loads a row instead of four.
+            const float* p0 = phi + phi_index((size_t)gd.z * K2 + gd.y, gd.x, b, P1);
+            const size_t s2 = (size_t)P1 * kChunk * 2, s3 = (size_t)K2 * s2;   // floats per n2 row, n3 plane
+            const bool odd = gd.x & 1;
 #pragma unroll
             for (int c30 = 0; c30 < NO; c30 += CS) {
               float v[CS * NO * NO];
-#pragma unroll
-              for (int cs = 0; cs < CS; ++cs)
-#pragma unroll
-                for (int c2 = 0; c2 < NO; ++c2) {
-                  const float* rowp = p0 - (size_t)(c30 + cs) * s3 - (size_t)c2 * s2;
-#pragma unroll
-                  for (int c1 = 0; c1 < NO; ++c1) v[(cs * NO + c2) * NO + c1] = rowp[-c1 * kChunk];
-                }
+              if (odd) gather_rows4<CS, true>(p0, s2, s3, c30, v);
+              else gather_rows4<CS, false>(p0, s2, s3, c30, v);
 #pragma unroll
               for (int cs = 0; cs < CS; ++cs) {
                 const float fac1 = q * w[2 * NO + c30 + cs];
@@ -916,7 +936,7 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
           }
           int r1[NO];
 #pragma unroll
-          for (int c1 = 0; c1 < NO; ++c1) r1[c1] = wrapk(gd.x - c1, K1) * chunk + b;
+          for (int c1 = 0; c1 < NO; ++c1) r1[c1] = (int)phi_index(0, wrapk(gd.x - c1, K1), b, P1);
 #pragma unroll
           for (int c30 = 0; c30 < NO; c30 += CS) {
             float v[CS * NO * NO];
@@ -925,7 +945,7 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
               const int r3 = wrapk(gd.z - (c30 + cs), K3);
 #pragma unroll
               for (int c2 = 0; c2 < NO; ++c2) {
-                const float* rowp = phi + (size_t)(r3 * K2 + wrapk(gd.y - c2, K2)) * K1 * chunk;
+                const float* rowp = phi + phi_index((size_t)r3 * K2 + wrapk(gd.y - c2, K2), 0, 0, P1);
 #pragma unroll
                 for (int c1 = 0; c1 < NO; ++c1) v[(cs * NO + c2) * NO + c1] = rowp[r1[c1]];
               }
@@ -948,18 +968,18 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
           int r1[kMaxOrder];
 #pragma unroll
           for (int c1 = 0; c1 < kMaxOrder; ++c1)
-            if (c1 < n) { w1[c1] = w[c1]; r1[c1] = wrapk(gd.x - c1, K1); }
+            if (c1 < n) { w1[c1] = w[c1]; r1[c1] = (int)phi_index(0, wrapk(gd.x - c1, K1), b, P1); }
           for (int c3 = 0; c3 < n; ++c3) {
             const int r3 = wrapk(gd.z - c3, K3);
             const float fac1 = q * w[2 * n + c3];
             for (int c2 = 0; c2 < n; ++c2) {
               const int r2 = wrapk(gd.y - c2, K2);
               const float fac2 = fac1 * w[n + c2];
-              const float* rowp = phi + ((size_t)(r3 * K2 + r2) * K1) * chunk + b;
+              const float* rowp = phi + phi_index((size_t)r3 * K2 + r2, 0, 0, P1);
               float part = 0.0f;
 #pragma unroll
               for (int c1 = 0; c1 < kMaxOrder; ++c1)
-                if (c1 < n) part += (fac2 * w1[c1]) * rowp[(size_t)r1[c1] * chunk];
+                if (c1 < n) part += (fac2 * w1[c1]) * rowp[r1[c1]];
               e += (double)part;
             }
           }

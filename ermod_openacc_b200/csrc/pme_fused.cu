@@ -21,8 +21,9 @@
 //   k_pme_lines     a thread per (n3, n2) line and target: the complex-to-real
 //                   transform along k1 (a half-length complex FFT of the
 //                   Hermitian-packed line) in registers, written straight
-//                   into the insertion-fastest potential layout
-//                   phi[(n3*K2 + n2)*K1 + n1][32] that the gather reads
+//                   into the insertion-fastest potential layout the gather
+//                   reads: n1 pairs (phi(2m), phi(2m+1)) per target, 32
+//                   targets, for each line n3*K2 + n2
 //                   (K1 <= 64; k_pme_rows does K1 = 128 in shared memory).
 //
 // The FFTs are radix-8/4 Stockham stages (Govindaraju et al., "High
@@ -455,15 +456,12 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int ba
   }
   __syncthreads();
   fft_batch<FftShape<LM, LT, 5, 33, 1, TP>, kRowThreads, true>(S, twm, tid);
-  // phi[p][b], p = (n3 K2 + n2) K1 + n1, two n1 per complex value
-  float* out = phi + ((size_t)n3 * K2 + n2g) * K1 * 32;
+  // phi in n1 pairs: z[n] = (phi(2n), phi(2n+1)) of line (n3 K2 + n2g + j), target b
+  float2* out = (float2*)phi + ((size_t)n3 * K2 + n2g) * M * kChunk;
   for (int x = tid; x < T * M; x += kRowThreads) {
     const int b = x & 31, r = x >> 5;
     const int n = r & (M - 1), j = r >> LM;
-    const float2 z = S[n * TP + j * 33 + b];
-    float* o = out + ((size_t)j * K1 + 2 * n) * 32 + b;
-    o[0] = z.x;
-    o[32] = z.y;
+    out[((size_t)j * M + n) * kChunk + b] = S[n * TP + j * 33 + b];
   }
 }
 
@@ -475,8 +473,8 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int ba
 // 32 targets in shared memory (16-byte loads along n2; S[k1][n2][b] with a
 // row pitch of kLinePitch, so the staging stores and the per-line reads are
 // free of bank conflicts).  Each thread then packs its line (hermitian_pack),
-// transforms it in registers (idft_reg) and writes phi[p][b] for the 2M
-// points of the line: every store of a warp is one 128-byte row of the
+// transforms it in registers (idft_reg) and writes the line's M pairs
+// (phi(2n), phi(2n+1)): every store of a warp is one 256-byte row of the
 // insertion-fastest layout.
 // ---------------------------------------------------------------------------
 // pitch of the (n2, target) rows of S: 2 * 2q * pitch = 16 q (mod 32) words for the Q = kLineRows / 2
@@ -534,12 +532,10 @@ __global__ void __launch_bounds__(32 * kLineRows, 2) k_pme_lines(FrameArgs a, in
   const float2 xM = M <= kmax ? line[M * ROW] : make_float2(0.f, 0.f);
   hermitian_pack<LM>(Z, xM, tw);
   idft_reg<LM>(Z, tw);
-  float* o = phi + (size_t)(n3 * K2 + n2g + j) * K1 * 32 + b;
+  // z[n] = (phi(2n), phi(2n+1)): one 8-byte store per pair, a 256-byte row per warp
+  float2* o = (float2*)phi + (size_t)(n3 * K2 + n2g + j) * M * kChunk + b;
 #pragma unroll
-  for (int n = 0; n < M; ++n) {
-    o[(2 * n) * 32] = Z[n].x;
-    o[(2 * n + 1) * 32] = Z[n].y;
-  }
+  for (int n = 0; n < M; ++n) o[n * kChunk] = Z[n];
 }
 
 // ---------------------------------------------------------------------------
