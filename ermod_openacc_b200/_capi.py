@@ -32,6 +32,7 @@ ES_NVT, ES_NPT = 1, 2
 EL_COULOMB, EL_EWALD, EL_PME, EL_PPPM = 0, 1, 2, 3
 LJSWT_POT_CHM, LJSWT_POT_GMX, LJSWT_FRC_CHM, LJSWT_FRC_GMX = 0, 1, 2, 3
 INSPOS_RANDOM, INSPOS_NOCHANGE = 0, 1
+INSPOS_SPHERE, INSPOS_SLAB_GENERIC, INSPOS_SLAB_SYMMETRIC = 2, 3, 4
 INSROT_RANDOM, INSROT_NOCHANGE = 0, 1
 PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
 
@@ -55,7 +56,7 @@ class ErmodParams(C.Structure):
         ("proposal", C.c_int32),
         ("keep_uvengy", C.c_int32), ("ecorr_path", C.c_int32), ("spectrum_path", C.c_int32),
         ("graph_mode", C.c_int32), ("stage_timing", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("lwreg", C.c_float), ("upreg", C.c_float), ("hostspec", C.c_int32),
     ]
 
 
@@ -167,7 +168,7 @@ def load_library(path: str | None = None):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.ermod_abi_version() != 1:
+    if lib.ermod_abi_version() != 2:
         raise RuntimeError("libermod_b200.so ABI mismatch")
     if path is None:
         _LIB = lib

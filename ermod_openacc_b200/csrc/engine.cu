@@ -64,6 +64,7 @@ struct ermod_ctx {
   std::vector<int> uvmax, uvsoft;
   DeviceState d;
   int chunk = kChunk, batch = 0, ncell_cap = 0;
+  int nhost = 0;                      // atoms of the host aggregate (insposition 2..4)
   cufftHandle r2c = 0, c2r = 0;
   bool plans = false;
   void* tc_work = nullptr;
@@ -130,7 +131,8 @@ void free_all(ermod_ctx* c) {
                   d.E, d.Etot, d.tgtq, d.twt, d.sbin, d.gacc,
                   d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.edens_part, d.ecorr, d.eself,
                   d.slnuv, d.minuv, d.maxuv, d.scal, d.status, d.frame_i, d.dens, d.feat, d.mlp_f, d.mlp_b,
-                  d.vact, d.vlogit, d.vcdf, d.vq, d.ins_voxel, d.ins_feat, c->tc_work};
+                  d.vact, d.vlogit, d.vcdf, d.vq, d.ins_voxel, d.ins_feat, d.host_atom, d.host_mass, d.aggcen,
+                  c->tc_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->plans) {
@@ -273,9 +275,12 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     return bad(ERMOD_ERR_ARG, "set_prs");
   if (p.slttype < 1 || p.slttype > 3) return bad(ERMOD_ERR_ARG, "set_slt");
   if (p.slttype != ERMOD_SLT_SOLN &&
-      !((p.insposition == ERMOD_INSPOS_RANDOM || p.insposition == ERMOD_INSPOS_NOCHANGE) &&
+      !((p.insposition >= ERMOD_INSPOS_RANDOM && p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC) &&
         (p.insorient == ERMOD_INSROT_RANDOM || p.insorient == ERMOD_INSROT_NOCHANGE)))
     return bad(ERMOD_ERR_UNSUPPORTED, "ins_geo");
+  const bool region = p.slttype != ERMOD_SLT_SOLN && p.insposition >= ERMOD_INSPOS_SPHERE;
+  if (region && !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f && p.hostspec != 0))
+    return bad(ERMOD_ERR_ARG, "ins_reg");
   // topology (setparam / enginit / engconst bookkeeping)
   ctx->nummol = t->nummol;
   ctx->numsite.assign(t->numsite, t->numsite + t->nummol);
@@ -341,6 +346,21 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     molq[k] = q;
   }
   ctx->natoms = molbeg[ctx->slvmax];
+  // atoms of the host aggregate (com_aggregate, insertion.F90:587-614): molecules of the hostspec species
+  std::vector<int> host_atom;
+  std::vector<float> host_mass;
+  if (region) {
+    for (int k = 0; k < ctx->slvmax; ++k) {
+      const int i = ctx->tagpt[k], sp = ctx->uvspec[i];
+      if (sp < 1 || sp > 31 || !((p.hostspec >> (sp - 1)) & 1)) continue;
+      for (int j = 0; j < ctx->numsite[i]; ++j) {
+        host_atom.push_back(molbeg[k] + j);
+        host_mass.push_back(ctx->mass[ctx->molbeg_all[i] + j]);
+      }
+    }
+    if (host_atom.empty()) return bad(ERMOD_ERR_ARG, "ins_reg");
+  }
+  ctx->nhost = (int)host_atom.size();
   const int slt = ctx->sltlist[0];
   std::vector<int> slt_lj(ctx->s);
   std::vector<float> slt_q(ctx->s), slt_m(ctx->s);
@@ -452,6 +472,11 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   CK(h2d(d.ljlensq, t->ljlensq_mat, (size_t)ctx->ljtype_max * ctx->ljtype_max, st));
   CK(h2d(d.slt_lj, slt_lj.data(), S, st)); CK(h2d(d.slt_q, slt_q.data(), S, st));
   CK(h2d(d.slt_mass, slt_m.data(), S, st));
+  if (ctx->nhost > 0) {
+    CK(dalloc(&d.host_atom, ctx->nhost)); CK(dalloc(&d.host_mass, ctx->nhost)); CK(dalloc(&d.aggcen, 3));
+    CK(h2d(d.host_atom, host_atom.data(), ctx->nhost, st));
+    CK(h2d(d.host_mass, host_mass.data(), ctx->nhost, st));
+  }
   std::vector<float> bf(3 * S, 0.0f);
   if (t->bfcoord) std::memcpy(bf.data(), t->bfcoord, sizeof(float) * 3 * S);
   CK(h2d(d.bfcoord, bf.data(), 3 * S, st));
@@ -646,7 +671,9 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
   } else {
     g.cuboid = 1;
   }
-  if (refs && p.insposition == ERMOD_INSPOS_RANDOM && !g.periodic) return set_error(ctx, ERMOD_ERR_INS_GEO, "ins_geo");
+  if (refs && (p.insposition == ERMOD_INSPOS_RANDOM || p.insposition == ERMOD_INSPOS_SLAB_GENERIC ||
+               p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) && !g.periodic)
+    return set_error(ctx, ERMOD_ERR_INS_GEO, "ins_geo");   // insertion.F90:154-156, 185-187
   // ---- pair / PME constants ----
   PairParams& P = a.pp;
   P.lw = p.lwljcut; P.up = p.upljcut; P.lw2 = p.lwljcut * p.lwljcut; P.up2 = p.upljcut * p.upljcut;
@@ -800,9 +827,13 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
     if (n < 0) return set_error(ctx, ERMOD_ERR_CUDA, "prp_run");
     nl += n;
   }
+  if (refs && ctx->nhost > 0) {
+    launch_aggcen(d, ctx->nhost, st);
+    nl += 1;
+  }
   if (refs)
-    launch_insert(a, d, d.frame_i, p.iseed, p.insposition, p.insorient, fp.use_conf, fp.prop_gv, fp.prop_learned,
-                  st);
+    launch_insert(a, d, d.frame_i, p.iseed, p.insposition, p.insorient, p.lwreg, p.upreg, fp.use_conf, fp.prop_gv,
+                  fp.prop_learned, st);
   else launch_targets_soln(a, d, nullptr, st);
   CK(cudaMemsetAsync(d.selfrec, 0, sizeof(double) * ctx->maxdst, st));
   CK(cudaMemsetAsync(d.etot, 0, sizeof(double) * ctx->maxdst, st));

@@ -156,6 +156,9 @@ struct DeviceState {
   float* vlogit = nullptr;   // [G^3]
   double* vcdf = nullptr;    // [G^3] CDF of the proposal over the voxels
   float* vq = nullptr;       // [G^3] proposal probability of each voxel
+  int* host_atom = nullptr;  // [nhost] atoms of the host aggregate (insposition 2..4)
+  float* host_mass = nullptr;// [nhost]
+  double* aggcen = nullptr;  // [3] mass-weighted centre of the host aggregate, this frame
   int* ins_voxel = nullptr;  // [maxdst] voxel of each insertion
   float* ins_feat = nullptr; // [maxdst][64] features of each insertion's voxel (training data, on request)
 };
@@ -163,8 +166,9 @@ struct DeviceState {
 // ---- launchers (kernels.cu) -------------------------------------------
 void launch_prepare_solvent(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
 void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStream_t s);
+void launch_aggcen(const DeviceState& d, int nhost, cudaStream_t s);
 void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, int insposition,
-                   int insorient, int use_conf, int gv, int learned, cudaStream_t s);
+                   int insorient, float lwreg, float upreg, int use_conf, int gv, int learned, cudaStream_t s);
 // proposal (proposal.cu) and its network (mlp.cu)
 MlpLayout mlp_layout();
 void mlp_forward(const __nv_bfloat16* pw, const float* pf, const float* x, int n, float* act, float* logits,

@@ -212,7 +212,46 @@ __device__ void finish_target(const FrameArgs& a, int cnt, float4* __restrict__ 
 // gv > 0: record each insertion's voxel of the G^3 proposal grid; learned: draw
 // the voxel from the proposal CDF and scale the insertion's weight by
 // p/q = (1/G^3) / q_v (the position inside the voxel stays uniform).
+// com_aggregate (insertion.F90:587-614): the mass-weighted centre of the host
+// aggregate's atoms as the frame gives them, one block, FP64 sums in a fixed
+// order (per thread, then warps, then the block).
+constexpr int kAggThreads = 1024;
+
+__global__ void __launch_bounds__(kAggThreads) k_aggcen(int nhost, const int* __restrict__ host_atom,
+                                                       const float* __restrict__ host_mass,
+                                                       const float* __restrict__ posraw, double* __restrict__ aggcen) {
+  __shared__ double red[4][32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};   // m x, m y, m z, m
+  for (int i = tid; i < nhost; i += kAggThreads) {
+    const int at = host_atom[i];
+    const double m = host_mass[i];
+    acc[0] += m * posraw[3 * at];
+    acc[1] += m * posraw[3 * at + 1];
+    acc[2] += m * posraw[3 * at + 2];
+    acc[3] += m;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double v = warp_sum(acc[c]);
+    if (lane == 0) red[c][warp] = v;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    double t[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) t[c] = warp_sum(lane < kAggThreads / 32 ? red[c][lane] : 0.0);
+    if (lane == 0)
+      for (int c = 0; c < 3; ++c) aggcen[c] = t[3] > 0.0 ? t[c] / t[3] : 0.0;
+  }
+}
+
+void launch_aggcen(const DeviceState& d, int nhost, cudaStream_t s) {
+  k_aggcen<<<1, kAggThreads, 0, s>>>(nhost, d.host_atom, d.host_mass, d.posraw, d.aggcen);
+}
+
 __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int iseed, int insposition, int insorient,
+                         float lwreg, float upreg, const double* __restrict__ aggcen,
                          int use_conf, int gv, int learned, const double* __restrict__ cdf,
                          const float* __restrict__ qv, int* __restrict__ ins_voxel, float* __restrict__ insw,
                          const float* __restrict__ conf_all, const float* __restrict__ bfcoord,
@@ -271,6 +310,50 @@ __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int ise
       out[i].z = (out[i].z - c[2]) + cm[2];
     }
   }
+  if (insposition >= ERMOD_INSPOS_SPHERE && insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC) {
+    // set_solute_origin with insorigin 2: COM to the host aggregate centre (insertion.F90:122-124)
+    float c[3];
+    com(c);
+    const float ag[3] = {(float)aggcen[0], (float)aggcen[1], (float)aggcen[2]};
+    for (int i = 0; i < s; ++i) {
+      out[i].x = (out[i].x - c[0]) + ag[0];
+      out[i].y = (out[i].y - c[1]) + ag[1];
+      out[i].z = (out[i].z - c[2]) + ag[2];
+    }
+    // set_shift_com (insertion.F90:164-200)
+    const uint4 r4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, 0u, 0u), key);
+    float sh[3];
+    if (insposition == ERMOD_INSPOS_SPHERE) {
+      // radius uniform in volume over lwreg..upreg, direction uniform by rejection in the unit ball
+      const float lw3 = lwreg * lwreg * lwreg, up3 = upreg * upreg * upreg;
+      const float t = powf(u01(r4.x) * (up3 - lw3) + lw3, 1.0f / 3.0f);
+      float r[3] = {1.f, 0.f, 0.f}, nrm = 1.f;
+      for (uint32_t att = 1; att <= 64; ++att) {
+        const uint4 b4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, att, 2u), key);
+        const float x = u01(b4.x) * 2.f - 1.f, y = u01(b4.y) * 2.f - 1.f, z = u01(b4.z) * 2.f - 1.f;
+        const float n2 = x * x + y * y + z * z;
+        if (0.f < n2 && n2 <= 1.f) {
+          r[0] = x; r[1] = y; r[2] = z;
+          nrm = sqrtf(n2);
+          break;
+        }
+      }
+      for (int k = 0; k < 3; ++k) sh[k] = t * r[k] / nrm;
+    } else {
+      // slab: random in the cell's first two directions, dz = lwreg..upreg (either sign when symmetric)
+      float t = u01(r4.z) * (upreg - lwreg) + lwreg;
+      if (insposition == ERMOD_INSPOS_SLAB_SYMMETRIC && u01(r4.w) > 0.5f) t = -t;
+      const float l3 = sqrtf(a.g.cell[0][2] * a.g.cell[0][2] + a.g.cell[1][2] * a.g.cell[1][2] +
+                             a.g.cell[2][2] * a.g.cell[2][2]);   // celllen(3), engproc.F90:1045
+      const float r[3] = {u01(r4.x), u01(r4.y), t / l3};
+      for (int k = 0; k < 3; ++k) sh[k] = a.g.cell[k][0] * r[0] + a.g.cell[k][1] * r[1] + a.g.cell[k][2] * r[2];
+    }
+    for (int i = 0; i < s; ++i) {   // shift_solute_com
+      out[i].x += sh[0];
+      out[i].y += sh[1];
+      out[i].z += sh[2];
+    }
+  }
   if (insorient == ERMOD_INSROT_RANDOM) {  // apply_orientation (insertion.F90:348-369)
     float c[3];
     com(c);
@@ -303,8 +386,9 @@ __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int ise
 }
 
 void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, int insposition,
-                   int insorient, int use_conf, int gv, int learned, cudaStream_t s) {
-  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum_dev, iseed, insposition, insorient, use_conf, gv, learned,
+                   int insorient, float lwreg, float upreg, int use_conf, int gv, int learned, cudaStream_t s) {
+  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum_dev, iseed, insposition, insorient, lwreg, upreg,
+                                                    d.aggcen, use_conf, gv, learned,
                                                     d.vcdf, d.vq, d.ins_voxel, d.insw_in, d.ins_conf,
                                                     d.bfcoord, d.slt_mass, d.slt_q, d.tgt_raw, d.tgt_n, d.tgt_c);
 }

@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define ERMOD_ABI_VERSION 1
+#define ERMOD_ABI_VERSION 2
 
 /* ---- status codes --------------------------------------------------- */
 #define ERMOD_OK               0
@@ -80,6 +80,10 @@ extern "C" {
 #define ERMOD_LJSWT_FRC_GMX   3
 #define ERMOD_INSPOS_RANDOM   0
 #define ERMOD_INSPOS_NOCHANGE 1
+#define ERMOD_INSPOS_SPHERE   2   /* COM at the host aggregate centre + a point of the shell lwreg..upreg */
+#define ERMOD_INSPOS_SLAB_GENERIC   3   /* + cell . (u1, u2, dz / |c3|), lwreg < dz < upreg */
+#define ERMOD_INSPOS_SLAB_SYMMETRIC 4   /* the same with dz of either sign */
+/* insposition 5 (RMSD) and 6 (Gaussian) need the RefInfo reference structure: ERMOD_ERR_UNSUPPORTED */
 #define ERMOD_INSROT_RANDOM   0
 #define ERMOD_INSROT_NOCHANGE 1
 
@@ -115,7 +119,11 @@ typedef struct ermod_params {
                                      only when the frame's constants change), 1: direct launches */
   int32_t stage_timing;           /* 1: CUDA events between stages for ermod_get_timings
                                      (implies direct launches); 0: total frame time only */
-  int32_t reserved[3];
+  /* insertion region, insposition 2..4 (&ene_param lwreg, upreg, hostspec; engmain.F90:55-58, 77-90, 126-127).
+     The solute COM is first moved to the mass-weighted centre of the host aggregate (insorigin 2,
+     com_aggregate insertion.F90:587-614), then shifted as insertion.F90:164-200 does. */
+  float   lwreg, upreg;
+  int32_t hostspec;               /* bit (sp - 1) set: solvent species sp (uvspec) belongs to the host */
 } ermod_params;
 
 /*

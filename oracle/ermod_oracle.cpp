@@ -325,8 +325,12 @@ template <class T> struct Oracle {
     } else if (p.cltype != ERMOD_EL_COULOMB) {
       return fail(ERMOD_ERR_UNSUPPORTED, "set_prs");
     }
-    if (p.slttype != ERMOD_SLT_SOLN && !(p.insposition == ERMOD_INSPOS_RANDOM || p.insposition == ERMOD_INSPOS_NOCHANGE))
+    if (p.slttype != ERMOD_SLT_SOLN && !(p.insposition >= ERMOD_INSPOS_RANDOM &&
+                                         p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC))
       return fail(ERMOD_ERR_UNSUPPORTED, "ins_geo");
+    if (p.slttype != ERMOD_SLT_SOLN && p.insposition >= ERMOD_INSPOS_SPHERE &&
+        !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f && p.hostspec != 0))
+      return fail(ERMOD_ERR_ARG, "ins_reg");
     return ERMOD_OK;
   }
 
@@ -692,8 +696,25 @@ template <class T> struct Oracle {
     return h;
   }
 
-  // instslt('proc') for insposition RANDOM/NOCHANGE, insorient RANDOM/NOCHANGE
-  // (insertion.F90:86-98, 100-162, 307-375; bestfit.F90:252-297; quaternion rotate
+  // com_aggregate (insertion.F90:587-614): mass-weighted centre of the atoms of the solvent
+  // molecules whose species is in hostspec, from the frame's coordinates, summed in FP64.
+  void aggregate_center(const float* sitepos) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = 0; i < nummol; ++i) {
+      if (sluvid[i] != ERMOD_PT_SOLVENT || uvspec[i] < 1 || uvspec[i] > 31) continue;
+      if (!((p.hostspec >> (uvspec[i] - 1)) & 1)) continue;
+      for (int a = molbeg[i]; a < molbeg[i + 1]; ++a) {
+        const double m = (double)(float)sitemass[a];
+        for (int k = 0; k < 3; ++k) acc[k] += m * (double)sitepos[3 * a + k];
+        acc[3] += m;
+      }
+    }
+    for (int k = 0; k < 3; ++k) aggcen[k] = acc[3] > 0.0 ? acc[k] / acc[3] : 0.0;
+  }
+  double aggcen[3] = {0.0, 0.0, 0.0};
+
+  // instslt('proc') for insposition RANDOM/NOCHANGE/SPHERE/SLAB, insorient RANDOM/NOCHANGE
+  // (insertion.F90:86-98, 100-200, 307-375; bestfit.F90:252-297; quaternion rotate
   // bestfit.F90:74-99).  Writes the nsite solute coordinates of insertion cnt.
   void insert_one(int stnum, int cnt, const T* conf, T* out) const {
     const int s = nsite_slt;
@@ -720,6 +741,39 @@ template <class T> struct Oracle {
       for (int k = 0; k < 3; ++k) com[k] = cell[k][0] * r[0] + cell[k][1] * r[1] + cell[k][2] * r[2];
       com_of(c);  // set_solute_com(com)
       for (int a = 0; a < s; ++a) for (int k = 0; k < 3; ++k) out[3 * a + k] = (out[3 * a + k] - c[k]) + com[k];
+    } else if (p.insposition >= ERMOD_INSPOS_SPHERE && p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC) {
+      // insorigin 2: COM to the aggregate centre (insertion.F90:122-124), then set_shift_com (:164-200)
+      T c[3];
+      com_of(c);
+      const T ag[3] = {(T)(float)aggcen[0], (T)(float)aggcen[1], (T)(float)aggcen[2]};
+      for (int a = 0; a < s; ++a) for (int k = 0; k < 3; ++k) out[3 * a + k] = (out[3 * a + k] - c[k]) + ag[k];
+      uint32_t ctr[4] = {(uint32_t)cnt, (uint32_t)stnum, 0u, 0u}, r4[4];
+      philox4x32_10(ctr, key, r4);
+      T sh[3];
+      if (p.insposition == ERMOD_INSPOS_SPHERE) {
+        const T lw3 = (T)p.lwreg * (T)p.lwreg * (T)p.lwreg, up3 = (T)p.upreg * (T)p.upreg * (T)p.upreg;
+        const T t = std::pow((T)u01(r4[0]) * (up3 - lw3) + lw3, T(1) / T(3));
+        T r[3] = {T(1), T(0), T(0)}, nrm = T(1);
+        for (uint32_t att = 1; att <= 64; ++att) {
+          uint32_t bc[4] = {(uint32_t)cnt, (uint32_t)stnum, att, 2u}, b4[4];
+          philox4x32_10(bc, key, b4);
+          const T x = (T)u01(b4[0]) * T(2) - T(1), y = (T)u01(b4[1]) * T(2) - T(1), z = (T)u01(b4[2]) * T(2) - T(1);
+          const T n2 = x * x + y * y + z * z;
+          if (T(0) < n2 && n2 <= T(1)) {
+            r[0] = x; r[1] = y; r[2] = z;
+            nrm = std::sqrt(n2);
+            break;
+          }
+        }
+        for (int k = 0; k < 3; ++k) sh[k] = t * r[k] / nrm;
+      } else {
+        T t = (T)u01(r4[2]) * ((T)p.upreg - (T)p.lwreg) + (T)p.lwreg;
+        if (p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC && u01(r4[3]) > 0.5f) t = -t;
+        const T l3 = std::sqrt(cell[0][2] * cell[0][2] + cell[1][2] * cell[1][2] + cell[2][2] * cell[2][2]);
+        const T r[3] = {(T)u01(r4[0]), (T)u01(r4[1]), t / l3};
+        for (int k = 0; k < 3; ++k) sh[k] = cell[k][0] * r[0] + cell[k][1] * r[1] + cell[k][2] * r[2];
+      }
+      for (int a = 0; a < s; ++a) for (int k = 0; k < 3; ++k) out[3 * a + k] += sh[k];
     }
     if (p.insorient == ERMOD_INSROT_RANDOM) {
       T c[3];
@@ -861,7 +915,10 @@ template <class T> struct Oracle {
     for (size_t i = 0; i < 3 * (size_t)numatm_phys; ++i) pos[i] = (T)sitepos[i];
     insw.assign(maxdst, 1.0);
     if (refs) {
-      if (p.insposition == ERMOD_INSPOS_RANDOM && p.boxshp == ERMOD_SYS_NONPERIODIC) return fail(ERMOD_ERR_INS_GEO, "ins_geo");
+      if ((p.insposition == ERMOD_INSPOS_RANDOM || p.insposition == ERMOD_INSPOS_SLAB_GENERIC ||
+           p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) && p.boxshp == ERMOD_SYS_NONPERIODIC)
+        return fail(ERMOD_ERR_INS_GEO, "ins_geo");
+      if (p.insposition >= ERMOD_INSPOS_SPHERE) aggregate_center(sitepos);
       std::vector<T> conf(3 * s);
 #pragma omp parallel for num_threads(nthreads) firstprivate(conf) schedule(static)
       for (int cnt = 0; cnt < maxdst; ++cnt) {

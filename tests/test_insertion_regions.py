@@ -1,0 +1,106 @@
+"""Insertion regions (insposition 2..4, insertion.F90:164-200) on the CPU oracle.
+
+The solute's centre of mass goes first to the mass-weighted centre of the host
+aggregate (insorigin 2, com_aggregate insertion.F90:587-614), then:
+  sphere (2):          + a point of the shell lwreg <= r <= upreg, uniform in volume
+  slab generic (3):    + cell . (u1, u2, dz / |c3|), lwreg <= dz <= upreg
+  slab symmetric (4):  the same with dz of either sign, each with probability 1/2
+These tests check those geometries and distributions on the oracle's own
+placements; tests/test_parity_gpu.py checks the GPU's placements against it.
+"""
+import numpy as np
+import pytest
+
+from ermod_openacc_b200 import _capi as A
+from ermod_openacc_b200 import systems as S
+
+NINS = 2000
+
+
+def aggregate_center(topo, pos, hostspec):
+    xyz = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    mb = np.concatenate([[0], np.cumsum(topo.numsite)])
+    num, den = np.zeros(3), 0.0
+    for i in range(len(topo.numsite)):
+        sp = int(topo.uvspec[i])
+        if topo.sluvid[i] != A.PT_SOLVENT or sp < 1 or not (hostspec >> (sp - 1)) & 1:
+            continue
+        m = topo.sitemass[mb[i]:mb[i + 1]].astype(np.float64)
+        num += (m[:, None] * xyz[mb[i]:mb[i + 1]]).sum(axis=0)
+        den += m.sum()
+    return num / den
+
+
+def placements(oracle_mod, insposition, lwreg, upreg, insorient=A.INSROT_RANDOM, maxins=NINS, periodic=True):
+    w = S.make_workload(2, small=True, maxins=maxins)
+    prm = dict(w.params, insposition=insposition, insorient=insorient, lwreg=lwreg, upreg=upreg, hostspec=1,
+               corrcal=0)
+    orc = oracle_mod.Oracle(prm, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    assert orc.engconst(1, pos, cell) >= 0
+    s = int(w.topo.numsite[-1])
+    ins = np.asarray(orc.insertions(), dtype=np.float64).reshape(maxins, s, 3)
+    m = w.topo.sitemass[-s:].astype(np.float64)
+    com = (ins * m[None, :, None]).sum(axis=1) / m.sum()
+    return com, aggregate_center(w.topo, pos, 1), np.asarray(cell, dtype=np.float64).reshape(3, 3)
+
+
+def test_sphere_shell_uniform_in_volume(oracle_mod):
+    lw, up = 3.0, 8.0
+    com, ag, _ = placements(oracle_mod, A.INSPOS_SPHERE, lw, up)
+    r = np.linalg.norm(com - ag, axis=1)
+    assert r.min() >= lw - 1e-3 and r.max() <= up + 1e-3
+    # uniform in volume: F(r) = (r^3 - lw^3) / (up^3 - lw^3); Kolmogorov-Smirnov distance
+    rs = np.sort(r)
+    F = (rs ** 3 - lw ** 3) / (up ** 3 - lw ** 3)
+    ecdf = np.arange(1, len(rs) + 1) / len(rs)
+    assert np.max(np.abs(ecdf - F)) < 1.63 / np.sqrt(len(rs))   # 1% level
+    # isotropic directions: the mean unit vector is near zero
+    u = (com - ag) / r[:, None]
+    assert np.linalg.norm(u.mean(axis=0)) < 4.0 / np.sqrt(len(rs))
+
+
+@pytest.mark.parametrize("insposition", [A.INSPOS_SLAB_GENERIC, A.INSPOS_SLAB_SYMMETRIC])
+def test_slab_offsets(oracle_mod, insposition):
+    lw, up = 2.0, 6.0
+    com, ag, cell = placements(oracle_mod, insposition, lw, up)
+    dz = com[:, 2] - ag[2]                     # cuboid cell: the third cell vector is along z
+    a = np.abs(dz)
+    assert a.min() >= lw - 1e-3 and a.max() <= up + 1e-3
+    if insposition == A.INSPOS_SLAB_GENERIC:
+        assert np.all(dz > 0)
+    else:
+        frac_neg = (dz < 0).mean()
+        assert abs(frac_neg - 0.5) < 4 * 0.5 / np.sqrt(len(dz))
+    # x and y cover the cell uniformly from the aggregate centre
+    for k in (0, 1):
+        f = (com[:, k] - ag[k]) / cell[k, k]
+        assert f.min() >= -1e-6 and f.max() <= 1 + 1e-6
+        assert abs(f.mean() - 0.5) < 4 * np.sqrt(1 / 12) / np.sqrt(len(f))
+
+
+def test_region_without_rotation_keeps_the_body_frame(oracle_mod):
+    """insorient 1: only the COM moves; the solute keeps its body-fixed orientation."""
+    w = S.make_workload(2, small=True, maxins=16)
+    prm = dict(w.params, insposition=A.INSPOS_SPHERE, insorient=A.INSROT_NOCHANGE, lwreg=0.0, upreg=5.0,
+               hostspec=1, corrcal=0)
+    orc = oracle_mod.Oracle(prm, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    assert orc.engconst(1, pos, cell) >= 0
+    s = int(w.topo.numsite[-1])
+    ins = np.asarray(orc.insertions(), dtype=np.float64).reshape(16, s, 3)
+    bf = np.asarray(w.topo.bfcoord, dtype=np.float64).reshape(s, 3)
+    m = w.topo.sitemass[-s:].astype(np.float64)
+    bf_c = bf - (bf * m[:, None]).sum(axis=0) / m.sum()
+    for c in range(16):
+        rel = ins[c] - (ins[c] * m[:, None]).sum(axis=0) / m.sum()
+        np.testing.assert_allclose(rel, bf_c, atol=1e-6)
+
+
+def test_region_parameters_are_checked(oracle_mod):
+    w = S.make_workload(2, small=True, maxins=8)
+    for bad in (dict(hostspec=0, lwreg=1.0, upreg=2.0), dict(hostspec=1, lwreg=3.0, upreg=2.0),
+                dict(hostspec=1, lwreg=0.0, upreg=0.0)):
+        prm = dict(w.params, insposition=A.INSPOS_SPHERE, **bad)
+        with pytest.raises(Exception):
+            oracle_mod.Oracle(prm, w.topo, w.hist)

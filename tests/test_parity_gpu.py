@@ -81,6 +81,53 @@ def test_refs_ring_placement(lib, oracle_mod):
     assert np.all(wts == 1.0)
 
 
+@pytest.mark.parametrize("insposition", [A.INSPOS_SPHERE, A.INSPOS_SLAB_GENERIC, A.INSPOS_SLAB_SYMMETRIC])
+def test_refs_region_placement(lib, oracle_mod, insposition):
+    """Insertion regions (insertion.F90:164-200) around the water aggregate's centre: the GPU's
+    placements, from its FP64 aggregate centre and the same random streams, match the oracle's."""
+    w = S.make_workload(2, small=True, maxins=64)
+    prm = dict(w.params, insposition=insposition, lwreg=2.0, upreg=6.0, hostspec=1)
+    eng = Engine(prm, w.topo, w.hist)
+    orc = oracle_mod.Oracle(prm, w.topo, w.hist)
+    for fr in range(2):
+        pos, cell = w.frame(fr)
+        assert eng.engconst(fr + 1, pos, cell) >= 0
+        assert orc.engconst(fr + 1, pos, cell) >= 0
+        ins, _ = eng.insertions()
+        np.testing.assert_allclose(ins, orc.insertions(), atol=5e-5)
+
+
+def test_refs_region_energies_and_bins(lib, oracle_mod):
+    """Sphere insertion: energies and bins against the FP64 oracle on the GPU's placements."""
+    w = S.make_workload(2, small=True, maxins=96)
+    prm = dict(w.params, keep_uvengy=1, insposition=A.INSPOS_SPHERE, lwreg=0.0, upreg=6.0, hostspec=1)
+    eng = Engine(prm, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, u0 = eng.uvengy()
+    ins, _ = eng.insertions()
+    orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist)
+    assert orc.engconst(1, pos, cell, ins_conf=ins) >= 0
+    uo, u0o = orc.uvengy()
+    check_energies(u, uo)
+    np.testing.assert_allclose(u0, u0o, rtol=1e-6, atol=2e-5)
+    spec = phys_uvspec(w.topo)
+    bg = bins_of(u, eng.uvcrd, eng.uvmax, spec)
+    bo = bins_of(uo, eng.uvcrd, eng.uvmax, spec)
+    assert np.all((bg == bo) | near_edge(uo, eng.uvcrd, energy_tol(uo)))
+
+
+def test_slab_insertion_needs_a_periodic_cell(lib):
+    w = S.make_workload(2, small=True, maxins=8)
+    prm = dict(w.params, insposition=A.INSPOS_SLAB_SYMMETRIC, lwreg=1.0, upreg=3.0, hostspec=1,
+               boxshp=A.SYS_NONPERIODIC, cltype=A.EL_COULOMB, estype=A.ES_NVT)
+    eng = Engine(prm, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    with pytest.raises(ErmodError) as ei:
+        eng.engconst(1, pos, cell)
+    assert ei.value.code == A.ERMOD_ERR_INS_GEO
+
+
 @pytest.mark.parametrize("config,path", [(2, 1), (2, 2), (2, 3), (3, 1), (3, 2), (3, 3)])
 def test_refs_energies_and_bins(lib, oracle_mod, config, path):
     """PME solve 1: fixed-point spreading + cuFFT; fused solve with the solute spectrum
