@@ -132,7 +132,7 @@ void free_all(ermod_ctx* c) {
                   d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.edens_part, d.ecorr, d.eself,
                   d.slnuv, d.minuv, d.maxuv, d.scal, d.status, d.frame_i, d.dens, d.feat, d.mlp_f, d.mlp_b,
                   d.vact, d.vlogit, d.vcdf, d.vq, d.ins_voxel, d.ins_feat, d.host_atom, d.host_mass, d.aggcen,
-                  c->tc_work};
+                  d.atom_mass, d.skip, c->tc_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->plans) {
@@ -278,7 +278,11 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
       !((p.insposition >= ERMOD_INSPOS_RANDOM && p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC) &&
         (p.insorient == ERMOD_INSROT_RANDOM || p.insorient == ERMOD_INSROT_NOCHANGE)))
     return bad(ERMOD_ERR_UNSUPPORTED, "ins_geo");
-  const bool region = p.slttype != ERMOD_SLT_SOLN && p.insposition >= ERMOD_INSPOS_SPHERE;
+  // sphere / slab regions: refs insertion (set_shift_com) and soln configuration checks
+  // (check_mol_configuration); RMSD / Gaussian (5, 6) need the RefInfo structure, not built
+  if (p.slttype == ERMOD_SLT_SOLN && (p.insposition < ERMOD_INSPOS_RANDOM || p.insposition > ERMOD_INSPOS_SLAB_SYMMETRIC))
+    return bad(ERMOD_ERR_UNSUPPORTED, "ins_geo");
+  const bool region = p.insposition >= ERMOD_INSPOS_SPHERE;
   if (region && !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f && p.hostspec != 0))
     return bad(ERMOD_ERR_ARG, "ins_reg");
   // topology (setparam / enginit / engconst bookkeeping)
@@ -476,6 +480,16 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     CK(dalloc(&d.host_atom, ctx->nhost)); CK(dalloc(&d.host_mass, ctx->nhost)); CK(dalloc(&d.aggcen, 3));
     CK(h2d(d.host_atom, host_atom.data(), ctx->nhost, st));
     CK(h2d(d.host_mass, host_mass.data(), ctx->nhost, st));
+    if (!refs) {   // solute centres of mass for check_mol_configuration, and its verdicts
+      std::vector<float> am;
+      am.reserve(NA);
+      for (int k = 0; k < ctx->slvmax; ++k) {
+        const int i = ctx->tagpt[k];
+        for (int j = 0; j < ctx->numsite[i]; ++j) am.push_back(ctx->mass[ctx->molbeg_all[i] + j]);
+      }
+      CK(dalloc(&d.atom_mass, NA)); CK(dalloc(&d.skip, MD));
+      CK(h2d(d.atom_mass, am.data(), NA, st));
+    }
   }
   std::vector<float> bf(3 * S, 0.0f);
   if (t->bfcoord) std::memcpy(bf.data(), t->bfcoord, sizeof(float) * 3 * S);
@@ -674,6 +688,9 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
   if (refs && (p.insposition == ERMOD_INSPOS_RANDOM || p.insposition == ERMOD_INSPOS_SLAB_GENERIC ||
                p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) && !g.periodic)
     return set_error(ctx, ERMOD_ERR_INS_GEO, "ins_geo");   // insertion.F90:154-156, 185-187
+  if (!refs && (p.insposition == ERMOD_INSPOS_SLAB_GENERIC || p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) &&
+      !g.periodic)
+    return set_error(ctx, ERMOD_ERR_INS_GEO, "eng_slb");   // engproc.F90:1238
   // ---- pair / PME constants ----
   PairParams& P = a.pp;
   P.lw = p.lwljcut; P.up = p.upljcut; P.lw2 = p.lwljcut * p.lwljcut; P.up2 = p.upljcut * p.upljcut;
@@ -835,6 +852,11 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
     launch_insert(a, d, d.frame_i, p.iseed, p.insposition, p.insorient, p.lwreg, p.upreg, fp.use_conf, fp.prop_gv,
                   fp.prop_learned, st);
   else launch_targets_soln(a, d, nullptr, st);
+  if (!refs && ctx->nhost > 0) {   // check_mol_configuration of every solute
+    launch_aggcen(d, ctx->nhost, st);
+    launch_soln_region(a, d, p.insposition, p.lwreg, p.upreg, st);
+    nl += 2;
+  }
   CK(cudaMemsetAsync(d.selfrec, 0, sizeof(double) * ctx->maxdst, st));
   CK(cudaMemsetAsync(d.etot, 0, sizeof(double) * ctx->maxdst, st));
   CK(cudaMemsetAsync(d.flceng, 0, sizeof(double) * ctx->maxdst * ctx->numslv, st));

@@ -159,6 +159,8 @@ struct DeviceState {
   int* host_atom = nullptr;  // [nhost] atoms of the host aggregate (insposition 2..4)
   float* host_mass = nullptr;// [nhost]
   double* aggcen = nullptr;  // [3] mass-weighted centre of the host aggregate, this frame
+  float* atom_mass = nullptr;// [natoms] (soln region checks: solute centres of mass)
+  int* skip = nullptr;       // [maxdst] soln: 1 where check_mol_configuration rejects the solute this frame
   int* ins_voxel = nullptr;  // [maxdst] voxel of each insertion
   float* ins_feat = nullptr; // [maxdst][64] features of each insertion's voxel (training data, on request)
 };
@@ -167,6 +169,8 @@ struct DeviceState {
 void launch_prepare_solvent(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
 void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStream_t s);
 void launch_aggcen(const DeviceState& d, int nhost, cudaStream_t s);
+void launch_soln_region(const FrameArgs& a, const DeviceState& d, int insposition, float lwreg, float upreg,
+                        cudaStream_t s);
 void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, int insposition,
                    int insorient, float lwreg, float upreg, int use_conf, int gv, int learned, cudaStream_t s);
 // proposal (proposal.cu) and its network (mlp.cu)

@@ -250,6 +250,45 @@ void launch_aggcen(const DeviceState& d, int nhost, cudaStream_t s) {
   k_aggcen<<<1, kAggThreads, 0, s>>>(nhost, d.host_atom, d.host_mass, d.posraw, d.aggcen);
 }
 
+// check_mol_configuration (engproc.F90:1197-1324) for solutes in solution, sphere
+// and slab regions: the solute's centre of mass relative to the host aggregate's
+// centre (relative_com :1300-1323) must lie in lwreg..upreg, as a distance
+// (sphere) or along the third cell vector (slabs, invcl row 3 . dx * |c3|, its
+// absolute value for the symmetric slab).  skip[cnt] = 1 rejects solute cnt for
+// this frame: engconst skips its update_histogram (engproc.F90:447-450).
+__global__ void k_soln_region(FrameArgs a, int insposition, float lwreg, float upreg, const int* __restrict__ tgt_mol,
+                              const int* __restrict__ molbeg, const float* __restrict__ posraw,
+                              const float* __restrict__ atom_mass, const double* __restrict__ aggcen,
+                              int* __restrict__ skip) {
+  const int cnt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cnt >= a.maxdst) return;
+  const int k = tgt_mol[cnt];
+  double c[3] = {0.0, 0.0, 0.0}, msum = 0.0;
+  for (int at = molbeg[k]; at < molbeg[k + 1]; ++at) {
+    const double m = atom_mass[at];
+    for (int q = 0; q < 3; ++q) c[q] += m * posraw[3 * at + q];
+    msum += m;
+  }
+  float dx[3];
+  for (int q = 0; q < 3; ++q) dx[q] = (float)(c[q] / msum) - (float)aggcen[q];
+  float dist;
+  if (insposition == ERMOD_INSPOS_SPHERE) {
+    dist = sqrtf(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+  } else {
+    const float l3 = sqrtf(a.g.cell[0][2] * a.g.cell[0][2] + a.g.cell[1][2] * a.g.cell[1][2] +
+                           a.g.cell[2][2] * a.g.cell[2][2]);
+    dist = (a.g.invcl[2][0] * dx[0] + a.g.invcl[2][1] * dx[1] + a.g.invcl[2][2] * dx[2]) * l3;
+    if (insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) dist = fabsf(dist);
+  }
+  skip[cnt] = (lwreg > dist || dist > upreg) ? 1 : 0;
+}
+
+void launch_soln_region(const FrameArgs& a, const DeviceState& d, int insposition, float lwreg, float upreg,
+                        cudaStream_t s) {
+  k_soln_region<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, insposition, lwreg, upreg, d.tgt_mol, d.molbeg, d.posraw,
+                                                       d.atom_mass, d.aggcen, d.skip);
+}
+
 __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int iseed, int insposition, int insorient,
                          float lwreg, float upreg, const double* __restrict__ aggcen,
                          int use_conf, int gv, int learned, const double* __restrict__ cdf,
@@ -1098,11 +1137,11 @@ void launch_gather(const FrameArgs& a, const DeviceState& d, int base, int bb, i
 constexpr int kBinThreads = 256;
 constexpr int kMaxSpecSmem = 128;
 
-__global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slvmax, const double* __restrict__ Etot,
+__global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slvmax, double* __restrict__ Etot,
     const int* __restrict__ molspec, const int* __restrict__ spec_off, const double* __restrict__ uvcrd,
-    const int* __restrict__ uvsoft, const int* __restrict__ tgt_mol, uint32_t* __restrict__ counts,
-    double* __restrict__ etot, double* __restrict__ flceng, float* __restrict__ minuv, float* __restrict__ maxuv,
-    DevStatus* st) {
+    const int* __restrict__ uvsoft, const int* __restrict__ tgt_mol, const int* __restrict__ skip,
+    uint32_t* __restrict__ counts, double* __restrict__ etot, double* __restrict__ flceng, float* __restrict__ minuv,
+    float* __restrict__ maxuv, DevStatus* st) {
   extern __shared__ unsigned char smem_raw[];
   double* mesh = (double*)smem_raw;                                  // [ermax]
   uint32_t* hist = (uint32_t*)(mesh + ba.ermax);                     // [ermax_pad]
@@ -1110,6 +1149,14 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slv
   __shared__ double sfl[kMaxSpecSmem];
   __shared__ double red[32];
   const int bi = blockIdx.x, cnt = bb + bi;
+  if (skip && skip[cnt]) {
+    // a solute rejected by check_mol_configuration: no energies, no counts (engproc.F90:447-450, 755)
+    for (int i = threadIdx.x; i < ba.ermax_pad; i += blockDim.x) counts[(size_t)bi * ba.ermax_pad + i] = 0u;
+    for (int k = threadIdx.x; k < slvmax; k += blockDim.x) Etot[(size_t)bi * slvmax + k] = 0.0;
+    for (int q = threadIdx.x; q < ba.numslv; q += blockDim.x) flceng[(size_t)cnt * ba.numslv + q] = 0.0;
+    if (threadIdx.x == 0) etot[cnt] = 0.0;
+    return;
+  }
   for (int i = threadIdx.x; i < ba.ermax; i += blockDim.x) mesh[i] = uvcrd[i];
   for (int i = threadIdx.x; i < ba.ermax_pad; i += blockDim.x) hist[i] = 0u;
   for (int i = threadIdx.x; i < kMaxSpecSmem; i += blockDim.x) { smin[i] = FLT_MAX; smax[i] = -FLT_MAX; sfl[i] = 0.0; }
@@ -1170,8 +1217,8 @@ size_t bin_smem_bytes(const BinArgs& ba) { return sizeof(double) * ba.ermax + si
 void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int slvmax, cudaStream_t s) {
   if (nbatch <= 0) return;
   k_bin<<<nbatch, kBinThreads, bin_smem_bytes(ba), s>>>(ba, bb, slvmax, d.Etot, d.molspec, d.spec_off, d.uvcrd,
-                                                        d.uvsoft, d.tgt_mol, d.counts, d.etot, d.flceng, d.minuv,
-                                                        d.maxuv, d.status);
+                                                        d.uvsoft, d.tgt_mol, d.skip, d.counts, d.etot, d.flceng,
+                                                        d.minuv, d.maxuv, d.status);
 }
 
 int setup_bin_smem(const BinArgs& ba) {
@@ -1183,20 +1230,25 @@ int setup_bin_smem(const BinArgs& ba) {
 // ---------------------------------------------------------------------------
 // weights and accumulators
 // ---------------------------------------------------------------------------
-__global__ void k_offset_init(WeightArgs wa, int base, const double* __restrict__ selfrec,
-                              const double* __restrict__ selfreal, double* __restrict__ scal) {
+__global__ void k_offset_init(WeightArgs wa, int base, int n, const int* __restrict__ skip,
+                              const double* __restrict__ selfrec, const double* __restrict__ selfreal,
+                              double* __restrict__ scal) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  if (wa.rigid && scal[6] == 0.0) { scal[5] = selfreal[base]; scal[6] = 1.0; }
+  int c = base;   // the first target not rejected (engproc.F90:447-450)
+  if (skip) while (c < base + n && skip[c]) ++c;
+  if (c >= base + n) return;
+  if (wa.rigid && scal[6] == 0.0) { scal[5] = selfreal[c]; scal[6] = 1.0; }
   if (wa.wgtslf && scal[4] == 0.0) {
-    const double sr = wa.rigid ? scal[5] : selfreal[base];
-    scal[3] = selfrec[base] + sr + wa.resid_self;
+    const double sr = wa.rigid ? scal[5] : selfreal[c];
+    scal[3] = selfrec[c] + sr + wa.resid_self;
     scal[4] = 1.0;
   }
 }
 
 // per-target weight engnmfc (engproc.F90:883-903, volcorrect :1022-1038)
-__global__ void k_weights(WeightArgs wa, int base, int n, const double* __restrict__ selfrec,
-                          const double* __restrict__ selfreal, const float* __restrict__ insw,
+__global__ void k_weights(WeightArgs wa, int base, int n, const int* __restrict__ skip,
+                          const double* __restrict__ selfrec, const double* __restrict__ selfreal,
+                          const float* __restrict__ insw,
                           const double* __restrict__ escrd, double* __restrict__ u0, double* __restrict__ w,
                           double* __restrict__ twt, int* __restrict__ sbin, const double* __restrict__ scal,
                           DevStatus* st) {
@@ -1214,10 +1266,11 @@ __global__ void k_weights(WeightArgs wa, int base, int n, const double* __restri
     }
     tw = (double)wa.stat_weight_system * (double)insw[cnt] * wa.npt_factor;
     e *= tw;
-    w[cnt] = e;
-    twt[cnt] = tw;
+    const bool rej = skip && skip[cnt];   // rejected: no update_histogram (engproc.F90:447-450)
+    w[cnt] = rej ? 0.0 : e;
+    twt[cnt] = rej ? 0.0 : tw;
     int l = -1;
-    if (wa.selfcal) {  // getiduv(0, uvengy0) (engproc.F90:910-913)
+    if (wa.selfcal && !rej) {  // getiduv(0, uvengy0) (engproc.F90:910-913)
       int lo = 0, h = wa.esmax;
       if (uu < escrd[0]) lo = 0;
       else if (uu > escrd[wa.esmax - 1]) lo = wa.esmax;
@@ -1237,23 +1290,32 @@ __global__ void k_weights(WeightArgs wa, int base, int n, const double* __restri
 // histogram, slnuv (soln) and the self-energy min / max.
 constexpr int kSumThreads = 1024;
 
-__global__ void __launch_bounds__(kSumThreads) k_wsum(WeightArgs wa, int base, int n, const double* __restrict__ w,
-    const double* __restrict__ twt, const double* __restrict__ u0, const int* __restrict__ sbin,
+__global__ void __launch_bounds__(kSumThreads) k_wsum(WeightArgs wa, int base, int n, const int* __restrict__ skip,
+    const double* __restrict__ w, const double* __restrict__ twt, const double* __restrict__ u0,
+    const int* __restrict__ sbin,
     const double* __restrict__ flceng, double* __restrict__ scal, double* __restrict__ eself,
     double* __restrict__ slnuv, float* __restrict__ minuv, float* __restrict__ maxuv) {
   __shared__ double r0[32], r1[32];
   __shared__ float rm[32], rx[32];
+  __shared__ int rk[32];
   double a0 = 0.0, a1 = 0.0;
   float mn = FLT_MAX, mx = -FLT_MAX;
+  int kept = 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (skip && skip[base + i]) continue;
     a0 += w[base + i];
     a1 += twt[base + i];
     const float u = (float)u0[base + i];
     mn = fminf(mn, u);
     mx = fmaxf(mx, u);
+    ++kept;
   }
   a0 = warp_sum(a0); a1 = warp_sum(a1); mn = warp_min(mn); mx = warp_max(mx);
-  if ((threadIdx.x & 31) == 0) { r0[threadIdx.x >> 5] = a0; r1[threadIdx.x >> 5] = a1; rm[threadIdx.x >> 5] = mn; rx[threadIdx.x >> 5] = mx; }
+  for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+  if ((threadIdx.x & 31) == 0) {
+    r0[threadIdx.x >> 5] = a0; r1[threadIdx.x >> 5] = a1; rm[threadIdx.x >> 5] = mn; rx[threadIdx.x >> 5] = mx;
+    rk[threadIdx.x >> 5] = kept;
+  }
   __syncthreads();
   if (threadIdx.x < 32) {
     const bool ok = threadIdx.x < (blockDim.x >> 5);
@@ -1261,9 +1323,11 @@ __global__ void __launch_bounds__(kSumThreads) k_wsum(WeightArgs wa, int base, i
     a1 = warp_sum(ok ? r1[threadIdx.x] : 0.0);
     mn = warp_min(ok ? rm[threadIdx.x] : FLT_MAX);
     mx = warp_max(ok ? rx[threadIdx.x] : -FLT_MAX);
+    kept = ok ? rk[threadIdx.x] : 0;
+    for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
     if (threadIdx.x == 0) {
       scal[1] += a0;
-      scal[2] += (double)n;
+      scal[2] += (double)kept;
       scal[0] += a1;
       minuv[0] = fminf(minuv[0], mn);
       maxuv[0] = fmaxf(maxuv[0], mx);
@@ -1286,11 +1350,11 @@ __global__ void __launch_bounds__(kSumThreads) k_wsum(WeightArgs wa, int base, i
 
 void launch_weights(const DeviceState& d, const WeightArgs& wa, int base, int n, cudaStream_t s) {
   if (n <= 0) return;
-  k_offset_init<<<1, 32, 0, s>>>(wa, base, d.selfrec, d.selfreal, d.scal);
-  k_weights<<<(n + 255) / 256, 256, 0, s>>>(wa, base, n, d.selfrec, d.selfreal, d.insw_in, d.escrd, d.u0, d.w,
-                                             d.twt, d.sbin, d.scal, d.status);
-  k_wsum<<<1, kSumThreads, 0, s>>>(wa, base, n, d.w, d.twt, d.u0, d.sbin, d.flceng, d.scal, d.eself, d.slnuv,
-                                   d.minuv, d.maxuv);
+  k_offset_init<<<1, 32, 0, s>>>(wa, base, n, d.skip, d.selfrec, d.selfreal, d.scal);
+  k_weights<<<(n + 255) / 256, 256, 0, s>>>(wa, base, n, d.skip, d.selfrec, d.selfreal, d.insw_in, d.escrd, d.u0,
+                                             d.w, d.twt, d.sbin, d.scal, d.status);
+  k_wsum<<<1, kSumThreads, 0, s>>>(wa, base, n, d.skip, d.w, d.twt, d.u0, d.sbin, d.flceng, d.scal, d.eself,
+                                   d.slnuv, d.minuv, d.maxuv);
 }
 
 __global__ void k_edens(int base, int n, int ermax, int ermax_pad, int count_base, const double* __restrict__ w,

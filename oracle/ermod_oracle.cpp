@@ -328,7 +328,10 @@ template <class T> struct Oracle {
     if (p.slttype != ERMOD_SLT_SOLN && !(p.insposition >= ERMOD_INSPOS_RANDOM &&
                                          p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC))
       return fail(ERMOD_ERR_UNSUPPORTED, "ins_geo");
-    if (p.slttype != ERMOD_SLT_SOLN && p.insposition >= ERMOD_INSPOS_SPHERE &&
+    if (p.slttype == ERMOD_SLT_SOLN && !(p.insposition >= ERMOD_INSPOS_RANDOM &&
+                                         p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC))
+      return fail(ERMOD_ERR_UNSUPPORTED, "ins_geo");
+    if (p.insposition >= ERMOD_INSPOS_SPHERE &&
         !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f && p.hostspec != 0))
       return fail(ERMOD_ERR_ARG, "ins_reg");
     return ERMOD_OK;
@@ -928,6 +931,34 @@ template <class T> struct Oracle {
       }
       if (ins_weight) for (int c = 0; c < maxdst; ++c) insw[c] = ins_weight[c];
     }
+    // soln: check_mol_configuration (engproc.F90:1197-1324) for sphere / slab regions;
+    // a rejected solute gets no energies and no update_histogram (:447-450, 754-755)
+    std::vector<char> skip(maxdst, 0);
+    if (!refs && p.insposition >= ERMOD_INSPOS_SPHERE) {
+      const bool slab = p.insposition != ERMOD_INSPOS_SPHERE;
+      if (slab && p.boxshp == ERMOD_SYS_NONPERIODIC) return fail(ERMOD_ERR_INS_GEO, "eng_slb");
+      aggregate_center(sitepos);
+      const T l3 = std::sqrt(cell[0][2] * cell[0][2] + cell[1][2] * cell[1][2] + cell[2][2] * cell[2][2]);
+      for (int cnt = 0; cnt < maxdst; ++cnt) {
+        const int tagslt = sltlist[cnt];
+        double c[3] = {0.0, 0.0, 0.0}, msum = 0.0;   // relative_com (:1300-1323)
+        for (int a = molbeg[tagslt]; a < molbeg[tagslt + 1]; ++a) {
+          const double m = (double)(float)sitemass[a];
+          for (int k = 0; k < 3; ++k) c[k] += m * (double)sitepos[3 * a + k];
+          msum += m;
+        }
+        T dx[3];
+        for (int k = 0; k < 3; ++k) dx[k] = (T)(float)(c[k] / msum) - (T)(float)aggcen[k];
+        T dist;
+        if (!slab) {
+          dist = std::sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+        } else {
+          dist = (invcl[2][0] * dx[0] + invcl[2][1] * dx[1] + invcl[2][2] * dx[2]) * l3;
+          if (p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) dist = std::abs(dist);
+        }
+        skip[cnt] = ((T)p.lwreg > dist || dist > (T)p.upreg) ? 1 : 0;
+      }
+    }
     // PME setup (engconst :419-437)
     const bool pme = p.cltype == ERMOD_EL_PME;
     std::vector<T> wslv;
@@ -974,6 +1005,7 @@ template <class T> struct Oracle {
       std::vector<int> satoms;
 #pragma omp for schedule(dynamic, 1)
       for (int cnt = 0; cnt < maxdst; ++cnt) {
+        if (skip[cnt]) continue;
         const int tagslt = refs ? nummol - 1 : sltlist[cnt];
         const int ns = numsite[tagslt];
         satoms.resize(ns);
@@ -1005,6 +1037,7 @@ template <class T> struct Oracle {
     }
     // uvengy0 (engproc.F90:828-855); rigid refs reuse the first real self energy
     for (int cnt = 0; cnt < maxdst; ++cnt) {
+      if (skip[cnt]) continue;
       const int tagslt = refs ? nummol - 1 : sltlist[cnt];
       T pairep;
       if (refs) {
@@ -1020,6 +1053,7 @@ template <class T> struct Oracle {
     int warn = 0;
     std::vector<int> insdst(ermax);
     for (int cnt = 0; cnt < maxdst; ++cnt) {
+      if (skip[cnt]) continue;
       const int rc = update_histogram(cnt, (T)stat_weight_system, &warn, insdst);
       if (rc < 0) return rc;
     }

@@ -73,3 +73,29 @@ def nacl_system(ncell=4, d=2.8, ecdmin=-200.0, K=32, order=6, elecut=11.0):
 MADELUNG_NACL = 1.747564594633   # NaCl Madelung constant (nearest-neighbour distance convention)
 WIGNER_SC = -2.837297479         # Ewald self-image potential constant of a simple cubic lattice
 COULOMB = float(np.float32(18.22261721)) ** 2   # e^2/A in kcal/mol as the scaled charges carry it
+
+
+# Four LJ sites in an 8^3 water box, at these offsets (A) from the box centre; every pair is
+# at least 6.5 A apart, and waters are pushed out to 3 A from each, as for the soln workload.
+SOLN_SOLUTE_OFFSETS = np.array([[1.5, 0.0, 0.0], [-5.0, 0.0, 0.0], [0.0, 7.0, 0.0], [0.0, 0.0, -10.0]])
+
+
+def soln_multi_system(seed=11):
+    """Solutes in solution (slttype soln) with four solute molecules, for check_mol_configuration:
+    (params, topo, hist, sitepos, cell, offsets).  Species: 1 = the LJ sites, 2 = water."""
+    nside, box, K = 8, 24.9, 32
+    c0 = np.full(3, box / 2)
+    centres = c0 + SOLN_SOLUTE_OFFSETS
+    wat = S.water_box_frame(nside, box, seed).T.reshape(-1, 3, 3)   # (n, 3 sites, xyz)
+    for c in centres:
+        for i in range(len(wat)):
+            d = wat[i, 0] - c
+            d -= box * np.round(d / box)
+            r = np.linalg.norm(d)
+            if r < 3.0:
+                wat[i] += d / max(r, 1e-6) * (3.0 - r)
+    topo = S.Topology([S.lj_site(), S.water()], [len(centres), nside ** 3], [A.PT_SOLUTE, A.PT_SOLVENT])
+    prm = S.default_params(slttype=A.SLT_SOLN, ms1max=K, maxins=1, corrcal=0, wgtslf=0, hostspec=2)
+    pos = np.concatenate([centres, wat.reshape(-1, 3)], axis=0)
+    cell = np.diag([box] * 3).astype(np.float32)
+    return prm, topo, {}, A.as_f32(pos.ravel()), A.as_f32(cell.ravel(order="F")), SOLN_SOLUTE_OFFSETS

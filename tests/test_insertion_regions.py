@@ -104,3 +104,30 @@ def test_region_parameters_are_checked(oracle_mod):
         prm = dict(w.params, insposition=A.INSPOS_SPHERE, **bad)
         with pytest.raises(Exception):
             oracle_mod.Oracle(prm, w.topo, w.hist)
+
+
+# ---- solutes in solution: check_mol_configuration (engproc.F90:1197-1324) ----
+from _helpers import soln_multi_system  # noqa: E402
+
+
+@pytest.mark.parametrize("insposition,lw,up,expect", [
+    (A.INSPOS_SPHERE, 3.0, 8.0, [False, True, True, False]),          # |offset| 1.5, 5, 7, 10
+    (A.INSPOS_SLAB_SYMMETRIC, 8.0, 11.0, [False, False, False, True]), # |dz| 0, 0, 0, 10
+    (A.INSPOS_SLAB_GENERIC, 8.0, 11.0, [False, False, False, False]),  # dz = -10 is below the slab
+    (A.INSPOS_RANDOM, 0.0, 0.0, [True, True, True, True]),
+])
+def test_soln_configuration_check(oracle_mod, insposition, lw, up, expect):
+    """A solute whose centre of mass lies outside the region around the water aggregate's centre
+    is skipped for the frame: no energies and no update_histogram (engproc.F90:447-450, 754-755)."""
+    prm, topo, hist, pos, cell, _ = soln_multi_system()
+    prm = dict(prm, insposition=insposition, lwreg=lw, upreg=up, keep_uvengy=1)
+    orc = oracle_mod.Oracle(prm, topo, hist)
+    assert orc.engconst(1, pos, cell) >= 0
+    u, _ = orc.uvengy()
+    kept = np.array(expect)
+    assert np.all(np.any(u[kept] != 0.0, axis=1))
+    assert np.all(u[~kept] == 0.0)
+    a = orc.accum()
+    assert a["engsmpl"] == kept.sum()
+    # each kept solute bins every other molecule once, with the same weight (neutral solutes)
+    assert a["edens"].sum() == pytest.approx(a["engnorm"] * (u.shape[1] - 1), rel=1e-9, abs=1e-12)

@@ -117,6 +117,27 @@ def test_refs_region_energies_and_bins(lib, oracle_mod):
     assert np.all((bg == bo) | near_edge(uo, eng.uvcrd, energy_tol(uo)))
 
 
+@pytest.mark.parametrize("insposition,lw,up", [(A.INSPOS_SPHERE, 3.0, 8.0), (A.INSPOS_SLAB_SYMMETRIC, 8.0, 11.0)])
+def test_soln_configuration_check_matches_oracle(lib, oracle_mod, insposition, lw, up):
+    """Solutes in solution outside the region are skipped (check_mol_configuration): the same
+    solutes on the GPU and in the oracle, with the same energies and accumulators."""
+    from _helpers import soln_multi_system
+    prm, topo, hist, pos, cell, _ = soln_multi_system()
+    prm = dict(prm, insposition=insposition, lwreg=lw, upreg=up, keep_uvengy=1)
+    eng = Engine(prm, topo, hist)
+    orc = oracle_mod.Oracle(prm, topo, hist)
+    assert eng.engconst(1, pos, cell) >= 0
+    assert orc.engconst(1, pos, cell) >= 0
+    u, _ = eng.uvengy()
+    uo, _ = orc.uvengy()
+    np.testing.assert_array_equal(np.all(u == 0.0, axis=1), np.all(uo == 0.0, axis=1))
+    check_energies(u, uo)
+    a, b = eng.accum(), orc.accum()
+    assert a["engsmpl"] == b["engsmpl"] < 4
+    assert a["engnorm"] == pytest.approx(b["engnorm"], rel=1e-9)
+    np.testing.assert_allclose(a["edens"], b["edens"], rtol=1e-9, atol=1e-9 * max(1.0, b["engnorm"]))
+
+
 def test_slab_insertion_needs_a_periodic_cell(lib):
     w = S.make_workload(2, small=True, maxins=8)
     prm = dict(w.params, insposition=A.INSPOS_SLAB_SYMMETRIC, lwreg=1.0, upreg=3.0, hostspec=1,
