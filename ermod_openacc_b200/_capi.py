@@ -33,6 +33,7 @@ EL_COULOMB, EL_EWALD, EL_PME, EL_PPPM = 0, 1, 2, 3
 LJSWT_POT_CHM, LJSWT_POT_GMX, LJSWT_FRC_CHM, LJSWT_FRC_GMX = 0, 1, 2, 3
 INSPOS_RANDOM, INSPOS_NOCHANGE = 0, 1
 INSPOS_SPHERE, INSPOS_SLAB_GENERIC, INSPOS_SLAB_SYMMETRIC = 2, 3, 4
+INSPOS_RMSD, INSPOS_GAUSS = 5, 6
 INSROT_RANDOM, INSROT_NOCHANGE = 0, 1
 PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
 
@@ -114,6 +115,7 @@ SIGNATURES = {
     "ermod_create": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(ErmodParams),
                                  C.POINTER(ErmodTopology), C.POINTER(ErmodMesh)]),
     "ermod_engclear": (C.c_int32, [C.c_void_p]),
+    "ermod_set_refstructure": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, _f32p, _f32p, _f32p, _f32p]),
     "ermod_engconst": (C.c_int32, [C.c_void_p, C.c_int32, _f32p, _f32p, C.c_float, _f32p, _f32p, _f32p]),
     "ermod_engconst_dev": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, _f32p, C.c_float,
                                        C.c_void_p, C.c_void_p]),

@@ -192,6 +192,7 @@ enum : int {
   kErrOverflow = 16,  // internal capacity exceeded
   kErrGrid = 32,      // a PME grid index outside the grid
   kErrTimeout = 64,   // a bounded wait on an mbarrier expired
+  kErrInsRej = 128,   // an insertion found no configuration in the RMSD window within kInsTries
 };
 
 struct DevStatus {

@@ -65,6 +65,9 @@ struct ermod_ctx {
   DeviceState d;
   int chunk = kChunk, batch = 0, ncell_cap = 0;
   int nhost = 0;                      // atoms of the host aggregate (insposition 2..4)
+  int nref = 0;                       // atoms of the RefInfo host (insposition 5, 6)
+  bool gauss_init = false;            // Gaussian insertion constants fixed at the first frame
+  float gauss_l[3] = {0.f, 0.f, 0.f}, gauss_z0 = 0.f, gauss_z1 = 0.f;
   cufftHandle r2c = 0, c2r = 0;
   bool plans = false;
   void* tc_work = nullptr;
@@ -132,7 +135,8 @@ void free_all(ermod_ctx* c) {
                   d.boxinfo, d.partial, d.done, d.uvengy, d.counts, d.edens, d.edens_part, d.ecorr, d.eself,
                   d.slnuv, d.minuv, d.maxuv, d.scal, d.status, d.frame_i, d.dens, d.feat, d.mlp_f, d.mlp_b,
                   d.vact, d.vlogit, d.vcdf, d.vq, d.ins_voxel, d.ins_feat, d.host_atom, d.host_mass, d.aggcen,
-                  d.atom_mass, d.skip, c->tc_work};
+                  d.atom_mass, d.skip, d.ref_atom, d.ref_host, d.ref_host_w, d.ref_slt, d.ref_slt_w, d.ref_bf,
+                  c->tc_work};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->plans) {
@@ -275,15 +279,18 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     return bad(ERMOD_ERR_ARG, "set_prs");
   if (p.slttype < 1 || p.slttype > 3) return bad(ERMOD_ERR_ARG, "set_slt");
   if (p.slttype != ERMOD_SLT_SOLN &&
-      !((p.insposition >= ERMOD_INSPOS_RANDOM && p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC) &&
+      !((p.insposition >= ERMOD_INSPOS_RANDOM && p.insposition <= ERMOD_INSPOS_GAUSS) &&
         (p.insorient == ERMOD_INSROT_RANDOM || p.insorient == ERMOD_INSROT_NOCHANGE)))
     return bad(ERMOD_ERR_UNSUPPORTED, "ins_geo");
-  // sphere / slab regions: refs insertion (set_shift_com) and soln configuration checks
-  // (check_mol_configuration); RMSD / Gaussian (5, 6) need the RefInfo structure, not built
-  if (p.slttype == ERMOD_SLT_SOLN && (p.insposition < ERMOD_INSPOS_RANDOM || p.insposition > ERMOD_INSPOS_SLAB_SYMMETRIC))
+  // sphere / slab regions around the host aggregate and RMSD / Gaussian insertion against the
+  // RefInfo structure: refs insertion (set_shift_com) and soln configuration checks
+  // (check_mol_configuration)
+  if (p.slttype == ERMOD_SLT_SOLN && (p.insposition < ERMOD_INSPOS_RANDOM || p.insposition > ERMOD_INSPOS_GAUSS))
     return bad(ERMOD_ERR_UNSUPPORTED, "ins_geo");
-  const bool region = p.insposition >= ERMOD_INSPOS_SPHERE;
+  const bool region = p.insposition >= ERMOD_INSPOS_SPHERE && p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC;
   if (region && !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f && p.hostspec != 0))
+    return bad(ERMOD_ERR_ARG, "ins_reg");
+  if (p.insposition >= ERMOD_INSPOS_RMSD && !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f))
     return bad(ERMOD_ERR_ARG, "ins_reg");
   // topology (setparam / enginit / engconst bookkeeping)
   ctx->nummol = t->nummol;
@@ -487,10 +494,12 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
         const int i = ctx->tagpt[k];
         for (int j = 0; j < ctx->numsite[i]; ++j) am.push_back(ctx->mass[ctx->molbeg_all[i] + j]);
       }
-      CK(dalloc(&d.atom_mass, NA)); CK(dalloc(&d.skip, MD));
+      CK(dalloc(&d.atom_mass, NA));
       CK(h2d(d.atom_mass, am.data(), NA, st));
     }
   }
+  // soln: the verdicts of check_mol_configuration (sphere / slab around the aggregate, RMSD to RefInfo)
+  if (!refs && (ctx->nhost > 0 || p.insposition == ERMOD_INSPOS_RMSD)) CK(dalloc(&d.skip, MD));
   std::vector<float> bf(3 * S, 0.0f);
   if (t->bfcoord) std::memcpy(bf.data(), t->bfcoord, sizeof(float) * 3 * S);
   CK(h2d(d.bfcoord, bf.data(), 3 * S, st));
@@ -551,6 +560,44 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   double sc[8] = {0, 0, 0, -(double)FLT_MAX, 0, 0, 0, 0};
   CK(h2d(d.scal, sc, 8, st));
   CK(cudaStreamSynchronize(st));
+  return ERMOD_OK;
+}
+
+int32_t ermod_set_refstructure(ermod_ctx* ctx, int32_t refspec, int32_t nhost, const float* host_crd,
+                               const float* host_w, const float* slt_crd, const float* slt_w) {
+  if (!ctx || refspec == 0 || nhost <= 0 || !host_crd || !host_w || !slt_crd || !slt_w) return ERMOD_ERR_ARG;
+  ctx->err.clear();
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->st));
+  // refhost_specatm (insertion.F90:686-702): every atom of the refspec molecules, in molecule order
+  std::vector<int> atoms;
+  int off = 0;
+  for (int k = 0; k < ctx->slvmax; ++k) {
+    const int i = ctx->tagpt[k], sp = ctx->uvspec[i];
+    if (sp >= 1 && sp <= 31 && ((refspec >> (sp - 1)) & 1))
+      for (int j = 0; j < ctx->numsite[i]; ++j) atoms.push_back(off + j);
+    off += ctx->numsite[i];
+  }
+  if ((int)atoms.size() != nhost) return set_error(ctx, ERMOD_ERR_ARG, "ins_ref");
+  double wh = 0.0, wsl = 0.0;
+  for (int i = 0; i < nhost; ++i) wh += host_w[i];
+  for (int i = 0; i < ctx->s; ++i) wsl += slt_w[i];
+  if (!(wh > 0.0) || !(wsl > 0.0)) return set_error(ctx, ERMOD_ERR_ARG, "bst_zrw");   // bestfit.F90:261
+  DeviceState& d = ctx->d;
+  for (void* q : {(void*)d.ref_atom, (void*)d.ref_host, (void*)d.ref_host_w, (void*)d.ref_slt, (void*)d.ref_slt_w,
+                  (void*)d.ref_bf})
+    if (q) cudaFree(q);
+  const size_t n = nhost, S = ctx->s;
+  CK(dalloc(&d.ref_atom, n)); CK(dalloc(&d.ref_host, 3 * n)); CK(dalloc(&d.ref_host_w, n));
+  CK(dalloc(&d.ref_slt, 3 * S)); CK(dalloc(&d.ref_slt_w, S)); CK(dalloc(&d.ref_bf, 3 * S));
+  CK(h2d(d.ref_atom, atoms.data(), n, ctx->st));
+  CK(h2d(d.ref_host, host_crd, 3 * n, ctx->st));
+  CK(h2d(d.ref_host_w, host_w, n, ctx->st));
+  CK(h2d(d.ref_slt, slt_crd, 3 * S, ctx->st));
+  CK(h2d(d.ref_slt_w, slt_w, S, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->nref = nhost;
+  ctx->gkey.clear();   // the frame graph holds the old buffers: capture it again
   return ERMOD_OK;
 }
 
@@ -691,6 +738,23 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
   if (!refs && (p.insposition == ERMOD_INSPOS_SLAB_GENERIC || p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) &&
       !g.periodic)
     return set_error(ctx, ERMOD_ERR_INS_GEO, "eng_slb");   // engproc.F90:1238
+  if (p.insposition >= ERMOD_INSPOS_RMSD && ctx->nref == 0 && (refs || p.insposition == ERMOD_INSPOS_RMSD))
+    return set_error(ctx, ERMOD_ERR_ARG, "ins_ref");        // load_refstructure (insertion.F90:676-770)
+  if (refs && p.insposition == ERMOD_INSPOS_GAUSS && !ctx->gauss_init) {
+    // uniform_gauss_mixture keeps the first call's cell (insertion.F90:268-274): l = (|c_k|/2)/upreg,
+    // z0 = 8 l1 l2 l3, z1 = pi^(3/2) erf(l1) erf(l2) erf(l3)
+    double z0 = 8.0, z1 = std::pow(kPi, 1.5);
+    for (int k = 0; k < 3; ++k) {
+      const double len = std::sqrt(c[0][k] * c[0][k] + c[1][k] * c[1][k] + c[2][k] * c[2][k]);
+      const double l = 0.5 * len / p.upreg;
+      ctx->gauss_l[k] = (float)l;
+      z0 *= l;
+      z1 *= std::erf(l);
+    }
+    ctx->gauss_z0 = (float)z0;
+    ctx->gauss_z1 = (float)z1;
+    ctx->gauss_init = true;
+  }
   // ---- pair / PME constants ----
   PairParams& P = a.pp;
   P.lw = p.lwljcut; P.up = p.upljcut; P.lw2 = p.lwljcut * p.lwljcut; P.up2 = p.upljcut * p.upljcut;
@@ -848,14 +912,30 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
     launch_aggcen(d, ctx->nhost, st);
     nl += 1;
   }
-  if (refs)
-    launch_insert(a, d, d.frame_i, p.iseed, p.insposition, p.insorient, p.lwreg, p.upreg, fp.use_conf, fp.prop_gv,
-                  fp.prop_learned, st);
+  if (ctx->nref > 0 && p.insposition >= ERMOD_INSPOS_RMSD) {   // reffit's host fit, once per frame
+    launch_reffit(d, ctx->nref, ctx->s, st);
+    nl += 1;
+  }
+  if (refs) {
+    InsRegion rg{};
+    rg.insposition = p.insposition;
+    rg.insorient = p.insorient;
+    rg.lwreg = p.lwreg;
+    rg.upreg = p.upreg;
+    for (int k = 0; k < 3; ++k) rg.gl[k] = ctx->gauss_l[k];
+    rg.z0 = ctx->gauss_z0;
+    rg.z1 = ctx->gauss_z1;
+    launch_insert(a, d, d.frame_i, p.iseed, rg, fp.use_conf, fp.prop_gv, fp.prop_learned, st);
+  }
   else launch_targets_soln(a, d, nullptr, st);
   if (!refs && ctx->nhost > 0) {   // check_mol_configuration of every solute
     launch_aggcen(d, ctx->nhost, st);
     launch_soln_region(a, d, p.insposition, p.lwreg, p.upreg, st);
     nl += 2;
+  }
+  if (!refs && ctx->nref > 0 && p.insposition == ERMOD_INSPOS_RMSD) {
+    launch_soln_region(a, d, p.insposition, p.lwreg, p.upreg, st);
+    nl += 1;
   }
   CK(cudaMemsetAsync(d.selfrec, 0, sizeof(double) * ctx->maxdst, st));
   CK(cudaMemsetAsync(d.etot, 0, sizeof(double) * ctx->maxdst, st));
@@ -963,6 +1043,7 @@ static int frame_finish(ermod_ctx* ctx, bool timed, float total_ms) {
   if (hs.flags & kErrOverflow) return set_error(ctx, ERMOD_ERR_OVERFLOW, "ermod_ovf");
   if (hs.flags & kErrGrid) return set_error(ctx, ERMOD_ERR_OVERFLOW, "spr_box");
   if (hs.flags & kErrTimeout) return set_error(ctx, ERMOD_ERR_CUDA, "tc_wait");
+  if (hs.flags & kErrInsRej) return set_error(ctx, ERMOD_ERR_INS_GEO, "ins_rej");
   if ((hs.flags & kWarnMbin) && ctx->warn_bin_firsttime) {
     ctx->warn_bin_firsttime = false;
     return set_error(ctx, ERMOD_WARN_MBIN, "mbin");

@@ -160,6 +160,13 @@ struct DeviceState {
   float* host_mass = nullptr;// [nhost]
   double* aggcen = nullptr;  // [3] mass-weighted centre of the host aggregate, this frame
   float* atom_mass = nullptr;// [natoms] (soln region checks: solute centres of mass)
+  // RefInfo reference structure (insposition 5, 6)
+  int* ref_atom = nullptr;   // [nref] posraw atoms of the refspec molecules, in molecule order
+  float* ref_host = nullptr; // [3*nref] their reference coordinates
+  float* ref_host_w = nullptr;  // [nref] fit weights
+  float* ref_slt = nullptr;  // [3*s] reference solute coordinates
+  float* ref_slt_w = nullptr;// [s]
+  float* ref_bf = nullptr;   // [3*s] this frame's best-fit reference solute (reffit)
   int* skip = nullptr;       // [maxdst] soln: 1 where check_mol_configuration rejects the solute this frame
   int* ins_voxel = nullptr;  // [maxdst] voxel of each insertion
   float* ins_feat = nullptr; // [maxdst][64] features of each insertion's voxel (training data, on request)
@@ -171,8 +178,17 @@ void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStrea
 void launch_aggcen(const DeviceState& d, int nhost, cudaStream_t s);
 void launch_soln_region(const FrameArgs& a, const DeviceState& d, int insposition, float lwreg, float upreg,
                         cudaStream_t s);
-void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, int insposition,
-                   int insorient, float lwreg, float upreg, int use_conf, int gv, int learned, cudaStream_t s);
+// Insertion geometry of a frame (set_shift_com, insertion.F90:131-304)
+struct InsRegion {
+  int insposition, insorient;
+  float lwreg, upreg;
+  float gl[3];      // Gaussian insertion: (|c_k| / 2) / upreg of the first frame
+  float z0, z1;     // its mixture normalisations 8 l1 l2 l3 and pi^(3/2) erf(l1) erf(l2) erf(l3)
+};
+constexpr int kInsTries = 1024;   // configurations an RMSD-window insertion may try (the reference loops on)
+void launch_reffit(const DeviceState& d, int nref, int s, cudaStream_t st);
+void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, const InsRegion& rg,
+                   int use_conf, int gv, int learned, cudaStream_t s);
 // proposal (proposal.cu) and its network (mlp.cu)
 MlpLayout mlp_layout();
 void mlp_forward(const __nv_bfloat16* pw, const float* pf, const float* x, int n, float* act, float* logits,

@@ -20,6 +20,7 @@
 #include <cfloat>
 #include <cstdio>
 
+#include "bestfit.cuh"
 #include "engine.cuh"
 
 namespace erm {
@@ -250,6 +251,78 @@ void launch_aggcen(const DeviceState& d, int nhost, cudaStream_t s) {
   k_aggcen<<<1, kAggThreads, 0, s>>>(nhost, d.host_atom, d.host_mass, d.posraw, d.aggcen);
 }
 
+// reffit's first step (insertion.F90:658-666, fit_a_rotate_b bestfit.F90:309-336): the reference
+// host is fitted onto this frame's host atoms and the reference solute carried along,
+// ref_bf = R (ref_slt - c_ref) + c_frame.  One block, FP64 sums in a fixed order (per thread,
+// warps, block); the 4x4 eigenproblem and the carried solute on thread 0.
+__global__ void __launch_bounds__(kAggThreads) k_reffit(int nref, int s, const int* __restrict__ ref_atom,
+                                                       const float* __restrict__ posraw,
+                                                       const float* __restrict__ ref_host,
+                                                       const float* __restrict__ ref_host_w,
+                                                       const float* __restrict__ ref_slt, float* __restrict__ ref_bf) {
+  __shared__ double red[9][32];
+  __shared__ double cen[7];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  auto block_sum = [&](double (&v)[9], int nv) {
+    for (int c = 0; c < nv; ++c) {
+      const double t = warp_sum(v[c]);
+      if (lane == 0) red[c][warp] = t;
+    }
+    __syncthreads();
+    if (warp == 0)
+      for (int c = 0; c < nv; ++c) {
+        const double t = warp_sum(red[c][lane]);
+        if (lane == 0) red[c][0] = t;
+      }
+    __syncthreads();
+  };
+  // centres: sum w, sum w x_frame, sum w x_ref
+  double v[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int i = tid; i < nref; i += kAggThreads) {
+    const double w = ref_host_w[i];
+    const int at = ref_atom[i];
+    for (int k = 0; k < 3; ++k) {
+      v[1 + k] += w * posraw[3 * at + k];
+      v[4 + k] += w * ref_host[3 * i + k];
+    }
+    v[0] += w;
+  }
+  block_sum(v, 7);
+  if (tid == 0)
+    for (int c = 0; c < 7; ++c) cen[c] = c == 0 ? red[0][0] : red[c][0] / red[0][0];
+  __syncthreads();
+  // S[r][c] = sum w (x_ref - c_ref)_r (x_frame - c_frame)_c: the reference (moving) onto the frame
+  for (int c = 0; c < 9; ++c) v[c] = 0.0;
+  for (int i = tid; i < nref; i += kAggThreads) {
+    const double w = ref_host_w[i];
+    const int at = ref_atom[i];
+    double xr[3], xf[3];
+    for (int k = 0; k < 3; ++k) {
+      xr[k] = ref_host[3 * i + k] - cen[4 + k];
+      xf[k] = posraw[3 * at + k] - cen[1 + k];
+    }
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) v[3 * r + c] += w * xr[r] * xf[c];
+  }
+  block_sum(v, 9);
+  if (tid == 0) {
+    double S[3][3], q[4];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) S[r][c] = red[3 * r + c][0];
+    fit::rotation_from_s(S, q);
+    for (int i = 0; i < s; ++i) {
+      const double x[3] = {ref_slt[3 * i] - cen[4], ref_slt[3 * i + 1] - cen[5], ref_slt[3 * i + 2] - cen[6]};
+      double r[3];
+      fit::rotate(q, x, r);
+      for (int k = 0; k < 3; ++k) ref_bf[3 * i + k] = (float)(r[k] + cen[1 + k]);
+    }
+  }
+}
+
+void launch_reffit(const DeviceState& d, int nref, int s, cudaStream_t st) {
+  k_reffit<<<1, kAggThreads, 0, st>>>(nref, s, d.ref_atom, d.posraw, d.ref_host, d.ref_host_w, d.ref_slt, d.ref_bf);
+}
+
 // check_mol_configuration (engproc.F90:1197-1324) for solutes in solution, sphere
 // and slab regions: the solute's centre of mass relative to the host aggregate's
 // centre (relative_com :1300-1323) must lie in lwreg..upreg, as a distance
@@ -259,10 +332,17 @@ void launch_aggcen(const DeviceState& d, int nhost, cudaStream_t s) {
 __global__ void k_soln_region(FrameArgs a, int insposition, float lwreg, float upreg, const int* __restrict__ tgt_mol,
                               const int* __restrict__ molbeg, const float* __restrict__ posraw,
                               const float* __restrict__ atom_mass, const double* __restrict__ aggcen,
+                              const float* __restrict__ ref_bf, const float* __restrict__ ref_slt_w,
                               int* __restrict__ skip) {
   const int cnt = blockIdx.x * blockDim.x + threadIdx.x;
   if (cnt >= a.maxdst) return;
   const int k = tgt_mol[cnt];
+  if (insposition == ERMOD_INSPOS_RMSD) {
+    // RMSD of the solute to this frame's best-fit reference solute (engproc.F90:1249-1269)
+    const double rmsd = fit::rmsd_nofit(a.nsite, ref_bf, posraw + 3 * molbeg[k], ref_slt_w);
+    skip[cnt] = ((double)lwreg > rmsd || rmsd > (double)upreg) ? 1 : 0;
+    return;
+  }
   double c[3] = {0.0, 0.0, 0.0}, msum = 0.0;
   for (int at = molbeg[k]; at < molbeg[k + 1]; ++at) {
     const double m = atom_mass[at];
@@ -286,11 +366,12 @@ __global__ void k_soln_region(FrameArgs a, int insposition, float lwreg, float u
 void launch_soln_region(const FrameArgs& a, const DeviceState& d, int insposition, float lwreg, float upreg,
                         cudaStream_t s) {
   k_soln_region<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, insposition, lwreg, upreg, d.tgt_mol, d.molbeg, d.posraw,
-                                                       d.atom_mass, d.aggcen, d.skip);
+                                                       d.atom_mass, d.aggcen, d.ref_bf, d.ref_slt_w, d.skip);
 }
 
-__global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int iseed, int insposition, int insorient,
-                         float lwreg, float upreg, const double* __restrict__ aggcen,
+__global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int iseed, InsRegion rg,
+                         const double* __restrict__ aggcen, const float* __restrict__ ref_bf,
+                         const float* __restrict__ ref_slt_w, DevStatus* st,
                          int use_conf, int gv, int learned, const double* __restrict__ cdf,
                          const float* __restrict__ qv, int* __restrict__ ins_voxel, float* __restrict__ insw,
                          const float* __restrict__ conf_all, const float* __restrict__ bfcoord,
@@ -299,6 +380,8 @@ __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int ise
   const int cnt = blockIdx.x * blockDim.x + threadIdx.x;
   if (cnt >= a.maxdst) return;
   const int s = a.nsite;
+  const int insposition = rg.insposition, insorient = rg.insorient;
+  const float lwreg = rg.lwreg, upreg = rg.upreg;
   const int stnum = *stnum_dev;   // staged per frame, so a captured frame graph replays with the new value
   float4* out = tgt_raw + (size_t)cnt * s;
   const float* conf = use_conf ? conf_all + (size_t)3 * s * cnt : bfcoord;
@@ -393,13 +476,15 @@ __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int ise
       out[i].z += sh[2];
     }
   }
-  if (insorient == ERMOD_INSROT_RANDOM) {  // apply_orientation (insertion.F90:348-369)
+  // apply_orientation (insertion.F90:348-369): a random unit quaternion by rejection in the
+  // 4-ball, rotation about the centre of mass; counters (cnt, stnum, attempt, tag)
+  auto orient = [&](uint32_t tag) {
     float c[3];
     com(c);
     for (int i = 0; i < s; ++i) { out[i].x -= c[0]; out[i].y -= c[1]; out[i].z -= c[2]; }
     float q0 = 1.f, q1 = 0.f, q2 = 0.f, q3 = 0.f;
     for (uint32_t att = 1; att <= 64; ++att) {
-      const uint4 r4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, att, 1u), key);
+      const uint4 r4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, att, tag), key);
       const float t0 = u01(r4.x) * 2.f - 1.f, t1 = u01(r4.y) * 2.f - 1.f;
       const float t2 = u01(r4.z) * 2.f - 1.f, t3 = u01(r4.w) * 2.f - 1.f;
       const float n2 = t0 * t0 + t1 * t1 + t2 * t2 + t3 * t3;
@@ -420,16 +505,104 @@ __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int ise
       out[i].y = (t3 * c1 - t1 * c3 + t0 * c2 + q0 * t2) + c[1];
       out[i].z = (t1 * c2 - t2 * c1 + t0 * c3 + q0 * t3) + c[2];
     }
+  };
+  if (insposition == ERMOD_INSPOS_RMSD || insposition == ERMOD_INSPOS_GAUSS) {
+    // insorigin 3: try configurations until the RMSD to this frame's best-fit reference solute
+    // lies in lwreg..upreg (instslt insertion.F90:86-94, check_solute_configuration :617-643)
+    float wfac = 1.0f;
+    bool ok = false;
+    for (int tr = 0; tr < kInsTries && !ok; ++tr) {
+      const uint32_t tg = (uint32_t)tr << 8;
+      // set_solute_origin / reffit (:646-673): the conformation fitted onto the best-fit reference
+      {
+        double cr[3] = {0.0, 0.0, 0.0}, ca[3] = {0.0, 0.0, 0.0}, ws = 0.0;
+        for (int i = 0; i < s; ++i) {
+          const double w = ref_slt_w[i];
+          for (int k = 0; k < 3; ++k) { cr[k] += w * ref_bf[3 * i + k]; ca[k] += w * conf[3 * i + k]; }
+          ws += w;
+        }
+        for (int k = 0; k < 3; ++k) { cr[k] /= ws; ca[k] /= ws; }
+        double S[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+        for (int i = 0; i < s; ++i)
+          for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c)
+              S[r][c] += (double)ref_slt_w[i] * ((double)conf[3 * i + r] - ca[r]) * ((double)ref_bf[3 * i + c] - cr[c]);
+        double q[4];
+        fit::rotation_from_s(S, q);
+        for (int i = 0; i < s; ++i) {
+          const double v[3] = {conf[3 * i] - ca[0], conf[3 * i + 1] - ca[1], conf[3 * i + 2] - ca[2]};
+          double r[3];
+          fit::rotate(q, v, r);
+          out[i].x = (float)(r[0] + cr[0]);
+          out[i].y = (float)(r[1] + cr[1]);
+          out[i].z = (float)(r[2] + cr[2]);
+        }
+      }
+      // set_shift_com (:201-224 RMSD, :225-300 Gaussian)
+      float sh[3];
+      if (insposition == ERMOD_INSPOS_RMSD) {
+        float c[3];
+        com(c);
+        float maxd = 0.f;
+        for (int i = 0; i < s; ++i) {
+          const float dx = out[i].x - c[0], dy = out[i].y - c[1], dz = out[i].z - c[2];
+          maxd = fmaxf(maxd, dx * dx + dy * dy + dz * dz);
+        }
+        const float movmax = upreg + 3.0f * sqrtf(maxd);   // margin_factor 3
+        const uint4 r4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, tg, 3u), key);
+        sh[0] = movmax * (2.f * u01(r4.x) - 1.f);
+        sh[1] = movmax * (2.f * u01(r4.y) - 1.f);
+        sh[2] = movmax * (2.f * u01(r4.z) - 1.f);
+      } else {
+        // uniform_gauss_mixture: alternately uniform over +-l and N(0, 1/2) truncated at l, in
+        // units of sigma = upreg; the weight divided by the mixture density (WHAM form)
+        float sc[3];
+        if (((cnt + tr) & 1) == 0) {
+          const uint4 r4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, tg, 4u), key);
+          const float u[3] = {u01(r4.x), u01(r4.y), u01(r4.z)};
+          for (int k = 0; k < 3; ++k) sc[k] = (2.f * u[k] - 1.f) * rg.gl[k];
+        } else {
+          for (int k = 0; k < 3; ++k) {
+            sc[k] = 0.f;
+            for (uint32_t att = 1; att <= 64; ++att) {   // Box-Muller pairs, the first inside +-l
+              const uint4 r4 = philox4x32_10(make_uint4((uint32_t)cnt, (uint32_t)stnum, tg | att, 5u + k), key);
+              const float u1 = fmaxf(u01(r4.x), 1.0e-7f), u2 = u01(r4.y);
+              const float r = sqrtf(-2.f * logf(u1)) * cospif(2.f * u2) * 0.70710678f;
+              if (fabsf(r) < rg.gl[k]) { sc[k] = r; break; }
+            }
+          }
+        }
+        const float sq = sc[0] * sc[0] + sc[1] * sc[1] + sc[2] * sc[2];
+        wfac /= 0.5f / rg.z0 + 0.5f * expf(-sq) / rg.z1;
+        const float f[3] = {sc[0] / (2.f * rg.gl[0]), sc[1] / (2.f * rg.gl[1]), sc[2] / (2.f * rg.gl[2])};
+        for (int k = 0; k < 3; ++k) sh[k] = a.g.cell[k][0] * f[0] + a.g.cell[k][1] * f[1] + a.g.cell[k][2] * f[2];
+      }
+      for (int i = 0; i < s; ++i) { out[i].x += sh[0]; out[i].y += sh[1]; out[i].z += sh[2]; }
+      if (insorient == ERMOD_INSROT_RANDOM) orient(1u | tg);
+      double d = 0.0, ws = 0.0;   // rmsd_nofit (bestfit.F90:349-364)
+      for (int i = 0; i < s; ++i) {
+        const double dx = (double)out[i].x - ref_bf[3 * i], dy = (double)out[i].y - ref_bf[3 * i + 1];
+        const double dz = (double)out[i].z - ref_bf[3 * i + 2];
+        d += (double)ref_slt_w[i] * (dx * dx + dy * dy + dz * dz);
+        ws += ref_slt_w[i];
+      }
+      const double rmsd = sqrt(d / ws);
+      ok = !((double)lwreg > rmsd || rmsd > (double)upreg);
+    }
+    if (!ok) report(st, kErrInsRej, -1, cnt, 0.f);
+    if (insposition == ERMOD_INSPOS_GAUSS) insw[cnt] *= wfac;
+  } else if (insorient == ERMOD_INSROT_RANDOM) {
+    orient(1u);
   }
   finish_target(a, cnt, out, tgt_n + (size_t)cnt * s, tgt_c, qsite);
 }
 
-void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, int insposition,
-                   int insorient, float lwreg, float upreg, int use_conf, int gv, int learned, cudaStream_t s) {
-  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum_dev, iseed, insposition, insorient, lwreg, upreg,
-                                                    d.aggcen, use_conf, gv, learned,
-                                                    d.vcdf, d.vq, d.ins_voxel, d.insw_in, d.ins_conf,
-                                                    d.bfcoord, d.slt_mass, d.slt_q, d.tgt_raw, d.tgt_n, d.tgt_c);
+void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, const InsRegion& rg,
+                   int use_conf, int gv, int learned, cudaStream_t s) {
+  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum_dev, iseed, rg, d.aggcen, d.ref_bf, d.ref_slt_w, d.status,
+                                                    use_conf, gv, learned, d.vcdf, d.vq, d.ins_voxel, d.insw_in,
+                                                    d.ins_conf, d.bfcoord, d.slt_mass, d.slt_q, d.tgt_raw, d.tgt_n,
+                                                    d.tgt_c);
 }
 
 __global__ void k_targets_soln(FrameArgs a, const int* __restrict__ tgt_mol, const int* __restrict__ molbeg,

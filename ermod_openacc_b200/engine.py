@@ -123,6 +123,16 @@ class Engine:
                     minuv=mn, maxuv=mx, avslf=acc.avslf, engnorm=acc.engnorm, engsmpl=acc.engsmpl,
                     voffset=acc.voffset, voffset_initialized=acc.voffset_initialized)
 
+    def set_refstructure(self, refspec: int, host_crd, host_w, slt_crd, slt_w) -> int:
+        """RefInfo reference structure for insposition 5 / 6 (load_refstructure,
+        insertion.F90:676-770): the atoms of the refspec species (bit mask over uvspec) in
+        molecule order and the solute, with their fit weights."""
+        hc, hw, sc, sw = (A.as_f32(x) for x in (host_crd, host_w, slt_crd, slt_w))
+        self._ref = (hc, hw, sc, sw)
+        return self._check(self.lib.ermod_set_refstructure(self.ctx, int(refspec), len(hw), A.ptr(hc, C.c_float),
+                                                           A.ptr(hw, C.c_float), A.ptr(sc, C.c_float),
+                                                           A.ptr(sw, C.c_float)))
+
     def accum(self, ecorr: bool = True) -> dict:
         """Raw accumulators of the current division (engstore's inputs); ecorr=False leaves
         the ermax^2 correlation matrix on the device (its entry is None)."""

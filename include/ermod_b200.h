@@ -83,7 +83,9 @@ extern "C" {
 #define ERMOD_INSPOS_SPHERE   2   /* COM at the host aggregate centre + a point of the shell lwreg..upreg */
 #define ERMOD_INSPOS_SLAB_GENERIC   3   /* + cell . (u1, u2, dz / |c3|), lwreg < dz < upreg */
 #define ERMOD_INSPOS_SLAB_SYMMETRIC 4   /* the same with dz of either sign */
-/* insposition 5 (RMSD) and 6 (Gaussian) need the RefInfo reference structure: ERMOD_ERR_UNSUPPORTED */
+#define ERMOD_INSPOS_RMSD     5   /* translation within upreg + 3 r_max of the fitted reference, RMSD lwreg..upreg */
+#define ERMOD_INSPOS_GAUSS    6   /* uniform / Gaussian mixture around the fitted reference (experimental) */
+/* insposition 5 and 6 (insorigin 3) need ermod_set_refstructure before the first frame */
 #define ERMOD_INSROT_RANDOM   0
 #define ERMOD_INSROT_NOCHANGE 1
 
@@ -202,6 +204,23 @@ int32_t ermod_enginit_mesh(const ermod_hist* hist, int32_t numslv,
  */
 int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* params,
                      const ermod_topology* topo, const ermod_mesh* mesh);
+
+/*
+ * RefInfo reference structure (load_refstructure, erdst/insertion.F90:676-770)
+ * for insposition 5 (RMSD) and 6 (Gaussian): each frame, the reference host
+ * is fitted onto the frame's host atoms and the reference solute carried
+ * along (reffit, :646-673; fit_a_rotate_b, erdst/bestfit.F90:309-336); that
+ * best-fit solute is the insertion origin and the RMSD reference
+ * (check_solute_configuration :617-643, check_mol_configuration
+ * erdst/engproc.F90:1249-1269 for solutes in solution).
+ *   refspec   bit (sp - 1) set for each solvent species sp (uvspec) of the host
+ *   nhost     the atoms of the refspec molecules, in molecule order
+ *   host_crd  [3*nhost] their reference coordinates, host_w [nhost] fit weights
+ *   slt_crd   [3*s] the reference solute coordinates, slt_w [s] its weights
+ * Copies the arrays.  Call after ermod_create, before the first frame.
+ */
+int32_t ermod_set_refstructure(ermod_ctx* ctx, int32_t refspec, int32_t nhost, const float* host_crd,
+                               const float* host_w, const float* slt_crd, const float* slt_w);
 
 /* engclear (engproc.F90:321-340): zero the per-division accumulators. */
 int32_t ermod_engclear(ermod_ctx* ctx);

@@ -325,14 +325,12 @@ template <class T> struct Oracle {
     } else if (p.cltype != ERMOD_EL_COULOMB) {
       return fail(ERMOD_ERR_UNSUPPORTED, "set_prs");
     }
-    if (p.slttype != ERMOD_SLT_SOLN && !(p.insposition >= ERMOD_INSPOS_RANDOM &&
-                                         p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC))
+    if (!(p.insposition >= ERMOD_INSPOS_RANDOM && p.insposition <= ERMOD_INSPOS_GAUSS))
       return fail(ERMOD_ERR_UNSUPPORTED, "ins_geo");
-    if (p.slttype == ERMOD_SLT_SOLN && !(p.insposition >= ERMOD_INSPOS_RANDOM &&
-                                         p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC))
-      return fail(ERMOD_ERR_UNSUPPORTED, "ins_geo");
-    if (p.insposition >= ERMOD_INSPOS_SPHERE &&
+    if (p.insposition >= ERMOD_INSPOS_SPHERE && p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC &&
         !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f && p.hostspec != 0))
+      return fail(ERMOD_ERR_ARG, "ins_reg");
+    if (p.insposition >= ERMOD_INSPOS_RMSD && !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f))
       return fail(ERMOD_ERR_ARG, "ins_reg");
     return ERMOD_OK;
   }
@@ -716,10 +714,106 @@ template <class T> struct Oracle {
   }
   double aggcen[3] = {0.0, 0.0, 0.0};
 
+  // ---- RefInfo reference structure (insertion.F90:646-770, bestfit.F90:114-364) ----
+  std::vector<int> ref_atom;          // physical atoms of the refspec molecules, molecule order
+  std::vector<double> ref_host, ref_host_w, ref_slt, ref_slt_w, ref_bf;
+  bool gauss_init = false;
+  double gauss_l[3] = {0, 0, 0}, gauss_z0 = 0, gauss_z1 = 0;
+
+  int set_refstructure(int refspec, int nhost, const float* hc, const float* hw, const float* sc, const float* sw) {
+    ref_atom.clear();
+    for (int i = 0; i < nummol; ++i)
+      if (sluvid[i] == ERMOD_PT_SOLVENT && uvspec[i] >= 1 && uvspec[i] <= 31 && ((refspec >> (uvspec[i] - 1)) & 1))
+        for (int a = molbeg[i]; a < molbeg[i + 1]; ++a) ref_atom.push_back(a);
+    if ((int)ref_atom.size() != nhost) return fail(ERMOD_ERR_ARG, "ins_ref");
+    const int s = p.slttype == ERMOD_SLT_SOLN ? numsite[sltlist[0]] : nsite_slt;
+    ref_host.assign(hc, hc + 3 * nhost); ref_host_w.assign(hw, hw + nhost);
+    ref_slt.assign(sc, sc + 3 * s); ref_slt_w.assign(sw, sw + s);
+    ref_bf.assign(3 * s, 0.0);
+    return ERMOD_OK;
+  }
+
+  // Largest-eigenvalue eigenvector of a symmetric 4x4 matrix: cyclic Jacobi, the rotation
+  // angle from tan(2 phi) = 2 a_pq / (a_qq - a_pp), eigenvectors accumulated column-wise.
+  static void top_eigvec4(double a[4][4], double out[4]) {
+    double v[4][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+    for (int it = 0; it < 100; ++it) {
+      double off = 0;
+      for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) if (i != j) off += a[i][j] * a[i][j];
+      if (off < 1e-40) break;
+      for (int p0 = 0; p0 < 4; ++p0)
+        for (int q0 = p0 + 1; q0 < 4; ++q0) {
+          if (std::abs(a[p0][q0]) < 1e-300) continue;
+          const double phi = 0.5 * std::atan2(2 * a[p0][q0], a[q0][q0] - a[p0][p0]);
+          const double c = std::cos(phi), sn = std::sin(phi);
+          for (int k = 0; k < 4; ++k) {
+            const double x = a[k][p0], y = a[k][q0];
+            a[k][p0] = c * x - sn * y; a[k][q0] = sn * x + c * y;
+          }
+          for (int k = 0; k < 4; ++k) {
+            const double x = a[p0][k], y = a[q0][k];
+            a[p0][k] = c * x - sn * y; a[q0][k] = sn * x + c * y;
+          }
+          for (int k = 0; k < 4; ++k) {
+            const double x = v[k][p0], y = v[k][q0];
+            v[k][p0] = c * x - sn * y; v[k][q0] = sn * x + c * y;
+          }
+        }
+    }
+    int b = 0;
+    for (int i = 1; i < 4; ++i) if (a[i][i] > a[b][b]) b = i;
+    double n = 0;
+    for (int k = 0; k < 4; ++k) n += v[k][b] * v[k][b];
+    for (int k = 0; k < 4; ++k) out[k] = v[k][b] / std::sqrt(n);
+  }
+  // q (0, x) conj(q) as a rotation matrix applied to x
+  static void qrot(const double q[4], const double x[3], double r[3]) {
+    const double w = q[0], a = q[1], b = q[2], c = q[3];
+    const double R[3][3] = {{w * w + a * a - b * b - c * c, 2 * (a * b - w * c), 2 * (a * c + w * b)},
+                            {2 * (a * b + w * c), w * w - a * a + b * b - c * c, 2 * (b * c - w * a)},
+                            {2 * (a * c - w * b), 2 * (b * c + w * a), w * w - a * a - b * b + c * c}};
+    for (int i = 0; i < 3; ++i) r[i] = R[i][0] * x[0] + R[i][1] * x[1] + R[i][2] * x[2];
+  }
+  // fit_a_rotate_b: rotation of the centred `mov` onto the centred `ref` (Horn 1987), applied to
+  // the nb points b about mov's centre and placed at ref's centre
+  static void fit_rotate(int n, const double* ref, const double* mov, const double* w, int nb, const double* b,
+                         double* out) {
+    double cr[3] = {0, 0, 0}, cm[3] = {0, 0, 0}, ws = 0;
+    for (int i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) { cr[k] += w[i] * ref[3 * i + k]; cm[k] += w[i] * mov[3 * i + k]; }
+      ws += w[i];
+    }
+    for (int k = 0; k < 3; ++k) { cr[k] /= ws; cm[k] /= ws; }
+    double S[3][3] = {};
+    for (int i = 0; i < n; ++i)
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) S[r][c] += w[i] * (mov[3 * i + r] - cm[r]) * (ref[3 * i + c] - cr[c]);
+    double N[4][4] = {{S[0][0] + S[1][1] + S[2][2], S[1][2] - S[2][1], S[2][0] - S[0][2], S[0][1] - S[1][0]},
+                      {S[1][2] - S[2][1], S[0][0] - S[1][1] - S[2][2], S[0][1] + S[1][0], S[2][0] + S[0][2]},
+                      {S[2][0] - S[0][2], S[0][1] + S[1][0], -S[0][0] + S[1][1] - S[2][2], S[1][2] + S[2][1]},
+                      {S[0][1] - S[1][0], S[2][0] + S[0][2], S[1][2] + S[2][1], -S[0][0] - S[1][1] + S[2][2]}};
+    double q[4];
+    top_eigvec4(N, q);
+    for (int i = 0; i < nb; ++i) {
+      const double x[3] = {b[3 * i] - cm[0], b[3 * i + 1] - cm[1], b[3 * i + 2] - cm[2]};
+      double r[3];
+      qrot(q, x, r);
+      for (int k = 0; k < 3; ++k) out[3 * i + k] = r[k] + cr[k];
+    }
+  }
+  // reffit's host step: the reference host onto this frame's host atoms, carrying the reference solute
+  void reffit_frame(const float* sitepos) {
+    const int n = (int)ref_atom.size();
+    std::vector<double> cur(3 * (size_t)n);
+    for (int i = 0; i < n; ++i) for (int k = 0; k < 3; ++k) cur[3 * i + k] = sitepos[3 * ref_atom[i] + k];
+    fit_rotate(n, cur.data(), ref_host.data(), ref_host_w.data(), (int)ref_slt_w.size(), ref_slt.data(), ref_bf.data());
+    for (double& x : ref_bf) x = (double)(float)x;
+  }
+
   // instslt('proc') for insposition RANDOM/NOCHANGE/SPHERE/SLAB, insorient RANDOM/NOCHANGE
   // (insertion.F90:86-98, 100-200, 307-375; bestfit.F90:252-297; quaternion rotate
   // bestfit.F90:74-99).  Writes the nsite solute coordinates of insertion cnt.
-  void insert_one(int stnum, int cnt, const T* conf, T* out) const {
+  void insert_one(int stnum, int cnt, const T* conf, T* out) {
     const int s = nsite_slt;
     const int ab = molbeg[nummol - 1];
     for (int i = 0; i < 3 * s; ++i) out[i] = conf[i];
@@ -778,13 +872,34 @@ template <class T> struct Oracle {
       }
       for (int a = 0; a < s; ++a) for (int k = 0; k < 3; ++k) out[3 * a + k] += sh[k];
     }
+    if (p.insposition == ERMOD_INSPOS_RMSD || p.insposition == ERMOD_INSPOS_GAUSS) {
+      insert_refstr(stnum, cnt, conf, out);
+      return;
+    }
+    orient(stnum, cnt, 1u, out);
+  }
+
+  // apply_orientation (insertion.F90:348-369) with the counters (cnt, stnum, attempt, tag)
+  void orient(int stnum, int cnt, uint32_t tag, T* out) const {
+    const int s = nsite_slt;
+    const int ab = molbeg[nummol - 1];
+    auto com_of = [&](T c[3]) {
+      T msum = 0;
+      for (int a = 0; a < s; ++a) msum += sitemass[ab + a];
+      for (int k = 0; k < 3; ++k) {
+        T acc = 0;
+        for (int a = 0; a < s; ++a) acc += out[3 * a + k] * sitemass[ab + a];
+        c[k] = acc / msum;
+      }
+    };
+    const uint32_t key[2] = {(uint32_t)p.iseed, kStreamTag};
     if (p.insorient == ERMOD_INSROT_RANDOM) {
       T c[3];
       com_of(c);
       for (int a = 0; a < s; ++a) for (int k = 0; k < 3; ++k) out[3 * a + k] -= c[k];
       T q[4] = {T(1), T(0), T(0), T(0)};
       for (uint32_t att = 1; att <= 64; ++att) {
-        uint32_t ctr[4] = {(uint32_t)cnt, (uint32_t)stnum, att, 1u}, r4[4];
+        uint32_t ctr[4] = {(uint32_t)cnt, (uint32_t)stnum, att, tag}, r4[4];
         philox4x32_10(ctr, key, r4);
         T t[4], n2 = 0;
         for (int i = 0; i < 4; ++i) { t[i] = (T)u01(r4[i]) * T(2) - T(1); n2 += t[i] * t[i]; }
@@ -810,6 +925,82 @@ template <class T> struct Oracle {
       }
     }
   }
+
+  // insorigin 3 (insertion.F90:86-94, 131-304, 617-643): fit the conformation onto this frame's best-fit
+  // reference solute, shift (RMSD: uniform in a cube of half width upreg + 3 r_max; Gaussian: the
+  // uniform / Gaussian mixture, weight divided by its density), orient, and retry until the RMSD to
+  // the best-fit reference lies in lwreg..upreg (kInsTries attempts).
+  void insert_refstr(int stnum, int cnt, const T* conf, T* out) {
+    const int s = nsite_slt;
+    const int ab = molbeg[nummol - 1];
+    const uint32_t key[2] = {(uint32_t)p.iseed, kStreamTag};
+    std::vector<double> cf(3 * s), fo(3 * s);
+    for (int i = 0; i < 3 * s; ++i) cf[i] = (double)conf[i];
+    double wfac = 1.0;
+    bool ok = false;
+    for (int tr = 0; tr < kInsTries && !ok; ++tr) {
+      const uint32_t tg = (uint32_t)tr << 8;
+      fit_rotate(s, ref_bf.data(), cf.data(), ref_slt_w.data(), s, cf.data(), fo.data());
+      for (int i = 0; i < 3 * s; ++i) out[i] = (T)(float)fo[i];
+      T sh[3];
+      if (p.insposition == ERMOD_INSPOS_RMSD) {
+        T msum = 0, c[3] = {0, 0, 0};
+        for (int a = 0; a < s; ++a) msum += sitemass[ab + a];
+        for (int k = 0; k < 3; ++k) {
+          for (int a = 0; a < s; ++a) c[k] += out[3 * a + k] * sitemass[ab + a];
+          c[k] /= msum;
+        }
+        T maxd = 0;
+        for (int a = 0; a < s; ++a) {
+          T d2 = 0;
+          for (int k = 0; k < 3; ++k) d2 += (out[3 * a + k] - c[k]) * (out[3 * a + k] - c[k]);
+          maxd = std::max(maxd, d2);
+        }
+        const T movmax = (T)p.upreg + T(3) * std::sqrt(maxd);
+        uint32_t ctr[4] = {(uint32_t)cnt, (uint32_t)stnum, tg, 3u}, r4[4];
+        philox4x32_10(ctr, key, r4);
+        for (int k = 0; k < 3; ++k) sh[k] = movmax * (T(2) * (T)u01(r4[k]) - T(1));
+      } else {
+        T sc[3];
+        if (((cnt + tr) & 1) == 0) {
+          uint32_t ctr[4] = {(uint32_t)cnt, (uint32_t)stnum, tg, 4u}, r4[4];
+          philox4x32_10(ctr, key, r4);
+          for (int k = 0; k < 3; ++k) sc[k] = (T(2) * (T)u01(r4[k]) - T(1)) * (T)gauss_l[k];
+        } else {
+          for (int k = 0; k < 3; ++k) {
+            sc[k] = 0;
+            for (uint32_t att = 1; att <= 64; ++att) {
+              uint32_t ctr[4] = {(uint32_t)cnt, (uint32_t)stnum, tg | att, 5u + (uint32_t)k}, r4[4];
+              philox4x32_10(ctr, key, r4);
+              const double u1 = std::max((double)u01(r4[0]), 1.0e-7), u2 = (double)u01(r4[1]);
+              const double r = std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * kPi * u2) * std::sqrt(0.5);
+              if (std::abs(r) < gauss_l[k]) { sc[k] = (T)r; break; }
+            }
+          }
+        }
+        const T sq = sc[0] * sc[0] + sc[1] * sc[1] + sc[2] * sc[2];
+        wfac /= 0.5 / gauss_z0 + 0.5 * std::exp(-(double)sq) / gauss_z1;
+        T f[3];
+        for (int k = 0; k < 3; ++k) f[k] = sc[k] / (T(2) * (T)gauss_l[k]);
+        for (int k = 0; k < 3; ++k) sh[k] = cell[k][0] * f[0] + cell[k][1] * f[1] + cell[k][2] * f[2];
+      }
+      for (int a = 0; a < s; ++a) for (int k = 0; k < 3; ++k) out[3 * a + k] += sh[k];
+      orient(stnum, cnt, 1u | tg, out);
+      double d = 0, ws = 0;
+      for (int a = 0; a < s; ++a) {
+        double t = 0;
+        for (int k = 0; k < 3; ++k) t += ((double)out[3 * a + k] - ref_bf[3 * a + k]) * ((double)out[3 * a + k] - ref_bf[3 * a + k]);
+        d += ref_slt_w[a] * t;
+        ws += ref_slt_w[a];
+      }
+      const double rmsd = std::sqrt(d / ws);
+      ok = !((double)p.lwreg > rmsd || rmsd > (double)p.upreg);
+    }
+    if (!ok) ins_rejected[cnt] = 1;
+    if (p.insposition == ERMOD_INSPOS_GAUSS) insw[cnt] *= wfac;
+  }
+  std::vector<char> ins_rejected;
+  static constexpr int kInsTries = 1024;
 
   // binsearch + getiduv (engproc.F90:1078-1171).  Returns 0-based bin or <0 error.
   int getiduv(int pti, double engval, int* warn) {
@@ -921,7 +1112,26 @@ template <class T> struct Oracle {
       if ((p.insposition == ERMOD_INSPOS_RANDOM || p.insposition == ERMOD_INSPOS_SLAB_GENERIC ||
            p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) && p.boxshp == ERMOD_SYS_NONPERIODIC)
         return fail(ERMOD_ERR_INS_GEO, "ins_geo");
-      if (p.insposition >= ERMOD_INSPOS_SPHERE) aggregate_center(sitepos);
+      if (p.insposition >= ERMOD_INSPOS_SPHERE && p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC)
+        aggregate_center(sitepos);
+      if (p.insposition >= ERMOD_INSPOS_RMSD) {
+        if (ref_atom.empty()) return fail(ERMOD_ERR_ARG, "ins_ref");
+        reffit_frame(sitepos);
+        if (p.insposition == ERMOD_INSPOS_GAUSS && !gauss_init) {   // insertion.F90:268-274, first call
+          gauss_z0 = 8.0; gauss_z1 = std::pow(kPi, 1.5);
+          for (int k = 0; k < 3; ++k) {
+            const double len = std::sqrt((double)cell[0][k] * cell[0][k] + (double)cell[1][k] * cell[1][k] +
+                                         (double)cell[2][k] * cell[2][k]);
+            gauss_l[k] = (double)(float)(0.5 * len / p.upreg);
+            gauss_z0 *= gauss_l[k];
+            gauss_z1 *= std::erf(gauss_l[k]);
+          }
+          gauss_z0 = (double)(float)gauss_z0; gauss_z1 = (double)(float)gauss_z1;
+          gauss_init = true;
+        }
+      }
+      if (ins_weight) for (int c = 0; c < maxdst; ++c) insw[c] = ins_weight[c];
+      ins_rejected.assign(maxdst, 0);
       std::vector<T> conf(3 * s);
 #pragma omp parallel for num_threads(nthreads) firstprivate(conf) schedule(static)
       for (int cnt = 0; cnt < maxdst; ++cnt) {
@@ -929,12 +1139,32 @@ template <class T> struct Oracle {
         for (int i = 0; i < 3 * s; ++i) conf[i] = src ? (T)src[i] : bfcoord[i];
         insert_one(stnum, cnt, conf.data(), &pos[3 * ((size_t)numatm_phys + (size_t)cnt * s)]);
       }
-      if (ins_weight) for (int c = 0; c < maxdst; ++c) insw[c] = ins_weight[c];
+      for (int c = 0; c < maxdst; ++c) if (ins_rejected[c]) return fail(ERMOD_ERR_INS_GEO, "ins_rej");
     }
     // soln: check_mol_configuration (engproc.F90:1197-1324) for sphere / slab regions;
     // a rejected solute gets no energies and no update_histogram (:447-450, 754-755)
     std::vector<char> skip(maxdst, 0);
-    if (!refs && p.insposition >= ERMOD_INSPOS_SPHERE) {
+    if (!refs && p.insposition == ERMOD_INSPOS_RMSD) {   // engproc.F90:1249-1269
+      if (ref_atom.empty()) return fail(ERMOD_ERR_ARG, "ins_ref");
+      reffit_frame(sitepos);
+      const int ns = (int)ref_slt_w.size();
+      for (int cnt = 0; cnt < maxdst; ++cnt) {
+        const int a0 = molbeg[sltlist[cnt]];
+        double d = 0, ws = 0;
+        for (int a = 0; a < ns; ++a) {
+          double t = 0;
+          for (int k = 0; k < 3; ++k) {
+            const double x = (double)sitepos[3 * (a0 + a) + k] - ref_bf[3 * a + k];
+            t += x * x;
+          }
+          d += ref_slt_w[a] * t;
+          ws += ref_slt_w[a];
+        }
+        const double rmsd = std::sqrt(d / ws);
+        skip[cnt] = ((double)p.lwreg > rmsd || rmsd > (double)p.upreg) ? 1 : 0;
+      }
+    }
+    if (!refs && p.insposition >= ERMOD_INSPOS_SPHERE && p.insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC) {
       const bool slab = p.insposition != ERMOD_INSPOS_SPHERE;
       if (slab && p.boxshp == ERMOD_SYS_NONPERIODIC) return fail(ERMOD_ERR_INS_GEO, "eng_slb");
       aggregate_center(sitepos);
@@ -1241,6 +1471,19 @@ void orc_get_engfac(void* hv, double* out) {
   Handle* h = (Handle*)hv;
   if (h->d) { for (size_t i = 0; i < h->d->engfac.size(); ++i) out[i] = h->d->engfac[i]; }
   else { for (size_t i = 0; i < h->f->engfac.size(); ++i) out[i] = h->f->engfac[i]; }
+}
+
+void orc_get_insw(void* hv, double* w) {
+  Handle* h = (Handle*)hv;
+  const std::vector<double>& v = h->d ? h->d->insw : h->f->insw;
+  std::memcpy(w, v.data(), sizeof(double) * v.size());
+}
+
+int orc_set_refstructure(void* hv, int refspec, int nhost, const float* hc, const float* hw, const float* sc,
+                         const float* sw) {
+  Handle* h = (Handle*)hv;
+  return h->d ? h->d->set_refstructure(refspec, nhost, hc, hw, sc, sw)
+              : h->f->set_refstructure(refspec, nhost, hc, hw, sc, sw);
 }
 
 const char* orc_last_error(void* hv) {

@@ -56,6 +56,9 @@ def lib():
         L.orc_get_engfac.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.orc_last_error.restype = C.c_char_p
         L.orc_last_error.argtypes = [C.c_void_p]
+        L.orc_get_insw.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.orc_set_refstructure.restype = C.c_int
+        L.orc_set_refstructure.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.POINTER(C.c_float)] * 4
         _lib = L
     return _lib
 
@@ -126,6 +129,15 @@ class Oracle:
             self.L.orc_destroy(self.h)
             self.h = None
 
+    def set_refstructure(self, refspec, host_crd, host_w, slt_crd, slt_w):
+        hc, hw, sc, sw = (A.as_f32(x) for x in (host_crd, host_w, slt_crd, slt_w))
+        self._ref = (hc, hw, sc, sw)
+        rc = self.L.orc_set_refstructure(self.h, int(refspec), len(hw), A.ptr(hc, C.c_float), A.ptr(hw, C.c_float),
+                                         A.ptr(sc, C.c_float), A.ptr(sw, C.c_float))
+        if rc != 0:
+            raise RuntimeError(f"oracle set_refstructure failed {rc} {self.L.orc_last_error(self.h).decode()}")
+        return rc
+
     def engclear(self):
         self.L.orc_engclear(self.h)
 
@@ -153,6 +165,11 @@ class Oracle:
         o = np.zeros(3 * self.nsite_slt * self.maxdst, dtype=np.float32)
         self.L.orc_get_insertions(self.h, A.ptr(o, C.c_float))
         return o
+
+    def insertion_weights(self):
+        w = np.zeros(self.maxdst)
+        self.L.orc_get_insw(self.h, A.ptr(w, C.c_double))
+        return w
 
     def engfac(self):
         K1, K2, K3 = self.params["ms1max"], self.params["ms2max"], self.params["ms3max"]

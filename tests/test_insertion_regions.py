@@ -131,3 +131,94 @@ def test_soln_configuration_check(oracle_mod, insposition, lw, up, expect):
     assert a["engsmpl"] == kept.sum()
     # each kept solute bins every other molecule once, with the same weight (neutral solutes)
     assert a["edens"].sum() == pytest.approx(a["engnorm"] * (u.shape[1] - 1), rel=1e-9, abs=1e-12)
+
+
+# ---- RMSD / Gaussian insertion against the RefInfo structure (insorigin 3) ----
+def _rot(axis, ang):
+    axis = np.asarray(axis, dtype=np.float64) / np.linalg.norm(axis)
+    K = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+    return np.eye(3) + np.sin(ang) * K + (1 - np.cos(ang)) * K @ K
+
+
+def refinfo_case(maxins=256):
+    """The C2 small workload with a RefInfo whose host is this frame's water moved by a known rigid
+    motion M, and whose solute is M applied to a known placement slt0 of the ring: reffit must
+    carry the reference solute back onto slt0."""
+    w = S.make_workload(2, small=True, maxins=maxins)
+    pos, cell = w.frame(0)
+    xyz = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    R, t = _rot([1.0, 2.0, -0.5], 0.7), np.array([3.0, -4.0, 1.5])
+    host_ref = xyz @ R.T + t
+    s = int(w.topo.numsite[-1])
+    bf = np.asarray(w.topo.bfcoord, dtype=np.float64).reshape(s, 3)
+    slt0 = bf - bf.mean(axis=0) + np.array([12.0, 13.0, 11.0])
+    slt_ref = slt0 @ R.T + t
+    ref = dict(refspec=1, host_crd=host_ref.ravel(), host_w=np.ones(len(xyz)), slt_crd=slt_ref.ravel(),
+               slt_w=np.ones(s))
+    return w, pos, cell, ref, slt0
+
+
+def _rmsd(a, b):
+    return np.sqrt(((a - b) ** 2).sum(axis=-1).mean(axis=-1))
+
+
+@pytest.mark.parametrize("insorient", [A.INSROT_NOCHANGE, A.INSROT_RANDOM])
+def test_rmsd_insertion_window(oracle_mod, insorient):
+    w, pos, cell, ref, slt0 = refinfo_case()
+    lw, up = 1.0, 4.0
+    prm = dict(w.params, insposition=A.INSPOS_RMSD, insorient=insorient, lwreg=lw, upreg=up, corrcal=0)
+    orc = oracle_mod.Oracle(prm, w.topo, w.hist)
+    orc.set_refstructure(**ref)
+    assert orc.engconst(1, pos, cell) >= 0
+    s = slt0.shape[0]
+    ins = np.asarray(orc.insertions(), dtype=np.float64).reshape(-1, s, 3)
+    r = _rmsd(ins, slt0[None])
+    assert r.min() >= lw - 1e-3 and r.max() <= up + 1e-3
+    if insorient == A.INSROT_NOCHANGE:   # a pure translation of the fitted reference: rigid copies of slt0
+        rel = ins - ins.mean(axis=1, keepdims=True)
+        np.testing.assert_allclose(rel, np.broadcast_to(slt0 - slt0.mean(axis=0), rel.shape), atol=2e-4)
+    assert np.all(orc.insertion_weights() == 1.0)
+
+
+def test_gaussian_insertion_weights(oracle_mod):
+    """Mixture of uniform and Gaussian displacements: each weight is 1/q of the mixture density, so
+    with every first try accepted (a wide RMSD window) the weights average z0 = 8 l1 l2 l3."""
+    w, pos, cell, ref, slt0 = refinfo_case(maxins=4000)
+    up = 40.0
+    prm = dict(w.params, insposition=A.INSPOS_GAUSS, lwreg=0.0, upreg=up, corrcal=0)
+    orc = oracle_mod.Oracle(prm, w.topo, w.hist)
+    orc.set_refstructure(**ref)
+    assert orc.engconst(1, pos, cell) >= 0
+    wt = orc.insertion_weights()
+    L = np.linalg.norm(np.asarray(cell, dtype=np.float64).reshape(3, 3), axis=0)
+    l = (L / 2) / up
+    assert np.all(np.isfinite(wt)) and np.all(wt > 0)
+    assert abs(wt.mean() / (8 * np.prod(l)) - 1.0) < 0.1
+
+
+def test_soln_rmsd_check(oracle_mod):
+    """Solutes in solution with insposition 5: kept when their RMSD to the best-fit reference
+    solute lies in lwreg..upreg (engproc.F90:1249-1269)."""
+    from _helpers import soln_multi_system
+    prm, topo, hist, pos, cell, offs = soln_multi_system()
+    xyz = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    nslt = len(offs)
+    water = xyz[nslt:]
+    R, t = _rot([0.3, -1.0, 0.2], 1.1), np.array([-2.0, 1.0, 5.0])
+    ref = dict(refspec=2, host_crd=(water @ R.T + t).ravel(), host_w=np.ones(len(water)),
+               slt_crd=(xyz[1:2] @ R.T + t).ravel(), slt_w=np.ones(1))
+    prm = dict(prm, insposition=A.INSPOS_RMSD, lwreg=0.0, upreg=1.0, keep_uvengy=1)
+    orc = oracle_mod.Oracle(prm, topo, hist)
+    orc.set_refstructure(**ref)
+    assert orc.engconst(1, pos, cell) >= 0
+    u, _ = orc.uvengy()
+    np.testing.assert_array_equal(np.any(u != 0.0, axis=1), [False, True, False, False])
+    assert orc.accum()["engsmpl"] == 1
+
+
+def test_refstructure_is_required(oracle_mod):
+    w = S.make_workload(2, small=True, maxins=8)
+    prm = dict(w.params, insposition=A.INSPOS_RMSD, lwreg=0.0, upreg=4.0)
+    orc = oracle_mod.Oracle(prm, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    assert orc.engconst(1, pos, cell) < 0

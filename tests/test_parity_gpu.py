@@ -138,6 +138,48 @@ def test_soln_configuration_check_matches_oracle(lib, oracle_mod, insposition, l
     np.testing.assert_allclose(a["edens"], b["edens"], rtol=1e-9, atol=1e-9 * max(1.0, b["engnorm"]))
 
 
+@pytest.mark.parametrize("insposition,lw,up", [(A.INSPOS_RMSD, 1.0, 4.0), (A.INSPOS_GAUSS, 0.0, 40.0)])
+def test_refstr_insertion_matches_oracle(lib, oracle_mod, insposition, lw, up):
+    """RMSD and Gaussian insertion (insorigin 3): the GPU's per-frame reference fit, per-insertion
+    conformation fit, shifts, orientations, RMSD window and Gaussian weights against the oracle."""
+    from test_insertion_regions import refinfo_case
+    w, pos, cell, ref, _ = refinfo_case(maxins=64)
+    prm = dict(w.params, insposition=insposition, lwreg=lw, upreg=up)
+    eng = Engine(prm, w.topo, w.hist)
+    orc = oracle_mod.Oracle(prm, w.topo, w.hist)
+    eng.set_refstructure(**ref)
+    orc.set_refstructure(**ref)
+    for fr in range(2):
+        assert eng.engconst(fr + 1, pos, cell) >= 0
+        assert orc.engconst(fr + 1, pos, cell) >= 0
+        ins, wts = eng.insertions()
+        np.testing.assert_allclose(ins, orc.insertions(), atol=5e-5)
+        np.testing.assert_allclose(wts, orc.insertion_weights(), rtol=2e-5)
+
+
+def test_soln_rmsd_check_matches_oracle(lib, oracle_mod):
+    from _helpers import soln_multi_system
+    from test_insertion_regions import _rot
+    prm, topo, hist, pos, cell, offs = soln_multi_system()
+    xyz = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    water = xyz[len(offs):]
+    R, t = _rot([0.3, -1.0, 0.2], 1.1), np.array([-2.0, 1.0, 5.0])
+    ref = dict(refspec=2, host_crd=(water @ R.T + t).ravel(), host_w=np.ones(len(water)),
+               slt_crd=(xyz[1:2] @ R.T + t).ravel(), slt_w=np.ones(1))
+    prm = dict(prm, insposition=A.INSPOS_RMSD, lwreg=0.0, upreg=1.0, keep_uvengy=1)
+    eng = Engine(prm, topo, hist)
+    orc = oracle_mod.Oracle(prm, topo, hist)
+    eng.set_refstructure(**ref)
+    orc.set_refstructure(**ref)
+    assert eng.engconst(1, pos, cell) >= 0
+    assert orc.engconst(1, pos, cell) >= 0
+    u, _ = eng.uvengy()
+    uo, _ = orc.uvengy()
+    np.testing.assert_array_equal(np.any(u != 0.0, axis=1), [False, True, False, False])
+    check_energies(u, uo)
+    assert eng.accum()["engsmpl"] == orc.accum()["engsmpl"] == 1
+
+
 def test_slab_insertion_needs_a_periodic_cell(lib):
     w = S.make_workload(2, small=True, maxins=8)
     prm = dict(w.params, insposition=A.INSPOS_SLAB_SYMMETRIC, lwreg=1.0, upreg=3.0, hostspec=1,
