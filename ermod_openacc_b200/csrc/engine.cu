@@ -68,6 +68,7 @@ struct ermod_ctx {
   int nref = 0;                       // atoms of the RefInfo host (insposition 5, 6)
   bool gauss_init = false;            // Gaussian insertion constants fixed at the first frame
   float gauss_l[3] = {0.f, 0.f, 0.f}, gauss_z0 = 0.f, gauss_z1 = 0.f;
+  PppmGreen pppm{};                   // PPPM influence function inputs (cltype 3)
   cufftHandle r2c = 0, c2r = 0;
   bool plans = false;
   void* tc_work = nullptr;
@@ -269,9 +270,12 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     *out = ctx;
     return code;
   };
-  if (p.cltype != ERMOD_EL_PME && p.cltype != ERMOD_EL_COULOMB) return bad(ERMOD_ERR_UNSUPPORTED, "set_prs");
-  if (p.cltype == ERMOD_EL_PME && (p.splodr < 2 || p.splodr > kMaxOrder)) return bad(ERMOD_ERR_ARG, "set_ewa");
-  if (p.cltype == ERMOD_EL_PME &&
+  const bool mesh = p.cltype == ERMOD_EL_PME || p.cltype == ERMOD_EL_PPPM;
+  if (!mesh && p.cltype != ERMOD_EL_COULOMB) return bad(ERMOD_ERR_UNSUPPORTED, "set_prs");
+  if (mesh && (p.splodr < 2 || p.splodr > kMaxOrder)) return bad(ERMOD_ERR_ARG, "set_ewa");
+  // recpcal.F90:250-251: the PPPM denominator needs an even order
+  if (p.cltype == ERMOD_EL_PPPM && p.splodr % 2 != 0) return bad(ERMOD_ERR_ARG, "pppm_odr");
+  if (mesh &&
       (p.ms1max < p.splodr || p.ms2max < p.splodr || p.ms3max < p.splodr || p.ms1max > kMaxGrid ||
        p.ms2max > kMaxGrid || p.ms3max > kMaxGrid))
     return bad(ERMOD_ERR_ARG, "set_ewa");
@@ -389,7 +393,7 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   // engine shape
   ctx->chunk = kChunk;
   const int K1 = p.ms1max, K2 = p.ms2max, K3 = p.ms3max, Kh1 = K1 / 2 + 1;
-  const bool pme = p.cltype == ERMOD_EL_PME;
+  const bool pme = mesh;   // smooth PME and PPPM share the whole pipeline but the influence function
   ctx->batch = p.ecorr_batch > 0 ? p.ecorr_batch : 4096;
   ctx->batch = std::max(ctx->chunk, (ctx->batch + ctx->chunk - 1) / ctx->chunk * ctx->chunk);
   ctx->batch = std::min(ctx->batch, (ctx->maxdst + ctx->chunk - 1) / ctx->chunk * ctx->chunk);
@@ -536,6 +540,24 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     spline_axis(K3, p.splodr, sf.data() + K1 + K2);
     CK(h2d(d.splfc, sf.data(), K1 + K2 + K3, st));
   }
+  if (p.cltype == ERMOD_EL_PPPM) {
+    // calc_gfb_pppm (recpcal.F90:179-198): the alias sum of the order-P assignment function
+    // is a polynomial of degree P-1 in sin^2(k h / 2); the reference's recurrence for its
+    // coefficients, then the division by (2P-1)!
+    PppmGreen& pg = ctx->pppm;
+    pg.on = 1;
+    const int P = p.splodr;
+    for (int l = 0; l < kMaxOrder; ++l) pg.gfb[l] = 0.0;
+    pg.gfb[0] = 1.0;
+    for (int m = 1; m < P; ++m) {
+      for (int l = m; l >= 1; --l)
+        pg.gfb[l] = 4.0 * (pg.gfb[l] * (l - m) * (l - m - 0.5) - pg.gfb[l - 1] * (l - m - 1) * (l - m - 1));
+      pg.gfb[0] = 4.0 * pg.gfb[0] * m * (m + 0.5);
+    }
+    double fact = 1.0;
+    for (int i = 2; i <= 2 * P - 1; ++i) fact *= i;
+    for (int l = 0; l < P; ++l) pg.gfb[l] /= fact;
+  }
   if (pme && ctx->spath == 1) {
     int n[3] = {K3, K2, K1};
     int inR[3] = {K3, K2, K1}, onC[3] = {K3, K2, Kh1};
@@ -649,7 +671,7 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
   std::memset(&ph, 0, sizeof(ph));
   FramePlan& fp = ph.k;
   const bool refs = p.slttype != ERMOD_SLT_SOLN;
-  const bool pme = p.cltype == ERMOD_EL_PME;
+  const bool pme = p.cltype == ERMOD_EL_PME || p.cltype == ERMOD_EL_PPPM;
   const int K1 = p.ms1max, K2 = p.ms2max, K3 = p.ms3max;
   // ---- cell (engproc.F90:1049-1070, realcal.F90:776-896) ----
   double c[3][3];
@@ -810,6 +832,18 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
     bool changed = !ctx->pme_init;
     for (int i = 0; i < 9; ++i) if (ctx->prevcl[i] != cellin[i]) changed = true;
     ph.engfac = changed;
+    if (changed && ctx->pppm.on) {
+      // alias range (recpcal.F90:230-233, 243-244): LAMMPS's accuracy form with EPS_HOC = 1e-7
+      // per mesh axis, projected on each cell vector, in single precision and truncated
+      const float acc = std::pow(-std::log(1.0e-7f), 0.25f);
+      const float pi = (float)kPi;
+      const float mm[3] = {p.screen / (pi * (float)K1) * acc, p.screen / (pi * (float)K2) * acc,
+                           p.screen / (pi * (float)K3) * acc};
+      for (int j = 0; j < 3; ++j) {
+        ctx->pppm.mmax[j] = (int)(cf[0][j] * mm[0] + cf[1][j] * mm[1] + cf[2][j] * mm[2]);
+        if (ctx->pppm.mmax[j] < 0) return set_error(ctx, ERMOD_ERR_ARG, "pppm_mrg");
+      }
+    }
   }
   // ---- real-space self term: per insertion, or once for a rigid solute ----
   const bool rigid = p.slttype == ERMOD_SLT_REFS_RIGID;
@@ -1085,7 +1119,7 @@ static int engconst_run(ermod_ctx* ctx, int stnum, const float* cellin, float ws
   cudaStream_t st = ctx->st;
   ctx->h_frame[0] = stnum;
   CK(cudaMemcpyAsync(ctx->d.frame_i, ctx->h_frame, sizeof(int), cudaMemcpyHostToDevice, st));
-  if (ph.engfac) launch_engfac(ph.k.a, ctx->d, ph.inv, ph.vold, (double)ctx->p.screen, st);
+  if (ph.engfac) launch_engfac(ph.k.a, ctx->d, ph.inv, ph.vold, (double)ctx->p.screen, ctx->pppm, st);
   const bool timed = ctx->p.stage_timing != 0;
   const bool graph = !timed && ctx->p.graph_mode == 0 && ctx->real_threads != 0;
   float total = 0.f;
@@ -1277,7 +1311,7 @@ static int batch_run(ermod_batch* b, int stnum, const float* cell, float wsys) {
     if (cudaMemcpyAsync(ctx->d.frame_i, ctx->h_frame, sizeof(int), cudaMemcpyHostToDevice, b->st) != cudaSuccess)
       return ERMOD_ERR_CUDA;
     launch_fill(ctx->d.insw_in, 1.0f, ctx->maxdst, b->st);
-    if (ph[i].engfac) launch_engfac(ph[i].k.a, ctx->d, ph[i].inv, ph[i].vold, (double)ctx->p.screen, b->st);
+    if (ph[i].engfac) launch_engfac(ph[i].k.a, ctx->d, ph[i].inv, ph[i].vold, (double)ctx->p.screen, ctx->pppm, b->st);
   }
   if (cudaEventRecord(b->t0, b->st) != cudaSuccess) return ERMOD_ERR_CUDA;
   if (!tuned) {
@@ -1535,7 +1569,7 @@ int32_t ermod_get_insertion_samples(ermod_ctx* ctx, float* features, double* eto
 
 int32_t ermod_get_paths(const ermod_ctx* ctx, int32_t* spectrum_path, int32_t* ecorr_path) {
   if (!ctx) return ERMOD_ERR_ARG;
-  if (spectrum_path) *spectrum_path = ctx->p.cltype == ERMOD_EL_PME ? ctx->spath : 0;
+  if (spectrum_path) *spectrum_path = (ctx->p.cltype == ERMOD_EL_PME || ctx->p.cltype == ERMOD_EL_PPPM) ? ctx->spath : 0;
   if (ecorr_path) *ecorr_path = ctx->p.corrcal ? (ctx->use_tc ? 0 : 1) : -1;
   return ERMOD_OK;
 }

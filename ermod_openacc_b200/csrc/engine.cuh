@@ -204,8 +204,16 @@ void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int co
 void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, int threads, cudaStream_t s);
 int setup_real_smem(const FrameArgs& a);
 void launch_fill(float* p, float v, int n, cudaStream_t s);
+// Inputs of the PPPM optimal influence function (recpcal.F90:179-337): the alias sums run
+// over |n_i| <= mmax[i]; gfb[l] are the coefficients of the order-P assignment function's
+// alias sum as a polynomial in sin^2(k h / 2).  on = 0 selects the smooth-PME function.
+struct PppmGreen {
+  int on;
+  int mmax[3];
+  double gfb[kMaxOrder];
+};
 void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[3][3], double volume,
-                   double screen, cudaStream_t s);
+                   double screen, const PppmGreen& pg, cudaStream_t s);
 void launch_spread(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, cudaStream_t s);
 int setup_spread_smem();
 void launch_transpose_phi(const FrameArgs& a, const DeviceState& d, cudaStream_t s);

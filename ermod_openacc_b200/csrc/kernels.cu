@@ -9,6 +9,7 @@
 //   k_selfreal         realcal_self(_refs) in FP64 (realcal.F90:669-771)
 //   k_real             realcal_refs / realcal_soln / realcal_bare (realcal.F90:51-666)
 //   k_engfac           recpcal_spline_greenfunc (recpcal.F90:121-163)
+//   k_engfac_pppm      recpcal_pppm_greenfunc (recpcal.F90:179-337)
 //   k_spread           charge spreading of recpcal_prepare_solute(_refs) (recpcal.F90:380-399, 453-473)
 //   k_influence        self energy + influence multiply (recpcal.F90:482-497)
 //   k_gather_bin       recpcal_energy_refs/soln (recpcal.F90:592-710) + residual_ene(_refs)
@@ -908,13 +909,80 @@ __global__ void k_engfac(int K1, int K2, int K3, int Kh1, int order, Mat3d invcl
   if (engfacT) engfacT[((size_t)r1 * K3 + r3) * K2 + r2] = (float)factor;   // [k1][k3][k2] for k_pme_plane
 }
 
+// recpcal_pppm_greenfunc (recpcal.F90:217-337): Hockney and Eastwood's optimal influence
+// function for the order-P B-spline assignment.  A thread per half-spectrum point sums, over
+// the aliases k_n = k + 2 pi invcl^T (n1 K1, n2 K2, n3 K3) with |n_i| <= mmax[i],
+// (k . k_n) exp(-|k_n|^2 / 4 screen^2) U^2(k_n) / |k_n|^2, U^2 = prod_i (sin t_i / t_i)^(2P),
+// t_i = pi (m_i / K_i + n_i), and divides by k^2, the squared product of the axes' alias
+// polynomials sum_l gfb[l] sin^2(pi m_i / K_i)^l and the volume, times 4 pi.  The third
+// alias offset is n3 K3 (the reference's :311 uses K2 there).  FP64, stored as FP32 in the
+// same two layouts as the smooth-PME function.
+__global__ void k_engfac_pppm(int K1, int K2, int K3, int Kh1, int order, Mat3d invcl, double volume,
+                              double screen, PppmGreen pg, float* __restrict__ engfac,
+                              float* __restrict__ engfacT) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = K3 * K2 * Kh1;
+  if (i >= n) return;
+  const int r1 = i % Kh1, r2 = (i / Kh1) % K2, r3 = i / (Kh1 * K2);
+  double factor = 0.0;
+  if (!(r1 == 0 && r2 == 0 && r3 == 0)) {
+    const int rc[3] = {r1, r2, r3}, K[3] = {K1, K2, K3};
+    double inm[3], den = 1.0;
+    for (int m = 0; m < 3; ++m) {
+      inm[m] = rc[m] <= K[m] / 2 ? (double)rc[m] : (double)(rc[m] - K[m]);
+      const double sn = sin(kPi * inm[m] / K[m]), z = sn * sn;
+      double poly = 0.0;
+      for (int l = order - 1; l >= 0; --l) poly = pg.gfb[l] + poly * z;
+      den *= poly;
+    }
+    den *= den;
+    const double tp = 2.0 * kPi;
+    double k[3], step[3][3];   // step[m][c]: component c of the alias step 2 pi invcl^T (K_m e_m)
+    for (int c = 0; c < 3; ++c) {
+      k[c] = tp * (invcl.m[0][c] * inm[0] + invcl.m[1][c] * inm[1] + invcl.m[2][c] * inm[2]);
+      for (int m = 0; m < 3; ++m) step[m][c] = tp * invcl.m[m][c] * K[m];
+    }
+    const double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+    const double isc2 = 0.25 / (screen * screen);
+    auto usq = [&](int m, int nm) {
+      const double t = kPi * (inm[m] / K[m] + nm);
+      if (t == 0.0) return 1.0;
+      const double x = sin(t) / t, x2 = x * x;
+      double r = 1.0;
+      for (int e = 0; e < order; ++e) r *= x2;
+      return r;
+    };
+    double sum = 0.0;
+    for (int nx = -pg.mmax[0]; nx <= pg.mmax[0]; ++nx) {
+      const double u1 = usq(0, nx);
+      for (int ny = -pg.mmax[1]; ny <= pg.mmax[1]; ++ny) {
+        const double u12 = u1 * usq(1, ny);
+        for (int nz = -pg.mmax[2]; nz <= pg.mmax[2]; ++nz) {
+          const double u = u12 * usq(2, nz);
+          double km[3];
+          for (int c = 0; c < 3; ++c) km[c] = k[c] + nx * step[0][c] + ny * step[1][c] + nz * step[2][c];
+          const double kk = km[0] * km[0] + km[1] * km[1] + km[2] * km[2];
+          sum += (k[0] * km[0] + k[1] * km[1] + k[2] * km[2]) * exp(-kk * isc2) * u / kk;
+        }
+      }
+    }
+    factor = sum * 4.0 * kPi / (k2 * den) / volume;
+  }
+  engfac[i] = (float)factor;
+  if (engfacT) engfacT[((size_t)r1 * K3 + r3) * K2 + r2] = (float)factor;
+}
+
 void launch_engfac(const FrameArgs& a, const DeviceState& d, const double invcl[3][3], double volume, double screen,
-                   cudaStream_t s) {
+                   const PppmGreen& pg, cudaStream_t s) {
   Mat3d m;
   for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) m.m[i][j] = invcl[i][j];
   const int n = a.K3 * a.K2 * a.Kh1;
-  k_engfac<<<(n + 255) / 256, 256, 0, s>>>(a.K1, a.K2, a.K3, a.Kh1, a.order, m, volume, screen, d.splfc, d.engfac,
-                                         d.engfacT);
+  if (pg.on)
+    k_engfac_pppm<<<(n + 255) / 256, 256, 0, s>>>(a.K1, a.K2, a.K3, a.Kh1, a.order, m, volume, screen, pg,
+                                                d.engfac, d.engfacT);
+  else
+    k_engfac<<<(n + 255) / 256, 256, 0, s>>>(a.K1, a.K2, a.K3, a.Kh1, a.order, m, volume, screen, d.splfc,
+                                           d.engfac, d.engfacT);
 }
 
 // ---------------------------------------------------------------------------

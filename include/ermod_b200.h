@@ -96,6 +96,9 @@ extern "C" {
 /*
  * Run parameters: &ene_param after iniparam (erdst/setconf.F90:133-438)
  * has applied its defaults.  `temp` is kcal/mol (setconf.F90:304).
+ * cltype: ERMOD_EL_COULOMB, ERMOD_EL_PME, or ERMOD_EL_PPPM with an even splodr
+ * (recpcal_pppm_greenfunc, recpcal.F90:217-337); ERMOD_EL_EWALD is refused
+ * ("set_prs") as setconf.F90:318-320 refuses it.
  */
 typedef struct ermod_params {
   int32_t slttype, boxshp, estype, cltype, ljswitch;

@@ -316,11 +316,14 @@ template <class T> struct Oracle {
       gmx_force_params(12, (T)p.lwljcut, (T)p.upljcut, repA, repB, repC);
       gmx_force_params(6, (T)p.lwljcut, (T)p.upljcut, attA, attB, attC);
     }
-    if (p.cltype == ERMOD_EL_PME) {
+    if (p.cltype == ERMOD_EL_PME || p.cltype == ERMOD_EL_PPPM) {
+      // recpcal.F90:250-251: the PPPM denominator needs an even order
+      if (p.cltype == ERMOD_EL_PPPM && p.splodr % 2 != 0) return fail(ERMOD_ERR_ARG, "pppm_odr");
       K1 = p.ms1max; K2 = p.ms2max; K3 = p.ms3max; cce = K1 / 2;
       spl.init(p.splodr);
       f1.init(K1); f2.init(K2); f3.init(K3);
       init_spline_axis(K1, splfc1); init_spline_axis(K2, splfc2); init_spline_axis(K3, splfc3);
+      if (p.cltype == ERMOD_EL_PPPM) calc_gfb_pppm();
       engfac.assign((size_t)(cce + 1) * K2 * K3, T(0));
     } else if (p.cltype != ERMOD_EL_COULOMB) {
       return fail(ERMOD_ERR_UNSUPPORTED, "set_prs");
@@ -371,6 +374,108 @@ template <class T> struct Oracle {
             factor = std::exp(-chr) / rtp2 / (T)kPi / volume;
             rtp2 = splfc1[rc1] * splfc2[rc2] * splfc3[rc3];
             factor = factor / rtp2;
+          }
+          engfac[((size_t)rc3 * K2 + rc2) * (cce + 1) + rc1] = factor;
+        }
+    engfac[0] = T(0);
+  }
+
+  // calc_gfb_pppm (recpcal.F90:179-198).  gfb[l], l = 0 .. P-1, are the coefficients of
+  // sum_n U^2(k + 2 pi n / h) = sum_l gfb[l] z^l, z = sin^2(k h / 2), for the order-P
+  // assignment function U(k) = (sin(k h / 2) / (k h / 2))^P: the recurrence of the
+  // reference, then the division by (2P - 1)!.
+  std::vector<double> gfb;
+  void calc_gfb_pppm() {
+    const int P = p.splodr;
+    gfb.assign(P, 0.0);
+    gfb[0] = 1.0;
+    for (int m = 1; m < P; ++m) {
+      for (int l = m; l >= 1; --l)
+        gfb[l] = 4.0 * (gfb[l] * (l - m) * (l - m - 0.5) - gfb[l - 1] * (l - m - 1) * (l - m - 1));
+      gfb[0] = 4.0 * (gfb[0] * (-m) * (-m - 0.5));
+    }
+    double fact = 1.0;
+    for (int i = 2; i <= 2 * P - 1; ++i) fact *= i;
+    for (int l = 0; l < P; ++l) gfb[l] /= fact;
+  }
+
+  // gf_denom (recpcal.F90:201-214): the squared product of the three axes' alias sums
+  T gf_denom(const T z[3]) const {
+    T s[3] = {T(0), T(0), T(0)};
+    for (int l = p.splodr - 1; l >= 0; --l)
+      for (int a = 0; a < 3; ++a) s[a] = (T)gfb[l] + s[a] * z[a];
+    const T prod = s[0] * s[1] * s[2];
+    return prod * prod;
+  }
+
+  // Alias range of the PPPM sums (recpcal.F90:230-233, 243-244): m_max per mesh axis
+  // from LAMMPS's accuracy form with EPS_HOC = 1e-7, projected on each cell vector,
+  // in single precision and truncated as the reference's int().  -1 on a negative range.
+  static void pppm_mrange(const float c[3][3], float screen, int K1, int K2, int K3, int out[3]) {
+    const float acc = std::pow(-std::log(1.0e-7f), 0.25f);
+    const float pi = (float)kPi;
+    const float mm[3] = {screen / (pi * (float)K1) * acc, screen / (pi * (float)K2) * acc,
+                         screen / (pi * (float)K3) * acc};
+    for (int j = 0; j < 3; ++j) {
+      const int v = (int)(c[0][j] * mm[0] + c[1][j] * mm[1] + c[2][j] * mm[2]);
+      out[j] = v;
+    }
+  }
+
+  // recpcal_pppm_greenfunc (recpcal.F90:217-337): Hockney and Eastwood's optimal influence
+  // function, sum over aliases k_n = k + 2 pi invcl^T (n1 K1, n2 K2, n3 K3), |n_i| <= mmax[i],
+  // of (k . k_n) gamma(k_n) U^2(k_n) / |k_n|^2, times 4 pi / (k^2 denom V).  The third alias
+  // offset is n3 * K3; the reference's :311 multiplies n3 by K2 instead, which this does not
+  // repeat (it differs only when K2 != K3 and mmax[2] > 0).
+  int mrange[3] = {0, 0, 0};
+  void pppm_greenfunc() {
+    const T tp = T(2) * (T)kPi;
+    const T sc = (T)p.screen;
+    const int Kv[3] = {K1, K2, K3};
+    for (int rc3 = 0; rc3 < K3; ++rc3)
+      for (int rc2 = 0; rc2 < K2; ++rc2)
+        for (int rc1 = 0; rc1 <= cce; ++rc1) {
+          if (rc1 == 0 && rc2 == 0 && rc3 == 0) continue;
+          const int rcv[3] = {rc1, rc2, rc3};
+          T inm[3], z[3];
+          for (int a = 0; a < 3; ++a) {
+            inm[a] = rcv[a] <= Kv[a] / 2 ? T(rcv[a]) : T(rcv[a] - Kv[a]);
+            const T sn = std::sin((T)kPi * inm[a] / T(Kv[a]));
+            z[a] = sn * sn;
+          }
+          T k[3];
+          for (int i = 0; i < 3; ++i) k[i] = tp * (invcl[0][i] * inm[0] + invcl[1][i] * inm[1] + invcl[2][i] * inm[2]);
+          const T k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+          T factor = T(0);
+          if (k2 > T(0)) {
+            T sum = T(0);
+            T ukm[3];
+            auto usq = [&](int a, int n) {
+              const T t = (T)kPi * (inm[a] / T(Kv[a]) + T(n));
+              if (t == T(0)) return T(1);
+              const T x = std::sin(t) / t;
+              T r = T(1);
+              for (int e = 0; e < 2 * p.splodr; ++e) r *= x;
+              return r;
+            };
+            for (int nx = -mrange[0]; nx <= mrange[0]; ++nx) {
+              ukm[0] = usq(0, nx);
+              for (int ny = -mrange[1]; ny <= mrange[1]; ++ny) {
+                ukm[1] = usq(1, ny);
+                for (int nz = -mrange[2]; nz <= mrange[2]; ++nz) {
+                  ukm[2] = usq(2, nz);
+                  const T mN[3] = {T(nx * K1), T(ny * K2), T(nz * K3)};
+                  T km[3];
+                  for (int i = 0; i < 3; ++i)
+                    km[i] = k[i] + tp * (invcl[0][i] * mN[0] + invcl[1][i] * mN[1] + invcl[2][i] * mN[2]);
+                  T gam = T(1);
+                  for (int i = 0; i < 3; ++i) gam *= std::exp(T(-0.25) * (km[i] / sc) * (km[i] / sc));
+                  const T kk = km[0] * km[0] + km[1] * km[1] + km[2] * km[2];
+                  sum += (k[0] * km[0] + k[1] * km[1] + k[2] * km[2]) * gam * (ukm[0] * ukm[1] * ukm[2]) / kk;
+                }
+              }
+            }
+            factor = sum * T(4) * (T)kPi / (k2 * gf_denom(z)) / volume;
           }
           engfac[((size_t)rc3 * K2 + rc2) * (cce + 1) + rc1] = factor;
         }
@@ -1190,13 +1295,21 @@ template <class T> struct Oracle {
       }
     }
     // PME setup (engconst :419-437)
-    const bool pme = p.cltype == ERMOD_EL_PME;
+    const bool pme = p.cltype == ERMOD_EL_PME || p.cltype == ERMOD_EL_PPPM;
     std::vector<T> wslv;
     std::vector<int> gslv, slvtag(nummol, -1);
     if (pme) {
       bool changed = !pme_initialized;
       for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) if (prevcl[i][j] != cell[i][j]) changed = true;
-      if (changed) spline_greenfunc();
+      if (changed && p.cltype == ERMOD_EL_PPPM) {
+        float cf[3][3];
+        for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) cf[i][j] = (float)cell[i][j];
+        pppm_mrange(cf, p.screen, K1, K2, K3, mrange);
+        if (mrange[0] < 0 || mrange[1] < 0 || mrange[2] < 0) return fail(ERMOD_ERR_ARG, "pppm_mrg");
+        pppm_greenfunc();
+      } else if (changed) {
+        spline_greenfunc();
+      }
       for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) prevcl[i][j] = cell[i][j];
       pme_initialized = true;
       // recpcal_prepare_solvent (recpcal.F90:340-357)
@@ -1374,6 +1487,16 @@ int mesh_one(const ermod_hist* h, int pti, std::vector<double>& ercrd, int* pema
 extern "C" {
 
 void orc_philox4x32_10(const uint32_t* ctr, const uint32_t* key, uint32_t* out) { philox4x32_10(ctr, key, out); }
+
+// calc_gfb_pppm (recpcal.F90:179-198) for one order: out[0 .. order-1]
+void orc_pppm_gfb(int order, double* out) {
+  ermod_params p{};
+  p.splodr = order;
+  Oracle<double> o;
+  o.p = p;
+  o.calc_gfb_pppm();
+  for (int l = 0; l < order; ++l) out[l] = o.gfb[l];
+}
 
 double orc_spline_value(int order, double x) {
   Spline<double> s;

@@ -75,6 +75,13 @@ def spline_value(order: int, x: float) -> float:
     return lib().orc_spline_value(order, x)
 
 
+def pppm_gfb(order: int) -> np.ndarray:
+    """Coefficients of the PPPM alias-sum polynomial in sin^2(kh/2) (recpcal.F90:179-198)."""
+    out = np.zeros(order)
+    lib().orc_pppm_gfb(order, out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
 def binsearch(coord, v) -> int:
     c = A.as_f64(coord)
     return lib().orc_binsearch(A.ptr(c, C.c_double), len(c), float(v))

@@ -440,3 +440,75 @@ def test_fused_solve_matches_cufft_on_mixed_meshes(lib, mesh):
         u, u0 = out[path]
         check_energies(u, u1)
         np.testing.assert_allclose(u0, u01, rtol=1e-6, atol=2e-5)
+
+
+# ---------------------------------------------------------------------------
+# PPPM (cltype 3): the same pipeline with Hockney and Eastwood's influence function
+# (recpcal_pppm_greenfunc, recpcal.F90:217-337) computed on the device.
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("order,path,mesh,screen", [(4, 1, None, None), (4, 2, None, None), (6, 3, None, None),
+                                                    (4, 2, (16, 32, 16), 1.2), (6, 1, (16, 32, 16), 1.2)])
+def test_pppm_refs_energies_and_bins(lib, oracle_mod, order, path, mesh, screen):
+    """PPPM energies against the FP64 oracle on the GPU's placements; the coarse mixed mesh
+    with a wide screening takes alias sums with |n| <= 1 on the 16-point axes.  uvengy0 is
+    the small difference of the real-space self term -sum q^2 screen / sqrt(pi) and the
+    reciprocal self energy, which cancel; its FP32 tolerance is 2e-6 of that term's size
+    (2e-5 kcal/mol at screen 0.35, 7e-5 at 1.2)."""
+    w = S.make_workload(2, small=True, maxins=96)
+    prm = dict(w.params, keep_uvengy=1, spectrum_path=path, cltype=A.EL_PPPM, splodr=order)
+    if mesh is not None:
+        prm.update(ms1max=mesh[0], ms2max=mesh[1], ms3max=mesh[2], screen=screen)
+    eng = Engine(prm, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, u0 = eng.uvengy()
+    ins, _ = eng.insertions()
+    orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist)
+    assert orc.engconst(1, pos, cell, ins_conf=ins) >= 0
+    uo, u0o = orc.uvengy()
+    check_energies(u, uo)
+    q = w.topo.charge[-w.topo.numsite[-1]:].astype(np.float64)
+    self_term = float((q ** 2).sum()) * float(np.float32(prm["screen"])) / np.sqrt(np.pi)
+    np.testing.assert_allclose(u0, u0o, rtol=1e-6, atol=max(2e-5, 2e-6 * self_term))
+    spec = phys_uvspec(w.topo)
+    bg = bins_of(u, eng.uvcrd, eng.uvmax, spec)
+    bo = bins_of(uo, eng.uvcrd, eng.uvmax, spec)
+    assert np.all((bg == bo) | near_edge(uo, eng.uvcrd, energy_tol(uo)))
+    wrel = WREL * max(1.0, 2e-6 * self_term / 2e-5)
+    assert eng.accum()["engnorm"] == pytest.approx(orc.accum()["engnorm"], rel=wrel)
+
+
+@pytest.mark.parametrize("K,order,path", [(32, 6, 1), (32, 6, 2), (32, 8, 3), (64, 4, 2)])
+def test_pppm_madelung_gpu(lib, oracle_mod, K, order, path):
+    prm, topo, hist, pos, cell, ins, L = nacl_system(K=K, order=order)
+    prm = dict(prm, cltype=A.EL_PPPM)
+    eng = Engine(dict(prm, keep_uvengy=1, spectrum_path=path), topo, hist)
+    assert eng.engconst(1, pos, cell, ins_conf=ins) >= 0
+    u, u0 = eng.uvengy()
+    orc = oracle_mod.Oracle(prm, topo, hist)
+    assert orc.engconst(1, pos, cell, ins_conf=ins) == 0
+    uo, u0o = orc.uvengy()
+    # FP32 grids and FFT on +-18.2 (kcal/mol A)^1/2 ions: 1e-5 relative of the FP64 oracle
+    assert u.sum() == pytest.approx(uo.sum(), rel=1e-5)
+    assert u0[0] == pytest.approx(u0o[0], rel=1e-5)
+
+
+def test_pppm_soln_ljsite(lib, oracle_mod):
+    w = S.make_workload(1, small=True)
+    prm = dict(w.params, keep_uvengy=1, cltype=A.EL_PPPM, splodr=4)
+    eng = Engine(prm, w.topo, w.hist)
+    orc = oracle_mod.Oracle(prm, w.topo, w.hist)
+    for fr in range(2):
+        pos, cell = w.frame(fr)
+        assert eng.engconst(fr + 1, pos, cell) >= 0
+        assert orc.engconst(fr + 1, pos, cell) >= 0
+        u, _ = eng.uvengy()
+        uo, _ = orc.uvengy()
+        check_energies(u, uo)
+    np.testing.assert_allclose(eng.accum()["slnuv"], orc.accum()["slnuv"], rtol=1e-5, atol=1e-3)
+
+
+def test_pppm_odd_order_is_rejected(lib):
+    w = S.make_workload(2, small=True, maxins=32)
+    with pytest.raises(ErmodError, match="pppm_odr"):
+        Engine(dict(w.params, cltype=A.EL_PPPM, splodr=5), w.topo, w.hist)
