@@ -98,6 +98,18 @@ class ErmodAccum(C.Structure):
     ]
 
 
+class ErmodStoreInfo(C.Structure):
+    _fields_ = [
+        ("slttype", C.c_int32), ("corrcal", C.c_int32), ("selfcal", C.c_int32), ("wgtslf", C.c_int32),
+        ("division", C.c_int32), ("engdiv", C.c_int32),
+        ("numslv", C.c_int32), ("ermax", C.c_int32), ("esmax", C.c_int32),
+        ("uvcrd", _f64p), ("uvmax", _i32p), ("uvsoft", _i32p), ("escrd", _f64p),
+    ]
+
+
+ERR_IO, ERR_FORMAT, TRJ_EOF = -30, -31, 1
+
+
 def ptr(a, ctype):
     """Pointer to the data of a contiguous numpy array (None -> NULL)."""
     if a is None:
@@ -108,7 +120,7 @@ def ptr(a, ctype):
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libermod_b200.so")
 
-# Every symbol include/ermod_b200.h declares, with its ctypes signature.
+# Every symbol include/ermod_b200.h and include/ermod_io.h declare, with its ctypes signature.
 SIGNATURES = {
     "ermod_abi_version": (C.c_int32, []),
     "ermod_enginit_mesh": (C.c_int32, [C.POINTER(ErmodHist), C.c_int32, _f64p, _i32p, _i32p, _f64p, _i32p, _i32p]),
@@ -150,6 +162,16 @@ SIGNATURES = {
     "ermod_destroy": (None, [C.c_void_p]),
     "ermod_histogram_noalloc": (C.c_int32, [C.c_int32, C.c_int32, _f64p, C.c_int32, C.c_int32, _i32p, _f64p,
                                             _i32p, _i32p, C.c_int32, _f64p, _f64p]),
+    # include/ermod_io.h
+    "ermod_traj_open": (C.c_int32, [C.c_char_p, C.POINTER(C.c_void_p), _i32p, _i32p, _i32p]),
+    "ermod_traj_read": (C.c_int32, [C.c_void_p, C.c_int32, _f32p, _f32p]),
+    "ermod_traj_rewind": (C.c_int32, [C.c_void_p]),
+    "ermod_traj_close": (None, [C.c_void_p]),
+    "ermod_write_engstore": (C.c_int32, [C.c_char_p, C.POINTER(ErmodStoreInfo), C.POINTER(ErmodAccum), _f64p,
+                                         _f32p]),
+    "ermod_io_format": (C.c_int32, [C.c_int32, C.c_double, C.c_int32, C.c_int32, C.c_char_p, C.c_int32]),
+    "ermod_io_last_error": (C.c_char_p, []),
+    "ermod_rmsd_bestfit": (C.c_double, [C.c_int32, _f32p, _f32p, _f32p]),
 }
 
 NOALLOC_SCRATCH_BYTES = 32 << 20

@@ -25,7 +25,8 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["kT_of", "delta_mu"]
+__all__ = ["kT_of", "delta_mu", "representative_bins", "read_engfile", "read_corfile", "read_table",
+           "delta_mu_from_files"]
 
 
 def kT_of(temp_K: float) -> float:
@@ -177,3 +178,106 @@ def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: f
     terms = -kT * (rho - rho0) + lcent * rho + kT * fac * (rho - rho0)
     chmpt = np.array([terms[live & (spec == p)].sum() for p in range(1, nsp + 1)]) + np.asarray(aveuv)
     return chmpt, float(chmpt.sum() + slfeng)
+
+
+# ---------------------------------------------------------------------------
+# erdst's output files (engproc.F90:630-722) as slvfe reads them
+# ---------------------------------------------------------------------------
+def representative_bins(uvcrd, uvmax, uvsoft):
+    """representative_bin_info (engproc.F90:1355-1387) for every bin: (left, middle,
+    1/width, 1-based species); the last bin of a species has width 0 (1/width = 0)."""
+    c = np.asarray(uvcrd, dtype=np.float64)
+    left = c.copy()
+    middle = c.copy()
+    invwt = np.zeros(len(c))
+    spec = np.zeros(len(c), dtype=int)
+    base = 0
+    for p, (mx, sf) in enumerate(zip(uvmax, uvsoft)):
+        for idpt in range(1, mx + 1):
+            i = base + idpt - 1
+            spec[i] = p + 1
+            if i + 1 >= len(c):
+                continue
+            if idpt <= sf:
+                middle[i] = (c[i] + c[i + 1]) / 2.0
+                invwt[i] = 1.0 / (c[i + 1] - c[i])
+            elif idpt < mx:
+                middle[i] = np.sqrt(c[i] * c[i + 1])
+                invwt[i] = 1.0 / (c[i + 1] - c[i])
+        base += mx
+    return left, middle, invwt, spec
+
+
+def _fortran_real(tok: str) -> float:
+    """A real as Fortran list-directed input takes it, including the exponent form
+    without a letter ("0.1234567-100") that E editing writes beyond two exponent digits."""
+    t = tok.strip()
+    try:
+        return float(t)
+    except ValueError:
+        k = max(t.rfind("+"), t.rfind("-"))
+        if k > 0 and t[k - 1] not in "eEdD":
+            return float(t[:k] + "E" + t[k:])
+        return float(t.replace("D", "E").replace("d", "e"))
+
+
+def read_engfile(path) -> dict:
+    """engsln / engref (engproc.F90:686-699): one header line, then bin_left,
+    bin_middle, species, ratio (= the engstore-normalised distribution) and dens
+    (ratio / bin width) per bin, as slvfe's datread takes them (slvfe.F90:380-386)."""
+    rows = []
+    with open(path) as f:
+        f.readline()
+        for line in f:
+            if line.strip():
+                rows.append([_fortran_real(t) for t in line.split()])
+    a = np.array(rows)
+    return dict(left=a[:, 0], middle=a[:, 1], spec=a[:, 2].astype(int), ratio=a[:, 3], dens=a[:, 4])
+
+
+def read_corfile(path, ermax: int) -> np.ndarray:
+    """corsln / corref: one Fortran unformatted record of ermax x ermax FP64 values
+    (engproc.F90:702-713, read by slvfe.F90:404-407), column-major."""
+    raw = open(path, "rb").read()
+    n = ermax * ermax * 8
+    head = int(np.frombuffer(raw[:4], dtype="<i4")[0])
+    tail = int(np.frombuffer(raw[4 + n:8 + n], dtype="<i4")[0]) if len(raw) >= n + 8 else -1
+    if head != n or tail != n or len(raw) != n + 8:
+        raise ValueError(f"{path}: not one record of {ermax}x{ermax} FP64 values")
+    return np.frombuffer(raw[4:4 + n], dtype="<f8").reshape(ermax, ermax, order="F").copy()
+
+
+def read_table(path) -> np.ndarray:
+    """Numeric rows of aveuv.tt, weight_soln / weight_refs and the like (list-directed)."""
+    rows = []
+    with open(path) as f:
+        for line in f:
+            t = line.split()
+            if t and not t[0].startswith("#"):
+                try:
+                    rows.append([_fortran_real(x) for x in t])
+                except ValueError:
+                    continue   # a text header line (uvrange.tt)
+    return np.array(rows)
+
+
+def delta_mu_from_files(soln_dir, refs_dir, temp_K: float, suffix: str = "tt", slfslt: bool = False):
+    """slvfe on one division's files: engsln.<suffix> and aveuv.tt from the solution run,
+    engref.<suffix> and corref.<suffix> from the reference-solvent run; with slfslt the
+    solute self energy is weight_refs' third column averaged with its first-column
+    weights (slvfe.F90:257-286).  Returns delta_mu's (per-species, total)."""
+    import os
+    sln = read_engfile(os.path.join(soln_dir, f"engsln.{suffix}"))
+    ref = read_engfile(os.path.join(refs_dir, f"engref.{suffix}"))
+    if not np.array_equal(sln["spec"], ref["spec"]) or not np.allclose(sln["middle"], ref["middle"]):
+        raise ValueError("solution and reference-solvent meshes differ")
+    chi = read_corfile(os.path.join(refs_dir, f"corref.{suffix}"), len(ref["ratio"]))
+    av = read_table(os.path.join(soln_dir, "aveuv.tt"))
+    div = 1 if suffix == "tt" else int(suffix)
+    aveuv = av[div - 1, 1:]
+    slf = 0.0
+    if slfslt:
+        wr = read_table(os.path.join(refs_dir, "weight_refs"))
+        w = wr[:, 1] / wr[:, 1].sum()
+        slf = float(np.dot(w, wr[:, 2]))
+    return delta_mu(sln["ratio"], ref["ratio"], chi, sln["middle"], sln["spec"], temp_K, aveuv, slf)

@@ -12,12 +12,16 @@ from ermod_openacc_b200 import systems as S
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "ermod_b200.h")
+HEADERS = sorted(os.path.join(ROOT, "include", h) for h in os.listdir(os.path.join(ROOT, "include"))
+                 if h.endswith(".h"))
 
 
 def declared_functions():
-    txt = open(HEADER).read()
-    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(ermod_[a-z0-9_]+)\s*\(", txt)))
+    names = set()
+    for h in HEADERS:
+        txt = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        names |= set(re.findall(r"\b(ermod_[a-z0-9_]+)\s*\(", txt))
+    return sorted(names)
 
 
 def test_header_and_ctypes_agree():
@@ -35,8 +39,10 @@ def test_library_exports_every_declared_symbol(engine_lib):
 def test_struct_layouts_match_c(tmp_path):
     src = tmp_path / "layout.c"
     structs = {"ermod_params": A.ErmodParams, "ermod_topology": A.ErmodTopology, "ermod_mesh": A.ErmodMesh,
-               "ermod_hist": A.ErmodHist, "ermod_accum": A.ErmodAccum}
-    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+               "ermod_hist": A.ErmodHist, "ermod_accum": A.ErmodAccum, "ermod_store_info": A.ErmodStoreInfo}
+    io_header = os.path.join(ROOT, "include", "ermod_io.h")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', f'#include "{io_header}"',
+             "int main(void){"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
         for fname, _ in cls._fields_:

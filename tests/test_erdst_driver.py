@@ -1,0 +1,221 @@
+"""The erdst trajectory loop (ermod_openacc_b200.erdst.run): HISTORY / SysWght /
+SltConf / SltWght in, engstore's files out.  CPU tests drive it with the oracle behind
+the engine interface; the GPU test compares the CUDA engine's files with those."""
+import os
+
+import numpy as np
+import pytest
+
+from ermod_openacc_b200 import _capi as A
+from ermod_openacc_b200 import erdst
+from ermod_openacc_b200 import erdst_io as IO
+from ermod_openacc_b200 import slvfe as SF
+from ermod_openacc_b200 import systems as S
+from _dcd import write_dcd
+
+
+class OracleEngine:
+    """The oracle behind the engine interface the loop drives (test infrastructure)."""
+
+    def __init__(self, oracle_mod, params, topo, hist):
+        self.o = oracle_mod.Oracle(params, topo, hist, precision=8)
+        self.params = params
+        self.uvcrd, self.uvmax, self.uvsoft, self.escrd = self.o.uvcrd, self.o.uvmax, self.o.uvsoft, self.o.escrd
+        self.calls = []
+
+    def engclear(self):
+        self.o.engclear()
+
+    def engconst(self, stnum, pos, cell, w=1.0, ins_conf=None, ins_weight=None):
+        self.calls.append(dict(stnum=stnum, pos=pos.copy(), cell=cell.copy(), w=w,
+                               ins_conf=None if ins_conf is None else ins_conf.copy(),
+                               ins_weight=None if ins_weight is None else ins_weight.copy()))
+        return self.o.engconst(stnum, pos, cell, w, ins_conf=ins_conf, ins_weight=ins_weight)
+
+    def engstore(self):
+        raw = self.o.accum()
+        norm = self.o.accum(normalise=True)
+        sgn = -1.0 if self.params["slttype"] == A.SLT_SOLN else 1.0
+        with np.errstate(divide="ignore"):
+            av = np.array([raw["engnorm"] / raw["engsmpl"], raw["voffset"] + sgn * self.params["temp"] *
+                           np.log(norm["avslf"])])
+        return norm, av
+
+
+def _history(tmp_path, w, nframes, perm=None, name="HISTORY.dcd"):
+    frames, cells = [], []
+    for k in range(nframes):
+        pos, cell = w.frame(k)
+        p3 = np.asarray(pos, dtype=np.float32).reshape(-1, 3)
+        if perm is not None:   # HISTORY atom i is program atom perm[i]
+            p3 = p3[perm]
+        frames.append(p3)
+        c = np.asarray(cell, dtype=np.float64).reshape(3, 3, order="F")
+        cells.append([c[0, 0], 0.0, c[1, 1], 0.0, 0.0, c[2, 2]])   # orthorhombic: cosines 0
+    path = tmp_path / name
+    write_dcd(path, frames, cells)
+    return path
+
+
+def _read_frames(path, n):
+    with IO.Trajectory(path) as t:
+        return [t.read() for _ in range(n)]
+
+
+def _expected(oracle_mod, prm, topo, hist, frames, weights, stnums):
+    eng = OracleEngine(oracle_mod, prm, topo, hist)
+    for (pos, cell), wv, st in zip(frames, weights, stnums):
+        assert eng.engconst(st, pos, cell, wv) >= 0
+    return eng.engstore()
+
+
+def test_refs_divisions_weights_and_skips(engine_lib, oracle_mod, tmp_path):
+    w = S.make_workload(2, small=True, maxins=48)
+    prm = dict(w.params, selfcal=1)
+    hist_path = _history(tmp_path, w, 8)
+    wfile = tmp_path / "SysWght"
+    wts = [1.0, 0.5, 2.0, 1.5, 0.75, 1.25, 3.0, 0.25]
+    wfile.write_text("".join(f"{i + 1} {v}\n" for i, v in enumerate(wts)))
+    out = tmp_path / "out"
+    eng = OracleEngine(oracle_mod, prm, w.topo, w.hist)
+    res = erdst.run(prm, w.topo, w.hist, hist_path, out, maxcnf=8, skpcnf=2, engdiv=2, syswgt=wfile, engine=eng)
+    assert res["frames"] == 4
+    # skpcnf 2: frames 2, 4 | 6, 8 with their own weights, numbered 1..4
+    assert [c["stnum"] for c in eng.calls] == [1, 2, 3, 4]
+    assert [c["w"] for c in eng.calls] == [wts[1], wts[3], wts[5], wts[7]]
+    fr = _read_frames(hist_path, 8)
+    for c, k in zip(eng.calls, (1, 3, 5, 7)):
+        np.testing.assert_array_equal(c["pos"], fr[k][0])
+    assert sorted(os.listdir(out)) == ["corref.01", "corref.02", "engref.01", "engref.02", "slfeng.01",
+                                       "slfeng.02", "uvrange.tt", "weight_refs"]
+    for div, ks, st in ((1, (1, 3), (1, 2)), (2, (5, 7), (3, 4))):
+        norm, av = _expected(oracle_mod, prm, w.topo, w.hist, [fr[k] for k in ks], [wts[k] for k in ks], st)
+        e = SF.read_engfile(out / f"engref.{div:02d}")
+        np.testing.assert_allclose(e["ratio"], norm["edens"], rtol=1e-13, atol=1e-300)
+        # division 2 keeps the run's first voffset, the fresh oracle its own: rounding only
+        np.testing.assert_allclose(SF.read_corfile(out / f"corref.{div:02d}", len(e["ratio"])), norm["ecorr"].T,
+                                   rtol=1e-13, atol=1e-300)
+        # engnorm / engsmpl carries exp(voffset / kT) of the run's first frame: exact for
+        # division 1; the voffset-free second column in both
+        if div == 1:
+            np.testing.assert_allclose(res["avediv"][0], av, rtol=1e-12)
+        assert res["avediv"][div - 1, 1] == pytest.approx(av[1], rel=1e-10, abs=1e-12)
+    t = SF.read_table(out / "weight_refs")
+    np.testing.assert_allclose(t[:, 1], res["avediv"][:, 0], rtol=5.01e-8)
+
+
+def test_permutation(engine_lib, oracle_mod, tmp_path):
+    w = S.make_workload(2, small=True, maxins=24)
+    n = int(np.asarray(w.topo.numsite)[(w.topo.sluvid == A.PT_SOLVENT) | (w.topo.sluvid == A.PT_SOLUTE)].sum())
+    rng = np.random.default_rng(2)
+    perm = rng.permutation(n)                   # HISTORY atom i is program atom perm[i]
+    plain = _history(tmp_path, w, 2, name="plain.dcd")
+    shuffled = _history(tmp_path, w, 2, perm=perm, name="perm.dcd")
+    e1 = OracleEngine(oracle_mod, w.params, w.topo, w.hist)
+    erdst.run(w.params, w.topo, w.hist, plain, tmp_path / "a", maxcnf=2, engine=e1)
+    e2 = OracleEngine(oracle_mod, w.params, w.topo, w.hist)
+    erdst.run(w.params, w.topo, w.hist, shuffled, tmp_path / "b", maxcnf=2, engine=e2, permutation=perm + 1)
+    for c1, c2 in zip(e1.calls, e2.calls):
+        np.testing.assert_array_equal(c1["pos"], c2["pos"])
+    assert open(tmp_path / "a" / "engref.tt").read() == open(tmp_path / "b" / "engref.tt").read()
+    with pytest.raises(IO.IOError_, match="set_pmt"):
+        erdst.run(w.params, w.topo, w.hist, shuffled, tmp_path / "c", maxcnf=2, engine=e2,
+                  permutation=np.ones(n, dtype=int))
+
+
+def test_soln_aveuv(engine_lib, oracle_mod, tmp_path):
+    w = S.make_workload(1, small=True)
+    hist_path = _history(tmp_path, w, 4)
+    eng = OracleEngine(oracle_mod, w.params, w.topo, w.hist)
+    res = erdst.run(w.params, w.topo, w.hist, hist_path, tmp_path / "o", maxcnf=4, engdiv=2, engine=eng)
+    av = SF.read_table(tmp_path / "o" / "aveuv.tt")
+    assert av.shape == (2, 1 + w.topo.numslv)
+    np.testing.assert_allclose(av[:, 1:], res["aveuv"], atol=5e-6)
+    assert os.path.exists(tmp_path / "o" / "engsln.01") and os.path.exists(tmp_path / "o" / "engsln.02")
+
+
+def _flex_setup(tmp_path, nconf=7):
+    w = S.make_workload(2, small=True, maxins=5)
+    kinds = [A.PT_TEST_FLEX if k == A.PT_TEST_RIGID else k for k in w.topo.kinds]
+    topo = S.Topology(w.topo.species, w.topo.counts, kinds)
+    prm = dict(w.params, slttype=A.SLT_REFS_FLEX)
+    ref = np.asarray(w.topo.bfcoord, dtype=np.float64).reshape(-1, 3)
+    rng = np.random.default_rng(9)
+    confs = [ref + rng.normal(scale=s, size=ref.shape) for s in np.linspace(0.0, 0.6, nconf)]
+    write_dcd(tmp_path / "SltConf.dcd", confs, None, charmm=False)
+    (tmp_path / "SltWght").write_text("".join(f"{i + 1} {1.0 + 0.1 * i}\n" for i in range(nconf)))
+    return w, topo, prm, ref, confs
+
+
+def test_flexible_solute_conformations_weights_and_rmsd_filter(engine_lib, oracle_mod, tmp_path):
+    w, topo, prm, ref, confs = _flex_setup(tmp_path)
+    hist_path = _history(tmp_path, w, 3)
+    wts = np.ones(len(ref), dtype=np.float32)
+    rms = np.array([IO.rmsd_bestfit(ref, c, wts) for c in confs])
+    lw, up = 0.05, 0.6
+    ok = np.nonzero((rms >= lw) & (rms <= up))[0]
+    assert 1 < len(ok) < len(confs)
+    eng = OracleEngine(oracle_mod, prm, topo, w.hist)
+    erdst.run(prm, topo, w.hist, hist_path, tmp_path / "o", maxcnf=3, engine=eng,
+              sltconf=tmp_path / "SltConf.dcd", sltwgt=tmp_path / "SltWght",
+              insstructure=erdst.INSSTR_RMSD, lwstr=lw, upstr=up, refslt=(ref, wts))
+    # accepted conformations in file order, wrapping around, with their own weights
+    seq = [ok[i % len(ok)] for i in range(3 * prm["maxins"])]
+    got_c = np.concatenate([c["ins_conf"].reshape(-1, len(ref), 3) for c in eng.calls])
+    got_w = np.concatenate([c["ins_weight"] for c in eng.calls])
+    for g, k in zip(got_c, seq):
+        np.testing.assert_array_equal(g, np.asarray(confs[k], dtype=np.float32))
+    np.testing.assert_allclose(got_w, [1.0 + 0.1 * k for k in seq], rtol=1e-6)
+    # no filter: every conformation in order
+    eng2 = OracleEngine(oracle_mod, prm, topo, w.hist)
+    erdst.run(prm, topo, w.hist, hist_path, tmp_path / "p", maxcnf=1, engine=eng2,
+              sltconf=tmp_path / "SltConf.dcd")
+    np.testing.assert_array_equal(eng2.calls[0]["ins_conf"].reshape(-1, len(ref), 3),
+                                  np.asarray(confs[:5], dtype=np.float32))
+    assert np.all(eng2.calls[0]["ins_weight"] == 1.0)
+
+
+def test_run_errors(engine_lib, oracle_mod, tmp_path):
+    w = S.make_workload(2, small=True, maxins=8)
+    hist_path = _history(tmp_path, w, 2)
+    eng = OracleEngine(oracle_mod, w.params, w.topo, w.hist)
+    with pytest.raises(IO.IOError_, match="eng_par"):
+        erdst.run(w.params, w.topo, w.hist, hist_path, tmp_path / "o", maxcnf=2, engdiv=3, engine=eng)
+    with pytest.raises(IO.IOError_, match="set_trj"):          # fewer frames than maxcnf
+        erdst.run(w.params, w.topo, w.hist, hist_path, tmp_path / "o", maxcnf=4, engine=eng)
+    w1 = S.make_workload(1, small=True)
+    with pytest.raises(IO.IOError_, match="set_trj"):          # atom count of another system
+        erdst.run(w1.params, w1.topo, w1.hist, hist_path, tmp_path / "o", maxcnf=1,
+                  engine=OracleEngine(oracle_mod, w1.params, w1.topo, w1.hist))
+
+
+@pytest.mark.gpu
+def test_gpu_engine_files_match_oracle(engine_lib, oracle_mod, tmp_path):
+    """The CUDA engine behind the same loop writes the files the FP64 oracle writes,
+    within the engine's tolerances (normalised distributions at 5e-5 relative)."""
+    from ermod_openacc_b200 import Engine
+    w = S.make_workload(2, small=True, maxins=64)
+    hist_path = _history(tmp_path, w, 4)
+    prm = dict(w.params, keep_uvengy=1)
+    gpu = Engine(prm, w.topo, w.hist)
+    erdst.run(prm, w.topo, w.hist, hist_path, tmp_path / "g", maxcnf=4, engdiv=2, engine=gpu)
+    ins = []
+    # the oracle on the GPU's placements: flexible, file-driven, unchanged
+    orc_prm = dict(prm, slttype=A.SLT_REFS_FLEX, insposition=A.INSPOS_NOCHANGE, insorient=A.INSROT_NOCHANGE)
+    kinds = [A.PT_TEST_FLEX if k == A.PT_TEST_RIGID else k for k in w.topo.kinds]
+    topo_f = S.Topology(w.topo.species, w.topo.counts, kinds)
+    gpu2 = Engine(prm, w.topo, w.hist)
+    fr = _read_frames(hist_path, 4)
+    for k, (pos, cell) in enumerate(fr):
+        assert gpu2.engconst(k + 1, pos, cell) >= 0
+        ins.append(gpu2.insertions()[0])
+    orc = OracleEngine(oracle_mod, orc_prm, topo_f, w.hist)
+    for div in (1, 2):
+        orc.engclear()
+        for k in ((0, 1) if div == 1 else (2, 3)):
+            assert orc.engconst(k + 1, fr[k][0], fr[k][1], 1.0, ins_conf=ins[k].ravel()) >= 0
+        norm, _ = orc.engstore()
+        e = SF.read_engfile(tmp_path / "g" / f"engref.{div:02d}")
+        assert e["ratio"].sum() == pytest.approx(norm["edens"].sum(), rel=5e-5)
+        # bins identical except energies at a mesh edge: a few counts move to a neighbour
+        assert np.abs(e["ratio"] - norm["edens"]).sum() <= 1e-3 * norm["edens"].sum()
