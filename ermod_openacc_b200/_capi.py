@@ -34,6 +34,7 @@ LJSWT_POT_CHM, LJSWT_POT_GMX, LJSWT_FRC_CHM, LJSWT_FRC_GMX = 0, 1, 2, 3
 INSPOS_RANDOM, INSPOS_NOCHANGE = 0, 1
 INSPOS_SPHERE, INSPOS_SLAB_GENERIC, INSPOS_SLAB_SYMMETRIC = 2, 3, 4
 INSPOS_RMSD, INSPOS_GAUSS = 5, 6
+INSSTR_NOREJECT, INSSTR_RMSD = 0, 1
 INSROT_RANDOM, INSROT_NOCHANGE = 0, 1
 PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
 
@@ -58,6 +59,7 @@ class ErmodParams(C.Structure):
         ("keep_uvengy", C.c_int32), ("ecorr_path", C.c_int32), ("spectrum_path", C.c_int32),
         ("graph_mode", C.c_int32), ("stage_timing", C.c_int32),
         ("lwreg", C.c_float), ("upreg", C.c_float), ("hostspec", C.c_int32),
+        ("insstructure", C.c_int32), ("lwstr", C.c_float), ("upstr", C.c_float),
     ]
 
 
@@ -192,7 +194,7 @@ def load_library(path: str | None = None):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.ermod_abi_version() != 2:
+    if lib.ermod_abi_version() != 3:
         raise RuntimeError("libermod_b200.so ABI mismatch")
     if path is None:
         _LIB = lib

@@ -119,6 +119,42 @@ ERM_HD void fit_a_rotate_b(int n, const float* refa, const float* a, const float
   }
 }
 
+// rmsd_bestfit (bestfit.F90:339-346) without a buffer for the fitted points: the rotation
+// that best maps x onto ref (weights w), each fitted point rounded to FP32 as fit_a_rotate_b
+// stores it, then the weighted RMSD from ref.  Returns -1 when the weights sum to zero.
+ERM_HD double rmsd_bestfit(int n, const float* ref, const float* x, const float* w) {
+  double cr[3] = {0.0, 0.0, 0.0}, cx[3] = {0.0, 0.0, 0.0}, ws = 0.0;
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) {
+      cr[k] += (double)w[i] * ref[3 * i + k];
+      cx[k] += (double)w[i] * x[3 * i + k];
+    }
+    ws += w[i];
+  }
+  if (ws == 0.0) return -1.0;
+  for (int k = 0; k < 3; ++k) { cr[k] /= ws; cx[k] /= ws; }
+  double S[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  for (int i = 0; i < n; ++i)
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c)
+        S[r][c] += (double)w[i] * ((double)x[3 * i + r] - cx[r]) * ((double)ref[3 * i + c] - cr[c]);
+  double q[4];
+  rotation_from_s(S, q);
+  double d = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double v[3] = {(double)x[3 * i] - cx[0], (double)x[3 * i + 1] - cx[1], (double)x[3 * i + 2] - cx[2]};
+    double r[3];
+    rotate(q, v, r);
+    double t = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double e = (double)ref[3 * i + k] - (double)(float)(r[k] + cr[k]);
+      t += e * e;
+    }
+    d += (double)w[i] * t;
+  }
+  return sqrt(d / ws);
+}
+
 // rmsd_nofit (bestfit.F90:349-364)
 ERM_HD double rmsd_nofit(int n, const float* x, const float* y, const float* w) {
   double d = 0.0, ws = 0.0;

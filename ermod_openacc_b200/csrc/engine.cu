@@ -296,6 +296,8 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     return bad(ERMOD_ERR_ARG, "ins_reg");
   if (p.insposition >= ERMOD_INSPOS_RMSD && !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f))
     return bad(ERMOD_ERR_ARG, "ins_reg");
+  if (p.insstructure != ERMOD_INSSTR_NOREJECT && p.insstructure != ERMOD_INSSTR_RMSD)
+    return bad(ERMOD_ERR_ARG, "ins_str");   // "Unknown insstructure" (engproc.F90:1293-1294)
   // topology (setparam / enginit / engconst bookkeeping)
   ctx->nummol = t->nummol;
   ctx->numsite.assign(t->numsite, t->numsite + t->nummol);
@@ -503,7 +505,8 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
     }
   }
   // soln: the verdicts of check_mol_configuration (sphere / slab around the aggregate, RMSD to RefInfo)
-  if (!refs && (ctx->nhost > 0 || p.insposition == ERMOD_INSPOS_RMSD)) CK(dalloc(&d.skip, MD));
+  if (!refs && (ctx->nhost > 0 || p.insposition == ERMOD_INSPOS_RMSD || p.insstructure == ERMOD_INSSTR_RMSD))
+    CK(dalloc(&d.skip, MD));
   std::vector<float> bf(3 * S, 0.0f);
   if (t->bfcoord) std::memcpy(bf.data(), t->bfcoord, sizeof(float) * 3 * S);
   CK(h2d(d.bfcoord, bf.data(), 3 * S, st));
@@ -760,7 +763,8 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
   if (!refs && (p.insposition == ERMOD_INSPOS_SLAB_GENERIC || p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) &&
       !g.periodic)
     return set_error(ctx, ERMOD_ERR_INS_GEO, "eng_slb");   // engproc.F90:1238
-  if (p.insposition >= ERMOD_INSPOS_RMSD && ctx->nref == 0 && (refs || p.insposition == ERMOD_INSPOS_RMSD))
+  if (ctx->nref == 0 && ((p.insposition >= ERMOD_INSPOS_RMSD && (refs || p.insposition == ERMOD_INSPOS_RMSD)) ||
+                         (!refs && p.insstructure == ERMOD_INSSTR_RMSD)))
     return set_error(ctx, ERMOD_ERR_ARG, "ins_ref");        // load_refstructure (insertion.F90:676-770)
   if (refs && p.insposition == ERMOD_INSPOS_GAUSS && !ctx->gauss_init) {
     // uniform_gauss_mixture keeps the first call's cell (insertion.F90:268-274): l = (|c_k|/2)/upreg,
@@ -962,13 +966,13 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
     launch_insert(a, d, d.frame_i, p.iseed, rg, fp.use_conf, fp.prop_gv, fp.prop_learned, st);
   }
   else launch_targets_soln(a, d, nullptr, st);
-  if (!refs && ctx->nhost > 0) {   // check_mol_configuration of every solute
-    launch_aggcen(d, ctx->nhost, st);
-    launch_soln_region(a, d, p.insposition, p.lwreg, p.upreg, st);
-    nl += 2;
-  }
-  if (!refs && ctx->nref > 0 && p.insposition == ERMOD_INSPOS_RMSD) {
-    launch_soln_region(a, d, p.insposition, p.lwreg, p.upreg, st);
+  if (!refs && d.skip) {   // check_mol_configuration of every solute
+    if (ctx->nhost > 0) {
+      launch_aggcen(d, ctx->nhost, st);
+      nl += 1;
+    }
+    const SolnCheck ck{p.insposition, p.lwreg, p.upreg, p.insstructure, p.lwstr, p.upstr};
+    launch_soln_region(a, d, ck, st);
     nl += 1;
   }
   CK(cudaMemsetAsync(d.selfrec, 0, sizeof(double) * ctx->maxdst, st));

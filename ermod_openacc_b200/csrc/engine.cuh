@@ -176,8 +176,14 @@ struct DeviceState {
 void launch_prepare_solvent(const FrameArgs& a, const DeviceState& d, cudaStream_t s);
 void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStream_t s);
 void launch_aggcen(const DeviceState& d, int nhost, cudaStream_t s);
-void launch_soln_region(const FrameArgs& a, const DeviceState& d, int insposition, float lwreg, float upreg,
-                        cudaStream_t s);
+// check_mol_configuration's inputs for solutes in solution (engproc.F90:1197-1295)
+struct SolnCheck {
+  int insposition;
+  float lwreg, upreg;
+  int insstructure;
+  float lwstr, upstr;
+};
+void launch_soln_region(const FrameArgs& a, const DeviceState& d, const SolnCheck& ck, cudaStream_t s);
 // Insertion geometry of a frame (set_shift_com, insertion.F90:131-304)
 struct InsRegion {
   int insposition, insorient;

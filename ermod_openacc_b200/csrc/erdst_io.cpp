@@ -424,12 +424,7 @@ extern "C" int32_t ermod_write_engstore(const char* dir, const ermod_store_info*
 // rmsd_bestfit (bestfit.F90:339-346): fit `crd` onto `ref` with weights w, then the weighted RMSD.
 extern "C" double ermod_rmsd_bestfit(int32_t n, const float* ref, const float* crd, const float* w) {
   if (n <= 0 || !ref || !crd || !w) return -1.0;
-  double ws = 0.0;
-  for (int i = 0; i < n; ++i) ws += w[i];
-  if (ws == 0.0) return -1.0;   // halt_with_error('bst_zrw') in the reference
-  std::vector<float> fitted((size_t)3 * n);
-  erm::fit::fit_a_rotate_b(n, ref, crd, w, n, crd, fitted.data());
-  return erm::fit::rmsd_nofit(n, ref, fitted.data(), w);
+  return erm::fit::rmsd_bestfit(n, ref, crd, w);   // -1: halt_with_error('bst_zrw') in the reference
 }
 
 extern "C" const char* ermod_io_last_error(void) { return g_err; }

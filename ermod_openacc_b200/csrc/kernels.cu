@@ -330,20 +330,44 @@ void launch_reffit(const DeviceState& d, int nref, int s, cudaStream_t st) {
 // (sphere) or along the third cell vector (slabs, invcl row 3 . dx * |c3|, its
 // absolute value for the symmetric slab).  skip[cnt] = 1 rejects solute cnt for
 // this frame: engconst skips its update_histogram (engproc.F90:447-450).
-__global__ void k_soln_region(FrameArgs a, int insposition, float lwreg, float upreg, const int* __restrict__ tgt_mol,
+__device__ int region_out(const FrameArgs& a, int insposition, float lwreg, float upreg, int k,
+                          const int* __restrict__ molbeg, const float* __restrict__ posraw,
+                          const float* __restrict__ atom_mass, const double* __restrict__ aggcen);
+
+// check_mol_configuration (engproc.F90:1197-1295) for every solute in solution: the
+// insposition window, then the insstructure RMSD window; skip[cnt] = 1 rejects the solute
+__global__ void k_soln_region(FrameArgs a, SolnCheck ck, const int* __restrict__ tgt_mol,
                               const int* __restrict__ molbeg, const float* __restrict__ posraw,
                               const float* __restrict__ atom_mass, const double* __restrict__ aggcen,
-                              const float* __restrict__ ref_bf, const float* __restrict__ ref_slt_w,
-                              int* __restrict__ skip) {
+                              const float* __restrict__ ref_bf, const float* __restrict__ ref_slt,
+                              const float* __restrict__ ref_slt_w, int* __restrict__ skip) {
   const int cnt = blockIdx.x * blockDim.x + threadIdx.x;
   if (cnt >= a.maxdst) return;
   const int k = tgt_mol[cnt];
+  const int insposition = ck.insposition;
+  const float lwreg = ck.lwreg, upreg = ck.upreg;
+  const float* xs = posraw + 3 * molbeg[k];
+  int out = 0;
   if (insposition == ERMOD_INSPOS_RMSD) {
     // RMSD of the solute to this frame's best-fit reference solute (engproc.F90:1249-1269)
-    const double rmsd = fit::rmsd_nofit(a.nsite, ref_bf, posraw + 3 * molbeg[k], ref_slt_w);
-    skip[cnt] = ((double)lwreg > rmsd || rmsd > (double)upreg) ? 1 : 0;
-    return;
+    const double rmsd = fit::rmsd_nofit(a.nsite, ref_bf, xs, ref_slt_w);
+    out = ((double)lwreg > rmsd || rmsd > (double)upreg) ? 1 : 0;
+  } else if (insposition >= ERMOD_INSPOS_SPHERE && insposition <= ERMOD_INSPOS_SLAB_SYMMETRIC) {
+    out = region_out(a, insposition, lwreg, upreg, k, molbeg, posraw, atom_mass, aggcen);
   }
+  if (!out && ck.insstructure == ERMOD_INSSTR_RMSD) {
+    // the solute's own structure against RefInfo's solute (engproc.F90:1277-1295)
+    const double rmsd = fit::rmsd_bestfit(a.nsite, ref_slt, xs, ref_slt_w);
+    out = ((double)ck.lwstr > rmsd || rmsd > (double)ck.upstr) ? 1 : 0;
+  }
+  skip[cnt] = out;
+}
+
+// relative_com of solute k against the aggregate centre and the sphere / slab window
+// (engproc.F90:1223-1247); 1 when the solute lies outside [lwreg, upreg]
+__device__ int region_out(const FrameArgs& a, int insposition, float lwreg, float upreg, int k,
+                          const int* __restrict__ molbeg, const float* __restrict__ posraw,
+                          const float* __restrict__ atom_mass, const double* __restrict__ aggcen) {
   double c[3] = {0.0, 0.0, 0.0}, msum = 0.0;
   for (int at = molbeg[k]; at < molbeg[k + 1]; ++at) {
     const double m = atom_mass[at];
@@ -361,13 +385,12 @@ __global__ void k_soln_region(FrameArgs a, int insposition, float lwreg, float u
     dist = (a.g.invcl[2][0] * dx[0] + a.g.invcl[2][1] * dx[1] + a.g.invcl[2][2] * dx[2]) * l3;
     if (insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) dist = fabsf(dist);
   }
-  skip[cnt] = (lwreg > dist || dist > upreg) ? 1 : 0;
+  return (lwreg > dist || dist > upreg) ? 1 : 0;
 }
 
-void launch_soln_region(const FrameArgs& a, const DeviceState& d, int insposition, float lwreg, float upreg,
-                        cudaStream_t s) {
-  k_soln_region<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, insposition, lwreg, upreg, d.tgt_mol, d.molbeg, d.posraw,
-                                                       d.atom_mass, d.aggcen, d.ref_bf, d.ref_slt_w, d.skip);
+void launch_soln_region(const FrameArgs& a, const DeviceState& d, const SolnCheck& ck, cudaStream_t s) {
+  k_soln_region<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, ck, d.tgt_mol, d.molbeg, d.posraw, d.atom_mass, d.aggcen,
+                                                       d.ref_bf, d.ref_slt, d.ref_slt_w, d.skip);
 }
 
 __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int iseed, InsRegion rg,

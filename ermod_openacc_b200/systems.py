@@ -309,7 +309,7 @@ def default_params(**kw) -> dict:
              iseed=123456789, temp=300.0 * KB_KCAL, elecut=12.0, lwljcut=10.0, upljcut=12.0, screen=0.35,
              ins_chunk=0, ecorr_batch=0, weight_bits=0, proposal=A.PROPOSAL_UNIFORM,
              keep_uvengy=0, ecorr_path=0, spectrum_path=0, graph_mode=0, stage_timing=0,
-             lwreg=0.0, upreg=0.0, hostspec=0)
+             lwreg=0.0, upreg=0.0, hostspec=0, insstructure=0, lwstr=0.0, upstr=0.0)
     p.update(kw)
     for k in ("ms2max", "ms3max"):
         if k not in kw:

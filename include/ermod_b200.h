@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define ERMOD_ABI_VERSION 2
+#define ERMOD_ABI_VERSION 3
 
 /* ---- status codes --------------------------------------------------- */
 #define ERMOD_OK               0
@@ -86,6 +86,8 @@ extern "C" {
 #define ERMOD_INSPOS_RMSD     5   /* translation within upreg + 3 r_max of the fitted reference, RMSD lwreg..upreg */
 #define ERMOD_INSPOS_GAUSS    6   /* uniform / Gaussian mixture around the fitted reference (experimental) */
 /* insposition 5 and 6 (insorigin 3) need ermod_set_refstructure before the first frame */
+#define ERMOD_INSSTR_NOREJECT 0   /* insstructure (engmain.F90) */
+#define ERMOD_INSSTR_RMSD     1
 #define ERMOD_INSROT_RANDOM   0
 #define ERMOD_INSROT_NOCHANGE 1
 
@@ -129,6 +131,12 @@ typedef struct ermod_params {
      com_aggregate insertion.F90:587-614), then shifted as insertion.F90:164-200 does. */
   float   lwreg, upreg;
   int32_t hostspec;               /* bit (sp - 1) set: solvent species sp (uvspec) belongs to the host */
+  /* structure check of solutes in solution (&ene_param insstructure, lwstr, upstr): with
+     ERMOD_INSSTR_RMSD a solute whose best-fit RMSD from RefInfo's solute lies outside
+     [lwstr, upstr] is skipped for the frame (check_mol_configuration, engproc.F90:1277-1295).
+     Refs mode ignores these: getsolute's filter acts on the conformations the host passes. */
+  int32_t insstructure;
+  float   lwstr, upstr;
 } ermod_params;
 
 /*

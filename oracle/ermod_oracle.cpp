@@ -335,6 +335,8 @@ template <class T> struct Oracle {
       return fail(ERMOD_ERR_ARG, "ins_reg");
     if (p.insposition >= ERMOD_INSPOS_RMSD && !(p.lwreg >= 0.f && p.upreg >= p.lwreg && p.upreg > 0.f))
       return fail(ERMOD_ERR_ARG, "ins_reg");
+    if (p.insstructure != ERMOD_INSSTR_NOREJECT && p.insstructure != ERMOD_INSSTR_RMSD)
+      return fail(ERMOD_ERR_ARG, "ins_str");
     return ERMOD_OK;
   }
 
@@ -1292,6 +1294,30 @@ template <class T> struct Oracle {
           if (p.insposition == ERMOD_INSPOS_SLAB_SYMMETRIC) dist = std::abs(dist);
         }
         skip[cnt] = ((T)p.lwreg > dist || dist > (T)p.upreg) ? 1 : 0;
+      }
+    }
+    if (!refs && p.insstructure == ERMOD_INSSTR_RMSD) {   // engproc.F90:1277-1295
+      if (ref_atom.empty()) return fail(ERMOD_ERR_ARG, "ins_ref");
+      const int ns = (int)ref_slt_w.size();
+      std::vector<double> cf(3 * ns), fo(3 * ns);
+      for (int cnt = 0; cnt < maxdst; ++cnt) {
+        if (skip[cnt]) continue;                            // the region check came first
+        const int a0 = molbeg[sltlist[cnt]];
+        for (int i = 0; i < 3 * ns; ++i) cf[i] = (double)sitepos[3 * a0 + i];
+        // rmsd_bestfit (bestfit.F90:339-346): fit, the fitted points stored as default reals
+        fit_rotate(ns, ref_slt.data(), cf.data(), ref_slt_w.data(), ns, cf.data(), fo.data());
+        double d = 0, ws = 0;
+        for (int a = 0; a < ns; ++a) {
+          double t = 0;
+          for (int k = 0; k < 3; ++k) {
+            const double x = (double)(float)fo[3 * a + k] - ref_slt[3 * a + k];
+            t += x * x;
+          }
+          d += ref_slt_w[a] * t;
+          ws += ref_slt_w[a];
+        }
+        const double rmsd = std::sqrt(d / ws);
+        skip[cnt] = ((double)p.lwstr > rmsd || rmsd > (double)p.upstr) ? 1 : 0;
       }
     }
     // PME setup (engconst :419-437)

@@ -99,3 +99,42 @@ def soln_multi_system(seed=11):
     pos = np.concatenate([centres, wat.reshape(-1, 3)], axis=0)
     cell = np.diag([box] * 3).astype(np.float32)
     return prm, topo, {}, A.as_f32(pos.ravel()), A.as_f32(cell.ravel(order="F")), SOLN_SOLUTE_OFFSETS
+
+
+def soln_struct_system(stretch=(1.0, 1.05, 1.3, 1.6), seed=11):
+    """Solutes in solution with four water-shaped 3-site solutes whose two O-H bonds are
+    stretched by `stretch`, each turned by its own rotation, at SOLN_SOLUTE_OFFSETS in the 8^3
+    water box, for check_mol_configuration's structure test: (params, topo, hist, sitepos,
+    cell, ideal solute coordinates [3, 3], solute weights)."""
+    nside, box, K = 8, 24.9, 32
+    c0 = np.full(3, box / 2)
+    centres = c0 + SOLN_SOLUTE_OFFSETS
+    wat = S.water_box_frame(nside, box, seed).T.reshape(-1, 3, 3)
+    for c in centres:
+        for i in range(len(wat)):
+            d = wat[i, 0] - c
+            d -= box * np.round(d / box)
+            r = np.linalg.norm(d)
+            if r < 3.5:
+                wat[i] += d / max(r, 1e-6) * (3.5 - r)
+    w = S.water()
+    ideal = w.coords.T.copy()                       # O at the origin, H1, H2
+    rng = np.random.default_rng(seed + 1)
+    slts = []
+    for c, s in zip(centres, stretch):
+        g = ideal.copy()
+        g[1:] *= s
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        a, b, cc, d = q
+        R = np.array([[a * a + b * b - cc * cc - d * d, 2 * (b * cc - a * d), 2 * (b * d + a * cc)],
+                      [2 * (b * cc + a * d), a * a - b * b + cc * cc - d * d, 2 * (cc * d - a * b)],
+                      [2 * (b * d - a * cc), 2 * (cc * d + a * b), a * a - b * b - cc * cc + d * d]])
+        slts.append((g - g.mean(axis=0)) @ R.T + c)
+    solute = S.Species("wshape", w.charge, w.sigma, w.eps, w.mass, w.coords)
+    topo = S.Topology([solute, S.water()], [len(centres), nside ** 3], [A.PT_SOLUTE, A.PT_SOLVENT])
+    prm = S.default_params(slttype=A.SLT_SOLN, ms1max=K, maxins=1, corrcal=0, wgtslf=0, hostspec=2)
+    pos = np.concatenate([np.concatenate(slts, axis=0), wat.reshape(-1, 3)], axis=0)
+    cell = np.diag([box] * 3).astype(np.float32)
+    return (prm, topo, {}, A.as_f32(pos.ravel()), A.as_f32(cell.ravel(order="F")), ideal,
+            np.asarray(w.mass, dtype=np.float64))

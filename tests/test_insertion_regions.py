@@ -216,6 +216,62 @@ def test_soln_rmsd_check(oracle_mod):
     assert orc.accum()["engsmpl"] == 1
 
 
+def _structure_case(lw, up, **extra):
+    from _helpers import soln_struct_system
+    prm, topo, hist, pos, cell, ideal, wts = soln_struct_system()
+    xyz = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    water = xyz[12:]
+    prm = dict(prm, insstructure=A.INSSTR_RMSD, lwstr=lw, upstr=up, keep_uvengy=1, **extra)
+    ref = dict(refspec=2, host_crd=water.ravel(), host_w=np.ones(len(water)), slt_crd=ideal.ravel(), slt_w=wts)
+    return prm, topo, hist, pos, cell, ref, xyz[:12].reshape(4, 3, 3), ideal, wts
+
+
+def _kabsch(ref, x, w):
+    cr = (w[:, None] * ref).sum(0) / w.sum()
+    cx = (w[:, None] * x).sum(0) / w.sum()
+    U, _, Vt = np.linalg.svd(((x - cx) * w[:, None]).T @ (ref - cr))
+    R = Vt.T @ np.diag([1.0, 1.0, np.sign(np.linalg.det(Vt.T @ U.T))]) @ U.T
+    return float(np.sqrt((w * (((x - cx) @ R.T + cr - ref) ** 2).sum(1)).sum() / w.sum()))
+
+
+def test_soln_structure_check(oracle_mod):
+    """insstructure 1 in solution: a solute whose best-fit RMSD from RefInfo's solute lies
+    outside lwstr..upstr is skipped for the frame (engproc.F90:1277-1295)."""
+    prm, topo, hist, pos, cell, ref, slts, ideal, wts = _structure_case(0.0, 0.05)
+    rms = np.array([_kabsch(ideal, g, wts) for g in slts])     # mass weights: 0, 0.016, 0.094, 0.188
+    keep = (rms >= 0.0) & (rms <= 0.05)
+    assert keep.tolist() == [True, True, False, False]
+    assert np.all(np.abs(rms - 0.05) > 0.03)
+    orc = oracle_mod.Oracle(prm, topo, hist)
+    assert orc.engconst(1, pos, cell) < 0                       # RefInfo is required
+    assert orc.last_error() == "ins_ref"
+    orc = oracle_mod.Oracle(prm, topo, hist)
+    orc.set_refstructure(**ref)
+    assert orc.engconst(1, pos, cell) >= 0
+    u, _ = orc.uvengy()
+    np.testing.assert_array_equal(np.any(u != 0.0, axis=1), keep)
+    assert orc.accum()["engsmpl"] == keep.sum()
+    # lower bound only: the two distorted solutes
+    prm2, *_ = _structure_case(0.05, 10.0)
+    orc = oracle_mod.Oracle(prm2, topo, hist)
+    orc.set_refstructure(**ref)
+    assert orc.engconst(1, pos, cell) >= 0
+    np.testing.assert_array_equal(np.any(orc.uvengy()[0] != 0.0, axis=1), ~keep)
+    # with the sphere window as well: both checks apply (the region first)
+    prm3, *_ = _structure_case(0.0, 0.05, insposition=A.INSPOS_SPHERE, lwreg=0.0, upreg=3.0)
+    orc = oracle_mod.Oracle(prm3, topo, hist)
+    orc.set_refstructure(**ref)
+    assert orc.engconst(1, pos, cell) >= 0
+    near = np.linalg.norm(slts.mean(axis=1) - 24.9 / 2, axis=1) < 3.0
+    np.testing.assert_array_equal(np.any(orc.uvengy()[0] != 0.0, axis=1), keep & near)
+
+
+def test_unknown_insstructure_is_refused(oracle_mod):
+    prm, topo, hist, *_ = _structure_case(0.0, 0.1)
+    with pytest.raises(RuntimeError, match="ins_str"):
+        oracle_mod.Oracle(dict(prm, insstructure=2), topo, hist)
+
+
 def test_refstructure_is_required(oracle_mod):
     w = S.make_workload(2, small=True, maxins=8)
     prm = dict(w.params, insposition=A.INSPOS_RMSD, lwreg=0.0, upreg=4.0)

@@ -180,6 +180,30 @@ def test_soln_rmsd_check_matches_oracle(lib, oracle_mod):
     assert eng.accum()["engsmpl"] == orc.accum()["engsmpl"] == 1
 
 
+@pytest.mark.parametrize("lw,up,region", [(0.0, 0.05, False), (0.05, 10.0, False), (0.0, 0.05, True)])
+def test_soln_structure_check_matches_oracle(lib, oracle_mod, lw, up, region):
+    """insstructure 1 in solution (engproc.F90:1277-1295): the same solutes kept as the
+    oracle, with the same energies; with the sphere window both checks apply."""
+    from test_insertion_regions import _structure_case
+    extra = dict(insposition=A.INSPOS_SPHERE, lwreg=0.0, upreg=3.0) if region else {}
+    prm, topo, hist, pos, cell, ref, slts, ideal, wts = _structure_case(lw, up, **extra)
+    eng = Engine(prm, topo, hist)
+    with pytest.raises(ErmodError, match="ins_ref"):
+        eng.engconst(1, pos, cell)
+    eng.set_refstructure(**ref)
+    orc = oracle_mod.Oracle(prm, topo, hist)
+    orc.set_refstructure(**ref)
+    assert eng.engconst(1, pos, cell) >= 0
+    assert orc.engconst(1, pos, cell) >= 0
+    u, _ = eng.uvengy()
+    uo, _ = orc.uvengy()
+    kept = np.any(uo != 0.0, axis=1)
+    assert 0 < kept.sum() < len(kept)
+    np.testing.assert_array_equal(np.any(u != 0.0, axis=1), kept)
+    check_energies(u, uo)
+    assert eng.accum()["engsmpl"] == orc.accum()["engsmpl"] == kept.sum()
+
+
 def test_slab_insertion_needs_a_periodic_cell(lib):
     w = S.make_workload(2, small=True, maxins=8)
     prm = dict(w.params, insposition=A.INSPOS_SLAB_SYMMETRIC, lwreg=1.0, upreg=3.0, hostspec=1,
