@@ -122,7 +122,7 @@ def ptr(a, ctype):
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libermod_b200.so")
 
-# Every symbol include/ermod_b200.h and include/ermod_io.h declare, with its ctypes signature.
+# Every symbol include/*.h declares, with its ctypes signature.
 SIGNATURES = {
     "ermod_abi_version": (C.c_int32, []),
     "ermod_enginit_mesh": (C.c_int32, [C.POINTER(ErmodHist), C.c_int32, _f64p, _i32p, _i32p, _f64p, _i32p, _i32p]),
@@ -174,6 +174,10 @@ SIGNATURES = {
     "ermod_io_format": (C.c_int32, [C.c_int32, C.c_double, C.c_int32, C.c_int32, C.c_char_p, C.c_int32]),
     "ermod_io_last_error": (C.c_char_p, []),
     "ermod_rmsd_bestfit": (C.c_double, [C.c_int32, _f32p, _f32p, _f32p]),
+    # include/ermod_slvfe.h
+    "ermod_slvfe_delta_mu": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, _f64p, _f64p, _f64p, _f64p, _i32p,
+                                         C.c_double, _f64p, C.c_double, _f64p, _f64p]),
+    "ermod_slvfe_last_error": (C.c_char_p, []),
 }
 
 NOALLOC_SCRATCH_BYTES = 32 << 20

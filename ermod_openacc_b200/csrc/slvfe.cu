@@ -1,0 +1,501 @@
+// slvfe.cu -- slvfe's free-energy functional (chmpot) for one data set on the GPU, in FP64,
+// with slvfe's default options (sfemain.F90:22-64): py-hnc, regularised Cholesky solve of
+// the reference-solvent equation, eczr zero shift, harmonic extrapolation weights, linear
+// extrapolation of omega in solution, normalize 'yes', no bin merging.
+//
+//   k_slv_prep     distnorm's per-species scaling of rho / rho0 (slvfe.F90:1467-1502) and
+//                  omega in solution where both distributions are sampled (getslncv :875-930)
+//   k_slv_distnorm the chi0 row scaling (slvfe.F90:1503-1525): Gauss-Seidel sweeps over the
+//                  bins in one CTA, each bin's correction from the corrections already
+//                  updated in this sweep, to 1e-8 within 100 sweeps
+//   k_slv_extrap   omega in solution for bins sampled on one side only (:930-1001): a
+//                  weighted linear fit over the species' sampled bins, a thread per bin
+//   k_slv_reg      the per-species regularisation trace / count^2 (getinscv :1003-1120)
+//   k_slv_build    A = chi0 - rho0 rho0^T (+ reg per species block, 1 on unsampled
+//                  diagonals), padded to a multiple of the tile with the identity
+//   k_chol_*       blocked right-looking Cholesky of A (32 x 32 FP64 tiles: diagonal
+//                  factor, panel solve, trailing update)
+//   k_slv_solve    forward and backward substitution for the reference-solvent omega
+//   k_slv_chmpot   the eczr zero shift, the functional and its per-species sums (:744-803)
+//
+// Every reduction is a fixed-order tree, so a run is reproducible bit for bit.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/ermod_slvfe.h"
+
+namespace {
+
+constexpr int kTile = 32;
+constexpr int kNT = 1024;          // threads of the single-CTA kernels
+constexpr int kMaxSpecies = 16;
+constexpr double kTol = 1.0e-8;    // distnorm convergence (slvfe.F90:1520)
+constexpr int kItrMax = 100;
+constexpr double kTiny = 1.0e-8;   // zero-bin tie (slvfe.F90:1180)
+
+enum : int { kOk = 0, kErrNorm = 1, kErrExtrap = 2, kErrChol = 3, kErrZero = 4 };
+
+thread_local const char* g_err = "";
+
+// the first failing step's code stays: later kernels run on, as the host learns of it only at the end
+__device__ void set_status(int* st, int code) { atomicCAS(st, 0, code); }
+
+__device__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// fixed-order sum of one value per thread of a kNT-thread block
+__device__ double block_sum(double v, double* sh) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double r = l < kNT / 32 ? sh[l] : 0.0;
+    r = warp_sum(r);
+    if (l == 0) sh[0] = r;
+  }
+  __syncthreads();
+  return sh[0];
+}
+
+__device__ double block_max(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double r = l < kNT / 32 ? sh[l] : -INFINITY;
+    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+    if (l == 0) sh[0] = r;
+  }
+  __syncthreads();
+  return sh[0];
+}
+
+__device__ double block_min(double v, double* sh) { return -block_max(-v, sh); }
+
+struct SlvArgs {
+  int n, nsp;
+  double kT;
+  const double* rd;     // rho in solution as read (engstore-normalised)
+  const double* rr;     // rho0 in the reference solvent as read
+  const double* crd;    // bin coordinates (engsln's bin_middle)
+  const int* spec;      // 1-based species of each bin
+  double* rho;          // scaled rho
+  double* rho0;         // scaled rho0
+  double* nummol;       // [nsp] molecules per species
+  double* omega;        // omega in solution
+  int* both;            // 1: sampled in both systems
+  double* harm;         // rho rho0 / (rho + rho0)
+  double* reg;          // [nsp]
+  int* status;
+};
+
+// ---- distnorm's scaling and the directly sampled omega -------------------------------
+__global__ void __launch_bounds__(kNT) k_slv_prep(SlvArgs a) {
+  __shared__ double sh[32];
+  const int n = a.n;
+  for (int p = 1; p <= a.nsp; ++p) {
+    double s = 0.0, s0 = 0.0;
+    for (int i = threadIdx.x; i < n; i += kNT)
+      if (a.spec[i] == p) { s += a.rd[i]; s0 += a.rr[i]; }
+    s = block_sum(s, sh);
+    s0 = block_sum(s0, sh);
+    const double nm = rint(s);
+    if (threadIdx.x == 0) a.nummol[p - 1] = nm;
+    const double f = s > 0.0 ? nm / s : 0.0, f0 = s0 > 0.0 ? nm / s0 : 0.0;
+    for (int i = threadIdx.x; i < n; i += kNT)
+      if (a.spec[i] == p) { a.rho[i] = a.rd[i] * f; a.rho0[i] = a.rr[i] * f0; }
+  }
+  __syncthreads();
+  double mn = INFINITY, mn0 = INFINITY;
+  for (int i = threadIdx.x; i < n; i += kNT) {
+    if (a.rd[i] > 0.0) mn = fmin(mn, a.rd[i]);
+    if (a.rr[i] > 0.0) mn0 = fmin(mn0, a.rr[i]);
+  }
+  mn = block_min(mn, sh);
+  mn0 = block_min(mn0, sh);
+  for (int i = threadIdx.x; i < n; i += kNT) {
+    const double r = a.rho[i], r0 = a.rho0[i];
+    const double rs = fmin(r / mn, 10.0), rr = fmin(r0 / mn0, 10.0);
+    const int b = (rint(rs) >= 1.0 && rint(rr) >= 1.0) ? 1 : 0;
+    a.both[i] = b;
+    a.omega[i] = b ? -a.kT * log(r / r0) - a.crd[i] : 0.0;
+    const double hs = r + r0;
+    a.harm[i] = hs > 0.0 ? r * r0 / hs : 0.0;
+  }
+}
+
+// ---- chi0 row scaling: Gauss-Seidel sweeps in one CTA --------------------------------
+__global__ void __launch_bounds__(kNT) k_slv_distnorm(SlvArgs a, double* __restrict__ chi) {
+  extern __shared__ double corr[];            // [n]
+  __shared__ double part[32 * kMaxSpecies];
+  __shared__ double sh[32];
+  const int n = a.n, nsp = a.nsp;
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < n; i += kNT) corr[i] = 1.0;
+  __syncthreads();
+  for (int it = 0;; ++it) {
+    for (int i = 0; i < n; ++i) {
+      const double* col = chi + (size_t)i * n;
+      double acc[kMaxSpecies];
+      for (int p = 0; p < nsp; ++p) acc[p] = 0.0;
+      for (int j = threadIdx.x; j < n; j += kNT) {
+        const double v = corr[j] * col[j];
+        const int p = a.spec[j] - 1;
+        for (int q = 0; q < nsp; ++q) acc[q] += q == p ? v : 0.0;
+      }
+      for (int p = 0; p < nsp; ++p) {
+        const double v = warp_sum(acc[p]);
+        if (l == 0) part[w * kMaxSpecies + p] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int p = 0; p < nsp; ++p) {
+          double d = 0.0;
+          for (int q = 0; q < kNT / 32; ++q) d += part[q * kMaxSpecies + p];
+          if (d > 0.0) s += a.nummol[p] / d;
+        }
+        corr[i] = s / nsp * a.rho0[i];
+      }
+      __syncthreads();
+    }
+    // chi *= corr corr^T
+    for (size_t e = threadIdx.x; e < (size_t)n * n; e += kNT) {
+      const int r = (int)(e % n), c = (int)(e / n);
+      chi[e] *= corr[r] * corr[c];
+    }
+    double err = 0.0;
+    for (int i = threadIdx.x; i < n; i += kNT)
+      if (a.rho0[i] > 0.0) err = fmax(err, fabs(corr[i] - 1.0));
+    err = block_max(err, sh);
+    if (err <= kTol) return;
+    if (it + 1 >= kItrMax) {
+      if (threadIdx.x == 0) set_status(a.status, kErrNorm);
+      return;
+    }
+  }
+}
+
+// ---- omega in solution where one distribution is empty: weighted linear fit ----------
+__global__ void k_slv_extrap(SlvArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  if (i >= n || a.both[i]) return;
+  if (a.rho[i] <= 0.0) { a.omega[i] = 0.0; return; }
+  const int sp = a.spec[i];
+  auto same = [&](int k) { return a.spec[k] == sp && a.both[k]; };
+  int m = 0, k = n - 1;
+  for (int q = i - 1; q >= 0; --q) if (same(q)) { m = q; break; }
+  for (int q = i + 1; q < n; ++q) if (same(q)) { k = q; break; }
+  int j;
+  if (a.both[m] && a.both[k]) j = abs(m - i) < abs(k - i) ? m : k;
+  else if (a.both[m] || a.both[k]) j = a.both[m] ? m : k;
+  else { set_status(a.status, kErrExtrap); return; }
+  const double kT = a.kT, cj = a.crd[j], ci = a.crd[i];
+  double wsum = 0.0;
+  for (int q = 0; q < n; ++q) {
+    if (!same(q)) continue;
+    double sh = a.crd[q] - cj;
+    if (q < i) sh = -sh - 2.0 * (cj - ci);
+    const double wq = exp(-sh / kT) * a.harm[q];
+    if (wq > 0.0) wsum += wq;
+  }
+  double m1 = 0.0, m2 = 0.0, my = 0.0, mxy = 0.0;
+  for (int q = 0; q < n; ++q) {
+    if (!same(q)) continue;
+    double sh = a.crd[q] - cj;
+    if (q < i) sh = -sh - 2.0 * (cj - ci);
+    double wq = exp(-sh / kT) * a.harm[q];
+    if (!(wq > 0.0)) continue;
+    wq /= wsum;
+    const double x = a.crd[q], y = a.omega[q];
+    m1 += wq * x; m2 += wq * x * x; my += wq * y; mxy += wq * x * y;
+  }
+  const double den = m2 - m1 * m1;
+  const double c0 = (m2 * my - m1 * mxy) / den, c1 = (mxy - m1 * my) / den;
+  a.omega[i] = c0 + c1 * ci;
+}
+
+// ---- regularisation per species: trace of the sampled block / count^2 ----------------
+__global__ void __launch_bounds__(kNT) k_slv_reg(SlvArgs a, const double* __restrict__ chi) {
+  __shared__ double sh[32];
+  const int n = a.n;
+  for (int p = 1; p <= a.nsp; ++p) {
+    double t = 0.0, c = 0.0;
+    for (int i = threadIdx.x; i < n; i += kNT)
+      if (a.spec[i] == p && a.rho0[i] > 0.0) {
+        t += chi[(size_t)i * n + i] - a.rho0[i] * a.rho0[i];
+        c += 1.0;
+      }
+    t = block_sum(t, sh);
+    c = block_sum(c, sh);
+    if (threadIdx.x == 0) a.reg[p - 1] = c > 0.0 ? t / (c * c) : 0.0;
+  }
+}
+
+// ---- the padded system matrix and right-hand side ------------------------------------
+__global__ void k_slv_build(SlvArgs a, const double* __restrict__ chi, int N, double* __restrict__ A,
+                            double* __restrict__ b) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)N * N) return;
+  const int r = (int)(e % N), c = (int)(e / N);   // column-major
+  const int n = a.n;
+  double v;
+  if (r >= n || c >= n) {
+    v = r == c ? 1.0 : 0.0;
+  } else {
+    const bool pr = a.rho0[r] > 0.0, pc = a.rho0[c] > 0.0;
+    if (pr && pc) {
+      v = chi[(size_t)c * n + r] - a.rho0[r] * a.rho0[c];
+      if (a.spec[r] == a.spec[c]) v += a.reg[a.spec[r] - 1];
+    } else {
+      v = r == c ? 1.0 : 0.0;
+    }
+  }
+  A[e] = v;
+  if (c == 0) b[r] = (r < n && a.rho0[r] > 0.0) ? -a.kT * (a.rho[r] - a.rho0[r]) : 0.0;
+}
+
+// ---- blocked Cholesky, lower, column-major, 32 x 32 tiles ----------------------------
+__global__ void __launch_bounds__(kTile * kTile) k_chol_diag(double* __restrict__ A, int N, int kt, int* status) {
+  __shared__ double t[kTile][kTile + 1];
+  const int r = threadIdx.x % kTile, c = threadIdx.x / kTile, k0 = kt * kTile;
+  t[r][c] = A[(size_t)(k0 + c) * N + k0 + r];
+  __syncthreads();
+  for (int j = 0; j < kTile; ++j) {
+    if (r == j && c == j) {
+      const double d = t[j][j];
+      if (!(d > 0.0)) set_status(status, kErrChol);
+      t[j][j] = sqrt(fmax(d, 1e-300));
+    }
+    __syncthreads();
+    if (c == j && r > j) t[r][j] /= t[j][j];
+    __syncthreads();
+    if (c > j && r >= c) t[r][c] -= t[r][j] * t[c][j];
+    __syncthreads();
+  }
+  if (r >= c) A[(size_t)(k0 + c) * N + k0 + r] = t[r][c];
+}
+
+// tiles below the diagonal: X L_kk^T = A_ik, a thread per row of the tile
+__global__ void __launch_bounds__(kTile) k_chol_panel(double* __restrict__ A, int N, int kt) {
+  __shared__ double L[kTile][kTile + 1];
+  const int r = threadIdx.x, k0 = kt * kTile, i0 = (kt + 1 + blockIdx.x) * kTile;
+  for (int c = 0; c < kTile; ++c) L[r][c] = A[(size_t)(k0 + c) * N + k0 + r];
+  __syncthreads();
+  double x[kTile];
+  for (int c = 0; c < kTile; ++c) x[c] = A[(size_t)(k0 + c) * N + i0 + r];
+  for (int c = 0; c < kTile; ++c) {
+    double v = x[c];
+    for (int l = 0; l < c; ++l) v -= x[l] * L[c][l];
+    x[c] = v / L[c][c];
+  }
+  for (int c = 0; c < kTile; ++c) A[(size_t)(k0 + c) * N + i0 + r] = x[c];
+}
+
+// trailing update A_ij -= A_ik A_jk^T for the lower tiles i >= j > k
+__global__ void __launch_bounds__(kTile * kTile) k_chol_update(double* __restrict__ A, int N, int kt) {
+  __shared__ double P[kTile][kTile + 1], Q[kTile][kTile + 1];
+  // blockIdx.x enumerates the lower-triangle tile pairs (i, j), j <= i, of the trailing matrix
+  int b = blockIdx.x, j = 0;
+  const int m = N / kTile - kt - 1;
+  while (b >= m - j) { b -= m - j; ++j; }
+  const int i = j + b;
+  const int r = threadIdx.x % kTile, c = threadIdx.x / kTile;
+  const int k0 = kt * kTile, i0 = (kt + 1 + i) * kTile, j0 = (kt + 1 + j) * kTile;
+  P[r][c] = A[(size_t)(k0 + c) * N + i0 + r];
+  Q[r][c] = A[(size_t)(k0 + c) * N + j0 + r];
+  __syncthreads();
+  double s = 0.0;
+  for (int l = 0; l < kTile; ++l) s += P[r][l] * Q[c][l];
+  A[(size_t)(j0 + c) * N + i0 + r] -= s;
+}
+
+// ---- L L^T x = b, one CTA: tiles of forward then backward substitution ---------------
+__global__ void __launch_bounds__(kNT) k_slv_solve(const double* __restrict__ A, int N, double* __restrict__ b) {
+  __shared__ double xs[kTile];
+  const int nt = N / kTile;
+  for (int kt = 0; kt < nt; ++kt) {      // L y = b
+    const int k0 = kt * kTile;
+    if (threadIdx.x == 0)
+      for (int c = 0; c < kTile; ++c) {
+        double v = b[k0 + c];
+        for (int l = 0; l < c; ++l) v -= A[(size_t)(k0 + l) * N + k0 + c] * xs[l];
+        xs[c] = v / A[(size_t)(k0 + c) * N + k0 + c];
+        b[k0 + c] = xs[c];
+      }
+    __syncthreads();
+    for (int r = k0 + kTile + threadIdx.x; r < N; r += kNT) {
+      double v = 0.0;
+      for (int l = 0; l < kTile; ++l) v += A[(size_t)(k0 + l) * N + r] * xs[l];
+      b[r] -= v;
+    }
+    __syncthreads();
+  }
+  for (int kt = nt - 1; kt >= 0; --kt) { // L^T x = y
+    const int k0 = kt * kTile;
+    if (threadIdx.x == 0)
+      for (int c = kTile - 1; c >= 0; --c) {
+        double v = b[k0 + c];
+        for (int l = c + 1; l < kTile; ++l) v -= A[(size_t)(k0 + c) * N + k0 + l] * xs[l];
+        xs[c] = v / A[(size_t)(k0 + c) * N + k0 + c];
+        b[k0 + c] = xs[c];
+      }
+    __syncthreads();
+    for (int r = threadIdx.x; r < k0; r += kNT) {   // row r of L^T is column r of L
+      double v = 0.0;
+      for (int l = 0; l < kTile; ++l) v += A[(size_t)r * N + k0 + l] * xs[l];
+      b[r] -= v;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ double pyhnc_soln(double f) { return f < 0.0 ? f + f / (exp(-f) - 1.0) + 1.0 : f / 2.0; }
+__device__ double pyhnc_refs(double f) { return f < 0.0 ? log1p(-f) * (1.0 / f - 1.0) + 1.0 : f / 2.0; }
+
+// ---- eczr zero shift, the functional and its per-species sums ------------------------
+__global__ void __launch_bounds__(kNT) k_slv_chmpot(SlvArgs a, const double* __restrict__ x,
+                                                    const double* __restrict__ aveuv, double* __restrict__ chmpt) {
+  __shared__ double sh[32];
+  __shared__ double zx[kMaxSpecies];
+  const int n = a.n;
+  if (threadIdx.x < a.nsp) {   // the last bin pair of the species around zero energy
+    const int p = threadIdx.x + 1;
+    int k = -1, prev = -1;
+    for (int q = 0; q < n; ++q) {
+      if (a.spec[q] != p) continue;
+      if (prev >= 0 && q == prev + 1 && a.crd[prev] <= 0.0 && 0.0 <= a.crd[q]) {
+        const double lo = fabs(a.crd[prev]), hi = a.crd[q];
+        if (hi > lo + kTiny) k = prev;
+        else if (hi < lo - kTiny) k = q;
+        else k = a.rho0[prev] >= a.rho0[q] ? prev : q;
+      }
+      prev = q;
+    }
+    if (k < 0) set_status(a.status, kErrZero);
+    zx[threadIdx.x] = k >= 0 ? x[k] : 0.0;
+  }
+  __syncthreads();
+  const double kT = a.kT;
+  for (int p = 1; p <= a.nsp; ++p) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += kNT) {
+      if (a.spec[i] != p) continue;
+      const double r = a.rho[i], r0 = a.rho0[i];
+      if (!(r > 0.0 || r0 > 0.0)) continue;
+      const double om0 = (r0 > 0.0 ? -kT * (r - r0) / r0 - x[i] : 0.0) + zx[p - 1];
+      const double hs = r + r0;
+      const double wt = r >= r0 ? 1.0 : 1.0 - ((r - r0) / (hs > 0.0 ? hs : 1.0)) * ((r - r0) / (hs > 0.0 ? hs : 1.0));
+      const double fac = wt * pyhnc_soln(a.omega[i] / kT) + (1.0 - wt) * pyhnc_refs(om0 / kT);
+      const double lcent = -(a.omega[i] + a.crd[i]);
+      s += -kT * (r - r0) + lcent * r + kT * fac * (r - r0);
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) chmpt[p - 1] = s + aveuv[p - 1];
+  }
+}
+
+int fail(int code, const char* name) {
+  g_err = name;
+  return code;
+}
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n) { return cudaMalloc((void**)p, sizeof(T) * (n ? n : 1)); }
+
+}  // namespace
+
+extern "C" const char* ermod_slvfe_last_error(void) { return g_err; }
+
+extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n, int32_t nsp, const double* rho_sln,
+                                        const double* rho_ref, const double* chi_ref, const double* crd,
+                                        const int32_t* spec, double kT, const double* aveuv, double slfeng,
+                                        double* chmpt, double* total) {
+  if (n < 2 || nsp < 1 || nsp > kMaxSpecies || !rho_sln || !rho_ref || !chi_ref || !crd || !spec || !aveuv ||
+      !chmpt || !(kT > 0.0))
+    return fail(ERMOD_ERR_ARG, "slv_arg");
+  for (int i = 0; i < n; ++i)
+    if (spec[i] < 1 || spec[i] > nsp) return fail(ERMOD_ERR_ARG, "slv_arg");
+  if ((size_t)n * sizeof(double) > 160 * 1024) return fail(ERMOD_ERR_ARG, "slv_siz");   // corr in shared memory
+  if (cudaSetDevice(device) != cudaSuccess) return fail(ERMOD_ERR_CUDA, "slv_cud");
+  const int N = (n + kTile - 1) / kTile * kTile;
+  const size_t nn = (size_t)n * n, NN = (size_t)N * N;
+  double *d_rd = nullptr, *d_rr = nullptr, *d_crd = nullptr, *d_chi = nullptr, *d_rho = nullptr, *d_rho0 = nullptr;
+  double *d_nm = nullptr, *d_om = nullptr, *d_harm = nullptr, *d_reg = nullptr, *d_A = nullptr, *d_b = nullptr;
+  double *d_av = nullptr, *d_out = nullptr;
+  int *d_spec = nullptr, *d_both = nullptr, *d_st = nullptr;
+  cudaStream_t st = nullptr;
+  int rc = ERMOD_OK;
+  auto cleanup = [&]() {
+    for (void* p : {(void*)d_rd, (void*)d_rr, (void*)d_crd, (void*)d_chi, (void*)d_rho, (void*)d_rho0, (void*)d_nm,
+                    (void*)d_om, (void*)d_harm, (void*)d_reg, (void*)d_A, (void*)d_b, (void*)d_av, (void*)d_out,
+                    (void*)d_spec, (void*)d_both, (void*)d_st})
+      if (p) cudaFree(p);
+    if (st) cudaStreamDestroy(st);
+  };
+  bool ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && dalloc(&d_rd, n) == cudaSuccess && dalloc(&d_rr, n) == cudaSuccess && dalloc(&d_crd, n) == cudaSuccess;
+  ok = ok && dalloc(&d_chi, nn) == cudaSuccess && dalloc(&d_rho, n) == cudaSuccess && dalloc(&d_rho0, n) == cudaSuccess;
+  ok = ok && dalloc(&d_nm, nsp) == cudaSuccess && dalloc(&d_om, n) == cudaSuccess && dalloc(&d_harm, n) == cudaSuccess;
+  ok = ok && dalloc(&d_reg, nsp) == cudaSuccess && dalloc(&d_A, NN) == cudaSuccess && dalloc(&d_b, N) == cudaSuccess;
+  ok = ok && dalloc(&d_av, nsp) == cudaSuccess && dalloc(&d_out, nsp) == cudaSuccess;
+  ok = ok && dalloc(&d_spec, n) == cudaSuccess && dalloc(&d_both, n) == cudaSuccess && dalloc(&d_st, 1) == cudaSuccess;
+  if (!ok) { cleanup(); return fail(ERMOD_ERR_CUDA, "slv_mem"); }
+  ok = cudaMemcpyAsync(d_rd, rho_sln, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_rr, rho_ref, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_crd, crd, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_chi, chi_ref, 8 * nn, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_spec, spec, 4 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_av, aveuv, 8 * nsp, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemsetAsync(d_st, 0, sizeof(int), st) == cudaSuccess;
+  SlvArgs a{n, nsp, kT, d_rd, d_rr, d_crd, d_spec, d_rho, d_rho0, d_nm, d_om, d_both, d_harm, d_reg, d_st};
+  const size_t corr_smem = (size_t)n * sizeof(double);
+  if (ok && corr_smem > 48 * 1024)
+    ok = cudaFuncSetAttribute(k_slv_distnorm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)corr_smem) ==
+         cudaSuccess;
+  if (ok) {
+    k_slv_prep<<<1, kNT, 0, st>>>(a);
+    k_slv_distnorm<<<1, kNT, corr_smem, st>>>(a, d_chi);
+    k_slv_extrap<<<(n + 127) / 128, 128, 0, st>>>(a);
+    k_slv_reg<<<1, kNT, 0, st>>>(a, d_chi);
+    k_slv_build<<<(unsigned)((NN + 255) / 256), 256, 0, st>>>(a, d_chi, N, d_A, d_b);
+    const int nt = N / kTile;
+    for (int kt = 0; kt < nt; ++kt) {
+      k_chol_diag<<<1, kTile * kTile, 0, st>>>(d_A, N, kt, d_st);
+      const int m = nt - kt - 1;
+      if (m > 0) {
+        k_chol_panel<<<m, kTile, 0, st>>>(d_A, N, kt);
+        k_chol_update<<<m * (m + 1) / 2, kTile * kTile, 0, st>>>(d_A, N, kt);
+      }
+    }
+    k_slv_solve<<<1, kNT, 0, st>>>(d_A, N, d_b);
+    k_slv_chmpot<<<1, kNT, 0, st>>>(a, d_b, d_av, d_out);
+    ok = cudaGetLastError() == cudaSuccess;
+  }
+  int status = 0;
+  ok = ok && cudaMemcpyAsync(&status, d_st, sizeof(int), cudaMemcpyDeviceToHost, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(chmpt, d_out, 8 * nsp, cudaMemcpyDeviceToHost, st) == cudaSuccess;
+  ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
+  if (!ok) rc = fail(ERMOD_ERR_CUDA, "slv_cud");
+  else if (status == kErrNorm) rc = fail(ERMOD_ERR_SLVFE, "slv_nrm");
+  else if (status == kErrExtrap) rc = fail(ERMOD_ERR_SLVFE, "slv_ext");
+  else if (status == kErrChol) rc = fail(ERMOD_ERR_SLVFE, "slv_chl");
+  else if (status == kErrZero) rc = fail(ERMOD_ERR_SLVFE, "slv_zer");
+  if (rc == ERMOD_OK && total) {
+    double s = slfeng;
+    for (int p = 0; p < nsp; ++p) s += chmpt[p];
+    *total = s;
+  }
+  cleanup();
+  return rc;
+}

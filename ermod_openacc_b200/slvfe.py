@@ -25,8 +25,8 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["kT_of", "delta_mu", "representative_bins", "read_engfile", "read_corfile", "read_table",
-           "delta_mu_from_files"]
+__all__ = ["kT_of", "delta_mu", "delta_mu_gpu", "representative_bins", "read_engfile", "read_corfile",
+           "read_table", "delta_mu_from_files"]
 
 
 def kT_of(temp_K: float) -> float:
@@ -259,6 +259,32 @@ def read_table(path) -> np.ndarray:
                 except ValueError:
                     continue   # a text header line (uvrange.tt)
     return np.array(rows)
+
+
+def delta_mu_gpu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0,
+                 device: int = 0):
+    """delta_mu on the GPU (include/ermod_slvfe.h): the same functional, options and
+    arguments, FP64 CUDA kernels.  Raises RuntimeError with slvfe's failure name; there is
+    no eigenvalue fallback on this path."""
+    import ctypes as C
+    from . import _capi as A
+    lib = A.load_library()
+    rd = A.as_f64(edist)
+    rr = A.as_f64(edens)
+    chi = np.asfortranarray(np.asarray(ecorr, dtype=np.float64))
+    crd = A.as_f64(uvcrd)
+    spec = np.ascontiguousarray(uvspec, dtype=np.int32)
+    av = A.as_f64(np.atleast_1d(aveuv))
+    nsp = int(spec.max())
+    out = np.zeros(nsp)
+    tot = C.c_double()
+    rc = lib.ermod_slvfe_delta_mu(device, len(rd), nsp, A.ptr(rd, C.c_double), A.ptr(rr, C.c_double),
+                                  chi.ctypes.data_as(C.POINTER(C.c_double)), A.ptr(crd, C.c_double),
+                                  A.ptr(spec, C.c_int32), kT_of(temp_K), A.ptr(av, C.c_double), float(slfeng),
+                                  A.ptr(out, C.c_double), C.byref(tot))
+    if rc != 0:
+        raise RuntimeError(f"{lib.ermod_slvfe_last_error().decode()} ({rc})")
+    return out, tot.value
 
 
 def delta_mu_from_files(soln_dir, refs_dir, temp_K: float, suffix: str = "tt", slfslt: bool = False):

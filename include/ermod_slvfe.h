@@ -1,0 +1,49 @@
+/*
+ * ermod_slvfe.h -- slvfe's free-energy functional (chmpot, slvfe.F90:744-803 with
+ * distnorm :1467-1542, getslncv :875-1001 and getinscv :1003-1232) for one data set on
+ * the GPU in FP64, with slvfe's default options (sfemain.F90:22-64): functional py-hnc,
+ * invmtrx 'reg' (Cholesky), zerosft 'eczr', wgtfnform 'harm', extsln 'lin',
+ * normalize 'yes', no bin merging.  Same library and conventions as ermod_b200.h.
+ */
+#ifndef ERMOD_SLVFE_H
+#define ERMOD_SLVFE_H
+
+#include <stdint.h>
+
+#include "ermod_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ERMOD_ERR_SLVFE     (-40)  /* the functional cannot be evaluated on these distributions */
+
+/*
+ * rho_sln [n]   the solution distribution as engsln's ratio column holds it
+ * rho_ref [n]   the reference-solvent distribution (engref's ratio column)
+ * chi_ref [n*n] the reference-solvent correlation matrix (corref), column-major
+ * crd [n]       bin coordinates (engsln's bin_middle), spec [n] 1-based species
+ * kT            kcal/mol (temp * 8.314510e-3 / 4.184, slvfe.F90:272)
+ * aveuv [nsp]   average solute-solvent energy per species in solution
+ * slfeng        solute self energy (slfslt 'yes'), else 0
+ * Writes chmpt[nsp] (per-species free energies, aveuv included) and *total
+ * (their sum + slfeng).  ERMOD_ERR_SLVFE with ermod_slvfe_last_error():
+ *   "slv_nrm" chi0 normalisation did not converge in 100 sweeps;
+ *   "slv_ext" a solution-side bin has no sampled neighbour to extrapolate from;
+ *   "slv_chl" the regularised matrix is not positive definite (slvfe's eigenvalue
+ *             fallback is not part of the GPU path);
+ *   "slv_zer" a species' mesh has no bin pair around zero energy.
+ */
+int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n, int32_t nsp, const double* rho_sln,
+                             const double* rho_ref, const double* chi_ref, const double* crd,
+                             const int32_t* spec, double kT, const double* aveuv, double slfeng,
+                             double* chmpt, double* total);
+
+/* Name of the last error of ermod_slvfe_delta_mu on this thread. */
+const char* ermod_slvfe_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ERMOD_SLVFE_H */

@@ -73,3 +73,71 @@ def test_product_matches_restatement_on_engine_distributions(oracle_mod, slvfe_o
     b = slvfe_oracle.delta_mu(sln["edens"], rfa["edens"], rfa["ecorr"], orc.uvcrd, spec, 300.0, aveuv)
     assert np.isfinite(a[1]) and abs(a[1]) < 1e3
     assert a[1] == pytest.approx(b[1], rel=1e-6, abs=1e-6)
+
+
+# ---------------------------------------------------------------------------
+# The GPU functional (include/ermod_slvfe.h) against the host module
+# ---------------------------------------------------------------------------
+def _two_species(seed=7):
+    rng = np.random.default_rng(seed)
+    crd1, r01, _ = synthetic(80, seed)
+    crd2 = np.concatenate([np.linspace(-3.0, -0.02, 20), np.linspace(0.02, 15.0, 40)])
+    r02 = rng.uniform(0.5, 2.0, len(crd2))
+    r02 *= 30.0 / r02.sum()
+    crd = np.concatenate([crd1, crd2])
+    rho0 = np.concatenate([r01, r02])
+    chi0 = np.outer(rho0, rho0) + np.diag(rho0)
+    spec = np.concatenate([np.ones(len(crd1), dtype=int), np.full(len(crd2), 2)])
+    rho = rho0 * np.exp(-0.2 * np.tanh(crd / 2.0))
+    rho[len(crd1) - 4:len(crd1)] = 0.0
+    for p, n in ((1, 100.0), (2, 30.0)):
+        rho[spec == p] *= n / rho[spec == p].sum()
+    return rho, rho0, chi0, crd, spec
+
+
+@pytest.mark.gpu
+def test_gpu_functional_matches_host_on_synthetic(engine_lib):
+    crd, rho0, chi0 = synthetic(seed=5)
+    spec = np.ones(len(crd), dtype=int)
+    rho = rho0 * np.exp(-0.3 * np.tanh(crd / 3.0))
+    rho[-5:] = 0.0
+    rho *= 100.0 / rho.sum()
+    a = SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0], slfeng=0.25)
+    b = SF.delta_mu_gpu(rho, rho0, chi0, crd, spec, 300.0, [-1.0], slfeng=0.25)
+    np.testing.assert_allclose(b[0], a[0], rtol=1e-9, atol=1e-9)
+    assert b[1] == pytest.approx(a[1], abs=1e-9)
+    per, tot = SF.delta_mu_gpu(rho0, rho0, chi0, crd, spec, 300.0, [-3.25], slfeng=0.5)
+    assert per[0] == pytest.approx(-3.25, abs=1e-10) and tot == pytest.approx(-2.75, abs=1e-10)
+
+
+@pytest.mark.gpu
+def test_gpu_functional_two_species(engine_lib):
+    rho, rho0, chi0, crd, spec = _two_species()
+    a = SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4])
+    b = SF.delta_mu_gpu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4])
+    np.testing.assert_allclose(b[0], a[0], rtol=1e-9, atol=1e-9)
+
+
+@pytest.mark.gpu
+def test_gpu_functional_on_engine_distributions(engine_lib, oracle_mod):
+    """rho, rho0 and chi0 from the FP64 oracle engine (LJ site in water), bin middles as slvfe reads them."""
+    orc, sln, rfa = _distributions(oracle_mod)
+    _, middle, _, spec = SF.representative_bins(orc.uvcrd, orc.uvmax, orc.uvsoft)
+    aveuv = [float(sln["slnuv"][0])]
+    a = SF.delta_mu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv)
+    b = SF.delta_mu_gpu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv)
+    assert np.isfinite(b[1])
+    # a 1396-bin regularised solve: FP64 rounding of two Cholesky orders, far below slvfe's 0.01
+    assert b[1] == pytest.approx(a[1], abs=1e-6)
+
+
+@pytest.mark.gpu
+def test_gpu_functional_failures(engine_lib):
+    crd, rho0, chi0 = synthetic(seed=5)
+    spec = np.ones(len(crd), dtype=int)
+    with pytest.raises(RuntimeError, match="slv_zer"):        # no bin pair around zero
+        SF.delta_mu_gpu(rho0, rho0, chi0, np.abs(crd) + 0.1, spec, 300.0, [0.0])
+    with pytest.raises(RuntimeError, match="slv_chl"):        # chi0 - rho0 rho0^T negative definite
+        SF.delta_mu_gpu(rho0, rho0, np.outer(rho0, rho0) - 0.5 * np.diag(rho0), crd, spec, 300.0, [0.0])
+    with pytest.raises(RuntimeError, match="slv_nrm"):        # no correlation at all
+        SF.delta_mu_gpu(rho0, rho0, np.zeros_like(chi0), crd, spec, 300.0, [0.0])
