@@ -59,7 +59,7 @@ class _SoluteSource:
     per insertion, the structure weight, and the RMSD filter against RefInfo's solute."""
 
     def __init__(self, sltconf, nsite, sltwgt=None, insstructure=INSSTR_NOREJECT, lwstr=0.0, upstr=0.0,
-                 refslt=None, max_reject=1_000_000):
+                 refslt=None):
         self.traj = IO.Trajectory(sltconf)
         if self.traj.natoms != nsite:
             raise IO.IOError_(A.ERR_FORMAT, "ins_siz")
@@ -74,27 +74,32 @@ class _SoluteSource:
             self.ref_w = A.as_f32(refslt[1]).ravel()
             if len(self.ref_w) != nsite:
                 raise IO.IOError_(A.ERMOD_ERR_ARG, "ins_siz")
-        self.max_reject = max_reject
+        self.wraps = 0   # wrap-arounds since the last accepted conformation
 
     def _next_conf(self):
         fr = self.traj.read()
         if fr is None:   # OUTconfig's wrap-around (setconf.F90:106-116)
             self.traj.rewind()
+            self.wraps += 1
             fr = self.traj.read()
             if fr is None:
                 raise IO.IOError_(A.ERR_FORMAT, "slt_trj")
         return fr[0].reshape(-1, 3)
 
     def next(self):
-        for _ in range(self.max_reject):
+        while True:
             crd = self._next_conf()
             w = self.wgt.next() if self.wgt else 1.0
             if self.insstructure == INSSTR_NOREJECT:
                 return crd, w
             r = IO.rmsd_bestfit(self.ref_crd, crd, self.ref_w)
             if self.lwstr <= r <= self.upstr:
+                self.wraps = 0
                 return crd, w
-        raise IO.IOError_(A.ERMOD_ERR_ARG, "ins_str")
+            if self.wraps >= 2:
+                # two whole passes over SltConf without an accepted structure: the reference's
+                # reading loop would never end (insertion.F90:464-506)
+                raise IO.IOError_(A.ERMOD_ERR_ARG, "ins_str")
 
     def batch(self, n):
         conf = np.zeros((n, self.nsite, 3), dtype=np.float32)

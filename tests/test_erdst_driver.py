@@ -175,6 +175,16 @@ def test_flexible_solute_conformations_weights_and_rmsd_filter(engine_lib, oracl
     assert np.all(eng2.calls[0]["ins_weight"] == 1.0)
 
 
+def test_no_accepted_structure_is_an_error(engine_lib, oracle_mod, tmp_path):
+    w, topo, prm, ref, confs = _flex_setup(tmp_path)
+    hist_path = _history(tmp_path, w, 1)
+    eng = OracleEngine(oracle_mod, prm, topo, w.hist)
+    with pytest.raises(IO.IOError_, match="ins_str"):
+        erdst.run(prm, topo, w.hist, hist_path, tmp_path / "o", maxcnf=1, engine=eng,
+                  sltconf=tmp_path / "SltConf.dcd", insstructure=erdst.INSSTR_RMSD, lwstr=5.0, upstr=6.0,
+                  refslt=(ref, np.ones(len(ref))))
+
+
 def test_run_errors(engine_lib, oracle_mod, tmp_path):
     w = S.make_workload(2, small=True, maxins=8)
     hist_path = _history(tmp_path, w, 2)
