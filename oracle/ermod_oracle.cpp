@@ -292,6 +292,7 @@ template <class T> struct Oracle {
       if (t->bfcoord) bfcoord.assign(t->bfcoord, t->bfcoord + 3 * nsite_slt);
       else bfcoord.assign(3 * nsite_slt, T(0));
       maxdst = p.maxins;
+      if (maxdst < 1) return fail(ERMOD_ERR_ARG, "set_ins");   // setconf.F90:352
     } else {
       maxdst = numslt;
     }

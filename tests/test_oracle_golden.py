@@ -169,3 +169,10 @@ def test_fp32_vs_fp64_oracle(oracle_mod):
     soft = np.abs(u8) < 1.0e3
     assert soft.mean() > 0.9
     assert np.all(np.abs(u4 - u8)[soft] <= 1e-4 * np.abs(u8[soft]) + 1e-4)
+
+
+def test_no_insertions_is_refused(oracle_mod):
+    """maxins < 1 in refs mode halts with set_ins (setconf.F90:346-353)."""
+    w = S.make_workload(2, small=True, maxins=8)
+    with pytest.raises(RuntimeError, match="set_ins"):
+        oracle_mod.Oracle(dict(w.params, maxins=0), w.topo, w.hist)

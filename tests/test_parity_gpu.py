@@ -536,3 +536,77 @@ def test_pppm_odd_order_is_rejected(lib):
     w = S.make_workload(2, small=True, maxins=32)
     with pytest.raises(ErmodError, match="pppm_odr"):
         Engine(dict(w.params, cltype=A.EL_PPPM, splodr=5), w.topo, w.hist)
+
+
+# ---------------------------------------------------------------------------
+# Edge cases: triclinic cells, ragged insertion counts, no insertions
+# ---------------------------------------------------------------------------
+def _triclinic(w, rotate):
+    """Frame 0 of `w` mapped onto a sheared cell (columns a, b, c), optionally with the whole
+    system turned by a rotation so that the cell is no longer upper triangular."""
+    from test_insertion_regions import _rot
+    pos, _ = w.frame(0)
+    L = float(w.box)
+    H = np.array([[L, 0.2 * L, 0.1 * L], [0.0, L, 0.15 * L], [0.0, 0.0, L]])
+    x = np.asarray(pos, dtype=np.float64).reshape(-1, 3) / L @ H.T
+    if rotate:
+        R = _rot([0.4, -0.3, 1.0], 0.6)
+        H = R @ H
+        x = x @ R.T
+    return A.as_f32(x.ravel()), A.as_f32(H.ravel(order="F"))
+
+
+@pytest.mark.parametrize("rotate,path", [(False, 1), (False, 2), (True, 1), (True, 2), (True, 3)])
+def test_triclinic_cells_match_oracle(lib, oracle_mod, rotate, path):
+    """Sheared and rotated cells: the normalisation of realcal_prepare (QR, reduction of the
+    off-diagonal components, realcal.F90:776-896), the minimum image and PME's inverted cell.
+    A rotated cell is turned back by the QR factor in FP32, which moves atoms by ~1e-6 A: the
+    reference's own FP32 algorithm (the oracle at precision 4) then exceeds 1e-5 relative on
+    high-energy molecules, so there the criterion is no larger error than it has."""
+    w = S.make_workload(2, small=True, maxins=64)
+    prm = dict(w.params, keep_uvengy=1, spectrum_path=path, elecut=9.0, upljcut=9.0, lwljcut=8.0)
+    pos, cell = _triclinic(w, rotate)
+    eng = Engine(prm, w.topo, w.hist)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, u0 = eng.uvengy()
+    ins, _ = eng.insertions()
+    orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist)
+    assert orc.engconst(1, pos, cell, ins_conf=ins) >= 0
+    uo, u0o = orc.uvengy()
+    np.testing.assert_allclose(u0, u0o, rtol=1e-6, atol=2e-5)
+    if not rotate:
+        check_energies(u, uo)
+        return
+    o4 = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist, precision=4)
+    assert o4.engconst(1, pos, cell, ins_conf=ins) >= 0
+    u4, _ = o4.uvengy()
+    soft = np.abs(uo) < 1.0e3
+    e_gpu, e_sp = np.abs(u - uo)[soft], np.abs(u4 - uo)[soft]
+    assert e_gpu.max() <= 1.5 * e_sp.max() + 2e-5
+    assert np.percentile(e_gpu, 99) <= 1.5 * np.percentile(e_sp, 99) + 2e-5
+    assert np.median(e_gpu) <= 2e-5
+
+
+@pytest.mark.parametrize("maxins", [1, 45, 77])
+def test_ragged_insertion_counts_match_oracle(lib, oracle_mod, maxins):
+    """Insertion counts that fill no PME chunk of 32 or leave a partial last chunk."""
+    w = S.make_workload(2, small=True, maxins=maxins)
+    prm = dict(w.params, keep_uvengy=1)
+    eng = Engine(prm, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, u0 = eng.uvengy()
+    assert u.shape[0] == maxins
+    ins, _ = eng.insertions()
+    orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist)
+    assert orc.engconst(1, pos, cell, ins_conf=ins) >= 0
+    uo, u0o = orc.uvengy()
+    check_energies(u, uo)
+    np.testing.assert_allclose(u0, u0o, rtol=1e-6, atol=2e-5)
+    assert eng.accum()["engnorm"] == pytest.approx(orc.accum()["engnorm"], rel=WREL)
+
+
+def test_no_insertions_is_refused(lib):
+    w = S.make_workload(2, small=True, maxins=8)
+    with pytest.raises(ErmodError, match="set_ins"):
+        Engine(dict(w.params, maxins=0), w.topo, w.hist)
