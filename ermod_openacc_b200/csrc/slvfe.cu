@@ -84,6 +84,9 @@ __device__ double block_min(double v, double* sh) { return -block_max(-v, sh); }
 struct SlvArgs {
   int n, nsp;
   double kT;
+  int n0;               // bins as read (before grouping)
+  const double* rd0;    // rho in solution as read, for getslncv's threshold (slvfe.F90:884)
+  const double* rr0;    // rho0 as read
   const double* rd;     // rho in solution as read (engstore-normalised)
   const double* rr;     // rho0 in the reference solvent as read
   const double* crd;    // bin coordinates (engsln's bin_middle)
@@ -116,9 +119,9 @@ __global__ void __launch_bounds__(kNT) k_slv_prep(SlvArgs a) {
   }
   __syncthreads();
   double mn = INFINITY, mn0 = INFINITY;
-  for (int i = threadIdx.x; i < n; i += kNT) {
-    if (a.rd[i] > 0.0) mn = fmin(mn, a.rd[i]);
-    if (a.rr[i] > 0.0) mn0 = fmin(mn0, a.rr[i]);
+  for (int i = threadIdx.x; i < a.n0; i += kNT) {
+    if (a.rd0[i] > 0.0) mn = fmin(mn, a.rd0[i]);
+    if (a.rr0[i] > 0.0) mn0 = fmin(mn0, a.rr0[i]);
   }
   mn = block_min(mn, sh);
   mn0 = block_min(mn0, sh);
@@ -131,6 +134,37 @@ __global__ void __launch_bounds__(kNT) k_slv_prep(SlvArgs a) {
     const double hs = r + r0;
     a.harm[i] = hs > 0.0 ? r * r0 / hs : 0.0;
   }
+}
+
+// ---- chmpot's grouping of consecutive bins (slvfe.F90:609-698) ------------------------
+// merged bin k covers the bins [rng[k].x, rng[k].y) as read; rng[k].z = 1 for the last merged
+// bin of a species, whose coordinate is that species' last coordinate as read
+__global__ void k_slv_merge_vec(int g, const int4* __restrict__ rng, const double* __restrict__ rd,
+                                const double* __restrict__ rr, const double* __restrict__ crd,
+                                const int* __restrict__ spec, double* __restrict__ mrd, double* __restrict__ mrr,
+                                double* __restrict__ mcrd, int* __restrict__ mspec) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= g) return;
+  const int4 r = rng[k];
+  double s = 0.0, s0 = 0.0, c = 0.0;
+  for (int i = r.x; i < r.y; ++i) { s += rd[i]; s0 += rr[i]; c += crd[i]; }
+  mrd[k] = s;
+  mrr[k] = s0;
+  mcrd[k] = r.z ? crd[r.y - 1] : c / (double)(r.y - r.x);
+  mspec[k] = spec[r.x];
+}
+
+// column-major g x g sums of the n0 x n0 matrix over the bins of each merged pair, fixed order
+__global__ void k_slv_merge_mat(int g, int n0, const int4* __restrict__ rng, const double* __restrict__ chi0,
+                                double* __restrict__ chi) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)g * g) return;
+  const int r = (int)(e % g), c = (int)(e / g);
+  const int4 R = rng[r], Cc = rng[c];
+  double s = 0.0;
+  for (int j = Cc.x; j < Cc.y; ++j)
+    for (int i = R.x; i < R.y; ++i) s += chi0[(size_t)j * n0 + i];
+  chi[e] = s;
 }
 
 // ---- chi0 row scaling: Gauss-Seidel sweeps in one CTA --------------------------------
@@ -417,33 +451,53 @@ cudaError_t dalloc(T** p, size_t n) { return cudaMalloc((void**)p, sizeof(T) * (
 
 extern "C" const char* ermod_slvfe_last_error(void) { return g_err; }
 
-extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n, int32_t nsp, const double* rho_sln,
-                                        const double* rho_ref, const double* chi_ref, const double* crd,
-                                        const int32_t* spec, double kT, const double* aveuv, double slfeng,
-                                        double* chmpt, double* total) {
-  if (n < 2 || nsp < 1 || nsp > kMaxSpecies || !rho_sln || !rho_ref || !chi_ref || !crd || !spec || !aveuv ||
-      !chmpt || !(kT > 0.0))
+extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n0, int32_t nsp, int32_t group,
+                                        const double* rho_sln, const double* rho_ref, const double* chi_ref,
+                                        const double* crd, const int32_t* spec, double kT, const double* aveuv,
+                                        double slfeng, double* chmpt, double* total) {
+  if (n0 < 2 || nsp < 1 || nsp > kMaxSpecies || group < 1 || !rho_sln || !rho_ref || !chi_ref || !crd || !spec ||
+      !aveuv || !chmpt || !(kT > 0.0))
     return fail(ERMOD_ERR_ARG, "slv_arg");
-  for (int i = 0; i < n; ++i)
-    if (spec[i] < 1 || spec[i] > nsp) return fail(ERMOD_ERR_ARG, "slv_arg");
+  for (int i = 0; i < n0; ++i)
+    if (spec[i] < 1 || spec[i] > nsp || (i > 0 && spec[i] < spec[i - 1])) return fail(ERMOD_ERR_ARG, "slv_arg");
+  // chmpot's grouping (slvfe.F90:613-640): per species floor(bins / group) merged bins, the last
+  // one taking the remainder; the index bookkeeping is host work, the sums run on the device
+  std::vector<int4> rng;
+  for (int i = 0; i < n0;) {
+    int j = i;
+    while (j < n0 && spec[j] == spec[i]) ++j;
+    const int m = (j - i) / group;
+    if (m < 1) return fail(ERMOD_ERR_ARG, "slv_grp");
+    for (int q = 0; q < m; ++q)
+      rng.push_back(make_int4(i + q * group, q < m - 1 ? i + (q + 1) * group : j, q == m - 1 ? 1 : 0, 0));
+    i = j;
+  }
+  const int n = (int)rng.size();
+  if (n < 2) return fail(ERMOD_ERR_ARG, "slv_grp");
   if ((size_t)n * sizeof(double) > 160 * 1024) return fail(ERMOD_ERR_ARG, "slv_siz");   // corr in shared memory
   if (cudaSetDevice(device) != cudaSuccess) return fail(ERMOD_ERR_CUDA, "slv_cud");
   const int N = (n + kTile - 1) / kTile * kTile;
-  const size_t nn = (size_t)n * n, NN = (size_t)N * N;
+  const size_t nn = (size_t)n * n, NN = (size_t)N * N, nn0 = (size_t)n0 * n0;
+  double *d_rd0 = nullptr, *d_rr0 = nullptr, *d_crd0 = nullptr, *d_chi0 = nullptr;
   double *d_rd = nullptr, *d_rr = nullptr, *d_crd = nullptr, *d_chi = nullptr, *d_rho = nullptr, *d_rho0 = nullptr;
   double *d_nm = nullptr, *d_om = nullptr, *d_harm = nullptr, *d_reg = nullptr, *d_A = nullptr, *d_b = nullptr;
   double *d_av = nullptr, *d_out = nullptr;
-  int *d_spec = nullptr, *d_both = nullptr, *d_st = nullptr;
+  int *d_spec0 = nullptr, *d_spec = nullptr, *d_both = nullptr, *d_st = nullptr;
+  int4* d_rng = nullptr;
   cudaStream_t st = nullptr;
   int rc = ERMOD_OK;
   auto cleanup = [&]() {
-    for (void* p : {(void*)d_rd, (void*)d_rr, (void*)d_crd, (void*)d_chi, (void*)d_rho, (void*)d_rho0, (void*)d_nm,
-                    (void*)d_om, (void*)d_harm, (void*)d_reg, (void*)d_A, (void*)d_b, (void*)d_av, (void*)d_out,
-                    (void*)d_spec, (void*)d_both, (void*)d_st})
+    for (void* p : {(void*)d_rd0, (void*)d_rr0, (void*)d_crd0, (void*)d_chi0, (void*)d_rd, (void*)d_rr,
+                    (void*)d_crd, (void*)d_chi, (void*)d_rho, (void*)d_rho0, (void*)d_nm, (void*)d_om,
+                    (void*)d_harm, (void*)d_reg, (void*)d_A, (void*)d_b, (void*)d_av, (void*)d_out,
+                    (void*)d_spec0, (void*)d_spec, (void*)d_both, (void*)d_st, (void*)d_rng})
       if (p) cudaFree(p);
     if (st) cudaStreamDestroy(st);
   };
   bool ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && dalloc(&d_rd0, n0) == cudaSuccess && dalloc(&d_rr0, n0) == cudaSuccess;
+  ok = ok && dalloc(&d_crd0, n0) == cudaSuccess && dalloc(&d_chi0, nn0) == cudaSuccess;
+  ok = ok && dalloc(&d_spec0, n0) == cudaSuccess && dalloc(&d_rng, n) == cudaSuccess;
   ok = ok && dalloc(&d_rd, n) == cudaSuccess && dalloc(&d_rr, n) == cudaSuccess && dalloc(&d_crd, n) == cudaSuccess;
   ok = ok && dalloc(&d_chi, nn) == cudaSuccess && dalloc(&d_rho, n) == cudaSuccess && dalloc(&d_rho0, n) == cudaSuccess;
   ok = ok && dalloc(&d_nm, nsp) == cudaSuccess && dalloc(&d_om, n) == cudaSuccess && dalloc(&d_harm, n) == cudaSuccess;
@@ -451,19 +505,24 @@ extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n, int32_t nsp, 
   ok = ok && dalloc(&d_av, nsp) == cudaSuccess && dalloc(&d_out, nsp) == cudaSuccess;
   ok = ok && dalloc(&d_spec, n) == cudaSuccess && dalloc(&d_both, n) == cudaSuccess && dalloc(&d_st, 1) == cudaSuccess;
   if (!ok) { cleanup(); return fail(ERMOD_ERR_CUDA, "slv_mem"); }
-  ok = cudaMemcpyAsync(d_rd, rho_sln, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
-  ok = ok && cudaMemcpyAsync(d_rr, rho_ref, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
-  ok = ok && cudaMemcpyAsync(d_crd, crd, 8 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
-  ok = ok && cudaMemcpyAsync(d_chi, chi_ref, 8 * nn, cudaMemcpyHostToDevice, st) == cudaSuccess;
-  ok = ok && cudaMemcpyAsync(d_spec, spec, 4 * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = cudaMemcpyAsync(d_rd0, rho_sln, 8 * n0, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_rr0, rho_ref, 8 * n0, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_crd0, crd, 8 * n0, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_chi0, chi_ref, 8 * nn0, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_spec0, spec, 4 * n0, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_rng, rng.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, st) == cudaSuccess;
   ok = ok && cudaMemcpyAsync(d_av, aveuv, 8 * nsp, cudaMemcpyHostToDevice, st) == cudaSuccess;
   ok = ok && cudaMemsetAsync(d_st, 0, sizeof(int), st) == cudaSuccess;
-  SlvArgs a{n, nsp, kT, d_rd, d_rr, d_crd, d_spec, d_rho, d_rho0, d_nm, d_om, d_both, d_harm, d_reg, d_st};
+  SlvArgs a{n, nsp, kT, n0, d_rd0, d_rr0, d_rd, d_rr, d_crd, d_spec, d_rho, d_rho0, d_nm, d_om, d_both, d_harm,
+            d_reg, d_st};
   const size_t corr_smem = (size_t)n * sizeof(double);
   if (ok && corr_smem > 48 * 1024)
     ok = cudaFuncSetAttribute(k_slv_distnorm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)corr_smem) ==
          cudaSuccess;
   if (ok) {
+    k_slv_merge_vec<<<(n + 127) / 128, 128, 0, st>>>(n, d_rng, d_rd0, d_rr0, d_crd0, d_spec0, d_rd, d_rr, d_crd,
+                                                     d_spec);
+    k_slv_merge_mat<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(n, n0, d_rng, d_chi0, d_chi);
     k_slv_prep<<<1, kNT, 0, st>>>(a);
     k_slv_distnorm<<<1, kNT, corr_smem, st>>>(a, d_chi);
     k_slv_extrap<<<(n + 127) / 128, 128, 0, st>>>(a);

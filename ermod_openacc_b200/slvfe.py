@@ -8,7 +8,7 @@ one data set with slvfe's defaults (slvfe/sfemain.F90:22-64):
 
   functional 'py-hnc', invmtrx 'reg', zerosft 'eczr', wgtfnform 'harm',
   extsln 'lin', extthres 1, minthres 0, normalize 'yes', slncor 'not',
-  ljlrc 'not', uvread 'yes' (aveuv given), no bin merging (group 1, inft 0).
+  ljlrc 'not', uvread 'yes' (aveuv given), bins merged by `group` with inft 0.
 
 Steps (slvfe.F90 line ranges):
   distnorm   1467-1542  rho, rho0 scaled to N per species; chi0 made
@@ -25,7 +25,7 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["kT_of", "delta_mu", "delta_mu_gpu", "representative_bins", "read_engfile", "read_corfile",
+__all__ = ["kT_of", "delta_mu", "delta_mu_gpu", "merge_bins", "representative_bins", "read_engfile", "read_corfile",
            "read_table", "delta_mu_from_files"]
 
 
@@ -95,8 +95,64 @@ def _zero_bin(crd, dens, mask, tiny=1.0e-8):
     return k
 
 
-def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0):
+def merge_groups(uvspec, group: int):
+    """chmpot's bin grouping with inft = 0 (slvfe.F90:609-640): per species, `group`
+    consecutive bins form one merged bin and the last merged bin also takes the remainder.
+    Returns (merged index of every bin, start and end of every merged bin, 1 for the last
+    merged bin of each species)."""
+    spec = np.asarray(uvspec)
+    n = len(spec)
+    idr = np.zeros(n, dtype=np.int64)
+    starts, ends, last = [], [], []
+    i = 0
+    while i < n:
+        j = i
+        while j < n and spec[j] == spec[i]:
+            j += 1
+        m = (j - i) // group
+        if m < 1:
+            raise ValueError(f"species {spec[i]} has fewer bins than the group size {group}")
+        idr[i:j] = len(starts) + np.minimum(np.arange(j - i) // group, m - 1)
+        for q in range(m):
+            starts.append(i + q * group)
+            ends.append(i + (q + 1) * group if q < m - 1 else j)
+            last.append(1 if q == m - 1 else 0)
+        i = j
+    return idr, np.array(starts), np.array(ends), np.array(last)
+
+
+def merge_bins(edist, edens, ecorr, uvcrd, uvspec, group: int):
+    """The merged distributions, correlation matrix, coordinates and species
+    (slvfe.F90:642-698): sums over each group, the mean coordinate, and the species'
+    last original coordinate for its last merged bin."""
+    idr, st, en, last = merge_groups(uvspec, group)
+    P = np.zeros((len(st), len(idr)))
+    P[idr, np.arange(len(idr))] = 1.0
+    crd = np.asarray(uvcrd, dtype=np.float64)
+    mc = (P @ crd) / P.sum(axis=1)
+    mc[last == 1] = crd[en[last == 1] - 1]
+    chi = np.asarray(ecorr, dtype=np.float64)
+    return (P @ np.asarray(edist, dtype=np.float64), P @ np.asarray(edens, dtype=np.float64), P @ chi @ P.T, mc,
+            np.asarray(uvspec)[st])
+
+
+def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0, group: int = 1):
     """(per-species solvation free energies, total) in kcal/mol.
+
+    group > 1 first merges that many consecutive bins per species: chmpot's grouping with
+    inft 0 (slvfe.F90:609-698).  The reference reports group pickgr = 3 in its range and
+    merge modes (sfemain.F90:55, slvfe.F90:1647)."""
+    # the sampled-bin thresholds use the smallest values of the data as read (slvfe.F90:884-885)
+    rd_min = float(np.min(np.asarray(edist)[np.asarray(edist) > 0.0]))
+    rr_min = float(np.min(np.asarray(edens)[np.asarray(edens) > 0.0]))
+    if group > 1:
+        edist, edens, ecorr, uvcrd, uvspec = merge_bins(edist, edens, ecorr, uvcrd, uvspec, group)
+    return _delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng, rd_min, rr_min)
+
+
+def _delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float, rd_min: float,
+              rr_min: float):
+    """delta_mu on the mesh as given.
 
     edist: rho (solution, engstore-normalised); edens, ecorr: rho0 and chi0
     (reference solvent); uvcrd: bin coordinates; uvspec: 1-based species of
@@ -113,8 +169,8 @@ def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: f
     nummol = [float(np.rint(rd[spec == p].sum())) for p in range(1, nsp + 1)]
     rho, rho0, chi = _normalise(rd, rr, cr, spec, nummol)
     # omega in solution: direct where both distributions are sampled
-    ratio_s = np.minimum(rho / rd[rd > 0.0].min(), 10.0)
-    ratio_r = np.minimum(rho0 / rr[rr > 0.0].min(), 10.0)
+    ratio_s = np.minimum(rho / rd_min, 10.0)
+    ratio_r = np.minimum(rho0 / rr_min, 10.0)
     both = (np.rint(ratio_s) >= 1) & (np.rint(ratio_r) >= 1)
     omega = np.zeros(n)
     with np.errstate(divide="ignore", invalid="ignore"):
@@ -262,7 +318,7 @@ def read_table(path) -> np.ndarray:
 
 
 def delta_mu_gpu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0,
-                 device: int = 0):
+                 device: int = 0, group: int = 1):
     """delta_mu on the GPU (include/ermod_slvfe.h): the same functional, options and
     arguments, FP64 CUDA kernels.  Raises RuntimeError with slvfe's failure name; there is
     no eigenvalue fallback on this path."""
@@ -278,7 +334,7 @@ def delta_mu_gpu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfen
     nsp = int(spec.max())
     out = np.zeros(nsp)
     tot = C.c_double()
-    rc = lib.ermod_slvfe_delta_mu(device, len(rd), nsp, A.ptr(rd, C.c_double), A.ptr(rr, C.c_double),
+    rc = lib.ermod_slvfe_delta_mu(device, len(rd), nsp, group, A.ptr(rd, C.c_double), A.ptr(rr, C.c_double),
                                   chi.ctypes.data_as(C.POINTER(C.c_double)), A.ptr(crd, C.c_double),
                                   A.ptr(spec, C.c_int32), kT_of(temp_K), A.ptr(av, C.c_double), float(slfeng),
                                   A.ptr(out, C.c_double), C.byref(tot))
@@ -287,7 +343,8 @@ def delta_mu_gpu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfen
     return out, tot.value
 
 
-def delta_mu_from_files(soln_dir, refs_dir, temp_K: float, suffix: str = "tt", slfslt: bool = False):
+def delta_mu_from_files(soln_dir, refs_dir, temp_K: float, suffix: str = "tt", slfslt: bool = False,
+                        group: int = 1):
     """slvfe on one division's files: engsln.<suffix> and aveuv.tt from the solution run,
     engref.<suffix> and corref.<suffix> from the reference-solvent run; with slfslt the
     solute self energy is weight_refs' third column averaged with its first-column
@@ -306,4 +363,4 @@ def delta_mu_from_files(soln_dir, refs_dir, temp_K: float, suffix: str = "tt", s
         wr = read_table(os.path.join(refs_dir, "weight_refs"))
         w = wr[:, 1] / wr[:, 1].sum()
         slf = float(np.dot(w, wr[:, 2]))
-    return delta_mu(sln["ratio"], ref["ratio"], chi, sln["middle"], sln["spec"], temp_K, aveuv, slf)
+    return delta_mu(sln["ratio"], ref["ratio"], chi, sln["middle"], sln["spec"], temp_K, aveuv, slf, group=group)

@@ -22,7 +22,11 @@ extern "C" {
  * rho_sln [n]   the solution distribution as engsln's ratio column holds it
  * rho_ref [n]   the reference-solvent distribution (engref's ratio column)
  * chi_ref [n*n] the reference-solvent correlation matrix (corref), column-major
- * crd [n]       bin coordinates (engsln's bin_middle), spec [n] 1-based species
+ * crd [n]       bin coordinates (engsln's bin_middle), spec [n] 1-based species, each
+ *               species' bins contiguous and in order
+ * group         bins merged per species first (chmpot's grouping with inft 0,
+ *               slvfe.F90:609-698; the reference reports group 3 in its range / merge
+ *               modes, sfemain.F90:55); 1 = the mesh as read
  * kT            kcal/mol (temp * 8.314510e-3 / 4.184, slvfe.F90:272)
  * aveuv [nsp]   average solute-solvent energy per species in solution
  * slfeng        solute self energy (slfslt 'yes'), else 0
@@ -33,8 +37,9 @@ extern "C" {
  *   "slv_chl" the regularised matrix is not positive definite (slvfe's eigenvalue
  *             fallback is not part of the GPU path);
  *   "slv_zer" a species' mesh has no bin pair around zero energy.
+ * ERMOD_ERR_ARG "slv_grp" when a species has fewer bins than `group`.
  */
-int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n, int32_t nsp, const double* rho_sln,
+int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n, int32_t nsp, int32_t group, const double* rho_sln,
                              const double* rho_ref, const double* chi_ref, const double* crd,
                              const int32_t* spec, double kT, const double* aveuv, double slfeng,
                              double* chmpt, double* total);

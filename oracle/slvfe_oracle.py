@@ -2,8 +2,8 @@
 solvation free energy for the checker (tests/ only).
 
 Follows slvfe/slvfe.F90 with the defaults of slvfe/sfemain.F90:22-64 for a
-single data set (clcond 'basic', group 1, inft 0, so the bin mapping of
-chmpot is the identity): functional 'py-hnc', invmtrx 'reg', zerosft
+single data set (clcond 'basic', inft 0; group 1 makes the bin mapping of
+chmpot the identity, larger groups go through merge_bins): functional 'py-hnc', invmtrx 'reg', zerosft
 'eczr', wgtfnform 'harm', wgtf2smpl 'yes', extsln 'lin', extthres 1,
 minthres 0, normalize 'yes', slncor 'not', ljlrc 'not', uvread 'yes'.
 Written with explicit loops in the reference's order, in FP64.
@@ -105,7 +105,67 @@ def _zeroec(pti, edvec, uvcrd, uvspec, tiny=1.0e-8):
     return k
 
 
-def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0):
+def merge_bins(rddst, rddns, rdcor, rdcrd, rdspec, group):
+    """chmpot's grouping of `group` consecutive bins per species with inft = 0
+    (slvfe.F90:609-698), in the reference's loop order, 1-based indices as there."""
+    rddst, rddns, rdcor = (np.asarray(x, dtype=np.float64) for x in (rddst, rddns, rdcor))
+    rdcrd = np.asarray(rdcrd, dtype=np.float64)
+    rdspec = np.asarray(rdspec)
+    ermax = len(rddst)
+    numslv = int(rdspec.max())
+    rduvmax = [0] * (numslv + 1)
+    for iduv in range(ermax):
+        rduvmax[int(rdspec[iduv])] += 1
+    uvmax = [0] * (numslv + 1)
+    idrduv = [0] * (ermax + 1)
+    gemax = 0
+    for pti in range(1, numslv + 1):
+        k = 0                                   # rduvcore(pti) * inft / 100 with inft = 0
+        m = (rduvmax[pti] - k) // group
+        uvmax[pti] = m
+        gemax += m
+        if pti == 1:
+            cnt, j = 1, 0
+        else:
+            cnt, j = 1 + sum(rduvmax[1:pti]), sum(uvmax[1:pti])
+        for iduv in range(cnt, cnt + rduvmax[pti]):
+            k = (iduv - cnt) // group + 1
+            if k >= m:
+                k = m
+            idrduv[iduv] = k + j
+    uvcrd = [0.0] * (gemax + 1)
+    gpnum = [0] * (gemax + 1)
+    uvspec = [0] * (gemax + 1)
+    for iduv in range(1, ermax + 1):
+        k = idrduv[iduv]
+        uvcrd[k] += rdcrd[iduv - 1]
+        gpnum[k] += 1
+        uvspec[k] = int(rdspec[iduv - 1])
+    for k in range(1, gemax + 1):
+        if gpnum[k] > 0:
+            uvcrd[k] /= gpnum[k]
+    cnt, k = rduvmax[1], uvmax[1]
+    for pti in range(1, numslv + 1):
+        if pti > 1:
+            cnt += rduvmax[pti]
+            k += uvmax[pti]
+        uvcrd[k] = rdcrd[cnt - 1]
+    edist = [0.0] * (gemax + 1)
+    edens = [0.0] * (gemax + 1)
+    for iduv in range(1, ermax + 1):
+        k = idrduv[iduv]
+        edist[k] += rddst[iduv - 1]
+        edens[k] += rddns[iduv - 1]
+    ecorr = np.zeros((gemax + 1, gemax + 1))
+    for iduv in range(1, ermax + 1):
+        k = idrduv[iduv]
+        for iduvp in range(1, ermax + 1):
+            ecorr[idrduv[iduvp], k] += rdcor[iduvp - 1, iduv - 1]
+    return (np.array(edist[1:]), np.array(edens[1:]), ecorr[1:, 1:], np.array(uvcrd[1:]),
+            np.array(uvspec[1:]))
+
+
+def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0, group=1):
     """Solvation free energy (kcal/mol) per solvent species and in total.
 
     edist  solution energy distribution per bin (engsln), edens / ecorr the
@@ -113,7 +173,13 @@ def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0):
     engstore writes them; uvcrd the bin coordinates, uvspec the species of
     each bin (1-based); aveuv the average solute-solvent energy per species
     in solution, slfeng the solute self energy added with slfslt = 'yes'.
+    group merges that many consecutive bins per species first (chmpot, slvfe.F90:609-698).
     Returns (chmpt[numslv], total)."""
+    # getslncv's thresholds use the smallest sampled values of the data as read (slvfe.F90:884-885)
+    min_rddst = np.asarray(edist, dtype=np.float64)[np.asarray(edist) > 0.0].min()
+    min_rddns = np.asarray(edens, dtype=np.float64)[np.asarray(edens) > 0.0].min()
+    if group > 1:
+        edist, edens, ecorr, uvcrd, uvspec = merge_bins(edist, edens, ecorr, uvcrd, uvspec, group)
     rddst = np.asarray(edist, dtype=np.float64)
     rddns = np.asarray(edens, dtype=np.float64)
     rdcor = np.asarray(ecorr, dtype=np.float64)
@@ -126,8 +192,6 @@ def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0):
     nummol = [float(np.rint(rddst[uvspec == pti].sum())) for pti in range(1, numslv + 1)]
     edist_, edens_, ecorr_ = _distnorm(rddst, rddns, rdcor, uvspec, nummol, numslv)
     # ---- getslncv (slvfe.F90:875-1001), extsln = 'lin', zerosft = 'eczr' ----
-    min_rddst = rddst[rddst > 0.0].min()
-    min_rddns = rddns[rddns > 0.0].min()
     ext = np.ones(gemax, dtype=bool)
     for iduv in range(gemax):
         j = min(10, int(np.rint(edist_[iduv] / min_rddst))) if edist_[iduv] / min_rddst <= 10 else 10

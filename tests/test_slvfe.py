@@ -119,13 +119,15 @@ def test_gpu_functional_two_species(engine_lib):
 
 
 @pytest.mark.gpu
-def test_gpu_functional_on_engine_distributions(engine_lib, oracle_mod):
-    """rho, rho0 and chi0 from the FP64 oracle engine (LJ site in water), bin middles as slvfe reads them."""
+@pytest.mark.parametrize("group", [1, 3])
+def test_gpu_functional_on_engine_distributions(engine_lib, oracle_mod, group):
+    """rho, rho0 and chi0 from the FP64 oracle engine (LJ site in water), bin middles as slvfe
+    reads them; group 3 is the bin merging the reference reports (pickgr)."""
     orc, sln, rfa = _distributions(oracle_mod)
     _, middle, _, spec = SF.representative_bins(orc.uvcrd, orc.uvmax, orc.uvsoft)
     aveuv = [float(sln["slnuv"][0])]
-    a = SF.delta_mu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv)
-    b = SF.delta_mu_gpu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv)
+    a = SF.delta_mu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv, group=group)
+    b = SF.delta_mu_gpu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv, group=group)
     assert np.isfinite(b[1])
     # a 1396-bin regularised solve: FP64 rounding of two Cholesky orders, far below slvfe's 0.01
     assert b[1] == pytest.approx(a[1], abs=1e-6)
@@ -141,3 +143,38 @@ def test_gpu_functional_failures(engine_lib):
         SF.delta_mu_gpu(rho0, rho0, np.outer(rho0, rho0) - 0.5 * np.diag(rho0), crd, spec, 300.0, [0.0])
     with pytest.raises(RuntimeError, match="slv_nrm"):        # no correlation at all
         SF.delta_mu_gpu(rho0, rho0, np.zeros_like(chi0), crd, spec, 300.0, [0.0])
+
+
+@pytest.mark.parametrize("group", [2, 3, 5])
+def test_bin_merging_matches_restatement(slvfe_oracle, group):
+    """chmpot's grouping (slvfe.F90:609-698): merged arrays and delta mu of the product module
+    against the loop-by-loop restatement, two species of uneven bin counts."""
+    rho, rho0, chi0, crd, spec = _two_species()
+    a = SF.merge_bins(rho, rho0, chi0, crd, spec, group)
+    b = slvfe_oracle.merge_bins(rho, rho0, chi0, crd, spec, group)
+    for x, y in zip(a, b):
+        np.testing.assert_allclose(x, y, rtol=1e-13, atol=1e-13)
+    # the last merged bin of a species keeps its last coordinate and takes the remainder
+    n1 = int((spec == 1).sum())
+    assert a[3][n1 // group - 1] == crd[n1 - 1]
+    pa = SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], group=group)
+    pb = slvfe_oracle.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], group=group)
+    np.testing.assert_allclose(pa[0], pb[0], rtol=1e-9, atol=1e-9)
+
+
+def test_identical_distributions_give_aveuv_merged():
+    crd, rho0, chi0 = synthetic()
+    spec = np.ones(len(crd), dtype=int)
+    per, tot = SF.delta_mu(rho0, rho0, chi0, crd, spec, 300.0, [-3.25], slfeng=0.5, group=3)
+    assert per[0] == pytest.approx(-3.25, abs=1e-10) and tot == pytest.approx(-2.75, abs=1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("group", [2, 3])
+def test_gpu_functional_merged_bins(engine_lib, group):
+    rho, rho0, chi0, crd, spec = _two_species()
+    a = SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], group=group)
+    b = SF.delta_mu_gpu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], group=group)
+    np.testing.assert_allclose(b[0], a[0], rtol=1e-9, atol=1e-9)
+    with pytest.raises(RuntimeError, match="slv_grp"):
+        SF.delta_mu_gpu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], group=1000)
