@@ -455,7 +455,8 @@ def main_delta_mu(args):
         eng.engconst(i + 1, *sln_w.frame(i))
     sln, _ = eng.engstore()
     rho, aveuv = sln["edens"], [float(sln["slnuv"][0])]
-    uvcrd, spec = eng.uvcrd, np.ones(eng.ermax, dtype=int)
+    # slvfe reads engsln's bin middles (slvfe.F90:385) and reports bins merged by pickgr = 3
+    _, middle, _, spec = slvfe.representative_bins(eng.uvcrd, eng.uvmax, eng.uvsoft)
     eng.close()
     # reference solvent: pure disordered water, insertions of the same solute
     ref_topo = S.Topology([S.water(), slt], [nside ** 3, 1], [A.PT_SOLVENT, A.PT_TEST_RIGID])
@@ -466,7 +467,7 @@ def main_delta_mu(args):
 
     def dmu(e):
         acc, _ = e.engstore()
-        return slvfe.delta_mu(rho, acc["edens"], acc["ecorr"], uvcrd, spec, temp_K, aveuv)[1]
+        return slvfe.delta_mu_gpu(rho, acc["edens"], acc["ecorr"], middle, spec, temp_K, aveuv, group=3)[1]
 
     def run(mode, iseed, nfr, params=None, checkpoints=()):
         e = Engine(dict(ref_prm, proposal=mode, iseed=iseed), ref_topo, {})
@@ -529,6 +530,7 @@ def main_delta_mu(args):
             "higher_is_better": False, "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"delta-mu-{name}-water4096-disordered", "insertions_per_frame": nins,
                        "voxels_per_side": gv, "mix_uniform": eps, "replicas": reps,
+                       "slvfe": {"bin_coordinates": "engsln bin_middle", "group": 3, "path": "GPU FP64"},
                        "judge": {"frames": judge_frames, "insertions": judge_frames * nins,
                                  "delta_mu_kcal": judge, "gpu_s": judge_ms / 1e3}},
             "uniform": curves["uniform"], "learned": curves["learned"],
