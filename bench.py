@@ -432,9 +432,9 @@ def main_delta_mu(args):
     A ring-recipe solute (--solute-sites, default a single LJ site) in 4096 waters (49.6 A box, disordered
     packing: the lattice has no cavities for the proposal to find), PME 64^3.  rho and aveuv come from
     soln-mode frames with the solute at the box centre; rho0 / chi0 from refs insertions, 2048 per frame;
-    delta-mu from the py-hnc functional (ermod_openacc_b200.slvfe).  The judge is a uniform run of
-    `judge_frames` frames; each mode runs `reps` independent replicas and its error after n frames is the
-    RMS over replicas of the difference to the judge.  Times are CUDA-event device times of the frames; the
+    delta-mu from the py-hnc functional (ermod_openacc_b200.slvfe).  The yardstick is a uniform run of
+    `long_frames` frames; each mode runs `reps` independent replicas and its error after n frames is the
+    RMS over replicas of the difference to the yardstick.  Times are CUDA-event device times of the frames; the
     learned mode also reports the device time of its training (sample frames + training kernels)."""
     import torch
     import __graft_entry__ as ge
@@ -482,8 +482,8 @@ def main_delta_mu(args):
         e.close()
         return res, ms
 
-    judge_frames = 400
-    judge, judge_ms = run(A.PROPOSAL_UNIFORM, 999, judge_frames)
+    long_frames = 400
+    long_dmu, long_ms = run(A.PROPOSAL_UNIFORM, 999, long_frames)
     # training: uniform samples of 12 frames, 20 epochs of the device kernels
     e = Engine(dict(ref_prm, corrcal=0), ref_topo, {})
     e.proposal_config(gv, eps, feature_cells=gv)
@@ -516,7 +516,7 @@ def main_delta_mu(args):
         for r in range(reps):
             out, ms = run(mode, 100 + r, max(cps), params if mode == A.PROPOSAL_LEARNED else None, cps)
             for c in cps:
-                errs[c].append(out[c][0] - judge)
+                errs[c].append(out[c][0] - long_dmu)
             mspf.append(ms / max(cps))
         rms = {c: float(np.sqrt(np.mean(np.square(errs[c])))) for c in cps}
         m = float(np.mean(mspf))
@@ -531,8 +531,8 @@ def main_delta_mu(args):
             "config": {"workload": f"delta-mu-{name}-water4096-disordered", "insertions_per_frame": nins,
                        "voxels_per_side": gv, "mix_uniform": eps, "replicas": reps,
                        "slvfe": {"bin_coordinates": "engsln bin_middle", "group": 3, "path": "GPU FP64"},
-                       "judge": {"frames": judge_frames, "insertions": judge_frames * nins,
-                                 "delta_mu_kcal": judge, "gpu_s": judge_ms / 1e3}},
+                       "long_uniform_run": {"frames": long_frames, "insertions": long_frames * nins,
+                                 "delta_mu_kcal": long_dmu, "gpu_s": long_ms / 1e3}},
             "uniform": curves["uniform"], "learned": curves["learned"],
             "training_gpu_s": (sample_ms + train_ms) / 1e3,
             "speedup_uniform_over_learned": None if (tu is None or tl is None) else tu / tl}

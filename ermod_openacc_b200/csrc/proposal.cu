@@ -1,7 +1,7 @@
 // proposal.cu -- where refs-mode insertions go.  No reference counterpart:
 // erdst places the test particle's centre of mass uniformly in the cell
 // (insertion.F90:152-162).  The learned proposal keeps that as a component
-// and as the judge: the cell is cut into G^3 voxels of fractional size 1/G,
+// and as the yardstick: the cell is cut into G^3 voxels of fractional size 1/G,
 //
 //   q_v = eps / V + (1 - eps) * softmax(s)_v,   V = G^3,
 //

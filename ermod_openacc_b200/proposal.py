@@ -6,7 +6,7 @@ proposal q_v = eps / V + (1 - eps) softmax(s)_v and weights every insertion
 by p/q (csrc/proposal.cu).  Training data come from plain uniform insertion:
 the features of each insertion's voxel and a label that marks insertions
 whose total solute-solvent energy lies below a quantile of the uniform
-energies, i.e. where the solute fits.  Uniform insertion stays the judge:
+energies, i.e. where the solute fits.  Uniform insertion stays the yardstick:
 the importance weights make the learned run estimate the uniform-insertion
 distributions.
 """
