@@ -51,6 +51,9 @@ def parse():
                     help="2: the headline refs frame; 4: 64 solutes batched into one graph per frame; "
                          "5: GPU time to delta-mu within 0.05 kcal/mol, learned vs uniform insertion")
     ap.add_argument("--solute-sites", type=int, default=1, help="config 5: sites of the ring-recipe solute")
+    ap.add_argument("--mix-uniform", type=float, default=0.2, help="config 5: uniform share eps of the proposal")
+    ap.add_argument("--label-quantile", type=float, default=0.05,
+                    help="config 5: training label 1 for this lowest fraction of insertion energies")
     return ap.parse_args()
 
 
@@ -441,7 +444,7 @@ def main_delta_mu(args):
     ge.build_engine()
     from ermod_openacc_b200 import Engine, _capi as A, proposal as P, slvfe, systems as S
     torch.cuda.set_device(0)
-    nins, gv, eps, npool = 2048, 32, 0.2, 8
+    nins, gv, eps, npool = 2048, 32, args.mix_uniform, 8
     base = S.make_workload(2, seed=11)
     slt = S.lj_site() if args.solute_sites == 1 else S.ring_recipe_solute(args.solute_sites, 5)
     box, nside = base.box, base.nside
@@ -497,7 +500,7 @@ def main_delta_mu(args):
         es.append(en)
     e.close()
     feats, etot = np.concatenate(fs), np.concatenate(es)
-    y, _ = P.labels_from_energies(etot, quantile=0.05)
+    y, _ = P.labels_from_energies(etot, quantile=args.label_quantile)
     tr = P.Trainer(P.init_params(7), max_batch=2048)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
@@ -529,7 +532,8 @@ def main_delta_mu(args):
     line = {"metric": "s to delta-mu +/-0.05 kcal/mol", "value": tl, "unit": "s", "n_gpus": 1,
             "higher_is_better": False, "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"delta-mu-{name}-water4096-disordered", "insertions_per_frame": nins,
-                       "voxels_per_side": gv, "mix_uniform": eps, "replicas": reps,
+                       "voxels_per_side": gv, "mix_uniform": eps, "label_quantile": args.label_quantile,
+                       "replicas": reps,
                        "slvfe": {"bin_coordinates": "engsln bin_middle", "group": 3, "path": "GPU FP64"},
                        "long_uniform_run": {"frames": long_frames, "insertions": long_frames * nins,
                                  "delta_mu_kcal": long_dmu, "gpu_s": long_ms / 1e3}},
