@@ -26,7 +26,7 @@ from __future__ import annotations
 import numpy as np
 
 __all__ = ["kT_of", "delta_mu", "delta_mu_gpu", "merge_bins", "representative_bins", "read_engfile", "read_corfile",
-           "read_table", "delta_mu_from_files"]
+           "read_table", "delta_mu_from_files", "merge_mode"]
 
 
 def kT_of(temp_K: float) -> float:
@@ -364,3 +364,72 @@ def delta_mu_from_files(soln_dir, refs_dir, temp_K: float, suffix: str = "tt", s
         w = wr[:, 1] / wr[:, 1].sum()
         slf = float(np.dot(w, wr[:, 2]))
     return delta_mu(sln["ratio"], ref["ratio"], chi, sln["middle"], sln["spec"], temp_K, aveuv, slf, group=group)
+
+
+def _suffixes(directory, prefix):
+    import os
+    names = [f for f in os.listdir(directory) if f.startswith(prefix + ".")]
+    nums = sorted(int(f.split(".")[1]) for f in names if f.split(".")[1].isdigit())
+    if nums:
+        return [f"{n:02d}" for n in nums]
+    if prefix + ".tt" in names:
+        return ["tt"]
+    raise FileNotFoundError(f"no {prefix} files in {directory}")
+
+
+def merge_mode(soln_dir, refs_dir, temp_K: float, numdiv: int = 0, group: int = 3, slfslt: bool = False,
+               gpu: bool = False, device: int = 0) -> dict:
+    """slvfe's clcond 'merge' for one (group, inft 0): the solution runs engsln.NN split into
+    numdiv blocks, each block's distribution and aveuv the weight_soln-weighted mean of its
+    runs; the reference-solvent runs engref.NN / corref.NN merged over all runs with
+    weight_refs (refmerge 'yes'); delta mu per block, their mean and the 95 % error
+    2 s / sqrt(n) with the n / (n - 1) variance (datread slvfe.F90:292-444, wrtmerge
+    :1733-1790).  numdiv <= 0 or >= the number of runs takes every run as a block; a count
+    that does not divide it moves up to the next divisor (sfemain.F90:148-153)."""
+    import os
+    ssuf = _suffixes(soln_dir, "engsln")
+    rsuf = _suffixes(refs_dir, "engref")
+    numsln, numref = len(ssuf), len(rsuf)
+    if numdiv <= 0 or numdiv >= numsln:
+        numdiv = numsln
+    while numsln % numdiv:
+        numdiv += 1
+    def weights(path, n):
+        if os.path.exists(path):
+            t = read_table(path)
+            return t[:n, 1].astype(np.float64), t
+        return np.ones(n), None
+    wsln, _ = weights(os.path.join(soln_dir, "weight_soln"), numsln)
+    wref, wref_tab = weights(os.path.join(refs_dir, "weight_refs"), numref)
+    wref = wref / wref.sum()
+    refs = [read_engfile(os.path.join(refs_dir, f"engref.{s}")) for s in rsuf]
+    middle, spec = refs[0]["middle"], refs[0]["spec"]
+    n = len(middle)
+    rr = sum(w * r["ratio"] for w, r in zip(wref, refs))
+    chi = sum(w * read_corfile(os.path.join(refs_dir, f"corref.{s}"), n) for w, s in zip(wref, rsuf))
+    slf = 0.0
+    if slfslt:
+        if wref_tab is None or wref_tab.shape[1] < 3:
+            raise ValueError("slfslt needs the self energies of weight_refs")
+        slf = float(np.dot(wref, wref_tab[:numref, 2]))
+    uvene = read_table(os.path.join(soln_dir, "aveuv.tt"))[:numsln, 1:]
+    per = numsln // numdiv
+    f = delta_mu_gpu if gpu else delta_mu
+    kw = dict(device=device) if gpu else {}
+    blocks = []
+    for b in range(numdiv):
+        idx = range(b * per, (b + 1) * per)
+        w = wsln[list(idx)] / wsln[list(idx)].sum()
+        runs = [read_engfile(os.path.join(soln_dir, f"engsln.{ssuf[i]}")) for i in idx]
+        if any(not np.array_equal(r["spec"], spec) or not np.allclose(r["left"], refs[0]["left"]) for r in runs):
+            raise ValueError("solution and reference-solvent energy coordinates are inconsistent")
+        rd = sum(wi * r["ratio"] for wi, r in zip(w, runs))
+        aveuv = w @ uvene[list(idx)]
+        blocks.append(f(rd, rr, chi, middle, spec, temp_K, aveuv, slf, group=group, **kw)[1])
+    blocks = np.array(blocks)
+    mean = float(blocks.mean())
+    err = None
+    if numdiv > 1:
+        std = np.sqrt(numdiv / (numdiv - 1.0)) * np.sqrt(max((blocks ** 2).mean() - mean ** 2, 0.0))
+        err = float(2.0 * std / np.sqrt(numdiv))
+    return dict(blocks=blocks, mean=mean, error95=err, numdiv=numdiv, group=group)

@@ -229,3 +229,38 @@ def test_gpu_engine_files_match_oracle(engine_lib, oracle_mod, tmp_path):
         assert e["ratio"].sum() == pytest.approx(norm["edens"].sum(), rel=5e-5)
         # bins identical except energies at a mesh edge: a few counts move to a neighbour
         assert np.abs(e["ratio"] - norm["edens"]).sum() <= 1e-3 * norm["edens"].sum()
+
+
+def test_slvfe_merge_mode_over_divisions(engine_lib, oracle_mod, tmp_path):
+    """erdst's division files -> slvfe's merge mode (datread / wrtmerge): per-block delta mu from
+    the weight-averaged runs, the mean and the 95 % error 2 s / sqrt(n)."""
+    w = S.make_workload(1, small=True)
+    sd, rd = tmp_path / "soln", tmp_path / "refs"
+    erdst.run(w.params, w.topo, w.hist, _history(tmp_path, w, 4, name="sln.dcd"), sd, maxcnf=4, engdiv=4,
+              engine=OracleEngine(oracle_mod, w.params, w.topo, w.hist))
+    topo = S.Topology([S.water(), S.lj_site()], [w.nside ** 3, 1], [A.PT_SOLVENT, A.PT_TEST_RIGID])
+    prm = S.default_params(ms1max=32, maxins=500, selfcal=0)
+    wr = S.Workload("refs-ljsite", prm, topo, w.hist, w.box, w.nside, 4, w.seed + 11)
+    erdst.run(prm, topo, w.hist, _history(tmp_path, wr, 4, name="ref.dcd"), rd, maxcnf=4, engdiv=2,
+              engine=OracleEngine(oracle_mod, prm, topo, w.hist))
+    out = SF.merge_mode(sd, rd, 300.0, numdiv=2, group=3)
+    assert out["numdiv"] == 2 and len(out["blocks"]) == 2
+    # block 1 by hand: soln runs 1-2 weighted by weight_soln, refs runs 1-2 by weight_refs
+    ws = SF.read_table(sd / "weight_soln")[:, 1]
+    wrf = SF.read_table(rd / "weight_refs")[:, 1]
+    wrf = wrf / wrf.sum()
+    e = [SF.read_engfile(sd / f"engsln.{i:02d}") for i in (1, 2)]
+    r = [SF.read_engfile(rd / f"engref.{i:02d}") for i in (1, 2)]
+    n = len(e[0]["ratio"])
+    chi = sum(wi * SF.read_corfile(rd / f"corref.{i:02d}", n) for wi, i in zip(wrf, (1, 2)))
+    wb = ws[:2] / ws[:2].sum()
+    uv = SF.read_table(sd / "aveuv.tt")[:2, 1:]
+    dm = SF.delta_mu(wb[0] * e[0]["ratio"] + wb[1] * e[1]["ratio"], wrf[0] * r[0]["ratio"] + wrf[1] * r[1]["ratio"],
+                     chi, e[0]["middle"], e[0]["spec"], 300.0, wb @ uv, group=3)[1]
+    assert out["blocks"][0] == pytest.approx(dm, rel=1e-12, abs=1e-12)
+    b = out["blocks"]
+    assert out["mean"] == pytest.approx(b.mean(), rel=1e-14)
+    assert out["error95"] == pytest.approx(2.0 * np.std(b, ddof=1) / np.sqrt(2), rel=1e-9)
+    # numdiv that does not divide the runs moves up to the next divisor; 0 takes every run
+    assert SF.merge_mode(sd, rd, 300.0, numdiv=3, group=3)["numdiv"] == 4
+    assert SF.merge_mode(sd, rd, 300.0, numdiv=0, group=3)["numdiv"] == 4
