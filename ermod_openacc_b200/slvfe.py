@@ -26,7 +26,7 @@ from __future__ import annotations
 import numpy as np
 
 __all__ = ["kT_of", "delta_mu", "delta_mu_gpu", "merge_bins", "representative_bins", "read_engfile", "read_corfile",
-           "read_table", "delta_mu_from_files", "merge_mode"]
+           "read_table", "delta_mu_from_files", "merge_mode", "merge_scan"]
 
 
 def kT_of(temp_K: float) -> float:
@@ -375,6 +375,17 @@ def _suffixes(directory, prefix):
     if prefix + ".tt" in names:
         return ["tt"]
     raise FileNotFoundError(f"no {prefix} files in {directory}")
+
+
+def merge_scan(soln_dir, refs_dir, temp_K: float, numdiv: int = 0, groups=(1, 2, 3, 4, 5), pickgr: int = 3,
+               slfslt: bool = False, gpu: bool = False, device: int = 0) -> dict:
+    """slvfe's merge mode over the default parameter sets of infchk 'not' (numprm 5: groups
+    1..5 with inft 0, slvfe.F90:193-199): the table per group, and the headline at group
+    pickgr (sfemain.F90:55)."""
+    table = {g: merge_mode(soln_dir, refs_dir, temp_K, numdiv, g, slfslt, gpu, device) for g in groups}
+    if pickgr not in table:
+        raise ValueError(f"pickgr {pickgr} is not among the groups {tuple(groups)}")
+    return dict(table=table, picked=table[pickgr], pickgr=pickgr)
 
 
 def merge_mode(soln_dir, refs_dir, temp_K: float, numdiv: int = 0, group: int = 3, slfslt: bool = False,
