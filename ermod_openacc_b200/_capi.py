@@ -175,7 +175,8 @@ SIGNATURES = {
     "ermod_io_last_error": (C.c_char_p, []),
     "ermod_rmsd_bestfit": (C.c_double, [C.c_int32, _f32p, _f32p, _f32p]),
     # include/ermod_slvfe.h
-    "ermod_slvfe_delta_mu": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, _f64p, _f64p, _f64p, _f64p,
+    "ermod_slvfe_delta_mu": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _f64p, _f64p,
+                                         _f64p, _f64p,
                                          _i32p,
                                          C.c_double, _f64p, C.c_double, _f64p, _f64p]),
     "ermod_slvfe_last_error": (C.c_char_p, []),

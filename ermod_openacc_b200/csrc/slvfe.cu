@@ -451,22 +451,31 @@ cudaError_t dalloc(T** p, size_t n) { return cudaMalloc((void**)p, sizeof(T) * (
 
 extern "C" const char* ermod_slvfe_last_error(void) { return g_err; }
 
-extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n0, int32_t nsp, int32_t group,
+extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n0, int32_t nsp, int32_t group, int32_t inft,
                                         const double* rho_sln, const double* rho_ref, const double* chi_ref,
                                         const double* crd, const int32_t* spec, double kT, const double* aveuv,
                                         double slfeng, double* chmpt, double* total) {
-  if (n0 < 2 || nsp < 1 || nsp > kMaxSpecies || group < 1 || !rho_sln || !rho_ref || !chi_ref || !crd || !spec ||
+  if (n0 < 2 || nsp < 1 || nsp > kMaxSpecies || group < 1 || inft < 0 || inft > 100 || !rho_sln || !rho_ref || !chi_ref || !crd || !spec ||
       !aveuv || !chmpt || !(kT > 0.0))
     return fail(ERMOD_ERR_ARG, "slv_arg");
   for (int i = 0; i < n0; ++i)
     if (spec[i] < 1 || spec[i] > nsp || (i > 0 && spec[i] < spec[i - 1])) return fail(ERMOD_ERR_ARG, "slv_arg");
-  // chmpot's grouping (slvfe.F90:613-640): per species floor(bins / group) merged bins, the last
-  // one taking the remainder; the index bookkeeping is host work, the sums run on the device
+  // chmpot's grouping (slvfe.F90:613-640): per species (bins - rduvcore * inft / 100) / group
+  // merged bins, the last one taking the rest; rduvcore, the bins since the coordinate spacing
+  // last stayed constant, counted as datread does (slvfe.F90:114-135).  The index bookkeeping
+  // is host work, the sums run on the device.
   std::vector<int4> rng;
   for (int i = 0; i < n0;) {
     int j = i;
     while (j < n0 && spec[j] == spec[i]) ++j;
-    const int m = (j - i) / group;
+    int core = 0;
+    double dprev = 0.0;
+    for (int q = i + 1; q < j; ++q) {
+      const double d = crd[q] - crd[q - 1];
+      if (q - i + 1 > 2) core = std::fabs(d - dprev) < 1.0e-8 ? 0 : core + 1;
+      dprev = d;
+    }
+    const int m = (j - i - core * inft / 100) / group;
     if (m < 1) return fail(ERMOD_ERR_ARG, "slv_grp");
     for (int q = 0; q < m; ++q)
       rng.push_back(make_int4(i + q * group, q < m - 1 ? i + (q + 1) * group : j, q == m - 1 ? 1 : 0, 0));

@@ -95,11 +95,31 @@ def _zero_bin(crd, dens, mask, tiny=1.0e-8):
     return k
 
 
-def merge_groups(uvspec, group: int):
-    """chmpot's bin grouping with inft = 0 (slvfe.F90:609-640): per species, `group`
-    consecutive bins form one merged bin and the last merged bin also takes the remainder.
-    Returns (merged index of every bin, start and end of every merged bin, 1 for the last
-    merged bin of each species)."""
+def core_counts(uvcrd, uvspec, tiny: float = 1.0e-8):
+    """rduvcore per species as datread counts it from the bin coordinates (slvfe.F90:114-135):
+    the bins since the spacing last stayed constant, i.e. the logarithmic core mesh."""
+    crd = np.asarray(uvcrd, dtype=np.float64)
+    spec = np.asarray(uvspec)
+    out = {}
+    for i in range(len(crd)):
+        p = int(spec[i])
+        if i == 0 or spec[i - 1] != p:
+            cnt, core, prev_d = 1, 0, None
+        else:
+            cnt += 1
+            d = crd[i] - crd[i - 1]
+            if cnt > 2:
+                core = 0 if abs(d - prev_d) < tiny else core + 1
+            prev_d = d
+        out[p] = core
+    return out
+
+
+def merge_groups(uvspec, group: int, core=None, inft: int = 0):
+    """chmpot's bin grouping (slvfe.F90:609-640): per species, `group` consecutive bins form
+    one merged bin; with inft the last rduvcore * inft / 100 bins of the core mesh go into
+    the species' last merged bin too, which also takes the remainder.  Returns (merged index
+    of every bin, start and end of every merged bin, 1 for the last merged bin of each species)."""
     spec = np.asarray(uvspec)
     n = len(spec)
     idr = np.zeros(n, dtype=np.int64)
@@ -109,7 +129,8 @@ def merge_groups(uvspec, group: int):
         j = i
         while j < n and spec[j] == spec[i]:
             j += 1
-        m = (j - i) // group
+        kc = (core[int(spec[i])] * inft) // 100 if inft else 0
+        m = (j - i - kc) // group
         if m < 1:
             raise ValueError(f"species {spec[i]} has fewer bins than the group size {group}")
         idr[i:j] = len(starts) + np.minimum(np.arange(j - i) // group, m - 1)
@@ -121,11 +142,12 @@ def merge_groups(uvspec, group: int):
     return idr, np.array(starts), np.array(ends), np.array(last)
 
 
-def merge_bins(edist, edens, ecorr, uvcrd, uvspec, group: int):
+def merge_bins(edist, edens, ecorr, uvcrd, uvspec, group: int, inft: int = 0):
     """The merged distributions, correlation matrix, coordinates and species
     (slvfe.F90:642-698): sums over each group, the mean coordinate, and the species'
     last original coordinate for its last merged bin."""
-    idr, st, en, last = merge_groups(uvspec, group)
+    core = core_counts(uvcrd, uvspec) if inft else None
+    idr, st, en, last = merge_groups(uvspec, group, core, inft)
     P = np.zeros((len(st), len(idr)))
     P[idr, np.arange(len(idr))] = 1.0
     crd = np.asarray(uvcrd, dtype=np.float64)
@@ -136,7 +158,8 @@ def merge_bins(edist, edens, ecorr, uvcrd, uvspec, group: int):
             np.asarray(uvspec)[st])
 
 
-def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0, group: int = 1):
+def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0, group: int = 1,
+             inft: int = 0):
     """(per-species solvation free energies, total) in kcal/mol.
 
     group > 1 first merges that many consecutive bins per species: chmpot's grouping with
@@ -145,8 +168,8 @@ def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: f
     # the sampled-bin thresholds use the smallest values of the data as read (slvfe.F90:884-885)
     rd_min = float(np.min(np.asarray(edist)[np.asarray(edist) > 0.0]))
     rr_min = float(np.min(np.asarray(edens)[np.asarray(edens) > 0.0]))
-    if group > 1:
-        edist, edens, ecorr, uvcrd, uvspec = merge_bins(edist, edens, ecorr, uvcrd, uvspec, group)
+    if group > 1 or inft:
+        edist, edens, ecorr, uvcrd, uvspec = merge_bins(edist, edens, ecorr, uvcrd, uvspec, group, inft)
     return _delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng, rd_min, rr_min)
 
 
@@ -318,7 +341,7 @@ def read_table(path) -> np.ndarray:
 
 
 def delta_mu_gpu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0,
-                 device: int = 0, group: int = 1):
+                 device: int = 0, group: int = 1, inft: int = 0):
     """delta_mu on the GPU (include/ermod_slvfe.h): the same functional, options and
     arguments, FP64 CUDA kernels.  Raises RuntimeError with slvfe's failure name; there is
     no eigenvalue fallback on this path."""
@@ -334,7 +357,7 @@ def delta_mu_gpu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfen
     nsp = int(spec.max())
     out = np.zeros(nsp)
     tot = C.c_double()
-    rc = lib.ermod_slvfe_delta_mu(device, len(rd), nsp, group, A.ptr(rd, C.c_double), A.ptr(rr, C.c_double),
+    rc = lib.ermod_slvfe_delta_mu(device, len(rd), nsp, group, inft, A.ptr(rd, C.c_double), A.ptr(rr, C.c_double),
                                   chi.ctypes.data_as(C.POINTER(C.c_double)), A.ptr(crd, C.c_double),
                                   A.ptr(spec, C.c_int32), kT_of(temp_K), A.ptr(av, C.c_double), float(slfeng),
                                   A.ptr(out, C.c_double), C.byref(tot))
@@ -377,19 +400,25 @@ def _suffixes(directory, prefix):
     raise FileNotFoundError(f"no {prefix} files in {directory}")
 
 
-def merge_scan(soln_dir, refs_dir, temp_K: float, numdiv: int = 0, groups=(1, 2, 3, 4, 5), pickgr: int = 3,
+# (group, inft) of slvfe's default parameter sets (slvfe.F90:177-199)
+PARAMS_INFCHK_NOT = tuple((g, 0) for g in range(1, 6))
+PARAMS_INFCHK_YES = ((1, 0), (1, 60), (1, 80), (1, 100), (2, 0), (3, 0), (4, 0), (5, 0), (5, 60), (5, 80), (5, 100))
+
+
+def merge_scan(soln_dir, refs_dir, temp_K: float, numdiv: int = 0, infchk: bool = False, pickgr: int = 3,
                slfslt: bool = False, gpu: bool = False, device: int = 0) -> dict:
-    """slvfe's merge mode over the default parameter sets of infchk 'not' (numprm 5: groups
-    1..5 with inft 0, slvfe.F90:193-199): the table per group, and the headline at group
-    pickgr (sfemain.F90:55)."""
-    table = {g: merge_mode(soln_dir, refs_dir, temp_K, numdiv, g, slfslt, gpu, device) for g in groups}
-    if pickgr not in table:
-        raise ValueError(f"pickgr {pickgr} is not among the groups {tuple(groups)}")
-    return dict(table=table, picked=table[pickgr], pickgr=pickgr)
+    """slvfe's merge mode over its default parameter sets (numprm 5 with infchk 'not', 11 with
+    'yes'; slvfe.F90:177-199): the table per (group, inft), and the headline at
+    (pickgr, inft 0) (sfemain.F90:55, slvfe.F90:1647)."""
+    sets = PARAMS_INFCHK_YES if infchk else PARAMS_INFCHK_NOT
+    table = {(g, i): merge_mode(soln_dir, refs_dir, temp_K, numdiv, g, slfslt, gpu, device, inft=i) for g, i in sets}
+    if (pickgr, 0) not in table:
+        raise ValueError(f"pickgr {pickgr} is not among the parameter sets")
+    return dict(table=table, picked=table[(pickgr, 0)], pickgr=pickgr)
 
 
 def merge_mode(soln_dir, refs_dir, temp_K: float, numdiv: int = 0, group: int = 3, slfslt: bool = False,
-               gpu: bool = False, device: int = 0) -> dict:
+               gpu: bool = False, device: int = 0, inft: int = 0) -> dict:
     """slvfe's clcond 'merge' for one (group, inft 0): the solution runs engsln.NN split into
     numdiv blocks, each block's distribution and aveuv the weight_soln-weighted mean of its
     runs; the reference-solvent runs engref.NN / corref.NN merged over all runs with
@@ -436,11 +465,11 @@ def merge_mode(soln_dir, refs_dir, temp_K: float, numdiv: int = 0, group: int = 
             raise ValueError("solution and reference-solvent energy coordinates are inconsistent")
         rd = sum(wi * r["ratio"] for wi, r in zip(w, runs))
         aveuv = w @ uvene[list(idx)]
-        blocks.append(f(rd, rr, chi, middle, spec, temp_K, aveuv, slf, group=group, **kw)[1])
+        blocks.append(f(rd, rr, chi, middle, spec, temp_K, aveuv, slf, group=group, inft=inft, **kw)[1])
     blocks = np.array(blocks)
     mean = float(blocks.mean())
     err = None
     if numdiv > 1:
         std = np.sqrt(numdiv / (numdiv - 1.0)) * np.sqrt(max((blocks ** 2).mean() - mean ** 2, 0.0))
         err = float(2.0 * std / np.sqrt(numdiv))
-    return dict(blocks=blocks, mean=mean, error95=err, numdiv=numdiv, group=group)
+    return dict(blocks=blocks, mean=mean, error95=err, numdiv=numdiv, group=group, inft=inft)

@@ -27,6 +27,8 @@ extern "C" {
  * group         bins merged per species first (chmpot's grouping with inft 0,
  *               slvfe.F90:609-698; the reference reports group 3 in its range / merge
  *               modes, sfemain.F90:55); 1 = the mesh as read
+ * inft          percentage (0..100) of each species' core bins (rduvcore, counted from
+ *               crd as datread does) that join its last merged bin (slvfe.F90:613-615)
  * kT            kcal/mol (temp * 8.314510e-3 / 4.184, slvfe.F90:272)
  * aveuv [nsp]   average solute-solvent energy per species in solution
  * slfeng        solute self energy (slfslt 'yes'), else 0
@@ -39,7 +41,8 @@ extern "C" {
  *   "slv_zer" a species' mesh has no bin pair around zero energy.
  * ERMOD_ERR_ARG "slv_grp" when a species has fewer bins than `group`.
  */
-int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n, int32_t nsp, int32_t group, const double* rho_sln,
+int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n, int32_t nsp, int32_t group, int32_t inft,
+                             const double* rho_sln,
                              const double* rho_ref, const double* chi_ref, const double* crd,
                              const int32_t* spec, double kT, const double* aveuv, double slfeng,
                              double* chmpt, double* total);

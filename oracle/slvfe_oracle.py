@@ -105,9 +105,34 @@ def _zeroec(pti, edvec, uvcrd, uvspec, tiny=1.0e-8):
     return k
 
 
-def merge_bins(rddst, rddns, rdcor, rdcrd, rdspec, group):
-    """chmpot's grouping of `group` consecutive bins per species with inft = 0
-    (slvfe.F90:609-698), in the reference's loop order, 1-based indices as there."""
+def _rduvcore(rdcrd, rdspec, tiny=1.0e-8):
+    """datread's count of the core (non-uniformly spaced) bins per species (slvfe.F90:114-135)."""
+    rduvmax, rduvcore = {}, {}
+    k = 0
+    crdprev = crddif_prev = 0.0
+    for iduv in range(len(rdcrd)):
+        pti, crdnow = int(rdspec[iduv]), float(rdcrd[iduv])
+        if pti != k:
+            rduvmax[pti] = 1
+            rduvcore[pti] = 0
+            k = pti
+        else:
+            rduvmax[pti] += 1
+            crddif_now = crdnow - crdprev
+            if rduvmax[pti] > 2:
+                if abs(crddif_now - crddif_prev) < tiny:
+                    rduvcore[pti] = 0
+                else:
+                    rduvcore[pti] += 1
+            crddif_prev = crddif_now
+        crdprev = crdnow
+    return rduvcore
+
+
+def merge_bins(rddst, rddns, rdcor, rdcrd, rdspec, group, inft=0):
+    """chmpot's grouping of `group` consecutive bins per species (slvfe.F90:609-698), the
+    last rduvcore * inft / 100 core bins joining the last merged bin, in the reference's
+    loop order, 1-based indices as there."""
     rddst, rddns, rdcor = (np.asarray(x, dtype=np.float64) for x in (rddst, rddns, rdcor))
     rdcrd = np.asarray(rdcrd, dtype=np.float64)
     rdspec = np.asarray(rdspec)
@@ -116,11 +141,12 @@ def merge_bins(rddst, rddns, rdcor, rdcrd, rdspec, group):
     rduvmax = [0] * (numslv + 1)
     for iduv in range(ermax):
         rduvmax[int(rdspec[iduv])] += 1
+    rduvcore = _rduvcore(rdcrd, rdspec)
     uvmax = [0] * (numslv + 1)
     idrduv = [0] * (ermax + 1)
     gemax = 0
     for pti in range(1, numslv + 1):
-        k = 0                                   # rduvcore(pti) * inft / 100 with inft = 0
+        k = rduvcore[pti] * inft // 100
         m = (rduvmax[pti] - k) // group
         uvmax[pti] = m
         gemax += m
@@ -165,7 +191,7 @@ def merge_bins(rddst, rddns, rdcor, rdcrd, rdspec, group):
             np.array(uvspec[1:]))
 
 
-def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0, group=1):
+def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0, group=1, inft=0):
     """Solvation free energy (kcal/mol) per solvent species and in total.
 
     edist  solution energy distribution per bin (engsln), edens / ecorr the
@@ -178,8 +204,8 @@ def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0, grou
     # getslncv's thresholds use the smallest sampled values of the data as read (slvfe.F90:884-885)
     min_rddst = np.asarray(edist, dtype=np.float64)[np.asarray(edist) > 0.0].min()
     min_rddns = np.asarray(edens, dtype=np.float64)[np.asarray(edens) > 0.0].min()
-    if group > 1:
-        edist, edens, ecorr, uvcrd, uvspec = merge_bins(edist, edens, ecorr, uvcrd, uvspec, group)
+    if group > 1 or inft:
+        edist, edens, ecorr, uvcrd, uvspec = merge_bins(edist, edens, ecorr, uvcrd, uvspec, group, inft)
     rddst = np.asarray(edist, dtype=np.float64)
     rddns = np.asarray(edens, dtype=np.float64)
     rdcor = np.asarray(ecorr, dtype=np.float64)

@@ -266,5 +266,5 @@ def test_slvfe_merge_mode_over_divisions(engine_lib, oracle_mod, tmp_path):
     assert SF.merge_mode(sd, rd, 300.0, numdiv=0, group=3)["numdiv"] == 4
     # the default scan of groups 1..5, headlined at pickgr 3
     scan = SF.merge_scan(sd, rd, 300.0, numdiv=2)
-    assert sorted(scan["table"]) == [1, 2, 3, 4, 5] and scan["pickgr"] == 3
+    assert sorted(scan["table"]) == [(g, 0) for g in range(1, 6)] and scan["pickgr"] == 3
     assert scan["picked"]["mean"] == pytest.approx(out["mean"], rel=1e-14)

@@ -119,15 +119,17 @@ def test_gpu_functional_two_species(engine_lib):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("group", [1, 3])
-def test_gpu_functional_on_engine_distributions(engine_lib, oracle_mod, group):
+@pytest.mark.parametrize("group,inft", [(1, 0), (3, 0), (5, 80)])
+def test_gpu_functional_on_engine_distributions(engine_lib, oracle_mod, group, inft):
     """rho, rho0 and chi0 from the FP64 oracle engine (LJ site in water), bin middles as slvfe
-    reads them; group 3 is the bin merging the reference reports (pickgr)."""
+    reads them; group 3 is the bin merging the reference reports (pickgr), (5, 80) one of the
+    infchk 'yes' sets."""
     orc, sln, rfa = _distributions(oracle_mod)
     _, middle, _, spec = SF.representative_bins(orc.uvcrd, orc.uvmax, orc.uvsoft)
     aveuv = [float(sln["slnuv"][0])]
-    a = SF.delta_mu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv, group=group)
-    b = SF.delta_mu_gpu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv, group=group)
+    a = SF.delta_mu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv, group=group, inft=inft)
+    b = SF.delta_mu_gpu(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, 300.0, aveuv, group=group,
+                        inft=inft)
     assert np.isfinite(b[1])
     # a 1396-bin regularised solve: FP64 rounding of two Cholesky orders, far below slvfe's 0.01
     assert b[1] == pytest.approx(a[1], abs=1e-6)
@@ -178,3 +180,19 @@ def test_gpu_functional_merged_bins(engine_lib, group):
     np.testing.assert_allclose(b[0], a[0], rtol=1e-9, atol=1e-9)
     with pytest.raises(RuntimeError, match="slv_grp"):
         SF.delta_mu_gpu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], group=1000)
+
+
+@pytest.mark.parametrize("group,inft", [(1, 60), (1, 100), (5, 80), (2, 0)])
+def test_core_merging_matches_restatement(oracle_mod, slvfe_oracle, group, inft):
+    """inft > 0 (infchk 'yes'): the last rduvcore * inft / 100 core bins of each species join
+    its last merged bin; rduvcore counted from the bin coordinates as datread does, on the
+    engine's own mesh (linear soft region, logarithmic core)."""
+    orc, sln, rfa = _distributions(oracle_mod)
+    _, middle, _, spec = SF.representative_bins(orc.uvcrd, orc.uvmax, orc.uvsoft)
+    core = SF.core_counts(middle, spec)[1]
+    assert core > 50                     # the logarithmic core of the mesh
+    a = SF.merge_bins(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, group, inft)
+    b = slvfe_oracle.merge_bins(sln["edens"], rfa["edens"], rfa["ecorr"], middle, spec, group, inft)
+    assert len(a[0]) == (len(middle) - core * inft // 100) // group
+    for x, y in zip(a, b):
+        np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-12)
