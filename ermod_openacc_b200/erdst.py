@@ -10,9 +10,14 @@
     with its SltWght weight and the insstructure RMSD filter (getsolute,
     insertion.F90:393-543), wrapping around at the end of either file;
   * engstore normalises and writes the division's files (engproc.F90:630-722).
-The MPI frame distribution and the namelist parsing stay outside: the caller
-passes &ene_param as a dict and the topology objects of
-`ermod_openacc_b200.systems`.
+With a torch.distributed process group the frames are shared as
+getconf_parallel shares them among MPI ranks (setconf.F90:931-980): each batch
+of world-size frames gives rank r its r-th frame, numbered stnum + r + 1; the
+SltConf conformations go to the ranks in turn, per insertion, as getsolute
+hands them out (insertion.F90:458-528); engstore reduces over the ranks
+(ermod_openacc_b200.parallel) and rank 0 writes the files.  The namelist
+parsing stays outside: the caller passes &ene_param as a dict and the topology
+objects of `ermod_openacc_b200.systems`.
 """
 from __future__ import annotations
 
@@ -114,13 +119,21 @@ class _SoluteSource:
 
 def run(params: dict, topo, hist: dict | None, history, outdir, maxcnf: int, skpcnf: int = 1, engdiv: int = 1,
         syswgt=None, permutation=None, sltconf=None, sltwgt=None, insstructure: int = INSSTR_NOREJECT,
-        lwstr: float = 0.0, upstr: float = 0.0, refslt=None, engine=None, device: int = 0) -> dict:
+        lwstr: float = 0.0, upstr: float = 0.0, refslt=None, engine=None, device: int = 0, dist_group=None,
+        reduce_device=None) -> dict:
     """One erdst run over the HISTORY trajectory `history`, writing engstore's files into
     `outdir`.  permutation: 1-based target index of each HISTORY atom (the permutation file
     of getconf_parallel); syswgt / sltwgt: weight files; sltconf: the SltConf trajectory of
     a flexible solute; refslt: (coordinates, weights) of RefInfo's solute for insstructure 1.
-    `engine` is a ready context with engclear / engconst / engstore (an `Engine` is made
-    on `device` when None).  Returns avediv, aveuv and the frames processed."""
+    `engine` is a ready context with engclear / engconst / engstore / accum (an `Engine` is
+    made on `device` when None).  dist_group: a torch.distributed group to share the frames
+    over (None: this process alone); reduce_device: where the cross-rank sums run ("cuda:N"
+    for NCCL, None for gloo on the host).  Returns avediv, aveuv and the frames this rank
+    processed."""
+    world, rank = 1, 0
+    if dist_group is not None:
+        import torch.distributed as dist
+        world, rank = dist.get_world_size(dist_group), dist.get_rank(dist_group)
     frames_per_div = maxcnf // skpcnf // engdiv if skpcnf > 0 and engdiv > 0 else 0
     if frames_per_div <= 0:
         raise IO.IOError_(A.ERMOD_ERR_ARG, "eng_par")
@@ -152,38 +165,57 @@ def run(params: dict, topo, hist: dict | None, history, outdir, maxcnf: int, skp
     avediv = np.zeros((engdiv, 2))
     aveuv = np.zeros((engdiv, topo.numslv), dtype=np.float32) if soln else None
     stnum = 0
+    processed = 0
     try:
         for div in range(1, engdiv + 1):
             engine.engclear()
-            for _ in range(frames_per_div):
-                pos = cell = None
-                weight = 1.0
-                for _ in range(skpcnf):
-                    fr = traj.read()
-                    if fr is None:
-                        raise IO.IOError_(A.ERR_FORMAT, "set_trj")
-                    pos, cell = fr
-                    weight = wsys.next() if wsys else 1.0
-                if perm is not None:
-                    p3 = pos.reshape(-1, 3)
+            done = 0
+            while done < frames_per_div:
+                nread = min(world, frames_per_div - done)   # getconf_parallel's batch
+                mine = None
+                for iproc in range(nread):
+                    pos = cell = None
+                    weight = 1.0
+                    for _ in range(skpcnf):
+                        fr = traj.read()
+                        if fr is None:
+                            raise IO.IOError_(A.ERR_FORMAT, "set_trj")
+                        pos, cell = fr
+                        weight = wsys.next() if wsys else 1.0
+                    if iproc == rank:
+                        mine = (pos, cell, weight)
+                if perm is not None and mine is not None:
+                    p3 = mine[0].reshape(-1, 3)
                     out = np.empty_like(p3)
                     out[perm] = p3
-                    pos = out.ravel()
-                stnum += 1
+                    mine = (out.ravel(), mine[1], mine[2])
                 kw = {}
                 if flex:
-                    conf, wgt = src.batch(params["maxins"])
-                    kw = dict(ins_conf=conf.ravel(), ins_weight=wgt)
-                rc = engine.engconst(stnum, pos, cell, weight, **kw)
-                if rc < 0:
-                    raise IO.IOError_(rc, "eng_cns")
-            norm, av = engine.engstore()
+                    # getsolute: per insertion, one conformation for each active rank in turn
+                    nins = params["maxins"]
+                    confs, wgts = src.batch(nins * nread)
+                    sel = np.arange(nins) * nread + rank
+                    if rank < nread:
+                        kw = dict(ins_conf=confs[sel].ravel(), ins_weight=wgts[sel])
+                if rank < nread:
+                    rc = engine.engconst(stnum + rank + 1, mine[0], mine[1], mine[2], **kw)
+                    if rc < 0:
+                        raise IO.IOError_(rc, "eng_cns")
+                    processed += 1
+                stnum += nread
+                done += nread
+            if world > 1:
+                from . import parallel
+                norm, av = parallel.engstore_all(engine, group=dist_group, device=reduce_device)
+            else:
+                norm, av = engine.engstore()
             avediv[div - 1] = av
             if soln:
                 aveuv[div - 1] = norm["slnuv"]
-            IO.write_engstore(outdir, params, mesh, norm, div, engdiv, avediv, aveuv)
+            if rank == 0:
+                IO.write_engstore(outdir, params, mesh, norm, div, engdiv, avediv, aveuv)
     finally:
         traj.close()
         if src is not None:
             src.close()
-    return dict(avediv=avediv, aveuv=aveuv, frames=stnum)
+    return dict(avediv=avediv, aveuv=aveuv, frames=processed)

@@ -32,6 +32,9 @@ class OracleEngine:
                                ins_weight=None if ins_weight is None else ins_weight.copy()))
         return self.o.engconst(stnum, pos, cell, w, ins_conf=ins_conf, ins_weight=ins_weight)
 
+    def accum(self):
+        return self.o.accum()
+
     def engstore(self):
         raw = self.o.accum()
         norm = self.o.accum(normalise=True)
@@ -268,3 +271,50 @@ def test_slvfe_merge_mode_over_divisions(engine_lib, oracle_mod, tmp_path):
     scan = SF.merge_scan(sd, rd, 300.0, numdiv=2)
     assert sorted(scan["table"]) == [(g, 0) for g in range(1, 6)] and scan["pickgr"] == 3
     assert scan["picked"]["mean"] == pytest.approx(out["mean"], rel=1e-14)
+
+
+
+def _dist_rank(rank, port, hist_path, outdir, engdiv):
+    import os
+    import torch.distributed as dist
+    import oracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    w = S.make_workload(2, small=True, maxins=24)
+    prm = dict(w.params, selfcal=1)
+    eng = OracleEngine(oracle, prm, w.topo, w.hist)
+    res = erdst.run(prm, w.topo, w.hist, hist_path, outdir, maxcnf=4, engdiv=engdiv, engine=eng,
+                    dist_group=dist.group.WORLD)
+    assert res["frames"] == 4 // 2
+    # the reference's frame numbering: rank r takes frames r+1, r+3 (stnum + r + 1 per batch)
+    assert [c["stnum"] for c in eng.calls] == [rank + 1, rank + 3]
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_frames_shared_over_two_ranks_match_one_process(engine_lib, oracle_mod, tmp_path):
+    """getconf_parallel's frame sharing and engstore's reduction on two gloo ranks (CPU): rank 0's
+    files equal those of one process that ran every frame, to the rounding of the voffset rescale."""
+    import socket
+    import torch.multiprocessing as mp
+    w = S.make_workload(2, small=True, maxins=24)
+    prm = dict(w.params, selfcal=1)
+    hist_path = _history(tmp_path, w, 4)
+    one = OracleEngine(oracle_mod, prm, w.topo, w.hist)
+    erdst.run(prm, w.topo, w.hist, hist_path, tmp_path / "one", maxcnf=4, engdiv=2, engine=one)
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    mp.spawn(_dist_rank, args=(port, hist_path, tmp_path / "two", 2), nprocs=2, join=True)
+    assert sorted(os.listdir(tmp_path / "two")) == sorted(os.listdir(tmp_path / "one"))
+    for div in (1, 2):
+        a = SF.read_engfile(tmp_path / "one" / f"engref.{div:02d}")
+        b = SF.read_engfile(tmp_path / "two" / f"engref.{div:02d}")
+        np.testing.assert_allclose(b["ratio"], a["ratio"], rtol=1e-12, atol=1e-300)
+        n = len(a["ratio"])
+        np.testing.assert_allclose(SF.read_corfile(tmp_path / "two" / f"corref.{div:02d}", n),
+                                   SF.read_corfile(tmp_path / "one" / f"corref.{div:02d}", n), rtol=1e-12,
+                                   atol=1e-300)
+    t1, t2 = SF.read_table(tmp_path / "one" / "weight_refs"), SF.read_table(tmp_path / "two" / "weight_refs")
+    np.testing.assert_allclose(t2, t1, rtol=2e-7)
