@@ -318,3 +318,45 @@ def test_frames_shared_over_two_ranks_match_one_process(engine_lib, oracle_mod, 
                                    atol=1e-300)
     t1, t2 = SF.read_table(tmp_path / "one" / "weight_refs"), SF.read_table(tmp_path / "two" / "weight_refs")
     np.testing.assert_allclose(t2, t1, rtol=2e-7)
+
+
+def _dist_flex_rank(rank, port, root, out):
+    import os
+    import torch.distributed as dist
+    import oracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    import pathlib
+    root = pathlib.Path(root)
+    w, topo, prm, ref, confs = _flex_setup(root / f"r{rank}", nconf=7)
+    prm = dict(prm, maxins=3)
+    eng = OracleEngine(oracle, prm, topo, w.hist)
+    erdst.run(prm, topo, w.hist, root / "HISTORY.dcd", root / f"o{rank}", maxcnf=4, engine=eng,
+              sltconf=root / f"r{rank}" / "SltConf.dcd", sltwgt=root / f"r{rank}" / "SltWght",
+              dist_group=dist.group.WORLD)
+    got = np.concatenate([c["ins_conf"].reshape(-1, len(ref), 3) for c in eng.calls])
+    np.save(out.format(rank), got)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_conformations_handed_out_per_insertion_over_two_ranks(engine_lib, oracle_mod, tmp_path):
+    """getsolute on two ranks: per insertion, one SltConf conformation for each active rank in
+    turn (insertion.F90:458-528), wrapping around at the end of the file."""
+    import socket
+    import torch.multiprocessing as mp
+    w, topo, prm, ref, confs = _flex_setup(tmp_path, nconf=7)
+    _history(tmp_path, w, 4)
+    for r in (0, 1):
+        (tmp_path / f"r{r}").mkdir()
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = str(tmp_path / "conf{}.npy")
+    mp.spawn(_dist_flex_rank, args=(port, str(tmp_path), out), nprocs=2, join=True)
+    seq = np.arange(12) % 7          # 2 batches x 3 insertions x 2 ranks, in file order with wrap-around
+    for r in (0, 1):
+        got = np.load(out.format(r))
+        want = [seq[b * 6 + i * 2 + r] for b in range(2) for i in range(3)]
+        np.testing.assert_array_equal(got, np.asarray([confs[k] for k in want], dtype=np.float32))
