@@ -1,0 +1,34 @@
+"""bench.py's JSON contract where it can run without a GPU: the reference arm (the CPU port of
+the reference algorithm) and the helpers the roofline uses."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_line():
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0",
+                          "--ref-sample", "8"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
+    assert line["e2e"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["config"]["workload"] == "refs-ring12-water4096"
+
+
+def test_roofline_helpers():
+    sys.path.insert(0, ROOT)
+    import bench
+    from ermod_openacc_b200 import systems as S
+    assert bench.traffic_from_profiles("k_pme_plane") > 0
+    assert bench.traffic_from_profiles("no_such_kernel") is None
+    w = S.make_workload(2)
+    for stage in ("gather", "bin", "pme_plane", "site_tables"):
+        assert bench.kernel_bytes(stage, w, 32, 12288, 4096, 1396, 2000, 12) > 0
