@@ -21,11 +21,44 @@ LIB = os.path.join(HERE, "liboracle.so")
 _lib = None
 
 
+REF_DCD = os.path.join(HERE, "_ref", "libref_dcd.so")
+
+
 def build(force: bool = False) -> str:
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(
             os.path.join(HERE, "ermod_oracle.cpp")):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
+    # the reference's own DCD reader behind the test shim: built only where its sources are
+    if force or not os.path.exists(REF_DCD):
+        subprocess.run(["make", "-C", HERE, "-s", "ref"], check=False, capture_output=True)
     return LIB
+
+
+def ref_dcd_frames(path: str):
+    """Every frame of a DCD file as the reference's vendored VMD plugin reads it: a list of
+    (crd [3*natoms] float32, [A, B, C, alpha, beta, gamma] float32), or None when the
+    reference reader is not built here."""
+    if not os.path.exists(REF_DCD):
+        return None
+    L = C.CDLL(REF_DCD)
+    L.ref_dcd_open.restype = C.c_void_p
+    L.ref_dcd_open.argtypes = [C.c_char_p, C.POINTER(C.c_int)]
+    L.ref_dcd_read.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.ref_dcd_close.argtypes = [C.c_void_p]
+    na = C.c_int()
+    h = L.ref_dcd_open(os.fsencode(path), C.byref(na))
+    if not h:
+        raise RuntimeError(f"the reference DCD reader cannot open {path}")
+    frames = []
+    while True:
+        crd = np.zeros(3 * na.value, dtype=np.float32)
+        box = np.zeros(6, dtype=np.float32)
+        if L.ref_dcd_read(h, na.value, crd.ctypes.data_as(C.POINTER(C.c_float)),
+                          box.ctypes.data_as(C.POINTER(C.c_float))) != 0:
+            break
+        frames.append((crd, box))
+    L.ref_dcd_close(h)
+    return frames
 
 
 def lib():

@@ -287,3 +287,40 @@ def test_engstore_divisions(engine_lib, oracle_mod, tmp_path):
         IO.write_engstore(tmp_path, prm, mesh, norm, 4, 3, avediv)
     with pytest.raises(IO.IOError_, match="sto_opn"):
         IO.write_engstore(tmp_path / "no" / "such" / "dir", prm, mesh, norm, 1, 3, avediv)
+
+
+def _vmdfio_cell(box):
+    """vmdfio.c:355-373 on the plugin's FP32 A, B, C, alpha, beta, gamma."""
+    A_, B, Cc, al, be, ga = (float(v) for v in box)
+    x, y = np.cos(ga * np.pi / 180.0), np.sin(ga * np.pi / 180.0)
+    u = np.cos(be * np.pi / 180.0)
+    v = (np.cos(al * np.pi / 180.0) - x * u) / y
+    w = np.sqrt(1.0 - u * u - v * v)
+    return np.array([A_, 0, 0, B * x, B * y, 0, Cc * u, Cc * v, Cc * w], dtype=np.float32)
+
+
+@pytest.mark.parametrize("variant", ["charmm_cos_le", "charmm_cos_be", "namd_deg", "xplor", "triclinic", "dim4"])
+def test_dcd_reader_matches_reference_plugin(engine_lib, oracle_mod, tmp_path, variant):
+    """The library's reader against the reference's own DCD reader (its vendored VMD plugin,
+    built from source by the oracle recipe): the same coordinates, and the cell vmdfio builds."""
+    fr = _frames(3, natoms=11, seed=4)
+    par = (40.0, 42.0, 45.0, 70.0, 80.0, 100.0) if variant == "triclinic" else (31.0, 32.5, 33.0, 90.0, 90.0, 90.0)
+    kw = dict(cells=[cell_record(*par, cosines=variant != "namd_deg")] * 3)
+    if variant == "charmm_cos_be":
+        kw["end"] = ">"
+    if variant == "xplor":
+        kw = dict(cells=None, charmm=False)
+    if variant == "dim4":
+        kw["dim4"] = True
+    p = tmp_path / f"{variant}.dcd"
+    write_dcd(p, fr, **kw)
+    ref = oracle_mod.ref_dcd_frames(str(p))
+    if ref is None:
+        pytest.skip("the reference sources are not here to build its DCD reader")
+    with IO.Trajectory(p) as t:
+        ours = [t.read() for _ in range(len(ref) + 1)]
+    assert len(ref) == 3 and ours[-1] is None
+    for (crd, box), (c2, cell) in zip(ref, ours[:-1]):
+        np.testing.assert_array_equal(c2, crd)
+        if variant != "xplor":
+            np.testing.assert_allclose(cell, _vmdfio_cell(box), rtol=1e-6, atol=1e-5)
