@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "engine.cuh"
@@ -23,11 +24,15 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
 constexpr int kMaxDevices = 64;
 void* g_scratch_addr[kMaxDevices] = {};
+std::mutex g_scratch_mu;   // first calls from several host threads look the address up once
 
 // Device address of the scratch array on the current device (host code sees
 // only a host-side stand-in for the symbol; the address must be queried).
+// Looked up on the first call per device and kept; a failed lookup is retried
+// on the next call.
 int scratch_address(int device, unsigned char** out) {
   if (device < 0 || device >= kMaxDevices) return ERMOD_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
   if (!g_scratch_addr[device]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return ERMOD_ERR_CUDA;
@@ -46,6 +51,7 @@ extern "C" int32_t ermod_histogram_noalloc(int32_t device, int32_t slttype, cons
                                            const double* uvcrd, const int32_t* uvmax, const int32_t* uvsoft,
                                            int32_t numslv, const double* weight, double* edens) {
   using namespace erm;
+  const bool soln = slttype == ERMOD_SLT_SOLN;
   if (!uvengy || !uvspec || !uvcrd || !uvmax || !weight || !edens || ntarget <= 0 || nmol <= 0 || numslv <= 0)
     return ERMOD_ERR_ARG;
   if (cudaSetDevice(device) != cudaSuccess) return ERMOD_ERR_CUDA;
@@ -74,6 +80,8 @@ extern "C" int32_t ermod_histogram_noalloc(int32_t device, int32_t slttype, cons
   float* d_min = (float*)take(sizeof(float) * (numslv + 1));
   float* d_max = (float*)take(sizeof(float) * (numslv + 1));
   double* d_edens = (double*)take(sizeof(double) * ermax);
+  // solutes in solution: k_bin also forms each target's per-species energy sums (flceng)
+  double* d_fl = soln ? (double*)take(sizeof(double) * (size_t)ntarget * numslv) : nullptr;
   DevStatus* d_st = (DevStatus*)take(sizeof(DevStatus));
   if (off > kNoallocBytes) return ERMOD_ERR_OVERFLOW;  // beyond ERMOD_NOALLOC_SCRATCH_BYTES
   // inputs into the scratch; outputs and counters start from zero / the
@@ -95,6 +103,7 @@ extern "C" int32_t ermod_histogram_noalloc(int32_t device, int32_t slttype, cons
   ok &= cudaMemcpyAsync(d_min, mn.data(), sizeof(float) * (numslv + 1), cudaMemcpyHostToDevice, s) == cudaSuccess;
   ok &= cudaMemcpyAsync(d_max, mx.data(), sizeof(float) * (numslv + 1), cudaMemcpyHostToDevice, s) == cudaSuccess;
   ok &= cudaMemsetAsync(d_edens, 0, sizeof(double) * ermax, s) == cudaSuccess;
+  if (d_fl) ok &= cudaMemsetAsync(d_fl, 0, sizeof(double) * (size_t)ntarget * numslv, s) == cudaSuccess;
   ok &= cudaMemsetAsync(d_st, 0, sizeof(DevStatus), s) == cudaSuccess;
   if (!ok) return ERMOD_ERR_CUDA;
   DeviceState d;
@@ -106,7 +115,7 @@ extern "C" int32_t ermod_histogram_noalloc(int32_t device, int32_t slttype, cons
   d.tgt_mol = nullptr;
   d.counts = d_counts;
   d.etot = d_etot;
-  d.flceng = nullptr;
+  d.flceng = d_fl;
   d.minuv = d_min;
   d.maxuv = d_max;
   d.status = d_st;
@@ -116,7 +125,7 @@ extern "C" int32_t ermod_histogram_noalloc(int32_t device, int32_t slttype, cons
   ba.ermax = ermax;
   ba.ermax_pad = ermax_pad;
   ba.numslv = numslv;
-  ba.slttype = slttype == ERMOD_SLT_SOLN ? ERMOD_SLT_SOLN : ERMOD_SLT_REFS_RIGID;
+  ba.slttype = soln ? ERMOD_SLT_SOLN : ERMOD_SLT_REFS_RIGID;
   if (setup_bin_smem(ba) != 0) return ERMOD_ERR_OVERFLOW;
   launch_bin(d, ba, 0, ntarget, nmol, s);
   launch_edens(d, 0, ntarget, ermax, ermax_pad, 0, s);
