@@ -123,6 +123,13 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libermod_b200.so")
 
 # Every symbol include/*.h declares, with its ctypes signature.
+class ErmodSlvfeOpts(C.Structure):
+    """ermod_slvfe_opts (include/ermod_slvfe.h)."""
+    _fields_ = [("functional", C.c_int32), ("evd", C.c_int32), ("et", C.c_double)]
+
+
+SLVFE_FUNCTIONALS = {"py-hnc": 0, "hnc": 1, "thnc": 2, "none": 3}
+
 SIGNATURES = {
     "ermod_abi_version": (C.c_int32, []),
     "ermod_enginit_mesh": (C.c_int32, [C.POINTER(ErmodHist), C.c_int32, _f64p, _i32p, _i32p, _f64p, _i32p, _i32p]),
@@ -179,6 +186,9 @@ SIGNATURES = {
                                          _f64p, _f64p,
                                          _i32p,
                                          C.c_double, _f64p, C.c_double, _f64p, _f64p]),
+    "ermod_slvfe_delta_mu_ex": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _f64p, _f64p,
+                                            _f64p, _f64p, _i32p, C.c_double, _f64p, C.c_double,
+                                            C.POINTER(ErmodSlvfeOpts), _f64p, _f64p, _i32p]),
     "ermod_slvfe_last_error": (C.c_char_p, []),
 }
 

@@ -16,10 +16,17 @@
 //   k_chol_*       blocked right-looking Cholesky of A (32 x 32 FP64 tiles: diagonal
 //                  factor, panel solve, trailing update)
 //   k_slv_solve    forward and backward substitution for the reference-solvent omega
+//   k_slv_check    posv_wrap's acceptance of that solution (slvfe.F90:520-531): the
+//                  largest residual against the regularised matrix, the largest element
+//   eigen-decomposition fallback (getinscv :1124-1170), when the Cholesky factor fails
+//   or the check rejects the solution: the unregularised matrix (k_slv_unreg) goes to
+//   cuSOLVER's Dsyevd, as the reference's syevr_wrap sends it to cusolverDnSsyevd; its
+//   first nsp eigenpairs are skipped in the pseudo-inverse (k_slv_evd_coef, k_slv_evd_x)
 //   k_slv_chmpot   the eczr zero shift, the functional and its per-species sums (:744-803)
 //
 // Every reduction is a fixed-order tree, so a run is reproducible bit for bit.
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <cmath>
 #include <cstdint>
@@ -99,6 +106,8 @@ struct SlvArgs {
   double* harm;         // rho rho0 / (rho + rho0)
   double* reg;          // [nsp]
   int* status;
+  int functional;       // ERMOD_SLVFE_PYHNC / HNC / THNC / NONE
+  double et;            // thnc threshold (kcal/mol)
 };
 
 // ---- distnorm's scaling and the directly sampled omega -------------------------------
@@ -394,8 +403,75 @@ __global__ void __launch_bounds__(kNT) k_slv_solve(const double* __restrict__ A,
   }
 }
 
+// ---- posv_wrap's acceptance (slvfe.F90:520-531) against the regularised matrix Areg ----
+constexpr double kPosvResidual = 1.0e-6, kPosvAbs = 1.0e6;
+
+__global__ void __launch_bounds__(kNT) k_slv_check(int n, int N, const double* __restrict__ Areg,
+                                                   const double* __restrict__ rhs, const double* __restrict__ x,
+                                                   double* __restrict__ out) {
+  __shared__ double sh[32];
+  double res = 0.0, big = 0.0;
+  for (int r = threadIdx.x; r < n; r += kNT) {
+    double v = 0.0;
+    for (int c = 0; c < n; ++c) v += Areg[(size_t)c * N + r] * x[c];
+    res = fmax(res, fabs(v - rhs[r]));
+    big = fmax(big, fabs(x[r]));
+  }
+  res = block_max(res, sh);
+  big = block_max(big, sh);
+  if (threadIdx.x == 0) { out[0] = res; out[1] = big; }
+}
+
+// ---- the eigen-decomposition fallback (getinscv, slvfe.F90:1124-1170) ------------------
+// E = chi0 - rho0 rho0^T on the sampled bins, the identity elsewhere (n x n, column-major)
+__global__ void k_slv_unreg(SlvArgs a, const double* __restrict__ chi, double* __restrict__ E) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  if (e >= (size_t)n * n) return;
+  const int r = (int)(e % n), c = (int)(e / n);
+  const bool pr = a.rho0[r] > 0.0, pc = a.rho0[c] > 0.0;
+  E[e] = (pr && pc) ? chi[(size_t)c * n + r] - a.rho0[r] * a.rho0[c] : (r == c ? 1.0 : 0.0);
+}
+
+// coef[i] = (sum over sampled bins p of -kT (rho - rho0)_p V[p][i]) / lambda_i for i >= nsp
+__global__ void k_slv_evd_coef(SlvArgs a, const double* __restrict__ V, const double* __restrict__ lam,
+                               double* __restrict__ coef) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  if (i >= n) return;
+  double s = 0.0;
+  if (i >= a.nsp) {
+    for (int p = 0; p < n; ++p)
+      if (a.rho0[p] > 0.0) s += -a.kT * (a.rho[p] - a.rho0[p]) * V[(size_t)i * n + p];
+    s /= lam[i];
+  }
+  coef[i] = s;
+}
+
+// x[p] = sum over i >= nsp of V[p][i] coef[i]
+__global__ void k_slv_evd_x(SlvArgs a, const double* __restrict__ V, const double* __restrict__ coef,
+                            double* __restrict__ x) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n;
+  if (p >= n) return;
+  double s = 0.0;
+  for (int i = a.nsp; i < n; ++i) s += V[(size_t)i * n + p] * coef[i];
+  x[p] = s;
+}
+
 __device__ double pyhnc_soln(double f) { return f < 0.0 ? f + f / (exp(-f) - 1.0) + 1.0 : f / 2.0; }
 __device__ double pyhnc_refs(double f) { return f < 0.0 ? log1p(-f) * (1.0 / f - 1.0) + 1.0 : f / 2.0; }
+
+// chmpot's integrands (slvfe.F90:759-774): py-hnc, hnc / thnc (thnc, :1417-1436), none
+__device__ void functional_terms(int functional, double om, double om0, double kT, double et, double* ls,
+                                 double* lr) {
+  switch (functional) {
+    case ERMOD_SLVFE_HNC: *ls = om / kT / 2.0; *lr = om0 / kT / 2.0; return;
+    case ERMOD_SLVFE_THNC: *ls = om / kT / 2.0; *lr = om0 < et ? 0.0 : om0 / kT / 2.0; return;
+    case ERMOD_SLVFE_NONE: *ls = 0.0; *lr = 0.0; return;
+    default: *ls = pyhnc_soln(om / kT); *lr = pyhnc_refs(om0 / kT); return;
+  }
+}
 
 // ---- eczr zero shift, the functional and its per-species sums ------------------------
 __global__ void __launch_bounds__(kNT) k_slv_chmpot(SlvArgs a, const double* __restrict__ x,
@@ -430,7 +506,9 @@ __global__ void __launch_bounds__(kNT) k_slv_chmpot(SlvArgs a, const double* __r
       const double om0 = (r0 > 0.0 ? -kT * (r - r0) / r0 - x[i] : 0.0) + zx[p - 1];
       const double hs = r + r0;
       const double wt = r >= r0 ? 1.0 : 1.0 - ((r - r0) / (hs > 0.0 ? hs : 1.0)) * ((r - r0) / (hs > 0.0 ? hs : 1.0));
-      const double fac = wt * pyhnc_soln(a.omega[i] / kT) + (1.0 - wt) * pyhnc_refs(om0 / kT);
+      double ls, lr;
+      functional_terms(a.functional, a.omega[i], om0, kT, a.et, &ls, &lr);
+      const double fac = wt * ls + (1.0 - wt) * lr;
       const double lcent = -(a.omega[i] + a.crd[i]);
       s += -kT * (r - r0) + lcent * r + kT * fac * (r - r0);
     }
@@ -455,8 +533,20 @@ extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n0, int32_t nsp,
                                         const double* rho_sln, const double* rho_ref, const double* chi_ref,
                                         const double* crd, const int32_t* spec, double kT, const double* aveuv,
                                         double slfeng, double* chmpt, double* total) {
+  const ermod_slvfe_opts o{ERMOD_SLVFE_PYHNC, 1, 0.0};
+  return ermod_slvfe_delta_mu_ex(device, n0, nsp, group, inft, rho_sln, rho_ref, chi_ref, crd, spec, kT, aveuv,
+                                 slfeng, &o, chmpt, total, nullptr);
+}
+
+extern "C" int32_t ermod_slvfe_delta_mu_ex(int32_t device, int32_t n0, int32_t nsp, int32_t group, int32_t inft,
+                                           const double* rho_sln, const double* rho_ref, const double* chi_ref,
+                                           const double* crd, const int32_t* spec, double kT, const double* aveuv,
+                                           double slfeng, const ermod_slvfe_opts* opts, double* chmpt,
+                                           double* total, int32_t* used_evd) {
+  if (used_evd) *used_evd = 0;
   if (n0 < 2 || nsp < 1 || nsp > kMaxSpecies || group < 1 || inft < 0 || inft > 100 || !rho_sln || !rho_ref || !chi_ref || !crd || !spec ||
-      !aveuv || !chmpt || !(kT > 0.0))
+      !aveuv || !chmpt || !(kT > 0.0) || !opts || opts->functional < ERMOD_SLVFE_PYHNC ||
+      opts->functional > ERMOD_SLVFE_NONE)
     return fail(ERMOD_ERR_ARG, "slv_arg");
   for (int i = 0; i < n0; ++i)
     if (spec[i] < 1 || spec[i] > nsp || (i > 0 && spec[i] < spec[i - 1])) return fail(ERMOD_ERR_ARG, "slv_arg");
@@ -490,17 +580,22 @@ extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n0, int32_t nsp,
   double *d_rd0 = nullptr, *d_rr0 = nullptr, *d_crd0 = nullptr, *d_chi0 = nullptr;
   double *d_rd = nullptr, *d_rr = nullptr, *d_crd = nullptr, *d_chi = nullptr, *d_rho = nullptr, *d_rho0 = nullptr;
   double *d_nm = nullptr, *d_om = nullptr, *d_harm = nullptr, *d_reg = nullptr, *d_A = nullptr, *d_b = nullptr;
-  double *d_av = nullptr, *d_out = nullptr;
-  int *d_spec0 = nullptr, *d_spec = nullptr, *d_both = nullptr, *d_st = nullptr;
+  double *d_av = nullptr, *d_out = nullptr, *d_A2 = nullptr, *d_rhs = nullptr, *d_chk = nullptr;
+  double *d_E = nullptr, *d_lam = nullptr, *d_coef = nullptr, *d_work = nullptr;
+  int *d_spec0 = nullptr, *d_spec = nullptr, *d_both = nullptr, *d_st = nullptr, *d_info = nullptr;
   int4* d_rng = nullptr;
   cudaStream_t st = nullptr;
+  cusolverDnHandle_t sol = nullptr;
   int rc = ERMOD_OK;
   auto cleanup = [&]() {
     for (void* p : {(void*)d_rd0, (void*)d_rr0, (void*)d_crd0, (void*)d_chi0, (void*)d_rd, (void*)d_rr,
                     (void*)d_crd, (void*)d_chi, (void*)d_rho, (void*)d_rho0, (void*)d_nm, (void*)d_om,
                     (void*)d_harm, (void*)d_reg, (void*)d_A, (void*)d_b, (void*)d_av, (void*)d_out,
-                    (void*)d_spec0, (void*)d_spec, (void*)d_both, (void*)d_st, (void*)d_rng})
+                    (void*)d_spec0, (void*)d_spec, (void*)d_both, (void*)d_st, (void*)d_rng, (void*)d_A2,
+                    (void*)d_rhs, (void*)d_chk, (void*)d_E, (void*)d_lam, (void*)d_coef, (void*)d_work,
+                    (void*)d_info})
       if (p) cudaFree(p);
+    if (sol) cusolverDnDestroy(sol);
     if (st) cudaStreamDestroy(st);
   };
   bool ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
@@ -513,6 +608,7 @@ extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n0, int32_t nsp,
   ok = ok && dalloc(&d_reg, nsp) == cudaSuccess && dalloc(&d_A, NN) == cudaSuccess && dalloc(&d_b, N) == cudaSuccess;
   ok = ok && dalloc(&d_av, nsp) == cudaSuccess && dalloc(&d_out, nsp) == cudaSuccess;
   ok = ok && dalloc(&d_spec, n) == cudaSuccess && dalloc(&d_both, n) == cudaSuccess && dalloc(&d_st, 1) == cudaSuccess;
+  ok = ok && dalloc(&d_A2, NN) == cudaSuccess && dalloc(&d_rhs, N) == cudaSuccess && dalloc(&d_chk, 2) == cudaSuccess;
   if (!ok) { cleanup(); return fail(ERMOD_ERR_CUDA, "slv_mem"); }
   ok = cudaMemcpyAsync(d_rd0, rho_sln, 8 * n0, cudaMemcpyHostToDevice, st) == cudaSuccess;
   ok = ok && cudaMemcpyAsync(d_rr0, rho_ref, 8 * n0, cudaMemcpyHostToDevice, st) == cudaSuccess;
@@ -523,7 +619,7 @@ extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n0, int32_t nsp,
   ok = ok && cudaMemcpyAsync(d_av, aveuv, 8 * nsp, cudaMemcpyHostToDevice, st) == cudaSuccess;
   ok = ok && cudaMemsetAsync(d_st, 0, sizeof(int), st) == cudaSuccess;
   SlvArgs a{n, nsp, kT, n0, d_rd0, d_rr0, d_rd, d_rr, d_crd, d_spec, d_rho, d_rho0, d_nm, d_om, d_both, d_harm,
-            d_reg, d_st};
+            d_reg, d_st, opts->functional, opts->et};
   const size_t corr_smem = (size_t)n * sizeof(double);
   if (ok && corr_smem > 48 * 1024)
     ok = cudaFuncSetAttribute(k_slv_distnorm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)corr_smem) ==
@@ -537,6 +633,8 @@ extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n0, int32_t nsp,
     k_slv_extrap<<<(n + 127) / 128, 128, 0, st>>>(a);
     k_slv_reg<<<1, kNT, 0, st>>>(a, d_chi);
     k_slv_build<<<(unsigned)((NN + 255) / 256), 256, 0, st>>>(a, d_chi, N, d_A, d_b);
+    ok = cudaMemcpyAsync(d_A2, d_A, sizeof(double) * NN, cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(d_rhs, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, st) == cudaSuccess;
     const int nt = N / kTile;
     for (int kt = 0; kt < nt; ++kt) {
       k_chol_diag<<<1, kTile * kTile, 0, st>>>(d_A, N, kt, d_st);
@@ -547,13 +645,55 @@ extern "C" int32_t ermod_slvfe_delta_mu(int32_t device, int32_t n0, int32_t nsp,
       }
     }
     k_slv_solve<<<1, kNT, 0, st>>>(d_A, N, d_b);
+    k_slv_check<<<1, kNT, 0, st>>>(n, N, d_A2, d_rhs, d_b, d_chk);
+    ok = ok && cudaGetLastError() == cudaSuccess;
+  }
+  // posv_wrap's verdict decides between the Cholesky solution and the eigen-decomposition
+  int status = 0;
+  double chk[2] = {0.0, 0.0};
+  ok = ok && cudaMemcpyAsync(&status, d_st, sizeof(int), cudaMemcpyDeviceToHost, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(chk, d_chk, sizeof(chk), cudaMemcpyDeviceToHost, st) == cudaSuccess;
+  ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
+  const bool rejected = status == kErrChol || (status == kOk && !(chk[0] <= kPosvResidual && chk[1] <= kPosvAbs));
+  if (ok && rejected && opts->evd) {
+    int lwork = 0, info = 0;
+    ok = dalloc(&d_E, nn) == cudaSuccess && dalloc(&d_lam, n) == cudaSuccess && dalloc(&d_coef, n) == cudaSuccess &&
+         dalloc(&d_info, 1) == cudaSuccess;
+    ok = ok && cusolverDnCreate(&sol) == CUSOLVER_STATUS_SUCCESS && cusolverDnSetStream(sol, st) == CUSOLVER_STATUS_SUCCESS;
+    if (ok) {
+      k_slv_unreg<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(a, d_chi, d_E);
+      ok = cudaGetLastError() == cudaSuccess;
+    }
+    ok = ok && cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, d_E, n, d_lam,
+                                           &lwork) == CUSOLVER_STATUS_SUCCESS;
+    ok = ok && dalloc(&d_work, (size_t)lwork) == cudaSuccess;
+    ok = ok && cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, d_E, n, d_lam, d_work, lwork,
+                                d_info) == CUSOLVER_STATUS_SUCCESS;
+    ok = ok && cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
+    if (ok && info != 0) status = kErrChol;   // "Failed inversion of correlation matrix" (slvfe.F90:1134)
+    if (ok && info == 0) {
+      k_slv_evd_coef<<<(n + 127) / 128, 128, 0, st>>>(a, d_E, d_lam, d_coef);
+      k_slv_evd_x<<<(n + 127) / 128, 128, 0, st>>>(a, d_E, d_coef, d_b);
+      ok = cudaGetLastError() == cudaSuccess;
+      if (status == kErrChol) {
+        status = kOk;
+        ok = ok && cudaMemsetAsync(d_st, 0, sizeof(int), st) == cudaSuccess;
+      }
+      if (used_evd) *used_evd = 1;
+    }
+  } else if (ok && rejected && status == kOk) {
+    status = kErrChol;   // the solution posv_wrap rejects, with the fallback switched off
+  }
+  if (ok && status == kOk) {
     k_slv_chmpot<<<1, kNT, 0, st>>>(a, d_b, d_av, d_out);
     ok = cudaGetLastError() == cudaSuccess;
   }
-  int status = 0;
-  ok = ok && cudaMemcpyAsync(&status, d_st, sizeof(int), cudaMemcpyDeviceToHost, st) == cudaSuccess;
+  int status2 = 0;
+  ok = ok && cudaMemcpyAsync(&status2, d_st, sizeof(int), cudaMemcpyDeviceToHost, st) == cudaSuccess;
   ok = ok && cudaMemcpyAsync(chmpt, d_out, 8 * nsp, cudaMemcpyDeviceToHost, st) == cudaSuccess;
   ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
+  if (status == kOk) status = status2;
   if (!ok) rc = fail(ERMOD_ERR_CUDA, "slv_cud");
   else if (status == kErrNorm) rc = fail(ERMOD_ERR_SLVFE, "slv_nrm");
   else if (status == kErrExtrap) rc = fail(ERMOD_ERR_SLVFE, "slv_ext");

@@ -46,6 +46,32 @@ def _pyhnc_refs(f):
     return np.where(f < 0.0, py, f / 2.0)
 
 
+FUNCTIONALS = ("py-hnc", "hnc", "thnc", "none")
+
+
+def _functional_terms(functional: str, omega, omega0, kT: float, et: float):
+    """Per-bin integrands of the solution and reference-solvent sides (chmpot,
+    slvfe.F90:759-774): py-hnc (pyhnc :1439-1465), hnc and thnc (thnc :1417-1436: half the
+    indirect PMF over kT; thnc zeroes the reference side where its PMF lies below et),
+    none (zero)."""
+    f, f0 = omega / kT, omega0 / kT
+    if functional == "py-hnc":
+        return _pyhnc_soln(f), _pyhnc_refs(f0)
+    if functional == "hnc":
+        return f / 2.0, f0 / 2.0
+    if functional == "thnc":
+        return f / 2.0, np.where(omega0 < et, 0.0, f0 / 2.0)
+    if functional == "none":
+        return np.zeros_like(f), np.zeros_like(f0)
+    raise ValueError(f"functional {functional!r}: one of {FUNCTIONALS}")
+
+
+# posv_wrap's acceptance of the regularised Cholesky solve (slvfe.F90:478, 520-531): a larger
+# residual or solution element sends getinscv to the eigen-decomposition (:1124-1170)
+POSV_RESIDUAL = 1.0e-6
+POSV_ABS = 1.0e6
+
+
 def _normalise(edist, edens, ecorr, spec, nummol, tol=1.0e-8, itrmax=100):
     """distnorm: per-species scaling of rho and rho0, and the row scaling of chi0
     (a Gauss-Seidel sweep over the bins, as slvfe.F90:1503-1525 updates in place)."""
@@ -159,22 +185,26 @@ def merge_bins(edist, edens, ecorr, uvcrd, uvspec, group: int, inft: int = 0):
 
 
 def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0, group: int = 1,
-             inft: int = 0):
+             inft: int = 0, functional: str = "py-hnc", et: float = 0.0):
     """(per-species solvation free energies, total) in kcal/mol.
 
     group > 1 first merges that many consecutive bins per species: chmpot's grouping with
     inft 0 (slvfe.F90:609-698).  The reference reports group pickgr = 3 in its range and
-    merge modes (sfemain.F90:55, slvfe.F90:1647)."""
+    merge modes (sfemain.F90:55, slvfe.F90:1647).  functional: 'py-hnc' (the default),
+    'hnc', 'thnc' with threshold et (kcal/mol; sfemain.F90:177 selects thnc when et != 0)
+    or 'none' (slvfe.F90:759-774)."""
+    if functional not in FUNCTIONALS:
+        raise ValueError(f"functional {functional!r}: one of {FUNCTIONALS}")
     # the sampled-bin thresholds use the smallest values of the data as read (slvfe.F90:884-885)
     rd_min = float(np.min(np.asarray(edist)[np.asarray(edist) > 0.0]))
     rr_min = float(np.min(np.asarray(edens)[np.asarray(edens) > 0.0]))
     if group > 1 or inft:
         edist, edens, ecorr, uvcrd, uvspec = merge_bins(edist, edens, ecorr, uvcrd, uvspec, group, inft)
-    return _delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng, rd_min, rr_min)
+    return _delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng, rd_min, rr_min, functional, et)
 
 
 def _delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float, rd_min: float,
-              rr_min: float):
+              rr_min: float, functional: str = "py-hnc", et: float = 0.0):
     """delta_mu on the mesh as given.
 
     edist: rho (solution, engstore-normalised); edens, ecorr: rho0 and chi0
@@ -238,10 +268,15 @@ def _delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: 
         sp = pos & (spec == p)
         reg = np.trace(A[np.ix_(sp, sp)]) / sp.sum() ** 2
         Areg[np.ix_(sp, sp)] += reg
+    x = None
     try:
         L = np.linalg.cholesky(Areg)
         x = np.linalg.solve(L.T, np.linalg.solve(L, rhs))
+        if np.abs(Areg @ x - rhs).max() > POSV_RESIDUAL or np.abs(x).max() > POSV_ABS:
+            x = None
     except np.linalg.LinAlgError:
+        pass
+    if x is None:
         val, vec = np.linalg.eigh(A)
         coef = (vec[pos, nsp:].T @ ddiff[pos]) / val[nsp:]
         x = vec[:, nsp:] @ coef
@@ -253,7 +288,8 @@ def _delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: 
     live = (rho > 0.0) | (rho0 > 0.0)
     lcent = -(omega + crd)
     w = np.where(rho >= rho0, 1.0, 1.0 - ((rho - rho0) / np.where(hsum > 0.0, hsum, 1.0)) ** 2)
-    fac = w * _pyhnc_soln(omega / kT) + (1.0 - w) * _pyhnc_refs(omega0 / kT)
+    lsln, lref = _functional_terms(functional, omega, omega0, kT, et)
+    fac = w * lsln + (1.0 - w) * lref
     terms = -kT * (rho - rho0) + lcent * rho + kT * fac * (rho - rho0)
     chmpt = np.array([terms[live & (spec == p)].sum() for p in range(1, nsp + 1)]) + np.asarray(aveuv)
     return chmpt, float(chmpt.sum() + slfeng)
@@ -341,12 +377,16 @@ def read_table(path) -> np.ndarray:
 
 
 def delta_mu_gpu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfeng: float = 0.0,
-                 device: int = 0, group: int = 1, inft: int = 0):
-    """delta_mu on the GPU (include/ermod_slvfe.h): the same functional, options and
-    arguments, FP64 CUDA kernels.  Raises RuntimeError with slvfe's failure name; there is
-    no eigenvalue fallback on this path."""
+                 device: int = 0, group: int = 1, inft: int = 0, functional: str = "py-hnc", et: float = 0.0,
+                 evd: bool = True, info: dict | None = None):
+    """delta_mu on the GPU (include/ermod_slvfe.h, ermod_slvfe_delta_mu_ex): the same
+    functional, options and arguments, FP64 CUDA kernels, with getinscv's eigen-decomposition
+    fallback (evd=False reports slv_chl instead).  Raises RuntimeError with slvfe's failure
+    name; `info`, if given, receives {"used_evd": bool}."""
     import ctypes as C
     from . import _capi as A
+    if functional not in A.SLVFE_FUNCTIONALS:
+        raise ValueError(f"functional {functional!r}: one of {tuple(A.SLVFE_FUNCTIONALS)}")
     lib = A.load_library()
     rd = A.as_f64(edist)
     rr = A.as_f64(edens)
@@ -357,10 +397,14 @@ def delta_mu_gpu(edist, edens, ecorr, uvcrd, uvspec, temp_K: float, aveuv, slfen
     nsp = int(spec.max())
     out = np.zeros(nsp)
     tot = C.c_double()
-    rc = lib.ermod_slvfe_delta_mu(device, len(rd), nsp, group, inft, A.ptr(rd, C.c_double), A.ptr(rr, C.c_double),
-                                  chi.ctypes.data_as(C.POINTER(C.c_double)), A.ptr(crd, C.c_double),
-                                  A.ptr(spec, C.c_int32), kT_of(temp_K), A.ptr(av, C.c_double), float(slfeng),
-                                  A.ptr(out, C.c_double), C.byref(tot))
+    used = C.c_int32()
+    opts = A.ErmodSlvfeOpts(functional=A.SLVFE_FUNCTIONALS[functional], evd=1 if evd else 0, et=float(et))
+    rc = lib.ermod_slvfe_delta_mu_ex(device, len(rd), nsp, group, inft, A.ptr(rd, C.c_double), A.ptr(rr, C.c_double),
+                                     chi.ctypes.data_as(C.POINTER(C.c_double)), A.ptr(crd, C.c_double),
+                                     A.ptr(spec, C.c_int32), kT_of(temp_K), A.ptr(av, C.c_double), float(slfeng),
+                                     C.byref(opts), A.ptr(out, C.c_double), C.byref(tot), C.byref(used))
+    if info is not None:
+        info["used_evd"] = bool(used.value)
     if rc != 0:
         raise RuntimeError(f"{lib.ermod_slvfe_last_error().decode()} ({rc})")
     return out, tot.value

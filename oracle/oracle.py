@@ -24,13 +24,16 @@ _lib = None
 REF_DCD = os.path.join(HERE, "_ref", "libref_dcd.so")
 
 
-def build(force: bool = False) -> str:
+def build(force: bool = False, refsrc: str | None = None) -> str:
+    """Build liboracle.so; with `refsrc` (the reference's vmdplugins directory, or the
+    ERMOD_REFSRC environment variable) also the reference's own DCD reader into _ref/."""
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(
             os.path.join(HERE, "ermod_oracle.cpp")):
         subprocess.run(["make", "-C", HERE, "-s"], check=True)
     # the reference's own DCD reader behind the test shim: built only where its sources are
-    if force or not os.path.exists(REF_DCD):
-        subprocess.run(["make", "-C", HERE, "-s", "ref"], check=False, capture_output=True)
+    refsrc = refsrc or os.environ.get("ERMOD_REFSRC")
+    if refsrc and os.path.isdir(refsrc) and (force or not os.path.exists(REF_DCD)):
+        subprocess.run(["make", "-C", HERE, "-s", "ref", f"REFSRC={refsrc}"], check=False, capture_output=True)
     return LIB
 
 

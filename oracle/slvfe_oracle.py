@@ -41,6 +41,14 @@ def _pyhnc(indpmf: float, cnt: int, kT: float) -> float:
     return intg
 
 
+def _thnc(indpmf: float, et: float, cnt: int, kT: float) -> float:
+    """slvfe.F90:1417-1436."""
+    factor = indpmf / kT
+    if cnt == 2 and indpmf < et:
+        factor = 0.0
+    return factor / 2.0
+
+
 def _sfewgt(fsln: float, fref: float) -> float:
     """slvfe.F90:1402-1414."""
     if fsln >= fref:
@@ -191,7 +199,8 @@ def merge_bins(rddst, rddns, rdcor, rdcrd, rdspec, group, inft=0):
             np.array(uvspec[1:]))
 
 
-def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0, group=1, inft=0):
+def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0, group=1, inft=0, functional="py-hnc",
+             et=0.0):
     """Solvation free energy (kcal/mol) per solvent species and in total.
 
     edist  solution energy distribution per bin (engsln), edens / ecorr the
@@ -295,10 +304,17 @@ def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0, grou
             for p in range(gemax):
                 if uvspec[p] == pti and edvec[p] > 0.0:
                     inv[p, iduv] += regfac[pti - 1]
+    inscv = None
     try:
         L = np.linalg.cholesky(inv)
         inscv = np.linalg.solve(L.T, np.linalg.solve(L, work))
-    except np.linalg.LinAlgError:     # EVD fallback (slvfe.F90:1147-1170)
+        # posv_wrap (slvfe.F90:520-531): residual above 1e-6 or an element above 1e6 is a failure
+        residual = np.abs(inv @ inscv - work)
+        if residual.max() > 1.0e-6 or np.abs(inscv).max() > 1.0e6:
+            inscv = None
+    except np.linalg.LinAlgError:
+        pass
+    if inscv is None:                 # EVD fallback (slvfe.F90:1124-1170)
         egnval, vec = np.linalg.eigh(edmcr)
         inscv = np.zeros(gemax)
         for i in range(numslv, gemax):
@@ -308,7 +324,7 @@ def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0, grou
         inscv[iduv] = ddiff[iduv] / edvec[iduv] - inscv[iduv] if edvec[iduv] > 0.0 else 0.0
     for pti in range(1, numslv + 1):
         inscv[uvspec == pti] -= -zerouv[pti - 1]
-    # ---- chmpot (slvfe.F90:744-803), functional = 'py-hnc' ----
+    # ---- chmpot (slvfe.F90:744-803) ----
     chmpt = np.zeros(numslv)
     for pti in range(1, numslv + 1):
         slvfe = 0.0
@@ -320,8 +336,19 @@ def delta_mu(edist, edens, ecorr, uvcrd, uvspec, temp_K, aveuv, slfeng=0.0, grou
             slvfe -= kT * (edist_[iduv] - edens_[iduv])
             lcent = -(slncv[iduv] + zrsln[pti - 1] + uvcrd[iduv])
             slvfe += lcent * edist_[iduv]
-            lcsln = _pyhnc(slncv[iduv], 1, kT)
-            lcref = _pyhnc(inscv[iduv], 2, kT)
+            if functional == "py-hnc":
+                lcsln = _pyhnc(slncv[iduv], 1, kT)
+                lcref = _pyhnc(inscv[iduv], 2, kT)
+            elif functional == "hnc":
+                lcsln = _thnc(slncv[iduv], -np.inf, 1, kT)
+                lcref = _thnc(inscv[iduv], -np.inf, 2, kT)
+            elif functional == "thnc":
+                lcsln = _thnc(slncv[iduv], et, 1, kT)
+                lcref = _thnc(inscv[iduv], et, 2, kT)
+            elif functional == "none":
+                lcsln = lcref = 0.0
+            else:
+                raise ValueError(functional)
             ampl = _sfewgt(edist_[iduv], edens_[iduv])
             factor = ampl * lcsln + (1.0 - ampl) * lcref
             slvfe += kT * factor * (edist_[iduv] - edens_[iduv])

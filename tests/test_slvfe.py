@@ -75,6 +75,53 @@ def test_product_matches_restatement_on_engine_distributions(oracle_mod, slvfe_o
     assert a[1] == pytest.approx(b[1], rel=1e-6, abs=1e-6)
 
 
+@pytest.mark.parametrize("functional,et", [("hnc", 0.0), ("thnc", -0.5), ("thnc", 0.3), ("none", 0.0)])
+def test_functionals_match_restatement(slvfe_oracle, functional, et):
+    """chmpot's other functionals (slvfe.F90:759-774, thnc :1417-1436) against the loop-by-loop
+    restatement on two species."""
+    rho, rho0, chi0, crd, spec = _two_species()
+    a = SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], functional=functional, et=et)
+    b = slvfe_oracle.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], functional=functional, et=et)
+    np.testing.assert_allclose(a[0], b[0], rtol=1e-9, atol=1e-9)
+
+
+def test_thnc_threshold_limits():
+    """thnc with a threshold below every reference-side PMF is hnc; 'none' drops the integrand."""
+    rho, rho0, chi0, crd, spec = _two_species()
+    hnc = SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], functional="hnc")[1]
+    thnc = SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], functional="thnc", et=-1e30)[1]
+    assert thnc == pytest.approx(hnc, rel=1e-14)
+    with pytest.raises(ValueError):
+        SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], functional="pyhnc")
+
+
+def _ill_conditioned():
+    """One species whose chi0 - rho0 rho0^T has a near-null direction besides the constant one:
+    the regularised Cholesky solve then returns a huge solution element, which posv_wrap
+    (slvfe.F90:520-531) rejects, and getinscv falls back to the eigen-decomposition."""
+    crd, rho0, chi0 = synthetic(seed=9)
+    n = len(crd)
+    v = np.sin(np.arange(n) * 0.37)
+    v -= v.mean()
+    v /= np.linalg.norm(v)
+    A = chi0 - np.outer(rho0, rho0)
+    lam, vec = np.linalg.eigh(A)
+    A = A - (v @ A @ v - 1e-12) * np.outer(v, v)
+    chi = A + np.outer(rho0, rho0)
+    rho = rho0 * (1.0 + 0.05 * v * np.sqrt(n))
+    rho = np.clip(rho, 1e-3, None)
+    rho *= rho0.sum() / rho.sum()
+    return rho, rho0, chi, crd, np.ones(n, dtype=int)
+
+
+def test_posv_rejection_falls_back_to_evd(slvfe_oracle):
+    rho, rho0, chi, crd, spec = _ill_conditioned()
+    a = SF.delta_mu(rho, rho0, chi, crd, spec, 300.0, [-1.0])
+    b = slvfe_oracle.delta_mu(rho, rho0, chi, crd, spec, 300.0, [-1.0])
+    assert np.isfinite(a[1]) and abs(a[1]) < 1e3
+    np.testing.assert_allclose(a[0], b[0], rtol=1e-7, atol=1e-7)
+
+
 # ---------------------------------------------------------------------------
 # The GPU functional (include/ermod_slvfe.h) against the host module
 # ---------------------------------------------------------------------------
@@ -142,7 +189,8 @@ def test_gpu_functional_failures(engine_lib):
     with pytest.raises(RuntimeError, match="slv_zer"):        # no bin pair around zero
         SF.delta_mu_gpu(rho0, rho0, chi0, np.abs(crd) + 0.1, spec, 300.0, [0.0])
     with pytest.raises(RuntimeError, match="slv_chl"):        # chi0 - rho0 rho0^T negative definite
-        SF.delta_mu_gpu(rho0, rho0, np.outer(rho0, rho0) - 0.5 * np.diag(rho0), crd, spec, 300.0, [0.0])
+        SF.delta_mu_gpu(rho0, rho0, np.outer(rho0, rho0) - 0.5 * np.diag(rho0), crd, spec, 300.0, [0.0],
+                        evd=False)
     with pytest.raises(RuntimeError, match="slv_nrm"):        # no correlation at all
         SF.delta_mu_gpu(rho0, rho0, np.zeros_like(chi0), crd, spec, 300.0, [0.0])
 
@@ -196,3 +244,36 @@ def test_core_merging_matches_restatement(oracle_mod, slvfe_oracle, group, inft)
     assert len(a[0]) == (len(middle) - core * inft // 100) // group
     for x, y in zip(a, b):
         np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("functional,et", [("hnc", 0.0), ("thnc", 0.3), ("none", 0.0)])
+def test_gpu_functionals_match_host(engine_lib, functional, et):
+    rho, rho0, chi0, crd, spec = _two_species()
+    a = SF.delta_mu_gpu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], functional=functional, et=et)
+    b = SF.delta_mu(rho, rho0, chi0, crd, spec, 300.0, [-1.0, -0.4], functional=functional, et=et)
+    np.testing.assert_allclose(a[0], b[0], rtol=1e-9, atol=1e-9)
+
+
+@pytest.mark.gpu
+def test_gpu_evd_fallback_matches_host(engine_lib):
+    """posv_wrap rejects the regularised solution (an element above 1e6); the GPU then solves
+    by the eigen-decomposition of the unregularised matrix, as the host module does."""
+    rho, rho0, chi, crd, spec = _ill_conditioned()
+    info = {}
+    a = SF.delta_mu_gpu(rho, rho0, chi, crd, spec, 300.0, [-1.0], info=info)
+    assert info["used_evd"]
+    b = SF.delta_mu(rho, rho0, chi, crd, spec, 300.0, [-1.0])
+    np.testing.assert_allclose(a[0], b[0], rtol=1e-7, atol=1e-7)
+    with pytest.raises(RuntimeError, match="slv_chl"):
+        SF.delta_mu_gpu(rho, rho0, chi, crd, spec, 300.0, [-1.0], evd=False)
+    # a matrix the Cholesky factor rejects outright goes the same way
+    crd2, r0, _ = synthetic()
+    sp2 = np.ones(len(crd2), dtype=int)
+    chi_bad = np.outer(r0, r0) - 0.5 * np.diag(r0)
+    info = {}
+    r = r0 * np.exp(-0.3 * np.tanh(crd2 / 3.0))
+    g = SF.delta_mu_gpu(r, r0, chi_bad, crd2, sp2, 300.0, [0.0], info=info)
+    assert info["used_evd"]
+    h = SF.delta_mu(r, r0, chi_bad, crd2, sp2, 300.0, [0.0])
+    np.testing.assert_allclose(g[0], h[0], rtol=1e-7, atol=1e-7)
