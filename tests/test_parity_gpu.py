@@ -282,30 +282,41 @@ def test_histogram_is_exact_count(lib):
 
 
 def test_refs_accumulators_match_oracle(lib, oracle_mod):
-    """edens / ecorr / scalars over two frames agree with the oracle run on the same placements."""
+    """edens / ecorr / scalars over two frames: against the accumulators rebuilt from the GPU's
+    own bins and weights (every bin), and against the oracle run on the same placements on
+    every bin that no edge energy moved."""
+    from test_parity_full_gpu import rebuild_accumulators
     w = S.make_workload(2, small=True, maxins=64)
-    prm = dict(w.params, keep_uvengy=1)
+    prm = dict(w.params, keep_uvengy=1, estype=A.ES_NVT)
     eng = Engine(prm, w.topo, w.hist)
     orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist)
-    flips = 0
+    spec = phys_uvspec(w.topo)
+    frames, moved = [], np.zeros(eng.ermax, dtype=bool)
     for fr in range(2):
         pos, cell = w.frame(fr)
         assert eng.engconst(fr + 1, pos, cell) >= 0
         ins, _ = eng.insertions()
         assert orc.engconst(fr + 1, pos, cell, ins_conf=ins) >= 0
-        u, _ = eng.uvengy()
+        u, u0 = eng.uvengy()
         uo, _ = orc.uvengy()
-        spec = phys_uvspec(w.topo)
-        flips += int((bins_of(u, eng.uvcrd, eng.uvmax, spec) != bins_of(uo, eng.uvcrd, eng.uvmax, spec)).sum())
+        frames.append((u, u0))
+        bg, bo = bins_of(u, eng.uvcrd, eng.uvmax, spec), bins_of(uo, eng.uvcrd, eng.uvmax, spec)
+        moved[bg[bg != bo]] = True
+        moved[bo[bg != bo]] = True
     a, b = eng.accum(), orc.accum()
     assert a["engnorm"] == pytest.approx(b["engnorm"], rel=WREL)
     assert a["avslf"] == pytest.approx(b["avslf"], rel=1e-12)
     assert a["engsmpl"] == b["engsmpl"]
     assert a["voffset"] == pytest.approx(b["voffset"], abs=2e-5)
     n = w.topo.nummol - 1
-    if flips == 0:
-        np.testing.assert_allclose(a["edens"], b["edens"], rtol=WREL, atol=1e-9 * b["engnorm"])
-        np.testing.assert_allclose(a["ecorr"], b["ecorr"], rtol=WREL, atol=1e-9 * b["engnorm"] * n)
+    ed, ec, en = rebuild_accumulators(frames, eng.uvcrd, eng.uvmax, spec, prm["temp"], a["voffset"])
+    assert a["engnorm"] == pytest.approx(en, rel=1e-12)
+    np.testing.assert_allclose(a["edens"], ed, rtol=1e-12, atol=1e-15 * en)
+    np.testing.assert_allclose(a["ecorr"], ec, rtol=1e-7, atol=1e-12 * en)
+    keep = ~moved
+    np.testing.assert_allclose(a["edens"][keep], b["edens"][keep], rtol=WREL, atol=1e-9 * b["engnorm"])
+    np.testing.assert_allclose(a["ecorr"][np.ix_(keep, keep)], b["ecorr"][np.ix_(keep, keep)], rtol=WREL,
+                               atol=1e-9 * b["engnorm"] * n)
     # sum_j ecorr(j, i) = N_mol * edens(i)
     np.testing.assert_allclose(a["ecorr"].sum(axis=0), n * a["edens"], rtol=1e-6, atol=1e-6 * a["engnorm"])
     np.testing.assert_allclose(a["minuv"], b["minuv"], rtol=1e-4, atol=2e-5)
