@@ -47,10 +47,17 @@ def parse():
     ap.add_argument("--maxins", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=500, help="insertions per CPU reference step")
-    ap.add_argument("--config", type=int, default=2, choices=[2, 4, 5],
-                    help="2: the headline refs frame; 4: 64 solutes batched into one graph per frame; "
+    ap.add_argument("--config", type=int, default=2, choices=[2, 3, 4, 5],
+                    help="2: the headline refs frame; 3: the precision workload (32,768 waters, PME 128^3, "
+                         "60-site chain, 4,096 insertions); 4: 64 solutes batched into one graph per frame; "
                          "5: GPU time to delta-mu within 0.05 kcal/mol, learned vs uniform insertion")
-    ap.add_argument("--solute-sites", type=int, default=1, help="config 5: sites of the ring-recipe solute")
+    ap.add_argument("--solute-sites", type=int, default=200, help="config 5: sites of the ring-recipe solute")
+    ap.add_argument("--ins-per-frame", type=int, default=100000, help="config 5: insertions per frame")
+    ap.add_argument("--long-frames", type=int, default=100,
+                    help="config 5: frames of the uniform yardstick run (x insertions per frame)")
+    ap.add_argument("--max-frames", type=int, default=50, help="config 5: frames of each compared run")
+    ap.add_argument("--train-frames", type=int, default=10, help="config 5: uniform frames of training samples")
+    ap.add_argument("--replicas", type=int, default=2, help="config 5: independent runs per insertion mode")
     ap.add_argument("--mix-uniform", type=float, default=0.2, help="config 5: uniform share eps of the proposal")
     ap.add_argument("--label-quantile", type=float, default=0.05,
                     help="config 5: training label 1 for this lowest fraction of insertion energies")
@@ -58,44 +65,77 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clocks and clock-event (throttle) reasons sampled every 10 ms through NVML while running
+    (read-only queries), falling back to nvidia-smi at 200 ms where NVML is not importable."""
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
+        self.rows = []
         self.proc = None
+        self.thread = None
+
+    def _nvml_loop(self, nv, h):
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), [n for n, b in zip(self.NAMES, bits) if r & b]))
+            except Exception:
+                break
+            time.sleep(0.01)
 
     def __enter__(self):
+        self.stop = False
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.device]) if vis and vis.split(",")[0].isdigit() else self.device
+            h = nv.nvmlDeviceGetHandleByIndex(idx)
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+        except Exception:
+            self.thread = None
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                              "--format=csv,noheader,nounits", "-lms", "200"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            except OSError:
+                self.proc = None
         return self
 
     def __exit__(self, *exc):
-        self.out = ""
+        self.stop = True
+        if self.thread is not None:
+            self.thread.join(timeout=2)
         if self.proc is not None:
             self.proc.terminate()
             try:
-                self.out, _ = self.proc.communicate(timeout=5)
+                out, _ = self.proc.communicate(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                self.out, _ = self.proc.communicate()
+                out, _ = self.proc.communicate()
+            for r in (r.split(", ") for r in out.strip().splitlines() if r.count(",") >= 8):
+                if r[1].strip().isdigit():
+                    self.rows.append((float(r[1]), float(r[2]) if r[2].strip().isdigit() else None,
+                                      [self.NAMES[i] for i in range(4) if r[5 + i].strip().lower() == "active"]))
 
     def summary(self):
-        rows = [r.split(", ") for r in self.out.strip().splitlines() if r.count(",") >= 8]
-        if not rows:
+        if not self.rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].strip().isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows if r[1]]
+        reasons = sorted({n for r in self.rows for n in r[2]})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows), "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 
 def dist_init():
@@ -149,16 +189,36 @@ def path_bytes_per_unit(w, natoms: int, slvmax: int, ermax: int, maxdst: int, ns
     return B / (maxdst * slvmax)
 
 
-def traffic_from_profiles(kernel: str):
-    """dram bytes per launch of `kernel` from profiles/ncu_traffic.txt (written from an ncu capture)."""
-    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+def profile_table(name: str):
+    """{kernel: {column: value}} from a whitespace table under profiles/ ('#' lines are comments,
+    the first other line names the columns); {} when the file is absent."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
-        return None
+        return {}
+    rows, cols = {}, None
     for line in open(p):
+        if line.startswith("#") or not line.strip():
+            continue
         f = line.split()
-        if len(f) >= 2 and not line.startswith("#") and f[0] == kernel:
-            return float(f[1])
-    return None
+        if cols is None:
+            cols = f
+            continue
+        rows[f[0]] = {c: float(v) for c, v in zip(cols[1:], f[1:])}
+    return rows
+
+
+def bound_from_counters(c: dict) -> str:
+    """The resource that bounds a kernel, read from its ncu counters (fractions of peak):
+    the tensor pipe, DRAM, SM issue, or (none of them near its limit) memory latency."""
+    if not c:
+        return "unmeasured"
+    if c.get("tensor_pipe", 0.0) >= 0.5:
+        return "tensor"
+    if c.get("dram_frac", 0.0) >= 0.6:
+        return "hbm"
+    if c.get("issue_active", 0.0) >= 0.6 or max(c.get("fma_pipe", 0.0), c.get("lsu_pipe", 0.0)) >= 0.6:
+        return "sm-issue"
+    return "latency"
 
 
 def cpu_baseline(w, sample: int, threads: int):
@@ -247,7 +307,7 @@ def main():
         return main_batch(args)
     if args.config == 5:
         return main_delta_mu(args)
-    w = S.make_workload(CONFIG, maxins=args.maxins)
+    w = S.make_workload(args.config, maxins=args.maxins)
     if args.impl == "reference":
         run_reference(args, w)
         return
@@ -317,34 +377,36 @@ def main():
     value = ws * units * args.steps / (dev_ms * 1e-3)
     e2e = ws * units * args.steps / e2e_s
     paths = eng.paths()
-    # roofline of the dominant engine kernel, from a stage-timed pass of the same frames
+    # per-kernel stage times from a stage-timed pass of the same frames (direct launches)
     stage, nst = stage_pass(args, w, local, dev_pos, cell, flush)
-    ours = ["real", "spread", "influence", "pme_plane", "pme_rows", "site_tables", "transpose", "gather", "bin",
-            "ecorr"]
-    dom = max(ours, key=lambda k: stage[k])
-    nbatch = -(-eng.maxdst // 4096)
-    per_batch = ("real", "bin", "ecorr", "site_tables")
-    # stage["chunks"] sums the per-frame chunk counts over the stage-timed frames
-    n_launch = nbatch * nst if dom in per_batch else stage["chunks"]
-    per_launch_ms = stage[dom] / n_launch
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
         peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     chunk = 32
-    # achieved: the scope table's per-unit bytes x the units one launch of the dominant kernel
-    # serves (a frame's units over its launches); the kernel's own input/output bytes beside it
-    b_unit = path_bytes_per_unit(w, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
-    units_launch = units * nst / n_launch
-    bytes_launch = b_unit * units_launch
-    achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
-    kbytes_launch = kernel_bytes(dom, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
-    kachieved = kbytes_launch / (per_launch_ms * 1e-3) / 1e9
+    nbatch = -(-eng.maxdst // 4096)
+    per_batch = ("real", "bin", "ecorr", "site_tables")
     kname = {"gather": "k_gather", "bin": "k_bin", "real": "k_real", "spread": "k_spread_box",
              "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane",
              "pme_rows": "k_pme_lines" if w.params["ms1max"] <= 64 else "k_pme_rows",
-             "site_tables": "k_site_tables", "influence": "k_influence", "ecorr": "k_ecorr_tc"}[dom]
-    traffic = traffic_from_profiles(kname)
+             "site_tables": "k_site_tables", "influence": "k_influence", "ecorr": "k_ecorr_tc"}
+    counters = profile_table("kernel_counters.txt")
+    kernels = {}
+    for k, kn in kname.items():
+        if stage[k] <= 0:
+            continue
+        n_launch = nbatch * nst if k in per_batch else stage["chunks"]
+        ms = stage[k] / n_launch
+        io = kernel_bytes(k, w, chunk, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
+        c = counters.get(kn, {})
+        kernels[kn] = {"ms_per_frame": round(stage[k] / nst, 4), "launches_per_frame": n_launch / nst,
+                       "launch_ms": ms, "io_bytes_per_launch": io, "io_gbs": io / (ms * 1e-3) / 1e9,
+                       "io_frac": io / (ms * 1e-3) / 1e9 / peak, "bound": bound_from_counters(c),
+                       "ncu": c or None}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_per_frame"])
+    # the whole path against the scope table's algorithmic bytes per mol-pair
+    b_unit = path_bytes_per_unit(w, eng.natoms, eng.slvmax, eng.ermax, eng.maxdst, eng.nsite_slt)
+    traffic = profile_table("frame_traffic.txt").get(w.name, {}).get("dram_bytes_per_unit")
     stage_share = {k: round(stage[k] / max(stage["total"], 1e-9), 4) for k in Engine.STAGES
                    if k not in ("total", "chunks") and stage[k] > 0}
     if rank != 0:
@@ -364,22 +426,30 @@ def main():
                        "parallelism": f"frames sharded over {ws} rank(s), no collective in the step"},
             "stage_ms_per_frame": {k: round(stage[k] / nst, 4) for k in stage_share},
             "stage_share": stage_share,
-            "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": bytes_launch, "bytes_per_unit": b_unit,
-                         "units_per_launch": units_launch, "launch_ms": per_launch_ms,
-                         "kernel_io_bytes_per_launch": kbytes_launch, "kernel_io_frac": kachieved / peak,
-                         "path_frac": value * b_unit / 1e9 / peak},
+            # headline: the whole frame against the HBM roofline of the scope table's algorithmic bytes
+            # (a spectrum and a potential grid written and read per insertion, the FP64 energy matrix,
+            # ecorr once per batch); the fused solve keeps most of those bytes in L2, so the kernels
+            # themselves are bound by SM issue or latency: see roofline.kernels[*].bound
+            "roofline": {"kernel": "engconst frame (all kernels)", "bound": "hbm",
+                         "achieved": value * b_unit / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": value * b_unit / 1e9 / peak, "peak_source": peak_src,
+                         "traffic": None if traffic is None else traffic * units,
+                         "algorithmic_bytes_per_frame": b_unit * units, "bytes_per_unit": b_unit,
+                         "dominant_kernel": dom, "kernels": kernels},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(4 * 3 * eng.natoms + 4 * eng.maxdst),
                     "d2h_bytes_per_step": d2h_bytes_per_step(eng)},
             "gpu_launches": int(launches)}
+    parity = profile_table("parity_error_table.txt").get(w.name)
+    if parity:
+        line["parity_vs_fp64"] = parity
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s
     if ws == 1 and not args.no_cpu_baseline:
-        v, dt, u = cpu_baseline(w, 2000, os.cpu_count() or 1)
+        sample = 2000 if args.config == 2 else 128      # 10-30 s of host work at most
+        v, dt, u = cpu_baseline(w, sample, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-                                "sample": f"one frame of 2000 insertions x {u // 2000} waters ({dt:.1f} s), "
+                                "sample": f"one frame of {sample} insertions x {u // sample} waters ({dt:.1f} s), "
                                           "FP32 restatement of the reference algorithm on all host threads"}
     print(json.dumps(line))
     if ws > 1:
@@ -429,32 +499,36 @@ def main_batch(args):
 
 
 def main_delta_mu(args):
-    """Configuration 5 (scaled): GPU time until the energy-representation solvation free energy is within
+    """Configuration 5: GPU time until the energy-representation solvation free energy is within
     0.05 kcal/mol of a long uniform-insertion run, for uniform and for learned insertion.
 
-    A ring-recipe solute (--solute-sites, default a single LJ site) in 4096 waters (49.6 A box, disordered
-    packing: the lattice has no cavities for the proposal to find), PME 64^3.  rho and aveuv come from
-    soln-mode frames with the solute at the box centre; rho0 / chi0 from refs insertions, 2048 per frame;
-    delta-mu from the py-hnc functional (ermod_openacc_b200.slvfe).  The yardstick is a uniform run of
-    `long_frames` frames; each mode runs `reps` independent replicas and its error after n frames is the
-    RMS over replicas of the difference to the yardstick.  Times are CUDA-event device times of the frames; the
-    learned mode also reports the device time of its training (sample frames + training kernels)."""
+    Defaults follow the configuration: a 200-site ring-recipe solute in 4096 waters (49.6 A box,
+    PME 64^3), 100,000 insertions per frame, a network (64-128-128-128-1, BF16 weights, FP32
+    accumulation, over the 4x4x4 solvent-density features) trained on 1e6 uniform-insertion energies,
+    and a 1e7-insertion uniform run (100 frames) as the yardstick.  The water is a disordered packing
+    (the lattice has no cavities for a proposal to find); in the solution frames the waters keep 3 A
+    from every solute site.  rho and aveuv come from soln frames with the solute at the box centre,
+    rho0 / chi0 from refs insertions; delta-mu from the py-hnc functional on the GPU with slvfe's bin
+    middles and pickgr = 3 grouping.  Each mode runs `replicas` independent insertion streams over the
+    same solvent frames; its error after n frames is the RMS over replicas of the difference to the
+    yardstick.  Times are CUDA-event device times of the frames (the learned mode's training is
+    reported beside them)."""
     import torch
     import __graft_entry__ as ge
     ge.build_engine()
     from ermod_openacc_b200 import Engine, _capi as A, proposal as P, slvfe, systems as S
     torch.cuda.set_device(0)
-    nins, gv, eps, npool = 2048, 32, args.mix_uniform, 8
+    nins, gv, eps, npool = args.ins_per_frame, 32, args.mix_uniform, 16
     base = S.make_workload(2, seed=11)
     slt = S.lj_site() if args.solute_sites == 1 else S.ring_recipe_solute(args.solute_sites, 5)
     box, nside = base.box, base.nside
-    # solution: the solute fixed at the centre, waters kept 3 A away
+    # solution: the solute fixed at the centre, waters kept 3 A from every solute site
     sln_topo = S.Topology([slt, S.water()], [1, nside ** 3], [A.PT_SOLUTE, A.PT_SOLVENT])
     sln_prm = S.default_params(slttype=A.SLT_SOLN, ms1max=64, maxins=1, corrcal=0, wgtslf=0)
     sln_w = S.Workload("soln", sln_prm, sln_topo, {}, box, nside, npool, 11,
-                       solute_center=np.array([box / 2] * 3), packing="random")
+                       solute_center=np.array([box / 2] * 3), packing="random", avoid_sites=True, avoid_r=3.0)
     eng = Engine(sln_prm, sln_topo, {})
-    for i in range(npool):
+    for i in range(8):
         eng.engconst(i + 1, *sln_w.frame(i))
     sln, _ = eng.engstore()
     rho, aveuv = sln["edens"], [float(sln["slnuv"][0])]
@@ -485,15 +559,14 @@ def main_delta_mu(args):
         e.close()
         return res, ms
 
-    long_frames = 400
-    long_dmu, long_ms = run(A.PROPOSAL_UNIFORM, 999, long_frames)
-    # training: uniform samples of 12 frames, 20 epochs of the device kernels
+    long_dmu, long_ms = run(A.PROPOSAL_UNIFORM, 999, args.long_frames)
+    # training samples: uniform insertions (train_frames x nins energies), then the device trainer
     e = Engine(dict(ref_prm, corrcal=0), ref_topo, {})
     e.proposal_config(gv, eps, feature_cells=gv)
     sample_ms = 0.0
     fs, es = [], []
-    for i in range(12):
-        e.engconst(i + 1, *frames[i % npool])
+    for i in range(args.train_frames):
+        e.engconst(i + 1, *frames[(npool - 1 - i) % npool])
         sample_ms += e.last_ms()
         f, en, _ = e.insertion_samples()
         fs.append(f)
@@ -501,22 +574,21 @@ def main_delta_mu(args):
     e.close()
     feats, etot = np.concatenate(fs), np.concatenate(es)
     y, _ = P.labels_from_energies(etot, quantile=args.label_quantile)
-    tr = P.Trainer(P.init_params(7), max_batch=2048)
+    tr = P.Trainer(P.init_params(7), max_batch=4096)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    tr.fit(feats, y, epochs=20, batch=512, lr=1e-3)
+    tr.fit(feats, y, epochs=4, batch=4096, lr=1e-3)
     ev1.record()
     torch.cuda.synchronize()
     train_ms = ev0.elapsed_time(ev1)
     params = tr.params()
     tr.close()
-    cps = (1, 2, 4, 8, 16, 32, 64)
-    reps = 4
+    cps = tuple(c for c in (1, 2, 4, 8, 16, 32, 50, 64) if c <= args.max_frames)
     curves = {}
     for mode in (A.PROPOSAL_UNIFORM, A.PROPOSAL_LEARNED):
         errs = {c: [] for c in cps}
         mspf = []
-        for r in range(reps):
+        for r in range(args.replicas):
             out, ms = run(mode, 100 + r, max(cps), params if mode == A.PROPOSAL_LEARNED else None, cps)
             for c in cps:
                 errs[c].append(out[c][0] - long_dmu)
@@ -531,12 +603,13 @@ def main_delta_mu(args):
     name = "ljsite" if args.solute_sites == 1 else f"ring{args.solute_sites}"
     line = {"metric": "s to delta-mu +/-0.05 kcal/mol", "value": tl, "unit": "s", "n_gpus": 1,
             "higher_is_better": False, "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"delta-mu-{name}-water4096-disordered", "insertions_per_frame": nins,
+            "config": {"workload": f"learned-{name}-water4096-disordered", "insertions_per_frame": nins,
+                       "solute_sites": args.solute_sites, "frames_compared": max(cps),
                        "voxels_per_side": gv, "mix_uniform": eps, "label_quantile": args.label_quantile,
-                       "replicas": reps,
+                       "training_samples": int(len(etot)), "replicas": args.replicas,
                        "slvfe": {"bin_coordinates": "engsln bin_middle", "group": 3, "path": "GPU FP64"},
-                       "long_uniform_run": {"frames": long_frames, "insertions": long_frames * nins,
-                                 "delta_mu_kcal": long_dmu, "gpu_s": long_ms / 1e3}},
+                       "long_uniform_run": {"frames": args.long_frames, "insertions": args.long_frames * nins,
+                                            "delta_mu_kcal": long_dmu, "gpu_s": long_ms / 1e3}},
             "uniform": curves["uniform"], "learned": curves["learned"],
             "training_gpu_s": (sample_ms + train_ms) / 1e3,
             "speedup_uniform_over_learned": None if (tu is None or tl is None) else tu / tl}

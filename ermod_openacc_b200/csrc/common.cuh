@@ -34,12 +34,16 @@ struct PairParams {
 };
 
 // Minimum image of a difference of normalised coordinates (realcal.F90:115-128).
+// The cuboid case picks the image the reference's half - |half - |dx|| picks (realcal.F90:
+// 243-250), as dx - L rint(dx / L): a displacement shorter than half the box is left exact,
+// where the folded form rounds it to the ulp of half the box (~1e-6 A in a 50 A box, which
+// is 1e-5 of an r^-12 repulsion at contact).
 __device__ __forceinline__ void min_image(const CellGeom& g, float& x, float& y, float& z) {
   if (!g.periodic) return;
   if (g.cuboid) {
-    x = g.half[0] - fabsf(g.half[0] - fabsf(x));
-    y = g.half[1] - fabsf(g.half[1] - fabsf(y));
-    z = g.half[2] - fabsf(g.half[2] - fabsf(z));
+    x = fmaf(-g.len[0], rintf(x * g.inv[0]), x);
+    y = fmaf(-g.len[1], rintf(y * g.inv[1]), y);
+    z = fmaf(-g.len[2], rintf(z * g.inv[2]), z);
   } else {
     float f = roundf(z * g.inv[2]);
     x -= g.cn[0][2] * f; y -= g.cn[1][2] * f; z -= g.cn[2][2] * f;

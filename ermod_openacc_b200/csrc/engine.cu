@@ -51,6 +51,8 @@ size_t ecorr_tc_workspace(int n, int ermax);
 struct ermod_ctx {
   int device = 0;
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;            // real space, beside the PME chain of st
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev[9] = {};
   ermod_params p{};
   // host topology
@@ -64,6 +66,7 @@ struct ermod_ctx {
   std::vector<int> uvmax, uvsoft;
   DeviceState d;
   int chunk = kChunk, batch = 0, ncell_cap = 0;
+  float cell_h = 0.f;                    // cell-list edge picked by the tuner (0: not yet tuned, 4 A)
   int nhost = 0;                      // atoms of the host aggregate (insposition 2..4)
   int nref = 0;                       // atoms of the RefInfo host (insposition 5, 6)
   bool gauss_init = false;            // Gaussian insertion constants fixed at the first frame
@@ -152,6 +155,9 @@ void free_all(ermod_ctx* c) {
   if (c->h_frame) cudaFreeHost(c->h_frame);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
 }
 
@@ -393,6 +399,7 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   for (int a : atom_lj) if (a < 0 || a >= ctx->ljtype_max) return bad(ERMOD_ERR_ARG, "set_ljt");
   for (int a : slt_lj) if (a < 0 || a >= ctx->ljtype_max) return bad(ERMOD_ERR_ARG, "set_ljt");
   // engine shape
+  if (p.ins_chunk != 0 && p.ins_chunk != kChunk) return bad(ERMOD_ERR_ARG, "ins_chk");
   ctx->chunk = kChunk;
   const int K1 = p.ms1max, K2 = p.ms2max, K3 = p.ms3max, Kh1 = K1 / 2 + 1;
   const bool pme = mesh;   // smooth PME and PPPM share the whole pipeline but the influence function
@@ -404,6 +411,9 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
 
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
   DeviceState& d = ctx->d;
   const size_t NA = ctx->natoms, SM = ctx->slvmax, MD = ctx->maxdst, S = ctx->s;
@@ -669,6 +679,20 @@ struct FramePlanHost {
   double inv[3][3], vold;
 };
 
+// Cell grid of the real-space cell list for cells of edge >= hmin on the normalised cuboid
+// box (at most 64 a side, at least 3); false when no such grid fits.
+constexpr float kCellDefault = 4.0f;
+static bool cell_grid(const ermod_ctx* ctx, FrameArgs& a, float hmin, int& ncell) {
+  bool ok = true;
+  for (int dd = 0; dd < 3; ++dd) {
+    a.nc[dd] = std::max(1, std::min(64, (int)std::floor(a.g.len[dd] / hmin)));
+    a.ch[dd] = a.g.len[dd] / (float)a.nc[dd];
+    if (a.nc[dd] < 3) ok = false;
+  }
+  ncell = a.nc[0] * a.nc[1] * a.nc[2];
+  return ok && ncell <= ctx->ncell_cap;
+}
+
 static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_conf, FramePlanHost& ph) {
   const ermod_params& p = ctx->p;
   std::memset(&ph, 0, sizeof(ph));
@@ -802,14 +826,13 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
   P.bare = p.cltype == ERMOD_EL_COULOMB;
   a.slvmax = ctx->slvmax; a.natoms = ctx->natoms; a.nsite = ctx->s; a.maxdst = ctx->maxdst;
   a.K1 = K1; a.K2 = K2; a.K3 = K3; a.order = pme ? p.splodr : 1; a.Kh1 = K1 / 2 + 1;
-  // Fused solve: planes k1 whose every mode has exp(-pi^2 |k|^2 / screen^2) < kPlaneCut are not
+  // Fused solve: planes k1 whose every mode has exp(-pi^2 |k|^2 / screen^2) < kModeCut are not
   // transformed (|k| >= k1 / |a1| in plane k1, a1 the first cell vector).  Their share of any
   // molecule energy is below 1e-9 of the k = 0 Gaussian weight per mode, far under FP32 rounding.
   a.k1max = K1 / 2;
   if (pme) {
     const double a1 = std::sqrt(c[0][0] * c[0][0] + c[1][0] * c[1][0] + c[2][0] * c[2][0]);
-    const double kPlaneCut = 1e-9;
-    const double mcut = std::sqrt(-std::log(kPlaneCut)) * (double)p.screen * a1 / kPi;
+    const double mcut = std::sqrt(-std::log(kModeCut)) * (double)p.screen * a1 / kPi;
     a.k1max = std::max(0, std::min(K1 / 2, (int)std::floor(mcut) + 1));
   }
   a.ljtype_max = ctx->ljtype_max;
@@ -821,15 +844,7 @@ static int frame_plan(ermod_ctx* ctx, const float* cellin, float wsys, bool use_
   a.use_cells = 0;
   fp.ncell = 1;
   if (g.periodic && g.cuboid && !g.rotated) {
-    const float hmin = 4.0f;
-    bool ok = true;
-    for (int dd = 0; dd < 3; ++dd) {
-      a.nc[dd] = std::max(1, std::min(64, (int)std::floor(g.len[dd] / hmin)));
-      a.ch[dd] = g.len[dd] / (float)a.nc[dd];
-      if (a.nc[dd] < 3) ok = false;
-    }
-    fp.ncell = a.nc[0] * a.nc[1] * a.nc[2];
-    a.use_cells = ok && fp.ncell <= ctx->ncell_cap;
+    a.use_cells = cell_grid(ctx, a, ctx->cell_h > 0.f ? ctx->cell_h : kCellDefault, fp.ncell) ? 1 : 0;
   }
   // ---- influence function when the cell changes (engconst :423-433) ----
   if (pme) {
@@ -907,22 +922,45 @@ static void frame_commit(ermod_ctx* ctx, const float* cellin, const FramePlanHos
 // energies (a warp per molecule whatever the block size), so the choice only
 // moves time.  Tuned on the first frame with the frame's own data.
 static const int kRealCandidates[] = {128, 256, 512};
+static const float kCellCandidates[] = {3.0f, 4.0f, 5.0f, 6.0f};
 
-static int tune_real(ermod_ctx* ctx, const FrameArgs& a, int nbatch, cudaStream_t st) {
+// The real-space autotuner, run on the first frame with that frame's own data: every cell
+// edge of kCellCandidates (on cuboid periodic boxes) times every block size of
+// kRealCandidates, each timed on the second of two launches; the fastest pair is kept for
+// the context's later frames.  A molecule's energy is one fixed-order sum whatever the cell
+// grid and block size, so the choice moves only time.  The frame's own cell list is rebuilt
+// afterwards, so the rest of this frame runs on the grid it was planned with.
+static int tune_real(ermod_ctx* ctx, const FrameArgs& a, int ncell0, int nbatch, cudaStream_t st) {
   float best = 1e30f;
   int pick = 256;
+  float hpick = kCellDefault;
   cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1];
-  for (int rep = 0; rep < 2; ++rep)
-    for (int nt : kRealCandidates) {
-      CK(cudaEventRecord(e0, st));
-      launch_real(a, ctx->d, 0, nbatch, ctx->batch, nt, st);
-      CK(cudaEventRecord(e1, st));
-      CK(cudaEventSynchronize(e1));
-      float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, e0, e1));
-      if (rep == 1 && ms < best) { best = ms; pick = nt; }
+  const int nh = a.use_cells ? (int)(sizeof(kCellCandidates) / sizeof(float)) : 1;
+  for (int ih = 0; ih < nh; ++ih) {
+    FrameArgs b = a;
+    if (a.use_cells) {
+      int nc = 0;
+      if (!cell_grid(ctx, b, kCellCandidates[ih], nc)) continue;
+      launch_cells(b, ctx->d, nc, st);
     }
+    for (int rep = 0; rep < 2; ++rep)
+      for (int nt : kRealCandidates) {
+        CK(cudaEventRecord(e0, st));
+        launch_real(b, ctx->d, 0, nbatch, ctx->batch, nt, st);
+        CK(cudaEventRecord(e1, st));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep == 1 && ms < best) {
+          best = ms;
+          pick = nt;
+          hpick = a.use_cells ? kCellCandidates[ih] : kCellDefault;
+        }
+      }
+  }
+  if (a.use_cells) launch_cells(a, ctx->d, ncell0, st);
   ctx->real_threads = pick;
+  ctx->cell_h = hpick;
   return ERMOD_OK;
 }
 
@@ -992,10 +1030,19 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
   for (int bb = 0; bb < ctx->maxdst; bb += ctx->batch) {
     const int nbatch = std::min(ctx->batch, ctx->maxdst - bb);
     if (ctx->real_threads == 0) {
-      const int rc = tune_real(ctx, a, nbatch, st);
+      const int rc = tune_real(ctx, a, fp.ncell, nbatch, st);
       if (rc != ERMOD_OK) return rc;
     }
-    launch_real(a, d, bb, nbatch, ctx->batch, ctx->real_threads, st);
+    // Real space beside the PME chain: k_real on the second stream, joined before binning (the
+    // gather writes the reciprocal part, k_bin adds the real part).  Stage-timed runs keep one
+    // stream so that each stage's events bracket it alone; the arithmetic is the same.
+    const bool fork = pme && !timed;
+    if (fork) {
+      CK(cudaEventRecord(ctx->ev_fork, st));
+      CK(cudaStreamWaitEvent(ctx->st2, ctx->ev_fork, 0));
+    }
+    launch_real(a, d, bb, nbatch, ctx->batch, ctx->real_threads, fork ? ctx->st2 : st);
+    if (fork) CK(cudaEventRecord(ctx->ev_join, ctx->st2));
     M(kStReal);
     nl += 1;
     if (pme && ctx->spath != 1) {
@@ -1033,7 +1080,8 @@ static int frame_enqueue(ermod_ctx* ctx, const FramePlan& fp, cudaStream_t st, b
       M(kStGather);
       nl += 1;
     }
-    launch_bin(d, fp.ba, bb, nbatch, ctx->slvmax, st);
+    if (fork) CK(cudaStreamWaitEvent(st, ctx->ev_join, 0));   // the real-space energies of the batch
+    launch_bin(d, fp.ba, bb, nbatch, ctx->slvmax, ctx->batch, st);
     M(kStBin);
     nl += 1;
     if (d.uvengy)

@@ -20,6 +20,10 @@ constexpr int kInflBlocks = 64;    // CTAs per target in the influence multiply
 constexpr int kEdensSlices = 32;   // target slices of the edens reduction
 constexpr int kMaxGrid = 256;      // largest PME grid dimension (x rows are one CTA dimension)
 constexpr int kChunk = 32;         // PME solves per chunk: one warp lane per target
+// Fused PME solve: k1 planes whose every mode has a Gaussian factor exp(-pi^2 |k|^2 / screen^2)
+// below kModeCut are not transformed (their share of any molecule energy is below 1e-9 of the
+// k = 0 weight per mode, far under FP32 rounding).
+constexpr double kModeCut = 1e-9;
 constexpr int kMlpIn = 64;         // proposal network: 4x4x4 local density inputs
 constexpr int kMlpHidden = 128;    // width of its three hidden layers
 
@@ -241,7 +245,10 @@ struct BinArgs {
 };
 void launch_gather(const FrameArgs& a, const DeviceState& d, int base, int bb, int nb, int chunk, int batch,
                    bool pdl, cudaStream_t s);
-void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int slvmax, cudaStream_t s);
+// Bins a batch's energy rows; where d.E is set, first adds the real-space energies of the
+// batch (d.E, molecule-major with leading dimension `batch`) to Etot and writes the sum back.
+void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int slvmax, int batch,
+                cudaStream_t s);
 int setup_bin_smem(const BinArgs& ba);
 
 struct WeightArgs {

@@ -1235,8 +1235,10 @@ void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb
 // ---------------------------------------------------------------------------
 // PME gather + residual.  A warp per solvent molecule, lane = target of the
 // chunk (chunk == 32): the potential grid is stored target-fastest, so each
-// stencil point is one coalesced 128-byte row.  Writes the total energy of
-// every (target, molecule) pair into Etot[target][molecule] (the uvengy layout).
+// stencil point is one coalesced 128-byte row.  Writes the reciprocal-space and
+// residual energy of every (target, molecule) pair into Etot[target][molecule]
+// (the uvengy layout); k_bin adds the real-space energies, so that k_real runs
+// beside the whole PME chain.
 // ---------------------------------------------------------------------------
 constexpr int kGatherThreads = 256;
 
@@ -1262,12 +1264,36 @@ __device__ __forceinline__ void gather_rows4(const float* __restrict__ p0, size_
     }
 }
 
+// The stencil contraction of CS planes c3 (from c30) of one site, separably: along n1 then
+// n2 in FP32 (16 points a plane), each plane's q w3 share added to the FP64 energy.
+// v[(cs * NO + c2) * NO + c1] = phi(gd.x - c1, gd.y - c2, gd.z - c30 - cs); w = w1 | w2 | w3.
+template <int NO, int CS, class W>
+__device__ __forceinline__ void accumulate_planes(const float (&v)[CS * NO * NO], const W& w, int c30, float q,
+                                                  double& e) {
+  float w1[NO], w2[NO];
+#pragma unroll
+  for (int c = 0; c < NO; ++c) { w1[c] = w[c]; w2[c] = w[NO + c]; }
+#pragma unroll
+  for (int cs = 0; cs < CS; ++cs) {
+    float plane = 0.0f;
+#pragma unroll
+    for (int c2 = 0; c2 < NO; ++c2) {
+      const float* r = v + (cs * NO + c2) * NO;
+      float row = w1[0] * r[0];
+#pragma unroll
+      for (int c1 = 1; c1 < NO; ++c1) row = fmaf(w1[c1], r[c1], row);
+      plane = fmaf(w2[c2], row, plane);
+    }
+    e += (double)(q * w[2 * NO + c30 + cs]) * (double)plane;
+  }
+}
+
 template <int NO>
 __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(FrameArgs a, int base, int bb, int nb,
     int chunk, int batch, const int* __restrict__ molsorted, const int* __restrict__ molbeg,
     const float* __restrict__ molq, const float* __restrict__ atom_q, const float* __restrict__ spl,
-    const int4* __restrict__ grd, const float* __restrict__ phi, const double* __restrict__ Ereal,
-    const double* __restrict__ tgtq, const int* __restrict__ tgt_mol, double* __restrict__ Etot) {
+    const int4* __restrict__ grd, const float* __restrict__ phi, const double* __restrict__ tgtq,
+    const int* __restrict__ tgt_mol, double* __restrict__ Etot) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwt = (gridDim.x * blockDim.x) >> 5;
@@ -1282,7 +1308,7 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
   grid_dep_launch();                                  // the next chunk's planes may start filling the tail
   for (int m = gw; m < a.slvmax; m += nwt) {
     const int k = molsorted[m];
-    double e = active ? Ereal[(size_t)k * batch + bi] : 0.0;
+    double e = 0.0;
     const int b0 = molbeg[k], b1 = molbeg[k + 1];
     if (a.pme) {
       for (int at = b0; at < b1; ++at) {
@@ -1306,18 +1332,7 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
               float v[CS * NO * NO];
               if (odd) gather_rows4<CS, true>(p0, s2, s3, c30, v);
               else gather_rows4<CS, false>(p0, s2, s3, c30, v);
-#pragma unroll
-              for (int cs = 0; cs < CS; ++cs) {
-                const float fac1 = q * w[2 * NO + c30 + cs];
-#pragma unroll
-                for (int c2 = 0; c2 < NO; ++c2) {
-                  const float fac2 = fac1 * w[NO + c2];
-                  float part = 0.0f;
-#pragma unroll
-                  for (int c1 = 0; c1 < NO; ++c1) part += (fac2 * w[c1]) * v[(cs * NO + c2) * NO + c1];
-                  e += (double)part;
-                }
-              }
+              accumulate_planes<NO, CS>(v, w, c30, q, e);
             }
             continue;
           }
@@ -1337,18 +1352,7 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
                 for (int c1 = 0; c1 < NO; ++c1) v[(cs * NO + c2) * NO + c1] = rowp[r1[c1]];
               }
             }
-#pragma unroll
-            for (int cs = 0; cs < CS; ++cs) {
-              const float fac1 = q * w[2 * NO + c30 + cs];
-#pragma unroll
-              for (int c2 = 0; c2 < NO; ++c2) {
-                const float fac2 = fac1 * w[NO + c2];
-                float part = 0.0f;
-#pragma unroll
-                for (int c1 = 0; c1 < NO; ++c1) part += (fac2 * w[c1]) * v[(cs * NO + c2) * NO + c1];
-                e += (double)part;
-              }
-            }
+            accumulate_planes<NO, CS>(v, w, c30, q, e);
           }
         } else {
           float w1[kMaxOrder];
@@ -1385,8 +1389,8 @@ void launch_gather(const FrameArgs& a, const DeviceState& d, int base, int bb, i
   if (blocks < 1) blocks = 1;
 #define ERM_GATHER(NO) launch_k(pdl, blocks, kGatherThreads, 0, s, k_gather<NO>, a, base, bb, nb, chunk, batch, \
       (const int*)d.molsorted, (const int*)d.molbeg, (const float*)d.molq, (const float*)d.atom_q,         \
-      (const float*)d.spl, (const int4*)d.grd, (const float*)d.phi, (const double*)d.E,                     \
-      (const double*)d.tgtq, (const int*)d.tgt_mol, d.Etot)
+      (const float*)d.spl, (const int4*)d.grd, (const float*)d.phi, (const double*)d.tgtq,                  \
+      (const int*)d.tgt_mol, d.Etot)
   if (a.pme && a.order == 4) ERM_GATHER(4);
   else if (a.pme && a.order == 6) ERM_GATHER(6);
   else ERM_GATHER(0);
@@ -1402,6 +1406,7 @@ constexpr int kBinThreads = 256;
 constexpr int kMaxSpecSmem = 128;
 
 __global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slvmax, double* __restrict__ Etot,
+    const double* __restrict__ Ereal, int batch,
     const int* __restrict__ molspec, const int* __restrict__ spec_off, const double* __restrict__ uvcrd,
     const int* __restrict__ uvsoft, const int* __restrict__ tgt_mol, const int* __restrict__ skip,
     uint32_t* __restrict__ counts, double* __restrict__ etot, double* __restrict__ flceng, float* __restrict__ minuv,
@@ -1426,11 +1431,15 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slv
   for (int i = threadIdx.x; i < kMaxSpecSmem; i += blockDim.x) { smin[i] = FLT_MAX; smax[i] = -FLT_MAX; sfl[i] = 0.0; }
   __syncthreads();
   const int excl = tgt_mol ? tgt_mol[cnt] : -1;
-  const double* row = Etot + (size_t)bi * slvmax;
+  double* row = Etot + (size_t)bi * slvmax;
   double acc = 0.0;
   for (int k = threadIdx.x; k < slvmax; k += blockDim.x) {
     if (k == excl) continue;
-    const double e = row[k];
+    double e = row[k];
+    if (Ereal) {   // the real-space energy of the pair (molecule-major), added to the reciprocal part
+      e += Ereal[(size_t)k * batch + bi];
+      row[k] = e;
+    }
     const int pti = molspec[k];
     if (pti <= 0) { report(st, kErrEngCns, k, cnt, (float)e); continue; }
     const int lo = spec_off[pti - 1], num = spec_off[pti] - lo;
@@ -1478,16 +1487,24 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slv
 
 size_t bin_smem_bytes(const BinArgs& ba) { return sizeof(double) * ba.ermax + sizeof(uint32_t) * ba.ermax_pad; }
 
-void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int slvmax, cudaStream_t s) {
+void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int slvmax, int batch,
+                cudaStream_t s) {
   if (nbatch <= 0) return;
-  k_bin<<<nbatch, kBinThreads, bin_smem_bytes(ba), s>>>(ba, bb, slvmax, d.Etot, d.molspec, d.spec_off, d.uvcrd,
+  k_bin<<<nbatch, kBinThreads, bin_smem_bytes(ba), s>>>(ba, bb, slvmax, d.Etot, d.E, batch, d.molspec, d.spec_off,
+                                                        d.uvcrd,
                                                         d.uvsoft, d.tgt_mol, d.skip, d.counts, d.etot, d.flceng,
                                                         d.minuv, d.maxuv, d.status);
 }
 
+// The limit is a per-device attribute of k_bin shared by every context and the
+// allocation-free entry point: it is only ever raised, so a smaller mesh set up
+// later never lowers it below what a larger one needs.
 int setup_bin_smem(const BinArgs& ba) {
   const size_t b = bin_smem_bytes(ba);
   if (b > 200 * 1024) return -1;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, k_bin) != cudaSuccess) return -1;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= b) return 0;
   return cudaFuncSetAttribute(k_bin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b) == cudaSuccess ? 0 : -1;
 }
 

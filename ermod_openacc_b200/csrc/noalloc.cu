@@ -127,7 +127,7 @@ extern "C" int32_t ermod_histogram_noalloc(int32_t device, int32_t slttype, cons
   ba.numslv = numslv;
   ba.slttype = soln ? ERMOD_SLT_SOLN : ERMOD_SLT_REFS_RIGID;
   if (setup_bin_smem(ba) != 0) return ERMOD_ERR_OVERFLOW;
-  launch_bin(d, ba, 0, ntarget, nmol, s);
+  launch_bin(d, ba, 0, ntarget, nmol, 0, s);
   launch_edens(d, 0, ntarget, ermax, ermax_pad, 0, s);
   DevStatus hs;
   if (cudaMemcpyAsync(&hs, d_st, sizeof(hs), cudaMemcpyDeviceToHost, s) != cudaSuccess) return ERMOD_ERR_CUDA;

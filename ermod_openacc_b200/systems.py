@@ -124,9 +124,11 @@ def _rot_from_quat(q):
 def random_packing(n: int, box: float, rng, dmin: float = 2.5, max_tries: int = 5000, obstacle=None,
                    obstacle_r: float = 0.0):
     """n points in a periodic cube by random sequential addition with a minimum
-    separation `dmin` (and at least `obstacle_r` from the point `obstacle`): a
-    disordered packing with the density fluctuations and cavities of a liquid
-    (the lattice has none)."""
+    separation `dmin` (and at least `obstacle_r` from the point, or every row of the
+    points, `obstacle`): a disordered packing with the density fluctuations and cavities
+    of a liquid (the lattice has none)."""
+    if obstacle is not None:
+        obstacle = np.atleast_2d(np.asarray(obstacle, dtype=np.float64))
     nc = max(1, int(box // dmin))
     h = box / nc
     cells = {}
@@ -138,7 +140,7 @@ def random_packing(n: int, box: float, rng, dmin: float = 2.5, max_tries: int = 
             if obstacle is not None:
                 d = p - obstacle
                 d -= box * np.round(d / box)
-                if d @ d < obstacle_r * obstacle_r:
+                if np.einsum("ij,ij->i", d, d).min() < obstacle_r * obstacle_r:
                     continue
             c = tuple((p // h).astype(int) % nc)
             ok = True
@@ -172,8 +174,10 @@ def water_box_frame(nside: int, box: float, seed: int, jitter=0.3, avoid=None, a
 
     packing "lattice": centres of mass on the n^3 lattice plus Gaussian
     `jitter`; "random": a random sequential packing at the same density.
-    `avoid`: optional point; water oxygens closer than `avoid_r` are pushed
-    radially out to `avoid_r` (keeps a soln solute out of the hard core).
+    `avoid`: optional point (or rows of points); water oxygens closer than `avoid_r`
+    to it are pushed radially out to `avoid_r` (keeps a soln solute out of the hard
+    core).  With several points the random packing keeps every oxygen `avoid_r` away
+    from all of them; the lattice packing pushes from the nearest one.
     """
     rng = np.random.default_rng(seed)
     wat = water()
@@ -193,13 +197,15 @@ def water_box_frame(nside: int, box: float, seed: int, jitter=0.3, avoid=None, a
     for i in range(n):
         out[i] = (_rot_from_quat(q[i]) @ body).T + com[i]
     if avoid is not None:
-        avoid = np.asarray(avoid, dtype=np.float64)
+        avoid = np.atleast_2d(np.asarray(avoid, dtype=np.float64))
         for i in range(n):
             d = out[i, 0] - avoid
             d -= box * np.round(d / box)
-            r = np.linalg.norm(d)
+            rr = np.linalg.norm(d, axis=1)
+            j = int(np.argmin(rr))
+            r = rr[j]
             if r < avoid_r:
-                shift = d / max(r, 1e-6) * (avoid_r - r)
+                shift = d[j] / max(r, 1e-6) * (avoid_r - r)
                 out[i] += shift
     return out.reshape(-1, 3).T
 
@@ -344,11 +350,17 @@ class Workload:
     seed: int
     solute_center: np.ndarray | None = None     # soln: fixed solute position
     packing: str = "lattice"                     # water centres: "lattice" + jitter or "random"
+    avoid_sites: bool = False                    # soln: keep waters avoid_r from every solute site
+    avoid_r: float = 3.0
 
     def frame(self, i: int):
         """sitepos (3*numatm_phys float32, Fortran order) and cell (9 float32) of frame i."""
         avoid = self.solute_center
-        wat = water_box_frame(self.nside, self.box, self.seed * 1000003 + i, avoid=avoid, packing=self.packing)
+        if self.avoid_sites and self.solute_center is not None:
+            avoid = np.concatenate([(np.asarray(sp.coords) + self.solute_center[:, None]).T
+                                    for sp, kind in zip(self.topo.species, self.topo.kinds) if kind == A.PT_SOLUTE])
+        wat = water_box_frame(self.nside, self.box, self.seed * 1000003 + i, avoid=avoid, avoid_r=self.avoid_r,
+                              packing=self.packing)
         parts = []
         for sp, cnt, kind in zip(self.topo.species, self.topo.counts, self.topo.kinds):
             if kind == A.PT_SOLVENT and sp.name == "water":

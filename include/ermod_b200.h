@@ -112,7 +112,8 @@ typedef struct ermod_params {
   double  temp;                   /* kcal/mol */
   float   elecut, lwljcut, upljcut, screen;
   /* engine options (no reference counterpart; 0 = automatic) */
-  int32_t ins_chunk;              /* insertions per PME chunk (16 or 32; 0 = tuned) */
+  int32_t ins_chunk;              /* insertions per PME chunk: 0 or 32 (the chunk is one warp lane per
+                                     insertion; other values are refused with "ins_chk") */
   int32_t ecorr_batch;            /* insertions per ecorr GEMM batch (0 = auto) */
   int32_t weight_bits;            /* fixed-point bits of ecorr weights (0 = 24) */
   int32_t proposal;               /* ERMOD_PROPOSAL_* */
@@ -396,18 +397,26 @@ void ermod_batch_destroy(ermod_batch* b);
  * fastest, as returned by ermod_get_uvengy) with getiduv's rule and returns
  * edens(i) = sum over targets of weight(target) * count(target, i) (host,
  * [ermax] with ermax = sum(uvmax)).  uvspec [nmol] gives each molecule's
- * solvent species (0 = skipped with eng_cns as in the engine), uvcrd /
+ * solvent species (a 0 is an error, eng_cns, as in the engine), uvcrd /
  * uvmax / uvsoft the mesh (uvsoft may be NULL; it is used only when
  * slttype == ERMOD_SLT_SOLN).  Status codes as ermod_engconst.
+ *
+ * Solutes in solution (slttype == ERMOD_SLT_SOLN): the engine skips the
+ * solute's own molecule (its uvspec is 0).  Here every column of uvengy is
+ * binned, so leave the solute's column out of uvengy and its entry out of
+ * uvspec (nmol one less than the physical molecule count).
  *
  * All device memory it uses is one array of ERMOD_NOALLOC_SCRATCH_BYTES
  * compiled into the library, which every GPU that loads the library holds
  * until the process exits; requests that do not fit return
  * ERMOD_ERR_OVERFLOW.  The first call on a device looks up that array's
- * device address (cudaGetSymbolAddress) and caches it; make that first
- * call before any stream capture.  Calls run on the legacy default stream
- * and share the one array: calls that overlap on the GPU (other host
- * threads, other streams) race and must be serialised by the caller.
+ * device address (cudaGetSymbolAddress) and keeps it for later calls; make
+ * that first call before any stream capture.  The kept address belongs to
+ * the device's current context: after cudaDeviceReset it is stale, so do not
+ * call this entry point again in that process.  Calls run on the legacy
+ * default stream and share the one array: calls that overlap on the GPU
+ * (other host threads, other streams) race and must be serialised by the
+ * caller.
  */
 #define ERMOD_NOALLOC_SCRATCH_BYTES (32u << 20)
 int32_t ermod_histogram_noalloc(int32_t device, int32_t slttype, const double* uvengy, int32_t ntarget,

@@ -27,8 +27,12 @@ def test_roofline_helpers():
     sys.path.insert(0, ROOT)
     import bench
     from ermod_openacc_b200 import systems as S
-    assert bench.traffic_from_profiles("k_pme_plane") > 0
-    assert bench.traffic_from_profiles("no_such_kernel") is None
+    assert bench.profile_table("no_such_table.txt") == {}
+    assert bench.bound_from_counters({}) == "unmeasured"
+    assert bench.bound_from_counters({"tensor_pipe": 0.7}) == "tensor"
+    assert bench.bound_from_counters({"issue_active": 0.65, "fma_pipe": 0.44}) == "sm-issue"
+    assert bench.bound_from_counters({"issue_active": 0.3, "dram_frac": 0.1}) == "latency"
     w = S.make_workload(2)
+    assert 1000.0 < bench.path_bytes_per_unit(w, 12288, 4096, 1396, 2000, 12) < 1100.0
     for stage in ("gather", "bin", "pme_plane", "site_tables"):
         assert bench.kernel_bytes(stage, w, 32, 12288, 4096, 1396, 2000, 12) > 0

@@ -157,7 +157,8 @@ def test_precision_chain_full_size(lib, oracle_mod):
     assert np.all((bg == bo) | near_edge(uo, eng.uvcrd, edge_tol))
     st.update(workload=w.name, insertions=int(eng.maxdst), pme_solve=int(paths["spectrum_path"]),
               bin_flips=int((bg != bo).sum()), within_fp64_tolerance=frac_in_tol,
-              fp32_reference_algorithm=st32)
+              pairs_over_1e5=int((rel_err(u, uo)[soft] > 1e-5).sum()),
+              fp32_reference_algorithm=dict(st32, pairs_over_1e5=int((rel_err(u4, uo)[soft] > 1e-5).sum())))
     TABLE["precision-chain60-water32768 (C3, 64 insertions)"] = st
     eng.close()
 
