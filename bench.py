@@ -483,6 +483,17 @@ def main_batch(args):
             batch.engconst_dev(args.warmup + i + 1, dev_pos[args.warmup + i].data_ptr(), cell)
             dev_ms += batch.last_ms()
     sizes = [int(m.nsite_slt) for m in members]
+    # each member alone, its own one-graph frame, one after another: the batch graph's time against
+    # the sum of these says how much running the members as branches of one graph already overlaps,
+    # and bounds what a persistent frame kernel could still remove (launch and dependency gaps)
+    alone_ms = 0.0
+    for j, m in enumerate(members):
+        for i in range(2):
+            m.engconst_dev(nfr + 10 * j + i + 1, dev_pos[i % nfr].data_ptr(), cell)
+        flush.zero_()
+        torch.cuda.synchronize()
+        m.engconst_dev(nfr + 10 * j + 3, dev_pos[0].data_ptr(), cell)
+        alone_ms += m.last_ms()
     line = {"metric": METRIC, "value": units * args.steps / (dev_ms * 1e-3), "unit": UNIT, "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -491,7 +502,9 @@ def main_batch(args):
                        "solute_sites": [min(sizes), max(sizes), sum(sizes) / len(sizes)],
                        "insertions_per_solute": int(members[0].maxdst), "waters": int(members[0].slvmax),
                        "launch": "one CUDA graph per frame for all solutes",
-                       "l2": "flushed before every step (256 MiB write)"}}
+                       "l2": "flushed before every step (256 MiB write)"},
+            "members_alone_ms_sum": alone_ms,
+            "batch_over_alone": (dev_ms / args.steps) / alone_ms if alone_ms > 0 else None}
     clk_s = clk.summary()
     if clk_s:
         line["clocks"] = clk_s

@@ -31,9 +31,11 @@
 // on an mbarrier has an iteration limit; on expiry the kernel records an
 // error, waits (again bounded) for its MMAs in flight, frees its TMEM and
 // returns.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "engine.cuh"
 
@@ -340,6 +342,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ecorr_tc(int ermax, int kpad, c
   // mirror of tiles computed elsewhere
   if (j0 + kTileN <= i0) return;
   const QuantParams Q = *qp;
+  if (!Q.has_high) return;   // at most kMaxHigh bins above 255: k_ecorr_tma serves the batch
   const int P = Q.P;
   const int nk = kpad / kTileK;
   if (warp == 0) {
@@ -486,6 +489,220 @@ __global__ void __launch_bounds__(kThreads, 1) k_ecorr_tc(int ermax, int kpad, c
 
 constexpr size_t kSmemBytes = sizeof(TcSmem) + 1024;
 
+// ---- byte-digit terms, fed by TMA ---------------------------------------
+// With m = sum_d 256^d b_d (b_d = byte d of the integer weight), the low-byte part is
+//   sum_k w_k L_ik L_jk = wmin (L^T L)_ij + q sum_d 256^d (256 (L^T X_d)_ij + (L^T Y_d)_ij),
+// where b_dk L_jk = 256 X_djk + Y_djk splits the (at most 16-bit) product into two exact
+// bytes.  So 1 + 2 ceil(P / 8) INT8 GEMMs replace the 1 + P masked ones, and every operand
+// is a plain byte array that TMA can stream: T[term][bin][insertion], term 0 = L,
+// 1 + 2d = X_d, 2 + 2d = Y_d.
+constexpr int kMaxBytes = (kMaxDigits + 7) / 8;   // 4
+constexpr int kMaxTerms = 1 + 2 * kMaxBytes;      // 9
+constexpr int kTmaStages = 3;
+constexpr int kTmaGroup = 4;                      // terms per pass: 4 x 64 TMEM columns
+constexpr int kTmaThreads = 128;
+
+__global__ void k_ecorr_terms(int rows, int kpad, const uint8_t* __restrict__ L, const uint32_t* __restrict__ m,
+                              const QuantParams* __restrict__ qp, const int* __restrict__ high,
+                              uint8_t* __restrict__ XY) {
+  if (*high) return;
+  const int nd = (qp->P + 7) / 8;
+  const size_t slab = (size_t)rows * kpad;
+  const size_t i16 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;   // 16-insertion chunk of one bin
+  if (i16 * 16 >= slab) return;
+  const size_t off = i16 * 16;
+  const int k0 = (int)(off % (size_t)kpad);
+  const uint4 lv = *reinterpret_cast<const uint4*>(L + off);
+  const uint8_t* l = reinterpret_cast<const uint8_t*>(&lv);
+  for (int d = 0; d < nd; ++d) {
+    alignas(16) uint8_t x[16], y[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      const uint32_t v = ((m[k0 + e] >> (8 * d)) & 255u) * (uint32_t)l[e];
+      x[e] = (uint8_t)(v >> 8);
+      y[e] = (uint8_t)(v & 255u);
+    }
+    *reinterpret_cast<uint4*>(XY + (size_t)(2 * d) * slab + off) = *reinterpret_cast<const uint4*>(x);
+    *reinterpret_cast<uint4*>(XY + (size_t)(2 * d + 1) * slab + off) = *reinterpret_cast<const uint4*>(y);
+  }
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// TMA tile loads of this GPU's own memory into shared memory (no multicast)
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+struct TmaStage {
+  uint8_t a[kTileM * kTileK];              // L tile, 16 KB (1024-B aligned)
+  uint8_t b[kTmaGroup][kTileN * kTileK];   // term tiles, 8 KB each
+};
+struct TmaSmem {
+  TmaStage st[kTmaStages];
+  uint64_t full[kTmaStages], empty[kTmaStages], done;
+  uint32_t tmem_base;
+};
+constexpr size_t kTmaSmemBytes = sizeof(TmaSmem) + 1024;
+
+// A CTA per 128 x 64 tile of the upper triangle; thread 0 streams the tiles of every K step
+// (the L rows of the tile's 128 bins, the term rows of its 64 bins) into a ring of
+// kTmaStages stages, thread 32 issues the MMAs of each full stage into kTmaGroup TMEM
+// accumulators and commits the stage back, and the four warps read the accumulators
+// (lanes = rows) once the pass is done.  Every mbarrier wait has an iteration limit.
+__global__ void __launch_bounds__(kTmaThreads, 1) k_ecorr_tma(int ermax, int kpad,
+    const __grid_constant__ CUtensorMap tmapA, const __grid_constant__ CUtensorMap tmapB,
+    const QuantParams* __restrict__ qp, double* __restrict__ ecorr, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tsm_raw[];
+  TmaSmem& S = *reinterpret_cast<TmaSmem*>((void*)(((uintptr_t)tsm_raw + 1023) & ~(uintptr_t)1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int i0 = blockIdx.y * kTileM, j0 = blockIdx.x * kTileN;
+  if (j0 + kTileN <= i0) return;                 // the mirror of a tile computed elsewhere
+  const QuantParams Q = *qp;
+  if (Q.has_high) return;                        // k_ecorr_tc's limb products serve this batch
+  const int nterms = 1 + 2 * ((Q.P + 7) / 8);
+  const int nk = kpad / kTileK;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
+                 "r"(kTmaGroup * kTileN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kTmaStages; ++s) { mbar_init(&S.full[s], 1); mbar_init(&S.empty[s], 1); }
+    mbar_init(&S.done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+  bool ok = true;
+  int it = 0;                                    // K steps streamed so far (both roles count alike)
+  int pass = 0;
+  for (int t0 = 0; t0 < nterms && ok; t0 += kTmaGroup, ++pass) {
+    const int G = min(kTmaGroup, nterms - t0);
+    const uint32_t bytes = (uint32_t)(kTileM * kTileK + G * kTileN * kTileK);
+    if (tid == 0) {                              // producer
+      for (int kt = 0; kt < nk && ok; ++kt) {
+        const int i = it + kt, s = i % kTmaStages;
+        if (i >= kTmaStages && !mbar_wait(&S.empty[s], (uint32_t)((i / kTmaStages - 1) & 1))) { ok = false; break; }
+        mbar_expect_tx(&S.full[s], bytes);
+        tma_load_2d(S.st[s].a, &tmapA, kt * kTileK, i0, &S.full[s]);
+        for (int g = 0; g < G; ++g) tma_load_3d(S.st[s].b[g], &tmapB, kt * kTileK, j0, t0 + g, &S.full[s]);
+      }
+    } else if (tid == 32) {                      // MMA issuer
+      for (int kt = 0; kt < nk && ok; ++kt) {
+        const int i = it + kt, s = i % kTmaStages;
+        if (!mbar_wait(&S.full[s], (uint32_t)((i / kTmaStages) & 1))) { ok = false; break; }
+        tc_fence_after();
+        const uint64_t da0 = smem_desc(smem_u32(S.st[s].a));
+        for (int g = 0; g < G; ++g) {
+          const uint64_t db0 = smem_desc(smem_u32(S.st[s].b[g]));
+#pragma unroll
+          for (int ks = 0; ks < kTileK / 32; ++ks)
+            mma_i8(tmem + (uint32_t)(g * kTileN), da0 + (uint64_t)(ks * 2), db0 + (uint64_t)(ks * 2),
+                   (kt > 0 || ks > 0) ? 1u : 0u);
+        }
+        mma_commit(&S.empty[s]);
+      }
+      if (ok) mma_commit(&S.done);
+    }
+    it += nk;
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok) break;
+    ok = __syncthreads_and(mbar_wait(&S.done, (uint32_t)(pass & 1))) != 0;
+    if (!ok) break;
+    // epilogue: warp w owns TMEM lanes 32w..32w+31 = rows i0 + 32w + lane
+    tc_fence_after();
+    const int row = i0 + warp * 32 + lane;
+    for (int cc = 0; cc < kTileN; cc += 32) {
+      double acc[32];
+#pragma unroll
+      for (int e = 0; e < 32; ++e) acc[e] = 0.0;
+      for (int g = 0; g < G; ++g) {
+        const int term = t0 + g;
+        const int d = (term - 1) >> 1;
+        const double scale = term == 0 ? Q.wmin : ldexp(Q.q, 8 * d + (((term - 1) & 1) ? 0 : 8));
+        uint32_t v[32];
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(g * kTileN + cc), v);
+#pragma unroll
+        for (int e = 0; e < 32; ++e) acc[e] += scale * (double)(int32_t)v[e];
+      }
+      if (row < ermax) {
+#pragma unroll
+        for (int e = 0; e < 32; ++e) {
+          const int col = j0 + cc + e;
+          if (col >= ermax || col < row) continue;
+          ecorr[(size_t)row * ermax + col] += acc[e];
+          if (col > row) ecorr[(size_t)col * ermax + row] += acc[e];
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();                             // TMEM free for the next pass
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(err, kErrTimeout);
+    mbar_wait(&S.done, (uint32_t)(pass & 1));    // bounded: MMAs in flight finish before TMEM goes
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmaGroup * kTileN));
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, []() {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  });
+  return fn;
+}
+
+// u8 tensor maps over the term array T[kMaxTerms][rows][kpad]: A = term 0 in 128-row boxes,
+// B = any term in 64-row boxes; 128-byte rows, 128-byte swizzle (the UMMA K-major layout)
+bool make_term_maps(uint8_t* T, int rows, int kpad, CUtensorMap* a, CUtensorMap* b) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dimA[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+  const cuuint64_t strA[1] = {(cuuint64_t)kpad};
+  const cuuint32_t boxA[2] = {(cuuint32_t)kTileK, (cuuint32_t)kTileM};
+  const cuuint32_t es2[2] = {1, 1};
+  if (enc(a, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, T, dimA, strA, boxA, es2, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+      CUDA_SUCCESS)
+    return false;
+  const cuuint64_t dimB[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, (cuuint64_t)kMaxTerms};
+  const cuuint64_t strB[2] = {(cuuint64_t)kpad, (cuuint64_t)rows * kpad};
+  const cuuint32_t boxB[3] = {(cuuint32_t)kTileK, (cuuint32_t)kTileN, 1};
+  const cuuint32_t es3[3] = {1, 1, 1};
+  return enc(b, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, T, dimB, strB, boxB, es3, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
 }  // namespace
 
 int ecorr_tc_available() { return 1; }
@@ -493,27 +710,25 @@ int ecorr_tc_available() { return 1; }
 size_t ecorr_tc_workspace(int n, int ermax) {
   const size_t kpad = (size_t)(n + kTileK - 1) / kTileK * kTileK;
   const size_t ermax_pad = (size_t)(ermax + 127) / 128 * 128;
-  return 2 * ermax_pad * kpad + 4 * kpad + (kpad / kTileK) * (kMaxDigits + 1) * 8 * 2 + 256 + 64 +
+  return (kMaxTerms + 1) * ermax_pad * kpad + 4 * kpad + (kpad / kTileK) * (kMaxDigits + 1) * 8 * 2 + 256 + 64 +
          sizeof(int) * (ermax_pad + kMaxHigh + 4);
 }
 
 // ecorr += C^T diag(w) C for targets [base, base+n) of the batch starting at count_base
 int launch_ecorr_tc(const DeviceState& d, int base, int n, int ermax, int ermax_pad, int count_base, int weight_bits,
                     void* work, size_t work_bytes, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_ecorr_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes) != cudaSuccess)
-      return -1;
-    attr = true;
-  }
+  if (raise_smem_limit(k_ecorr_tc, kSmemBytes) != cudaSuccess) return -1;
+  if (raise_smem_limit(k_ecorr_tma, kTmaSmemBytes) != cudaSuccess) return -1;
   const int kpad = (n + kTileK - 1) / kTileK * kTileK;
   const size_t nbits = (size_t)(kpad / kTileK) * (kMaxDigits + 1) * 8;
-  const size_t need = 2 * (size_t)ermax_pad * kpad + 4 * (size_t)kpad + 2 * nbits + 256 + 64 +
+  const size_t slab = (size_t)ermax_pad * kpad;
+  const size_t need = (kMaxTerms + 1) * slab + 4 * (size_t)kpad + 2 * nbits + 256 + 64 +
                       sizeof(int) * (ermax_pad + kMaxHigh + 4);
   if (need > work_bytes) return -2;
-  uint8_t* ctl = (uint8_t*)work;
-  uint8_t* cth = ctl + (size_t)ermax_pad * kpad;
-  uint32_t* m = (uint32_t*)(cth + (size_t)ermax_pad * kpad);
+  uint8_t* ctl = (uint8_t*)work;                 // term 0 of T[kMaxTerms][ermax_pad][kpad]
+  uint8_t* xy = ctl + slab;                      // terms 1 .. kMaxTerms - 1
+  uint8_t* cth = ctl + (size_t)kMaxTerms * slab;
+  uint32_t* m = (uint32_t*)(cth + slab);
   uint16_t* gbits = (uint16_t*)(m + kpad);
   QuantParams* qp = (QuantParams*)((uint8_t*)(gbits + nbits) + ((16 - (nbits * 2) % 16) % 16));
   int* high = (int*)((uint8_t*)qp + 64);
@@ -528,6 +743,11 @@ int launch_ecorr_tc(const DeviceState& d, int base, int n, int ermax, int ermax_
   k_high_list<<<1, kListThreads, 0, s>>>(ermax, hbin, hl, nh, high);
   k_quantize<<<1, 1024, 0, s>>>(base, n, kpad, weight_bits > 0 ? weight_bits : 24, d.w, m, gbits, qp, high);
   dim3 gg((ermax_pad + kTileN - 1) / kTileN, (ermax_pad + kTileM - 1) / kTileM);
+  CUtensorMap map_a, map_b;
+  if (!make_term_maps(ctl, ermax_pad, kpad, &map_a, &map_b)) return -4;
+  const size_t chunks = slab / 16;
+  k_ecorr_terms<<<(unsigned)((chunks + 255) / 256), 256, 0, s>>>(ermax_pad, kpad, ctl, m, qp, high, xy);
+  k_ecorr_tma<<<gg, kTmaThreads, kTmaSmemBytes, s>>>(ermax, kpad, map_a, map_b, qp, d.ecorr, errw);
   k_ecorr_tc<<<gg, kThreads, kSmemBytes, s>>>(ermax, kpad, ctl, cth, gbits, qp, d.ecorr, errw);
   k_ecorr_high<<<dim3((ermax + 31) / 32, kMaxHigh), kHighWarps * 32, 0, s>>>(n, ermax, ermax_pad, cnt, d.w + base,
                                                                               hbin, hl, nh, d.ecorr);

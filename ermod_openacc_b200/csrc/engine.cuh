@@ -66,6 +66,15 @@ cudaError_t launch_k(bool pdl, dim3 grid, dim3 block, size_t smem, cudaStream_t 
   return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
 }
 
+// A kernel's dynamic shared-memory limit is a per-device attribute that every context of
+// the process shares: raise it to `bytes` when below, never lower it (a context set up later
+// for a smaller solute or mesh must not make an earlier context's launches fail).
+cudaError_t raise_smem_limit_fn(const void* kernel, size_t bytes);
+template <class F>
+cudaError_t raise_smem_limit(F* kernel, size_t bytes) {
+  return raise_smem_limit_fn((const void*)kernel, bytes);
+}
+
 // Float offset of phi(n1) of grid line `line` (= n3 K2 + n2) and target b in the
 // pair layout: n1 pairs of kChunk targets, P1 = ceil(K1 / 2) pairs per line.
 __host__ __device__ __forceinline__ size_t phi_index(size_t line, int n1, int b, int P1) {

@@ -22,6 +22,8 @@
 #include <cstdio>
 
 #include "bestfit.cuh"
+#include <mutex>
+
 #include "engine.cuh"
 
 namespace erm {
@@ -875,8 +877,8 @@ size_t real_smem(const FrameArgs& a) {
 
 int setup_real_smem(const FrameArgs& a) {
   const int b = (int)real_smem(a);
-  if (cudaFuncSetAttribute(k_real<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess) return -1;
-  if (cudaFuncSetAttribute(k_real<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess) return -1;
+  if (raise_smem_limit(k_real<true>, (size_t)b) != cudaSuccess) return -1;
+  if (raise_smem_limit(k_real<false>, (size_t)b) != cudaSuccess) return -1;
   return 0;
 }
 
@@ -1154,10 +1156,7 @@ void launch_clear_box(const FrameArgs& a, const DeviceState& d, int chunk, cudaS
   k_clear_box<<<chunk, 256, 0, s>>>(a, d.boxinfo, d.grid);
 }
 
-int setup_spread_smem() {
-  return cudaFuncSetAttribute(k_spread_box, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpreadSmemBytes) ==
-                 cudaSuccess ? 0 : -1;
-}
+int setup_spread_smem() { return raise_smem_limit(k_spread_box, (size_t)kSpreadSmemBytes) == cudaSuccess ? 0 : -1; }
 
 // influence multiply + FP64 self energy of each target (recpcal.F90:482-497).
 // The self energy is reduced deterministically: per-block partials, summed in
@@ -1496,16 +1495,24 @@ void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int
                                                         d.minuv, d.maxuv, d.status);
 }
 
-// The limit is a per-device attribute of k_bin shared by every context and the
-// allocation-free entry point: it is only ever raised, so a smaller mesh set up
-// later never lowers it below what a larger one needs.
+// Shared by every context and the allocation-free entry point: only ever raised.
 int setup_bin_smem(const BinArgs& ba) {
   const size_t b = bin_smem_bytes(ba);
   if (b > 200 * 1024) return -1;
+  return raise_smem_limit(k_bin, b) == cudaSuccess ? 0 : -1;
+}
+
+namespace {
+std::mutex g_smem_limit_mu;   // concurrent context set-ups must not interleave get and set
+}
+
+cudaError_t raise_smem_limit_fn(const void* kernel, size_t bytes) {
+  std::lock_guard<std::mutex> lk(g_smem_limit_mu);
   cudaFuncAttributes fa;
-  if (cudaFuncGetAttributes(&fa, k_bin) != cudaSuccess) return -1;
-  if ((size_t)fa.maxDynamicSharedSizeBytes >= b) return 0;
-  return cudaFuncSetAttribute(k_bin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b) == cudaSuccess ? 0 : -1;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 // ---------------------------------------------------------------------------

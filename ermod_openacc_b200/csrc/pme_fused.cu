@@ -569,11 +569,8 @@ size_t rows_smem(const FrameArgs& a) {
 
 template <int L2, int L3>
 cudaError_t plane_attr(const FrameArgs& a) {
-  cudaError_t e = cudaFuncSetAttribute(k_pme_plane<L2, L3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)plane_smem(a, true));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_pme_plane<L2, L3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)plane_smem(a, false));
+  cudaError_t e = raise_smem_limit(k_pme_plane<L2, L3, true>, plane_smem(a, true));
+  if (e == cudaSuccess) e = raise_smem_limit(k_pme_plane<L2, L3, false>, plane_smem(a, false));
   return e;
 }
 
@@ -613,10 +610,10 @@ int setup_fused(const FrameArgs& a) {
   if (e != cudaSuccess) return -1;
   const int lm = lg(a.K1 / 2);
   const int sm = (int)rows_smem(a);
-  if (lm == 3) e = cudaFuncSetAttribute(k_pme_lines<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem(8));
-  if (lm == 4) e = cudaFuncSetAttribute(k_pme_lines<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem(16));
-  if (lm == 5) e = cudaFuncSetAttribute(k_pme_lines<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem(32));
-  if (lm == 6) e = cudaFuncSetAttribute(k_pme_rows<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (lm == 3) e = raise_smem_limit(k_pme_lines<3>, lines_smem(8));
+  if (lm == 4) e = raise_smem_limit(k_pme_lines<4>, lines_smem(16));
+  if (lm == 5) e = raise_smem_limit(k_pme_lines<5>, lines_smem(32));
+  if (lm == 6) e = raise_smem_limit(k_pme_rows<6>, (size_t)sm);
   return e == cudaSuccess ? 0 : -1;
 }
 

@@ -79,3 +79,19 @@ def test_batch_rejects_mismatched_solvent(lib):
         Batch([ea, eb])
     with pytest.raises(Exception):
         Batch([ea, ea])
+
+
+def test_contexts_of_different_sizes_coexist(engine_lib):
+    """Kernel shared-memory limits are per-device attributes shared by every context: a context
+    created later for a smaller solute must not lower them below what an earlier context with a
+    larger solute launches with (real-space solute tiles, direct-sum site tiles)."""
+    big = S.make_batch_workloads(1, small=True, maxins=32, site_range=(64, 64))[0]
+    eb = Engine(big.params, big.topo, big.hist)
+    small = S.make_workload(2, small=True, maxins=32)
+    es = Engine(small.params, small.topo, small.hist)
+    assert eb.nsite_slt == 64 and es.nsite_slt == 12
+    assert eb.engconst(1, *big.frame(0)) >= 0
+    assert es.engconst(1, *small.frame(0)) >= 0
+    assert eb.engconst(2, *big.frame(1)) >= 0
+    eb.close()
+    es.close()
