@@ -162,6 +162,7 @@ SIGNATURES = {
     "ermod_mlp_create": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.POINTER(C.c_float)]),
     "ermod_mlp_nparams": (C.c_int32, []),
     "ermod_mlp_forward": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_float)]),
+    "ermod_mlp_activations": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_float)]),
     "ermod_mlp_gradients": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32,
                                         C.POINTER(C.c_float), C.POINTER(C.c_double)]),
     "ermod_mlp_train_step": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32,

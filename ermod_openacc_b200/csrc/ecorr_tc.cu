@@ -38,10 +38,13 @@
 #include <mutex>
 
 #include "engine.cuh"
+#include "tc_sm100.cuh"
 
 namespace erm {
 
 namespace {
+
+using namespace tc;
 
 constexpr int kTileM = 128;          // bins of the A side (TMEM lanes)
 constexpr int kTileN = 64;           // bins of the B side (TMEM columns per accumulator)
@@ -50,7 +53,6 @@ constexpr int kMaxGroup = 8;         // accumulators per pass: 8 x 64 = 512 TMEM
 constexpr int kThreads = 256;
 constexpr int kMaxDigits = 30;
 constexpr int kMaxHigh = 64;         // bins with counts above 255 handled by the FP64 correction
-constexpr long long kSpinLimit = 1LL << 22;   // try_wait polls: a few seconds at most
 
 struct QuantParams {
   int P;              // weight digits
@@ -59,46 +61,6 @@ struct QuantParams {
   int pad;
   double wmin, q;     // w = wmin + m * q
 };
-
-// ---- PTX helpers --------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (long long it = 0; it < kSpinLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-// K-major, 128-byte swizzle, 8-row groups 1024 bytes apart (CUTLASS UMMA::SmemDescriptor layout)
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
-  d |= (uint64_t)1 << 16;                          // leading byte offset (16 B units), unused for SW128 K-major
-  d |= (uint64_t)(1024 >> 4) << 32;                // stride byte offset: 8-row groups
-  d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
-  d |= (uint64_t)2 << 61;                          // SWIZZLE_128B
-  return d;
-}
 
 // instruction descriptor: kind::i8, D = s32, A = B = u8, both K-major, M = 128, N = 64
 __host__ __device__ constexpr uint32_t idesc_i8() {
@@ -114,29 +76,6 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
       :
       : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// byte offset of (row, 16-byte chunk) in a 128-byte-swizzled K-major tile
-__device__ __forceinline__ uint32_t swz(int row, int chunk) {
-  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4));
 }
 
 // 4 mask bits -> 4 bytes of 0x00 / 0xFF
@@ -236,15 +175,31 @@ __global__ void __launch_bounds__(kHighWarps * 32) k_ecorr_high(int n, int ermax
   const int per = (n + kHighWarps - 1) / kHighWarps;
   const int i0 = warp * per, i1 = min(n, i0 + per);
   double acc = 0.0;
-  if (b < ermax)
-    for (int i = i0; i < i1; ++i) {
-      const uint32_t ch = counts[(size_t)i * ermax_pad + h];
-      if (ch == 0u) continue;
-      const uint32_t cb = counts[(size_t)i * ermax_pad + b];
-      if (cb == 0u) continue;
-      const double full = (double)cb * (double)ch, low = (double)(cb & 255u) * (double)(ch & 255u);
-      acc += w[i] * (full - low);
+  if (b < ermax) {
+    // branch-free and four insertions deep, so that the loads of a group are in flight together;
+    // c_b c_h - l_b l_h is an exact integer below 2^53, summed in insertion order
+    int i = i0;
+    for (; i + 4 <= i1; i += 4) {
+      uint32_t ch[4], cb[4];
+      double wi[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        ch[u] = counts[(size_t)(i + u) * ermax_pad + h];
+        cb[u] = counts[(size_t)(i + u) * ermax_pad + b];
+        wi[u] = w[i + u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint64_t full = (uint64_t)cb[u] * ch[u], low = (uint64_t)(cb[u] & 255u) * (ch[u] & 255u);
+        acc += wi[u] * (double)(full - low);
+      }
     }
+    for (; i < i1; ++i) {
+      const uint32_t ch = counts[(size_t)i * ermax_pad + h], cb = counts[(size_t)i * ermax_pad + b];
+      const uint64_t full = (uint64_t)cb * ch, low = (uint64_t)(cb & 255u) * (ch & 255u);
+      acc += w[i] * (double)(full - low);
+    }
+  }
   red[warp][lane] = acc;
   __syncthreads();
   if (warp == 0 && b < ermax) {
@@ -551,8 +506,10 @@ struct TmaStage {
   uint8_t a[kTileM * kTileK];              // L tile, 16 KB (1024-B aligned)
   uint8_t b[kTmaGroup][kTileN * kTileK];   // term tiles, 8 KB each
 };
+constexpr int kTilePitch = kTileN + 1;             // doubles per row of the accumulated tile
 struct TmaSmem {
   TmaStage st[kTmaStages];
+  double tile[kTileM * kTilePitch];                 // the tile's FP64 sum over the passes
   uint64_t full[kTmaStages], empty[kTmaStages], done;
   uint32_t tmem_base;
 };
@@ -625,34 +582,74 @@ __global__ void __launch_bounds__(kTmaThreads, 1) k_ecorr_tma(int ermax, int kpa
     if (!ok) break;
     ok = __syncthreads_and(mbar_wait(&S.done, (uint32_t)(pass & 1))) != 0;
     if (!ok) break;
-    // epilogue: warp w owns TMEM lanes 32w..32w+31 = rows i0 + 32w + lane
+    // the pass's terms into the tile: warp w owns TMEM lanes 32w..32w+31 = tile rows
     tc_fence_after();
-    const int row = i0 + warp * 32 + lane;
-    for (int cc = 0; cc < kTileN; cc += 32) {
-      double acc[32];
+    {
+      double* trow = S.tile + (warp * 32 + lane) * kTilePitch;
+      for (int cc = 0; cc < kTileN; cc += 32) {
+        double acc[32];
 #pragma unroll
-      for (int e = 0; e < 32; ++e) acc[e] = 0.0;
-      for (int g = 0; g < G; ++g) {
-        const int term = t0 + g;
-        const int d = (term - 1) >> 1;
-        const double scale = term == 0 ? Q.wmin : ldexp(Q.q, 8 * d + (((term - 1) & 1) ? 0 : 8));
-        uint32_t v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(g * kTileN + cc), v);
+        for (int e = 0; e < 32; ++e) acc[e] = pass == 0 ? 0.0 : trow[cc + e];
+        for (int g = 0; g < G; ++g) {
+          const int term = t0 + g;
+          const int d = (term - 1) >> 1;
+          const double scale = term == 0 ? Q.wmin : ldexp(Q.q, 8 * d + (((term - 1) & 1) ? 0 : 8));
+          uint32_t v[32];
+          tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(g * kTileN + cc), v);
 #pragma unroll
-        for (int e = 0; e < 32; ++e) acc[e] += scale * (double)(int32_t)v[e];
-      }
-      if (row < ermax) {
-#pragma unroll
-        for (int e = 0; e < 32; ++e) {
-          const int col = j0 + cc + e;
-          if (col >= ermax || col < row) continue;
-          ecorr[(size_t)row * ermax + col] += acc[e];
-          if (col > row) ecorr[(size_t)col * ermax + row] += acc[e];
+          for (int e = 0; e < 32; ++e) acc[e] += scale * (double)(int32_t)v[e];
         }
+#pragma unroll
+        for (int e = 0; e < 32; ++e) trow[cc + e] = acc[e];
       }
     }
     tc_fence_before();
     __syncthreads();                             // TMEM free for the next pass
+  }
+  if (ok) {
+    // ecorr += the tile (upper triangle, diagonal once) and its mirror, every element owned by
+    // one thread; eight values loaded before they are added and stored, so the loads overlap.
+    // Upper part: a warp per row in turn, lanes over the columns (256-byte rows).
+    for (int r0 = warp * 8; r0 < kTileM; r0 += 4 * 8) {
+      double cur[8][2];
+      size_t at[8][2];
+      bool on[8][2];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int row = i0 + r0 + u, col = j0 + lane + 32 * h;
+          on[u][h] = row < ermax && col < ermax && col >= row;
+          at[u][h] = (size_t)row * ermax + col;
+          cur[u][h] = on[u][h] ? ecorr[at[u][h]] : 0.0;
+        }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (on[u][h]) ecorr[at[u][h]] = cur[u][h] + S.tile[(r0 + u) * kTilePitch + lane + 32 * h];
+    }
+    // Mirror: a warp per column in turn, lanes over the rows (256-byte column runs of the
+    // row-major matrix): element (col, row) for col > row.
+    for (int c0 = warp * 4; c0 < kTileN; c0 += 4 * 4) {
+      double cur[4][4];
+      size_t at[4][4];
+      bool on[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int rb = 0; rb < 4; ++rb) {
+          const int row = i0 + rb * 32 + lane, col = j0 + c0 + u;
+          on[u][rb] = row < ermax && col < ermax && col > row;
+          at[u][rb] = (size_t)col * ermax + row;
+          cur[u][rb] = on[u][rb] ? ecorr[at[u][rb]] : 0.0;
+        }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int rb = 0; rb < 4; ++rb)
+          if (on[u][rb]) ecorr[at[u][rb]] = cur[u][rb] + S.tile[(rb * 32 + lane) * kTilePitch + c0 + u];
+    }
   }
   if (!ok) {
     if (tid == 0) atomicOr(err, kErrTimeout);

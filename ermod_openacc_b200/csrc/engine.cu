@@ -131,7 +131,7 @@ void free_all(ermod_ctx* c) {
   DeviceState& d = c->d;
   void* ptrs[] = {d.molbeg, d.molspec, d.molq, d.atom_lj, d.atom_q, d.ljene, d.ljlensq, d.slt_lj, d.slt_q,
                   d.slt_mass, d.bfcoord, d.uvcrd, d.spec_off, d.uvsoft, d.escrd, d.posraw, d.slvn, d.spl, d.grd,
-                  d.anchor, d.cellof, d.cellcount, d.cellstart, d.molsorted, d.rmol, d.ins_conf, d.insw_in,
+                  d.grec, d.mrec, d.anchor, d.cellof, d.cellcount, d.cellstart, d.molsorted, d.rmol, d.ins_conf, d.insw_in,
                   d.tgt_raw, d.tgt_n, d.tgt_c, d.tgt_mol, d.selfreal, d.selfrec, d.u0, d.w, d.etot, d.flceng,
                   d.grid, d.spec, d.phin, d.phi, d.engfac, d.engfacT, d.fft_tw, d.fft_twd, d.sitetab, d.sitestn,
                   d.splfc,
@@ -410,8 +410,13 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   *out = ctx;
 
   CK(cudaSetDevice(device));
-  CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
+  {
+    // the PME chain on st comes first; real space on st2 fills the SMs it leaves
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithPriority(&ctx->st, cudaStreamNonBlocking, hi));
+    CK(cudaStreamCreateWithPriority(&ctx->st2, cudaStreamNonBlocking, lo));
+  }
   CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
@@ -426,6 +431,7 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   CK(dalloc(&d.uvcrd, ctx->ermax)); CK(dalloc(&d.spec_off, ctx->numslv + 1)); CK(dalloc(&d.uvsoft, ctx->numslv));
   CK(dalloc(&d.escrd, std::max(1, ctx->esmax)));
   CK(dalloc(&d.posraw, 3 * NA)); CK(dalloc(&d.slvn, NA)); CK(dalloc(&d.spl, NA * 3 * order)); CK(dalloc(&d.grd, NA));
+  if (pme && gather_rec_ok(order, K1, K2, K3)) { CK(dalloc(&d.grec, NA * kRecWords)); CK(dalloc(&d.mrec, SM)); }
   CK(dalloc(&d.anchor, SM)); CK(dalloc(&d.cellof, SM)); CK(dalloc(&d.cellcount, ctx->ncell_cap));
   CK(dalloc(&d.cellstart, ctx->ncell_cap + 1)); CK(dalloc(&d.molsorted, SM)); CK(dalloc(&d.rmol, 1));
   CK(dalloc(&d.ins_conf, 3 * S * MD)); CK(dalloc(&d.insw_in, MD));
@@ -1158,7 +1164,7 @@ static cudaError_t capture_graph(cudaStream_t st, cudaGraphExec_t* exec, Body bo
       *exec = nullptr;
     }
   }
-  if (!*exec) e = cudaGraphInstantiate(exec, graph, 0);
+  if (!*exec) e = cudaGraphInstantiate(exec, graph, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(graph);
   return e;
 }

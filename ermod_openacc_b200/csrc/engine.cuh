@@ -58,11 +58,19 @@ cudaError_t launch_k(bool pdl, dim3 grid, dim3 block, size_t smem, cudaStream_t 
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
+  // the stream's priority as the launch's own, so that a kernel node captured into a graph keeps it
+  int prio = 0;
+  cudaStreamGetPriority(s, &prio);
+  cudaLaunchAttribute at[2];
+  int na = 0;
+  at[na].id = cudaLaunchAttributePriority;
+  at[na++].val.priority = prio;
+  if (pdl) {
+    at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[na++].val.programmaticStreamSerializationAllowed = 1;
+  }
   cfg.attrs = at;
-  cfg.numAttrs = pdl ? 1 : 0;
+  cfg.numAttrs = na;
   return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
 }
 
@@ -73,6 +81,17 @@ cudaError_t raise_smem_limit_fn(const void* kernel, size_t bytes);
 template <class F>
 cudaError_t raise_smem_limit(F* kernel, size_t bytes) {
   return raise_smem_limit_fn((const void*)kernel, bytes);
+}
+
+// Order-4 gather record of one solvent atom, 16 words (64 bytes): the n1 and n2
+// B-spline weights, the atom's charge times the n3 weights (FP32 product), and
+// {float offset of phi(gd.x) of row (gd.z, gd.y), target 0, in the pair layout;
+// flags; gd.x | gd.y << 10 | gd.z << 20; 0}.  kRecWrap: some stencil index wraps.
+constexpr int kRecWords = 16, kRecWrap = 1, kRecOdd = 2;
+// records need the offset in 31 bits and each grid index (0..K) in 10
+__host__ __device__ __forceinline__ bool gather_rec_ok(int order, int K1, int K2, int K3) {
+  return order == 4 && K1 < 1024 && K2 < 1024 && K3 < 1024 &&
+         (double)K3 * K2 * (((K1 + 1) / 2) * 2) * 32 < 2147483647.0;
 }
 
 // Float offset of phi(n1) of grid line `line` (= n3 K2 + n2) and target b in the
@@ -105,6 +124,8 @@ struct DeviceState {
   float4* slvn = nullptr;    // [natoms] normalised x,y,z + charge
   float* spl = nullptr;      // [natoms*3*order]
   int4* grd = nullptr;       // [natoms]
+  float* grec = nullptr;     // [natoms*kRecWords] order-4 gather records, on meshes gather_rec_ok allows
+  int4* mrec = nullptr;      // [slvmax] {molecule, first atom, atoms, charge bits} in cell order
   float4* anchor = nullptr;  // [slvmax] first-site position, w = molecule extent
   int* cellof = nullptr;     // [slvmax]
   int* cellcount = nullptr;  // [ncell_cap]
@@ -211,7 +232,7 @@ void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_de
 // proposal (proposal.cu) and its network (mlp.cu)
 MlpLayout mlp_layout();
 void mlp_forward(const __nv_bfloat16* pw, const float* pf, const float* x, int n, float* act, float* logits,
-                 cudaStream_t s);
+                 int* err, cudaStream_t s);
 int mlp_forward_launches();
 void launch_to_bf16(int n, const float* src, __nv_bfloat16* dst, cudaStream_t s);
 int launch_proposal(const FrameArgs& a, const DeviceState& d, int gv, int gf, float eps, bool learned,

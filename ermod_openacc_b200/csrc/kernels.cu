@@ -18,6 +18,8 @@
 //   k_weights          update_histogram weights and scalar accumulators (engproc.F90:883-915, 939-941)
 //   k_edens            edens += engnmfc * insdst (engproc.F90:943-947)
 //   k_ecorr_simt       ecorr += engnmfc * insdst insdst^T (engproc.F90:948-962), FP64 reference kernel
+#include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cstdio>
 
@@ -32,7 +34,8 @@ namespace erm {
 // solvent preparation
 // ---------------------------------------------------------------------------
 __global__ void k_prepare_solvent(FrameArgs a, const float* __restrict__ posraw, const float* __restrict__ atom_q,
-                                  float4* __restrict__ slvn, float* __restrict__ spl, int4* __restrict__ grd) {
+                                  float4* __restrict__ slvn, float* __restrict__ spl, int4* __restrict__ grd,
+                                  float* __restrict__ grec) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.natoms) return;
   const float x = posraw[3 * i], y = posraw[3 * i + 1], z = posraw[3 * i + 2];
@@ -46,15 +49,27 @@ __global__ void k_prepare_solvent(FrameArgs a, const float* __restrict__ posraw,
     }
     const int K[3] = {a.K1, a.K2, a.K3};
     int gi[3];
+    float wr[3][kMaxOrder];
     for (int m = 0; m < 3; ++m) {
       const float f = inm[m] * (float)K[m];
       const int rci = (int)f;
-      float w[kMaxOrder];
-      spline_weights(f - (float)rci, a.order, w);
-      for (int spi = 0; spi < a.order; ++spi) spl[((size_t)i * 3 + m) * a.order + spi] = w[spi];
+      spline_weights(f - (float)rci, a.order, wr[m]);
+      for (int spi = 0; spi < a.order; ++spi) spl[((size_t)i * 3 + m) * a.order + spi] = wr[m][spi];
       gi[m] = rci;
     }
     grd[i] = make_int4(gi[0], gi[1], gi[2], 0);
+    if (grec) {   // order 4 (gather_rec_ok)
+      const float q = atom_q[i];
+      const bool wrap = !(gi[0] >= 3 && gi[1] >= 3 && gi[2] >= 3 && gi[0] < a.K1 && gi[1] < a.K2 && gi[2] < a.K3);
+      const int P1 = (a.K1 + 1) / 2;
+      const int off = wrap ? 0 : (int)phi_index((size_t)gi[2] * a.K2 + gi[1], gi[0], 0, P1);
+      float4* r = reinterpret_cast<float4*>(grec + (size_t)i * kRecWords);
+      r[0] = make_float4(wr[0][0], wr[0][1], wr[0][2], wr[0][3]);
+      r[1] = make_float4(wr[1][0], wr[1][1], wr[1][2], wr[1][3]);
+      r[2] = make_float4(q * wr[2][0], q * wr[2][1], q * wr[2][2], q * wr[2][3]);
+      r[3] = make_float4(__int_as_float(off), __int_as_float((wrap ? kRecWrap : 0) | ((gi[0] & 1) ? kRecOdd : 0)),
+                         __int_as_float(gi[0] | gi[1] << 10 | gi[2] << 20), 0.f);
+    }
   }
   float nx = x, ny = y, nz = z;
   if (g.periodic) {
@@ -84,7 +99,8 @@ void launch_fill(float* p, float v, int n, cudaStream_t s) {
 
 void launch_prepare_solvent(const FrameArgs& a, const DeviceState& d, cudaStream_t s) {
   if (a.natoms <= 0) return;
-  k_prepare_solvent<<<(a.natoms + 255) / 256, 256, 0, s>>>(a, d.posraw, d.atom_q, d.slvn, d.spl, d.grd);
+  k_prepare_solvent<<<(a.natoms + 255) / 256, 256, 0, s>>>(a, d.posraw, d.atom_q, d.slvn, d.spl, d.grd,
+                                                           a.pme ? d.grec : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -160,6 +176,15 @@ __global__ void k_iota(int n, int* __restrict__ out) {
   if (k < n) out[k] = k;
 }
 
+// the gather's molecule records in cell order: {molecule, first atom, atoms, charge bits}
+__global__ void k_mol_records(int slvmax, const int* __restrict__ molsorted, const int* __restrict__ molbeg,
+                              const float* __restrict__ molq, int4* __restrict__ mrec) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= slvmax) return;
+  const int k = molsorted[m];
+  mrec[m] = make_int4(k, molbeg[k], molbeg[k + 1] - molbeg[k], __float_as_int(molq[k]));
+}
+
 void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStream_t s) {
   if (a.slvmax <= 0) return;
   cudaMemsetAsync(d.rmol, 0, sizeof(float), s);
@@ -171,6 +196,8 @@ void launch_cells(const FrameArgs& a, const DeviceState& d, int ncell, cudaStrea
   } else {
     k_iota<<<(a.slvmax + 255) / 256, 256, 0, s>>>(a.slvmax, d.molsorted);
   }
+  if (a.pme && d.mrec)
+    k_mol_records<<<(a.slvmax + 255) / 256, 256, 0, s>>>(a.slvmax, d.molsorted, d.molbeg, d.molq, d.mrec);
 }
 
 // ---------------------------------------------------------------------------
@@ -890,14 +917,12 @@ void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int
   if (nb <= 0) return;  // `chunk` is the row stride of E: the batch size
   if (threads <= 0 || threads > kRealMaxThreads || threads % 32) threads = 256;
   const size_t sm = real_smem(a);
-  if (a.nsite > kRealWideSites)
-    k_real<true><<<nb, threads, sm, s>>>(a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, d.slt_lj, d.molbeg, d.slvn,
-                                          d.atom_lj, d.ljene, d.ljlensq, d.anchor, d.cellstart, d.molsorted, d.rmol,
-                                          d.E);
-  else
-    k_real<false><<<nb, threads, sm, s>>>(a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, d.slt_lj, d.molbeg, d.slvn,
-                                           d.atom_lj, d.ljene, d.ljlensq, d.anchor, d.cellstart, d.molsorted, d.rmol,
-                                           d.E);
+  // launch_k: a graph node of this launch keeps the stream's (lower) priority beside the PME chain
+#define ERM_REAL(W) launch_k(false, nb, threads, sm, s, k_real<W>, a, base, chunk, d.tgt_n, d.tgt_c, d.tgt_mol, \
+      d.slt_lj, d.molbeg, d.slvn, d.atom_lj, d.ljene, d.ljlensq, d.anchor, d.cellstart, d.molsorted, d.rmol, d.E)
+  if (a.nsite > kRealWideSites) ERM_REAL(true);
+  else ERM_REAL(false);
+#undef ERM_REAL
 }
 
 // ---------------------------------------------------------------------------
@@ -1240,6 +1265,7 @@ void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb
 // beside the whole PME chain.
 // ---------------------------------------------------------------------------
 constexpr int kGatherThreads = 256;
+constexpr int kMaxDevices = 64;     // per-device caches of launch shapes
 
 // The order-4 stencil rows of CS planes c3 (from c30) of one site, no wrap: v[(cs * 4 + c2) * 4 + c1]
 // = phi(gd.x - c1) of row (gd.z - c30 - cs, gd.y - c2).  p0 points at phi(gd.x) of the site's row;
@@ -1381,9 +1407,116 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
   }
 }
 
+// The order-4 gather from per-atom records (k_prepare_solvent) and per-molecule records in
+// cell order (k_mol_records): the same stencil sums as k_gather<4>, in the same order, with
+// fewer dependent loads.  A warp's first molecule record and the records of its first two
+// atoms are fetched before the wait on the k1 transform (they are frame tables, complete
+// before the chunk chain starts); lanes 0-15 hold one atom's record, lanes 16-31 the next
+// one's, and every record is broadcast from there by shuffles.  The records of the next
+// two atoms (or of the next molecule's first two) are in flight while the current ones'
+// stencils are summed.
+// LK1, LK2 > 0: the mesh's K1 = 2^LK1, K2 = 2^LK2 at compile time, so that every stencil row
+// is the site's base pointer plus a constant offset; 0: taken from FrameArgs.
+template <int LK1, int LK2>
+__global__ void __launch_bounds__(kGatherThreads, 2) k_gather_rec(FrameArgs a, int base, int bb, int nb,
+    const int4* __restrict__ mrec, const float* __restrict__ grec, const float* __restrict__ phi,
+    const double* __restrict__ tgtq, const int* __restrict__ tgt_mol, double* __restrict__ Etot) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwt = (gridDim.x * blockDim.x) >> 5;
+  const int b = lane;
+  const bool active = b < nb;
+  const int cnt = base + b, bi = cnt - bb;
+  const double qslt = active ? tgtq[cnt] : 0.0;
+  const int excl = (active && tgt_mol) ? tgt_mol[cnt] : -1;
+  const int K1 = LK1 ? 1 << LK1 : a.K1, K2 = LK2 ? 1 << LK2 : a.K2, K3 = a.K3, P1 = (K1 + 1) / 2;
+  const size_t s2 = (size_t)P1 * kChunk * 2, s3 = (size_t)K2 * s2;   // floats per n2 row, n3 plane
+  const int half = lane >> 4, word = lane & 15;
+  int m = gw;
+  int4 mr = m < a.slvmax ? mrec[m] : make_int4(0, 0, 0, 0);
+  float rv = half < mr.z ? grec[(size_t)(mr.y + half) * kRecWords + word] : 0.f;
+  grid_dep_wait();                                    // the potential grid of this chunk is complete
+  grid_dep_launch();                                  // the next chunk's planes may start filling the tail
+  while (m < a.slvmax) {
+    const int mn = m + nwt;
+    const int4 mrn = mn < a.slvmax ? mrec[mn] : make_int4(0, 0, 0, 0);
+    double e = 0.0;
+    if (mr.z <= 0) rv = half < mrn.z ? grec[(size_t)(mrn.y + half) * kRecWords + word] : 0.f;
+    for (int p = 0; p < mr.z; p += 2) {
+      // the records after this pair: atoms p + 2, p + 3, or the next molecule's first two
+      float nxt;
+      if (p + 2 < mr.z) nxt = p + 2 + half < mr.z ? grec[(size_t)(mr.y + p + 2 + half) * kRecWords + word] : 0.f;
+      else nxt = half < mrn.z ? grec[(size_t)(mrn.y + half) * kRecWords + word] : 0.f;
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        if (p + h >= mr.z) break;
+        const int src = h * 16;
+        float wl[12];
+#pragma unroll
+        for (int c = 0; c < 12; ++c) wl[c] = __shfl_sync(0xffffffffu, rv, src + c);
+        const int off = __float_as_int(__shfl_sync(0xffffffffu, rv, src + 12));
+        const int flags = __float_as_int(__shfl_sync(0xffffffffu, rv, src + 13));
+        float v[64];
+        if (!(flags & kRecWrap)) {
+          const float* p0 = phi + (size_t)off + 2 * b;
+          if (flags & kRecOdd) gather_rows4<4, true>(p0, s2, s3, 0, v);
+          else gather_rows4<4, false>(p0, s2, s3, 0, v);
+        } else {
+          const int gp = __float_as_int(__shfl_sync(0xffffffffu, rv, src + 14));
+          const int gx = gp & 1023, gy = (gp >> 10) & 1023, gz = gp >> 20;
+          int r1[4];
+#pragma unroll
+          for (int c1 = 0; c1 < 4; ++c1) r1[c1] = (int)phi_index(0, wrapk(gx - c1, K1), b, P1);
+#pragma unroll
+          for (int cs = 0; cs < 4; ++cs) {
+            const int r3 = wrapk(gz - cs, K3);
+#pragma unroll
+            for (int c2 = 0; c2 < 4; ++c2) {
+              const float* rowp = phi + phi_index((size_t)r3 * K2 + wrapk(gy - c2, K2), 0, 0, P1);
+#pragma unroll
+              for (int c1 = 0; c1 < 4; ++c1) v[(cs * 4 + c2) * 4 + c1] = rowp[r1[c1]];
+            }
+          }
+        }
+        // wl[8 + c3] is q w3(c3), formed in FP32 as k_gather<4> forms it; times 1.0f it stays exact
+        accumulate_planes<4, 4>(v, wl, 0, 1.0f, e);
+      }
+      rv = nxt;
+    }
+    e -= a.pivol * qslt * (double)__int_as_float(mr.w);
+    if (active) Etot[(size_t)bi * a.slvmax + mr.x] = (mr.x == excl) ? 0.0 : e;
+    mr = mrn;
+    m = mn;
+  }
+}
+
 void launch_gather(const FrameArgs& a, const DeviceState& d, int base, int bb, int nb, int chunk, int batch,
                    bool pdl, cudaStream_t s) {
   int blocks = (a.slvmax * 32 + kGatherThreads - 1) / kGatherThreads;
+  if (a.pme && a.order == 4 && d.grec) {
+    // no more CTAs than are resident at once: every warp fetches its first records early
+    static std::atomic<int> resident[kMaxDevices];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int cap = dev >= 0 && dev < kMaxDevices ? resident[dev].load() : 0;
+    if (cap == 0) {
+      int per_sm = 0, sms = 0;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_rec<0, 0>, kGatherThreads, 0);
+      cap = std::max(1, per_sm * sms);
+      if (dev >= 0 && dev < kMaxDevices) resident[dev].store(cap);
+    }
+    blocks = std::max(1, std::min(blocks, cap));
+#define ERM_GATHER_REC(L1, L2) launch_k(pdl, blocks, kGatherThreads, 0, s, k_gather_rec<L1, L2>, a, base, bb, nb, \
+      (const int4*)d.mrec, (const float*)d.grec, (const float*)d.phi, (const double*)d.tgtq, (const int*)d.tgt_mol, \
+      d.Etot)
+    if (a.K1 == 64 && a.K2 == 64) ERM_GATHER_REC(6, 6);
+    else if (a.K1 == 32 && a.K2 == 32) ERM_GATHER_REC(5, 5);
+    else if (a.K1 == 128 && a.K2 == 128) ERM_GATHER_REC(7, 7);
+    else ERM_GATHER_REC(0, 0);
+#undef ERM_GATHER_REC
+    return;
+  }
   if (blocks > 148 * 8) blocks = 148 * 8;
   if (blocks < 1) blocks = 1;
 #define ERM_GATHER(NO) launch_k(pdl, blocks, kGatherThreads, 0, s, k_gather<NO>, a, base, bb, nb, chunk, batch, \

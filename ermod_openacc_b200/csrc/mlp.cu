@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "engine.cuh"
+#include "tc_sm100.cuh"
 
 namespace erm {
 
@@ -146,6 +147,196 @@ __global__ void k_adam(int n, float lr, float b1, float b2, float eps, float c1,
   wb[i] = __float2bfloat16_rn(w[i]);
 }
 
+// ---- the forward pass on the tensor cores (tcgen05, kind::tf32) -----------
+// One CTA per 128 samples, 128 threads.  The three hidden layers are 128 x 128 x K
+// MMAs (K = 64, 128, 128) with the samples on the M side: A = the layer's input
+// rows, B = the weight matrix [out][in], both K-major in 128-byte-swizzled shared
+// memory (32 TF32 per 128-byte row, one 16 KB atom per 32 of K).  The BF16 weights
+// are exact in TF32; the inputs are rounded to TF32 (nearest, ties away) as they
+// are staged.  The FP32 accumulator (TMEM, 128 lanes x 128 columns) gets the FP32
+// bias and the ReLU in the epilogue, which stores the activation in FP32 (the
+// backward pass reads it) and stages it, rounded, as the next layer's A.  The
+// output layer is a 128-term FP32 dot product per sample, in column order.  Every
+// mbarrier wait has an iteration limit; on expiry the kernel sets *err and skips.
+constexpr int kFwdRows = 128;
+constexpr int kFwdAtoms = kMlpHidden / 32;            // K atoms of a 128-wide input
+
+struct FwdSmem {
+  uint32_t a[kFwdAtoms][kFwdRows * 32];               // layer input, TF32 bits, 4 x 16 KB
+  uint32_t b[kFwdAtoms][kMlpHidden * 32];             // weights, TF32 bits, 4 x 16 KB
+  uint64_t bar;
+  uint32_t tmem_base;
+};
+constexpr size_t kFwdSmemBytes = sizeof(FwdSmem) + 1024;
+
+// instruction descriptor: kind::tf32, D = F32, A = B = TF32, both K-major, M = 128, N = 128
+__host__ __device__ constexpr uint32_t idesc_tf32() {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kMlpHidden >> 3) << 17) | ((uint32_t)(kFwdRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  const uint32_t idesc = idesc_tf32();
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// element (row, k) of a K-major swizzled operand of `atoms` x 16 KB: 32 TF32 per atom row
+__device__ __forceinline__ uint32_t* tf32_slot(uint32_t (*op)[kFwdRows * 32], int row, int k) {
+  const int atom = k >> 5, kk = k & 31;
+  return (uint32_t*)((unsigned char*)op[atom] + tc::swz(row, kk >> 2)) + (kk & 3);
+}
+
+// Operand staging with 16-byte loads, kStageBatch in flight per thread: x rows (FP32, 4 per
+// load) and weight rows (BF16, 8 per load) into the swizzled TF32 layout; every group of four
+// consecutive k lands in one 16-byte chunk of a row.  Unaligned sources take the scalar loop.
+constexpr int kStageBatch = 16;
+
+__device__ __forceinline__ void stage_x(uint32_t (*a)[kFwdRows * 32], const float* __restrict__ x, int r0, int n,
+                                        int tid) {
+  constexpr int Q = kMlpIn / 4, TOT = kFwdRows * Q;            // float4 per row, per tile
+  if (((uintptr_t)x & 15) == 0) {
+#pragma unroll 1
+    for (int e0 = 0; e0 < TOT; e0 += kStageBatch * kFwdRows) {
+      float4 v[kStageBatch];
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int e = e0 + u * kFwdRows + tid, row = e / Q;
+        v[u] = (e < TOT && r0 + row < n) ? __ldg((const float4*)(x + (size_t)(r0 + row) * kMlpIn) + (e - row * Q))
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int e = e0 + u * kFwdRows + tid, row = e / Q;
+        if (e < TOT)
+          *(uint4*)tf32_slot(a, row, (e - row * Q) * 4) =
+              make_uint4(to_tf32(v[u].x), to_tf32(v[u].y), to_tf32(v[u].z), to_tf32(v[u].w));
+      }
+    }
+  } else {
+    for (int e = tid; e < kFwdRows * kMlpIn; e += kFwdRows) {
+      const int row = e / kMlpIn, k = e - row * kMlpIn;
+      const float v = (r0 + row < n) ? x[(size_t)(r0 + row) * kMlpIn + k] : 0.f;
+      *tf32_slot(a, row, k) = to_tf32(v);
+    }
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void stage_w(uint32_t (*b)[kMlpHidden * 32], const __nv_bfloat16* __restrict__ w, int tid) {
+  constexpr int Q = K / 8, TOT = kMlpHidden * Q;               // 16-byte groups per row, per matrix
+  if (((uintptr_t)w & 15) == 0) {
+#pragma unroll 1
+    for (int e0 = 0; e0 < TOT; e0 += kStageBatch * kFwdRows) {
+      uint4 v[kStageBatch];
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int e = e0 + u * kFwdRows + tid;
+        v[u] = e < TOT ? __ldg((const uint4*)w + e) : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int e = e0 + u * kFwdRows + tid, o = e / Q, k = (e - o * Q) * 8;
+        if (e < TOT) {
+          // a BF16 is the high half of its FP32 (and TF32) pattern
+          const uint32_t p[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+          *(uint4*)tf32_slot(b, o, k) = make_uint4(p[0] << 16, p[0] & 0xffff0000u, p[1] << 16, p[1] & 0xffff0000u);
+          *(uint4*)tf32_slot(b, o, k + 4) = make_uint4(p[2] << 16, p[2] & 0xffff0000u, p[3] << 16, p[3] & 0xffff0000u);
+        }
+      }
+    }
+  } else {
+    for (int e = tid; e < kMlpHidden * K; e += kFwdRows) {
+      const int o = e / K, k = e - o * K;
+      *tf32_slot(b, o, k) = __float_as_uint(__bfloat162float(w[e]));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kFwdRows, 1) k_mlp_fwd_tc(const __nv_bfloat16* __restrict__ pw,
+    const float* __restrict__ pf, const float* __restrict__ x, int n, float* __restrict__ act,
+    float* __restrict__ logits, int* __restrict__ err, MlpLayout L) {
+  using namespace tc;
+  extern __shared__ __align__(1024) unsigned char fsm_raw[];
+  FwdSmem& S = *reinterpret_cast<FwdSmem*>((void*)(((uintptr_t)fsm_raw + 1023) & ~(uintptr_t)1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = blockIdx.x * kFwdRows;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
+                 "r"(kMlpHidden));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    mbar_init(&S.bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // layer 1 input: x rows, rounded to TF32 (rows past n are zero)
+  stage_x(S.a, x, r0, n, tid);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem_base;
+  bool ok = true;
+  const int row = r0 + warp * 32 + lane;              // this thread's sample (TMEM lane)
+  float out = 0.f;
+  const int woff[3] = {L.w1, L.w2, L.w3}, boff[3] = {L.b1, L.b2, L.b3}, kin[3] = {kMlpIn, kMlpHidden, kMlpHidden};
+  for (int layer = 0; layer < 3; ++layer) {
+    const int K = kin[layer];
+    // weights [out][K] (BF16, exact in TF32) as the B operand
+    if (K == kMlpIn) stage_w<kMlpIn>(S.b, pw + woff[layer], tid);
+    else stage_w<kMlpHidden>(S.b, pw + woff[layer], tid);
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      for (int atom = 0; atom < K / 32; ++atom) {
+        const uint64_t da = smem_desc(smem_u32(S.a[atom])), db = smem_desc(smem_u32(S.b[atom]));
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks)   // K = 8 TF32 (32 bytes) per MMA
+          mma_tf32(tmem, da + (uint64_t)(ks * 2), db + (uint64_t)(ks * 2), (atom > 0 || ks > 0) ? 1u : 0u);
+      }
+      mma_commit(&S.bar);
+    }
+    const bool done = mbar_wait(&S.bar, (uint32_t)(layer & 1));
+    ok = __syncthreads_and(done && ok) != 0;
+    if (!ok) break;
+    tc_fence_after();
+    float* h = act ? act + (size_t)layer * n * kMlpHidden : nullptr;
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+      for (int e = 0; e < 32; ++e) {
+        const int col = c0 + e;
+        const float z = fmaxf(__uint_as_float(v[e]) + pf[boff[layer] + col], 0.f);
+        if (act && row < n) h[(size_t)row * kMlpHidden + col] = z;
+        if (layer < 2) *tf32_slot(S.a, warp * 32 + lane, col) = to_tf32(z);
+        else out = fmaf(z, __bfloat162float(pw[L.w4 + col]), out);
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  if (ok && row < n) logits[row] = out + pf[L.b4];
+  if (!ok) {
+    if (tid == 0 && err) atomicOr(err, kErrTimeout);
+    mbar_wait(&S.bar, 0u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMlpHidden));
+}
+
 }  // namespace
 
 // ---- shared by the engine: inference over the voxels of a frame ----------
@@ -165,23 +356,18 @@ MlpLayout mlp_layout() {
 }
 
 // Biases stay FP32 (the FP32 copy of the parameters is passed as `pf`); the
-// weight matrices are read as BF16.  act: [3][n][128] scratch; logits: [n].
+// weight matrices are read as BF16.  act: [3][n][128] hidden activations for the
+// backward pass, or NULL (inference); logits: [n].  err (device, may be NULL):
+// kErrTimeout is or-ed in if a tensor-core wait gave up.
 void mlp_forward(const __nv_bfloat16* pw, const float* pf, const float* x, int n, float* act, float* logits,
-                 cudaStream_t s) {
-  const MlpLayout L = mlp_layout();
-  float* h1 = act;
-  float* h2 = act + (size_t)n * kMlpHidden;
-  float* h3 = h2 + (size_t)n * kMlpHidden;
-  gemm(n, kMlpHidden, kMlpIn, x, kMlpIn, 1, pw + L.w1, 1, kMlpIn, h1, kMlpHidden, pf + L.b1, 1,
-       (const float*)nullptr, 0, s);
-  gemm(n, kMlpHidden, kMlpHidden, h1, kMlpHidden, 1, pw + L.w2, 1, kMlpHidden, h2, kMlpHidden, pf + L.b2, 1,
-       (const float*)nullptr, 0, s);
-  gemm(n, kMlpHidden, kMlpHidden, h2, kMlpHidden, 1, pw + L.w3, 1, kMlpHidden, h3, kMlpHidden, pf + L.b3, 1,
-       (const float*)nullptr, 0, s);
-  gemm(n, 1, kMlpHidden, h3, kMlpHidden, 1, pw + L.w4, 1, 1, logits, 1, pf + L.b4, 0, (const float*)nullptr, 0, s);
+                 int* err, cudaStream_t s) {
+  if (n <= 0) return;
+  raise_smem_limit(k_mlp_fwd_tc, kFwdSmemBytes);
+  k_mlp_fwd_tc<<<(n + kFwdRows - 1) / kFwdRows, kFwdRows, kFwdSmemBytes, s>>>(pw, pf, x, n, act, logits, err,
+                                                                             mlp_layout());
 }
 
-int mlp_forward_launches() { return 4; }
+int mlp_forward_launches() { return 1; }
 
 }  // namespace erm
 
@@ -197,13 +383,25 @@ struct ermod_mlp {
   float *x = nullptr, *y = nullptr, *act = nullptr, *s = nullptr, *gs = nullptr, *l = nullptr;
   float *d3 = nullptr, *d2 = nullptr, *d1 = nullptr;
   double* loss = nullptr;
+  int* dev_err = nullptr;        // set by the tensor-core forward if a wait gave up
   long long t = 0;
   std::string err;
 };
 
 namespace {
+// the tensor-core forward's error word, read (and cleared) after the stream is synchronised
+int take_dev_err(ermod_mlp* p) {
+  int e = 0;
+  if (cudaMemcpy(&e, p->dev_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return ERMOD_ERR_CUDA;
+  if (e == 0) return ERMOD_OK;
+  cudaMemset(p->dev_err, 0, sizeof(int));
+  p->err = "tc_wait";
+  return ERMOD_ERR_CUDA;
+}
+
 void mlp_free(ermod_mlp* p) {
-  void* ptrs[] = {p->w, p->m, p->v, p->g, p->wb, p->x, p->y, p->act, p->s, p->gs, p->l, p->d3, p->d2, p->d1, p->loss};
+  void* ptrs[] = {p->w, p->m, p->v, p->g, p->wb, p->x, p->y, p->act, p->s, p->gs, p->l, p->d3, p->d2, p->d1, p->loss,
+                  p->dev_err};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->st) cudaStreamDestroy(p->st);
@@ -223,7 +421,7 @@ void backward(ermod_mlp* p, int n) {
   const MlpLayout L = mlp_layout();
   cudaStream_t s = p->st;
   const __nv_bfloat16* wb = p->wb;
-  mlp_forward(wb, p->w, p->x, n, p->act, p->s, s);
+  mlp_forward(wb, p->w, p->x, n, p->act, p->s, p->dev_err, s);
   float* h1 = p->act;
   float* h2 = p->act + (size_t)n * kMlpHidden;
   float* h3 = h2 + (size_t)n * kMlpHidden;
@@ -267,11 +465,12 @@ int32_t ermod_mlp_create(ermod_mlp** out, int32_t device, int32_t max_batch, con
             A(&p->wb, np) == 0 && A(&p->x, B * kMlpIn) == 0 && A(&p->y, B) == 0 &&
             A(&p->act, 3 * B * kMlpHidden) == 0 && A(&p->s, B) == 0 && A(&p->gs, B) == 0 && A(&p->l, B) == 0 &&
             A(&p->d3, B * kMlpHidden) == 0 && A(&p->d2, B * kMlpHidden) == 0 && A(&p->d1, B * kMlpHidden) == 0 &&
-            A(&p->loss, 1) == 0;
+            A(&p->loss, 1) == 0 && A(&p->dev_err, 1) == 0;
   if (ok) {
     ok = cudaMemcpyAsync(p->w, init_params, sizeof(float) * np, cudaMemcpyHostToDevice, p->st) == cudaSuccess &&
          cudaMemsetAsync(p->m, 0, sizeof(float) * np, p->st) == cudaSuccess &&
-         cudaMemsetAsync(p->v, 0, sizeof(float) * np, p->st) == cudaSuccess;
+         cudaMemsetAsync(p->v, 0, sizeof(float) * np, p->st) == cudaSuccess &&
+         cudaMemsetAsync(p->dev_err, 0, sizeof(int), p->st) == cudaSuccess;
     k_to_bf16<<<(np + 255) / 256, 256, 0, p->st>>>(np, p->w, p->wb);
     ok = ok && cudaStreamSynchronize(p->st) == cudaSuccess && cudaGetLastError() == cudaSuccess;
   }
@@ -292,9 +491,21 @@ int32_t ermod_mlp_forward(ermod_mlp* p, const float* x, int32_t n, float* logits
   if (cudaSetDevice(p->device) != cudaSuccess) return ERMOD_ERR_CUDA;
   int rc = stage(p, x, nullptr, n);
   if (rc != ERMOD_OK) return rc;
-  mlp_forward(p->wb, p->w, p->x, n, p->act, p->s, p->st);
+  mlp_forward(p->wb, p->w, p->x, n, p->act, p->s, p->dev_err, p->st);
   if (cudaMemcpyAsync(logits, p->s, sizeof(float) * n, cudaMemcpyDeviceToHost, p->st) != cudaSuccess ||
       cudaStreamSynchronize(p->st) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+    return ERMOD_ERR_CUDA;
+  return take_dev_err(p);
+}
+
+// the hidden activations [3][n][128] (FP32, after bias and ReLU) of the last
+// forward or gradient pass over n samples
+int32_t ermod_mlp_activations(ermod_mlp* p, int32_t n, float* act) {
+  if (!p || !act || n <= 0 || n > p->max_batch) return ERMOD_ERR_ARG;
+  if (cudaSetDevice(p->device) != cudaSuccess) return ERMOD_ERR_CUDA;
+  if (cudaMemcpyAsync(act, p->act, sizeof(float) * 3 * (size_t)n * kMlpHidden, cudaMemcpyDeviceToHost, p->st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(p->st) != cudaSuccess)
     return ERMOD_ERR_CUDA;
   return ERMOD_OK;
 }
@@ -311,6 +522,7 @@ int32_t ermod_mlp_gradients(ermod_mlp* p, const float* x, const float* y, int32_
   if (loss && cudaMemcpyAsync(loss, p->loss, sizeof(double), cudaMemcpyDeviceToHost, p->st) != cudaSuccess)
     return ERMOD_ERR_CUDA;
   if (cudaStreamSynchronize(p->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ERMOD_ERR_CUDA;
+  if (take_dev_err(p) != ERMOD_OK) return ERMOD_ERR_CUDA;
   return ERMOD_OK;
 }
 
@@ -329,6 +541,7 @@ int32_t ermod_mlp_train_step(ermod_mlp* p, const float* x, const float* y, int32
   if (loss && cudaMemcpyAsync(loss, p->loss, sizeof(double), cudaMemcpyDeviceToHost, p->st) != cudaSuccess)
     return ERMOD_ERR_CUDA;
   if (cudaStreamSynchronize(p->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ERMOD_ERR_CUDA;
+  if (take_dev_err(p) != ERMOD_OK) return ERMOD_ERR_CUDA;
   return ERMOD_OK;
 }
 

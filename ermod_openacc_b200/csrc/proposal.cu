@@ -145,7 +145,7 @@ int launch_proposal(const FrameArgs& a, const DeviceState& d, int gv, int gf, fl
   k_features<<<(V * kMlpIn + 255) / 256, 256, 0, s>>>(gv, gf, (float)mean, inv_sd, d.dens, d.feat);
   ++nl;
   if (learned) {
-    mlp_forward(d.mlp_b, d.mlp_f, d.feat, V, d.vact, d.vlogit, s);
+    mlp_forward(d.mlp_b, d.mlp_f, d.feat, V, nullptr, d.vlogit, &d.status->flags, s);
     k_prop_cdf<<<1, kCdfThreads, 0, s>>>(V, (double)eps, d.vlogit, d.vcdf, d.vq);
     nl += mlp_forward_launches() + 1;
   }

@@ -85,6 +85,14 @@ class Trainer:
             out[i:i + len(xb)] = ob
         return out
 
+    def activations(self, n: int) -> np.ndarray:
+        """The hidden activations [3][n][128] of the last forward or gradient pass (n samples)."""
+        a = np.zeros((3, n, 128), dtype=np.float32)
+        rc = self.lib.ermod_mlp_activations(self.h, n, A.ptr(a, C.c_float))
+        if rc != 0:
+            raise ErmodError(rc, "mlp_activations")
+        return a
+
     def gradients(self, x: np.ndarray, y: np.ndarray):
         x = np.ascontiguousarray(x, dtype=np.float32)
         y = np.ascontiguousarray(y, dtype=np.float32)

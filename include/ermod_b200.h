@@ -370,6 +370,9 @@ typedef struct ermod_mlp ermod_mlp;
 int32_t ermod_mlp_create(ermod_mlp** out, int32_t device, int32_t max_batch, const float* init_params);
 int32_t ermod_mlp_nparams(void);
 int32_t ermod_mlp_forward(ermod_mlp* m, const float* x, int32_t n, float* logits);
+/* The hidden activations act[3][n][128] (after bias and ReLU, FP32) of the last
+ * forward or gradient pass, which ran over n samples. */
+int32_t ermod_mlp_activations(ermod_mlp* m, int32_t n, float* act);
 int32_t ermod_mlp_gradients(ermod_mlp* m, const float* x, const float* y, int32_t n, float* grad, double* loss);
 int32_t ermod_mlp_train_step(ermod_mlp* m, const float* x, const float* y, int32_t n, float lr, double* loss);
 int32_t ermod_mlp_get_params(ermod_mlp* m, float* params);

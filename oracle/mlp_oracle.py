@@ -33,6 +33,14 @@ def bf16_round(x):
     return r.astype(np.uint32).view(np.float32)
 
 
+def tf32_round(x):
+    """FP32 -> TF32 (10-bit mantissa) -> FP32, round to nearest with ties away from zero, as the
+    device's cvt.rna.tf32.f32 stages the hidden layers' inputs for the tensor cores."""
+    u = np.asarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x1000) >> 13) << 13
+    return r.astype(np.uint32).view(np.float32)
+
+
 def unpack(p, round_weights=True):
     L = layout()
     get = lambda k: np.asarray(p[L[k][0]:L[k][0] + L[k][1]])
@@ -46,21 +54,36 @@ def unpack(p, round_weights=True):
     return W1, rb(get("b1")), W2, rb(get("b2")), W3, rb(get("b3")), w4, float(rb(get("b4"))[0])
 
 
-def forward(p, x, round_weights=True):
+def forward(p, x, round_weights=True, tf32_inputs=False):
+    """Logits and the activations (x, h1, h2, h3).  tf32_inputs: each hidden layer's input is
+    rounded to TF32 before its product, as the device's tensor-core forward stages it (the
+    activations returned, which the backward pass uses, stay unrounded)."""
     W1, b1, W2, b2, W3, b3, w4, b4 = unpack(p, round_weights)
     x = np.asarray(x, dtype=np.float64)
-    h1 = np.maximum(x @ W1.T + b1, 0.0)
-    h2 = np.maximum(h1 @ W2.T + b2, 0.0)
-    h3 = np.maximum(h2 @ W3.T + b3, 0.0)
+    t = (lambda a: tf32_round(a).astype(np.float64)) if tf32_inputs else (lambda a: a)
+    h1 = np.maximum(t(x) @ W1.T + b1, 0.0)
+    h1 = h1.astype(np.float32).astype(np.float64) if tf32_inputs else h1
+    h2 = np.maximum(t(h1) @ W2.T + b2, 0.0)
+    h2 = h2.astype(np.float32).astype(np.float64) if tf32_inputs else h2
+    h3 = np.maximum(t(h2) @ W3.T + b3, 0.0)
     s = h3 @ w4 + b4
     return s, (x, h1, h2, h3)
 
 
-def loss_and_grad(p, x, y, round_weights=True):
+def loss_and_grad(p, x, y, round_weights=True, tf32_inputs=False, acts=None):
     """Mean BCE-with-logits loss and its gradient w.r.t. the parameter vector
-    (w.r.t. the weights as used, i.e. after BF16 rounding)."""
+    (w.r.t. the weights as used, i.e. after BF16 rounding; the TF32 rounding of the
+    forward's inputs, when asked, is passed straight through).  acts: given hidden
+    activations (h1, h2, h3) to differentiate at instead of this module's own forward
+    pass -- the device's, so that a TF32 rounding that falls the other way on one
+    side of a rounding boundary does not count as a backward-pass error."""
     W1, b1, W2, b2, W3, b3, w4, b4 = unpack(p, round_weights)
-    s, (x, h1, h2, h3) = forward(p, x, round_weights)
+    if acts is None:
+        s, (x, h1, h2, h3) = forward(p, x, round_weights, tf32_inputs)
+    else:
+        x = np.asarray(x, dtype=np.float64)
+        h1, h2, h3 = (np.asarray(a, dtype=np.float64) for a in acts)
+        s = h3 @ w4 + b4
     y = np.asarray(y, dtype=np.float64)
     n = len(s)
     loss = np.mean(np.logaddexp(0.0, s) - y * s)
