@@ -191,7 +191,8 @@ def path_bytes_per_unit(w, natoms: int, slvmax: int, ermax: int, maxdst: int, ns
 
 def profile_table(name: str):
     """{kernel: {column: value}} from a whitespace table under profiles/ ('#' lines are comments,
-    the first other line names the columns); {} when the file is absent."""
+    the first other line names the columns, '-' marks a value not captured); {} when the file
+    is absent."""
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return {}
@@ -203,7 +204,7 @@ def profile_table(name: str):
         if cols is None:
             cols = f
             continue
-        rows[f[0]] = {c: float(v) for c, v in zip(cols[1:], f[1:])}
+        rows[f[0]] = {c: float(v) for c, v in zip(cols[1:], f[1:]) if v != "-"}
     return rows
 
 
@@ -389,10 +390,11 @@ def main():
     chunk = 32
     nbatch = -(-eng.maxdst // 4096)
     per_batch = ("real", "bin", "ecorr", "site_tables")
-    kname = {"gather": "k_gather", "bin": "k_bin", "real": "k_real", "spread": "k_spread_box",
-             "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane",
+    order4 = w.params["splodr"] == 4 and max(w.params["ms1max"], w.params["ms2max"], w.params["ms3max"]) < 1024
+    kname = {"gather": "k_gather_rec" if order4 else "k_gather", "bin": "k_bin", "real": "k_real",
+             "spread": "k_spread_box", "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane",
              "pme_rows": "k_pme_lines" if w.params["ms1max"] <= 64 else "k_pme_rows",
-             "site_tables": "k_site_tables", "influence": "k_influence", "ecorr": "k_ecorr_tc"}
+             "site_tables": "k_site_tables", "influence": "k_influence", "ecorr": "k_ecorr_tma"}
     counters = profile_table("kernel_counters.txt")
     kernels = {}
     for k, kn in kname.items():

@@ -33,7 +33,9 @@ def test_roofline_helpers():
     assert bench.bound_from_counters({"issue_active": 0.65, "fma_pipe": 0.44}) == "sm-issue"
     assert bench.bound_from_counters({"issue_active": 0.3, "dram_frac": 0.1}) == "latency"
     assert bench.bound_from_counters({"issue_active": 0.36, "stall_mio": 4.4}) == "mio-queue"
-    assert set(bench.profile_table("kernel_counters.txt")) >= {"k_pme_plane", "k_pme_lines", "k_gather"}
+    table = bench.profile_table("kernel_counters.txt")
+    assert set(table) >= {"k_pme_plane", "k_pme_lines", "k_gather_rec", "k_ecorr_tma"}
+    assert "fma_pipe" not in table["k_mlp_fwd_tc"]                   # '-': not captured
     w = S.make_workload(2)
     assert 1000.0 < bench.path_bytes_per_unit(w, 12288, 4096, 1396, 2000, 12) < 1100.0
     for stage in ("gather", "bin", "pme_plane", "site_tables"):
