@@ -154,10 +154,10 @@ def kernel_bytes(stage: str, w, chunk: int, natoms: int, slvmax: int, ermax: int
     a1 = float(np.linalg.norm(np.asarray(w.frame(0)[1], dtype=np.float64).reshape(3, 3)[0]))
     k1max = min(K // 2, int(np.floor(np.sqrt(-np.log(1e-9)) * w.params["screen"] * a1 / np.pi)) + 1)
     KK, KH = K ** 3, K * K * (k1max + 1)
-    if stage == "gather":       # potential grid once + real-space energies in + totals out + splines
-        return chunk * KK * 4 + slvmax * chunk * 8 * 2 + natoms * (12 * n + 16)
-    if stage == "bin":          # every target's energy row in, its count row out (one launch per batch)
-        return min(maxdst, 4096) * (slvmax * 8 + ermax * 4)
+    if stage == "gather":       # potential grid once + reciprocal energies out + per-atom and per-molecule records
+        return chunk * KK * 4 + slvmax * chunk * 8 + natoms * (64 if n == 4 else 12 * n + 16) + slvmax * 16
+    if stage == "bin":          # every target's reciprocal and real-space energy rows in, its count row out
+        return min(maxdst, 4096) * (slvmax * 8 * 2 + ermax * 4)
     if stage == "influence":    # spectrum read + write, influence function read
         return chunk * KH * 8 * 2 + KH * 4
     if stage == "pme_plane":    # site tables in, transformed planes out once, influence function in

@@ -791,7 +791,7 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
       }
     }
     acc = warp_sum(acc);
-    if (lane == 0) E[(size_t)k * chunk + b] = acc;
+    if (lane == 0) E[(size_t)b * a.slvmax + k] = acc;
   };
 
   // the cells around the target (all cells when the range covers the box)
@@ -886,7 +886,7 @@ __global__ void __launch_bounds__(kRealMaxThreads) k_real(FrameArgs a, int base,
         acc += (double)pair_energy(a.pp, dis2, lje[lj * ljmax + li], ljs[lj * ljmax + li], xi.w * xj.w);
       }
     }
-    if (lane < qn) E[(size_t)k * chunk + b] = acc;
+    if (lane < qn) E[(size_t)b * a.slvmax + k] = acc;
     __syncwarp();
     if (lane < qn - 32) q[lane] = q[32 + lane];
     qn = qn > 32 ? qn - 32 : 0;
@@ -1538,7 +1538,7 @@ constexpr int kBinThreads = 256;
 constexpr int kMaxSpecSmem = 128;
 
 __global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slvmax, double* __restrict__ Etot,
-    const double* __restrict__ Ereal, int batch,
+    const double* __restrict__ Ereal, bool keep_total,
     const int* __restrict__ molspec, const int* __restrict__ spec_off, const double* __restrict__ uvcrd,
     const int* __restrict__ uvsoft, const int* __restrict__ tgt_mol, const int* __restrict__ skip,
     uint32_t* __restrict__ counts, double* __restrict__ etot, double* __restrict__ flceng, float* __restrict__ minuv,
@@ -1564,13 +1564,26 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slv
   __syncthreads();
   const int excl = tgt_mol ? tgt_mol[cnt] : -1;
   double* row = Etot + (size_t)bi * slvmax;
+  const double* rrow = Ereal ? Ereal + (size_t)bi * slvmax : nullptr;
   double acc = 0.0;
+  // a thread's running minimum and maximum of its current species (exact, order-free), flushed
+  // to shared memory when the species changes: one atomic pair per run instead of per molecule
+  int run_sp = 0;
+  float run_min = FLT_MAX, run_max = -FLT_MAX;
+  auto flush_run = [&]() {
+    if (run_sp > 0 && run_sp < kMaxSpecSmem) {
+      atomic_min_f(&smin[run_sp], run_min);
+      atomic_max_f(&smax[run_sp], run_max);
+    }
+    run_min = FLT_MAX;
+    run_max = -FLT_MAX;
+  };
   for (int k = threadIdx.x; k < slvmax; k += blockDim.x) {
     if (k == excl) continue;
     double e = row[k];
-    if (Ereal) {   // the real-space energy of the pair (molecule-major), added to the reciprocal part
-      e += Ereal[(size_t)k * batch + bi];
-      row[k] = e;
+    if (rrow) {   // the real-space energy of the pair, added to the reciprocal part
+      e += rrow[k];
+      if (keep_total) row[k] = e;
     }
     const int pti = molspec[k];
     if (pti <= 0) { report(st, kErrEngCns, k, cnt, (float)e); continue; }
@@ -1591,8 +1604,12 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slv
     acc += e;
     const float ef = (float)e;
     if (pti < kMaxSpecSmem) {
-      atomic_min_f(&smin[pti], ef);
-      atomic_max_f(&smax[pti], ef);
+      if (pti != run_sp) {
+        flush_run();
+        run_sp = pti;
+      }
+      run_min = fminf(run_min, ef);
+      run_max = fmaxf(run_max, ef);
       if (ba.slttype == ERMOD_SLT_SOLN) atomicAdd(&sfl[pti], e);
     } else {
       atomic_min_f(&minuv[pti], ef);
@@ -1600,6 +1617,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin(BinArgs ba, int bb, int slv
       if (ba.slttype == ERMOD_SLT_SOLN) atomicAdd(&flceng[(size_t)cnt * ba.numslv + pti - 1], e);
     }
   }
+  flush_run();
   acc = warp_sum(acc);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
@@ -1622,7 +1640,9 @@ size_t bin_smem_bytes(const BinArgs& ba) { return sizeof(double) * ba.ermax + si
 void launch_bin(const DeviceState& d, const BinArgs& ba, int bb, int nbatch, int slvmax, int batch,
                 cudaStream_t s) {
   if (nbatch <= 0) return;
-  k_bin<<<nbatch, kBinThreads, bin_smem_bytes(ba), s>>>(ba, bb, slvmax, d.Etot, d.E, batch, d.molspec, d.spec_off,
+  // the summed energies go back to Etot only when the per-molecule energies are kept (uvengy)
+  k_bin<<<nbatch, kBinThreads, bin_smem_bytes(ba), s>>>(ba, bb, slvmax, d.Etot, d.E, d.uvengy != nullptr, d.molspec,
+                                                        d.spec_off,
                                                         d.uvcrd,
                                                         d.uvsoft, d.tgt_mol, d.skip, d.counts, d.etot, d.flceng,
                                                         d.minuv, d.maxuv, d.status);
