@@ -86,8 +86,9 @@ cudaError_t raise_smem_limit(F* kernel, size_t bytes) {
 // Order-4 gather record of one solvent atom, 16 words (64 bytes): the n1 and n2
 // B-spline weights, the atom's charge times the n3 weights (FP32 product), and
 // {float offset of phi(gd.x) of row (gd.z, gd.y), target 0, in the pair layout;
-// flags; gd.x | gd.y << 10 | gd.z << 20; 0}.  kRecWrap: some stencil index wraps.
-constexpr int kRecWords = 16, kRecWrap = 1, kRecOdd = 2;
+// flags; gd.x | gd.y << 10 | gd.z << 20; 0}.  kRecWrap: some stencil index wraps;
+// kRecWrapX: an n1 index wraps (a stencil row is then not contiguous in n1).
+constexpr int kRecWords = 16, kRecWrap = 1, kRecOdd = 2, kRecWrapX = 4;
 // records need the offset in 31 bits and each grid index (0..K) in 10
 __host__ __device__ __forceinline__ bool gather_rec_ok(int order, int K1, int K2, int K3) {
   return order == 4 && K1 < 1024 && K2 < 1024 && K3 < 1024 &&

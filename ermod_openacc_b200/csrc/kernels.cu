@@ -60,14 +60,16 @@ __global__ void k_prepare_solvent(FrameArgs a, const float* __restrict__ posraw,
     grd[i] = make_int4(gi[0], gi[1], gi[2], 0);
     if (grec) {   // order 4 (gather_rec_ok)
       const float q = atom_q[i];
-      const bool wrap = !(gi[0] >= 3 && gi[1] >= 3 && gi[2] >= 3 && gi[0] < a.K1 && gi[1] < a.K2 && gi[2] < a.K3);
+      const bool wrapx = !(gi[0] >= 3 && gi[0] < a.K1);
+      const bool wrap = wrapx || !(gi[1] >= 3 && gi[2] >= 3 && gi[1] < a.K2 && gi[2] < a.K3);
       const int P1 = (a.K1 + 1) / 2;
       const int off = wrap ? 0 : (int)phi_index((size_t)gi[2] * a.K2 + gi[1], gi[0], 0, P1);
       float4* r = reinterpret_cast<float4*>(grec + (size_t)i * kRecWords);
       r[0] = make_float4(wr[0][0], wr[0][1], wr[0][2], wr[0][3]);
       r[1] = make_float4(wr[1][0], wr[1][1], wr[1][2], wr[1][3]);
       r[2] = make_float4(q * wr[2][0], q * wr[2][1], q * wr[2][2], q * wr[2][3]);
-      r[3] = make_float4(__int_as_float(off), __int_as_float((wrap ? kRecWrap : 0) | ((gi[0] & 1) ? kRecOdd : 0)),
+      r[3] = make_float4(__int_as_float(off),
+                         __int_as_float((wrap ? kRecWrap : 0) | (wrapx ? kRecWrapX : 0) | ((gi[0] & 1) ? kRecOdd : 0)),
                          __int_as_float(gi[0] | gi[1] << 10 | gi[2] << 20), 0.f);
     }
   }
@@ -1461,6 +1463,27 @@ __global__ void __launch_bounds__(kGatherThreads, 2) k_gather_rec(FrameArgs a, i
           const float* p0 = phi + (size_t)off + 2 * b;
           if (flags & kRecOdd) gather_rows4<4, true>(p0, s2, s3, 0, v);
           else gather_rows4<4, false>(p0, s2, s3, 0, v);
+        } else if (!(flags & kRecWrapX)) {
+          // only n2 or n3 wraps: each row is contiguous in n1, loaded in pairs as above
+          const int gp = __float_as_int(__shfl_sync(0xffffffffu, rv, src + 14));
+          const int gx = gp & 1023, gy = (gp >> 10) & 1023, gz = gp >> 20;
+          const bool odd = flags & kRecOdd;
+#pragma unroll
+          for (int cs = 0; cs < 4; ++cs) {
+            const int r3 = wrapk(gz - cs, K3);
+#pragma unroll
+            for (int c2 = 0; c2 < 4; ++c2) {
+              const float* r = phi + phi_index((size_t)r3 * K2 + wrapk(gy - c2, K2), gx, b, P1);
+              float* o = v + (cs * 4 + c2) * 4;
+              if (odd) {   // pairs (gx-1, gx) and (gx-3, gx-2)
+                const float2 p = *(const float2*)(r - 1), q = *(const float2*)(r - 1 - 2 * kChunk);
+                o[0] = p.y; o[1] = p.x; o[2] = q.y; o[3] = q.x;
+              } else {     // gx alone, pair (gx-2, gx-1), gx-3 alone
+                const float2 p = *(const float2*)(r - 2 * kChunk);
+                o[0] = r[0]; o[1] = p.y; o[2] = p.x; o[3] = r[-4 * kChunk + 1];
+              }
+            }
+          }
         } else {
           const int gp = __float_as_int(__shfl_sync(0xffffffffu, rv, src + 14));
           const int gx = gp & 1023, gy = (gp >> 10) & 1023, gz = gp >> 20;
