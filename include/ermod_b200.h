@@ -362,9 +362,11 @@ int32_t ermod_get_insertion_samples(ermod_ctx* ctx, float* features, double* eto
 
 /*
  * The proposal network's trainer: hand-written forward, backward and Adam
- * kernels on one device (no reference counterpart).  Loss: mean binary
- * cross-entropy of the logit against labels y in [0, 1].  Batches are host
- * arrays x[n*64], y[n], n <= max_batch.
+ * kernels on one device (no reference counterpart).  The forward pass runs the
+ * three hidden layers on the tensor cores (TF32 inputs, rounded to nearest with
+ * ties away from zero; BF16 weights; FP32 accumulation), the backward pass and
+ * Adam on the CUDA cores.  Loss: mean binary cross-entropy of the logit against
+ * labels y in [0, 1].  Batches are host arrays x[n*64], y[n], n <= max_batch.
  */
 typedef struct ermod_mlp ermod_mlp;
 int32_t ermod_mlp_create(ermod_mlp** out, int32_t device, int32_t max_batch, const float* init_params);
