@@ -58,13 +58,17 @@ __device__ __forceinline__ void min_image(const CellGeom& g, float& x, float& y,
 // Coulomb for one site pair at squared distance dis2 (realcal.F90:129-197).
 // FP32, as the reference's default build.  erfcf replaces 1-erf (more
 // accurate for large arguments; the difference is below FP32 resolution of
-// the pair energy).
+// the pair energy).  One correctly rounded reciprocal square root replaces the
+// reference's sqrt and its two divisions: r = dis2 / sqrt(dis2), sigma^2 / r^2 and
+// q q' erfc / r are products with it, each within two FP32 roundings of the
+// divided form.
 __device__ __forceinline__ float pair_energy(const PairParams& P, float dis2, float ljeps, float ljsgm2,
                                              float qq) {
-  const float rst = sqrtf(dis2);
+  const float rinv = __frsqrt_rn(dis2);
+  const float rst = dis2 > 0.0f ? dis2 * rinv : 0.0f;   // coincident sites: r = 0, as sqrt gives
   float eplj = 0.0f;
   if (!(rst > P.up)) {
-    const float invr2 = ljsgm2 / dis2;
+    const float invr2 = ljsgm2 * (rinv * rinv);
     const float invr6 = invr2 * invr2 * invr2;
     if (P.ljswitch <= 1) {
       eplj = 4.0f * ljeps * invr6 * (invr6 - 1.0f);
@@ -109,7 +113,7 @@ __device__ __forceinline__ float pair_energy(const PairParams& P, float dis2, fl
     }
   }
   float epcl = 0.0f;
-  if (rst < P.reelcut) epcl = P.bare ? qq / rst : qq * erfcf(P.screen * rst) / rst;
+  if (rst < P.reelcut) epcl = P.bare ? qq * rinv : qq * erfcf(P.screen * rst) * rinv;
   return eplj + epcl;
 }
 
