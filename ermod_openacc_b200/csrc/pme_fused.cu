@@ -33,10 +33,12 @@
 // rounded to FP32.  All sums run in a fixed order, so results are bitwise
 // reproducible.  The result equals spreading + R2C + influence + C2R of the
 // cuFFT path up to FP32 rounding.
+#include <algorithm>
 #include <cmath>
 
 #include "engine.cuh"
 #include "regfft.cuh"
+#include "tc_sm100.cuh"
 
 namespace erm {
 
@@ -200,15 +202,143 @@ __global__ void __launch_bounds__(256) k_site_tables(FrameArgs a, int base, int 
 }
 
 // ---------------------------------------------------------------------------
+// Direct site sums on the tensor cores (64 x 64 planes, up to 16 sites).  For one
+// (target, k1) plane X(k3, k2) = sum_s B3_s(k3) D_s(k2), D_s = q_s B1_s(k1) B2_s(k2), as
+// one real product of a 128 x 32 by a 32 x 64 operand: rows m < 64 give Re X(k3 = m),
+// rows m >= 64 Im X(k3 = m - 64); column k = 2 s + part.  A(m, 2s) = Re B3, A(m, 2s+1) =
+// -Im B3 for the real rows, Im B3 and Re B3 for the imaginary ones; B(k2, 2s) = Re D,
+// B(k2, 2s+1) = Im D.  Every value is split into two TF32 terms (hi = v rounded to TF32,
+// lo = v - hi rounded again) and the three products hi*hi, hi*lo and lo*hi are
+// accumulated in FP32 in TMEM (`tcgen05.mma kind::tf32`, M = 128, N = 64, K = 8 a step):
+// the dropped lo*lo term and the split's rounding are below 2^-22 of each product, the
+// FP32 level of the CUDA-core sums it replaces.
+// ---------------------------------------------------------------------------
+namespace tcs {
+constexpr int kRows = 128, kCols = 64, kK = 32, kMaxSites = kK / 2;
+constexpr int kAB = kRows * kK * 4, kBB = kCols * kK * 4;          // bytes of one A / B operand (TF32)
+constexpr int kOperandBytes = 2 * kAB + 2 * kBB;                   // hi and lo of each
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kCols >> 3) << 17) |
+                            ((uint32_t)(kRows >> 4) << 24);        // kind::tf32, D = F32, K-major A and B
+
+__device__ __forceinline__ uint32_t tf32_bits(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+// element (row, k) of a 128-byte-swizzled K-major tile, 32 TF32 a row
+__device__ __forceinline__ uint32_t* slot(unsigned char* tile, int row, int k) {
+  return (uint32_t*)(tile + tc::swz(row, k >> 2)) + (k & 3);
+}
+// the pair (v0, v1) at columns (k, k + 1), k even: one 8-byte store into each of hi and lo
+__device__ __forceinline__ void put_split2(unsigned char* hi, unsigned char* lo, int row, int k, float v0, float v1) {
+  const uint32_t h0 = tf32_bits(v0), h1 = tf32_bits(v1);
+  *reinterpret_cast<uint2*>(slot(hi, row, k)) = make_uint2(h0, h1);
+  *reinterpret_cast<uint2*>(slot(lo, row, k)) =
+      make_uint2(tf32_bits(v0 - __uint_as_float(h0)), tf32_bits(v1 - __uint_as_float(h1)));
+}
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+// X of plane k1 of the target whose site tables start at pair0, into plane[k3 * PITCH + k2]
+// (re, im).  `opnd` (kOperandBytes, 1024-byte aligned) may alias the plane: the operands are
+// dead once the MMAs have completed, before the plane is written.  NTHR threads, 8 warps.
+template <int PITCH, int NTHR>
+__device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, int nk, int Kh1, int k1,
+                          unsigned char* opnd, float2* plane, uint64_t* bar, uint32_t* tmem_slot,
+                          int* __restrict__ errflags) {
+  static_assert(NTHR == 256, "eight warps: four TMEM lane quarters by two column halves");
+  using namespace tc;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  unsigned char* ahi = opnd;
+  unsigned char* alo = ahi + kAB;
+  unsigned char* bhi = alo + kAB;
+  unsigned char* blo = bhi + kBB;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // K steps of 8 columns that the s sites fill; the columns past 2 s of the last step are zeroed
+  const int nks = (2 * s + 7) / 8;
+  if (2 * s < 8 * nks) {
+    const int k0 = 2 * s, k1e = 8 * nks;                   // zero columns [k0, k1e), even bounds
+    const int per = (k1e - k0) / 2;                        // column pairs a row
+    for (int x = tid; x < (kRows + kCols) * per; x += NTHR) {
+      const int r = x / per, k = k0 + 2 * (x - r * per);
+      if (r < kRows) {
+        *reinterpret_cast<uint2*>(slot(ahi, r, k)) = make_uint2(0u, 0u);
+        *reinterpret_cast<uint2*>(slot(alo, r, k)) = make_uint2(0u, 0u);
+      } else {
+        *reinterpret_cast<uint2*>(slot(bhi, r - kRows, k)) = make_uint2(0u, 0u);
+        *reinterpret_cast<uint2*>(slot(blo, r - kRows, k)) = make_uint2(0u, 0u);
+      }
+    }
+  }
+  for (int e = tid; e < s * 64; e += NTHR) {
+    const int t = e >> 6, q = e & 63;
+    const float2* row = tab + (pair0 + t) * nk;
+    const float2 b3 = row[Kh1 + 64 + q];
+    put_split2(ahi, alo, q, 2 * t, b3.x, -b3.y);
+    put_split2(ahi, alo, 64 + q, 2 * t, b3.y, b3.x);
+    const float2 d = fft::cmul(row[k1], row[Kh1 + q]);   // q B1(k1) B2(k2 = q)
+    put_split2(bhi, blo, q, 2 * t, d.x, d.y);
+  }
+  fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  if (tid == 0) {
+    const uint64_t dah = smem_desc(smem_u32(ahi)), dal = smem_desc(smem_u32(alo));
+    const uint64_t dbh = smem_desc(smem_u32(bhi)), dbl = smem_desc(smem_u32(blo));
+    for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbh + 2 * ks, ks > 0 ? 1u : 0u);
+    for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbl + 2 * ks, 1u);
+    for (int ks = 0; ks < nks; ++ks) mma(tmem, dal + 2 * ks, dbh + 2 * ks, 1u);
+    mma_commit(bar);
+  }
+  // bounded wait; on expiry flag the error and wait (bounded) once more before TMEM is read and freed
+  const bool ok = __syncthreads_and(mbar_wait(bar, 0u)) != 0;
+  if (!ok) {
+    if (tid == 0) atomicOr(errflags, kErrTimeout);
+    mbar_wait(bar, 0u);
+  }
+  tc_fence_after();
+  {
+    const int quarter = warp & 3, half = warp >> 2;
+    uint32_t v[32];
+    tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * 32), v);
+    const int m = quarter * 32 + lane, k3 = m & 63, part = m >> 6;
+    float* dst = reinterpret_cast<float*>(plane + k3 * PITCH + half * 32) + part;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) dst[2 * j] = __uint_as_float(v[j]);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+}
+}  // namespace tcs
+
+// ---------------------------------------------------------------------------
 // k_pme_plane<LK2, LK3, DIRECT>: grid (k1max + 1, targets), K2*K3/E threads.  Thread
 // tid owns the points (k2 = tid mod K2, k3 = (tid / K2) * E + e), e < E.
 // Solute sites are staged ts at a time from the batch's site tables.
 // ---------------------------------------------------------------------------
-template <int LK2, int LK3, bool DIRECT>
+template <int LK2, int LK3, bool DIRECT, bool TCS = false>
 __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::MINB) k_pme_plane(FrameArgs a,
     int tbase, int ts, const float2* __restrict__ tab, const float* __restrict__ stn,
     const float* __restrict__ engfacT, const float2* __restrict__ fft_tw, float2* __restrict__ Y,
-    double* __restrict__ partial) {
+    double* __restrict__ partial, int* __restrict__ errflags) {
   using C = PlaneCfg<LK2, LK3>;
   constexpr int K2 = C::K2, K3 = C::K3, PITCH = C::PITCH, E = C::E, NTHR = C::NTHR;
   extern __shared__ __align__(16) unsigned char psm[];
@@ -230,7 +360,16 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
   float2 acc[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
-  if (!DIRECT && C::FIXED) {
+  if constexpr (TCS) {
+    static_assert(DIRECT && K2 == 64 && K3 == 64, "tensor-core site sums: 64 x 64 planes, direct sums");
+    __shared__ __align__(8) uint64_t tcs_bar;
+    __shared__ uint32_t tcs_tmem;
+    unsigned char* opnd = (unsigned char*)(((uintptr_t)plane + 1023) & ~(uintptr_t)1023);
+    tcs::site_sums<PITCH, NTHR>(tab, pair0, s, nk, Kh1, k1, opnd, plane, &tcs_bar, &tcs_tmem, errflags);
+    float2* mine = plane + k30 * PITCH + k2;
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[e] = mine[e * PITCH];
+  } else if (!DIRECT && C::FIXED) {
     // q_a B1_a(k1) w2 w3 scattered on the (n2, n3) plane: a thread per (site, stencil point),
     // integer atomics in 2^-40 fixed point (exact, order-independent), real then imaginary part
     constexpr double kFix = 1099511627776.0, kUnfix = 1.0 / 1099511627776.0;
@@ -558,6 +697,13 @@ size_t plane_smem(const FrameArgs& a, bool direct) {
   return sizeof(float2) * (size_t)(a.K2 + a.K3) + sizeof(float2) * (size_t)a.K3 * (a.K2 + 1) + tile;
 }
 
+// the tensor-core site-sum variant (64 x 64 planes): twiddles, then the plane or the TF32
+// operands aliased over it, 1024-byte aligned
+size_t plane_smem_tcs() {
+  const size_t plane = sizeof(float2) * 64 * 65;
+  return sizeof(float2) * 128 + 1024 + std::max(plane, (size_t)tcs::kOperandBytes);
+}
+
 size_t rows_smem(const FrameArgs& a) {
   const int M = a.K1 / 2, G2 = 256 / M;
   return sizeof(float2) * (size_t)(a.K1 + M) + sizeof(float2) * (size_t)a.Kh1 * G2 * 33;
@@ -571,6 +717,8 @@ template <int L2, int L3>
 cudaError_t plane_attr(const FrameArgs& a) {
   cudaError_t e = raise_smem_limit(k_pme_plane<L2, L3, true>, plane_smem(a, true));
   if (e == cudaSuccess) e = raise_smem_limit(k_pme_plane<L2, L3, false>, plane_smem(a, false));
+  if constexpr (L2 == 6 && L3 == 6)
+    if (e == cudaSuccess) e = raise_smem_limit(k_pme_plane<6, 6, true, true>, plane_smem_tcs());
   return e;
 }
 
@@ -579,14 +727,23 @@ void plane_launch(const FrameArgs& a, const DeviceState& d, int tbase, int nb, b
   using C = PlaneCfg<L2, L3>;
   const dim3 grid(a.k1max + 1, nb);   // planes above k1max carry no influence-function weight
   const int ts = site_tile(a);
+  int* err = d.status ? &d.status->flags : nullptr;
+  if constexpr (L2 == 6 && L3 == 6) {
+    if (direct && a.nsite <= tcs::kMaxSites) {   // site sums on the tensor cores
+      launch_k(pdl, grid, C::NTHR, plane_smem_tcs(), s, k_pme_plane<6, 6, true, true>, a, tbase, ts,
+               (const float2*)d.sitetab, (const float*)d.sitestn, (const float*)d.engfacT,
+               (const float2*)d.fft_tw, d.spec, d.partial, err);
+      return;
+    }
+  }
   if (direct)
     launch_k(pdl, grid, C::NTHR, plane_smem(a, true), s, k_pme_plane<L2, L3, true>, a, tbase, ts,
              (const float2*)d.sitetab, (const float*)d.sitestn, (const float*)d.engfacT, (const float2*)d.fft_tw,
-             d.spec, d.partial);
+             d.spec, d.partial, err);
   else
     launch_k(pdl, grid, C::NTHR, plane_smem(a, false), s, k_pme_plane<L2, L3, false>, a, tbase, ts,
              (const float2*)d.sitetab, (const float*)d.sitestn, (const float*)d.engfacT, (const float2*)d.fft_tw,
-             d.spec, d.partial);
+             d.spec, d.partial, err);
 }
 }  // namespace
 
