@@ -444,6 +444,7 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   fa.pme = pme; fa.K1 = K1; fa.K2 = K2; fa.K3 = K3; fa.Kh1 = Kh1; fa.nsite = ctx->s; fa.order = order;
   fa.ljtype_max = ctx->ljtype_max;
   if (setup_real_smem(fa) != 0) return bad(ERMOD_ERR_CUDA, "real_smem");
+  if (setup_insert_smem(ctx->s) != 0) return bad(ERMOD_ERR_CUDA, "ins_smem");
   const bool fused_ok = pme && fused_supported(fa);
   if (p.spectrum_path < 0 || p.spectrum_path > 3) return bad(ERMOD_ERR_ARG, "spc_path");
   if (pme && p.spectrum_path >= 2 && !fused_ok) return bad(ERMOD_ERR_UNSUPPORTED, "spc_path");

@@ -244,6 +244,7 @@ void launch_selfreal(const FrameArgs& a, const DeviceState& d, int first, int co
                      cudaStream_t s);
 void launch_real(const FrameArgs& a, const DeviceState& d, int base, int nb, int chunk, int threads, cudaStream_t s);
 int setup_real_smem(const FrameArgs& a);
+int setup_insert_smem(int nsite);
 void launch_fill(float* p, float v, int n, cudaStream_t s);
 // Inputs of the PPPM optimal influence function (recpcal.F90:179-337): the alias sums run
 // over |n_i| <= mmax[i]; gfb[l] are the coefficients of the order-P assignment function's

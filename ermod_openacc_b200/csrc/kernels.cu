@@ -424,7 +424,15 @@ void launch_soln_region(const FrameArgs& a, const DeviceState& d, const SolnChec
                                                        d.ref_bf, d.ref_slt, d.ref_slt_w, d.skip);
 }
 
-__global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int iseed, InsRegion rg,
+// Solutes of up to kInsSmemSites sites are placed in shared memory (a slice of an odd number of
+// float4 per thread, so that the threads' 16-byte accesses fall in distinct banks) and copied out
+// once; larger ones are placed in tgt_raw directly.
+constexpr int kInsThreads = 128, kInsSmemSites = 32;
+__host__ __device__ inline int ins_pitch(int s) { return s | 1; }
+size_t insert_smem(int s) { return s <= kInsSmemSites ? sizeof(float4) * kInsThreads * ins_pitch(s) : 0; }
+
+__global__ void __launch_bounds__(kInsThreads) k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int iseed,
+                         InsRegion rg,
                          const double* __restrict__ aggcen, const float* __restrict__ ref_bf,
                          const float* __restrict__ ref_slt_w, DevStatus* st,
                          int use_conf, int gv, int learned, const double* __restrict__ cdf,
@@ -438,7 +446,9 @@ __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int ise
   const int insposition = rg.insposition, insorient = rg.insorient;
   const float lwreg = rg.lwreg, upreg = rg.upreg;
   const int stnum = *stnum_dev;   // staged per frame, so a captured frame graph replays with the new value
-  float4* out = tgt_raw + (size_t)cnt * s;
+  extern __shared__ float4 ins_site[];
+  float4* const gout = tgt_raw + (size_t)cnt * s;
+  float4* const out = s <= kInsSmemSites ? ins_site + (size_t)threadIdx.x * ins_pitch(s) : gout;
   const float* conf = use_conf ? conf_all + (size_t)3 * s * cnt : bfcoord;
   float msum = 0.0f;
   for (int i = 0; i < s; ++i) {
@@ -649,12 +659,19 @@ __global__ void k_insert(FrameArgs a, const int* __restrict__ stnum_dev, int ise
   } else if (insorient == ERMOD_INSROT_RANDOM) {
     orient(1u);
   }
+  if (out != gout)
+    for (int i = 0; i < s; ++i) gout[i] = out[i];
   finish_target(a, cnt, out, tgt_n + (size_t)cnt * s, tgt_c, qsite);
+}
+
+int setup_insert_smem(int nsite) {
+  return raise_smem_limit(k_insert, insert_smem(nsite)) == cudaSuccess ? 0 : -1;
 }
 
 void launch_insert(const FrameArgs& a, const DeviceState& d, const int* stnum_dev, int iseed, const InsRegion& rg,
                    int use_conf, int gv, int learned, cudaStream_t s) {
-  k_insert<<<(a.maxdst + 127) / 128, 128, 0, s>>>(a, stnum_dev, iseed, rg, d.aggcen, d.ref_bf, d.ref_slt_w, d.status,
+  k_insert<<<(a.maxdst + kInsThreads - 1) / kInsThreads, kInsThreads, insert_smem(a.nsite), s>>>(
+      a, stnum_dev, iseed, rg, d.aggcen, d.ref_bf, d.ref_slt_w, d.status,
                                                     use_conf, gv, learned, d.vcdf, d.vq, d.ins_voxel, d.insw_in,
                                                     d.ins_conf, d.bfcoord, d.slt_mass, d.slt_q, d.tgt_raw, d.tgt_n,
                                                     d.tgt_c);
