@@ -211,10 +211,12 @@ __global__ void __launch_bounds__(256) k_site_tables(FrameArgs a, int base, int 
 // lo = v - hi rounded again) and the three products hi*hi, hi*lo and lo*hi are
 // accumulated in FP32 in TMEM (`tcgen05.mma kind::tf32`, M = 128, N = 64, K = 8 a step):
 // the dropped lo*lo term and the split's rounding are below 2^-22 of each product, the
-// FP32 level of the CUDA-core sums it replaces.
+// FP32 level of the CUDA-core sums it replaces.  More than 16 sites: tiles of 16 sites
+// (K = 32) accumulate in the same TMEM columns, each tile's operands staged once the
+// previous tile's MMAs have completed.
 // ---------------------------------------------------------------------------
 namespace tcs {
-constexpr int kRows = 128, kCols = 64, kK = 32, kMaxSites = kK / 2;
+constexpr int kRows = 128, kCols = 64, kK = 32, kTileSites = kK / 2, kMaxSites = 4 * kTileSites;
 constexpr int kAB = kRows * kK * 4, kBB = kCols * kK * 4;          // bytes of one A / B operand (TF32)
 constexpr int kOperandBytes = 2 * kAB + 2 * kBB;                   // hi and lo of each
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kCols >> 3) << 17) |
@@ -269,49 +271,56 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
     mbar_init(bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // K steps of 8 columns that the s sites fill; the columns past 2 s of the last step are zeroed
-  const int nks = (2 * s + 7) / 8;
-  if (2 * s < 8 * nks) {
-    const int k0 = 2 * s, k1e = 8 * nks;                   // zero columns [k0, k1e), even bounds
-    const int per = (k1e - k0) / 2;                        // column pairs a row
-    for (int x = tid; x < (kRows + kCols) * per; x += NTHR) {
-      const int r = x / per, k = k0 + 2 * (x - r * per);
-      if (r < kRows) {
-        *reinterpret_cast<uint2*>(slot(ahi, r, k)) = make_uint2(0u, 0u);
-        *reinterpret_cast<uint2*>(slot(alo, r, k)) = make_uint2(0u, 0u);
-      } else {
-        *reinterpret_cast<uint2*>(slot(bhi, r - kRows, k)) = make_uint2(0u, 0u);
-        *reinterpret_cast<uint2*>(slot(blo, r - kRows, k)) = make_uint2(0u, 0u);
+  bool ok = true;
+  uint32_t tmem = 0;                                   // read once the first tile's barrier has passed (s >= 1)
+  int tile = 0;
+  for (int t0 = 0; t0 < s && ok; t0 += kTileSites, ++tile) {
+    const int ns = min(kTileSites, s - t0);
+    // K steps of 8 columns that the tile's sites fill; the columns past 2 ns of the last step are zeroed
+    const int nks = (2 * ns + 7) / 8;
+    if (2 * ns < 8 * nks) {
+      const int k0 = 2 * ns, k1e = 8 * nks;                 // zero columns [k0, k1e), even bounds
+      const int per = (k1e - k0) / 2;                       // column pairs a row
+      for (int x = tid; x < (kRows + kCols) * per; x += NTHR) {
+        const int r = x / per, k = k0 + 2 * (x - r * per);
+        if (r < kRows) {
+          *reinterpret_cast<uint2*>(slot(ahi, r, k)) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint2*>(slot(alo, r, k)) = make_uint2(0u, 0u);
+        } else {
+          *reinterpret_cast<uint2*>(slot(bhi, r - kRows, k)) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint2*>(slot(blo, r - kRows, k)) = make_uint2(0u, 0u);
+        }
       }
     }
-  }
-  for (int e = tid; e < s * 64; e += NTHR) {
-    const int t = e >> 6, q = e & 63;
-    const float2* row = tab + (pair0 + t) * nk;
-    const float2 b3 = row[Kh1 + 64 + q];
-    put_split2(ahi, alo, q, 2 * t, b3.x, -b3.y);
-    put_split2(ahi, alo, 64 + q, 2 * t, b3.y, b3.x);
-    const float2 d = fft::cmul(row[k1], row[Kh1 + q]);   // q B1(k1) B2(k2 = q)
-    put_split2(bhi, blo, q, 2 * t, d.x, d.y);
-  }
-  fence_proxy_async();
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-  if (tid == 0) {
-    const uint64_t dah = smem_desc(smem_u32(ahi)), dal = smem_desc(smem_u32(alo));
-    const uint64_t dbh = smem_desc(smem_u32(bhi)), dbl = smem_desc(smem_u32(blo));
-    for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbh + 2 * ks, ks > 0 ? 1u : 0u);
-    for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbl + 2 * ks, 1u);
-    for (int ks = 0; ks < nks; ++ks) mma(tmem, dal + 2 * ks, dbh + 2 * ks, 1u);
-    mma_commit(bar);
-  }
-  // bounded wait; on expiry flag the error and wait (bounded) once more before TMEM is read and freed
-  const bool ok = __syncthreads_and(mbar_wait(bar, 0u)) != 0;
-  if (!ok) {
-    if (tid == 0) atomicOr(errflags, kErrTimeout);
-    mbar_wait(bar, 0u);
+    for (int e = tid; e < ns * 64; e += NTHR) {
+      const int t = e >> 6, q = e & 63;
+      const float2* row = tab + (pair0 + t0 + t) * nk;
+      const float2 b3 = row[Kh1 + 64 + q];
+      put_split2(ahi, alo, q, 2 * t, b3.x, -b3.y);
+      put_split2(ahi, alo, 64 + q, 2 * t, b3.y, b3.x);
+      const float2 d = fft::cmul(row[k1], row[Kh1 + q]);   // q B1(k1) B2(k2 = q)
+      put_split2(bhi, blo, q, 2 * t, d.x, d.y);
+    }
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    tmem = *tmem_slot;
+    if (tid == 0) {
+      const uint64_t dah = smem_desc(smem_u32(ahi)), dal = smem_desc(smem_u32(alo));
+      const uint64_t dbh = smem_desc(smem_u32(bhi)), dbl = smem_desc(smem_u32(blo));
+      for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbh + 2 * ks, (t0 > 0 || ks > 0) ? 1u : 0u);
+      for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbl + 2 * ks, 1u);
+      for (int ks = 0; ks < nks; ++ks) mma(tmem, dal + 2 * ks, dbh + 2 * ks, 1u);
+      mma_commit(bar);
+    }
+    // the tile's MMAs complete before its operands are overwritten or TMEM is read (bounded wait;
+    // on expiry the error is flagged and the kernel waits once more, bounded, before going on)
+    ok = __syncthreads_and(mbar_wait(bar, (uint32_t)(tile & 1))) != 0;
+    if (!ok) {
+      if (tid == 0) atomicOr(errflags, kErrTimeout);
+      mbar_wait(bar, (uint32_t)(tile & 1));
+    }
   }
   tc_fence_after();
   {

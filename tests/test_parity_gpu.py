@@ -457,10 +457,11 @@ def test_runs_are_bit_reproducible(lib, path):
         assert a[k] == b[k]
 
 
-@pytest.mark.parametrize("mesh", [(32, 64, 16), (128, 32, 64), (16, 32, 32)])
+@pytest.mark.parametrize("mesh", [(32, 64, 16), (128, 32, 64), (16, 32, 32), (32, 64, 64)])
 def test_fused_solve_matches_cufft_on_mixed_meshes(lib, mesh):
     """The fused PME solve (both spectrum builds) against spreading + cuFFT on meshes
-    with a different size along every axis."""
+    with a different size along every axis; (32, 64, 64) runs the direct site sums on the
+    tensor cores (64 x 64 planes)."""
     w = S.make_workload(2, small=True, maxins=64)
     prm = dict(w.params, keep_uvengy=1, ms1max=mesh[0], ms2max=mesh[1], ms3max=mesh[2])
     pos, cell = w.frame(0)
@@ -475,6 +476,33 @@ def test_fused_solve_matches_cufft_on_mixed_meshes(lib, mesh):
         u, u0 = out[path]
         check_energies(u, u1)
         np.testing.assert_allclose(u0, u01, rtol=1e-6, atol=2e-5)
+
+
+@pytest.mark.parametrize("path", [2, 3])
+def test_chain_on_64x64_planes_matches_oracle(lib, oracle_mod, path):
+    """The 60-site chain on a (32, 64, 64) mesh: the direct site sums on the tensor cores in
+    four tiles of 16 sites (path 2), and plane spreading (path 3), against the FP64 oracle,
+    with the FP32-reference bar of the chain (no larger error than the reference's own FP32
+    algorithm on the same placements)."""
+    w = S.make_workload(3, small=True, maxins=96)
+    prm = dict(w.params, keep_uvengy=1, spectrum_path=path, ms1max=32, ms2max=64, ms3max=64)
+    eng = Engine(prm, w.topo, w.hist)
+    pos, cell = w.frame(0)
+    assert eng.engconst(1, pos, cell) >= 0
+    u, _ = eng.uvengy()
+    ins, _ = eng.insertions()
+    orc = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist)
+    assert orc.engconst(1, pos, cell, ins_conf=ins) >= 0
+    uo, _ = orc.uvengy()
+    o4 = oracle_mod.Oracle(file_driven(prm), flex_topo(w.topo), w.hist, precision=4)
+    assert o4.engconst(1, pos, cell, ins_conf=ins) >= 0
+    u4, _ = o4.uvengy()
+    soft = np.abs(uo) < 1.0e3
+    e_gpu, e_sp = np.abs(u - uo)[soft], np.abs(u4 - uo)[soft]
+    assert e_gpu.max() <= 1.5 * e_sp.max() + 2e-5
+    assert np.percentile(e_gpu, 99) <= 1.5 * np.percentile(e_sp, 99) + 2e-5
+    assert np.median(e_gpu) <= 2e-5
+    eng.close()
 
 
 # ---------------------------------------------------------------------------
