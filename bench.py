@@ -211,7 +211,7 @@ def profile_table(name: str):
 def bound_from_counters(c: dict) -> str:
     """The resource that bounds a kernel, read from its ncu counters (fractions of peak, stalls
     per issued instruction): the tensor pipe, DRAM, SM issue, the shared-memory / LSU queue
-    (MIO throttle), or -- none of them near its limit -- memory latency."""
+    (MIO throttle), the L1 / shared-memory unit, or -- none of them near its limit -- memory latency."""
     if not c:
         return "unmeasured"
     if c.get("tensor_pipe", 0.0) >= 0.5:
@@ -220,6 +220,8 @@ def bound_from_counters(c: dict) -> str:
         return "hbm"
     if c.get("issue_active", 0.0) >= 0.6 or max(c.get("fma_pipe", 0.0), c.get("lsu_pipe", 0.0)) >= 0.6:
         return "sm-issue"
+    if c.get("l1_frac", 0.0) >= 0.65:
+        return "l1-smem"
     if c.get("stall_mio", 0.0) >= 2.0:
         return "mio-queue"
     return "latency"

@@ -33,6 +33,7 @@ def test_roofline_helpers():
     assert bench.bound_from_counters({"issue_active": 0.65, "fma_pipe": 0.44}) == "sm-issue"
     assert bench.bound_from_counters({"issue_active": 0.3, "dram_frac": 0.1}) == "latency"
     assert bench.bound_from_counters({"issue_active": 0.36, "stall_mio": 4.4}) == "mio-queue"
+    assert bench.bound_from_counters({"issue_active": 0.44, "l1_frac": 0.72, "stall_mio": 2.0}) == "l1-smem"
     table = bench.profile_table("kernel_counters.txt")
     assert set(table) >= {"k_pme_plane", "k_pme_lines", "k_gather_rec", "k_ecorr_tma"}
     assert "fma_pipe" not in table["k_mlp_fwd_tc"]                   # '-': not captured
