@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--maxins", type=int, default=None)
+    ap.add_argument("--spectrum-path", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="PME solute spectrum (configs 2 and 3): 0 automatic, 1 spread + cuFFT, 2 direct site "
+                         "sums, 3 plane spreading")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=500, help="insertions per CPU reference step")
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 4, 5],
@@ -314,6 +317,8 @@ def main():
     if args.config == 5:
         return main_delta_mu(args)
     w = S.make_workload(args.config, maxins=args.maxins)
+    if args.spectrum_path:
+        w.params["spectrum_path"] = args.spectrum_path
     if args.impl == "reference":
         run_reference(args, w)
         return

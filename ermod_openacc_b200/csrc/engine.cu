@@ -107,7 +107,7 @@ struct ermod_ctx {
 // With spectrum_path == 0 the fused solve builds the solute spectrum by direct
 // site sums up to this many sites and by plane spreading + forward FFT above:
 // the sums cost s * K2 * K3 per plane, the FFT a fixed ~K2 * K3 * log(K2 K3).
-constexpr int kDirectAutoSites = 16, kDirectAutoSitesTc = 32;
+constexpr int kDirectAutoSites = 16, kDirectAutoSitesTc64 = 32, kDirectAutoSitesTc128 = 64;
 
 enum Stage { kStPrep = 1, kStIns = 2, kStReal = 3, kStSpread = 4, kStR2C = 5, kStInfl = 6, kStC2R = 7,
              kStGather = 8, kStBin = 9, kStWeights = 10, kStEcorr = 11, kStChunks = 12, kStTranspose = 13,
@@ -448,9 +448,11 @@ int32_t ermod_create(ermod_ctx** out, int32_t device, const ermod_params* prm, c
   const bool fused_ok = pme && fused_supported(fa);
   if (p.spectrum_path < 0 || p.spectrum_path > 3) return bad(ERMOD_ERR_ARG, "spc_path");
   if (pme && p.spectrum_path >= 2 && !fused_ok) return bad(ERMOD_ERR_UNSUPPORTED, "spc_path");
-  // direct site sums up to 16 sites; on 64 x 64 planes they run on the tensor cores and beat
-  // plane spreading up to about 32 sites (measured on the refs ring recipe in 4096 waters)
-  const int direct_auto = (K2 == 64 && K3 == 64) ? kDirectAutoSitesTc : kDirectAutoSites;
+  // direct site sums up to 16 sites; on square 64 and 128 planes they run on the tensor cores
+  // and beat plane spreading up to about 32 sites (64 x 64: ring-recipe solutes in 4096 waters)
+  // and past 60 (128 x 128: the 60-site chain in 32,768 waters, 92.9 against 109.6 ms a frame)
+  const int direct_auto = (K2 == 64 && K3 == 64) ? kDirectAutoSitesTc64
+                          : (K2 == 128 && K3 == 128) ? kDirectAutoSitesTc128 : kDirectAutoSites;
   if (p.spectrum_path == 0) ctx->spath = fused_ok ? (ctx->s <= direct_auto ? 2 : 3) : 1;
   else ctx->spath = p.spectrum_path;
   if (pme) {

@@ -216,11 +216,20 @@ __global__ void __launch_bounds__(256) k_site_tables(FrameArgs a, int base, int 
 // previous tile's MMAs have completed.
 // ---------------------------------------------------------------------------
 namespace tcs {
-constexpr int kRows = 128, kCols = 64, kK = 32, kTileSites = kK / 2, kMaxSites = 4 * kTileSites;
-constexpr int kAB = kRows * kK * 4, kBB = kCols * kK * 4;          // bytes of one A / B operand (TF32)
-constexpr int kOperandBytes = 2 * kAB + 2 * kBB;                   // hi and lo of each
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kCols >> 3) << 17) |
-                            ((uint32_t)(kRows >> 4) << 24);        // kind::tf32, D = F32, K-major A and B
+constexpr int kK = 32, kTileSites = kK / 2, kMaxSites = 4 * kTileSites;
+constexpr int kTileRows = 128;                                     // rows of one MMA (M)
+// A KN x KN plane: 2 KN product rows (Re, then Im, of X(k3)) in 2 KN / 128 M tiles, N = KN columns
+template <int KN>
+struct Shape {
+  static_assert(KN == 64 || KN == 128, "64 x 64 or 128 x 128 planes");
+  static constexpr int kMTiles = 2 * KN / kTileRows;
+  static constexpr int kAB = kTileRows * kK * 4;                  // bytes of one A tile (TF32)
+  static constexpr int kBB = KN * kK * 4;                         // bytes of the B operand
+  static constexpr int kOperandBytes = 2 * (kMTiles * kAB + kBB);  // hi and lo of each
+  static constexpr int kTmemCols = kMTiles * KN;                  // 64 or 256
+  static constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(KN >> 3) << 17) |
+                                     ((uint32_t)(kTileRows >> 4) << 24);   // kind::tf32, D = F32, K-major
+};
 
 __device__ __forceinline__ uint32_t tf32_bits(float x) {
   uint32_t r;
@@ -238,39 +247,45 @@ __device__ __forceinline__ void put_split2(unsigned char* hi, unsigned char* lo,
   *reinterpret_cast<uint2*>(slot(lo, row, k)) =
       make_uint2(tf32_bits(v0 - __uint_as_float(h0)), tf32_bits(v1 - __uint_as_float(h1)));
 }
-__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
   const uint32_t z = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
       :
-      : "r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
 // X of plane k1 of the target whose site tables start at pair0, into plane[k3 * PITCH + k2]
-// (re, im).  `opnd` (kOperandBytes, 1024-byte aligned) may alias the plane: the operands are
-// dead once the MMAs have completed, before the plane is written.  NTHR threads, 8 warps.
-template <int PITCH, int NTHR>
+// (re, im).  Product row r < KN is Re X(k3 = r), r >= KN is Im X(k3 = r - KN); row r lives in
+// M tile r / 128 at tile row r % 128, whose accumulator takes TMEM columns [tile KN, tile KN + KN).
+// `opnd` (Shape<KN>::kOperandBytes, 1024-byte aligned) may alias the plane: the operands are
+// dead once the MMAs have completed, before the plane is written.  NTHR threads, a multiple of 4
+// warps: a warp reads the TMEM lane quarter warp % 4.
+template <int KN, int PITCH, int NTHR>
 __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, int nk, int Kh1, int k1,
                           unsigned char* opnd, float2* plane, uint64_t* bar, uint32_t* tmem_slot,
                           int* __restrict__ errflags) {
-  static_assert(NTHR == 256, "eight warps: four TMEM lane quarters by two column halves");
+  using Sh = Shape<KN>;
+  constexpr int NW = NTHR / 32, MT = Sh::kMTiles;
+  static_assert(NW % 4 == 0, "whole TMEM lane quarters");
   using namespace tc;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  unsigned char* ahi = opnd;
-  unsigned char* alo = ahi + kAB;
-  unsigned char* bhi = alo + kAB;
-  unsigned char* blo = bhi + kBB;
+  unsigned char* ahi = opnd;                          // MT tiles of kAB
+  unsigned char* alo = ahi + MT * Sh::kAB;
+  unsigned char* bhi = alo + MT * Sh::kAB;
+  unsigned char* blo = bhi + Sh::kBB;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(kCols));
+                 "r"(Sh::kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
     mbar_init(bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  auto arow = [&](unsigned char* base, int r) { return base + (r / kTileRows) * Sh::kAB; };
   bool ok = true;
   uint32_t tmem = 0;                                   // read once the first tile's barrier has passed (s >= 1)
   int tile = 0;
@@ -281,23 +296,23 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
     if (2 * ns < 8 * nks) {
       const int k0 = 2 * ns, k1e = 8 * nks;                 // zero columns [k0, k1e), even bounds
       const int per = (k1e - k0) / 2;                       // column pairs a row
-      for (int x = tid; x < (kRows + kCols) * per; x += NTHR) {
+      for (int x = tid; x < (2 * KN + KN) * per; x += NTHR) {
         const int r = x / per, k = k0 + 2 * (x - r * per);
-        if (r < kRows) {
-          *reinterpret_cast<uint2*>(slot(ahi, r, k)) = make_uint2(0u, 0u);
-          *reinterpret_cast<uint2*>(slot(alo, r, k)) = make_uint2(0u, 0u);
+        if (r < 2 * KN) {
+          *reinterpret_cast<uint2*>(slot(arow(ahi, r), r % kTileRows, k)) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint2*>(slot(arow(alo, r), r % kTileRows, k)) = make_uint2(0u, 0u);
         } else {
-          *reinterpret_cast<uint2*>(slot(bhi, r - kRows, k)) = make_uint2(0u, 0u);
-          *reinterpret_cast<uint2*>(slot(blo, r - kRows, k)) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint2*>(slot(bhi, r - 2 * KN, k)) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint2*>(slot(blo, r - 2 * KN, k)) = make_uint2(0u, 0u);
         }
       }
     }
-    for (int e = tid; e < ns * 64; e += NTHR) {
-      const int t = e >> 6, q = e & 63;
+    for (int e = tid; e < ns * KN; e += NTHR) {
+      const int t = e / KN, q = e - t * KN;
       const float2* row = tab + (pair0 + t0 + t) * nk;
-      const float2 b3 = row[Kh1 + 64 + q];
-      put_split2(ahi, alo, q, 2 * t, b3.x, -b3.y);
-      put_split2(ahi, alo, 64 + q, 2 * t, b3.y, b3.x);
+      const float2 b3 = row[Kh1 + KN + q];
+      put_split2(arow(ahi, q), arow(alo, q), q % kTileRows, 2 * t, b3.x, -b3.y);
+      put_split2(arow(ahi, KN + q), arow(alo, KN + q), (KN + q) % kTileRows, 2 * t, b3.y, b3.x);
       const float2 d = fft::cmul(row[k1], row[Kh1 + q]);   // q B1(k1) B2(k2 = q)
       put_split2(bhi, blo, q, 2 * t, d.x, d.y);
     }
@@ -307,11 +322,14 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
     tc_fence_after();
     tmem = *tmem_slot;
     if (tid == 0) {
-      const uint64_t dah = smem_desc(smem_u32(ahi)), dal = smem_desc(smem_u32(alo));
       const uint64_t dbh = smem_desc(smem_u32(bhi)), dbl = smem_desc(smem_u32(blo));
-      for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbh + 2 * ks, (t0 > 0 || ks > 0) ? 1u : 0u);
-      for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbl + 2 * ks, 1u);
-      for (int ks = 0; ks < nks; ++ks) mma(tmem, dal + 2 * ks, dbh + 2 * ks, 1u);
+      for (int mt = 0; mt < MT; ++mt) {
+        const uint32_t d = tmem + (uint32_t)(mt * KN);
+        const uint64_t dah = smem_desc(smem_u32(ahi + mt * Sh::kAB)), dal = smem_desc(smem_u32(alo + mt * Sh::kAB));
+        for (int ks = 0; ks < nks; ++ks) mma(d, dah + 2 * ks, dbh + 2 * ks, Sh::kIdesc, (t0 > 0 || ks > 0) ? 1u : 0u);
+        for (int ks = 0; ks < nks; ++ks) mma(d, dah + 2 * ks, dbl + 2 * ks, Sh::kIdesc, 1u);
+        for (int ks = 0; ks < nks; ++ks) mma(d, dal + 2 * ks, dbh + 2 * ks, Sh::kIdesc, 1u);
+      }
       mma_commit(bar);
     }
     // the tile's MMAs complete before its operands are overwritten or TMEM is read (bounded wait;
@@ -324,17 +342,23 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
   }
   tc_fence_after();
   {
-    const int quarter = warp & 3, half = warp >> 2;
-    uint32_t v[32];
-    tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * 32), v);
-    const int m = quarter * 32 + lane, k3 = m & 63, part = m >> 6;
-    float* dst = reinterpret_cast<float*>(plane + k3 * PITCH + half * 32) + part;
+    // units (M tile, 32-column block) of this warp's lane quarter, shared by the NW / 4 warps of it
+    const int quarter = warp & 3, wq = warp >> 2;
+    constexpr int UNITS = MT * (KN / 32), WPQ = NW / 4;
+    for (int u = wq; u < UNITS; u += WPQ) {
+      const int mt = u / (KN / 32), cb = u - mt * (KN / 32);
+      uint32_t v[32];
+      tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mt * KN + cb * 32), v);
+      const int r = mt * kTileRows + quarter * 32 + lane, k3 = r % KN, part = r / KN;
+      float* dst = reinterpret_cast<float*>(plane + k3 * PITCH + cb * 32) + part;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) dst[2 * j] = __uint_as_float(v[j]);
+      for (int j = 0; j < 32; ++j) dst[2 * j] = __uint_as_float(v[j]);
+    }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Sh::kTmemCols));
 }
 }  // namespace tcs
 
@@ -370,11 +394,11 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
   if constexpr (TCS) {
-    static_assert(DIRECT && K2 == 64 && K3 == 64, "tensor-core site sums: 64 x 64 planes, direct sums");
+    static_assert(DIRECT && K2 == K3 && (K2 == 64 || K2 == 128), "tensor-core site sums: square 64 or 128 planes");
     __shared__ __align__(8) uint64_t tcs_bar;
     __shared__ uint32_t tcs_tmem;
     unsigned char* opnd = (unsigned char*)(((uintptr_t)plane + 1023) & ~(uintptr_t)1023);
-    tcs::site_sums<PITCH, NTHR>(tab, pair0, s, nk, Kh1, k1, opnd, plane, &tcs_bar, &tcs_tmem, errflags);
+    tcs::site_sums<K2, PITCH, NTHR>(tab, pair0, s, nk, Kh1, k1, opnd, plane, &tcs_bar, &tcs_tmem, errflags);
     float2* mine = plane + k30 * PITCH + k2;
 #pragma unroll
     for (int e = 0; e < E; ++e) acc[e] = mine[e * PITCH];
@@ -708,9 +732,10 @@ size_t plane_smem(const FrameArgs& a, bool direct) {
 
 // the tensor-core site-sum variant (64 x 64 planes): twiddles, then the plane or the TF32
 // operands aliased over it, 1024-byte aligned
+template <int KN>
 size_t plane_smem_tcs() {
-  const size_t plane = sizeof(float2) * 64 * 65;
-  return sizeof(float2) * 128 + 1024 + std::max(plane, (size_t)tcs::kOperandBytes);
+  const size_t plane = sizeof(float2) * KN * (KN + 1);
+  return sizeof(float2) * 2 * KN + 1024 + std::max(plane, (size_t)tcs::Shape<KN>::kOperandBytes);
 }
 
 size_t rows_smem(const FrameArgs& a) {
@@ -726,8 +751,8 @@ template <int L2, int L3>
 cudaError_t plane_attr(const FrameArgs& a) {
   cudaError_t e = raise_smem_limit(k_pme_plane<L2, L3, true>, plane_smem(a, true));
   if (e == cudaSuccess) e = raise_smem_limit(k_pme_plane<L2, L3, false>, plane_smem(a, false));
-  if constexpr (L2 == 6 && L3 == 6)
-    if (e == cudaSuccess) e = raise_smem_limit(k_pme_plane<6, 6, true, true>, plane_smem_tcs());
+  if constexpr (L2 == L3 && (L2 == 6 || L2 == 7))
+    if (e == cudaSuccess) e = raise_smem_limit(k_pme_plane<L2, L3, true, true>, plane_smem_tcs<(1 << L2)>());
   return e;
 }
 
@@ -737,9 +762,9 @@ void plane_launch(const FrameArgs& a, const DeviceState& d, int tbase, int nb, b
   const dim3 grid(a.k1max + 1, nb);   // planes above k1max carry no influence-function weight
   const int ts = site_tile(a);
   int* err = d.status ? &d.status->flags : nullptr;
-  if constexpr (L2 == 6 && L3 == 6) {
+  if constexpr (L2 == L3 && (L2 == 6 || L2 == 7)) {
     if (direct && a.nsite <= tcs::kMaxSites) {   // site sums on the tensor cores
-      launch_k(pdl, grid, C::NTHR, plane_smem_tcs(), s, k_pme_plane<6, 6, true, true>, a, tbase, ts,
+      launch_k(pdl, grid, C::NTHR, plane_smem_tcs<(1 << L2)>(), s, k_pme_plane<L2, L3, true, true>, a, tbase, ts,
                (const float2*)d.sitetab, (const float*)d.sitestn, (const float*)d.engfacT,
                (const float2*)d.fft_tw, d.spec, d.partial, err);
       return;

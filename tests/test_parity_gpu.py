@@ -457,11 +457,11 @@ def test_runs_are_bit_reproducible(lib, path):
         assert a[k] == b[k]
 
 
-@pytest.mark.parametrize("mesh", [(32, 64, 16), (128, 32, 64), (16, 32, 32), (32, 64, 64)])
+@pytest.mark.parametrize("mesh", [(32, 64, 16), (128, 32, 64), (16, 32, 32), (32, 64, 64), (32, 128, 128)])
 def test_fused_solve_matches_cufft_on_mixed_meshes(lib, mesh):
     """The fused PME solve (both spectrum builds) against spreading + cuFFT on meshes
-    with a different size along every axis; (32, 64, 64) runs the direct site sums on the
-    tensor cores (64 x 64 planes)."""
+    with a different size along every axis; (32, 64, 64) and (32, 128, 128) run the direct
+    site sums on the tensor cores (square 64 and 128 planes)."""
     w = S.make_workload(2, small=True, maxins=64)
     prm = dict(w.params, keep_uvengy=1, ms1max=mesh[0], ms2max=mesh[1], ms3max=mesh[2])
     pos, cell = w.frame(0)
@@ -478,14 +478,14 @@ def test_fused_solve_matches_cufft_on_mixed_meshes(lib, mesh):
         np.testing.assert_allclose(u0, u01, rtol=1e-6, atol=2e-5)
 
 
-@pytest.mark.parametrize("path", [2, 3])
-def test_chain_on_64x64_planes_matches_oracle(lib, oracle_mod, path):
-    """The 60-site chain on a (32, 64, 64) mesh: the direct site sums on the tensor cores in
-    four tiles of 16 sites (path 2), and plane spreading (path 3), against the FP64 oracle,
+@pytest.mark.parametrize("path,plane", [(2, 64), (3, 64), (2, 128)])
+def test_chain_on_square_planes_matches_oracle(lib, oracle_mod, path, plane):
+    """The 60-site chain on a (32, plane, plane) mesh: the direct site sums on the tensor cores
+    in four tiles of 16 sites (path 2), and plane spreading (path 3), against the FP64 oracle,
     with the FP32-reference bar of the chain (no larger error than the reference's own FP32
     algorithm on the same placements)."""
     w = S.make_workload(3, small=True, maxins=96)
-    prm = dict(w.params, keep_uvengy=1, spectrum_path=path, ms1max=32, ms2max=64, ms3max=64)
+    prm = dict(w.params, keep_uvengy=1, spectrum_path=path, ms1max=32, ms2max=plane, ms3max=plane)
     eng = Engine(prm, w.topo, w.hist)
     pos, cell = w.frame(0)
     assert eng.engconst(1, pos, cell) >= 0
