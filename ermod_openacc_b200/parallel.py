@@ -10,10 +10,13 @@ no exchange inside a frame; a division ends with
   2. sums of avslf, engnorm, engsmpl, eself, slnuv, edens, ecorr
      (engproc.F90:580-595), min / max of minuv / maxuv (engproc.F90:597-602).
 
-The reference reduces to rank 0; here every rank receives the result
-(all-reduce), which rank 0 then normalises exactly as engstore does.  The
-communicator is any torch.distributed group: NCCL for device tensors, gloo
-for host tensors.
+The reference reduces to rank 0; here every rank receives the result, which
+rank 0 then normalises exactly as engstore does.  The sums are formed in rank
+order from an all-gather of every rank's partials, so every rank holds the same
+bits and the result does not depend on the collective's internal reduction order
+(ring or tree, which a library may pick by size and rank count); minima and maxima,
+which are exact in any order, use an all-reduce.  The communicator is any
+torch.distributed group: NCCL for device tensors, gloo for host tensors.
 """
 from __future__ import annotations
 
@@ -48,13 +51,22 @@ def reduce_accumulators(acc: dict, slttype: int, wgtslf: int, temp: float, group
             out["slnuv"] = out["slnuv"] * scale
         out["voffset"] = v_max
 
+    nrank = dist.get_world_size(group=group)
+
     def allsum(x, op=None):
         if x is None:
             return None
         arr = np.asarray(x, dtype=np.float64)
         t = torch.from_numpy(np.ascontiguousarray(arr)).to(dev)
-        dist.all_reduce(t, op=op or dist.ReduceOp.SUM, group=group)
-        r = t.cpu().numpy()
+        if op is not None:                      # MIN / MAX: exact in any order
+            dist.all_reduce(t, op=op, group=group)
+            r = t.cpu().numpy()
+        else:                                   # SUM: in rank order, the same on every rank
+            parts = [torch.empty_like(t) for _ in range(nrank)]
+            dist.all_gather(parts, t, group=group)
+            r = parts[0].cpu().numpy().copy()
+            for p in parts[1:]:
+                r += p.cpu().numpy()
         return r if arr.ndim else float(r)
 
     for k in ("avslf", "engnorm", "engsmpl"):

@@ -73,3 +73,35 @@ def test_two_rank_reduction_matches_one_process(tmp_path, slttype):
     np.testing.assert_allclose(r["avediv"], avediv, rtol=1e-12, atol=1e-12)
     assert r["engsmpl"] == len(u0)
     assert r["minuv"][1] == cnt.min() and r["maxuv"][1] == cnt.max()
+
+
+def _rank_sum(rank, port, nrank, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=nrank)
+    rng = np.random.default_rng(100 + rank)
+    acc = dict(edens=rng.normal(size=NBIN) * 10.0 ** rng.uniform(-8, 8, NBIN), ecorr=None, eself=None, slnuv=None,
+               minuv=None, maxuv=None, avslf=float(rng.normal()), engnorm=float(rng.normal() * 1e6),
+               engsmpl=float(rank + 1), voffset=0.0, voffset_initialized=1)
+    tot = PR.reduce_accumulators(acc, A.SLT_REFS_RIGID, 0, TEMP)
+    np.savez(out + f".{rank}.npz", edens=tot["edens"], engnorm=tot["engnorm"])
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sums_are_in_rank_order_and_identical_on_every_rank(tmp_path):
+    """Three gloo ranks with partials spread over 16 decades: every rank gets the same bits, and
+    they are the sequential sum in rank order."""
+    out = str(tmp_path / "s")
+    mp.spawn(_rank_sum, args=(free_port(), 3, out), nprocs=3, join=True)
+    res = [np.load(out + f".{r}.npz") for r in range(3)]
+    expect = None
+    for r in range(3):
+        rng = np.random.default_rng(100 + r)
+        e = rng.normal(size=NBIN) * 10.0 ** rng.uniform(-8, 8, NBIN)
+        expect = e.copy() if expect is None else expect + e
+    for r in range(3):
+        np.testing.assert_array_equal(res[r]["edens"], expect)
+        assert res[r]["engnorm"] == res[0]["engnorm"]
+
