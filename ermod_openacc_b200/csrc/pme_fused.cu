@@ -217,18 +217,20 @@ __global__ void __launch_bounds__(256) k_site_tables(FrameArgs a, int base, int 
 // ---------------------------------------------------------------------------
 namespace tcs {
 constexpr int kK = 32, kTileSites = kK / 2, kMaxSites = 4 * kTileSites;
-constexpr int kTileRows = 128;                                     // rows of one MMA (M)
-// A KN x KN plane: 2 KN product rows (Re, then Im, of X(k3)) in 2 KN / 128 M tiles, N = KN columns
+constexpr int kRows = 128;                                          // M of every MMA
+// A KN x KN plane, transposed: product row = k2 (KN = 64: rows 64..127 repeat rows 0..63, so
+// that each of the four TMEM lane quarters holds the k2 of the warps that read it), product
+// column = 2 k3 + part (part 0: Re, 1: Im), N = 2 KN.
 template <int KN>
 struct Shape {
   static_assert(KN == 64 || KN == 128, "64 x 64 or 128 x 128 planes");
-  static constexpr int kMTiles = 2 * KN / kTileRows;
-  static constexpr int kAB = kTileRows * kK * 4;                  // bytes of one A tile (TF32)
-  static constexpr int kBB = KN * kK * 4;                         // bytes of the B operand
-  static constexpr int kOperandBytes = 2 * (kMTiles * kAB + kBB);  // hi and lo of each
-  static constexpr int kTmemCols = kMTiles * KN;                  // 64 or 256
-  static constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(KN >> 3) << 17) |
-                                     ((uint32_t)(kTileRows >> 4) << 24);   // kind::tf32, D = F32, K-major
+  static constexpr int kN = 2 * KN;
+  static constexpr int kAB = kRows * kK * 4;                      // bytes of the A operand (TF32)
+  static constexpr int kBB = kN * kK * 4;                         // bytes of the B operand
+  static constexpr int kOperandBytes = 2 * (kAB + kBB);           // hi and lo of each
+  static constexpr int kTmemCols = kN;                            // 128 or 256
+  static constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kN >> 3) << 17) |
+                                     ((uint32_t)(kRows >> 4) << 24);   // kind::tf32, D = F32, K-major
 };
 
 __device__ __forceinline__ uint32_t tf32_bits(float x) {
@@ -257,24 +259,25 @@ __device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, u
       : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
-// X of plane k1 of the target whose site tables start at pair0, into plane[k3 * PITCH + k2]
-// (re, im).  Product row r < KN is Re X(k3 = r), r >= KN is Im X(k3 = r - KN); row r lives in
-// M tile r / 128 at tile row r % 128, whose accumulator takes TMEM columns [tile KN, tile KN + KN).
-// `opnd` (Shape<KN>::kOperandBytes, 1024-byte aligned) may alias the plane: the operands are
-// dead once the MMAs have completed, before the plane is written.  NTHR threads, a multiple of 4
-// warps: a warp reads the TMEM lane quarter warp % 4.
-template <int KN, int PITCH, int NTHR>
-__device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, int nk, int Kh1, int k1,
-                          unsigned char* opnd, float2* plane, uint64_t* bar, uint32_t* tmem_slot,
-                          int* __restrict__ errflags) {
+// X(k3, k2) of plane k1 of the target whose site tables start at pair0, straight into the
+// calling thread's registers in the plane kernel's layout: acc[e] = X(k30 + e, k2) with
+// k2 = tid mod KN, k30 = E (tid / KN).  The product is X^T: A(k2, 2 s + c) = (Re, Im) of
+// D_s(k2) = q B1_s(k1) B2_s(k2); B(2 k3 + p, 2 s + c) = (Re B3, -Im B3) for p = 0 and
+// (Im B3, Re B3) for p = 1.  Thread lane l of warp w reads TMEM lane 32 (w mod 4) + l, which
+// holds k2 = (32 w + l) mod KN (a repeated row when KN = 64), and the 2 E columns of its k3
+// range.  `opnd` (Shape<KN>::kOperandBytes, 1024-byte aligned) may alias the plane buffer, which
+// this function does not write.  NTHR = KN * KN / E threads.
+template <int KN, int E, int NTHR>
+__device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, int nk, int Kh1, int k1, int k30,
+                          unsigned char* opnd, uint64_t* bar, uint32_t* tmem_slot, int* __restrict__ errflags,
+                          float2 (&acc)[E]) {
   using Sh = Shape<KN>;
-  constexpr int NW = NTHR / 32, MT = Sh::kMTiles;
-  static_assert(NW % 4 == 0, "whole TMEM lane quarters");
+  static_assert(NTHR == KN * KN / E && (2 * E) % 32 == 0, "whole 32-column TMEM loads");
   using namespace tc;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  unsigned char* ahi = opnd;                          // MT tiles of kAB
-  unsigned char* alo = ahi + MT * Sh::kAB;
-  unsigned char* bhi = alo + MT * Sh::kAB;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  unsigned char* ahi = opnd;
+  unsigned char* alo = ahi + Sh::kAB;
+  unsigned char* bhi = alo + Sh::kAB;
   unsigned char* blo = bhi + Sh::kBB;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -285,7 +288,6 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
     mbar_init(bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  auto arow = [&](unsigned char* base, int r) { return base + (r / kTileRows) * Sh::kAB; };
   bool ok = true;
   uint32_t tmem = 0;                                   // read once the first tile's barrier has passed (s >= 1)
   int tile = 0;
@@ -296,25 +298,26 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
     if (2 * ns < 8 * nks) {
       const int k0 = 2 * ns, k1e = 8 * nks;                 // zero columns [k0, k1e), even bounds
       const int per = (k1e - k0) / 2;                       // column pairs a row
-      for (int x = tid; x < (2 * KN + KN) * per; x += NTHR) {
+      for (int x = tid; x < (kRows + Sh::kN) * per; x += NTHR) {
         const int r = x / per, k = k0 + 2 * (x - r * per);
-        if (r < 2 * KN) {
-          *reinterpret_cast<uint2*>(slot(arow(ahi, r), r % kTileRows, k)) = make_uint2(0u, 0u);
-          *reinterpret_cast<uint2*>(slot(arow(alo, r), r % kTileRows, k)) = make_uint2(0u, 0u);
+        if (r < kRows) {
+          *reinterpret_cast<uint2*>(slot(ahi, r, k)) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint2*>(slot(alo, r, k)) = make_uint2(0u, 0u);
         } else {
-          *reinterpret_cast<uint2*>(slot(bhi, r - 2 * KN, k)) = make_uint2(0u, 0u);
-          *reinterpret_cast<uint2*>(slot(blo, r - 2 * KN, k)) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint2*>(slot(bhi, r - kRows, k)) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint2*>(slot(blo, r - kRows, k)) = make_uint2(0u, 0u);
         }
       }
     }
     for (int e = tid; e < ns * KN; e += NTHR) {
       const int t = e / KN, q = e - t * KN;
       const float2* row = tab + (pair0 + t0 + t) * nk;
-      const float2 b3 = row[Kh1 + KN + q];
-      put_split2(arow(ahi, q), arow(alo, q), q % kTileRows, 2 * t, b3.x, -b3.y);
-      put_split2(arow(ahi, KN + q), arow(alo, KN + q), (KN + q) % kTileRows, 2 * t, b3.y, b3.x);
       const float2 d = fft::cmul(row[k1], row[Kh1 + q]);   // q B1(k1) B2(k2 = q)
-      put_split2(bhi, blo, q, 2 * t, d.x, d.y);
+      put_split2(ahi, alo, q, 2 * t, d.x, d.y);
+      if (KN == 64) put_split2(ahi, alo, 64 + q, 2 * t, d.x, d.y);
+      const float2 b3 = row[Kh1 + KN + q];                // B3(k3 = q)
+      put_split2(bhi, blo, 2 * q, 2 * t, b3.x, -b3.y);
+      put_split2(bhi, blo, 2 * q + 1, 2 * t, b3.y, b3.x);
     }
     fence_proxy_async();
     tc_fence_before();
@@ -322,14 +325,11 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
     tc_fence_after();
     tmem = *tmem_slot;
     if (tid == 0) {
+      const uint64_t dah = smem_desc(smem_u32(ahi)), dal = smem_desc(smem_u32(alo));
       const uint64_t dbh = smem_desc(smem_u32(bhi)), dbl = smem_desc(smem_u32(blo));
-      for (int mt = 0; mt < MT; ++mt) {
-        const uint32_t d = tmem + (uint32_t)(mt * KN);
-        const uint64_t dah = smem_desc(smem_u32(ahi + mt * Sh::kAB)), dal = smem_desc(smem_u32(alo + mt * Sh::kAB));
-        for (int ks = 0; ks < nks; ++ks) mma(d, dah + 2 * ks, dbh + 2 * ks, Sh::kIdesc, (t0 > 0 || ks > 0) ? 1u : 0u);
-        for (int ks = 0; ks < nks; ++ks) mma(d, dah + 2 * ks, dbl + 2 * ks, Sh::kIdesc, 1u);
-        for (int ks = 0; ks < nks; ++ks) mma(d, dal + 2 * ks, dbh + 2 * ks, Sh::kIdesc, 1u);
-      }
+      for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbh + 2 * ks, Sh::kIdesc, (t0 > 0 || ks > 0) ? 1u : 0u);
+      for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbl + 2 * ks, Sh::kIdesc, 1u);
+      for (int ks = 0; ks < nks; ++ks) mma(tmem, dal + 2 * ks, dbh + 2 * ks, Sh::kIdesc, 1u);
       mma_commit(bar);
     }
     // the tile's MMAs complete before its operands are overwritten or TMEM is read (bounded wait;
@@ -341,19 +341,12 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
     }
   }
   tc_fence_after();
-  {
-    // units (M tile, 32-column block) of this warp's lane quarter, shared by the NW / 4 warps of it
-    const int quarter = warp & 3, wq = warp >> 2;
-    constexpr int UNITS = MT * (KN / 32), WPQ = NW / 4;
-    for (int u = wq; u < UNITS; u += WPQ) {
-      const int mt = u / (KN / 32), cb = u - mt * (KN / 32);
-      uint32_t v[32];
-      tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mt * KN + cb * 32), v);
-      const int r = mt * kTileRows + quarter * 32 + lane, k3 = r % KN, part = r / KN;
-      float* dst = reinterpret_cast<float*>(plane + k3 * PITCH + cb * 32) + part;
 #pragma unroll
-      for (int j = 0; j < 32; ++j) dst[2 * j] = __uint_as_float(v[j]);
-    }
+  for (int c = 0; c < 2 * E; c += 32) {
+    uint32_t v[32];
+    tmem_ld32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(2 * k30 + c), v);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) acc[c / 2 + j] = make_float2(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]));
   }
   tc_fence_before();
   __syncthreads();
@@ -398,10 +391,7 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
     __shared__ __align__(8) uint64_t tcs_bar;
     __shared__ uint32_t tcs_tmem;
     unsigned char* opnd = (unsigned char*)(((uintptr_t)plane + 1023) & ~(uintptr_t)1023);
-    tcs::site_sums<K2, PITCH, NTHR>(tab, pair0, s, nk, Kh1, k1, opnd, plane, &tcs_bar, &tcs_tmem, errflags);
-    float2* mine = plane + k30 * PITCH + k2;
-#pragma unroll
-    for (int e = 0; e < E; ++e) acc[e] = mine[e * PITCH];
+    tcs::site_sums<K2, E, NTHR>(tab, pair0, s, nk, Kh1, k1, k30, opnd, &tcs_bar, &tcs_tmem, errflags, acc);
   } else if (!DIRECT && C::FIXED) {
     // q_a B1_a(k1) w2 w3 scattered on the (n2, n3) plane: a thread per (site, stencil point),
     // integer atomics in 2^-40 fixed point (exact, order-independent), real then imaginary part
