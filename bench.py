@@ -398,8 +398,12 @@ def main():
     nbatch = -(-eng.maxdst // 4096)
     per_batch = ("real", "bin", "ecorr", "site_tables")
     order4 = w.params["splodr"] == 4 and max(w.params["ms1max"], w.params["ms2max"], w.params["ms3max"]) < 1024
+    # square 64 planes with direct site sums on the tensor cores run two planes per CTA
+    pair = (w.params["ms2max"] == 64 and w.params["ms3max"] == 64 and paths["spectrum_path"] == 2
+            and eng.nsite_slt <= 64)
     kname = {"gather": "k_gather_rec" if order4 else "k_gather", "bin": "k_bin", "real": "k_real",
-             "spread": "k_spread_box", "transpose": "k_transpose_phi", "pme_plane": "k_pme_plane",
+             "spread": "k_spread_box", "transpose": "k_transpose_phi",
+             "pme_plane": "k_pme_plane_pair" if pair else "k_pme_plane",
              "pme_rows": "k_pme_lines" if w.params["ms1max"] <= 64 else "k_pme_rows",
              "site_tables": "k_site_tables", "influence": "k_influence", "ecorr": "k_ecorr_tma"}
     counters = profile_table("kernel_counters.txt")

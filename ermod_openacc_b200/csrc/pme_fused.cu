@@ -202,18 +202,17 @@ __global__ void __launch_bounds__(256) k_site_tables(FrameArgs a, int base, int 
 }
 
 // ---------------------------------------------------------------------------
-// Direct site sums on the tensor cores (64 x 64 planes, up to 16 sites).  For one
-// (target, k1) plane X(k3, k2) = sum_s B3_s(k3) D_s(k2), D_s = q_s B1_s(k1) B2_s(k2), as
-// one real product of a 128 x 32 by a 32 x 64 operand: rows m < 64 give Re X(k3 = m),
-// rows m >= 64 Im X(k3 = m - 64); column k = 2 s + part.  A(m, 2s) = Re B3, A(m, 2s+1) =
-// -Im B3 for the real rows, Im B3 and Re B3 for the imaginary ones; B(k2, 2s) = Re D,
-// B(k2, 2s+1) = Im D.  Every value is split into two TF32 terms (hi = v rounded to TF32,
-// lo = v - hi rounded again) and the three products hi*hi, hi*lo and lo*hi are
-// accumulated in FP32 in TMEM (`tcgen05.mma kind::tf32`, M = 128, N = 64, K = 8 a step):
-// the dropped lo*lo term and the split's rounding are below 2^-22 of each product, the
-// FP32 level of the CUDA-core sums it replaces.  More than 16 sites: tiles of 16 sites
-// (K = 32) accumulate in the same TMEM columns, each tile's operands staged once the
-// previous tile's MMAs have completed.
+// Direct site sums on the tensor cores (square 64 and 128 planes, up to 64 sites).  For one
+// (target, k1) plane X(k3, k2) = sum_s B3_s(k3) D_s(k2), D_s = q_s B1_s(k1) B2_s(k2), is formed
+// transposed, as one real product of a 128 x 2s operand A (row k2: Re D, Im D per site) by a
+// 2s x 2K operand B (for each k3 the columns (Re B3, -Im B3) and (Im B3, Re B3)): product row
+// k2, column 2 k3 + part is the real or imaginary part of X(k3, k2).  Every value is split
+// into two TF32 terms (hi = v rounded to TF32, lo = v - hi rounded again) and the three
+// products hi*hi, hi*lo and lo*hi are accumulated in FP32 in TMEM (`tcgen05.mma kind::tf32`,
+// M = 128, N = 2K, K = 8 a step): the dropped lo*lo term and the split's rounding are below
+// 2^-22 of each product, the FP32 level of the CUDA-core sums it replaces.  More than 16
+// sites: tiles of 16 sites (K = 32) accumulate in the same TMEM columns, each tile's operands
+// staged once the previous tile's MMAs have completed.
 // ---------------------------------------------------------------------------
 namespace tcs {
 constexpr int kK = 32, kTileSites = kK / 2, kMaxSites = 4 * kTileSites;
@@ -259,21 +258,20 @@ __device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, u
       : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
-// X(k3, k2) of plane k1 of the target whose site tables start at pair0, straight into the
-// calling thread's registers in the plane kernel's layout: acc[e] = X(k30 + e, k2) with
-// k2 = tid mod KN, k30 = E (tid / KN).  The product is X^T: A(k2, 2 s + c) = (Re, Im) of
-// D_s(k2) = q B1_s(k1) B2_s(k2); B(2 k3 + p, 2 s + c) = (Re B3, -Im B3) for p = 0 and
-// (Im B3, Re B3) for p = 1.  Thread lane l of warp w reads TMEM lane 32 (w mod 4) + l, which
-// holds k2 = (32 w + l) mod KN (a repeated row when KN = 64), and the 2 E columns of its k3
-// range.  `opnd` (Shape<KN>::kOperandBytes, 1024-byte aligned) may alias the plane buffer, which
-// this function does not write.  NTHR = KN * KN / E threads.
-template <int KN, int E, int NTHR>
-__device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, int nk, int Kh1, int k1, int k30,
-                          unsigned char* opnd, uint64_t* bar, uint32_t* tmem_slot, int* __restrict__ errflags,
-                          float2 (&acc)[E]) {
+// The staging, MMAs and bounded wait of site_sums; returns the TMEM address of the product,
+// which the caller reads and then frees with tmem_release.  Rows 0..KN-1 of A hold D_s(k2) of
+// plane k1A of the target whose site tables start at pairA.  KN = 64: rows 64..127 hold those
+// of plane k1B of the target at pairB (zero when k1B < 0).  Two targets take two rounds, each
+// with its own B3 and the other half's A rows zero, accumulating in the same TMEM columns.
+template <int KN, int NTHR>
+__device__ uint32_t site_mma(const float2* __restrict__ tab, size_t pairA, int k1A, size_t pairB, int k1B, int s,
+                             int nk, int Kh1, unsigned char* opnd, uint64_t* bar, uint32_t* tmem_slot,
+                             int* __restrict__ errflags) {
   using Sh = Shape<KN>;
-  static_assert(NTHR == KN * KN / E && (2 * E) % 32 == 0, "whole 32-column TMEM loads");
   using namespace tc;
+  constexpr int NI = kTileSites * KN / NTHR;           // staging items of a thread per loop, full tile
+  static_assert(NI * NTHR == kTileSites * KN, "whole items per thread");
+  constexpr int NB = NI < 4 ? NI : 4;                   // items loaded together (registers)
   const int tid = threadIdx.x, warp = tid >> 5;
   unsigned char* ahi = opnd;
   unsigned char* alo = ahi + Sh::kAB;
@@ -291,7 +289,11 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
   bool ok = true;
   uint32_t tmem = 0;                                   // read once the first tile's barrier has passed (s >= 1)
   int tile = 0;
+  const bool cross = KN == 64 && k1B >= 0 && pairB != pairA;
+  for (int round = 0; round < (cross ? 2 : 1); ++round)
   for (int t0 = 0; t0 < s && ok; t0 += kTileSites, ++tile) {
+    const bool onA = !cross || round == 0, onB = k1B >= 0 && (!cross || round == 1);
+    const size_t pb3 = round == 0 ? pairA : pairB;    // the target whose B3 this round multiplies
     const int ns = min(kTileSites, s - t0);
     // K steps of 8 columns that the tile's sites fill; the columns past 2 ns of the last step are zeroed
     const int nks = (2 * ns + 7) / 8;
@@ -309,15 +311,75 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
         }
       }
     }
-    for (int e = tid; e < ns * KN; e += NTHR) {
-      const int t = e / KN, q = e - t * KN;
-      const float2* row = tab + (pair0 + t0 + t) * nk;
-      const float2 d = fft::cmul(row[k1], row[Kh1 + q]);   // q B1(k1) B2(k2 = q)
-      put_split2(ahi, alo, q, 2 * t, d.x, d.y);
-      if (KN == 64) put_split2(ahi, alo, 64 + q, 2 * t, d.x, d.y);
-      const float2 b3 = row[Kh1 + KN + q];                // B3(k3 = q)
-      put_split2(bhi, blo, 2 * q, 2 * t, b3.x, -b3.y);
-      put_split2(bhi, blo, 2 * q + 1, 2 * t, b3.y, b3.x);
+    // The item orders put the 16 lanes of a half warp on 16 distinct (16-byte chunk, half)
+    // slots of the swizzled rows, so the 8-byte stores are free of bank conflicts: a lane's
+    // chunk is (t / 2) ^ (row mod 8), its half t mod 2.
+    // A rows k2 = q: item bits 0-2 q mod 8, bit 3 t mod 2, bits 4.. q / 8, then t / 2.  Each
+    // loop loads NB items of the thread at a time, then splits and stores them, so that the
+    // table reads are in flight together.
+#pragma unroll 1
+    for (int u0 = 0; u0 < NI; u0 += NB) {
+      const int lim = ((ns + 1) >> 1) * 2 * KN;
+      const bool same = pairB == pairA;
+      float2 c1v[NB], b2v[NB], c1w[NB], b2w[NB];
+#pragma unroll
+      for (int u = 0; u < NB; ++u) {
+        const int x = tid + (u0 + u) * NTHR;
+        const int q = (x & 7) | (((x >> 4) & (KN / 8 - 1)) << 3);
+        const int t = ((x >> 3) & 1) | ((x / (2 * KN)) << 1);
+        const float2 z = make_float2(0.f, 0.f);
+        c1v[u] = z; b2v[u] = z; c1w[u] = z; b2w[u] = z;
+        if (x < lim && t < ns) {
+          const float2* row = tab + (pairA + t0 + t) * nk;
+          b2v[u] = row[Kh1 + q];
+          if (onA) c1v[u] = row[k1A];
+          if (KN == 64 && onB) {
+            const float2* rb = same ? row : tab + (pairB + t0 + t) * nk;
+            c1w[u] = rb[k1B];
+            if (!same) b2w[u] = rb[Kh1 + q];
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < NB; ++u) {
+        const int x = tid + (u0 + u) * NTHR;
+        const int q = (x & 7) | (((x >> 4) & (KN / 8 - 1)) << 3);
+        const int t = ((x >> 3) & 1) | ((x / (2 * KN)) << 1);
+        if (x < lim && t < ns) {
+          const float2 d = fft::cmul(c1v[u], b2v[u]);       // q B1(k1) B2(k2 = q); zero when off
+          put_split2(ahi, alo, q, 2 * t, d.x, d.y);
+          if (KN == 64) {
+            const float2 e = fft::cmul(c1w[u], same ? b2v[u] : b2w[u]);
+            put_split2(ahi, alo, 64 + q, 2 * t, e.x, e.y);
+          }
+        }
+      }
+    }
+    // B row pairs (2 c2, 2 c2 + 1): item bits 0-1 c2 mod 4, bits 2-3 t mod 4, bits 4.. c2 / 4,
+    // then t / 4.  Pair c2 holds k3 = c2.
+#pragma unroll 1
+    for (int u0 = 0; u0 < NI; u0 += NB) {
+      const int lim = ((ns + 3) >> 2) * 4 * KN;
+      float2 v[NB];
+#pragma unroll
+      for (int u = 0; u < NB; ++u) {
+        const int x = tid + (u0 + u) * NTHR;
+        const int c2 = (x & 3) | (((x >> 4) & (KN / 4 - 1)) << 2);
+        const int t = ((x >> 2) & 3) | ((x / (4 * KN)) << 2);
+        const int k3 = c2;
+        v[u] = make_float2(0.f, 0.f);
+        if (x < lim && t < ns) v[u] = tab[(pb3 + t0 + t) * nk + Kh1 + KN + k3];
+      }
+#pragma unroll
+      for (int u = 0; u < NB; ++u) {
+        const int x = tid + (u0 + u) * NTHR;
+        const int c2 = (x & 3) | (((x >> 4) & (KN / 4 - 1)) << 2);
+        const int t = ((x >> 2) & 3) | ((x / (4 * KN)) << 2);
+        if (x < lim && t < ns) {
+          put_split2(bhi, blo, 2 * c2, 2 * t, v[u].x, -v[u].y);
+          put_split2(bhi, blo, 2 * c2 + 1, 2 * t, v[u].y, v[u].x);
+        }
+      }
     }
     fence_proxy_async();
     tc_fence_before();
@@ -327,7 +389,8 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
     if (tid == 0) {
       const uint64_t dah = smem_desc(smem_u32(ahi)), dal = smem_desc(smem_u32(alo));
       const uint64_t dbh = smem_desc(smem_u32(bhi)), dbl = smem_desc(smem_u32(blo));
-      for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbh + 2 * ks, Sh::kIdesc, (t0 > 0 || ks > 0) ? 1u : 0u);
+      for (int ks = 0; ks < nks; ++ks)
+        mma(tmem, dah + 2 * ks, dbh + 2 * ks, Sh::kIdesc, (round > 0 || t0 > 0 || ks > 0) ? 1u : 0u);
       for (int ks = 0; ks < nks; ++ks) mma(tmem, dah + 2 * ks, dbl + 2 * ks, Sh::kIdesc, 1u);
       for (int ks = 0; ks < nks; ++ks) mma(tmem, dal + 2 * ks, dbh + 2 * ks, Sh::kIdesc, 1u);
       mma_commit(bar);
@@ -341,17 +404,41 @@ __device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, i
     }
   }
   tc_fence_after();
+  return tmem;
+}
+
+// every thread's TMEM reads are complete before warp 0 frees the columns
+template <int KN>
+__device__ __forceinline__ void tmem_release(uint32_t tmem) {
+  tc::tc_fence_before();
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Shape<KN>::kTmemCols));
+}
+
+// X(k3, k2) of plane k1 of the target whose site tables start at pair0, straight into the
+// calling thread's registers in the plane kernel's layout: acc[e] = X(k30 + e, k2) with
+// k2 = tid mod KN, k30 = E (tid / KN).  The product is X^T: A(k2, 2 s + c) = (Re, Im) of
+// D_s(k2) = q B1_s(k1) B2_s(k2); B(2 k3 + p, 2 s + c) = (Re B3, -Im B3) for p = 0 and
+// (Im B3, Re B3) for p = 1.  Thread lane l of warp w reads TMEM lane 32 (w mod 4) + l, which
+// holds k2 = (32 w + l) mod KN, and the 2 E columns of its k3 range.  `opnd`
+// (Shape<KN>::kOperandBytes, 1024-byte aligned) may alias the plane buffer, which this
+// function does not write.  NTHR = KN * KN / E threads.
+template <int KN, int E, int NTHR>
+__device__ void site_sums(const float2* __restrict__ tab, size_t pair0, int s, int nk, int Kh1, int k1, int k30,
+                          unsigned char* opnd, uint64_t* bar, uint32_t* tmem_slot, int* __restrict__ errflags,
+                          float2 (&acc)[E]) {
+  static_assert(NTHR == KN * KN / E && (2 * E) % 32 == 0, "whole 32-column TMEM loads");
+  const uint32_t tmem = site_mma<KN, NTHR>(tab, pair0, k1, pair0, k1, s, nk, Kh1, opnd, bar, tmem_slot, errflags);
+  const int warp = threadIdx.x >> 5;
 #pragma unroll
   for (int c = 0; c < 2 * E; c += 32) {
     uint32_t v[32];
-    tmem_ld32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(2 * k30 + c), v);
+    tc::tmem_ld32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(2 * k30 + c), v);
 #pragma unroll
     for (int j = 0; j < 16; ++j) acc[c / 2 + j] = make_float2(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]));
   }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Sh::kTmemCols));
+  tmem_release<KN>(tmem);
 }
 }  // namespace tcs
 
@@ -387,7 +474,7 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
   if constexpr (TCS) {
-    static_assert(DIRECT && K2 == K3 && (K2 == 64 || K2 == 128), "tensor-core site sums: square 64 or 128 planes");
+    static_assert(DIRECT && K2 == K3 && K2 == 128, "tensor-core site sums here: 128 x 128 planes (k_pme_plane_pair: 64)");
     __shared__ __align__(8) uint64_t tcs_bar;
     __shared__ uint32_t tcs_tmem;
     unsigned char* opnd = (unsigned char*)(((uintptr_t)plane + 1023) & ~(uintptr_t)1023);
@@ -534,6 +621,100 @@ __global__ void __launch_bounds__(PlaneCfg<LK2, LK3>::NTHR, PlaneCfg<LK2, LK3>::
     v = warp_sum(v);
     if (tid == 0) partial[(size_t)b * Kh1 + k1] = v;
   }
+  // Launched behind the previous chunk's gather, which reads the potential grid that this
+  // chunk's k1 transform overwrites: this grid does not complete before that gather has.
+  grid_dep_wait();
+}
+
+// ---------------------------------------------------------------------------
+// k_pme_plane_pair<LK>: two planes per CTA, K x K planes (K = 2^LK = 64), 2K threads.  The
+// chunk's planes (target b, k1 <= k1max) are numbered p = b (k1max + 1) + k1 and CTA c takes
+// p = 2c and 2c + 1, so a chunk of 32 targets is at most 32 (k1max + 1) / 2 CTAs, one resident
+// wave at 3 CTAs per SM for k1max < 27.  B3 does not depend on k1, so one tensor-core product
+// serves two planes of a target: A rows 0..63 hold D(k2) of the first plane, rows 64..127
+// those of the second (zero past the chunk's last plane); a pair that spans two targets takes
+// two rounds (tcs::site_mma).  TMEM lane quarter w holds the rows that warp w reads.
+// Thread (half = tid / K, k2 = tid mod K) takes all K of its column from TMEM, applies G,
+// and transforms the column in registers (idft64_reg); one transpose through shared memory
+// hands each thread a row n3 for the second axis, and the rows go back through shared
+// memory so that each warp store is one 256-byte row of Y.
+// Grid ceil(targets (k1max + 1) / 2).
+// ---------------------------------------------------------------------------
+template <int LK>
+__global__ void __launch_bounds__(2 << LK, 3) k_pme_plane_pair(FrameArgs a, int tbase, int nb,
+    const float2* __restrict__ tab, const float* __restrict__ engfacT, Tw64 t64, float2* __restrict__ Y,
+    double* __restrict__ partial, int* __restrict__ errflags) {
+  constexpr int K = 1 << LK, NTHR = 2 * K, P = K + 1;
+  static_assert(K == 64, "64 x 64 planes");
+  extern __shared__ __align__(16) unsigned char psm[];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int half = tid >> LK, i = tid & (K - 1);          // plane of the pair; column k2, later row n3
+  const int kp = a.k1max + 1, p0 = 2 * blockIdx.x;
+  const bool has1 = p0 + 1 < nb * kp;
+  const int b0 = p0 / kp, k1a = p0 - b0 * kp;
+  const int b1 = has1 ? (p0 + 1) / kp : b0, k1b = has1 ? p0 + 1 - b1 * kp : -1;
+  const bool live = half == 0 || has1;
+  const int b = half ? b1 : b0, k1 = half && has1 ? k1b : k1a;
+  const int Kh1 = a.Kh1, s = a.nsite, nk = Kh1 + 2 * K;
+  unsigned char* opnd = (unsigned char*)(((uintptr_t)psm + 1023) & ~(uintptr_t)1023);
+  float2* xp = (float2*)opnd + half * K * P;              // this plane's [n][P], over the dead operands
+  float gv[K];                                            // G of column k2, prefetched during the staging
+  {
+    const float* gk = engfacT + (size_t)k1 * K * K + i;
+#pragma unroll
+    for (int e = 0; e < K; ++e) gv[e] = gk[(size_t)e * K];
+  }
+  __shared__ __align__(8) uint64_t tcs_bar;
+  __shared__ uint32_t tcs_tmem;
+  const uint32_t tmem =
+      tcs::site_mma<K, NTHR>(tab, (size_t)(tbase + b0) * s, k1a, (size_t)(tbase + b1) * s, k1b, s, nk, Kh1,
+                             opnd, &tcs_bar, &tcs_tmem, errflags);
+  // influence function and the plane's share of the self energy (recpcal.F90:482-497);
+  // each mode's G |Qhat|^2 is formed in FP32 (~1e-7 relative) and summed in FP64
+  float2 z[K];
+  double self = 0.0;
+#pragma unroll
+  for (int c = 0; c < 2 * K; c += 32) {
+    uint32_t v[32];
+    tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int k3 = c / 2 + j;
+      const float xr = __uint_as_float(v[2 * j]), xi = __uint_as_float(v[2 * j + 1]), g = gv[k3];
+      self += (double)(g * (xr * xr + xi * xi));
+      z[k3] = make_float2(xr * g, xi * g);
+    }
+  }
+  if (k1 == 0 || 2 * k1 == a.K1) self *= 0.5;
+  tcs::tmem_release<K>(tmem);                             // also: every thread is past the MMAs
+  idft64_reg(z, t64);                                     // column k2: n3 = 4 c + d at z[16 d + c]
+#pragma unroll
+  for (int d = 0; d < 4; ++d)
+#pragma unroll
+    for (int c = 0; c < 16; ++c) xp[(4 * c + d) * P + i] = z[16 * d + c];
+  __syncthreads();
+#pragma unroll
+  for (int k2 = 0; k2 < K; ++k2) z[k2] = xp[i * P + k2];  // row n3 = i
+  idft64_reg(z, t64);                                     // n2 = 4 c + d at z[16 d + c]
+  __syncthreads();
+#pragma unroll
+  for (int d = 0; d < 4; ++d)
+#pragma unroll
+    for (int c = 0; c < 16; ++c) xp[i * P + 4 * c + d] = z[16 * d + c];
+  __syncthreads();
+  grid_dep_launch();                                      // the k1 transform may start filling the tail
+  if (live) {
+    float2* y = Y + ((size_t)b * Kh1 + k1) * K * K + i;
+#pragma unroll 8
+    for (int e = 0; e < K; ++e) y[(size_t)e * K] = xp[e * P + i];
+  }
+  // each plane's share of the self energy over its two warps, in a fixed order; the k1
+  // transform sums the planes of each target (self_energy_sum)
+  __shared__ double red[NTHR / 32];
+  self = warp_sum(self);
+  if ((tid & 31) == 0) red[warp] = self;
+  __syncthreads();
+  if (i == 0 && live) partial[(size_t)b * Kh1 + k1] = red[2 * half] + red[2 * half + 1];
   // Launched behind the previous chunk's gather, which reads the potential grid that this
   // chunk's k1 transform overwrites: this grid does not complete before that gather has.
   grid_dep_wait();
@@ -704,6 +885,15 @@ __global__ void __launch_bounds__(32 * kLineRows, 2) k_pme_lines(FrameArgs a, in
 // host side
 // ---------------------------------------------------------------------------
 namespace {
+Tw64 make_tw64() {
+  Tw64 t;
+  for (int m = 0; m < 64; ++m) {
+    const double ang = 2.0 * kPi * (double)m / 64.0;
+    t.w[m] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
+  }
+  return t;
+}
+
 bool pow2_in(int k, int lo, int hi) { return k >= lo && k <= hi && (k & (k - 1)) == 0; }
 int lg(int k) { int l = 0; while ((1 << l) < k) ++l; return l; }
 
@@ -728,6 +918,15 @@ size_t plane_smem_tcs() {
   return sizeof(float2) * 2 * KN + 1024 + std::max(plane, (size_t)tcs::Shape<KN>::kOperandBytes);
 }
 
+// k_pme_plane_pair<LK>: the TF32 operands and, aliased over them, the two planes' K (K + 1)
+// float2 rows, 1024-byte aligned
+template <int LK>
+size_t plane_smem_pair() {
+  constexpr int K = 1 << LK;
+  const size_t rows = sizeof(float2) * (size_t)(2 * K * (K + 1));
+  return 1024 + std::max(rows, (size_t)tcs::Shape<K>::kOperandBytes);
+}
+
 size_t rows_smem(const FrameArgs& a) {
   const int M = a.K1 / 2, G2 = 256 / M;
   return sizeof(float2) * (size_t)(a.K1 + M) + sizeof(float2) * (size_t)a.Kh1 * G2 * 33;
@@ -741,8 +940,10 @@ template <int L2, int L3>
 cudaError_t plane_attr(const FrameArgs& a) {
   cudaError_t e = raise_smem_limit(k_pme_plane<L2, L3, true>, plane_smem(a, true));
   if (e == cudaSuccess) e = raise_smem_limit(k_pme_plane<L2, L3, false>, plane_smem(a, false));
-  if constexpr (L2 == L3 && (L2 == 6 || L2 == 7))
+  if constexpr (L2 == 7 && L3 == 7)
     if (e == cudaSuccess) e = raise_smem_limit(k_pme_plane<L2, L3, true, true>, plane_smem_tcs<(1 << L2)>());
+  if constexpr (L2 == 6 && L3 == 6)
+    if (e == cudaSuccess) e = raise_smem_limit(k_pme_plane_pair<6>, plane_smem_pair<6>());
   return e;
 }
 
@@ -752,7 +953,16 @@ void plane_launch(const FrameArgs& a, const DeviceState& d, int tbase, int nb, b
   const dim3 grid(a.k1max + 1, nb);   // planes above k1max carry no influence-function weight
   const int ts = site_tile(a);
   int* err = d.status ? &d.status->flags : nullptr;
-  if constexpr (L2 == L3 && (L2 == 6 || L2 == 7)) {
+  if constexpr (L2 == 6 && L3 == 6) {
+    if (direct && a.nsite <= tcs::kMaxSites) {   // site sums on the tensor cores, two planes per CTA
+      static const Tw64 t64 = make_tw64();
+      const int npairs = (nb * (a.k1max + 1) + 1) / 2;
+      launch_k(pdl, dim3(npairs), 2 << L2, plane_smem_pair<6>(), s, k_pme_plane_pair<6>, a, tbase, nb,
+               (const float2*)d.sitetab, (const float*)d.engfacT, t64, d.spec, d.partial, err);
+      return;
+    }
+  }
+  if constexpr (L2 == 7 && L3 == 7) {
     if (direct && a.nsite <= tcs::kMaxSites) {   // site sums on the tensor cores
       launch_k(pdl, grid, C::NTHR, plane_smem_tcs<(1 << L2)>(), s, k_pme_plane<L2, L3, true, true>, a, tbase, ts,
                (const float2*)d.sitetab, (const float*)d.sitestn, (const float*)d.engfacT,
@@ -832,17 +1042,6 @@ void launch_pme_plane(const FrameArgs& a, const DeviceState& d, int tbase, int n
   ERM_PLANE_SIZES(ERM_LAUNCH)
 #undef ERM_LAUNCH
 }
-
-namespace {
-Tw64 make_tw64() {
-  Tw64 t;
-  for (int m = 0; m < 64; ++m) {
-    const double ang = 2.0 * kPi * (double)m / 64.0;
-    t.w[m] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
-  }
-  return t;
-}
-}  // namespace
 
 void launch_pme_rows(const FrameArgs& a, const DeviceState& d, int base, int nb, bool pdl, cudaStream_t s) {
   static const Tw64 tw = make_tw64();

@@ -107,6 +107,31 @@ ERM_HD void idft_reg(float2 (&Z)[1 << LM], const Tw64& t) {
   }
 }
 
+// In-register inverse DFT of length 64, unnormalised, with the outputs in a 4 x 16 order:
+//   x(4 c + d) = sum_k Z[k] exp(+2 pi i k (4 c + d) / 64) is left in Z[16 d + c].
+// One radix-4 step over k = a + 16 b (b < 4) with the twiddle w_64^(a d), then a length-16
+// DFT of each d group:  x(4c + d) = sum_a w_16^(a c) w_64^(a d) sum_b w_4^(b d) Z[a + 16 b].
+ERM_HD void idft64_reg(float2 (&Z)[64], const Tw64& t) {
+#pragma unroll
+  for (int a = 0; a < 16; ++a) {
+    float2 v0 = Z[a], v1 = Z[a + 16], v2 = Z[a + 32], v3 = Z[a + 48];
+    dft4<true>(v0, v1, v2, v3);
+    Z[a] = v0;
+    Z[a + 16] = a == 0 ? v1 : cmul(v1, wplus<64>(t, a));
+    Z[a + 32] = a == 0 ? v2 : cmul(v2, wplus<64>(t, 2 * a));
+    Z[a + 48] = a == 0 ? v3 : cmul(v3, wplus<64>(t, 3 * a));
+  }
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    float2 v[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) v[c] = Z[16 * d + c];
+    idft_reg<4>(v, t);
+#pragma unroll
+    for (int c = 0; c < 16; ++c) Z[16 * d + c] = v[c];
+  }
+}
+
 // Hermitian packing of a half spectrum X[0..M] (X[0], X[M] real) of a real
 // sequence of length K1 = 2M into a length-M complex sequence Z:
 //   Z[k] = (X[k] + conj X[M-k]) + i (X[k] - conj X[M-k]) exp(+2 pi i k / K1),
