@@ -813,28 +813,27 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_pme_rows(FrameArgs a, int ba
 // Grid (K3, K2 / kLineRows), 32 * kLineRows threads; warp j takes row
 // n2 = blockIdx.y * kLineRows + j, lane b the target.  The CTA first stages
 // the half spectra Y[b][k1][n3][n2], k1 <= k1max, of its kLineRows rows and
-// 32 targets in shared memory (16-byte loads along n2; S[k1][n2][b] with a
-// row pitch of kLinePitch, so the staging stores and the per-line reads are
-// free of bank conflicts).  Each thread then packs its line (hermitian_pack),
-// transforms it in registers (idft_reg) and writes the line's M pairs
-// (phi(2n), phi(2n+1)): every store of a warp is one 256-byte row of the
-// insertion-fastest layout.
+// 32 targets in shared memory (16-byte loads along n2), each line's k1 run
+// contiguous: S[j JP + b LP + k1], LP = M + 2, JP = 32 LP + 4.  With these
+// pitches a half warp's 8-byte staging stores and a quarter warp's 16-byte
+// line reads fall on distinct banks, and a thread reads its line in M / 2 + 1
+// 16-byte loads.  Each thread then packs its line (hermitian_pack), transforms
+// it in registers (idft_reg) and writes the line's M pairs (phi(2n), phi(2n+1)):
+// every store of a warp is one 256-byte row of the insertion-fastest layout.
 // ---------------------------------------------------------------------------
-// pitch of the (n2, target) rows of S: 2 * 2q * pitch = 16 q (mod 32) words for the Q = kLineRows / 2
-// float4 of a staging load, so that a half-warp's 64-bit stores hit distinct banks
-constexpr int kLinePitch = kLineRows == 8 ? 34 : 36;
+__host__ __device__ constexpr int line_lp(int M) { return M + 2; }
+__host__ __device__ constexpr int line_jp(int M) { return 32 * line_lp(M) + 4; }
 
-size_t lines_smem(int M) { return sizeof(float2) * (size_t)(M + 1) * kLineRows * kLinePitch; }
+size_t lines_smem(int M) { return sizeof(float2) * (size_t)kLineRows * line_jp(M); }
 
 template <int LM>
 __global__ void __launch_bounds__(32 * kLineRows, 2) k_pme_lines(FrameArgs a, int base, int nb,
     const float2* __restrict__ Y, Tw64 tw, const double* __restrict__ partial, double* __restrict__ selfrec,
     float* __restrict__ phi) {
   constexpr int M = 1 << LM, K1 = 2 * M, Kh1 = M + 1, NT = 32 * kLineRows;
-  constexpr int ROW = kLineRows * kLinePitch;             // float2 per k1 row of S
-  constexpr int Q = kLineRows / 2;                        // float4 per (target, k1): two rows each
-  static_assert(kLineRows == 4 || kLineRows == 8, "4 or 8 rows per CTA");
-  extern __shared__ __align__(16) float2 S[];              // [M + 1][kLineRows][kLinePitch]
+  constexpr int LP = line_lp(M), JP = line_jp(M);
+  static_assert(kLineRows == 4, "staging items: 2 row pairs x 2 k1 x 32 targets per 128 threads");
+  extern __shared__ __align__(16) float2 S[];              // [kLineRows][32][LP] + pads
   const int K2 = a.K2, K3 = a.K3;
   const int tid = threadIdx.x;
   const int n3 = blockIdx.x, n2g = blockIdx.y * kLineRows;
@@ -843,36 +842,45 @@ __global__ void __launch_bounds__(32 * kLineRows, 2) k_pme_lines(FrameArgs a, in
   grid_dep_wait();                                    // the planes of this chunk are complete
   self_energy_sum(a, base, nb, Kh1, partial, selfrec);
   {
-    // staging item (k1, bs, q): the float4 of rows 2q, 2q+1 of target bs at k1
-    const int q = tid & (Q - 1), bs = (tid / Q) & 31;
+    // staging item (u, x = tid): rows 2q, 2q + 1 of target bs at k1 = 2u + kp, one float4;
+    // q = x mod 2, kp = bit 1, bs = bits 2-6, so a warp's loads are 16 whole 32-byte sectors
+    const int q = tid & 1, kp = (tid >> 1) & 1, bs = ((tid >> 2) & 7) | (((tid >> 5) & 3) << 3);
     const bool on = bs < nb;
     const float4* src = (const float4*)(Y + (size_t)bs * Kh1 * plane + (size_t)n3 * K2 + n2g + 2 * q);
-    float2* dst = S + (2 * q) * kLinePitch + bs;
+    float2* dst = S + (2 * q) * JP + bs * LP;
     // every load is issued before the first store, from a clamped (always valid) k1, so that
     // they are all in flight together; rows above k1max and targets past nb are not used
-    constexpr int PER = NT / (32 * Q);                      // k1 rows per pass of the CTA
-    constexpr int NPASS = (M + PER) / PER;                  // passes covering k1 = 0..M
+    constexpr int NPASS = (M + 2) / 2;                      // k1 = 0..M+1 in pairs
+    static_assert(NT == 128, "one k1 pair per pass");
     float4 v[NPASS];
 #pragma unroll
-    for (int u = 0; u < NPASS; ++u) v[u] = __ldg(src + (size_t)min(u * PER + tid / (32 * Q), kmax) * (plane / 2));
+    for (int u = 0; u < NPASS; ++u) v[u] = __ldg(src + (size_t)min(2 * u + kp, kmax) * (plane / 2));
 #pragma unroll
     for (int u = 0; u < NPASS; ++u) {
-      const int k1 = u * PER + tid / (32 * Q);
-      if (k1 <= kmax) {
+      const int k1 = 2 * u + kp;
+      if (k1 <= kmax && k1 <= M) {
         const float4 t = on ? v[u] : make_float4(0.f, 0.f, 0.f, 0.f);
-        dst[k1 * ROW] = make_float2(t.x, t.y);
-        dst[k1 * ROW + kLinePitch] = make_float2(t.z, t.w);
+        dst[k1] = make_float2(t.x, t.y);
+        dst[JP + k1] = make_float2(t.z, t.w);
       }
     }
   }
   __syncthreads();
   grid_dep_launch();                                  // the gather may start filling the tail
   const int b = tid & 31, j = tid >> 5;
-  const float2* line = S + j * kLinePitch + b;
+  const float4* line = reinterpret_cast<const float4*>(S + j * JP + b * LP);
   float2 Z[M];
 #pragma unroll
-  for (int k = 0; k < M; ++k) Z[k] = k <= kmax ? line[k * ROW] : make_float2(0.f, 0.f);
-  const float2 xM = M <= kmax ? line[M * ROW] : make_float2(0.f, 0.f);
+  for (int kk = 0; kk < M / 2; ++kk) {
+    const float4 w = line[kk];
+    Z[2 * kk] = 2 * kk <= kmax ? make_float2(w.x, w.y) : make_float2(0.f, 0.f);
+    Z[2 * kk + 1] = 2 * kk + 1 <= kmax ? make_float2(w.z, w.w) : make_float2(0.f, 0.f);
+  }
+  float2 xM = make_float2(0.f, 0.f);
+  if (M <= kmax) {
+    const float4 w = line[M / 2];
+    xM = make_float2(w.x, w.y);
+  }
   hermitian_pack<LM>(Z, xM, tw);
   idft_reg<LM>(Z, tw);
   // z[n] = (phi(2n), phi(2n+1)): one 8-byte store per pair, a 256-byte row per warp
