@@ -160,7 +160,7 @@ struct DeviceState {
   float2* sitetab = nullptr; // [batch*s*(Kh1 [+K2+K3])] per (target, site) stencil transforms of a batch
   float* sitestn = nullptr;  // [batch*s*(2+2*kMaxOrder)] per (target, site) stencils (plane spreading)
   double* splfc = nullptr;   // [K1+K2+K3]
-  double* E = nullptr;       // [slvmax*batch] real-space energies of the batch, molecule-major
+  double* E = nullptr;       // [batch*slvmax] real-space energies of the batch, target-major
   double* Etot = nullptr;    // [batch*slvmax] total pair energies of the batch, target-major (uvengy layout)
   double* tgtq = nullptr;    // [maxdst] net charge of each target's solute
   double* twt = nullptr;     // [maxdst] total_weight of each target
