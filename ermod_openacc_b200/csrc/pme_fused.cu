@@ -311,73 +311,88 @@ __device__ uint32_t site_mma(const float2* __restrict__ tab, size_t pairA, int k
         }
       }
     }
-    // The item orders put the 16 lanes of a half warp on 16 distinct (16-byte chunk, half)
-    // slots of the swizzled rows, so the 8-byte stores are free of bank conflicts: a lane's
-    // chunk is (t / 2) ^ (row mod 8), its half t mod 2.
-    // A rows k2 = q: item bits 0-2 q mod 8, bit 3 t mod 2, bits 4.. q / 8, then t / 2.  Each
-    // loop loads NB items of the thread at a time, then splits and stores them, so that the
-    // table reads are in flight together.
+    if constexpr (KN == 128) {
+      // 128 x 128 planes (one target, one plane): consecutive lanes take consecutive k2 and k3,
+      // so the table reads are 256-byte runs.  Measured on the 60-site chain, this order keeps
+      // the plane stage at 43 ms a frame where the bank-conflict-free order below took 48.
+      for (int e = tid; e < ns * KN; e += NTHR) {
+        const int t = e / KN, q = e - t * KN;
+        const float2* row = tab + (pairA + t0 + t) * nk;
+        const float2 d = fft::cmul(row[k1A], row[Kh1 + q]);   // q B1(k1) B2(k2 = q)
+        put_split2(ahi, alo, q, 2 * t, d.x, d.y);
+        const float2 b3 = row[Kh1 + KN + q];                  // B3(k3 = q)
+        put_split2(bhi, blo, 2 * q, 2 * t, b3.x, -b3.y);
+        put_split2(bhi, blo, 2 * q + 1, 2 * t, b3.y, b3.x);
+      }
+    } else {
+      // The item orders put the 16 lanes of a half warp on 16 distinct (16-byte chunk, half)
+      // slots of the swizzled rows, so the 8-byte stores are free of bank conflicts: a lane's
+      // chunk is (t / 2) ^ (row mod 8), its half t mod 2.
+      // A rows k2 = q: item bits 0-2 q mod 8, bit 3 t mod 2, bits 4.. q / 8, then t / 2.  Each
+      // loop loads NB items of the thread at a time, then splits and stores them, so that the
+      // table reads are in flight together.
 #pragma unroll 1
-    for (int u0 = 0; u0 < NI; u0 += NB) {
-      const int lim = ((ns + 1) >> 1) * 2 * KN;
-      const bool same = pairB == pairA;
-      float2 c1v[NB], b2v[NB], c1w[NB], b2w[NB];
+      for (int u0 = 0; u0 < NI; u0 += NB) {
+        const int lim = ((ns + 1) >> 1) * 2 * KN;
+        const bool same = pairB == pairA;
+        float2 c1v[NB], b2v[NB], c1w[NB], b2w[NB];
 #pragma unroll
-      for (int u = 0; u < NB; ++u) {
-        const int x = tid + (u0 + u) * NTHR;
-        const int q = (x & 7) | (((x >> 4) & (KN / 8 - 1)) << 3);
-        const int t = ((x >> 3) & 1) | ((x / (2 * KN)) << 1);
-        const float2 z = make_float2(0.f, 0.f);
-        c1v[u] = z; b2v[u] = z; c1w[u] = z; b2w[u] = z;
-        if (x < lim && t < ns) {
-          const float2* row = tab + (pairA + t0 + t) * nk;
-          b2v[u] = row[Kh1 + q];
-          if (onA) c1v[u] = row[k1A];
-          if (KN == 64 && onB) {
-            const float2* rb = same ? row : tab + (pairB + t0 + t) * nk;
-            c1w[u] = rb[k1B];
-            if (!same) b2w[u] = rb[Kh1 + q];
+        for (int u = 0; u < NB; ++u) {
+          const int x = tid + (u0 + u) * NTHR;
+          const int q = (x & 7) | (((x >> 4) & (KN / 8 - 1)) << 3);
+          const int t = ((x >> 3) & 1) | ((x / (2 * KN)) << 1);
+          const float2 z = make_float2(0.f, 0.f);
+          c1v[u] = z; b2v[u] = z; c1w[u] = z; b2w[u] = z;
+          if (x < lim && t < ns) {
+            const float2* row = tab + (pairA + t0 + t) * nk;
+            b2v[u] = row[Kh1 + q];
+            if (onA) c1v[u] = row[k1A];
+            if (KN == 64 && onB) {
+              const float2* rb = same ? row : tab + (pairB + t0 + t) * nk;
+              c1w[u] = rb[k1B];
+              if (!same) b2w[u] = rb[Kh1 + q];
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+          const int x = tid + (u0 + u) * NTHR;
+          const int q = (x & 7) | (((x >> 4) & (KN / 8 - 1)) << 3);
+          const int t = ((x >> 3) & 1) | ((x / (2 * KN)) << 1);
+          if (x < lim && t < ns) {
+            const float2 d = fft::cmul(c1v[u], b2v[u]);       // q B1(k1) B2(k2 = q); zero when off
+            put_split2(ahi, alo, q, 2 * t, d.x, d.y);
+            if (KN == 64) {
+              const float2 e = fft::cmul(c1w[u], same ? b2v[u] : b2w[u]);
+              put_split2(ahi, alo, 64 + q, 2 * t, e.x, e.y);
+            }
           }
         }
       }
-#pragma unroll
-      for (int u = 0; u < NB; ++u) {
-        const int x = tid + (u0 + u) * NTHR;
-        const int q = (x & 7) | (((x >> 4) & (KN / 8 - 1)) << 3);
-        const int t = ((x >> 3) & 1) | ((x / (2 * KN)) << 1);
-        if (x < lim && t < ns) {
-          const float2 d = fft::cmul(c1v[u], b2v[u]);       // q B1(k1) B2(k2 = q); zero when off
-          put_split2(ahi, alo, q, 2 * t, d.x, d.y);
-          if (KN == 64) {
-            const float2 e = fft::cmul(c1w[u], same ? b2v[u] : b2w[u]);
-            put_split2(ahi, alo, 64 + q, 2 * t, e.x, e.y);
-          }
-        }
-      }
-    }
-    // B row pairs (2 c2, 2 c2 + 1): item bits 0-1 c2 mod 4, bits 2-3 t mod 4, bits 4.. c2 / 4,
-    // then t / 4.  Pair c2 holds k3 = c2.
+      // B row pairs (2 c2, 2 c2 + 1): item bits 0-1 c2 mod 4, bits 2-3 t mod 4, bits 4.. c2 / 4,
+      // then t / 4.  Pair c2 holds k3 = c2.
 #pragma unroll 1
-    for (int u0 = 0; u0 < NI; u0 += NB) {
-      const int lim = ((ns + 3) >> 2) * 4 * KN;
-      float2 v[NB];
+      for (int u0 = 0; u0 < NI; u0 += NB) {
+        const int lim = ((ns + 3) >> 2) * 4 * KN;
+        float2 v[NB];
 #pragma unroll
-      for (int u = 0; u < NB; ++u) {
-        const int x = tid + (u0 + u) * NTHR;
-        const int c2 = (x & 3) | (((x >> 4) & (KN / 4 - 1)) << 2);
-        const int t = ((x >> 2) & 3) | ((x / (4 * KN)) << 2);
-        const int k3 = c2;
-        v[u] = make_float2(0.f, 0.f);
-        if (x < lim && t < ns) v[u] = tab[(pb3 + t0 + t) * nk + Kh1 + KN + k3];
-      }
+        for (int u = 0; u < NB; ++u) {
+          const int x = tid + (u0 + u) * NTHR;
+          const int c2 = (x & 3) | (((x >> 4) & (KN / 4 - 1)) << 2);
+          const int t = ((x >> 2) & 3) | ((x / (4 * KN)) << 2);
+          const int k3 = c2;
+          v[u] = make_float2(0.f, 0.f);
+          if (x < lim && t < ns) v[u] = tab[(pb3 + t0 + t) * nk + Kh1 + KN + k3];
+        }
 #pragma unroll
-      for (int u = 0; u < NB; ++u) {
-        const int x = tid + (u0 + u) * NTHR;
-        const int c2 = (x & 3) | (((x >> 4) & (KN / 4 - 1)) << 2);
-        const int t = ((x >> 2) & 3) | ((x / (4 * KN)) << 2);
-        if (x < lim && t < ns) {
-          put_split2(bhi, blo, 2 * c2, 2 * t, v[u].x, -v[u].y);
-          put_split2(bhi, blo, 2 * c2 + 1, 2 * t, v[u].y, v[u].x);
+        for (int u = 0; u < NB; ++u) {
+          const int x = tid + (u0 + u) * NTHR;
+          const int c2 = (x & 3) | (((x >> 4) & (KN / 4 - 1)) << 2);
+          const int t = ((x >> 2) & 3) | ((x / (4 * KN)) << 2);
+          if (x < lim && t < ns) {
+            put_split2(bhi, blo, 2 * c2, 2 * t, v[u].x, -v[u].y);
+            put_split2(bhi, blo, 2 * c2 + 1, 2 * t, v[u].y, v[u].x);
+          }
         }
       }
     }
