@@ -1285,7 +1285,7 @@ void launch_influence(const FrameArgs& a, const DeviceState& d, int base, int nb
 // (the uvengy layout); k_bin adds the real-space energies, so that k_real runs
 // beside the whole PME chain.
 // ---------------------------------------------------------------------------
-constexpr int kGatherThreads = 256;
+constexpr int kGatherThreads = 128;
 constexpr int kMaxDevices = 64;     // per-device caches of launch shapes
 
 // The order-4 stencil rows of CS planes c3 (from c30) of one site, no wrap: v[(cs * 4 + c2) * 4 + c1]
@@ -1335,7 +1335,7 @@ __device__ __forceinline__ void accumulate_planes(const float (&v)[CS * NO * NO]
 }
 
 template <int NO>
-__global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(FrameArgs a, int base, int bb, int nb,
+__global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 4 : 8) k_gather(FrameArgs a, int base, int bb, int nb,
     int chunk, int batch, const int* __restrict__ molsorted, const int* __restrict__ molbeg,
     const float* __restrict__ molq, const float* __restrict__ atom_q, const float* __restrict__ spl,
     const int4* __restrict__ grd, const float* __restrict__ phi, const double* __restrict__ tgtq,
@@ -1439,7 +1439,7 @@ __global__ void __launch_bounds__(kGatherThreads, NO > 0 ? 2 : 4) k_gather(Frame
 // LK1, LK2 > 0: the mesh's K1 = 2^LK1, K2 = 2^LK2 at compile time, so that every stencil row
 // is the site's base pointer plus a constant offset; 0: taken from FrameArgs.
 template <int LK1, int LK2>
-__global__ void __launch_bounds__(kGatherThreads, 2) k_gather_rec(FrameArgs a, int base, int bb, int nb,
+__global__ void __launch_bounds__(kGatherThreads, 4) k_gather_rec(FrameArgs a, int base, int bb, int nb,
     const int4* __restrict__ mrec, const float* __restrict__ grec, const float* __restrict__ phi,
     const double* __restrict__ tgtq, const int* __restrict__ tgt_mol, double* __restrict__ Etot) {
   const int lane = threadIdx.x & 31;
