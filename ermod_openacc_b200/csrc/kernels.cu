@@ -1559,7 +1559,7 @@ void launch_gather(const FrameArgs& a, const DeviceState& d, int base, int bb, i
 #undef ERM_GATHER_REC
     return;
   }
-  if (blocks > 148 * 8) blocks = 148 * 8;
+  if (blocks > 148 * 2048 / kGatherThreads) blocks = 148 * 2048 / kGatherThreads;   // 2048 threads an SM
   if (blocks < 1) blocks = 1;
 #define ERM_GATHER(NO) launch_k(pdl, blocks, kGatherThreads, 0, s, k_gather<NO>, a, base, bb, nb, chunk, batch, \
       (const int*)d.molsorted, (const int*)d.molbeg, (const float*)d.molq, (const float*)d.atom_q,         \
